@@ -1,0 +1,362 @@
+"""Benchmark of the SGEMM / GEMV hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--mode split_bf16x3|split_bf16x6|native]
+
+Workload (one step): C <- 1.5 * A B + 0.5 * C, column-major, m = n = k = 8192,
+fp32 operands i.i.d. U[-1, 1] (seeded), resident in HBM (3 x 256 MiB, larger
+than the 126 MB L2, so no flush is needed between steps), computed by
+coral_sgemm in the selected GEMM mode.  Also measured in the same run: the
+plain-FP32 kernel on the same operands, SGEMV N and T at 8192 x 8192 (GB/s of
+algorithmic traffic), and the max relative error of the headline result
+against the double-double CPU oracle on 4096 sampled entries.
+
+Multi-GPU: replicas only -- every rank runs the same independent workload, no
+collective on the data path; timing is the max over ranks (CUDA events), value
+is the sum of work over that time.
+
+--impl reference times CORAL's own CPU algorithm for the same metric (its
+sgemm_nn blocking and microkernel order restated in C, oracle/oracle.c
+port_sgemm_nn; the Rust crate cannot be built on this host) on a bounded
+sample of the workload, single-threaded as the reference is.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("SGEMM TFLOP/s split-BF16x3 vs plain FP32 @8192 at ≤1e-6 rel err; GEMV GB/s")
+M = N = K = 8192
+ALPHA, BETA = 1.5, 0.5
+GEMV_BYTES = 4 * (M * N + N + 2 * M)  # A once, x once, y read + written
+FP32_FMA_PEAK_TFLOPS = 148 * 128 * 2 * 1.965  # nominal: SMs x FP32 lanes x 2 x max clock (GHz)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), d.get(
+            "bf16_tflops_sustained", 1400.0), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def max_over_ranks(value: float, world: int, cuda: bool) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if cuda else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------------ CPU arm --
+def cpu_sample_tflops(budget_s: float, size: int = 2048):
+    """Times CORAL's restated sgemm_nn on a size^3 sample for ~budget_s seconds."""
+    import oracle
+    rng = np.random.default_rng(0)
+    a = rng.uniform(-1, 1, size * size).astype(np.float32)
+    b = rng.uniform(-1, 1, size * size).astype(np.float32)
+    c = rng.uniform(-1, 1, size * size).astype(np.float32)
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        oracle.port_sgemm_nn(size, size, size, ALPHA, a, size, b, size, BETA, c, size)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s:
+            break
+    return 2.0 * size ** 3 * reps / el / 1e12, reps, el
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    size = 2048
+    for _ in range(args.warmup):
+        cpu_sample_tflops(0.0, size)
+    t0 = time.perf_counter()
+    val, reps, el = cpu_sample_tflops(0.0, size)
+    per = el
+    steps_vals = [val]
+    for _ in range(max(0, args.steps - 1)):
+        v, _, e = cpu_sample_tflops(0.0, size)
+        steps_vals.append(v)
+        per += e
+    total = time.perf_counter() - t0
+    value = 2.0 * size ** 3 * args.steps / total / 1e12
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "sgemm_nn_fp32", "m": size, "n": size, "k": size,
+                   "alpha": ALPHA, "beta": BETA, "sample_of": "8192^3",
+                   "parallelism": "single-thread CPU"},
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": 1, "kind": "port",
+                         "sample": f"sgemm NN {size}^3 per step, CORAL sgemm_nn blocking "
+                                   f"(MC/NC/KC 384/576/256, 8x12 microkernel) restated in C; "
+                                   f"host has {os.cpu_count()} cores, reference is single-threaded"},
+        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm --
+def run_ours(args, world, rank, local):
+    import torch
+
+    import coral_b200 as cb
+    from coral_b200 import _lib
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    mode = {"native": cb.GemmMode.NATIVE, "split_bf16x3": cb.GemmMode.SPLIT_BF16X3,
+            "split_bf16x6": cb.GemmMode.SPLIT_BF16X6}[args.mode]
+    g = torch.Generator(device=dev)
+    g.manual_seed(1234 + rank)
+    A = torch.empty(M * K, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
+    B = torch.empty(K * N, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
+    C0 = torch.empty(M * N, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
+    C = C0.clone()
+    h = cb.handle()
+    stream = torch.cuda.current_stream()
+
+    def step(m_):
+        h.set_gemm_mode(m_)
+        cb.sgemm(0, 0, M, N, K, ALPHA, A, M, B, K, BETA, C, M)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = lib.coral_kernel_launches()
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = lib.coral_kernel_launches() - l0
+        barrier(world)
+        ms = e0.elapsed_time(e1) / steps
+        return max_over_ranks(ms, world, True), launches
+
+    # accuracy of the headline mode on sampled entries (single call from C0)
+    import oracle
+    C.copy_(C0)
+    step(mode)
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(7)
+    ns = 4096
+    ii, jj = rng.integers(0, M, ns), rng.integers(0, N, ns)
+    idx = torch.from_numpy(ii + jj * M).to(dev)
+    got = C[idx].double().cpu().numpy()
+    sub_a = A.cpu().numpy()
+    sub_b = B.cpu().numpy()
+    want, bound = oracle.gemm_sample(0, 0, M, N, K, ALPHA, sub_a, M, sub_b, K, BETA,
+                                     C0.cpu().numpy(), M, ii, jj)
+    del sub_a, sub_b
+    err = np.abs(got - want)
+    acc = {"samples": ns, "max_rel_componentwise": float((err / bound).max()),
+           "max_rel_normwise": float(err.max() / np.abs(want).max()),
+           "max_rel_elementwise_p50": float(np.median(err / np.abs(want)))}
+
+    with ClockSampler(local) as clocks:
+        ms, launches = timed(lambda: step(mode), args.steps, args.warmup)
+    clk = clocks.summary()
+    flops = 2.0 * M * N * K
+    value = world * flops / (ms * 1e-3) / 1e12
+
+    native_ms = None
+    if mode != cb.GemmMode.NATIVE:
+        native_ms, _ = timed(lambda: step(cb.GemmMode.NATIVE), max(2, args.steps // 2), 1)
+    h.set_gemm_mode(mode)
+
+    # GEMV N/T at 8192 x 8192 on the same A
+    x = torch.empty(N, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
+    y = torch.empty(M, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
+    gemv = {}
+    for tr, name in ((0, "n"), (1, "t")):
+        gms, _ = timed(lambda: cb.sgemv(tr, M, N, ALPHA, A, M, x, 1, BETA, y, 1), 20, 3)
+        gemv[name] = GEMV_BYTES / (gms * 1e-3) / 1e9
+
+    hbm, bf16, bf16s, src = peaks()
+    if mode == cb.GemmMode.NATIVE:
+        roof = {"bound": "tensor", "achieved": flops / (ms * 1e-3) / 1e12,
+                "peak": FP32_FMA_PEAK_TFLOPS, "unit": "TFLOP/s",
+                "frac": flops / (ms * 1e-3) / 1e12 / FP32_FMA_PEAK_TFLOPS, "traffic": None,
+                "kernel": "k_gemm_simt<float>", "peak_source": "nominal FP32 FMA pipe (no measured figure)"}
+    else:
+        roof = {"bound": "tensor", "achieved": flops / (ms * 1e-3) / 1e12, "peak": bf16,
+                "unit": "TFLOP/s", "frac": flops / (ms * 1e-3) / 1e12 / bf16, "traffic": None,
+                "kernel": "split GEMM", "peak_source": f"{src} bf16 burst"}
+
+    # e2e through the host-slice C ABI: pinned host operands, H2D + compute + D2H per step
+    e2e = None
+    if not args.skip_e2e:
+        import ctypes
+        Ah = A.cpu().pin_memory()
+        Bh = B.cpu().pin_memory()
+        Ch = C0.cpu().pin_memory()
+        lib.coral_host_set_gemm_mode(int(mode))
+        vp = ctypes.c_void_p
+
+        def host_step():
+            st = lib.coral_host_sgemm(0, 0, M, N, K, ALPHA, vp(Ah.data_ptr()), M, vp(Bh.data_ptr()),
+                                      K, BETA, vp(Ch.data_ptr()), M)
+            if st != 0:
+                raise RuntimeError(f"coral_host_sgemm failed: {st}")
+        host_step()
+        barrier(world)
+        t0 = time.perf_counter()
+        esteps = max(2, args.steps // 2)
+        for _ in range(esteps):
+            host_step()
+        el = (time.perf_counter() - t0) / esteps
+        el = max_over_ranks(el, world, True)
+        e2e = {"value": world * flops / el / 1e12, "unit": "TFLOP/s",
+               "h2d_bytes_per_step": 3 * M * N * 4, "d2h_bytes_per_step": M * N * 4,
+               "ms_per_step": el * 1e3, "timing": "host wall clock around the synchronous call"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        v, reps, el = cpu_sample_tflops(10.0)
+        cpu = {"value": v, "unit": "TFLOP/s", "cores": 1, "kind": "port",
+               "sample": f"sgemm NN 2048^3 x {reps} ({el:.1f} s), CORAL sgemm_nn blocking restated "
+                         f"in C, 1 thread of {os.cpu_count()}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"sgemm_nn_{args.mode}", "m": M, "n": N, "k": K,
+                       "alpha": ALPHA, "beta": BETA, "gemm_mode": args.mode,
+                       "l2": "inputs 768 MiB > L2, no flush", "parallelism": f"replicas x{world}"},
+            "accuracy": acc,
+            "plain_fp32_tflops": (world * flops / (native_ms * 1e-3) / 1e12) if native_ms else value,
+            "gemv_gbs": {"n": gemv["n"], "t": gemv["t"], "peak": hbm,
+                         "frac_n": gemv["n"] / hbm, "frac_t": gemv["t"] / hbm},
+            "roofline": roof, "clocks": clk, "gpu_launches": int(launches),
+            "e2e": e2e, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["native", "split_bf16x3", "split_bf16x6"], default="native")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

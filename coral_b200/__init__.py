@@ -1,0 +1,19 @@
+"""coral_b200 -- CORAL's column-major BLAS API on one NVIDIA B200.
+
+Hand-written sm_100a CUDA kernels behind a C ABI (include/coral_b200.h,
+libcoral_b200.so); this package is the Python mirror of the reference's
+routine signatures (``coral_b200.blas``) plus the ctypes binding
+(``coral_b200._lib``).
+"""
+from .blas import (  # noqa: F401
+    CoralDiagonal, CoralError, CoralTranspose, CoralTriangular, GemmMode, Handle, cgemm,
+    chemv, dgemm, gemm_mode, handle, isamax, saxpy, scopy, sdot, set_gemm_mode, sgemm, sgemv,
+    sger, snrm2, sscal, sswap, ssymv, ssyr, ssyr2, strmv, strsv, zgemm,
+)
+
+__all__ = [
+    "CoralDiagonal", "CoralError", "CoralTranspose", "CoralTriangular", "GemmMode", "Handle",
+    "cgemm", "chemv", "dgemm", "gemm_mode", "handle", "isamax", "saxpy", "scopy", "sdot",
+    "set_gemm_mode", "sgemm", "sgemv", "sger", "snrm2", "sscal", "sswap", "ssymv", "ssyr",
+    "ssyr2", "strmv", "strsv", "zgemm",
+]

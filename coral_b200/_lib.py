@@ -1,0 +1,103 @@
+"""ctypes binding of libcoral_b200.so (the C ABI declared in include/coral_b200.h).
+
+The library is loaded from the package directory, where
+``python -m coral_b200.build`` (or ``__graft_entry__.build()``) puts it.  There
+is no fallback: if the library is missing or cannot be loaded, every call
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libcoral_b200.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "coral_b200.h")
+
+_lib = None
+
+_sz = C.c_size_t
+_i = C.c_int
+_f = C.c_float
+_d = C.c_double
+_vp = C.c_void_p
+_h = C.c_void_p
+_st = C.c_int
+
+# name -> argtypes (restype is coral_status_t = int unless listed in _RESTYPE)
+SIGNATURES = {
+    "coral_create": [C.POINTER(_h)],
+    "coral_destroy": [_h],
+    "coral_set_stream": [_h, _vp],
+    "coral_get_stream": [_h, C.POINTER(_vp)],
+    "coral_set_pointer_mode": [_h, _i],
+    "coral_set_gemm_mode": [_h, _i],
+    "coral_get_gemm_mode": [_h, C.POINTER(_i)],
+    "coral_set_wait_limit": [_h, C.c_uint64],
+    "coral_sync": [_h],
+    "coral_last_bad_arg": [_h],
+    "coral_status_string": [_st],
+    "coral_last_cuda_error": [_h],
+    "coral_abi_version": [],
+    "coral_kernel_launches": [],
+    "coral_sdot": [_h, _sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_saxpy": [_h, _sz, _f, _vp, _sz, _vp, _sz],
+    "coral_snrm2": [_h, _sz, _vp, _sz, _vp],
+    "coral_isamax": [_h, _sz, _vp, _sz, _vp],
+    "coral_scopy": [_h, _sz, _vp, _sz, _vp, _sz],
+    "coral_sswap": [_h, _sz, _vp, _sz, _vp, _sz],
+    "coral_sscal": [_h, _sz, _f, _vp, _sz],
+    "coral_sgemv": [_h, _i, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
+    "coral_ssymv": [_h, _i, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
+    "coral_chemv": [_h, _i, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
+    "coral_strsv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],
+    "coral_strmv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],
+    "coral_sger": [_h, _sz, _sz, _f, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_ssyr": [_h, _i, _sz, _f, _vp, _sz, _vp, _sz],
+    "coral_ssyr2": [_h, _i, _sz, _f, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_sgemm": [_h, _i, _i, _sz, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
+    "coral_dgemm": [_h, _i, _i, _sz, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz],
+    "coral_cgemm": [_h, _i, _i, _sz, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
+    "coral_zgemm": [_h, _i, _i, _sz, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
+    "coral_host_sgemm": [_i, _i, _sz, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
+    "coral_host_sgemv": [_i, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
+    "coral_host_sdot": [_sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_host_saxpy": [_sz, _f, _vp, _sz, _vp, _sz],
+    "coral_host_isamax": [_sz, _vp, _sz, _vp],
+    "coral_host_strsv": [_i, _i, _i, _sz, _vp, _sz, _vp, _sz],
+    "coral_host_set_gemm_mode": [_i],
+}
+
+_RESTYPE = {
+    "coral_last_bad_arg": C.c_int,
+    "coral_status_string": C.c_char_p,
+    "coral_last_cuda_error": C.c_char_p,
+    "coral_abi_version": C.c_int,
+    "coral_kernel_launches": C.c_uint64,
+}
+
+
+def header_symbols(path: str = HEADER) -> list[str]:
+    """Names of every function declared in include/coral_b200.h."""
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(coral_\w+)\s*\(", text)))
+
+
+def load() -> C.CDLL:
+    """Loads the library (once) and declares every signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m coral_b200.build` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(LIB_PATH)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = _RESTYPE.get(name, _st)
+    _lib = lib
+    return lib

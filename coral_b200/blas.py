@@ -1,0 +1,307 @@
+"""CORAL's BLAS API over the B200 engine.
+
+Every function keeps the name, argument order and argument meaning of the
+reference routine it replaces (coral-aarch64/src/level{1,2,3}); matrices and
+vectors are CUDA tensors (``torch.Tensor`` on an sm_100 device) whose storage
+plays the role of the reference's slices/pointers, and work is enqueued on
+PyTorch's current stream.  Routines that update in place (``y``, ``x``, ``c``,
+``matrix``) update the tensor passed in; routines that return a value in the
+reference (``sdot``, ``snrm2``, ``isamax``) return it.
+
+Where the reference would ``debug_assert!`` (bad increments, short buffers,
+lda too small) these functions raise :class:`CoralError` carrying the BLAS
+argument position, instead of undefined behaviour.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import threading
+
+from . import _lib
+
+
+class CoralTranspose(enum.IntEnum):
+    """coral-aarch64/src/enums.rs:1-6."""
+    NoTranspose = 0
+    Transpose = 1
+    ConjugateTranspose = 2
+
+
+class CoralTriangular(enum.IntEnum):
+    """coral-aarch64/src/enums.rs:8-12."""
+    UpperTriangular = 0
+    LowerTriangular = 1
+
+
+class CoralDiagonal(enum.IntEnum):
+    """coral-aarch64/src/enums.rs:14-18."""
+    UnitDiagonal = 0
+    NonUnitDiagonal = 1
+
+
+class GemmMode(enum.IntEnum):
+    NATIVE = 0
+    SPLIT_BF16X3 = 1
+    OZAKI_INT8 = 2
+    SPLIT_BF16X6 = 3
+
+
+STATUS = {0: "CORAL_OK", 1: "CORAL_ERR_INVALID_ARG", 2: "CORAL_ERR_CUDA",
+          3: "CORAL_ERR_TIMEOUT", 4: "CORAL_ERR_ALLOC", 5: "CORAL_ERR_NOT_SUPPORTED",
+          6: "CORAL_ERR_NO_DEVICE"}
+
+
+class CoralError(RuntimeError):
+    def __init__(self, status: int, routine: str, bad_arg: int = 0, detail: str = ""):
+        self.status = status
+        self.bad_arg = bad_arg
+        msg = f"{routine}: {STATUS.get(status, status)}"
+        if status == 1:
+            msg += f" (argument {bad_arg})"
+        if detail:
+            msg += f": {detail}"
+        super().__init__(msg)
+
+
+class Handle:
+    """Owns a coral_handle_t bound to a CUDA stream."""
+
+    def __init__(self):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        st = self.lib.coral_create(C.byref(h))
+        if st != 0:
+            raise CoralError(st, "coral_create")
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.coral_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def bind_current_stream(self) -> None:
+        import torch
+        self.lib.coral_set_stream(self.h, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+
+    def set_gemm_mode(self, mode: int) -> None:
+        self.check(self.lib.coral_set_gemm_mode(self.h, int(mode)), "coral_set_gemm_mode")
+
+    def gemm_mode(self) -> int:
+        m = C.c_int()
+        self.check(self.lib.coral_get_gemm_mode(self.h, C.byref(m)), "coral_get_gemm_mode")
+        return m.value
+
+    def set_wait_limit(self, spins: int) -> None:
+        self.check(self.lib.coral_set_wait_limit(self.h, spins), "coral_set_wait_limit")
+
+    def sync(self) -> None:
+        self.check(self.lib.coral_sync(self.h), "coral_sync")
+
+    def check(self, status: int, routine: str) -> None:
+        if status != 0:
+            bad = self.lib.coral_last_bad_arg(self.h) if self.h else 0
+            detail = (self.lib.coral_last_cuda_error(self.h) or b"").decode() if status == 2 else ""
+            raise CoralError(status, routine, bad, detail)
+
+    def call(self, name: str, *args) -> None:
+        self.bind_current_stream()
+        self.check(getattr(self.lib, name)(self.h, *args), name)
+
+
+_tls = threading.local()
+
+
+def handle() -> Handle:
+    """This thread's default handle."""
+    h = getattr(_tls, "handle", None)
+    if h is None:
+        h = Handle()
+        _tls.handle = h
+    return h
+
+
+def _ptr(t, dtypes, name: str):
+    """Device address of tensor `t` (None -> NULL)."""
+    if t is None:
+        return None
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if t.dtype not in dtypes:
+        raise TypeError(f"{name} has dtype {t.dtype}, expected one of {dtypes}")
+    return C.c_void_p(t.data_ptr())
+
+
+def _f32():
+    import torch
+    return (torch.float32,)
+
+
+def _f64():
+    import torch
+    return (torch.float64,)
+
+
+def _c64():
+    import torch
+    return (torch.complex64, torch.float32)
+
+
+def _c128():
+    import torch
+    return (torch.complex128, torch.float64)
+
+
+# ---------------------------------------------------------------- level 1 ----
+def sdot(n, x, incx, y, incy) -> float:
+    """level1/sdot.rs:42-161."""
+    r = C.c_float()
+    handle().call("coral_sdot", n, _ptr(x, _f32(), "x"), incx, _ptr(y, _f32(), "y"), incy,
+                  C.cast(C.byref(r), C.c_void_p))
+    return r.value
+
+
+def saxpy(n, alpha, x, incx, y, incy) -> None:
+    """level1/saxpy.rs:42-131 (y updated in place)."""
+    handle().call("coral_saxpy", n, alpha, _ptr(x, _f32(), "x"), incx, _ptr(y, _f32(), "y"), incy)
+
+
+def snrm2(n, x, incx) -> float:
+    """level1/snrm2.rs:45-149."""
+    r = C.c_float()
+    handle().call("coral_snrm2", n, _ptr(x, _f32(), "x"), incx, C.cast(C.byref(r), C.c_void_p))
+    return r.value
+
+
+def isamax(n, x, incx) -> int:
+    """level1/isamax.rs:43-151 (0-based index)."""
+    r = C.c_size_t()
+    handle().call("coral_isamax", n, _ptr(x, _f32(), "x"), incx, C.cast(C.byref(r), C.c_void_p))
+    return r.value
+
+
+def scopy(n, x, incx, y, incy) -> None:
+    """level1/scopy.rs:28-58."""
+    handle().call("coral_scopy", n, _ptr(x, _f32(), "x"), incx, _ptr(y, _f32(), "y"), incy)
+
+
+def sswap(n, x, incx, y, incy) -> None:
+    """level1/sswap.rs:35-118."""
+    handle().call("coral_sswap", n, _ptr(x, _f32(), "x"), incx, _ptr(y, _f32(), "y"), incy)
+
+
+def sscal(n, alpha, x, incx) -> None:
+    """level1/sscal.rs:30-66."""
+    handle().call("coral_sscal", n, alpha, _ptr(x, _f32(), "x"), incx)
+
+
+# ---------------------------------------------------------------- level 2 ----
+def sgemv(trans, n_rows, n_cols, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
+    """level2/sgemv.rs:63-80."""
+    handle().call("coral_sgemv", int(trans), n_rows, n_cols, alpha, _ptr(matrix, _f32(), "matrix"),
+                  lda, _ptr(x, _f32(), "x"), incx, beta, _ptr(y, _f32(), "y"), incy)
+
+
+def ssymv(uplo, n, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
+    """level2/ssymv.rs:99-394."""
+    handle().call("coral_ssymv", int(uplo), n, alpha, _ptr(matrix, _f32(), "matrix"), lda,
+                  _ptr(x, _f32(), "x"), incx, beta, _ptr(y, _f32(), "y"), incy)
+
+
+def _pair(z, ctype):
+    arr = (ctype * 2)(complex(z).real, complex(z).imag)
+    return C.cast(arr, C.c_void_p), arr
+
+
+def chemv(uplo, n, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
+    """level2/chemv.rs:96-447 (alpha/beta: complex or [re, im])."""
+    if isinstance(alpha, (list, tuple)):
+        alpha = complex(alpha[0], alpha[1])
+    if isinstance(beta, (list, tuple)):
+        beta = complex(beta[0], beta[1])
+    pa, ka = _pair(alpha, C.c_float)
+    pb, kb = _pair(beta, C.c_float)
+    handle().call("coral_chemv", int(uplo), n, pa, _ptr(matrix, _c64(), "matrix"), lda,
+                  _ptr(x, _c64(), "x"), incx, pb, _ptr(y, _c64(), "y"), incy)
+
+
+def strsv(uplo, transpose, diagonal, n, matrix, lda, x, incx) -> None:
+    """level2/strsv.rs:60-74 (x solved in place)."""
+    handle().call("coral_strsv", int(uplo), int(transpose), int(diagonal), n,
+                  _ptr(matrix, _f32(), "matrix"), lda, _ptr(x, _f32(), "x"), incx)
+
+
+def strmv(uplo, transpose, diagonal, n, matrix, lda, x, incx) -> None:
+    """level2/strmv.rs:59-73 (x updated in place)."""
+    handle().call("coral_strmv", int(uplo), int(transpose), int(diagonal), n,
+                  _ptr(matrix, _f32(), "matrix"), lda, _ptr(x, _f32(), "x"), incx)
+
+
+def sger(n_rows, n_cols, alpha, x, incx, y, incy, matrix, lda) -> None:
+    """level2/sger.rs:68-132."""
+    handle().call("coral_sger", n_rows, n_cols, alpha, _ptr(x, _f32(), "x"), incx,
+                  _ptr(y, _f32(), "y"), incy, _ptr(matrix, _f32(), "matrix"), lda)
+
+
+def ssyr(uplo, n, alpha, x, incx, matrix, lda) -> None:
+    """level2/ssyr.rs:63-181."""
+    handle().call("coral_ssyr", int(uplo), n, alpha, _ptr(x, _f32(), "x"), incx,
+                  _ptr(matrix, _f32(), "matrix"), lda)
+
+
+def ssyr2(uplo, n, alpha, x, incx, y, incy, matrix, lda) -> None:
+    """level2/ssyr2.rs:59-197."""
+    handle().call("coral_ssyr2", int(uplo), n, alpha, _ptr(x, _f32(), "x"), incx,
+                  _ptr(y, _f32(), "y"), incy, _ptr(matrix, _f32(), "matrix"), lda)
+
+
+# ---------------------------------------------------------------- level 3 ----
+def sgemm(op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> None:
+    """level3/sgemm.rs:106-130; arithmetic per the handle's GEMM mode."""
+    handle().call("coral_sgemm", int(op_a), int(op_b), m, n, k, alpha, _ptr(a, _f32(), "a"), lda,
+                  _ptr(b, _f32(), "b"), ldb, beta, _ptr(c, _f32(), "c"), ldc)
+
+
+def dgemm(op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> None:
+    """level3/dgemm.rs:107."""
+    handle().call("coral_dgemm", int(op_a), int(op_b), m, n, k, alpha, _ptr(a, _f64(), "a"), lda,
+                  _ptr(b, _f64(), "b"), ldb, beta, _ptr(c, _f64(), "c"), ldc)
+
+
+def cgemm(op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> None:
+    """level3/cgemm.rs:127-157 (alpha/beta: complex or [re, im])."""
+    if isinstance(alpha, (list, tuple)):
+        alpha = complex(alpha[0], alpha[1])
+    if isinstance(beta, (list, tuple)):
+        beta = complex(beta[0], beta[1])
+    pa, ka = _pair(alpha, C.c_float)
+    pb, kb = _pair(beta, C.c_float)
+    handle().call("coral_cgemm", int(op_a), int(op_b), m, n, k, pa, _ptr(a, _c64(), "a"), lda,
+                  _ptr(b, _c64(), "b"), ldb, pb, _ptr(c, _c64(), "c"), ldc)
+
+
+def zgemm(op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> None:
+    """level3/zgemm.rs:123 (alpha/beta: complex or [re, im])."""
+    if isinstance(alpha, (list, tuple)):
+        alpha = complex(alpha[0], alpha[1])
+    if isinstance(beta, (list, tuple)):
+        beta = complex(beta[0], beta[1])
+    pa, ka = _pair(alpha, C.c_double)
+    pb, kb = _pair(beta, C.c_double)
+    handle().call("coral_zgemm", int(op_a), int(op_b), m, n, k, pa, _ptr(a, _c128(), "a"), lda,
+                  _ptr(b, _c128(), "b"), ldb, pb, _ptr(c, _c128(), "c"), ldc)
+
+
+def set_gemm_mode(mode: int) -> None:
+    handle().set_gemm_mode(mode)
+
+
+def gemm_mode() -> int:
+    return handle().gemm_mode()

@@ -1,0 +1,108 @@
+// Internal declarations shared by every translation unit of libcoral_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "../../include/coral_b200.h"
+
+namespace coral {
+
+constexpr int kNumSMs = 148;                 // B200: 2 dies x 74 SMs
+constexpr uint64_t kDefaultWaitLimit = 1ull << 26;  // ~1 s of 20-ns spins
+
+// Device status word bits (written by bounded waits, read by coral_sync).
+constexpr unsigned kStatusTimeout = 1u;
+
+struct Handle {
+  int device = 0;
+  int sm_count = kNumSMs;
+  cudaStream_t stream = nullptr;
+  int pointer_mode = CORAL_POINTER_HOST;
+  int gemm_mode = CORAL_GEMM_NATIVE;
+  uint64_t wait_limit = kDefaultWaitLimit;
+  int bad_arg = 0;
+  std::string cuda_error;
+
+  // Growable device scratch (partials of multi-block reductions, split
+  // operands of emulated GEMMs).  Never shrinks until coral_destroy.
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  // Small zero-initialised device area: reduction arrival counters, the
+  // status word and scalar results.  Laid out as `DeviceWords`.
+  struct DeviceWords* words = nullptr;
+  void* host_pinned = nullptr;  // 64 B pinned staging for scalar results
+  // Zeroed pool of per-tile arrival counters for single-launch multi-block
+  // combines; every kernel returns the counters it used to zero.
+  unsigned* counters = nullptr;
+};
+
+constexpr size_t kCounterPool = 1u << 16;
+
+// Fixed device-side bookkeeping; counters are returned to zero by the last
+// block of the reduction that used them, so the area stays reusable.
+struct DeviceWords {
+  unsigned status;                 // kStatus* bits
+  unsigned pad0;
+  unsigned counters[30];           // arrival counters of single-launch reductions
+  double dresult[4];               // scalar results (device pointer mode staging)
+  unsigned long long uresult[4];
+  unsigned char reserved[1024 - 4 * 32 - 64];
+};
+static_assert(sizeof(DeviceWords) == 1024, "DeviceWords layout");
+
+enum CounterSlot { kCtrDot = 0, kCtrNrm2 = 1, kCtrIamax = 2, kCtrGemv = 3, kCtrTrsv = 4,
+                   kCtrSymv = 5, kCtrMisc = 6 };
+
+// Ensure the handle owns at least `bytes` of scratch; returns nullptr on failure.
+void* scratch(Handle* h, size_t bytes);
+
+// Records the CUDA error text in the handle and maps it to a status.
+coral_status_t cuda_status(Handle* h, cudaError_t err);
+// Every kernel launch site reports through launch_status(), which also
+// counts the launch (coral_kernel_launches()).
+void count_launch();
+inline coral_status_t launch_status(Handle* h) {
+  count_launch();
+  return cuda_status(h, cudaGetLastError());
+}
+
+inline coral_status_t bad_arg(Handle* h, int pos) {
+  if (h) h->bad_arg = pos;
+  return CORAL_ERR_INVALID_ARG;
+}
+
+// Grid size for a streaming kernel of `work` independent items with `per_block`
+// items per block, capped at `waves` resident waves of the SM count.
+inline unsigned stream_grid(size_t work, size_t per_block, int sm_count, int blocks_per_sm) {
+  size_t g = (work + per_block - 1) / per_block;
+  size_t cap = (size_t)sm_count * blocks_per_sm;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Copies a scalar result produced at device address `src` to `dst` per the
+// pointer mode (host: waits on the stream).
+coral_status_t deliver_result(Handle* h, void* dst, const void* src, size_t bytes);
+
+// Per-thread default handle for the coral_host_* entry points.
+Handle* thread_handle();
+
+}  // namespace coral
+
+#define CORAL_CUDA(h, call)                                   \
+  do {                                                        \
+    cudaError_t e__ = (call);                                 \
+    if (e__ != cudaSuccess) return ::coral::cuda_status((h), e__); \
+  } while (0)
+
+#define CORAL_HANDLE(hh) \
+  ::coral::Handle* H = reinterpret_cast<::coral::Handle*>(hh); \
+  if (!H) return CORAL_ERR_INVALID_ARG; \
+  H->bad_arg = 0

@@ -1,0 +1,28 @@
+// Emulated-precision GEMM entry points whose tensor-core kernels are not
+// built into this library yet report CORAL_ERR_NOT_SUPPORTED.
+#include "common.cuh"
+
+namespace coral {
+
+coral_status_t enqueue_sgemm_split(Handle*, int, int, int, size_t, size_t, size_t, float,
+                                   const float*, size_t, const float*, size_t, float, float*,
+                                   size_t) {
+  return CORAL_ERR_NOT_SUPPORTED;
+}
+coral_status_t enqueue_dgemm_ozaki(Handle*, int, int, size_t, size_t, size_t, double,
+                                   const double*, size_t, const double*, size_t, double, double*,
+                                   size_t) {
+  return CORAL_ERR_NOT_SUPPORTED;
+}
+coral_status_t enqueue_cgemm_split(Handle*, int, int, int, size_t, size_t, size_t, float2,
+                                   const float2*, size_t, const float2*, size_t, float2, float2*,
+                                   size_t) {
+  return CORAL_ERR_NOT_SUPPORTED;
+}
+coral_status_t enqueue_zgemm_ozaki(Handle*, int, int, size_t, size_t, size_t, double2,
+                                   const double2*, size_t, const double2*, size_t, double2,
+                                   double2*, size_t) {
+  return CORAL_ERR_NOT_SUPPORTED;
+}
+
+}  // namespace coral

@@ -1,0 +1,353 @@
+// Handle lifecycle, status reporting, scratch management and the host-slice
+// drop-in wrappers of the C ABI.
+#include "common.cuh"
+
+#include <atomic>
+#include <cstdio>
+#include <mutex>
+
+namespace coral {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+coral_status_t cuda_status(Handle* h, cudaError_t err) {
+  if (err == cudaSuccess) return CORAL_OK;
+  if (h) h->cuda_error = cudaGetErrorString(err);
+  if (err == cudaErrorMemoryAllocation) return CORAL_ERR_ALLOC;
+  if (err == cudaErrorNoDevice || err == cudaErrorInsufficientDriver) return CORAL_ERR_NO_DEVICE;
+  return CORAL_ERR_CUDA;
+}
+
+void* scratch(Handle* h, size_t bytes) {
+  if (bytes <= h->scratch_bytes) return h->scratch;
+  // Round up to 64 MiB granules past the first 16 MiB to avoid re-allocation churn.
+  size_t want = bytes < (16u << 20) ? (16u << 20) : ((bytes + (64u << 20) - 1) & ~size_t((64u << 20) - 1));
+  if (h->scratch) {
+    // The old buffer may still be read by queued kernels of this stream.
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return nullptr;
+    cudaFree(h->scratch);
+    h->scratch = nullptr;
+    h->scratch_bytes = 0;
+  }
+  void* p = nullptr;
+  if (cudaMalloc(&p, want) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  h->scratch = p;
+  h->scratch_bytes = want;
+  return p;
+}
+
+coral_status_t deliver_result(Handle* h, void* dst, const void* src, size_t bytes) {
+  if (h->pointer_mode == CORAL_POINTER_DEVICE) {
+    CORAL_CUDA(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    return CORAL_OK;
+  }
+  CORAL_CUDA(h, cudaMemcpyAsync(h->host_pinned, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+  CORAL_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::memcpy(dst, h->host_pinned, bytes);
+  return CORAL_OK;
+}
+
+static coral_status_t create_handle(Handle** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) { cudaGetLastError(); return CORAL_ERR_NO_DEVICE; }
+  int major = 0, sms = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (major != 10) return CORAL_ERR_NO_DEVICE;  // kernels are built for sm_100a only
+  Handle* h = new Handle();
+  h->device = dev;
+  h->sm_count = sms > 0 ? sms : kNumSMs;
+  if (cudaMalloc(&h->words, sizeof(DeviceWords)) != cudaSuccess ||
+      cudaMemset(h->words, 0, sizeof(DeviceWords)) != cudaSuccess ||
+      cudaMalloc(&h->counters, kCounterPool * sizeof(unsigned)) != cudaSuccess ||
+      cudaMemset(h->counters, 0, kCounterPool * sizeof(unsigned)) != cudaSuccess ||
+      cudaMallocHost(&h->host_pinned, 64) != cudaSuccess) {
+    cudaGetLastError();
+    if (h->words) cudaFree(h->words);
+    if (h->counters) cudaFree(h->counters);
+    delete h;
+    return CORAL_ERR_ALLOC;
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) { delete h; return CORAL_ERR_CUDA; }
+  *out = h;
+  return CORAL_OK;
+}
+
+static void destroy_handle(Handle* h) {
+  if (!h) return;
+  cudaStreamSynchronize(h->stream);
+  if (h->scratch) cudaFree(h->scratch);
+  if (h->words) cudaFree(h->words);
+  if (h->counters) cudaFree(h->counters);
+  if (h->host_pinned) cudaFreeHost(h->host_pinned);
+  delete h;
+}
+
+// Per-thread handle plus growable device staging for the host-slice wrappers.
+struct ThreadState {
+  Handle* h = nullptr;
+  void* dev = nullptr;
+  size_t dev_bytes = 0;
+  ~ThreadState() {
+    if (dev) cudaFree(dev);
+    destroy_handle(h);
+  }
+};
+static thread_local ThreadState tls;
+
+Handle* thread_handle() {
+  if (!tls.h) {
+    Handle* h = nullptr;
+    if (create_handle(&h) != CORAL_OK) return nullptr;
+    tls.h = h;
+  }
+  return tls.h;
+}
+
+static void* thread_staging(size_t bytes) {
+  if (bytes <= tls.dev_bytes) return tls.dev;
+  if (tls.dev) { cudaStreamSynchronize(tls.h->stream); cudaFree(tls.dev); tls.dev = nullptr; tls.dev_bytes = 0; }
+  size_t want = (bytes + (1u << 20) - 1) & ~size_t((1u << 20) - 1);
+  if (cudaMalloc(&tls.dev, want) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+  tls.dev_bytes = want;
+  return tls.dev;
+}
+
+}  // namespace coral
+
+using namespace coral;
+
+extern "C" {
+
+int coral_abi_version(void) { return CORAL_B200_ABI_VERSION; }
+
+uint64_t coral_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
+
+coral_status_t coral_create(coral_handle_t* handle) {
+  if (!handle) return CORAL_ERR_INVALID_ARG;
+  Handle* h = nullptr;
+  coral_status_t s = create_handle(&h);
+  *handle = reinterpret_cast<coral_handle_t>(h);
+  return s;
+}
+
+coral_status_t coral_destroy(coral_handle_t handle) {
+  destroy_handle(reinterpret_cast<Handle*>(handle));
+  return CORAL_OK;
+}
+
+coral_status_t coral_set_stream(coral_handle_t handle, void* stream) {
+  CORAL_HANDLE(handle);
+  H->stream = reinterpret_cast<cudaStream_t>(stream);
+  return CORAL_OK;
+}
+
+coral_status_t coral_get_stream(coral_handle_t handle, void** stream) {
+  CORAL_HANDLE(handle);
+  if (!stream) return bad_arg(H, 1);
+  *stream = H->stream;
+  return CORAL_OK;
+}
+
+coral_status_t coral_set_pointer_mode(coral_handle_t handle, int mode) {
+  CORAL_HANDLE(handle);
+  if (mode != CORAL_POINTER_HOST && mode != CORAL_POINTER_DEVICE) return bad_arg(H, 1);
+  H->pointer_mode = mode;
+  return CORAL_OK;
+}
+
+coral_status_t coral_set_gemm_mode(coral_handle_t handle, int mode) {
+  CORAL_HANDLE(handle);
+  if (mode < CORAL_GEMM_NATIVE || mode > CORAL_GEMM_SPLIT_BF16X6) return bad_arg(H, 1);
+  H->gemm_mode = mode;
+  return CORAL_OK;
+}
+
+coral_status_t coral_get_gemm_mode(coral_handle_t handle, int* mode) {
+  CORAL_HANDLE(handle);
+  if (!mode) return bad_arg(H, 1);
+  *mode = H->gemm_mode;
+  return CORAL_OK;
+}
+
+coral_status_t coral_set_wait_limit(coral_handle_t handle, uint64_t spins) {
+  CORAL_HANDLE(handle);
+  H->wait_limit = spins ? spins : kDefaultWaitLimit;
+  return CORAL_OK;
+}
+
+coral_status_t coral_sync(coral_handle_t handle) {
+  CORAL_HANDLE(handle);
+  CORAL_CUDA(H, cudaStreamSynchronize(H->stream));
+  unsigned status = 0;
+  CORAL_CUDA(H, cudaMemcpy(&status, &H->words->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (status) {
+    unsigned zero = 0;
+    CORAL_CUDA(H, cudaMemcpy(&H->words->status, &zero, sizeof(unsigned), cudaMemcpyHostToDevice));
+    if (status & kStatusTimeout) return CORAL_ERR_TIMEOUT;
+  }
+  return CORAL_OK;
+}
+
+int coral_last_bad_arg(coral_handle_t handle) {
+  Handle* h = reinterpret_cast<Handle*>(handle);
+  return h ? h->bad_arg : 0;
+}
+
+const char* coral_last_cuda_error(coral_handle_t handle) {
+  Handle* h = reinterpret_cast<Handle*>(handle);
+  return h ? h->cuda_error.c_str() : "";
+}
+
+const char* coral_status_string(coral_status_t s) {
+  switch (s) {
+    case CORAL_OK: return "CORAL_OK";
+    case CORAL_ERR_INVALID_ARG: return "CORAL_ERR_INVALID_ARG";
+    case CORAL_ERR_CUDA: return "CORAL_ERR_CUDA";
+    case CORAL_ERR_TIMEOUT: return "CORAL_ERR_TIMEOUT";
+    case CORAL_ERR_ALLOC: return "CORAL_ERR_ALLOC";
+    case CORAL_ERR_NOT_SUPPORTED: return "CORAL_ERR_NOT_SUPPORTED";
+    case CORAL_ERR_NO_DEVICE: return "CORAL_ERR_NO_DEVICE";
+  }
+  return "CORAL_ERR_UNKNOWN";
+}
+
+// ---- host-slice drop-ins --------------------------------------------------
+
+static size_t vec_len(size_t n, size_t inc) { return n ? (n - 1) * inc + 1 : 0; }
+static size_t mat_len(size_t rows, size_t cols, size_t ld) {
+  return (rows && cols) ? (cols - 1) * ld + rows : 0;
+}
+static size_t up256(size_t bytes) { return (bytes + 255) & ~size_t(255); }
+
+#define HOST_PROLOGUE()                              \
+  Handle* H = thread_handle();                       \
+  if (!H) return CORAL_ERR_NO_DEVICE;                \
+  coral_handle_t hh = reinterpret_cast<coral_handle_t>(H)
+
+coral_status_t coral_host_set_gemm_mode(int mode) {
+  HOST_PROLOGUE();
+  return coral_set_gemm_mode(hh, mode);
+}
+
+coral_status_t coral_host_sgemm(int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
+                                const float* a, size_t lda, const float* b, size_t ldb,
+                                float beta, float* c, size_t ldc) {
+  HOST_PROLOGUE();
+  bool ta = op_a != CORAL_NO_TRANSPOSE, tb = op_b != CORAL_NO_TRANSPOSE;
+  size_t la = mat_len(ta ? k : m, ta ? m : k, lda);
+  size_t lb = mat_len(tb ? n : k, tb ? k : n, ldb);
+  size_t lc = mat_len(m, n, ldc);
+  size_t oa = 0, ob = up256(la * 4), oc = ob + up256(lb * 4);
+  char* d = static_cast<char*>(thread_staging(oc + up256(lc * 4) + 256));
+  if (!d) return CORAL_ERR_ALLOC;
+  float* da = reinterpret_cast<float*>(d + oa);
+  float* db = reinterpret_cast<float*>(d + ob);
+  float* dc = reinterpret_cast<float*>(d + oc);
+  if (la) CORAL_CUDA(H, cudaMemcpyAsync(da, a, la * 4, cudaMemcpyHostToDevice, H->stream));
+  if (lb) CORAL_CUDA(H, cudaMemcpyAsync(db, b, lb * 4, cudaMemcpyHostToDevice, H->stream));
+  if (lc) CORAL_CUDA(H, cudaMemcpyAsync(dc, c, lc * 4, cudaMemcpyHostToDevice, H->stream));
+  coral_status_t s = coral_sgemm(hh, op_a, op_b, m, n, k, alpha, da, lda, db, ldb, beta, dc, ldc);
+  if (s != CORAL_OK) return s;
+  if (lc) CORAL_CUDA(H, cudaMemcpyAsync(c, dc, lc * 4, cudaMemcpyDeviceToHost, H->stream));
+  return coral_sync(hh);
+}
+
+coral_status_t coral_host_sgemv(int trans, size_t n_rows, size_t n_cols, float alpha,
+                                const float* matrix, size_t lda, const float* x, size_t incx,
+                                float beta, float* y, size_t incy) {
+  HOST_PROLOGUE();
+  bool t = trans != CORAL_NO_TRANSPOSE;
+  size_t lm = mat_len(n_rows, n_cols, lda);
+  size_t lx = vec_len(t ? n_rows : n_cols, incx);
+  size_t ly = vec_len(t ? n_cols : n_rows, incy);
+  size_t ox = up256(lm * 4), oy = ox + up256(lx * 4);
+  char* d = static_cast<char*>(thread_staging(oy + up256(ly * 4) + 256));
+  if (!d) return CORAL_ERR_ALLOC;
+  float* dm = reinterpret_cast<float*>(d);
+  float* dx = reinterpret_cast<float*>(d + ox);
+  float* dy = reinterpret_cast<float*>(d + oy);
+  if (lm) CORAL_CUDA(H, cudaMemcpyAsync(dm, matrix, lm * 4, cudaMemcpyHostToDevice, H->stream));
+  if (lx) CORAL_CUDA(H, cudaMemcpyAsync(dx, x, lx * 4, cudaMemcpyHostToDevice, H->stream));
+  if (ly) CORAL_CUDA(H, cudaMemcpyAsync(dy, y, ly * 4, cudaMemcpyHostToDevice, H->stream));
+  coral_status_t s = coral_sgemv(hh, trans, n_rows, n_cols, alpha, dm, lda, dx, incx, beta, dy, incy);
+  if (s != CORAL_OK) return s;
+  if (ly) CORAL_CUDA(H, cudaMemcpyAsync(y, dy, ly * 4, cudaMemcpyDeviceToHost, H->stream));
+  return coral_sync(hh);
+}
+
+coral_status_t coral_host_sdot(size_t n, const float* x, size_t incx, const float* y,
+                               size_t incy, float* result) {
+  HOST_PROLOGUE();
+  if (!result) return CORAL_ERR_INVALID_ARG;
+  size_t lx = vec_len(n, incx), ly = vec_len(n, incy);
+  size_t oy = up256(lx * 4);
+  char* d = static_cast<char*>(thread_staging(oy + up256(ly * 4) + 256));
+  if (!d) return CORAL_ERR_ALLOC;
+  float* dx = reinterpret_cast<float*>(d);
+  float* dy = reinterpret_cast<float*>(d + oy);
+  if (lx) CORAL_CUDA(H, cudaMemcpyAsync(dx, x, lx * 4, cudaMemcpyHostToDevice, H->stream));
+  if (ly) CORAL_CUDA(H, cudaMemcpyAsync(dy, y, ly * 4, cudaMemcpyHostToDevice, H->stream));
+  int mode = H->pointer_mode;
+  H->pointer_mode = CORAL_POINTER_HOST;
+  coral_status_t s = coral_sdot(hh, n, dx, incx, dy, incy, result);
+  H->pointer_mode = mode;
+  if (s != CORAL_OK) return s;
+  return coral_sync(hh);
+}
+
+coral_status_t coral_host_saxpy(size_t n, float alpha, const float* x, size_t incx, float* y,
+                                size_t incy) {
+  HOST_PROLOGUE();
+  size_t lx = vec_len(n, incx), ly = vec_len(n, incy);
+  size_t oy = up256(lx * 4);
+  char* d = static_cast<char*>(thread_staging(oy + up256(ly * 4) + 256));
+  if (!d) return CORAL_ERR_ALLOC;
+  float* dx = reinterpret_cast<float*>(d);
+  float* dy = reinterpret_cast<float*>(d + oy);
+  if (lx) CORAL_CUDA(H, cudaMemcpyAsync(dx, x, lx * 4, cudaMemcpyHostToDevice, H->stream));
+  if (ly) CORAL_CUDA(H, cudaMemcpyAsync(dy, y, ly * 4, cudaMemcpyHostToDevice, H->stream));
+  coral_status_t s = coral_saxpy(hh, n, alpha, dx, incx, dy, incy);
+  if (s != CORAL_OK) return s;
+  if (ly) CORAL_CUDA(H, cudaMemcpyAsync(y, dy, ly * 4, cudaMemcpyDeviceToHost, H->stream));
+  return coral_sync(hh);
+}
+
+coral_status_t coral_host_isamax(size_t n, const float* x, size_t incx, size_t* index) {
+  HOST_PROLOGUE();
+  if (!index) return CORAL_ERR_INVALID_ARG;
+  size_t lx = vec_len(n, incx);
+  float* dx = static_cast<float*>(thread_staging(up256(lx * 4) + 256));
+  if (!dx) return CORAL_ERR_ALLOC;
+  if (lx) CORAL_CUDA(H, cudaMemcpyAsync(dx, x, lx * 4, cudaMemcpyHostToDevice, H->stream));
+  int mode = H->pointer_mode;
+  H->pointer_mode = CORAL_POINTER_HOST;
+  coral_status_t s = coral_isamax(hh, n, dx, incx, index);
+  H->pointer_mode = mode;
+  if (s != CORAL_OK) return s;
+  return coral_sync(hh);
+}
+
+coral_status_t coral_host_strsv(int uplo, int trans, int diag, size_t n, const float* matrix,
+                                size_t lda, float* x, size_t incx) {
+  HOST_PROLOGUE();
+  size_t lm = mat_len(n, n, lda), lx = vec_len(n, incx);
+  size_t ox = up256(lm * 4);
+  char* d = static_cast<char*>(thread_staging(ox + up256(lx * 4) + 256));
+  if (!d) return CORAL_ERR_ALLOC;
+  float* dm = reinterpret_cast<float*>(d);
+  float* dx = reinterpret_cast<float*>(d + ox);
+  if (lm) CORAL_CUDA(H, cudaMemcpyAsync(dm, matrix, lm * 4, cudaMemcpyHostToDevice, H->stream));
+  if (lx) CORAL_CUDA(H, cudaMemcpyAsync(dx, x, lx * 4, cudaMemcpyHostToDevice, H->stream));
+  coral_status_t s = coral_strsv(hh, uplo, trans, diag, n, dm, lda, dx, incx);
+  if (s != CORAL_OK) return s;
+  if (lx) CORAL_CUDA(H, cudaMemcpyAsync(x, dx, lx * 4, cudaMemcpyDeviceToHost, H->stream));
+  return coral_sync(hh);
+}
+
+}  // extern "C"

@@ -1,0 +1,197 @@
+/*
+ * coral_b200.h -- C ABI of the B200 BLAS engine.
+ *
+ * Drop-in boundary for CORAL's column-major BLAS routines (devdeliw/CORAL,
+ * crate coral-blas-aarch64).  Every routine keeps the reference's argument
+ * order and meaning; what changes is only what the Rust signature cannot say
+ * across an FFI boundary:
+ *
+ *   - a leading `coral_handle_t` carries the CUDA stream, scratch memory and
+ *     the device status word (bounded waits report CORAL_ERR_TIMEOUT);
+ *   - Rust slices become a plain pointer (length is implied by n/inc/ld, the
+ *     same relation the reference checks with `required_len_ok*`,
+ *     coral-aarch64/src/level1/assert_length_helpers.rs:8-15 and
+ *     coral-aarch64/src/level2/assert_length_helpers.rs:4-16);
+ *   - complex scalars `[f32; 2]` / `[f64; 2]` become `const float[2]` /
+ *     `const double[2]` (host memory);
+ *   - scalar results (`sdot`, `snrm2`, `isamax`) come back through an
+ *     out-pointer, interpreted per the handle's pointer mode (host by default);
+ *   - every call returns a coral_status_t instead of panicking.
+ *
+ * Matrix/vector pointers of the `coral_*` entry points are DEVICE pointers;
+ * kernels are enqueued on the handle's stream and the call returns without
+ * waiting (scalar results in host pointer mode wait for the stream).
+ * The `coral_host_*` entry points take HOST pointers with exactly the
+ * reference's argument list and semantics (no handle): they copy in, compute,
+ * copy out and synchronise, so a caller that holds host slices -- as every
+ * caller of the reference does -- can switch with no other change.
+ *
+ * Enum values follow the declaration order of coral-aarch64/src/enums.rs:1-18
+ * (what `as i32` yields on the Rust side):
+ *   CoralTranspose  { NoTranspose = 0, Transpose = 1, ConjugateTranspose = 2 }
+ *   CoralTriangular { UpperTriangular = 0, LowerTriangular = 1 }
+ *   CoralDiagonal   { UnitDiagonal = 0, NonUnitDiagonal = 1 }
+ *
+ * Increments are unsigned (`usize` in the reference) and must be >= 1 where
+ * the reference asserts `inc > 0`.
+ */
+#ifndef CORAL_B200_H
+#define CORAL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CORAL_B200_ABI_VERSION 1
+
+typedef enum coral_status {
+  CORAL_OK = 0,
+  CORAL_ERR_INVALID_ARG = 1,   /* argument check failed (see coral_last_bad_arg) */
+  CORAL_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+  CORAL_ERR_TIMEOUT = 3,       /* a bounded device wait gave up (status word set) */
+  CORAL_ERR_ALLOC = 4,         /* device/host allocation failed */
+  CORAL_ERR_NOT_SUPPORTED = 5, /* size or mode outside what the kernels handle */
+  CORAL_ERR_NO_DEVICE = 6      /* no sm_100 device visible */
+} coral_status_t;
+
+enum { CORAL_NO_TRANSPOSE = 0, CORAL_TRANSPOSE = 1, CORAL_CONJ_TRANSPOSE = 2 };
+enum { CORAL_UPPER = 0, CORAL_LOWER = 1 };
+enum { CORAL_UNIT = 0, CORAL_NON_UNIT = 1 };
+enum { CORAL_POINTER_HOST = 0, CORAL_POINTER_DEVICE = 1 };
+
+/* GEMM arithmetic for coral_sgemm / coral_cgemm / coral_dgemm / coral_zgemm. */
+enum {
+  CORAL_GEMM_NATIVE = 0,       /* FP32/FP64 FMA pipes, (complex: direct 4M) */
+  CORAL_GEMM_SPLIT_BF16X3 = 1, /* s/c: 2-way BF16 split, 3 tcgen05 products */
+  CORAL_GEMM_OZAKI_INT8 = 2,   /* d/z: INT8-slice emulation on tcgen05 */
+  CORAL_GEMM_SPLIT_BF16X6 = 3  /* s/c: 3-way BF16 split, 6 tcgen05 products */
+};
+
+typedef struct coral_handle_s* coral_handle_t;
+
+/* ---- handle ------------------------------------------------------------ */
+coral_status_t coral_create(coral_handle_t* handle);
+coral_status_t coral_destroy(coral_handle_t handle);
+/* `stream` is a cudaStream_t (NULL = legacy default stream). */
+coral_status_t coral_set_stream(coral_handle_t handle, void* stream);
+coral_status_t coral_get_stream(coral_handle_t handle, void** stream);
+coral_status_t coral_set_pointer_mode(coral_handle_t handle, int mode);
+coral_status_t coral_set_gemm_mode(coral_handle_t handle, int mode);
+coral_status_t coral_get_gemm_mode(coral_handle_t handle, int* mode);
+/* Iteration limit of every bounded device wait (0 restores the default). */
+coral_status_t coral_set_wait_limit(coral_handle_t handle, uint64_t spins);
+/* Wait for the stream, then report and clear the device status word. */
+coral_status_t coral_sync(coral_handle_t handle);
+/* 1-based position of the offending argument after CORAL_ERR_INVALID_ARG
+ * (the handle counts as position 0), as BLAS xerbla reports it. */
+int coral_last_bad_arg(coral_handle_t handle);
+const char* coral_status_string(coral_status_t status);
+const char* coral_last_cuda_error(coral_handle_t handle);
+int coral_abi_version(void);
+/* Number of CUDA kernels this library has launched in this process. */
+uint64_t coral_kernel_launches(void);
+
+/* ---- level 1 (coral-aarch64/src/level1) --------------------------------- */
+/* sdot.rs:42-161 */
+coral_status_t coral_sdot(coral_handle_t h, size_t n, const float* x, size_t incx,
+                          const float* y, size_t incy, float* result);
+/* saxpy.rs:42-131 */
+coral_status_t coral_saxpy(coral_handle_t h, size_t n, float alpha, const float* x,
+                           size_t incx, float* y, size_t incy);
+/* snrm2.rs:45-149 */
+coral_status_t coral_snrm2(coral_handle_t h, size_t n, const float* x, size_t incx,
+                           float* result);
+/* isamax.rs:43-151 -- 0-based index of the first max |x_i| */
+coral_status_t coral_isamax(coral_handle_t h, size_t n, const float* x, size_t incx,
+                            size_t* index);
+/* scopy.rs:28-58 */
+coral_status_t coral_scopy(coral_handle_t h, size_t n, const float* x, size_t incx,
+                           float* y, size_t incy);
+/* sswap.rs:35-118 */
+coral_status_t coral_sswap(coral_handle_t h, size_t n, float* x, size_t incx,
+                           float* y, size_t incy);
+/* sscal.rs:30-66 */
+coral_status_t coral_sscal(coral_handle_t h, size_t n, float alpha, float* x,
+                           size_t incx);
+
+/* ---- level 2 (coral-aarch64/src/level2) --------------------------------- */
+/* sgemv.rs:63-80 */
+coral_status_t coral_sgemv(coral_handle_t h, int trans, size_t n_rows, size_t n_cols,
+                           float alpha, const float* matrix, size_t lda,
+                           const float* x, size_t incx, float beta, float* y,
+                           size_t incy);
+/* ssymv.rs:99-110 */
+coral_status_t coral_ssymv(coral_handle_t h, int uplo, size_t n, float alpha,
+                           const float* matrix, size_t lda, const float* x,
+                           size_t incx, float beta, float* y, size_t incy);
+/* chemv.rs:96-107 -- interleaved (re, im) complex64, ld in complex units */
+coral_status_t coral_chemv(coral_handle_t h, int uplo, size_t n, const float alpha[2],
+                           const float* matrix, size_t lda, const float* x,
+                           size_t incx, const float beta[2], float* y, size_t incy);
+/* strsv.rs:60-74 */
+coral_status_t coral_strsv(coral_handle_t h, int uplo, int trans, int diag, size_t n,
+                           const float* matrix, size_t lda, float* x, size_t incx);
+/* strmv.rs:59-73 */
+coral_status_t coral_strmv(coral_handle_t h, int uplo, int trans, int diag, size_t n,
+                           const float* matrix, size_t lda, float* x, size_t incx);
+/* sger.rs:68-78 */
+coral_status_t coral_sger(coral_handle_t h, size_t n_rows, size_t n_cols, float alpha,
+                          const float* x, size_t incx, const float* y, size_t incy,
+                          float* matrix, size_t lda);
+/* ssyr.rs:63-71 */
+coral_status_t coral_ssyr(coral_handle_t h, int uplo, size_t n, float alpha,
+                          const float* x, size_t incx, float* matrix, size_t lda);
+/* ssyr2.rs:59-69 */
+coral_status_t coral_ssyr2(coral_handle_t h, int uplo, size_t n, float alpha,
+                           const float* x, size_t incx, const float* y, size_t incy,
+                           float* matrix, size_t lda);
+
+/* ---- level 3 (coral-aarch64/src/level3) --------------------------------- */
+/* sgemm.rs:106-130; arithmetic per coral_set_gemm_mode (NATIVE or SPLIT_BF16X3/X6) */
+coral_status_t coral_sgemm(coral_handle_t h, int op_a, int op_b, size_t m, size_t n,
+                           size_t k, float alpha, const float* a, size_t lda,
+                           const float* b, size_t ldb, float beta, float* c,
+                           size_t ldc);
+/* dgemm.rs:107; arithmetic per coral_set_gemm_mode (NATIVE or OZAKI_INT8) */
+coral_status_t coral_dgemm(coral_handle_t h, int op_a, int op_b, size_t m, size_t n,
+                           size_t k, double alpha, const double* a, size_t lda,
+                           const double* b, size_t ldb, double beta, double* c,
+                           size_t ldc);
+/* cgemm.rs:127-157 -- op in {N, T, C}; interleaved complex64 */
+coral_status_t coral_cgemm(coral_handle_t h, int op_a, int op_b, size_t m, size_t n,
+                           size_t k, const float alpha[2], const float* a, size_t lda,
+                           const float* b, size_t ldb, const float beta[2], float* c,
+                           size_t ldc);
+/* zgemm.rs:123 -- op in {N, T, C}; interleaved complex128 */
+coral_status_t coral_zgemm(coral_handle_t h, int op_a, int op_b, size_t m, size_t n,
+                           size_t k, const double alpha[2], const double* a, size_t lda,
+                           const double* b, size_t ldb, const double beta[2], double* c,
+                           size_t ldc);
+
+/* ---- host-slice drop-ins: the reference's exact argument lists ---------- */
+/* Pointers are HOST memory.  Return value as above; scalar-returning routines
+ * write through the trailing out-pointer.  Thread-safe: each host thread gets
+ * its own internal handle. */
+coral_status_t coral_host_sgemm(int op_a, int op_b, size_t m, size_t n, size_t k,
+                                float alpha, const float* a, size_t lda, const float* b,
+                                size_t ldb, float beta, float* c, size_t ldc);
+coral_status_t coral_host_sgemv(int trans, size_t n_rows, size_t n_cols, float alpha,
+                                const float* matrix, size_t lda, const float* x,
+                                size_t incx, float beta, float* y, size_t incy);
+coral_status_t coral_host_sdot(size_t n, const float* x, size_t incx, const float* y,
+                               size_t incy, float* result);
+coral_status_t coral_host_saxpy(size_t n, float alpha, const float* x, size_t incx,
+                                float* y, size_t incy);
+coral_status_t coral_host_isamax(size_t n, const float* x, size_t incx, size_t* index);
+coral_status_t coral_host_strsv(int uplo, int trans, int diag, size_t n,
+                                const float* matrix, size_t lda, float* x, size_t incx);
+/* Select the GEMM arithmetic of this thread's internal handle. */
+coral_status_t coral_host_set_gemm_mode(int mode);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CORAL_B200_H */

@@ -1,0 +1,231 @@
+"""CPU oracle for CORAL's BLAS semantics -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline arm may
+import this package, and only as the checker (or, for ``port_*``, as the
+timed reference CPU path).  The coral_b200 product never imports it.
+
+Wraps oracle/_build/liboracle.so (built from oracle.c by oracle/Makefile or
+:func:`build`).  Functions take numpy arrays.  Parity is pinned by
+tests/test_oracle_golden.py against the reference's known-answer doctests,
+its planted-maximum isamax cases, the closed-form fixtures of its test suite
+and scipy's OpenBLAS (the CBLAS class of oracle the reference's own tests
+link), stored as fixtures in tests/golden/.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+_lib = None
+
+
+def build() -> str:
+    """Compiles oracle.c with its Makefile; returns the library path."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH) or (
+                os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "oracle.c"))):
+            build()
+        _lib = C.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+_fp = C.POINTER(C.c_float)
+_dp = C.POINTER(C.c_double)
+_sz = C.c_size_t
+_i = C.c_int
+
+
+def _declare(L: C.CDLL) -> None:
+    L.or_saxpy_exact.argtypes = [_sz, C.c_float, _fp, _sz, _fp, _sz]
+    L.or_sscal_exact.argtypes = [_sz, C.c_float, _fp, _sz]
+    L.or_scopy_exact.argtypes = [_sz, _fp, _sz, _fp, _sz]
+    L.or_sswap_exact.argtypes = [_sz, _fp, _sz, _fp, _sz]
+    L.or_isamax_exact.argtypes = [_sz, _fp, _sz]
+    L.or_isamax_exact.restype = _sz
+    L.or_sdot_f64.argtypes = [_sz, _fp, _sz, _fp, _sz]
+    L.or_sdot_f64.restype = C.c_double
+    L.or_snrm2_f64.argtypes = [_sz, _fp, _sz]
+    L.or_snrm2_f64.restype = C.c_double
+    L.or_sgemv_f64.argtypes = [_i, _sz, _sz, C.c_float, _fp, _sz, _fp, _sz, C.c_float, _fp, _sz, _dp]
+    L.or_ssymv_f64.argtypes = [_i, _sz, C.c_float, _fp, _sz, _fp, _sz, C.c_float, _fp, _sz, _dp]
+    L.or_chemv_f64.argtypes = [_i, _sz, _fp, _fp, _sz, _fp, _sz, _fp, _fp, _sz, _dp]
+    L.or_strsv_f64.argtypes = [_i, _i, _i, _sz, _fp, _sz, _fp, _sz, _dp]
+    L.or_strmv_f64.argtypes = [_i, _i, _i, _sz, _fp, _sz, _fp, _sz, _dp]
+    L.or_sger_exact.argtypes = [_sz, _sz, C.c_float, _fp, _sz, _fp, _sz, _fp, _sz]
+    L.or_ssyr_exact.argtypes = [_i, _sz, C.c_float, _fp, _sz, _fp, _sz]
+    L.or_ssyr2_exact.argtypes = [_i, _sz, C.c_float, _fp, _sz, _fp, _sz, _fp, _sz]
+    L.or_gemm_sample.argtypes = [_i, _i, _i, _i, _sz, _sz, _sz, _dp, C.c_void_p, _sz, C.c_void_p,
+                                 _sz, _dp, C.c_void_p, _sz, _sz, C.POINTER(C.c_int64),
+                                 C.POINTER(C.c_int64), _dp, _dp]
+    L.port_sgemm_nn.argtypes = [_sz, _sz, _sz, C.c_float, _fp, _sz, _fp, _sz, C.c_float, _fp, _sz]
+    L.port_sgemv_n.argtypes = [_sz, _sz, C.c_float, _fp, _sz, _fp, C.c_float, _fp]
+    L.port_sgemv_t.argtypes = [_sz, _sz, C.c_float, _fp, _sz, _fp, C.c_float, _fp]
+    L.port_sdot.argtypes = [_sz, _fp, _fp]
+    L.port_sdot.restype = C.c_float
+
+
+def _f(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous, (a.dtype, a.flags)
+    return a.ctypes.data_as(_fp)
+
+
+def _d(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+# ---- level 1 -----------------------------------------------------------------
+def saxpy(n, alpha, x, incx, y, incy):
+    """In-place on a copy of y; returns it (bit-exact restatement)."""
+    y = np.array(y, dtype=np.float32, copy=True)
+    lib().or_saxpy_exact(n, alpha, _f(x), incx, _f(y), incy)
+    return y
+
+
+def sscal(n, alpha, x, incx):
+    x = np.array(x, dtype=np.float32, copy=True)
+    lib().or_sscal_exact(n, alpha, _f(x), incx)
+    return x
+
+
+def scopy(n, x, incx, y, incy):
+    y = np.array(y, dtype=np.float32, copy=True)
+    lib().or_scopy_exact(n, _f(x), incx, _f(y), incy)
+    return y
+
+
+def sswap(n, x, incx, y, incy):
+    x = np.array(x, dtype=np.float32, copy=True)
+    y = np.array(y, dtype=np.float32, copy=True)
+    lib().or_sswap_exact(n, _f(x), incx, _f(y), incy)
+    return x, y
+
+
+def isamax(n, x, incx) -> int:
+    return int(lib().or_isamax_exact(n, _f(x), incx))
+
+
+def sdot(n, x, incx, y, incy) -> float:
+    return float(lib().or_sdot_f64(n, _f(x), incx, _f(y), incy))
+
+
+def snrm2(n, x, incx) -> float:
+    return float(lib().or_snrm2_f64(n, _f(x), incx))
+
+
+# ---- level 2 -----------------------------------------------------------------
+def sgemv(trans, m, n, alpha, a, lda, x, incx, beta, y, incy) -> np.ndarray:
+    """Returns op(A)-product result y (float64, contiguous length of y)."""
+    ylen = n if trans else m
+    out = np.zeros(max(ylen, 1), np.float64)
+    lib().or_sgemv_f64(trans, m, n, alpha, _f(a), lda, _f(x), incx, beta, _f(y), incy, _d(out))
+    return out[:ylen]
+
+
+def ssymv(uplo, n, alpha, a, lda, x, incx, beta, y, incy) -> np.ndarray:
+    out = np.zeros(max(n, 1), np.float64)
+    lib().or_ssymv_f64(uplo, n, alpha, _f(a), lda, _f(x), incx, beta, _f(y), incy, _d(out))
+    return out[:n]
+
+
+def chemv(uplo, n, alpha, a, lda, x, incx, beta, y, incy) -> np.ndarray:
+    out = np.zeros(max(2 * n, 2), np.float64)
+    al = np.asarray(alpha, np.float32)
+    be = np.asarray(beta, np.float32)
+    lib().or_chemv_f64(uplo, n, _f(al), _f(a), lda, _f(x), incx, _f(be), _f(y), incy, _d(out))
+    return out[:2 * n]
+
+
+def strsv(uplo, trans, diag, n, a, lda, x, incx) -> np.ndarray:
+    out = np.zeros(max(n, 1), np.float64)
+    lib().or_strsv_f64(uplo, trans, diag, n, _f(a), lda, _f(x), incx, _d(out))
+    return out[:n]
+
+
+def strmv(uplo, trans, diag, n, a, lda, x, incx) -> np.ndarray:
+    out = np.zeros(max(n, 1), np.float64)
+    lib().or_strmv_f64(uplo, trans, diag, n, _f(a), lda, _f(x), incx, _d(out))
+    return out[:n]
+
+
+def sger(m, n, alpha, x, incx, y, incy, a, lda) -> np.ndarray:
+    a = np.array(a, dtype=np.float32, copy=True)
+    lib().or_sger_exact(m, n, alpha, _f(x), incx, _f(y), incy, _f(a), lda)
+    return a
+
+
+def ssyr(uplo, n, alpha, x, incx, a, lda) -> np.ndarray:
+    a = np.array(a, dtype=np.float32, copy=True)
+    lib().or_ssyr_exact(uplo, n, alpha, _f(x), incx, _f(a), lda)
+    return a
+
+
+def ssyr2(uplo, n, alpha, x, incx, y, incy, a, lda) -> np.ndarray:
+    a = np.array(a, dtype=np.float32, copy=True)
+    lib().or_ssyr2_exact(uplo, n, alpha, _f(x), incx, _f(y), incy, _f(a), lda)
+    return a
+
+
+# ---- level 3 -----------------------------------------------------------------
+def gemm_sample(op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, rows, cols):
+    """Double-double values of selected entries of alpha*op(A)op(B) + beta*C.
+
+    Arrays are flat column-major buffers of float32/float64 (real) or
+    complex64/complex128 (complex).  Returns (values, absbound): values is
+    complex128 for complex inputs else float64; absbound is
+    |alpha|*(|op(A)||op(B)|)_ij + |beta||C_ij| for component-wise errors.
+    """
+    cplx = np.iscomplexobj(a)
+    dbl = a.dtype in (np.float64, np.complex128)
+    rows = np.ascontiguousarray(rows, np.int64)
+    cols = np.ascontiguousarray(cols, np.int64)
+    cnt = rows.size
+    out = np.zeros(2 * max(cnt, 1), np.float64)
+    absb = np.zeros(max(cnt, 1), np.float64)
+    al = np.array([np.real(alpha), np.imag(alpha)], np.float64)
+    be = np.array([np.real(beta), np.imag(beta)], np.float64)
+    p = lambda arr: np.ascontiguousarray(arr).ctypes.data_as(C.c_void_p)  # noqa: E731
+    keep = [np.ascontiguousarray(x) for x in (a, b, c)]
+    lib().or_gemm_sample(int(dbl), int(cplx), op_a, op_b, m, n, k, _d(al), p(keep[0]), lda,
+                         p(keep[1]), ldb, _d(be), p(keep[2]), ldc, cnt,
+                         rows.ctypes.data_as(C.POINTER(C.c_int64)),
+                         cols.ctypes.data_as(C.POINTER(C.c_int64)), _d(out), _d(absb))
+    vals = out[:2 * cnt].reshape(cnt, 2)
+    if cplx:
+        return vals[:, 0] + 1j * vals[:, 1], absb[:cnt]
+    return vals[:, 0].copy(), absb[:cnt]
+
+
+def gemm_full(op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """Every entry of C (column-major m x n, as a 2-D array [m, n])."""
+    ii, jj = np.meshgrid(np.arange(m), np.arange(n), indexing="ij")
+    vals, absb = gemm_sample(op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
+                             ii.ravel(), jj.ravel())
+    return vals.reshape(m, n), absb.reshape(m, n)
+
+
+# ---- CORAL CPU algorithm restatements (timed as the reference CPU path) ------
+def port_sgemm_nn(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    lib().port_sgemm_nn(m, n, k, alpha, _f(a), lda, _f(b), ldb, beta, _f(c), ldc)
+
+
+def port_sgemv(trans, m, n, alpha, a, lda, x, beta, y):
+    fn = lib().port_sgemv_t if trans else lib().port_sgemv_n
+    fn(m, n, alpha, _f(a), lda, _f(x), beta, _f(y))
+
+
+def port_sdot(n, x, y) -> float:
+    return float(lib().port_sdot(n, _f(x), _f(y)))

@@ -1,0 +1,513 @@
+/*
+ * oracle.c -- CPU restatement of CORAL's BLAS semantics.  TEST INFRASTRUCTURE
+ * ONLY: used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+ * arm as the checker; nothing in the coral_b200 product links or calls it.
+ *
+ * Three kinds of functions:
+ *   or_*_exact  fp32 restatements that reproduce the reference's rounding
+ *               element for element (the GPU must match these bit for bit);
+ *   or_*_f64    FP64 (or double-double, `dd`) references of the mathematical
+ *               result, following the reference's quick returns and scaling
+ *               order, for tolerance-based parity and error measurement;
+ *   port_*      restatements of CORAL's own CPU algorithms (blocking, loop
+ *               order, fp32 accumulation) that bench.py times as the
+ *               reference CPU path, because the Rust crate cannot be built
+ *               here (no cargo, and coral-aarch64 is aarch64-only).
+ *
+ * Reference paths are relative to the devdeliw/CORAL checkout
+ * (coral-aarch64/src/...).  Compile with -ffp-contract=off: the reference's
+ * `a += b * c` in Rust is two roundings, and only explicit fmaf()/fma() may
+ * fuse.
+ */
+#include <math.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define UPPER 0
+#define LOWER 1
+#define UNIT 0
+#define NON_UNIT 1
+#define NOTRANS 0
+#define TRANS 1
+#define CONJTRANS 2
+
+/* ---------------- double-double helpers (Dekker/Knuth, with fma) --------- */
+typedef struct { double hi, lo; } dd;
+
+static inline dd dd_two_sum(double a, double b) {
+  double s = a + b, bb = s - a, e = (a - (s - bb)) + (b - bb);
+  dd r = {s, e};
+  return r;
+}
+static inline dd dd_add_prod(dd acc, double a, double b) {
+  double p = a * b, pe = fma(a, b, -p);
+  dd s = dd_two_sum(acc.hi, p);
+  s.lo += acc.lo + pe;
+  return dd_two_sum(s.hi, s.lo);
+}
+static inline double dd_val(dd a) { return a.hi + a.lo; }
+
+/* ============================ level 1 ==================================== */
+
+/* level1/saxpy.rs:42-131: fused body for the first n - n%8 elements of the
+ * unit-stride path (16- and 8-wide vfmaq_f32), `*y += alpha * x` otherwise. */
+void or_saxpy_exact(size_t n, float alpha, const float* x, size_t incx, float* y, size_t incy) {
+  if (n == 0 || alpha == 0.0f) return;
+  if (incx == 1 && incy == 1) {
+    size_t nf = n - (n % 8);
+    for (size_t i = 0; i < nf; ++i) y[i] = fmaf(alpha, x[i], y[i]);
+    for (size_t i = nf; i < n; ++i) y[i] += alpha * x[i];
+  } else {
+    for (size_t i = 0; i < n; ++i) y[i * incy] += alpha * x[i * incx];
+  }
+}
+
+/* level1/sscal.rs:30-66: multiplies even when alpha == 0. */
+void or_sscal_exact(size_t n, float alpha, float* x, size_t incx) {
+  if (n == 0 || incx == 0) return;
+  for (size_t i = 0; i < n; ++i) x[i * incx] = x[i * incx] * alpha;
+}
+
+/* level1/scopy.rs:28-58 */
+void or_scopy_exact(size_t n, const float* x, size_t incx, float* y, size_t incy) {
+  for (size_t i = 0; i < n; ++i) y[i * incy] = x[i * incx];
+}
+
+/* level1/sswap.rs:35-118 */
+void or_sswap_exact(size_t n, float* x, size_t incx, float* y, size_t incy) {
+  for (size_t i = 0; i < n; ++i) {
+    float t = x[i * incx];
+    x[i * incx] = y[i * incy];
+    y[i * incy] = t;
+  }
+}
+
+/* level1/isamax.rs:43-151: first index of the largest |x_i|; NaN never wins
+ * (mapped to -inf in the SIMD body, rejected by `v > best` in the scalar
+ * paths); n == 0 or incx == 0 -> 0. */
+size_t or_isamax_exact(size_t n, const float* x, size_t incx) {
+  if (n == 0 || incx == 0) return 0;
+  float best = -INFINITY;
+  size_t idx = 0;
+  for (size_t i = 0; i < n; ++i) {
+    float v = fabsf(x[i * incx]);
+    if (v > best) { best = v; idx = i; }
+  }
+  return idx;
+}
+
+/* level1/sdot.rs:42-161 (exact value of the fp32 inputs' dot product). */
+double or_sdot_f64(size_t n, const float* x, size_t incx, const float* y, size_t incy) {
+  dd acc = {0.0, 0.0};
+  for (size_t i = 0; i < n; ++i) acc = dd_add_prod(acc, x[i * incx], y[i * incy]);
+  return dd_val(acc);
+}
+
+/* level1/snrm2.rs:45-149 -- ||x||_2; n == 0 or incx == 0 -> 0. */
+double or_snrm2_f64(size_t n, const float* x, size_t incx) {
+  if (n == 0 || incx == 0) return 0.0;
+  dd acc = {0.0, 0.0};
+  for (size_t i = 0; i < n; ++i) acc = dd_add_prod(acc, x[i * incx], x[i * incx]);
+  return sqrt(dd_val(acc));
+}
+
+/* ============================ level 2 ==================================== */
+
+/* level2/sgemv_notranspose.rs:63-177, sgemv_transpose.rs:64-182:
+ * empty matrix or (alpha == 0 && beta == 1) -> no-op; beta != 1 -> y *= beta
+ * in fp32 (sscal); alpha == 0 -> done; x is scaled by alpha in fp32, then
+ * y += op(A) xs.  Output in double: y_out = fl32(beta*y) + sum. */
+void or_sgemv_f64(int trans, size_t m, size_t n, float alpha, const float* A, size_t lda,
+                  const float* x, size_t incx, float beta, const float* y, size_t incy,
+                  double* y_out) {
+  const int t = trans != NOTRANS;
+  const size_t ylen = t ? n : m, xlen = t ? m : n;
+  for (size_t i = 0; i < ylen; ++i) y_out[i] = y[i * incy];
+  if (m == 0 || n == 0) return;
+  if (alpha == 0.0f && beta == 1.0f) return;
+  if (beta != 1.0f)
+    for (size_t i = 0; i < ylen; ++i) y_out[i] = (double)(y[i * incy] * beta);
+  if (alpha == 0.0f) return;
+  float* xs = (float*)malloc(sizeof(float) * (xlen ? xlen : 1));
+  for (size_t j = 0; j < xlen; ++j) xs[j] = alpha * x[j * incx];
+  for (size_t i = 0; i < ylen; ++i) {
+    dd acc = {0.0, 0.0};
+    for (size_t j = 0; j < xlen; ++j) {
+      float a = t ? A[j + i * lda] : A[i + j * lda];
+      acc = dd_add_prod(acc, a, xs[j]);
+    }
+    y_out[i] += dd_val(acc);
+  }
+  free(xs);
+}
+
+/* level2/ssymv.rs:99-394: n == 0 or (alpha == 0 && beta == 1) -> no-op;
+ * x scaled by alpha in fp32; beta == 0 -> y = 0 (fill), beta != 1 -> y *= beta;
+ * only the `uplo` triangle of A is referenced. */
+void or_ssymv_f64(int uplo, size_t n, float alpha, const float* A, size_t lda, const float* x,
+                  size_t incx, float beta, const float* y, size_t incy, double* y_out) {
+  for (size_t i = 0; i < n; ++i) y_out[i] = y[i * incy];
+  if (n == 0) return;
+  if (alpha == 0.0f && beta == 1.0f) return;
+  float* xs = (float*)malloc(sizeof(float) * n);
+  for (size_t j = 0; j < n; ++j) xs[j] = alpha * x[j * incx];
+  for (size_t i = 0; i < n; ++i) {
+    float yb = beta == 0.0f ? 0.0f : (beta != 1.0f ? y[i * incy] * beta : y[i * incy]);
+    dd acc = {0.0, 0.0};
+    for (size_t j = 0; j < n; ++j) {
+      int stored = uplo == UPPER ? (i <= j) : (i >= j);
+      float a = stored ? A[i + j * lda] : A[j + i * lda];
+      acc = dd_add_prod(acc, a, xs[j]);
+    }
+    y_out[i] = (double)yb + dd_val(acc);
+  }
+  free(xs);
+}
+
+/* level2/chemv.rs:96-447: as ssymv for a Hermitian matrix stored in the
+ * `uplo` triangle; the other triangle is conj of the stored one and only
+ * Re(a_jj) is used on the diagonal (chemv.rs:179-182).  Complex scalars as
+ * (re, im); alpha*x and beta*y rounded in fp32 as the reference does. */
+void or_chemv_f64(int uplo, size_t n, const float alpha[2], const float* A, size_t lda,
+                  const float* x, size_t incx, const float beta[2], const float* y, size_t incy,
+                  double* y_out) {
+  for (size_t i = 0; i < n; ++i) {
+    y_out[2 * i] = y[2 * i * incy];
+    y_out[2 * i + 1] = y[2 * i * incy + 1];
+  }
+  if (n == 0) return;
+  if (alpha[0] == 0.0f && alpha[1] == 0.0f && beta[0] == 1.0f && beta[1] == 0.0f) return;
+  float* xs = (float*)malloc(sizeof(float) * 2 * n);
+  for (size_t j = 0; j < n; ++j) {
+    float xr = x[2 * j * incx], xi = x[2 * j * incx + 1];
+    xs[2 * j] = alpha[0] * xr - alpha[1] * xi;
+    xs[2 * j + 1] = alpha[0] * xi + alpha[1] * xr;
+  }
+  for (size_t i = 0; i < n; ++i) {
+    float yr = y[2 * i * incy], yi = y[2 * i * incy + 1], br, bi;
+    if (beta[0] == 0.0f && beta[1] == 0.0f) { br = 0.0f; bi = 0.0f; }
+    else if (beta[0] == 1.0f && beta[1] == 0.0f) { br = yr; bi = yi; }
+    else { br = yr * beta[0] - yi * beta[1]; bi = yr * beta[1] + yi * beta[0]; }
+    dd re = {0.0, 0.0}, im = {0.0, 0.0};
+    for (size_t j = 0; j < n; ++j) {
+      double ar, ai;
+      if (i == j) { ar = A[2 * (i + j * lda)]; ai = 0.0; }
+      else {
+        int stored = uplo == UPPER ? (i < j) : (i > j);
+        if (stored) { ar = A[2 * (i + j * lda)]; ai = A[2 * (i + j * lda) + 1]; }
+        else { ar = A[2 * (j + i * lda)]; ai = -A[2 * (j + i * lda) + 1]; }
+      }
+      re = dd_add_prod(re, ar, xs[2 * j]);
+      re = dd_add_prod(re, -ai, xs[2 * j + 1]);
+      im = dd_add_prod(im, ar, xs[2 * j + 1]);
+      im = dd_add_prod(im, ai, xs[2 * j]);
+    }
+    y_out[2 * i] = (double)br + dd_val(re);
+    y_out[2 * i + 1] = (double)bi + dd_val(im);
+  }
+  free(xs);
+}
+
+static inline double tri_elem(int uplo, int diag, const float* A, size_t lda, size_t i, size_t j) {
+  if (i == j) return diag == UNIT ? 1.0 : (double)A[i + j * lda];
+  if (uplo == UPPER ? (i < j) : (i > j)) return A[i + j * lda];
+  return 0.0;
+}
+
+/* level2/strsv.rs:60-74 -> strlsv.rs / strusv.rs: solve op(A) x = b in place
+ * (op = A or A^T; ConjugateTranspose == Transpose), in double. */
+void or_strsv_f64(int uplo, int trans, int diag, size_t n, const float* A, size_t lda,
+                  const float* b, size_t incx, double* x_out) {
+  const int t = trans != NOTRANS;
+  /* op(A) is lower when (uplo==LOWER) xor t */
+  const int lower = (uplo == LOWER) != t;
+  for (size_t i = 0; i < n; ++i) x_out[i] = b[i * incx];
+  if (lower) {
+    for (size_t i = 0; i < n; ++i) {
+      dd acc = {x_out[i], 0.0};
+      for (size_t k = 0; k < i; ++k) {
+        double a = t ? tri_elem(uplo, diag, A, lda, k, i) : tri_elem(uplo, diag, A, lda, i, k);
+        acc = dd_add_prod(acc, -a, x_out[k]);
+      }
+      double d = tri_elem(uplo, diag, A, lda, i, i);
+      x_out[i] = dd_val(acc) / d;
+    }
+  } else {
+    for (size_t ii = n; ii-- > 0;) {
+      dd acc = {x_out[ii], 0.0};
+      for (size_t k = ii + 1; k < n; ++k) {
+        double a = t ? tri_elem(uplo, diag, A, lda, k, ii) : tri_elem(uplo, diag, A, lda, ii, k);
+        acc = dd_add_prod(acc, -a, x_out[k]);
+      }
+      double d = tri_elem(uplo, diag, A, lda, ii, ii);
+      x_out[ii] = dd_val(acc) / d;
+    }
+  }
+}
+
+/* level2/strmv.rs:59-73 -> strlmv.rs / strumv.rs: x <- op(A) x, in double. */
+void or_strmv_f64(int uplo, int trans, int diag, size_t n, const float* A, size_t lda,
+                  const float* x, size_t incx, double* x_out) {
+  const int t = trans != NOTRANS;
+  for (size_t i = 0; i < n; ++i) {
+    dd acc = {0.0, 0.0};
+    for (size_t k = 0; k < n; ++k) {
+      double a = t ? tri_elem(uplo, diag, A, lda, k, i) : tri_elem(uplo, diag, A, lda, i, k);
+      if (a != 0.0) acc = dd_add_prod(acc, a, x[k * incx]);
+    }
+    x_out[i] = dd_val(acc);
+  }
+}
+
+/* level2/sger.rs:68-132 (bit-exact): unit strides go through saxpy per
+ * column (fused first m - m%8 rows, `+= a*x` for the rest), strided through
+ * mul_add; a column whose coefficient alpha*y_j is 0 is skipped. */
+void or_sger_exact(size_t m, size_t n, float alpha, const float* x, size_t incx, const float* y,
+                   size_t incy, float* A, size_t lda) {
+  if (m == 0 || n == 0 || alpha == 0.0f) return;
+  for (size_t j = 0; j < n; ++j) {
+    float coeff = alpha * y[j * incy];
+    if (coeff == 0.0f) continue;
+    float* col = A + j * lda;
+    if (incx == 1 && incy == 1) or_saxpy_exact(m, coeff, x, 1, col, 1);
+    else
+      for (size_t i = 0; i < m; ++i) col[i] = fmaf(x[i * incx], coeff, col[i]);
+  }
+}
+
+/* level2/ssyr.rs:63-181 (bit-exact). */
+void or_ssyr_exact(int uplo, size_t n, float alpha, const float* x, size_t incx, float* A,
+                   size_t lda) {
+  if (n == 0 || alpha == 0.0f) return;
+  for (size_t j = 0; j < n; ++j) {
+    float aj = alpha * x[j * incx];
+    if (aj == 0.0f) continue;
+    size_t lo = uplo == UPPER ? 0 : j, hi = uplo == UPPER ? j + 1 : n;
+    if (incx == 1) or_saxpy_exact(hi - lo, aj, x + lo, 1, A + j * lda + lo, 1);
+    else
+      for (size_t i = lo; i < hi; ++i) A[i + j * lda] = fmaf(x[i * incx], aj, A[i + j * lda]);
+  }
+}
+
+/* level2/ssyr2.rs:59-197 (bit-exact). */
+void or_ssyr2_exact(int uplo, size_t n, float alpha, const float* x, size_t incx, const float* y,
+                    size_t incy, float* A, size_t lda) {
+  if (n == 0 || alpha == 0.0f) return;
+  for (size_t j = 0; j < n; ++j) {
+    float ay = alpha * y[j * incy], ax = alpha * x[j * incx];
+    size_t lo = uplo == UPPER ? 0 : j, hi = uplo == UPPER ? j + 1 : n;
+    float* col = A + j * lda;
+    if (incx == 1 && incy == 1) {
+      if (ay != 0.0f) or_saxpy_exact(hi - lo, ay, x + lo, 1, col + lo, 1);
+      if (ax != 0.0f) or_saxpy_exact(hi - lo, ax, y + lo, 1, col + lo, 1);
+    } else {
+      if (ay == 0.0f && ax == 0.0f) continue;
+      for (size_t i = lo; i < hi; ++i) {
+        float a = fmaf(x[i * incx], ay, col[i]);
+        col[i] = fmaf(y[i * incy], ax, a);
+      }
+    }
+  }
+}
+
+/* ============================ level 3 ==================================== */
+
+/* level3/sgemm.rs:106-130 / dgemm.rs:107 / cgemm.rs:127-157 / zgemm.rs:123
+ * evaluated on selected entries (rows[s], cols[s]) of C, in double-double:
+ * C_ij <- alpha * sum_l op(A)_il op(B)_lj + beta * C_ij, with
+ * beta == 0 -> C not read (f32_edge.rs:37-58) and alpha == 0 or k == 0 ->
+ * scale only (sgemm_nn.rs:29-45).  `absval[s]` receives
+ * |alpha| * sum_l |op(A)_il||op(B)_lj| + |beta||C_ij| for component-wise
+ * error bounds.  `cplx` selects interleaved complex storage (ld in complex
+ * units); `dbl` selects double inputs.  Results are written as (re, im)
+ * pairs in out[2*s] (im = 0 for real). */
+void or_gemm_sample(int dbl, int cplx, int op_a, int op_b, size_t m, size_t n, size_t k,
+                    const double alpha[2], const void* A, size_t lda, const void* B, size_t ldb,
+                    const double beta[2], const void* C, size_t ldc, size_t count,
+                    const int64_t* rows, const int64_t* cols, double* out, double* absval) {
+  (void)m; (void)n;
+  const int w = cplx ? 2 : 1;
+#define LD(P, idx) (dbl ? ((const double*)(P))[idx] : (double)((const float*)(P))[idx])
+  for (size_t s = 0; s < count; ++s) {
+    size_t i = (size_t)rows[s], j = (size_t)cols[s];
+    dd re = {0.0, 0.0}, im = {0.0, 0.0};
+    double asum = 0.0;
+    int scale_only = (alpha[0] == 0.0 && alpha[1] == 0.0) || k == 0;
+    if (!scale_only) {
+      for (size_t l = 0; l < k; ++l) {
+        size_t ia = op_a == NOTRANS ? i + l * lda : l + i * lda;
+        size_t ib = op_b == NOTRANS ? l + j * ldb : j + l * ldb;
+        double ar = LD(A, w * ia), ai = cplx ? LD(A, w * ia + 1) : 0.0;
+        double br = LD(B, w * ib), bi = cplx ? LD(B, w * ib + 1) : 0.0;
+        if (cplx && op_a == CONJTRANS) ai = -ai;
+        if (cplx && op_b == CONJTRANS) bi = -bi;
+        re = dd_add_prod(re, ar, br);
+        asum += fabs(ar) * fabs(br);
+        if (cplx) {
+          re = dd_add_prod(re, -ai, bi);
+          im = dd_add_prod(im, ar, bi);
+          im = dd_add_prod(im, ai, br);
+          asum += fabs(ai) * fabs(bi) + fabs(ar) * fabs(bi) + fabs(ai) * fabs(br);
+        }
+      }
+    }
+    double pr = dd_val(re), pi = dd_val(im);
+    double cr = 0.0, ci = 0.0;
+    int beta0 = beta[0] == 0.0 && beta[1] == 0.0;
+    if (!beta0) {
+      cr = LD(C, w * (i + j * ldc));
+      ci = cplx ? LD(C, w * (i + j * ldc) + 1) : 0.0;
+    }
+    double rr = alpha[0] * pr - alpha[1] * pi + beta[0] * cr - beta[1] * ci;
+    double ri = alpha[0] * pi + alpha[1] * pr + beta[0] * ci + beta[1] * cr;
+    if (scale_only) {
+      rr = beta[0] * cr - beta[1] * ci;
+      ri = beta[0] * ci + beta[1] * cr;
+    }
+    out[2 * s] = rr;
+    out[2 * s + 1] = cplx ? ri : 0.0;
+    if (absval)
+      absval[s] = hypot(alpha[0], alpha[1]) * (scale_only ? 0.0 : asum) +
+                  hypot(beta[0], beta[1]) * hypot(cr, ci);
+  }
+#undef LD
+}
+
+/* ===================== CORAL CPU algorithm restatements =================== */
+
+/* level3/sgemm_nn.rs:10-99 with f32_packers.rs (MR x NR = 8 x 12 register
+ * tile, MC/NC/KC = 384/576/256 from sgemm.rs:92-94) and the microkernel's
+ * rank-1 update order (microkernel/f32_mrxnr.rs:46-95): NN only, fp32. */
+#define P_MR 8
+#define P_NR 12
+#define P_MC 384
+#define P_NC 576
+#define P_KC 256
+
+static void port_pack_a(size_t mc, size_t kc, const float* a, size_t lda, float* buf) {
+  for (size_t i0 = 0; i0 < mc; i0 += P_MR) {
+    size_t mr = mc - i0 < P_MR ? mc - i0 : P_MR;
+    for (size_t l = 0; l < kc; ++l)
+      for (size_t r = 0; r < P_MR; ++r) *buf++ = r < mr ? a[(i0 + r) + l * lda] : 0.0f;
+  }
+}
+
+static void port_pack_b(size_t kc, size_t nc, const float* b, size_t ldb, float* buf) {
+  for (size_t j0 = 0; j0 < nc; j0 += P_NR) {
+    size_t nr = nc - j0 < P_NR ? nc - j0 : P_NR;
+    for (size_t l = 0; l < kc; ++l)
+      for (size_t c = 0; c < P_NR; ++c) *buf++ = c < nr ? b[l + (j0 + c) * ldb] : 0.0f;
+  }
+}
+
+void port_sgemm_nn(size_t m, size_t n, size_t k, float alpha, const float* a, size_t lda,
+                   const float* b, size_t ldb, float beta, float* c, size_t ldc) {
+  if (alpha == 0.0f || k == 0) {
+    for (size_t j = 0; j < n; ++j)
+      for (size_t i = 0; i < m; ++i)
+        c[i + j * ldc] = beta == 0.0f ? 0.0f : (beta != 1.0f ? c[i + j * ldc] * beta : c[i + j * ldc]);
+    return;
+  }
+  float* abuf = (float*)aligned_alloc(64, sizeof(float) * (P_MC + P_MR) * P_KC);
+  float* bbuf = (float*)aligned_alloc(64, sizeof(float) * (P_NC + P_NR) * P_KC);
+  for (size_t j0 = 0; j0 < n; j0 += P_NC) {
+    size_t nc = n - j0 < P_NC ? n - j0 : P_NC;
+    for (size_t l0 = 0; l0 < k; l0 += P_KC) {
+      size_t kc = k - l0 < P_KC ? k - l0 : P_KC;
+      port_pack_b(kc, nc, b + l0 + j0 * ldb, ldb, bbuf);
+      float bp = l0 == 0 ? beta : 1.0f;
+      for (size_t i0 = 0; i0 < m; i0 += P_MC) {
+        size_t mc = m - i0 < P_MC ? m - i0 : P_MC;
+        port_pack_a(mc, kc, a + i0 + l0 * lda, lda, abuf);
+        for (size_t jr = 0; jr < nc; jr += P_NR) {
+          size_t nr = nc - jr < P_NR ? nc - jr : P_NR;
+          const float* bpan = bbuf + (jr / P_NR) * P_NR * kc;
+          for (size_t ir = 0; ir < mc; ir += P_MR) {
+            size_t mr = mc - ir < P_MR ? mc - ir : P_MR;
+            const float* apan = abuf + (ir / P_MR) * P_MR * kc;
+            float acc[P_NR][P_MR];
+            memset(acc, 0, sizeof(acc));
+            for (size_t l = 0; l < kc; ++l) {
+              const float* av = apan + l * P_MR;
+              const float* bv = bpan + l * P_NR;
+              for (int cc = 0; cc < P_NR; ++cc)
+                for (int r = 0; r < P_MR; ++r) acc[cc][r] = fmaf(av[r], bv[cc], acc[cc][r]);
+            }
+            for (size_t cc = 0; cc < nr; ++cc) {
+              float* col = c + (i0 + ir) + (j0 + jr + cc) * ldc;
+              for (size_t r = 0; r < mr; ++r) {
+                if (bp == 0.0f) col[r] = alpha * acc[cc][r];
+                else if (bp == 1.0f) col[r] += alpha * acc[cc][r];
+                else col[r] = bp * col[r] + alpha * acc[cc][r];
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  free(abuf);
+  free(bbuf);
+}
+
+/* level1_special/saxpyf.rs:59-499 as used by sgemv_notranspose.rs:108-115
+ * (lda == m fast path): y *= beta, xs = alpha*x, then y += A xs with 8-column
+ * blocks, fp32 FMA. */
+void port_sgemv_n(size_t m, size_t n, float alpha, const float* A, size_t lda, const float* x,
+                  float beta, float* y) {
+  if (m == 0 || n == 0 || (alpha == 0.0f && beta == 1.0f)) return;
+  if (beta != 1.0f)
+    for (size_t i = 0; i < m; ++i) y[i] = y[i] * beta;
+  if (alpha == 0.0f) return;
+  float* xs = (float*)malloc(sizeof(float) * n);
+  for (size_t j = 0; j < n; ++j) xs[j] = alpha * x[j];
+  size_t j = 0;
+  for (; j + 8 <= n; j += 8) {
+    const float* c0 = A + j * lda;
+    for (size_t i = 0; i < m; ++i) {
+      float acc = y[i];
+      for (int q = 0; q < 8; ++q) acc = fmaf(c0[i + q * lda], xs[j + q], acc);
+      y[i] = acc;
+    }
+  }
+  for (; j < n; ++j)
+    for (size_t i = 0; i < m; ++i) y[i] = fmaf(A[i + j * lda], xs[j], y[i]);
+  free(xs);
+}
+
+/* level1_special/sdotf.rs:59-289 as used by sgemv_transpose.rs (lda == m):
+ * y_j = beta*y_j + dot(A[:, j], alpha*x), 8 fp32 lane accumulators. */
+void port_sgemv_t(size_t m, size_t n, float alpha, const float* A, size_t lda, const float* x,
+                  float beta, float* y) {
+  if (m == 0 || n == 0 || (alpha == 0.0f && beta == 1.0f)) return;
+  if (beta != 1.0f)
+    for (size_t j = 0; j < n; ++j) y[j] = y[j] * beta;
+  if (alpha == 0.0f) return;
+  float* xs = (float*)malloc(sizeof(float) * m);
+  for (size_t i = 0; i < m; ++i) xs[i] = alpha * x[i];
+  for (size_t j = 0; j < n; ++j) {
+    const float* col = A + j * lda;
+    float acc[8] = {0};
+    size_t i = 0;
+    for (; i + 8 <= m; i += 8)
+      for (int q = 0; q < 8; ++q) acc[q] = fmaf(col[i + q], xs[i + q], acc[q]);
+    float s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+    for (; i < m; ++i) s += col[i] * xs[i];
+    y[j] += s;
+  }
+  free(xs);
+}
+
+/* level1/sdot.rs:60-145: 8 x 4-lane fp32 accumulators over 32-element steps. */
+float port_sdot(size_t n, const float* x, const float* y) {
+  float acc[32] = {0};
+  size_t i = 0;
+  for (; i + 32 <= n; i += 32)
+    for (int q = 0; q < 32; ++q) acc[q] = fmaf(x[i + q], y[i + q], acc[q]);
+  float s = 0.0f;
+  for (int q = 0; q < 32; ++q) s += acc[q];
+  for (; i < n; ++i) s += x[i] * y[i];
+  return s;
+}
