@@ -40,7 +40,7 @@ METRIC = ("SGEMM TFLOP/s split-BF16x3 vs plain FP32 @8192 at ≤1e-6 rel err; GE
 M = N = K = 8192
 ALPHA, BETA = 1.5, 0.5
 GEMV_BYTES = 4 * (M * N + N + 2 * M)  # A once, x once, y read + written
-FP32_FMA_PEAK_TFLOPS = 148 * 128 * 2 * 1.965  # nominal: SMs x FP32 lanes x 2 x max clock (GHz)
+FP32_FMA_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal: SMs x FP32 lanes x 2 x max clock
 
 
 def peaks():

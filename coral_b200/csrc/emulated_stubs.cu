@@ -4,18 +4,8 @@
 
 namespace coral {
 
-coral_status_t enqueue_sgemm_split(Handle*, int, int, int, size_t, size_t, size_t, float,
-                                   const float*, size_t, const float*, size_t, float, float*,
-                                   size_t) {
-  return CORAL_ERR_NOT_SUPPORTED;
-}
 coral_status_t enqueue_dgemm_ozaki(Handle*, int, int, size_t, size_t, size_t, double,
                                    const double*, size_t, const double*, size_t, double, double*,
-                                   size_t) {
-  return CORAL_ERR_NOT_SUPPORTED;
-}
-coral_status_t enqueue_cgemm_split(Handle*, int, int, int, size_t, size_t, size_t, float2,
-                                   const float2*, size_t, const float2*, size_t, float2, float2*,
                                    size_t) {
   return CORAL_ERR_NOT_SUPPORTED;
 }

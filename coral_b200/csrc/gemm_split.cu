@@ -1,0 +1,489 @@
+// Split-BF16 SGEMM / CGEMM on the 5th-generation tensor cores (tcgen05 + TMEM).
+//
+// An fp32 value a is split into bf16 pieces a = a0 + a1 (+ a2) + r, each piece
+// the round-to-nearest bf16 of what the previous ones left (exact fp32
+// subtractions).  With two pieces, |r| <= 2^-18 |a|; with three, 2^-27 |a|.
+//   SPLIT_BF16X3: op(A) op(B) ~ A0 B0 + A0 B1 + A1 B0          (3 products)
+//   SPLIT_BF16X6: ... + A1 B1 + A0 B2 + A2 B0                  (6 products)
+// Every product is exact in the tensor core and accumulates in fp32 in TMEM.
+//
+// Pipeline per call:
+//   1. split pre-pass: op(A) -> pieces [m][kp] and op(B)^T -> pieces [n][kp],
+//      bf16, K contiguous (kp = k rounded up to 8 so rows are 16-byte
+//      multiples).  Transposes through shared memory when the stored matrix
+//      is contiguous along M/N.  Complex operands use the 4M mapping folded
+//      into one real GEMM: A'' = [Re A | Im A] (k' = 2k) and rows
+//      2j, 2j+1 of B'' = [Re B_j | -Im B_j], [Im B_j | Re B_j], so that
+//      columns 2j, 2j+1 of A'' B''^T are Re and Im of C_j.
+//   2. GEMM kernel: one CTA per 128 x BN tile of C.  Warp 0 lane 0 issues
+//      TMA loads of all pieces of a 64-deep K slab into a 2-stage ring
+//      (128-byte swizzle, full/empty mbarriers); warp 1 lane 0 issues the
+//      tcgen05.mma products (M=128, N=BN, K=16 per instruction) into one
+//      fp32 TMEM accumulator of BN columns and commits each stage back to
+//      the producer; then all 4 warps read the accumulator row by row
+//      (tcgen05.ld 32x32b, thread = row) and apply the reference's epilogue
+//      (beta == 0: C = alpha*acc without reading C; beta == 1: C += alpha*acc;
+//      else beta*C + alpha*acc; f32_edge.rs:37-58) with coalesced column
+//      stores.
+// All waits are bounded: a wait that gives up sets the handle's status word
+// (reported as CORAL_ERR_TIMEOUT by coral_sync) and the CTA drains and exits.
+#include "common.cuh"
+#include "tc_common.cuh"
+
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+namespace coral {
+
+// ---- tensor-map encoding (driver entry point, no libcuda link) -------------
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+bool encode_kmajor_map(CUtensorMap* map, const void* base, int elem_bytes, uint64_t inner,
+                       uint64_t outer, uint64_t row_stride_bytes, uint32_t box_inner,
+                       uint32_t box_outer) {
+  auto fn = tmap_encode_fn();
+  if (!fn) return false;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (row_stride_bytes & 15)) return false;
+  cuuint64_t dims[2] = {inner, outer};
+  cuuint64_t strides[1] = {row_stride_bytes};
+  cuuint32_t box[2] = {box_inner, box_outer};
+  cuuint32_t estr[2] = {1, 1};
+  CUtensorMapDataType dt = elem_bytes == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                           : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+  CUresult r = fn(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+namespace {
+
+constexpr int kBM = 128;
+constexpr int kBK = 64;  // bf16 elements per 128-byte swizzled row
+constexpr int kStages = 2;
+constexpr int kGemmThreads = 128;
+
+template <int P> struct SplitPlan;
+// pairs (i, j): product A_i * B_j, smallest terms first
+template <> struct SplitPlan<3> {
+  static constexpr int kPieces = 2, kProducts = 3;
+  __host__ __device__ static constexpr int a(int q) { return q == 0 ? 1 : 0; }
+  __host__ __device__ static constexpr int b(int q) { return q == 1 ? 1 : 0; }
+};
+template <> struct SplitPlan<6> {
+  static constexpr int kPieces = 3, kProducts = 6;
+  __host__ __device__ static constexpr int a(int q) { return q == 0 ? 2 : (q == 2 || q == 3) ? 1 : 0; }
+  __host__ __device__ static constexpr int b(int q) { return q == 1 ? 2 : (q == 2 || q == 4) ? 1 : 0; }
+};
+
+struct SplitMaps {
+  CUtensorMap a[3];
+  CUtensorMap b[3];
+};
+
+// ---- 1. split pre-pass -------------------------------------------------------
+template <int NP>
+__device__ __forceinline__ void split_value(float v, __nv_bfloat16 (&p)[3]) {
+  p[0] = __float2bfloat16_rn(v);
+  float r = v - __bfloat162float(p[0]);
+  p[1] = __float2bfloat16_rn(r);
+  if (NP == 3) {
+    r = r - __bfloat162float(p[1]);
+    p[2] = __float2bfloat16_rn(r);
+  }
+}
+
+// Real operand: dst[p][r][l] = piece p of src(r, l), where src(r, l) is
+// X[l + r*ld] (K-major storage) or X[r + l*ld] (storage contiguous along r).
+// 32 x 32 tiles, 32 x 8 threads; the contiguous-along-r case transposes
+// through shared memory so both the loads and the stores are coalesced.
+template <int NP, bool kKMajorSrc>
+__global__ void __launch_bounds__(256)
+k_split_real(const float* __restrict__ X, size_t ld, int R, int Kd, __nv_bfloat16* __restrict__ dst,
+             size_t kp, size_t piece_stride) {
+  __shared__ float tile[32][33];
+  const int r0 = blockIdx.y * 32, l0 = blockIdx.x * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  if (kKMajorSrc) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int r = r0 + ty + 8 * q, l = l0 + tx;
+      tile[ty + 8 * q][tx] = (r < R && l < Kd) ? __ldg(X + l + (size_t)r * ld) : 0.f;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int l = l0 + ty + 8 * q, r = r0 + tx;
+      tile[tx][ty + 8 * q] = (r < R && l < Kd) ? __ldg(X + r + (size_t)l * ld) : 0.f;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    int r = r0 + ty + 8 * q, l = l0 + tx;
+    if (r < R && l < (int)kp) {
+      __nv_bfloat16 p[3];
+      split_value<NP>(tile[ty + 8 * q][tx], p);
+      size_t o = (size_t)r * kp + l;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) dst[i * piece_stride + o] = p[i];
+    }
+  }
+}
+
+// Complex operand, 4M layout.  src(r, l) is the complex element of op(X)
+// (conjugated when `conj`), storage K-major (X[l + r*ld]) or not (X[r + l*ld]).
+//   kIsB == false: dst row r = [Re src(r, :) | Im src(r, :)]          (k' = 2k)
+//   kIsB == true : dst row 2r = [Re | -Im], row 2r+1 = [Im | Re]       (k' = 2k)
+template <int NP, bool kKMajorSrc, bool kIsB>
+__global__ void __launch_bounds__(256)
+k_split_cplx(const float2* __restrict__ X, size_t ld, int R, int Kd, bool conj,
+             __nv_bfloat16* __restrict__ dst, size_t kp, size_t piece_stride) {
+  __shared__ float2 tile[32][33];
+  const int r0 = blockIdx.y * 32, l0 = blockIdx.x * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  if (kKMajorSrc) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int r = r0 + ty + 8 * q, l = l0 + tx;
+      tile[ty + 8 * q][tx] = (r < R && l < Kd) ? __ldg(X + l + (size_t)r * ld) : make_float2(0.f, 0.f);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int l = l0 + ty + 8 * q, r = r0 + tx;
+      tile[tx][ty + 8 * q] = (r < R && l < Kd) ? __ldg(X + r + (size_t)l * ld) : make_float2(0.f, 0.f);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    int r = r0 + ty + 8 * q, l = l0 + tx;
+    if (r >= R || l >= Kd) continue;
+    float2 v = tile[ty + 8 * q][tx];
+    if (conj) v.y = -v.y;
+    __nv_bfloat16 pr[3], pi[3], pn[3];
+    split_value<NP>(v.x, pr);
+    split_value<NP>(v.y, pi);
+    split_value<NP>(-v.y, pn);
+    if (!kIsB) {
+      size_t o = (size_t)r * kp;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        dst[i * piece_stride + o + l] = pr[i];
+        dst[i * piece_stride + o + Kd + l] = pi[i];
+      }
+    } else {
+      size_t o0 = (size_t)(2 * r) * kp, o1 = o0 + kp;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        dst[i * piece_stride + o0 + l] = pr[i];
+        dst[i * piece_stride + o0 + Kd + l] = pn[i];
+        dst[i * piece_stride + o1 + l] = pi[i];
+        dst[i * piece_stride + o1 + Kd + l] = pr[i];
+      }
+    }
+  }
+}
+
+// ---- 2. tcgen05 GEMM ---------------------------------------------------------
+struct EpiParams {
+  float* C;          // real: float column-major; complex: float2 column-major
+  size_t ldc;
+  int m, n;          // logical C extent (complex: n complex columns)
+  float alpha_re, alpha_im, beta_re, beta_im;
+  int complex_out;   // 1: accumulator columns (2j, 2j+1) are (Re, Im) of C column j
+};
+
+template <int NP, int BN>
+__global__ void __launch_bounds__(kGemmThreads, 1)
+k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int n_tiles,
+             EpiParams ep, unsigned* status, uint64_t limit_ns) {
+  using Plan = SplitPlan<NP>;
+  constexpr int kPieces = Plan::kPieces;
+  constexpr uint32_t kATile = kBM * kBK * 2;  // bytes per A piece tile
+  constexpr uint32_t kBTile = BN * kBK * 2;
+  constexpr uint32_t kStageBytes = kPieces * (kATile + kBTile);
+  constexpr uint32_t kIdesc = tc::idesc_bf16_f32(kBM, BN);
+
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages], done_bar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  // Tile order: groups of 16 M-tiles sweep all N-tiles, so the CTAs resident
+  // at one time share A and B slabs through L2.
+  int tile = blockIdx.x;
+  const int group = 16;
+  const int per_group = group * n_tiles;
+  const int g = tile / per_group;
+  const int gm0 = g * group;
+  const int gsz = min(group, m_tiles - gm0);
+  const int within = tile - g * per_group;
+  const int m_tile = gm0 + within % gsz;
+  const int n_tile = within / gsz;
+  const int m0 = m_tile * kBM, n0 = n_tile * BN;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      tc::mbar_init(&full_bar[s], 1);
+      tc::mbar_init(&empty_bar[s], 1);
+    }
+    tc::mbar_init(&done_bar, 1);
+    abort_flag = 0;
+    tc::fence_mbar_init();
+  }
+  if (warp == 1) {
+    tc::tmem_alloc(&tmem_slot, BN);
+    tc::tmem_relinquish();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  const int nk = (kdim + kBK - 1) / kBK;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer ----
+    for (int p = 0; p < kPieces; ++p) {
+      tc::prefetch_tmap(&maps.a[p]);
+      tc::prefetch_tmap(&maps.b[p]);
+    }
+    int issued = 0;
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % kStages;
+      if (kb >= kStages && !tc::mbar_wait(&empty_bar[s], ((kb / kStages) - 1) & 1, limit_ns)) {
+        atomicOr(status, kStatusTimeout);
+        atomicExch(&abort_flag, 1);
+        break;
+      }
+      if (*(volatile int*)&abort_flag) break;
+      uint8_t* st = smem + (size_t)s * kStageBytes;
+      tc::mbar_expect_tx(&full_bar[s], kStageBytes);
+      for (int p = 0; p < kPieces; ++p) {
+        tc::tma_load_2d(st + p * kATile, &maps.a[p], &full_bar[s], kb * kBK, m0);
+        tc::tma_load_2d(st + kPieces * kATile + p * kBTile, &maps.b[p], &full_bar[s], kb * kBK, n0);
+      }
+      issued = kb + 1;
+    }
+    // Drain: every issued load must land before the CTA may exit.
+    for (int kb = (issued > kStages ? issued - kStages : 0); kb < issued; ++kb)
+      tc::mbar_wait(&full_bar[kb % kStages], (kb / kStages) & 1, limit_ns);
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----
+    int kb = 0;
+    for (; kb < nk; ++kb) {
+      const int s = kb % kStages;
+      if (!tc::mbar_wait(&full_bar[s], (kb / kStages) & 1, limit_ns)) {
+        atomicOr(status, kStatusTimeout);
+        atomicExch(&abort_flag, 1);
+        break;
+      }
+      tc::tc_fence_after();
+      const uint32_t sa = tc::smem_u32(smem + (size_t)s * kStageBytes);
+      const uint32_t sb = sa + kPieces * kATile;
+#pragma unroll
+      for (int kk = 0; kk < kBK / 16; ++kk) {
+#pragma unroll
+        for (int q = 0; q < Plan::kProducts; ++q) {
+          const uint64_t ad = tc::desc_k_sw128(sa + Plan::a(q) * kATile + kk * 32);
+          const uint64_t bd = tc::desc_k_sw128(sb + Plan::b(q) * kBTile + kk * 32);
+          tc::mma_f16(tmem, ad, bd, kIdesc, (kb | kk | q) != 0);
+        }
+      }
+      tc::mma_commit(&empty_bar[s]);
+    }
+    tc::mma_commit(&done_bar);
+  }
+  __syncwarp();
+
+  // ---- epilogue: TMEM -> registers -> C ----
+  const bool ok = tc::mbar_wait(&done_bar, 0, limit_ns);
+  if (!ok) atomicOr(status, kStatusTimeout);
+  tc::tc_fence_after();
+  const bool store = ok && !*(volatile int*)&abort_flag;
+  const int row = m0 + warp * 32 + lane;
+  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  const bool beta0 = ep.beta_re == 0.f && ep.beta_im == 0.f;
+  const bool beta1 = ep.beta_re == 1.f && ep.beta_im == 0.f;
+#pragma unroll 1
+  for (int c0 = 0; c0 < BN; c0 += 32) {
+    uint32_t r[32];
+    tc::tmem_ld32(tmem + lane_base + c0, r);
+    tc::tmem_wait_ld();
+    if (!store || row >= ep.m) continue;
+    if (!ep.complex_out) {
+      float* crow = ep.C + row;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int col = n0 + c0 + j;
+        if (col >= ep.n) break;
+        float v = ep.alpha_re * __uint_as_float(r[j]);
+        float* cp = crow + (size_t)col * ep.ldc;
+        if (beta0) *cp = v;
+        else if (beta1) *cp = *cp + v;
+        else *cp = ep.beta_re * *cp + v;
+      }
+    } else {
+      float2* crow = reinterpret_cast<float2*>(ep.C) + row;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int col = (n0 + c0) / 2 + j;
+        if (col >= ep.n) break;
+        const float ar = __uint_as_float(r[2 * j]), ai = __uint_as_float(r[2 * j + 1]);
+        float2 v = make_float2(ep.alpha_re * ar - ep.alpha_im * ai, ep.alpha_re * ai + ep.alpha_im * ar);
+        float2* cp = crow + (size_t)col * ep.ldc;
+        if (!beta0) {
+          float2 c = *cp;
+          if (beta1) { v.x += c.x; v.y += c.y; }
+          else {
+            v.x += ep.beta_re * c.x - ep.beta_im * c.y;
+            v.y += ep.beta_re * c.y + ep.beta_im * c.x;
+          }
+        }
+        *cp = v;
+      }
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 1) tc::tmem_dealloc(tmem, BN);
+}
+
+template <int NP> constexpr int tile_n() { return NP == 3 ? 256 : 128; }
+
+template <int NP>
+size_t gemm_smem_bytes() {
+  constexpr int BN = tile_n<NP>();
+  return (size_t)kStages * SplitPlan<NP>::kPieces * (kBM * kBK * 2 + BN * kBK * 2) + 1024;
+}
+
+// Runs the GEMM kernel over prepared pieces: A pieces [mr][kp], B pieces [nr][kp].
+template <int NP>
+coral_status_t run_split_gemm(Handle* h, const __nv_bfloat16* ap, size_t a_piece, int mr,
+                              const __nv_bfloat16* bp, size_t b_piece, int nr, int kd, size_t kp,
+                              const EpiParams& ep) {
+  constexpr int BN = tile_n<NP>();
+  SplitMaps maps;
+  std::memset(&maps, 0, sizeof(maps));
+  for (int p = 0; p < SplitPlan<NP>::kPieces; ++p) {
+    if (!encode_kmajor_map(&maps.a[p], ap + p * a_piece, 2, (uint64_t)kd, (uint64_t)mr, kp * 2, kBK, kBM) ||
+        !encode_kmajor_map(&maps.b[p], bp + p * b_piece, 2, (uint64_t)kd, (uint64_t)nr, kp * 2, kBK, BN))
+      return CORAL_ERR_NOT_SUPPORTED;
+  }
+  const size_t smem = gemm_smem_bytes<NP>();
+  static bool attr_set = false;
+  if (!attr_set) {
+    CORAL_CUDA(h, cudaFuncSetAttribute(k_gemm_split<NP, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    attr_set = true;
+  }
+  const int m_tiles = (mr + kBM - 1) / kBM, n_tiles = (nr + BN - 1) / BN;
+  const uint64_t limit_ns = h->wait_limit * 32ull;  // default 2^26 * 32 ns ~ 2.1 s
+  k_gemm_split<NP, BN><<<m_tiles * n_tiles, kGemmThreads, smem, h->stream>>>(
+      maps, kd, m_tiles, n_tiles, ep, &h->words->status, limit_ns);
+  return launch_status(h);
+}
+
+template <int NP>
+coral_status_t sgemm_split_impl(Handle* h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                                float alpha, const float* A, size_t lda, const float* B, size_t ldb,
+                                float beta, float* C, size_t ldc) {
+  const size_t kp = (k + 7) & ~size_t(7);
+  const size_t a_piece = m * kp, b_piece = n * kp;
+  const size_t a_bytes = ((NP == 3 ? 2 : 3) * a_piece * 2 + 255) & ~size_t(255);
+  const size_t b_bytes = (NP == 3 ? 2 : 3) * b_piece * 2;
+  char* sc = static_cast<char*>(scratch(h, a_bytes + b_bytes));
+  if (!sc) return CORAL_ERR_ALLOC;
+  __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(sc);
+  __nv_bfloat16* bp = reinterpret_cast<__nv_bfloat16*>(sc + a_bytes);
+  // op(A) rows are i: storage K-major iff op_a is (conjugate) transpose.
+  dim3 ga((unsigned)((kp + 31) / 32), (unsigned)((m + 31) / 32));
+  if (op_a == CORAL_NO_TRANSPOSE)
+    k_split_real<NP, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ap, kp, a_piece);
+  else
+    k_split_real<NP, true><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ap, kp, a_piece);
+  coral_status_t s = launch_status(h);
+  if (s != CORAL_OK) return s;
+  // op(B)^T rows are j: storage K-major iff op_b is NoTranspose.
+  dim3 gb((unsigned)((kp + 31) / 32), (unsigned)((n + 31) / 32));
+  if (op_b == CORAL_NO_TRANSPOSE)
+    k_split_real<NP, true><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, bp, kp, b_piece);
+  else
+    k_split_real<NP, false><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, bp, kp, b_piece);
+  s = launch_status(h);
+  if (s != CORAL_OK) return s;
+  EpiParams ep{C, ldc, (int)m, (int)n, alpha, 0.f, beta, 0.f, 0};
+  return run_split_gemm<NP>(h, ap, a_piece, (int)m, bp, b_piece, (int)n, (int)k, kp, ep);
+}
+
+template <int NP>
+coral_status_t cgemm_split_impl(Handle* h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                                float2 alpha, const float2* A, size_t lda, const float2* B,
+                                size_t ldb, float2 beta, float2* C, size_t ldc) {
+  const size_t k2 = 2 * k;
+  const size_t kp = (k2 + 7) & ~size_t(7);
+  const size_t a_piece = m * kp, b_piece = 2 * n * kp;
+  const size_t a_bytes = ((NP == 3 ? 2 : 3) * a_piece * 2 + 255) & ~size_t(255);
+  const size_t b_bytes = (NP == 3 ? 2 : 3) * b_piece * 2;
+  char* sc = static_cast<char*>(scratch(h, a_bytes + b_bytes));
+  if (!sc) return CORAL_ERR_ALLOC;
+  __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(sc);
+  __nv_bfloat16* bp = reinterpret_cast<__nv_bfloat16*>(sc + a_bytes);
+  if (kp != k2) {  // zero the row tails so every byte TMA may read is defined
+    CORAL_CUDA(h, cudaMemsetAsync(sc, 0, a_bytes + b_bytes, h->stream));
+  }
+  dim3 ga((unsigned)((k + 31) / 32), (unsigned)((m + 31) / 32));
+  const bool ca = op_a == CORAL_CONJ_TRANSPOSE, cbj = op_b == CORAL_CONJ_TRANSPOSE;
+  if (op_a == CORAL_NO_TRANSPOSE)
+    k_split_cplx<NP, false, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ca, ap, kp, a_piece);
+  else
+    k_split_cplx<NP, true, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ca, ap, kp, a_piece);
+  coral_status_t s = launch_status(h);
+  if (s != CORAL_OK) return s;
+  dim3 gb((unsigned)((k + 31) / 32), (unsigned)((n + 31) / 32));
+  if (op_b == CORAL_NO_TRANSPOSE)
+    k_split_cplx<NP, true, true><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, cbj, bp, kp, b_piece);
+  else
+    k_split_cplx<NP, false, true><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, cbj, bp, kp, b_piece);
+  s = launch_status(h);
+  if (s != CORAL_OK) return s;
+  EpiParams ep{reinterpret_cast<float*>(C), ldc, (int)m, (int)n, alpha.x, alpha.y, beta.x, beta.y, 1};
+  return run_split_gemm<NP>(h, ap, a_piece, (int)m, bp, b_piece, (int)(2 * n), (int)k2, kp, ep);
+}
+
+}  // namespace
+
+coral_status_t enqueue_sgemm_split(Handle* h, int terms, int op_a, int op_b, size_t m, size_t n,
+                                   size_t k, float alpha, const float* A, size_t lda,
+                                   const float* B, size_t ldb, float beta, float* C, size_t ldc) {
+  if (m > (size_t)INT32_MAX / 2 || n > (size_t)INT32_MAX / 2 || k > (size_t)INT32_MAX / 2)
+    return CORAL_ERR_NOT_SUPPORTED;
+  return terms == 6 ? sgemm_split_impl<6>(h, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc)
+                    : sgemm_split_impl<3>(h, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+coral_status_t enqueue_cgemm_split(Handle* h, int terms, int op_a, int op_b, size_t m, size_t n,
+                                   size_t k, float2 alpha, const float2* A, size_t lda,
+                                   const float2* B, size_t ldb, float2 beta, float2* C, size_t ldc) {
+  if (m > (size_t)INT32_MAX / 4 || n > (size_t)INT32_MAX / 4 || k > (size_t)INT32_MAX / 4)
+    return CORAL_ERR_NOT_SUPPORTED;
+  return terms == 6 ? cgemm_split_impl<6>(h, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc)
+                    : cgemm_split_impl<3>(h, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+}  // namespace coral
