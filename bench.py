@@ -341,7 +341,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["native", "split_bf16x3", "split_bf16x6"], default="native")
+    ap.add_argument("--mode", choices=["native", "split_bf16x3", "split_bf16x6"], default="split_bf16x3")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     args = ap.parse_args()

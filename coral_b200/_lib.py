@@ -35,6 +35,7 @@ SIGNATURES = {
     "coral_set_gemm_mode": [_h, _i],
     "coral_get_gemm_mode": [_h, C.POINTER(_i)],
     "coral_set_wait_limit": [_h, C.c_uint64],
+    "coral_set_split_chunk": [_h, _i],
     "coral_sync": [_h],
     "coral_last_bad_arg": [_h],
     "coral_status_string": [_st],

@@ -98,6 +98,9 @@ class Handle:
         self.check(self.lib.coral_get_gemm_mode(self.h, C.byref(m)), "coral_get_gemm_mode")
         return m.value
 
+    def set_split_chunk(self, slabs: int) -> None:
+        self.check(self.lib.coral_set_split_chunk(self.h, slabs), "coral_set_split_chunk")
+
     def set_wait_limit(self, spins: int) -> None:
         self.check(self.lib.coral_set_wait_limit(self.h, spins), "coral_set_wait_limit")
 

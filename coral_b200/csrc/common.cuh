@@ -24,6 +24,8 @@ struct Handle {
   int pointer_mode = CORAL_POINTER_HOST;
   int gemm_mode = CORAL_GEMM_NATIVE;
   uint64_t wait_limit = kDefaultWaitLimit;
+  // K slabs (64 deep) per tensor-core accumulation chunk of the split GEMMs.
+  int split_chunk_kb = 16;
   int bad_arg = 0;
   std::string cuda_error;
 

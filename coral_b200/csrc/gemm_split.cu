@@ -72,7 +72,6 @@ namespace {
 constexpr int kBM = 128;
 constexpr int kBK = 64;  // bf16 elements per 128-byte swizzled row
 constexpr int kStages = 2;
-constexpr int kGemmThreads = 128;
 
 template <int P> struct SplitPlan;
 // pairs (i, j): product A_i * B_j, smallest terms first
@@ -93,12 +92,15 @@ struct SplitMaps {
 };
 
 // ---- 1. split pre-pass -------------------------------------------------------
-template <int NP>
+// NPC = number of bf16 pieces (2 or 3).
+template <int NPC>
 __device__ __forceinline__ void split_value(float v, __nv_bfloat16 (&p)[3]) {
+  static_assert(NPC == 2 || NPC == 3, "2 or 3 pieces");
   p[0] = __float2bfloat16_rn(v);
   float r = v - __bfloat162float(p[0]);
   p[1] = __float2bfloat16_rn(r);
-  if (NP == 3) {
+  p[2] = __float2bfloat16_rn(0.f);
+  if (NPC == 3) {
     r = r - __bfloat162float(p[1]);
     p[2] = __float2bfloat16_rn(r);
   }
@@ -108,7 +110,7 @@ __device__ __forceinline__ void split_value(float v, __nv_bfloat16 (&p)[3]) {
 // X[l + r*ld] (K-major storage) or X[r + l*ld] (storage contiguous along r).
 // 32 x 32 tiles, 32 x 8 threads; the contiguous-along-r case transposes
 // through shared memory so both the loads and the stores are coalesced.
-template <int NP, bool kKMajorSrc>
+template <int NPC, bool kKMajorSrc>
 __global__ void __launch_bounds__(256)
 k_split_real(const float* __restrict__ X, size_t ld, int R, int Kd, __nv_bfloat16* __restrict__ dst,
              size_t kp, size_t piece_stride) {
@@ -134,10 +136,10 @@ k_split_real(const float* __restrict__ X, size_t ld, int R, int Kd, __nv_bfloat1
     int r = r0 + ty + 8 * q, l = l0 + tx;
     if (r < R && l < (int)kp) {
       __nv_bfloat16 p[3];
-      split_value<NP>(tile[ty + 8 * q][tx], p);
+      split_value<NPC>(tile[ty + 8 * q][tx], p);
       size_t o = (size_t)r * kp + l;
 #pragma unroll
-      for (int i = 0; i < NP; ++i) dst[i * piece_stride + o] = p[i];
+      for (int i = 0; i < NPC; ++i) dst[i * piece_stride + o] = p[i];
     }
   }
 }
@@ -146,7 +148,7 @@ k_split_real(const float* __restrict__ X, size_t ld, int R, int Kd, __nv_bfloat1
 // (conjugated when `conj`), storage K-major (X[l + r*ld]) or not (X[r + l*ld]).
 //   kIsB == false: dst row r = [Re src(r, :) | Im src(r, :)]          (k' = 2k)
 //   kIsB == true : dst row 2r = [Re | -Im], row 2r+1 = [Im | Re]       (k' = 2k)
-template <int NP, bool kKMajorSrc, bool kIsB>
+template <int NPC, bool kKMajorSrc, bool kIsB>
 __global__ void __launch_bounds__(256)
 k_split_cplx(const float2* __restrict__ X, size_t ld, int R, int Kd, bool conj,
              __nv_bfloat16* __restrict__ dst, size_t kp, size_t piece_stride) {
@@ -174,20 +176,20 @@ k_split_cplx(const float2* __restrict__ X, size_t ld, int R, int Kd, bool conj,
     float2 v = tile[ty + 8 * q][tx];
     if (conj) v.y = -v.y;
     __nv_bfloat16 pr[3], pi[3], pn[3];
-    split_value<NP>(v.x, pr);
-    split_value<NP>(v.y, pi);
-    split_value<NP>(-v.y, pn);
+    split_value<NPC>(v.x, pr);
+    split_value<NPC>(v.y, pi);
+    split_value<NPC>(-v.y, pn);
     if (!kIsB) {
       size_t o = (size_t)r * kp;
 #pragma unroll
-      for (int i = 0; i < NP; ++i) {
+      for (int i = 0; i < NPC; ++i) {
         dst[i * piece_stride + o + l] = pr[i];
         dst[i * piece_stride + o + Kd + l] = pi[i];
       }
     } else {
       size_t o0 = (size_t)(2 * r) * kp, o1 = o0 + kp;
 #pragma unroll
-      for (int i = 0; i < NP; ++i) {
+      for (int i = 0; i < NPC; ++i) {
         dst[i * piece_stride + o0 + l] = pr[i];
         dst[i * piece_stride + o0 + Kd + l] = pn[i];
         dst[i * piece_stride + o1 + l] = pi[i];
@@ -206,162 +208,232 @@ struct EpiParams {
   int complex_out;   // 1: accumulator columns (2j, 2j+1) are (Re, Im) of C column j
 };
 
-template <int NP, int BN>
-__global__ void __launch_bounds__(kGemmThreads, 1)
-k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int n_tiles,
-             EpiParams ep, unsigned* status, uint64_t limit_ns) {
-  using Plan = SplitPlan<NP>;
-  constexpr int kPieces = Plan::kPieces;
-  constexpr uint32_t kATile = kBM * kBK * 2;  // bytes per A piece tile
-  constexpr uint32_t kBTile = BN * kBK * 2;
-  constexpr uint32_t kStageBytes = kPieces * (kATile + kBTile);
-  constexpr uint32_t kIdesc = tc::idesc_bf16_f32(kBM, BN);
-
-  extern __shared__ __align__(1024) uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages], done_bar;
-  __shared__ uint32_t tmem_slot;
-  __shared__ int abort_flag;
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-  // Tile order: groups of 16 M-tiles sweep all N-tiles, so the CTAs resident
-  // at one time share A and B slabs through L2.
-  int tile = blockIdx.x;
+// Tile order: groups of 16 M-tiles sweep all N-tiles, so CTAs resident at
+// the same time share A and B slabs through L2.
+__device__ __forceinline__ void tile_coords(int tile, int m_tiles, int n_tiles, int& mt, int& nt) {
   const int group = 16;
   const int per_group = group * n_tiles;
   const int g = tile / per_group;
   const int gm0 = g * group;
   const int gsz = min(group, m_tiles - gm0);
   const int within = tile - g * per_group;
-  const int m_tile = gm0 + within % gsz;
-  const int n_tile = within / gsz;
-  const int m0 = m_tile * kBM, n0 = n_tile * BN;
+  mt = gm0 + within % gsz;
+  nt = within / gsz;
+}
+
+// Persistent kernel, 2 + 8 warps:
+//   warp 0 lane 0: TMA producer over a 2-stage ring of K slabs (all pieces);
+//   warp 1 lane 0: tcgen05.mma issuer.  The K loop of a tile is cut into
+//     chunks of `chunk_kb` slabs; chunk c accumulates (from zero) into TMEM
+//     buffer c % 2 and is committed to chunk_full[c % 2];
+//   warps 2-9: drain each finished chunk into fp32 registers with
+//     round-to-nearest adds (thread = one row of the tile, half of the
+//     columns), release the buffer (chunk_empty), and after the tile's last
+//     chunk apply the epilogue and store C.
+// Draining per chunk bounds how many tensor-core accumulation steps any
+// partial sum goes through; the register adds round to nearest.
+constexpr int kEpiWarps = 8;
+constexpr int kSplitThreads = 64 + 32 * kEpiWarps;
+
+template <int NP, int BN>
+__global__ void __launch_bounds__(kSplitThreads, 1)
+k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int n_tiles,
+             int chunk_kb, EpiParams ep, unsigned* status, uint64_t limit_ns) {
+  using Plan = SplitPlan<NP>;
+  constexpr int kPieces = Plan::kPieces;
+  constexpr uint32_t kATile = kBM * kBK * 2;  // bytes per A piece tile
+  constexpr uint32_t kBTile = BN * kBK * 2;
+  constexpr uint32_t kStageBytes = kPieces * (kATile + kBTile);
+  constexpr uint32_t kIdesc = tc::idesc_bf16_f32(kBM, BN);
+  constexpr int kCols = BN / 2;  // accumulator columns per epilogue thread
+
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages];
+  __shared__ __align__(8) uint64_t chunk_full[2], chunk_empty[2];
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nk = (kdim + kBK - 1) / kBK;
+  const int chunks_per_tile = (nk + chunk_kb - 1) / chunk_kb;
+  const int total_tiles = m_tiles * n_tiles;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       tc::mbar_init(&full_bar[s], 1);
       tc::mbar_init(&empty_bar[s], 1);
     }
-    tc::mbar_init(&done_bar, 1);
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(&chunk_full[b], 1);
+      tc::mbar_init(&chunk_empty[b], kEpiWarps);
+    }
     abort_flag = 0;
     tc::fence_mbar_init();
   }
   if (warp == 1) {
-    tc::tmem_alloc(&tmem_slot, BN);
+    tc::tmem_alloc(&tmem_slot, 2 * BN);
     tc::tmem_relinquish();
   }
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = tmem_slot;
-  const int nk = (kdim + kBK - 1) / kBK;
 
-  if (warp == 0 && lane == 0) {
-    // ---- TMA producer ----
-    for (int p = 0; p < kPieces; ++p) {
-      tc::prefetch_tmap(&maps.a[p]);
-      tc::prefetch_tmap(&maps.b[p]);
-    }
-    int issued = 0;
-    for (int kb = 0; kb < nk; ++kb) {
-      const int s = kb % kStages;
-      if (kb >= kStages && !tc::mbar_wait(&empty_bar[s], ((kb / kStages) - 1) & 1, limit_ns)) {
-        atomicOr(status, kStatusTimeout);
-        atomicExch(&abort_flag, 1);
-        break;
-      }
-      if (*(volatile int*)&abort_flag) break;
-      uint8_t* st = smem + (size_t)s * kStageBytes;
-      tc::mbar_expect_tx(&full_bar[s], kStageBytes);
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- TMA producer ----
       for (int p = 0; p < kPieces; ++p) {
-        tc::tma_load_2d(st + p * kATile, &maps.a[p], &full_bar[s], kb * kBK, m0);
-        tc::tma_load_2d(st + kPieces * kATile + p * kBTile, &maps.b[p], &full_bar[s], kb * kBK, n0);
+        tc::prefetch_tmap(&maps.a[p]);
+        tc::prefetch_tmap(&maps.b[p]);
       }
-      issued = kb + 1;
-    }
-    // Drain: every issued load must land before the CTA may exit.
-    for (int kb = (issued > kStages ? issued - kStages : 0); kb < issued; ++kb)
-      tc::mbar_wait(&full_bar[kb % kStages], (kb / kStages) & 1, limit_ns);
-  } else if (warp == 1 && lane == 0) {
-    // ---- MMA issuer ----
-    int kb = 0;
-    for (; kb < nk; ++kb) {
-      const int s = kb % kStages;
-      if (!tc::mbar_wait(&full_bar[s], (kb / kStages) & 1, limit_ns)) {
-        atomicOr(status, kStatusTimeout);
-        atomicExch(&abort_flag, 1);
-        break;
-      }
-      tc::tc_fence_after();
-      const uint32_t sa = tc::smem_u32(smem + (size_t)s * kStageBytes);
-      const uint32_t sb = sa + kPieces * kATile;
-#pragma unroll
-      for (int kk = 0; kk < kBK / 16; ++kk) {
-#pragma unroll
-        for (int q = 0; q < Plan::kProducts; ++q) {
-          const uint64_t ad = tc::desc_k_sw128(sa + Plan::a(q) * kATile + kk * 32);
-          const uint64_t bd = tc::desc_k_sw128(sb + Plan::b(q) * kBTile + kk * 32);
-          tc::mma_f16(tmem, ad, bd, kIdesc, (kb | kk | q) != 0);
-        }
-      }
-      tc::mma_commit(&empty_bar[s]);
-    }
-    tc::mma_commit(&done_bar);
-  }
-  __syncwarp();
-
-  // ---- epilogue: TMEM -> registers -> C ----
-  const bool ok = tc::mbar_wait(&done_bar, 0, limit_ns);
-  if (!ok) atomicOr(status, kStatusTimeout);
-  tc::tc_fence_after();
-  const bool store = ok && !*(volatile int*)&abort_flag;
-  const int row = m0 + warp * 32 + lane;
-  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-  const bool beta0 = ep.beta_re == 0.f && ep.beta_im == 0.f;
-  const bool beta1 = ep.beta_re == 1.f && ep.beta_im == 0.f;
-#pragma unroll 1
-  for (int c0 = 0; c0 < BN; c0 += 32) {
-    uint32_t r[32];
-    tc::tmem_ld32(tmem + lane_base + c0, r);
-    tc::tmem_wait_ld();
-    if (!store || row >= ep.m) continue;
-    if (!ep.complex_out) {
-      float* crow = ep.C + row;
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const int col = n0 + c0 + j;
-        if (col >= ep.n) break;
-        float v = ep.alpha_re * __uint_as_float(r[j]);
-        float* cp = crow + (size_t)col * ep.ldc;
-        if (beta0) *cp = v;
-        else if (beta1) *cp = *cp + v;
-        else *cp = ep.beta_re * *cp + v;
-      }
-    } else {
-      float2* crow = reinterpret_cast<float2*>(ep.C) + row;
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int col = (n0 + c0) / 2 + j;
-        if (col >= ep.n) break;
-        const float ar = __uint_as_float(r[2 * j]), ai = __uint_as_float(r[2 * j + 1]);
-        float2 v = make_float2(ep.alpha_re * ar - ep.alpha_im * ai, ep.alpha_re * ai + ep.alpha_im * ar);
-        float2* cp = crow + (size_t)col * ep.ldc;
-        if (!beta0) {
-          float2 c = *cp;
-          if (beta1) { v.x += c.x; v.y += c.y; }
-          else {
-            v.x += ep.beta_re * c.x - ep.beta_im * c.y;
-            v.y += ep.beta_re * c.y + ep.beta_im * c.x;
+      int it = 0;  // k-slab counter across tiles
+      for (int tile = blockIdx.x; tile < total_tiles && !abort_flag; tile += gridDim.x) {
+        int mt, nt;
+        tile_coords(tile, m_tiles, n_tiles, mt, nt);
+        for (int kb = 0; kb < nk; ++kb, ++it) {
+          const int s = it % kStages;
+          if (it >= kStages && !tc::mbar_wait(&empty_bar[s], ((it / kStages) - 1) & 1, limit_ns)) {
+            atomicOr(status, kStatusTimeout);
+            atomicExch(&abort_flag, 1);
+            break;
+          }
+          if (*(volatile int*)&abort_flag) break;
+          uint8_t* st = smem + (size_t)s * kStageBytes;
+          tc::mbar_expect_tx(&full_bar[s], kStageBytes);
+          for (int p = 0; p < kPieces; ++p) {
+            tc::tma_load_2d(st + p * kATile, &maps.a[p], &full_bar[s], kb * kBK, mt * kBM);
+            tc::tma_load_2d(st + kPieces * kATile + p * kBTile, &maps.b[p], &full_bar[s], kb * kBK, nt * BN);
           }
         }
-        *cp = v;
+      }
+      // Drain: every issued load lands before the CTA may exit.
+      for (int j = (it > kStages ? it - kStages : 0); j < it; ++j)
+        tc::mbar_wait(&full_bar[j % kStages], (j / kStages) & 1, limit_ns);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---- MMA issuer ----
+      int it = 0, gc = 0;  // k-slab and chunk counters across tiles
+      bool stop = false;
+      for (int tile = blockIdx.x; tile < total_tiles && !stop; tile += gridDim.x) {
+        for (int c = 0; c < chunks_per_tile && !stop; ++c, ++gc) {
+          const int b = gc & 1;
+          if (gc >= 2 && !tc::mbar_wait(&chunk_empty[b], ((gc >> 1) - 1) & 1, limit_ns)) {
+            atomicOr(status, kStatusTimeout);
+            atomicExch(&abort_flag, 1);
+            stop = true;
+            break;
+          }
+          tc::tc_fence_after();
+          const uint32_t acc = tmem + b * BN;
+          const int kb0 = c * chunk_kb, kb1 = min(nk, kb0 + chunk_kb);
+          for (int kb = kb0; kb < kb1; ++kb, ++it) {
+            const int s = it % kStages;
+            if (!tc::mbar_wait(&full_bar[s], (it / kStages) & 1, limit_ns)) {
+              atomicOr(status, kStatusTimeout);
+              atomicExch(&abort_flag, 1);
+              stop = true;
+              break;
+            }
+            tc::tc_fence_after();
+            const uint32_t sa = tc::smem_u32(smem + (size_t)s * kStageBytes);
+            const uint32_t sb = sa + kPieces * kATile;
+#pragma unroll
+            for (int kk = 0; kk < kBK / 16; ++kk) {
+#pragma unroll
+              for (int q = 0; q < Plan::kProducts; ++q) {
+                const uint64_t ad = tc::desc_k_sw128(sa + Plan::a(q) * kATile + kk * 32);
+                const uint64_t bd = tc::desc_k_sw128(sb + Plan::b(q) * kBTile + kk * 32);
+                tc::mma_f16(acc, ad, bd, kIdesc, ((kb - kb0) | kk | q) != 0);
+              }
+            }
+            tc::mma_commit(&empty_bar[s]);
+          }
+          tc::mma_commit(&chunk_full[b]);
+        }
+      }
+    }
+  } else {
+    // ---- epilogue warps ----
+    const int ew = warp - 2;
+    const int quad = warp & 3;           // TMEM lane quadrant this warp may access
+    const int half = ew >> 2;            // column half of the tile
+    const uint32_t lane_base = (uint32_t)(quad * 32) << 16;
+    const bool beta0 = ep.beta_re == 0.f && ep.beta_im == 0.f;
+    const bool beta1 = ep.beta_re == 1.f && ep.beta_im == 0.f;
+    int gc = 0;
+    bool stop = false;
+    for (int tile = blockIdx.x; tile < total_tiles && !stop; tile += gridDim.x) {
+      int mt, nt;
+      tile_coords(tile, m_tiles, n_tiles, mt, nt);
+      float sum[kCols];
+#pragma unroll
+      for (int j = 0; j < kCols; ++j) sum[j] = 0.f;
+      for (int c = 0; c < chunks_per_tile; ++c, ++gc) {
+        const int b = gc & 1;
+        if (!tc::mbar_wait(&chunk_full[b], (gc >> 1) & 1, limit_ns)) {
+          atomicOr(status, kStatusTimeout);
+          stop = true;
+          break;
+        }
+        tc::tc_fence_after();
+        const uint32_t acc = tmem + b * BN + half * kCols + lane_base;
+#pragma unroll
+        for (int c0 = 0; c0 < kCols; c0 += 32) {
+          uint32_t r[32];
+          tc::tmem_ld32(acc + c0, r);
+          tc::tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 32; ++j) sum[c0 + j] += __uint_as_float(r[j]);
+        }
+        tc::tc_fence_before();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&chunk_empty[b]);
+      }
+      if (stop || *(volatile int*)&abort_flag) break;
+      const int row = mt * kBM + quad * 32 + lane;
+      if (row >= ep.m) continue;
+      const int col0 = nt * BN + half * kCols;  // first accumulator column of this thread
+      if (!ep.complex_out) {
+        float* crow = ep.C + row;
+#pragma unroll
+        for (int j = 0; j < kCols; ++j) {
+          const int col = col0 + j;
+          if (col < ep.n) {
+            float v = ep.alpha_re * sum[j];
+            float* cp = crow + (size_t)col * ep.ldc;
+            if (beta0) *cp = v;
+            else if (beta1) *cp = *cp + v;
+            else *cp = ep.beta_re * *cp + v;
+          }
+        }
+      } else {
+        float2* crow = reinterpret_cast<float2*>(ep.C) + row;
+#pragma unroll
+        for (int j = 0; j < kCols / 2; ++j) {
+          const int col = col0 / 2 + j;
+          if (col < ep.n) {
+            const float ar = sum[2 * j], ai = sum[2 * j + 1];
+            float2 v = make_float2(ep.alpha_re * ar - ep.alpha_im * ai, ep.alpha_re * ai + ep.alpha_im * ar);
+            float2* cp = crow + (size_t)col * ep.ldc;
+            if (!beta0) {
+              float2 cv = *cp;
+              if (beta1) { v.x += cv.x; v.y += cv.y; }
+              else {
+                v.x += ep.beta_re * cv.x - ep.beta_im * cv.y;
+                v.y += ep.beta_re * cv.y + ep.beta_im * cv.x;
+              }
+            }
+            *cp = v;
+          }
+        }
       }
     }
   }
   tc::tc_fence_before();
   __syncthreads();
-  if (warp == 1) tc::tmem_dealloc(tmem, BN);
+  if (warp == 1) tc::tmem_dealloc(tmem, 2 * BN);
 }
 
 template <int NP> constexpr int tile_n() { return NP == 3 ? 256 : 128; }
@@ -393,9 +465,11 @@ coral_status_t run_split_gemm(Handle* h, const __nv_bfloat16* ap, size_t a_piece
     attr_set = true;
   }
   const int m_tiles = (mr + kBM - 1) / kBM, n_tiles = (nr + BN - 1) / BN;
+  const int tiles = m_tiles * n_tiles;
+  const int grid = tiles < h->sm_count ? tiles : h->sm_count;
   const uint64_t limit_ns = h->wait_limit * 32ull;  // default 2^26 * 32 ns ~ 2.1 s
-  k_gemm_split<NP, BN><<<m_tiles * n_tiles, kGemmThreads, smem, h->stream>>>(
-      maps, kd, m_tiles, n_tiles, ep, &h->words->status, limit_ns);
+  k_gemm_split<NP, BN><<<grid, kSplitThreads, smem, h->stream>>>(
+      maps, kd, m_tiles, n_tiles, h->split_chunk_kb, ep, &h->words->status, limit_ns);
   return launch_status(h);
 }
 
@@ -403,10 +477,11 @@ template <int NP>
 coral_status_t sgemm_split_impl(Handle* h, int op_a, int op_b, size_t m, size_t n, size_t k,
                                 float alpha, const float* A, size_t lda, const float* B, size_t ldb,
                                 float beta, float* C, size_t ldc) {
+  constexpr int NPC = SplitPlan<NP>::kPieces;
   const size_t kp = (k + 7) & ~size_t(7);
   const size_t a_piece = m * kp, b_piece = n * kp;
-  const size_t a_bytes = ((NP == 3 ? 2 : 3) * a_piece * 2 + 255) & ~size_t(255);
-  const size_t b_bytes = (NP == 3 ? 2 : 3) * b_piece * 2;
+  const size_t a_bytes = (NPC * a_piece * 2 + 255) & ~size_t(255);
+  const size_t b_bytes = NPC * b_piece * 2;
   char* sc = static_cast<char*>(scratch(h, a_bytes + b_bytes));
   if (!sc) return CORAL_ERR_ALLOC;
   __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(sc);
@@ -414,17 +489,17 @@ coral_status_t sgemm_split_impl(Handle* h, int op_a, int op_b, size_t m, size_t 
   // op(A) rows are i: storage K-major iff op_a is (conjugate) transpose.
   dim3 ga((unsigned)((kp + 31) / 32), (unsigned)((m + 31) / 32));
   if (op_a == CORAL_NO_TRANSPOSE)
-    k_split_real<NP, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ap, kp, a_piece);
+    k_split_real<NPC, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ap, kp, a_piece);
   else
-    k_split_real<NP, true><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ap, kp, a_piece);
+    k_split_real<NPC, true><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ap, kp, a_piece);
   coral_status_t s = launch_status(h);
   if (s != CORAL_OK) return s;
   // op(B)^T rows are j: storage K-major iff op_b is NoTranspose.
   dim3 gb((unsigned)((kp + 31) / 32), (unsigned)((n + 31) / 32));
   if (op_b == CORAL_NO_TRANSPOSE)
-    k_split_real<NP, true><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, bp, kp, b_piece);
+    k_split_real<NPC, true><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, bp, kp, b_piece);
   else
-    k_split_real<NP, false><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, bp, kp, b_piece);
+    k_split_real<NPC, false><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, bp, kp, b_piece);
   s = launch_status(h);
   if (s != CORAL_OK) return s;
   EpiParams ep{C, ldc, (int)m, (int)n, alpha, 0.f, beta, 0.f, 0};
@@ -435,11 +510,12 @@ template <int NP>
 coral_status_t cgemm_split_impl(Handle* h, int op_a, int op_b, size_t m, size_t n, size_t k,
                                 float2 alpha, const float2* A, size_t lda, const float2* B,
                                 size_t ldb, float2 beta, float2* C, size_t ldc) {
+  constexpr int NPC = SplitPlan<NP>::kPieces;
   const size_t k2 = 2 * k;
   const size_t kp = (k2 + 7) & ~size_t(7);
   const size_t a_piece = m * kp, b_piece = 2 * n * kp;
-  const size_t a_bytes = ((NP == 3 ? 2 : 3) * a_piece * 2 + 255) & ~size_t(255);
-  const size_t b_bytes = (NP == 3 ? 2 : 3) * b_piece * 2;
+  const size_t a_bytes = (NPC * a_piece * 2 + 255) & ~size_t(255);
+  const size_t b_bytes = NPC * b_piece * 2;
   char* sc = static_cast<char*>(scratch(h, a_bytes + b_bytes));
   if (!sc) return CORAL_ERR_ALLOC;
   __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(sc);
@@ -450,16 +526,16 @@ coral_status_t cgemm_split_impl(Handle* h, int op_a, int op_b, size_t m, size_t 
   dim3 ga((unsigned)((k + 31) / 32), (unsigned)((m + 31) / 32));
   const bool ca = op_a == CORAL_CONJ_TRANSPOSE, cbj = op_b == CORAL_CONJ_TRANSPOSE;
   if (op_a == CORAL_NO_TRANSPOSE)
-    k_split_cplx<NP, false, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ca, ap, kp, a_piece);
+    k_split_cplx<NPC, false, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ca, ap, kp, a_piece);
   else
-    k_split_cplx<NP, true, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ca, ap, kp, a_piece);
+    k_split_cplx<NPC, true, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ca, ap, kp, a_piece);
   coral_status_t s = launch_status(h);
   if (s != CORAL_OK) return s;
   dim3 gb((unsigned)((k + 31) / 32), (unsigned)((n + 31) / 32));
   if (op_b == CORAL_NO_TRANSPOSE)
-    k_split_cplx<NP, true, true><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, cbj, bp, kp, b_piece);
+    k_split_cplx<NPC, true, true><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, cbj, bp, kp, b_piece);
   else
-    k_split_cplx<NP, false, true><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, cbj, bp, kp, b_piece);
+    k_split_cplx<NPC, false, true><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, cbj, bp, kp, b_piece);
   s = launch_status(h);
   if (s != CORAL_OK) return s;
   EpiParams ep{reinterpret_cast<float*>(C), ldc, (int)m, (int)n, alpha.x, alpha.y, beta.x, beta.y, 1};

@@ -175,6 +175,13 @@ coral_status_t coral_get_gemm_mode(coral_handle_t handle, int* mode) {
   return CORAL_OK;
 }
 
+coral_status_t coral_set_split_chunk(coral_handle_t handle, int slabs) {
+  CORAL_HANDLE(handle);
+  if (slabs < 1 || slabs > 1 << 20) return bad_arg(H, 1);
+  H->split_chunk_kb = slabs;
+  return CORAL_OK;
+}
+
 coral_status_t coral_set_wait_limit(coral_handle_t handle, uint64_t spins) {
   CORAL_HANDLE(handle);
   H->wait_limit = spins ? spins : kDefaultWaitLimit;

@@ -81,6 +81,9 @@ coral_status_t coral_get_stream(coral_handle_t handle, void** stream);
 coral_status_t coral_set_pointer_mode(coral_handle_t handle, int mode);
 coral_status_t coral_set_gemm_mode(coral_handle_t handle, int mode);
 coral_status_t coral_get_gemm_mode(coral_handle_t handle, int* mode);
+/* K depth, in 64-element slabs, of each tensor-core accumulation chunk of the
+ * split-BF16 GEMMs before it is added into fp32 registers (default 16). */
+coral_status_t coral_set_split_chunk(coral_handle_t handle, int slabs);
 /* Iteration limit of every bounded device wait (0 restores the default). */
 coral_status_t coral_set_wait_limit(coral_handle_t handle, uint64_t spins);
 /* Wait for the stream, then report and clear the device status word. */
