@@ -33,7 +33,12 @@
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
+#include <mutex>
+
 namespace coral {
+
+int gemm_bad_arg(int op_a, int op_b, size_t m, size_t n, size_t k, const void* a, size_t lda,
+                 const void* b, size_t ldb, const void* c, size_t ldc, bool complex_ops);
 
 // ---- tensor-map encoding (driver entry point, no libcuda link) -------------
 static PFN_cuTensorMapEncodeTiled_v12000 tmap_encode_fn() {
@@ -563,3 +568,131 @@ coral_status_t enqueue_cgemm_split(Handle* h, int terms, int op_a, int op_b, siz
 }
 
 }  // namespace coral
+
+// ---- allocation-free split-BF16x3 SGEMM ----------------------------------------
+// Some callers cannot let a library call cudaMalloc: a serving process that
+// reserves nearly all of HBM at start-up and sub-allocates it itself, a
+// latency-critical loop that cannot afford the implicit synchronisation of
+// cudaMalloc/cudaFree, or a deployment that forbids device allocation after
+// initialisation.  coral_sgemm_bf16x3_noalloc serves them: the bf16 pieces of
+// op(A) and op(B) go into this fixed array instead of handle scratch.
+//
+// The array is a file-scope __device__ variable, so every GPU that loads this
+// library holds it until the process exits.  Host code must not use its name
+// as a device address (on the host it is only a stand-in); the address comes
+// from cudaGetSymbolAddress, once per device, in noalloc_setup().
+namespace coral {
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB per device
+constexpr int kNoAllocMaxDevices = 64;
+
+struct NoAllocDevice {
+  bool ready = false;
+  unsigned char* scratch = nullptr;
+  unsigned* status = nullptr;
+  int sm_count = 0;
+};
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+__global__ void k_noalloc_scale(int m, int n, float beta, float* __restrict__ C, size_t ldc) {
+  size_t total = (size_t)m * n;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    float* cp = C + t % m + (t / m) * ldc;
+    *cp = beta == 0.f ? 0.f : beta * *cp;
+  }
+}
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+static __device__ __align__(256) unsigned g_noalloc_status;
+
+// One-time set-up for the current device: device addresses of the fixed
+// scratch and status word, the SM count, and the kernel's shared-memory limit.
+static coral_status_t noalloc_setup(NoAllocDevice** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices)
+    return CORAL_ERR_NO_DEVICE;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoAllocDevice& d = g_noalloc_dev[dev];
+  if (!d.ready) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_status(nullptr, e);
+    d.scratch = static_cast<unsigned char*>(p);
+    e = cudaGetSymbolAddress(&p, g_noalloc_status);
+    if (e != cudaSuccess) return cuda_status(nullptr, e);
+    d.status = static_cast<unsigned*>(p);
+    e = cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cuda_status(nullptr, e);
+    e = cudaFuncSetAttribute(k_gemm_split<3, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)gemm_smem_bytes<3>());
+    if (e != cudaSuccess) return cuda_status(nullptr, e);
+    d.ready = true;
+  }
+  *out = &d;
+  return CORAL_OK;
+}
+
+}  // namespace coral
+
+extern "C" coral_status_t coral_sgemm_bf16x3_noalloc(void* stream, int op_a, int op_b, size_t m,
+                                                     size_t n, size_t k, float alpha,
+                                                     const float* a, size_t lda, const float* b,
+                                                     size_t ldb, float beta, float* c, size_t ldc) {
+  using namespace coral;
+  if (gemm_bad_arg(op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, false) > 0)
+    return CORAL_ERR_INVALID_ARG;
+  const size_t kp = (k + 7) & ~size_t(7);
+  const size_t a_piece = m * kp, b_piece = n * kp;
+  const size_t a_bytes = (2 * a_piece * 2 + 255) & ~size_t(255);
+  const size_t b_bytes = 2 * b_piece * 2;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX || k > (size_t)INT32_MAX ||
+      a_bytes + b_bytes > kNoAllocScratchBytes)
+    return CORAL_ERR_NOT_SUPPORTED;  // the pieces do not fit the fixed scratch
+  if (m == 0 || n == 0) return CORAL_OK;
+  NoAllocDevice* d = nullptr;
+  coral_status_t s = noalloc_setup(&d);
+  if (s != CORAL_OK) return s;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (alpha == 0.0f || k == 0) {  // scale-only (sgemm_nn.rs:29-45)
+    if (beta == 1.0f) return CORAL_OK;
+    unsigned g = stream_grid(m * n, 256 * 4, d->sm_count, 8);
+    k_noalloc_scale<<<g, 256, 0, st>>>((int)m, (int)n, beta, c, ldc);
+    return launch_status(nullptr);
+  }
+  // The status word keeps the previous call's value: clear it first.
+  cudaError_t e = cudaMemsetAsync(d->status, 0, sizeof(unsigned), st);
+  if (e != cudaSuccess) return cuda_status(nullptr, e);
+  __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(d->scratch);
+  __nv_bfloat16* bp = reinterpret_cast<__nv_bfloat16*>(d->scratch + a_bytes);
+  // Every piece element the GEMM reads is rewritten here, so stale contents
+  // of the shared array from an earlier call never leak into this one.
+  dim3 ga((unsigned)((kp + 31) / 32), (unsigned)((m + 31) / 32));
+  if (op_a == CORAL_NO_TRANSPOSE)
+    k_split_real<2, false><<<ga, 256, 0, st>>>(a, lda, (int)m, (int)k, ap, kp, a_piece);
+  else
+    k_split_real<2, true><<<ga, 256, 0, st>>>(a, lda, (int)m, (int)k, ap, kp, a_piece);
+  if ((s = launch_status(nullptr)) != CORAL_OK) return s;
+  dim3 gb((unsigned)((kp + 31) / 32), (unsigned)((n + 31) / 32));
+  if (op_b == CORAL_NO_TRANSPOSE)
+    k_split_real<2, true><<<gb, 256, 0, st>>>(b, ldb, (int)n, (int)k, bp, kp, b_piece);
+  else
+    k_split_real<2, false><<<gb, 256, 0, st>>>(b, ldb, (int)n, (int)k, bp, kp, b_piece);
+  if ((s = launch_status(nullptr)) != CORAL_OK) return s;
+  SplitMaps maps;
+  std::memset(&maps, 0, sizeof(maps));
+  for (int p = 0; p < 2; ++p) {
+    if (!encode_kmajor_map(&maps.a[p], ap + p * a_piece, 2, k, m, kp * 2, kBK, kBM) ||
+        !encode_kmajor_map(&maps.b[p], bp + p * b_piece, 2, k, n, kp * 2, kBK, 256))
+      return CORAL_ERR_NOT_SUPPORTED;
+  }
+  const int m_tiles = (int)((m + kBM - 1) / kBM), n_tiles = (int)((n + 255) / 256);
+  const int tiles = m_tiles * n_tiles;
+  const int grid = tiles < d->sm_count ? tiles : d->sm_count;
+  EpiParams ep{c, ldc, (int)m, (int)n, alpha, 0.f, beta, 0.f, 0};
+  k_gemm_split<3, 256><<<grid, kSplitThreads, gemm_smem_bytes<3>(), st>>>(
+      maps, (int)k, m_tiles, n_tiles, 16, ep, d->status, kDefaultWaitLimit * 32ull);
+  return launch_status(nullptr);
+}

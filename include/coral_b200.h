@@ -174,6 +174,32 @@ coral_status_t coral_zgemm(coral_handle_t h, int op_a, int op_b, size_t m, size_
                            const double* b, size_t ldb, const double beta[2], double* c,
                            size_t ldc);
 
+/* ---- allocation-free split-BF16x3 SGEMM --------------------------------- */
+/* No counterpart in the reference (CORAL allocates its packing buffers on
+ * every call).  Same arguments and result as coral_sgemm in
+ * CORAL_GEMM_SPLIT_BF16X3 mode, with a cudaStream_t (NULL = legacy default
+ * stream) in place of the handle, for callers that must not have device
+ * memory allocated behind their back: a process that reserves nearly all of
+ * HBM up front and sub-allocates it itself, a latency-critical loop that
+ * cannot take cudaMalloc's implicit synchronisation, or a deployment that
+ * forbids device allocation after start-up.  It calls no cudaMalloc or
+ * cudaFree: the bf16 operand pieces live in a fixed 32 MiB device array that
+ * every GPU loading this library holds until the process exits.
+ *   - Sizes whose pieces need more than 32 MiB, i.e. 4 * (m + n) * kp bytes
+ *     with kp = k rounded up to a multiple of 8 (about m = n = k = 2048), are
+ *     rejected with CORAL_ERR_NOT_SUPPORTED before any work is enqueued.
+ *   - The first call on a device looks up the array's device address and sets
+ *     the kernel's shared-memory limit for that device; make that first call
+ *     before any stream capture on the device.
+ *   - All calls share the one array: calls whose work can overlap on the GPU
+ *     (different streams, or other host threads) race on it and must be
+ *     serialised by the caller.
+ * Device pointers; asynchronous on `stream`. */
+coral_status_t coral_sgemm_bf16x3_noalloc(void* stream, int op_a, int op_b, size_t m, size_t n,
+                                          size_t k, float alpha, const float* a, size_t lda,
+                                          const float* b, size_t ldb, float beta, float* c,
+                                          size_t ldc);
+
 /* ---- host-slice drop-ins: the reference's exact argument lists ---------- */
 /* Pointers are HOST memory.  Return value as above; scalar-returning routines
  * write through the trailing out-pointer.  Thread-safe: each host thread gets
