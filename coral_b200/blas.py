@@ -104,6 +104,16 @@ class Handle:
     def set_wait_limit(self, spins: int) -> None:
         self.check(self.lib.coral_set_wait_limit(self.h, spins), "coral_set_wait_limit")
 
+    def set_kernel_timing(self, enable: bool) -> None:
+        self.check(self.lib.coral_set_kernel_timing(self.h, int(enable)), "coral_set_kernel_timing")
+
+    def kernel_timing(self) -> tuple[float, int]:
+        """(summed ms, launches) of the dominant kernels timed since the last query."""
+        ms, n = C.c_double(), C.c_uint64()
+        self.check(self.lib.coral_get_kernel_timing(self.h, C.byref(ms), C.byref(n)),
+                   "coral_get_kernel_timing")
+        return ms.value, n.value
+
     def sync(self) -> None:
         self.check(self.lib.coral_sync(self.h), "coral_sync")
 

@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "../../include/coral_b200.h"
 
@@ -40,7 +42,16 @@ struct Handle {
   // Zeroed pool of per-tile arrival counters for single-launch multi-block
   // combines; every kernel returns the counters it used to zero.
   unsigned* counters = nullptr;
+  // Optional event timing of the dominant kernel of each call.
+  bool timing = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timing_events;
+  size_t timing_used = 0;
 };
+
+// Brackets one dominant-kernel launch with events when the handle's timing is
+// on: call timed_begin() before the launch and timed_end() after it.
+void timed_begin(Handle* h);
+void timed_end(Handle* h);
 
 constexpr size_t kCounterPool = 1u << 16;
 

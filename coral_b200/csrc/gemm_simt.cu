@@ -260,9 +260,12 @@ coral_status_t enqueue_gemm_simt(Handle* h, int op_a, int op_b, size_t m, size_t
   dim3 grid((unsigned)((m + BM - 1) / BM), (unsigned)((n + BN - 1) / BN));
   if (grid.y > 65535) return CORAL_ERR_NOT_SUPPORTED;
   // ConjugateTranspose on a real type means Transpose (sgemm.rs:97-103).
+  timed_begin(h);
   k_gemm_simt<T><<<grid, kSimtThreads, 0, h->stream>>>((int)m, (int)n, (int)k, alpha, A, lda, op_a,
                                                         B, ldb, op_b, beta, C, ldc);
-  return launch_status(h);
+  coral_status_t s = launch_status(h);
+  timed_end(h);
+  return s;
 }
 
 template coral_status_t enqueue_gemm_simt<float>(Handle*, int, int, size_t, size_t, size_t, float,

@@ -473,9 +473,12 @@ coral_status_t run_split_gemm(Handle* h, const __nv_bfloat16* ap, size_t a_piece
   const int tiles = m_tiles * n_tiles;
   const int grid = tiles < h->sm_count ? tiles : h->sm_count;
   const uint64_t limit_ns = h->wait_limit * 32ull;  // default 2^26 * 32 ns ~ 2.1 s
+  timed_begin(h);
   k_gemm_split<NP, BN><<<grid, kSplitThreads, smem, h->stream>>>(
       maps, kd, m_tiles, n_tiles, h->split_chunk_kb, ep, &h->words->status, limit_ns);
-  return launch_status(h);
+  coral_status_t s = launch_status(h);
+  timed_end(h);
+  return s;
 }
 
 template <int NP>

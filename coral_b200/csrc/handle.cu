@@ -78,9 +78,32 @@ static coral_status_t create_handle(Handle** out) {
   return CORAL_OK;
 }
 
+void timed_begin(Handle* h) {
+  if (!h->timing) return;
+  if (h->timing_used == h->timing_events.size()) {
+    cudaEvent_t a, b;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    h->timing_events.emplace_back(a, b);
+  }
+  cudaEventRecord(h->timing_events[h->timing_used].first, h->stream);
+}
+
+void timed_end(Handle* h) {
+  if (!h->timing || h->timing_used == h->timing_events.size()) return;
+  cudaEventRecord(h->timing_events[h->timing_used].second, h->stream);
+  ++h->timing_used;
+}
+
 static void destroy_handle(Handle* h) {
   if (!h) return;
   cudaStreamSynchronize(h->stream);
+  for (auto& e : h->timing_events) {
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
   if (h->scratch) cudaFree(h->scratch);
   if (h->words) cudaFree(h->words);
   if (h->counters) cudaFree(h->counters);
@@ -185,6 +208,30 @@ coral_status_t coral_set_split_chunk(coral_handle_t handle, int slabs) {
 coral_status_t coral_set_wait_limit(coral_handle_t handle, uint64_t spins) {
   CORAL_HANDLE(handle);
   H->wait_limit = spins ? spins : kDefaultWaitLimit;
+  return CORAL_OK;
+}
+
+coral_status_t coral_set_kernel_timing(coral_handle_t handle, int enable) {
+  CORAL_HANDLE(handle);
+  H->timing = enable != 0;
+  H->timing_used = 0;
+  return CORAL_OK;
+}
+
+coral_status_t coral_get_kernel_timing(coral_handle_t handle, double* total_ms, uint64_t* launches) {
+  CORAL_HANDLE(handle);
+  if (!total_ms) return bad_arg(H, 1);
+  if (!launches) return bad_arg(H, 2);
+  CORAL_CUDA(H, cudaStreamSynchronize(H->stream));
+  double sum = 0.0;
+  for (size_t i = 0; i < H->timing_used; ++i) {
+    float ms = 0.f;
+    CORAL_CUDA(H, cudaEventElapsedTime(&ms, H->timing_events[i].first, H->timing_events[i].second));
+    sum += ms;
+  }
+  *total_ms = sum;
+  *launches = H->timing_used;
+  H->timing_used = 0;
   return CORAL_OK;
 }
 

@@ -86,6 +86,12 @@ coral_status_t coral_get_gemm_mode(coral_handle_t handle, int* mode);
 coral_status_t coral_set_split_chunk(coral_handle_t handle, int slabs);
 /* Iteration limit of every bounded device wait (0 restores the default). */
 coral_status_t coral_set_wait_limit(coral_handle_t handle, uint64_t spins);
+/* Kernel timing: when enabled, the handle brackets the dominant kernel of each
+ * call (the GEMM main loop for level 3) with CUDA events on its stream;
+ * coral_get_kernel_timing waits for the stream and returns the summed
+ * duration (ms) and number of timed launches since the last query. */
+coral_status_t coral_set_kernel_timing(coral_handle_t handle, int enable);
+coral_status_t coral_get_kernel_timing(coral_handle_t handle, double* total_ms, uint64_t* launches);
 /* Wait for the stream, then report and clear the device status word. */
 coral_status_t coral_sync(coral_handle_t handle);
 /* 1-based position of the offending argument after CORAL_ERR_INVALID_ARG
