@@ -42,6 +42,10 @@ struct Handle {
   // Zeroed pool of per-tile arrival counters for single-launch multi-block
   // combines; every kernel returns the counters it used to zero.
   unsigned* counters = nullptr;
+  // TRSV: ready flags hold the epoch of the call that set them (never reset);
+  // tickets are handed out from a running counter starting at trsv_tickets.
+  unsigned trsv_epoch = 0;
+  unsigned long long trsv_tickets = 0;
   // Optional event timing of the dominant kernel of each call.
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timing_events;
@@ -54,6 +58,9 @@ void timed_begin(Handle* h);
 void timed_end(Handle* h);
 
 constexpr size_t kCounterPool = 1u << 16;
+// Counters [0, kTrsvFlagBase) are zero-reset arrival counters; the rest are
+// TRSV ready flags.
+constexpr size_t kTrsvFlagBase = 1u << 15;
 
 // Fixed device-side bookkeeping; counters are returned to zero by the last
 // block of the reduction that used them, so the area stays reusable.
@@ -63,7 +70,8 @@ struct DeviceWords {
   unsigned counters[30];           // arrival counters of single-launch reductions
   double dresult[4];               // scalar results (device pointer mode staging)
   unsigned long long uresult[4];
-  unsigned char reserved[1024 - 4 * 32 - 64];
+  unsigned long long trsv_ticket;  // running ticket counter of the TRSV kernel
+  unsigned char reserved[1024 - 4 * 32 - 64 - 8];
 };
 static_assert(sizeof(DeviceWords) == 1024, "DeviceWords layout");
 

@@ -213,7 +213,7 @@ coral_status_t enqueue_gemv(Handle* h, bool trans, size_t m, size_t n, float alp
     if (chunks < 1) chunks = 1;
     int cpc = (int)((n + chunks - 1) / chunks);
     chunks = (int)((n + cpc - 1) / cpc);
-    if (strips > (int)kCounterPool) return CORAL_ERR_NOT_SUPPORTED;
+    if (strips > (int)kTrsvFlagBase) return CORAL_ERR_NOT_SUPPORTED;
     float* part = nullptr;
     if (chunks > 1) {
       part = static_cast<float*>(scratch(h, (size_t)chunks * m * sizeof(float)));
@@ -236,7 +236,7 @@ coral_status_t enqueue_gemv(Handle* h, bool trans, size_t m, size_t n, float alp
   if (groups < 1) groups = 1;
   int cpg = (int)((n + groups - 1) / groups);
   groups = (int)((n + cpg - 1) / cpg);
-  if (groups > (int)kCounterPool) return CORAL_ERR_NOT_SUPPORTED;
+  if (groups > (int)kTrsvFlagBase) return CORAL_ERR_NOT_SUPPORTED;
   float* part = nullptr;
   if (rchunks > 1) {
     part = static_cast<float*>(scratch(h, (size_t)rchunks * n * sizeof(float)));
