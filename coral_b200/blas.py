@@ -98,6 +98,10 @@ class Handle:
         self.check(self.lib.coral_get_gemm_mode(self.h, C.byref(m)), "coral_get_gemm_mode")
         return m.value
 
+    def set_pointer_mode(self, mode: int) -> None:
+        """0: scalar results to host memory (waits); 1: to device memory (async)."""
+        self.check(self.lib.coral_set_pointer_mode(self.h, int(mode)), "coral_set_pointer_mode")
+
     def set_split_chunk(self, slabs: int) -> None:
         self.check(self.lib.coral_set_split_chunk(self.h, slabs), "coral_set_split_chunk")
 

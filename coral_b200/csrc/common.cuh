@@ -46,6 +46,10 @@ struct Handle {
   // tickets are handed out from a running counter starting at trsv_tickets.
   unsigned trsv_epoch = 0;
   unsigned long long trsv_tickets = 0;
+  // Epoch-tagged solution slots ((epoch << 32) | float bits), zeroed when
+  // (re)allocated so stale memory never carries a live epoch.
+  unsigned long long* trsv_slots = nullptr;
+  size_t trsv_slots_len = 0;
   // Optional event timing of the dominant kernel of each call.
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timing_events;

@@ -107,6 +107,7 @@ static void destroy_handle(Handle* h) {
   if (h->scratch) cudaFree(h->scratch);
   if (h->words) cudaFree(h->words);
   if (h->counters) cudaFree(h->counters);
+  if (h->trsv_slots) cudaFree(h->trsv_slots);
   if (h->host_pinned) cudaFreeHost(h->host_pinned);
   delete h;
 }

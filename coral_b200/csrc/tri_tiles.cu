@@ -92,22 +92,35 @@ k_tri_tiles(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x,
     vJ[tid] = kSym ? scale_x(alpha, v) : v;
   }
   T colacc = Cx<T>::zero();  // column part for column r, quarter q of the rows
+  // Tile elements of this thread (element e = tid + p * 256: row e % 64,
+  // column e / 64), loaded for tile ti+1 while tile ti is computed.
+  constexpr int kPer = kT * kT / kTriThreads;
+  T reg[kPer];
+  auto load_tile = [&](int I) {
+    const int r0 = I * kT;
+#pragma unroll
+    for (int p = 0; p < kPer; ++p) {
+      const int e = tid + p * kTriThreads;
+      const int gr = r0 + e % kT, gc = c0 + e / kT;
+      reg[p] = (gr < n && gc < n) ? __ldcs(A + gr + (size_t)gc * lda) : Cx<T>::zero();
+    }
+  };
+  load_tile(first + t0);
   for (int ti = t0; ti < t1; ++ti) {
     const int I = first + ti;
     const int r0 = I * kT;
     __syncthreads();
-    // Load the tile (rows r0.., cols c0..) column by column.
-#pragma unroll 4
-    for (int e = tid; e < kT * kT; e += kTriThreads) {
-      const int rr = e % kT, cc = e / kT;
-      const int gr = r0 + rr, gc = c0 + cc;
-      tile[cc][rr] = (gr < n && gc < n) ? __ldg(A + gr + (size_t)gc * lda) : Cx<T>::zero();
+#pragma unroll
+    for (int p = 0; p < kPer; ++p) {
+      const int e = tid + p * kTriThreads;
+      tile[e / kT][e % kT] = reg[p];
     }
     if (tid < kT) {
       const int gr = r0 + tid;
       T v = gr < n ? x[(size_t)gr * incx] : Cx<T>::zero();
       vI[tid] = kSym ? scale_x(alpha, v) : v;
     }
+    if (ti + 1 < t1) load_tile(I + 1);
     __syncthreads();
     const bool diag = I == J;
     if (diag) {

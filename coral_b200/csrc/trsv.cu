@@ -10,11 +10,13 @@
 //      applied) in shared memory and inverts it (independent of every other
 //      block, so it overlaps the solve of earlier blocks);
 //   2. streams its row panel of op(A), 4 tiles of 64 x 64 in flight, and
-//      for each tile waits for that block's ready flag (acquire), then
+//      for each tile waits for the solution x_k of that block, then
 //      accumulates tile * x_k -- tiles of early blocks are ready long before
 //      the last one, so the panel streams while the solve front advances;
-//   3. forms x_b = inv(D_b) (b_b - acc), writes it over b, and publishes its
-//      flag (release).
+//   3. forms x_b = inv(D_b) (b_b - acc), writes it over b, and publishes it
+//      as 64 epoch-tagged 64-bit slots ((epoch << 32) | float bits, store
+//      release).  A consumer polls the slots themselves: one round trip
+//      through L2 both signals readiness and delivers the values.
 // CORAL solves its diagonal blocks by substitution (strlsv.rs:66-140) with the
 // panel update through saxpyf/sdotf; here the blocked diagonal solve uses the
 // inverted 64 x 64 block as a small GEMV, which takes the serial substitution
@@ -30,13 +32,13 @@ constexpr int kG = 4;          // panel tiles loaded per group
 constexpr int kTrsvThreads = 256;
 constexpr int kPer = kNB * kNB / kTrsvThreads;  // tile elements per thread (16)
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_release64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 __device__ __forceinline__ uint64_t gtimer() {
   uint64_t t;
@@ -46,7 +48,7 @@ __device__ __forceinline__ uint64_t gtimer() {
 
 __global__ void __launch_bounds__(kTrsvThreads)
 k_trsv(int n, const float* __restrict__ A, size_t lda, float* x, size_t incx, bool lower_eff,
-       bool trans, bool unit, unsigned* flags, unsigned long long* ticket,
+       bool trans, bool unit, unsigned long long* slots, unsigned long long* ticket,
        unsigned long long ticket_base, unsigned epoch, unsigned* status, uint64_t limit_ns) {
   __shared__ float D[kNB][kNB + 1];    // D[r][c] = op(A)(r, c) of the diagonal block, then inv
   __shared__ float T[kNB][kNB + 1];    // T[c][r] = stored block element (row r, col c)
@@ -142,26 +144,30 @@ k_trsv(int n, const float* __restrict__ A, size_t lda, float* x, size_t incx, bo
       const int idx = g0 + g;
       if (idx >= npanel) break;
       const int k = lower_eff ? idx : blk + 1 + idx;
-      if (tid == 0) {
-        const uint64_t t0 = gtimer();
-        unsigned spins = 0;
-        while (ld_acquire(flags + k) != epoch) {
-          if (gtimer() - t0 > limit_ns || ((++spins & 15u) == 0 && *(volatile unsigned*)status != 0)) {
-            atomicOr(status, kStatusTimeout);
-            abort_flag = 1;
-            break;
-          }
-        }
-      }
-      __syncthreads();
-      if (abort_flag) return;
 #pragma unroll
       for (int p = 0; p < kPer; ++p) {
         const int e = tid + p * kTrsvThreads;
         T[e / kNB][e % kNB] = reg[g][p];
       }
-      if (tid < kNB) xk[tid] = (k * kNB + tid < n) ? __ldcg(x + (size_t)(k * kNB + tid) * incx) : 0.f;
+      if (tid < kNB) {
+        const unsigned long long* sp = slots + (size_t)k * kNB + tid;
+        unsigned long long v = ld_acquire64(sp);
+        if ((unsigned)(v >> 32) != epoch) {
+          const uint64_t t0 = gtimer();
+          unsigned spins = 0;
+          while ((unsigned)((v = ld_acquire64(sp)) >> 32) != epoch) {
+            if (gtimer() - t0 > limit_ns ||
+                ((++spins & 15u) == 0 && *(volatile unsigned*)status != 0)) {
+              atomicOr(status, kStatusTimeout);
+              abort_flag = 1;
+              break;
+            }
+          }
+        }
+        xk[tid] = __uint_as_float((unsigned)v);
+      }
       __syncthreads();
+      if (abort_flag) return;
       // op(A)(r, c) = stored(r, c) = T[c][r], or stored(c, r) = T[r][c] when transposed
       if (!trans) {
 #pragma unroll
@@ -184,12 +190,11 @@ k_trsv(int n, const float* __restrict__ A, size_t lda, float* x, size_t incx, bo
   for (int c = q * 16; c < q * 16 + 16; ++c) s = fmaf(D[r][c], rhs[c], s);
   red[q][r] = s;
   __syncthreads();
-  if (tid < kNB && b0 + tid < n)
-    x[(size_t)(b0 + tid) * incx] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
-  __syncthreads();
-  if (tid == 0) {
-    __threadfence();
-    st_release(flags + blk, epoch);
+  if (tid < kNB) {
+    const float v = (b0 + tid < n) ? (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]) : 0.f;
+    if (b0 + tid < n) x[(size_t)(b0 + tid) * incx] = v;
+    st_release64(slots + (size_t)blk * kNB + tid,
+                 ((unsigned long long)epoch << 32) | __float_as_uint(v));
   }
 }
 
@@ -210,7 +215,19 @@ extern "C" coral_status_t coral_strsv(coral_handle_t hh, int uplo, int trans, in
   if (!x) return bad_arg(H, 7);
   if (incx == 0) return bad_arg(H, 8);
   const size_t nblk = (n + kNB - 1) / kNB;
-  if (nblk > kCounterPool - kTrsvFlagBase || n > (size_t)INT32_MAX) return CORAL_ERR_NOT_SUPPORTED;
+  if (n > (size_t)INT32_MAX) return CORAL_ERR_NOT_SUPPORTED;
+  if (H->trsv_slots_len < nblk * kNB) {
+    if (H->trsv_slots) {
+      CORAL_CUDA(H, cudaStreamSynchronize(H->stream));
+      cudaFree(H->trsv_slots);
+      H->trsv_slots = nullptr;
+      H->trsv_slots_len = 0;
+    }
+    const size_t len = ((nblk * kNB + 65535) / 65536) * 65536;
+    CORAL_CUDA(H, cudaMalloc(&H->trsv_slots, len * sizeof(unsigned long long)));
+    CORAL_CUDA(H, cudaMemsetAsync(H->trsv_slots, 0, len * sizeof(unsigned long long), H->stream));
+    H->trsv_slots_len = len;
+  }
   const bool t = trans != CORAL_NO_TRANSPOSE;
   const bool lower_eff = (uplo == CORAL_LOWER) != t;
   H->trsv_epoch += 1;
@@ -219,7 +236,7 @@ extern "C" coral_status_t coral_strsv(coral_handle_t hh, int uplo, int trans, in
   H->trsv_tickets += nblk;
   timed_begin(H);
   k_trsv<<<(unsigned)nblk, kTrsvThreads, 0, H->stream>>>(
-      (int)n, matrix, lda, x, incx, lower_eff, t, diag == CORAL_UNIT, H->counters + kTrsvFlagBase,
+      (int)n, matrix, lda, x, incx, lower_eff, t, diag == CORAL_UNIT, H->trsv_slots,
       &H->words->trsv_ticket, base, H->trsv_epoch, &H->words->status, H->wait_limit * 32ull);
   coral_status_t s = launch_status(H);
   timed_end(H);
