@@ -193,6 +193,92 @@ def run_reference(args, world, rank):
 
 
 # ------------------------------------------------------------------ GPU arm --
+def precision_set(torch, cb, h, dev, g):
+    """Precision-GEMM configuration: DGEMM NN 4096^3 native vs Ozaki INT8
+    (uniform and ill-scaled rows), ZGEMM CC 2048^3 native vs Ozaki, SGEMM TT
+    8192^3 split-BF16x3; TFLOP/s (real flops: 2mnk, complex 8mnk) and the max
+    component-wise error on 1024 sampled entries against the double-double
+    oracle."""
+    import oracle
+    out = {}
+    rng = np.random.default_rng(17)
+    stream = torch.cuda.current_stream()
+
+    def run(fn, iters=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(iters):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / iters
+
+    def sample_err(fn_once, op, m, n, k, alpha, A, lda, B, ldb, beta, C0, Cm, ldc, cplx):
+        Cm.copy_(C0)
+        fn_once()
+        torch.cuda.synchronize()
+        ii, jj = rng.integers(0, m, 1024), rng.integers(0, n, 1024)
+        want, bound = oracle.gemm_sample(op, op, m, n, k, alpha, A.cpu().numpy(), lda, B.cpu().numpy(),
+                                         ldb, beta, C0.cpu().numpy(), ldc, ii, jj)
+        got = Cm.cpu().numpy()[ii + jj * ldc]
+        return float((np.abs(got - want) / bound).max())
+
+    # DGEMM 4096^3 NN
+    m = 4096
+    for ill in (False, True):
+        A = torch.empty(m * m, dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
+        if ill:
+            sc = torch.exp(2.0 * torch.randn(m, dtype=torch.float64, device=dev, generator=g))
+            A = (A.view(m, m) * sc[None, :]).reshape(-1).contiguous()
+        B = torch.empty(m * m, dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
+        C0 = torch.empty(m * m, dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
+        Cm = C0.clone()
+        for mode, name in ((cb.GemmMode.NATIVE, "native"), (cb.GemmMode.OZAKI_INT8, "ozaki_int8")):
+            h.set_gemm_mode(mode)
+            f = lambda: cb.dgemm(0, 0, m, m, m, 1.5, A, m, B, m, 0.5, Cm, m)  # noqa: E731
+            err = sample_err(f, 0, m, m, m, 1.5, A, m, B, m, 0.5, C0, Cm, m, False)
+            key = f"dgemm_nn_4096_{name}" + ("_illscaled" if ill else "")
+            entry = {"max_rel_componentwise": err}
+            if not ill:
+                ms = run(f)
+                entry.update({"ms": ms, "tflops": 2.0 * m ** 3 / (ms * 1e-3) / 1e12})
+            out[key] = entry
+        del A, B, C0, Cm
+    # ZGEMM CC 2048^3
+    m = 2048
+    A = torch.empty(m * m, dtype=torch.complex128, device=dev)
+    A.real.uniform_(-1, 1, generator=g); A.imag.uniform_(-1, 1, generator=g)
+    B = torch.empty(m * m, dtype=torch.complex128, device=dev)
+    B.real.uniform_(-1, 1, generator=g); B.imag.uniform_(-1, 1, generator=g)
+    C0 = torch.empty(m * m, dtype=torch.complex128, device=dev)
+    C0.real.uniform_(-1, 1, generator=g); C0.imag.uniform_(-1, 1, generator=g)
+    Cm = C0.clone()
+    for mode, name in ((cb.GemmMode.NATIVE, "native"), (cb.GemmMode.OZAKI_INT8, "ozaki_int8")):
+        h.set_gemm_mode(mode)
+        f = lambda: cb.zgemm(2, 2, m, m, m, 1.5 - 0.5j, A, m, B, m, 0.25 + 1j, Cm, m)  # noqa: E731
+        err = sample_err(f, 2, m, m, m, 1.5 - 0.5j, A, m, B, m, 0.25 + 1j, C0, Cm, m, True)
+        ms = run(f)
+        out[f"zgemm_cc_2048_{name}"] = {"ms": ms, "tflops": 8.0 * m ** 3 / (ms * 1e-3) / 1e12,
+                                        "max_rel_componentwise": err}
+    del A, B, C0, Cm
+    # SGEMM TT 8192^3 split-BF16x3
+    m = 8192
+    A = torch.empty(m * m, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
+    B = torch.empty(m * m, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
+    C0 = torch.empty(m * m, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
+    Cm = C0.clone()
+    h.set_gemm_mode(cb.GemmMode.SPLIT_BF16X3)
+    f = lambda: cb.sgemm(1, 1, m, m, m, 1.5, A, m, B, m, 0.5, Cm, m)  # noqa: E731
+    err = sample_err(f, 1, m, m, m, 1.5, A, m, B, m, 0.5, C0, Cm, m, False)
+    ms = run(f)
+    out["sgemm_tt_8192_split_bf16x3"] = {"ms": ms, "tflops": 2.0 * m ** 3 / (ms * 1e-3) / 1e12,
+                                         "max_rel_componentwise": err}
+    del A, B, C0, Cm
+    return out
+
+
 def level12_bandwidth(torch, cb, lib, h, dev, g):
     """GB/s of algorithmic traffic for the level-1/2 bandwidth configuration
     (SGEMV N/T 8192^2, SSYMV upper 8192, STRSV lower non-unit 4096 with
@@ -381,26 +467,6 @@ def run_ours(args, world, rank, local):
         native_ms, _ = timed(lambda: step(cb.GemmMode.NATIVE), max(2, args.steps // 2), 1)
     h.set_gemm_mode(mode)
 
-    # level-1/2 bandwidth set (includes GEMV N/T at 8192 x 8192)
-    l12 = level12_bandwidth(torch, cb, lib, h, dev, g)
-    gemv = {"n": l12["sgemv_n"]["gbs"], "t": l12["sgemv_t"]["gbs"]}
-
-    hbm, bf16, bf16s, src = peaks()
-    ach = flops / (kernel_ms * 1e-3) / 1e12  # useful 2mnk per launch / event-timed launch duration
-    if mode == cb.GemmMode.NATIVE:
-        roof = {"bound": "tensor", "achieved": ach, "peak": FP32_FMA_PEAK_TFLOPS, "unit": "TFLOP/s",
-                "frac": ach / FP32_FMA_PEAK_TFLOPS, "traffic": None,
-                "kernel": "k_gemm_simt<float>", "kernel_ms": kernel_ms,
-                "peak_source": "nominal FP32 FMA pipe at max clock (no measured figure)"}
-    else:
-        products = 3 if mode == cb.GemmMode.SPLIT_BF16X3 else 6
-        roof = {"bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
-                "frac": ach / bf16, "traffic": SPLIT_GEMM_TRAFFIC_PER_LAUNCH.get(products),
-                "kernel": f"k_gemm_split<{products}>", "kernel_ms": kernel_ms,
-                "tensor_issue_frac": products * ach / bf16,
-                "peak_source": f"{src} bf16 dense burst (MEASURED_PEAKS.json)",
-                "achieved_counts": "useful 2mnk flop; the tensor pipe executes products x that"}
-
     # e2e through the host-slice C ABI: pinned host operands, H2D + compute + D2H per step
     e2e = None
     if not args.skip_e2e:
@@ -408,6 +474,7 @@ def run_ours(args, world, rank, local):
         Ah = A.cpu().pin_memory()
         Bh = B.cpu().pin_memory()
         Ch = C0.cpu().pin_memory()
+        h.set_gemm_mode(mode)
         lib.coral_host_set_gemm_mode(int(mode))
         vp = ctypes.c_void_p
 
@@ -427,6 +494,31 @@ def run_ours(args, world, rank, local):
         e2e = {"value": world * flops / el / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": 3 * M * N * 4, "d2h_bytes_per_step": M * N * 4,
                "ms_per_step": el * 1e3, "timing": "host wall clock around the synchronous call"}
+        del Ah, Bh, Ch
+
+    # level-1/2 bandwidth set (includes GEMV N/T at 8192 x 8192)
+    del A, B, C0, C
+    torch.cuda.empty_cache()
+    l12 = level12_bandwidth(torch, cb, lib, h, dev, g)
+    prec = precision_set(torch, cb, h, dev, g) if not args.skip_precision else None
+    h.set_gemm_mode(mode)
+    gemv = {"n": l12["sgemv_n"]["gbs"], "t": l12["sgemv_t"]["gbs"]}
+
+    hbm, bf16, bf16s, src = peaks()
+    ach = flops / (kernel_ms * 1e-3) / 1e12  # useful 2mnk per launch / event-timed launch duration
+    if mode == cb.GemmMode.NATIVE:
+        roof = {"bound": "tensor", "achieved": ach, "peak": FP32_FMA_PEAK_TFLOPS, "unit": "TFLOP/s",
+                "frac": ach / FP32_FMA_PEAK_TFLOPS, "traffic": None,
+                "kernel": "k_gemm_simt<float>", "kernel_ms": kernel_ms,
+                "peak_source": "nominal FP32 FMA pipe at max clock (no measured figure)"}
+    else:
+        products = 3 if mode == cb.GemmMode.SPLIT_BF16X3 else 6
+        roof = {"bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
+                "frac": ach / bf16, "traffic": SPLIT_GEMM_TRAFFIC_PER_LAUNCH.get(products),
+                "kernel": f"k_gemm_split<{products}>", "kernel_ms": kernel_ms,
+                "tensor_issue_frac": products * ach / bf16,
+                "peak_source": f"{src} bf16 dense burst (MEASURED_PEAKS.json)",
+                "achieved_counts": "useful 2mnk flop; the tensor pipe executes products x that"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -449,6 +541,7 @@ def run_ours(args, world, rank, local):
             "gemv_gbs": {"n": gemv["n"], "t": gemv["t"], "peak": hbm,
                          "frac_n": gemv["n"] / hbm, "frac_t": gemv["t"] / hbm},
             "level12": l12,
+            "precision_gemm": prec,
             "roofline": roof, "clocks": clk, "gpu_launches": int(launches),
             "e2e": e2e, "cpu_baseline": cpu,
         }
@@ -464,6 +557,7 @@ def main():
     ap.add_argument("--mode", choices=["native", "split_bf16x3", "split_bf16x6"], default="split_bf16x3")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-precision", action="store_true")
     ap.add_argument("--size", type=int, default=0, help="m = n = k (profiling cases; default 8192)")
     ap.add_argument("--only-gemm", action="store_true", help="run warmup+steps GEMMs, print nothing")
     args = ap.parse_args()

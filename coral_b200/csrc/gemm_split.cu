@@ -56,7 +56,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 tmap_encode_fn() {
 
 bool encode_kmajor_map(CUtensorMap* map, const void* base, int elem_bytes, uint64_t inner,
                        uint64_t outer, uint64_t row_stride_bytes, uint32_t box_inner,
-                       uint32_t box_outer) {
+                       uint32_t box_outer, int swizzle_bytes) {
   auto fn = tmap_encode_fn();
   if (!fn) return false;
   if ((reinterpret_cast<uintptr_t>(base) & 15) || (row_stride_bytes & 15)) return false;
@@ -67,7 +67,8 @@ bool encode_kmajor_map(CUtensorMap* map, const void* base, int elem_bytes, uint6
   CUtensorMapDataType dt = elem_bytes == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
                                            : CU_TENSOR_MAP_DATA_TYPE_UINT8;
   CUresult r = fn(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  swizzle_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
@@ -463,11 +464,12 @@ coral_status_t run_split_gemm(Handle* h, const __nv_bfloat16* ap, size_t a_piece
       return CORAL_ERR_NOT_SUPPORTED;
   }
   const size_t smem = gemm_smem_bytes<NP>();
-  static bool attr_set = false;
-  if (!attr_set) {
+  static uint64_t attr_devices = 0;  // bit d: attribute set on device d
+  const uint64_t bit = h->device < 64 ? (1ull << h->device) : 0;
+  if (!(attr_devices & bit) || !bit) {
     CORAL_CUDA(h, cudaFuncSetAttribute(k_gemm_split<NP, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
-    attr_set = true;
+    attr_devices |= bit;
   }
   const int m_tiles = (mr + kBM - 1) / kBM, n_tiles = (nr + BN - 1) / BN;
   const int tiles = m_tiles * n_tiles;

@@ -165,6 +165,17 @@ __device__ __forceinline__ uint64_t desc_k_sw128(uint32_t saddr) {
   return d;
 }
 
+// Same for the 64-byte swizzle (rows of 64 bytes, 8-row / 512-byte atoms):
+// stride offset 512 B, layout SWIZZLE_64B = 4.
+__device__ __forceinline__ uint64_t desc_k_sw64(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;
+  d |= (uint64_t)(512u >> 4) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)4u << 61;
+  return d;
+}
+
 // Instruction descriptor, kind::f16: D fp32 (bits 4-5 = 1), A and B bf16
 // (bits 7-9, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at bits
 // 17-22, M >> 4 at bits 24-28.
@@ -185,6 +196,6 @@ __host__ __device__ constexpr uint32_t idesc_s8_s32(int M, int N) {
 // zero fill outside [0, inner) x [0, outer).  Returns false on failure.
 bool encode_kmajor_map(CUtensorMap* map, const void* base, int elem_bytes, uint64_t inner,
                        uint64_t outer, uint64_t row_stride_bytes, uint32_t box_inner,
-                       uint32_t box_outer);
+                       uint32_t box_outer, int swizzle_bytes = 128);
 
 }  // namespace coral
