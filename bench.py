@@ -279,6 +279,87 @@ def precision_set(torch, cb, h, dev, g):
     return out
 
 
+def batched_set(torch, cb, dev):
+    """Batched configuration: 4096 SGEMM instances (m, n, k log-uniform in
+    [16, 512], 50% NN / 50% TN) fp32 and bf16-input, and 1024 STRSV lower
+    non-unit instances (n log-uniform in [32, 1024], diagonally dominant),
+    each as one CUDA-graph replay; useful flop / byte counts per instance."""
+    rng = np.random.default_rng(2024)
+    out = {}
+    stream = torch.cuda.current_stream()
+
+    def graph_time(fn, reps=10):
+        fn()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                fn()
+        torch.cuda.current_stream().wait_stream(s)
+        g.replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            g.replay()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        del g
+        return e0.elapsed_time(e1) / reps
+
+    count = 4096
+    dims = np.exp(rng.uniform(np.log(16), np.log(512), (count, 3))).astype(np.int64)
+    ops = np.where(rng.uniform(size=count) < 0.5, 0, 1)
+    flops = float(2 * (dims[:, 0] * dims[:, 1] * dims[:, 2]).sum())
+    for bf16 in (False, True):
+        rec = np.zeros(count, dtype=cb.sgemm_problem_dtype())
+        sizes = [(int(m) * int(k), int(k) * int(n), int(m) * int(n)) for m, n, k in dims]
+        tot_a, tot_b, tot_c = (sum(x[i] for x in sizes) for i in range(3))
+        dt = torch.bfloat16 if bf16 else torch.float32
+        pa = torch.empty(tot_a, dtype=dt, device=dev).uniform_(-1, 1)
+        pb = torch.empty(tot_b, dtype=dt, device=dev).uniform_(-1, 1)
+        pc = torch.empty(tot_c, dtype=torch.float32, device=dev).uniform_(-1, 1)
+        oa = ob = oc = 0
+        es = pa.element_size()
+        for i, (m, n, k) in enumerate(dims):
+            m, n, k = int(m), int(n), int(k)
+            op_a = int(ops[i])
+            rec[i] = (op_a, 0, m, n, k, 1.5, 0.5, 0, pa.data_ptr() + oa * es, pb.data_ptr() + ob * es,
+                      pc.data_ptr() + oc * 4, m if op_a == 0 else k, k, m)
+            oa += m * k; ob += k * n; oc += m * n
+        desc = torch.from_numpy(rec.view(np.uint8)).to(dev)
+        ms = graph_time(lambda: cb.sgemm_grouped(1 if bf16 else 0, count, desc))
+        out["grouped_sgemm_4096_" + ("bf16in" if bf16 else "fp32")] = {
+            "ms": ms, "tflops": flops / (ms * 1e-3) / 1e12, "instances": count}
+        del pa, pb, pc, desc
+    count = 1024
+    ns = np.exp(rng.uniform(np.log(32), np.log(1024), count)).astype(np.int64)
+    rec = np.zeros(count, dtype=cb.strsv_problem_dtype())
+    tot = int((ns * ns).sum())
+    pa = torch.empty(tot, dtype=torch.float32, device=dev).uniform_(-1, 1)
+    px = torch.empty(int(ns.sum()), dtype=torch.float32, device=dev).uniform_(-1, 1)
+    oa = ox = 0
+    for i, n in enumerate(ns):
+        n = int(n)
+        blk = pa[oa:oa + n * n].view(n, n)
+        idx = torch.arange(n, device=dev)
+        blk[idx, idx] = float(n) + torch.rand(n, device=dev)
+        rec[i] = (1, 0, 1, n, pa.data_ptr() + oa * 4, px.data_ptr() + ox * 4, n, 1)
+        oa += n * n; ox += n
+    desc = torch.from_numpy(rec.view(np.uint8)).to(dev)
+    nbytes = float((4 * (ns * (ns + 1) // 2 + 2 * ns)).sum())
+    x0 = px.clone()
+
+    def trsv_batch():
+        px.copy_(x0)
+        cb.strsv_batched(count, desc)
+    ms = graph_time(trsv_batch)
+    out["strsv_batched_1024"] = {"ms": ms, "gbs": nbytes / (ms * 1e-3) / 1e9, "instances": count}
+    return out
+
+
 def level12_bandwidth(torch, cb, lib, h, dev, g):
     """GB/s of algorithmic traffic for the level-1/2 bandwidth configuration
     (SGEMV N/T 8192^2, SSYMV upper 8192, STRSV lower non-unit 4096 with
@@ -501,6 +582,7 @@ def run_ours(args, world, rank, local):
     torch.cuda.empty_cache()
     l12 = level12_bandwidth(torch, cb, lib, h, dev, g)
     prec = precision_set(torch, cb, h, dev, g) if not args.skip_precision else None
+    batched = batched_set(torch, cb, dev) if not args.skip_precision else None
     h.set_gemm_mode(mode)
     gemv = {"n": l12["sgemv_n"]["gbs"], "t": l12["sgemv_t"]["gbs"]}
 
@@ -542,6 +624,7 @@ def run_ours(args, world, rank, local):
                          "frac_n": gemv["n"] / hbm, "frac_t": gemv["t"] / hbm},
             "level12": l12,
             "precision_gemm": prec,
+            "batched": batched,
             "roofline": roof, "clocks": clk, "gpu_launches": int(launches),
             "e2e": e2e, "cpu_baseline": cpu,
         }

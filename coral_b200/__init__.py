@@ -8,12 +8,14 @@ routine signatures (``coral_b200.blas``) plus the ctypes binding
 from .blas import (  # noqa: F401
     CoralDiagonal, CoralError, CoralTranspose, CoralTriangular, GemmMode, Handle, cgemm,
     chemv, dgemm, gemm_mode, handle, isamax, saxpy, scopy, sdot, set_gemm_mode, sgemm, sgemv,
-    sger, snrm2, sscal, sswap, ssymv, ssyr, ssyr2, strmv, strsv, zgemm,
+    sger, snrm2, sscal, sswap, ssymv, ssyr, ssyr2, strmv, strsv, zgemm, sgemm_grouped,
+    strsv_batched, sgemm_problem_dtype, strsv_problem_dtype,
 )
 
 __all__ = [
     "CoralDiagonal", "CoralError", "CoralTranspose", "CoralTriangular", "GemmMode", "Handle",
     "cgemm", "chemv", "dgemm", "gemm_mode", "handle", "isamax", "saxpy", "scopy", "sdot",
     "set_gemm_mode", "sgemm", "sgemv", "sger", "snrm2", "sscal", "sswap", "ssymv", "ssyr",
-    "ssyr2", "strmv", "strsv", "zgemm",
+    "ssyr2", "strmv", "strsv", "zgemm", "sgemm_grouped", "strsv_batched", "sgemm_problem_dtype",
+    "strsv_problem_dtype",
 ]

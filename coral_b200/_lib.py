@@ -63,6 +63,8 @@ SIGNATURES = {
     "coral_dgemm": [_h, _i, _i, _sz, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz],
     "coral_cgemm": [_h, _i, _i, _sz, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
     "coral_zgemm": [_h, _i, _i, _sz, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
+    "coral_sgemm_grouped": [_h, _i, _sz, _vp],
+    "coral_strsv_batched": [_h, _sz, _vp],
     "coral_sgemm_bf16x3_noalloc": [_vp, _i, _i, _sz, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
     "coral_host_sgemm": [_i, _i, _sz, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
     "coral_host_sgemv": [_i, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],

@@ -322,3 +322,33 @@ def set_gemm_mode(mode: int) -> None:
 
 def gemm_mode() -> int:
     return handle().gemm_mode()
+
+
+# ------------------------------------------------------- batched (no reference) --
+SGEMM_PROBLEM_DTYPE = None
+
+
+def sgemm_problem_dtype():
+    """numpy dtype matching coral_sgemm_problem_t (80 bytes)."""
+    import numpy as np
+    return np.dtype([("op_a", "<i4"), ("op_b", "<i4"), ("m", "<i4"), ("n", "<i4"), ("k", "<i4"),
+                     ("alpha", "<f4"), ("beta", "<f4"), ("reserved", "<i4"), ("a", "<u8"),
+                     ("b", "<u8"), ("c", "<u8"), ("lda", "<i8"), ("ldb", "<i8"), ("ldc", "<i8")])
+
+
+def strsv_problem_dtype():
+    """numpy dtype matching coral_strsv_problem_t (48 bytes)."""
+    import numpy as np
+    return np.dtype([("uplo", "<i4"), ("trans", "<i4"), ("diag", "<i4"), ("n", "<i4"),
+                     ("a", "<u8"), ("x", "<u8"), ("lda", "<i8"), ("incx", "<i8")])
+
+
+def sgemm_grouped(input_type, count, problems) -> None:
+    """Grouped SGEMM over `count` descriptors held in the CUDA tensor `problems`
+    (uint8 storage of coral_sgemm_problem_t records)."""
+    handle().call("coral_sgemm_grouped", int(input_type), count, C.c_void_p(problems.data_ptr()))
+
+
+def strsv_batched(count, problems) -> None:
+    """Batched STRSV over `count` descriptors held in the CUDA tensor `problems`."""
+    handle().call("coral_strsv_batched", count, C.c_void_p(problems.data_ptr()))

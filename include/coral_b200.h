@@ -180,6 +180,36 @@ coral_status_t coral_zgemm(coral_handle_t h, int op_a, int op_b, size_t m, size_
                            const double* b, size_t ldb, const double beta[2], double* c,
                            size_t ldc);
 
+/* ---- batched / grouped (no reference counterpart) ----------------------- */
+/* One instance of a grouped SGEMM: the arguments of coral_sgemm.  `a`, `b`
+ * are float or bf16 (per the call's input type), `c` is float. */
+typedef struct coral_sgemm_problem {
+  int32_t op_a, op_b, m, n, k;
+  float alpha, beta;
+  int32_t reserved;
+  const void* a;
+  const void* b;
+  float* c;
+  int64_t lda, ldb, ldc;
+} coral_sgemm_problem_t;
+enum { CORAL_INPUT_F32 = 0, CORAL_INPUT_BF16 = 1 };
+/* Computes every instance of `problems` (an array of `count` descriptors in
+ * DEVICE memory) with coral_sgemm's semantics; bf16 inputs accumulate in
+ * fp32.  A fixed number of kernels, no host work per instance: capturable in
+ * a CUDA graph once a first uncaptured call has sized the handle's scratch. */
+coral_status_t coral_sgemm_grouped(coral_handle_t h, int input_type, size_t count,
+                                   const coral_sgemm_problem_t* problems);
+/* One instance of a batched STRSV: the arguments of coral_strsv. */
+typedef struct coral_strsv_problem {
+  int32_t uplo, trans, diag, n;
+  const float* a;
+  float* x;
+  int64_t lda, incx;
+} coral_strsv_problem_t;
+/* Solves every instance (descriptors in DEVICE memory) in one launch. */
+coral_status_t coral_strsv_batched(coral_handle_t h, size_t count,
+                                   const coral_strsv_problem_t* problems);
+
 /* ---- allocation-free split-BF16x3 SGEMM --------------------------------- */
 /* No counterpart in the reference (CORAL allocates its packing buffers on
  * every call).  Same arguments and result as coral_sgemm in
