@@ -64,6 +64,20 @@ SIGNATURES = {
     "coral_cgemm": [_h, _i, _i, _sz, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
     "coral_zgemm": [_h, _i, _i, _sz, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
     "coral_sgemm_grouped": [_h, _i, _sz, _vp],
+    "coral_set_gemm_config": [_h, _i, _i],
+    "coral_get_gemm_config": [_h, _i, _i, _i, _sz, _sz, _sz, C.POINTER(_i), C.POINTER(_i)],
+    "coral_selector_features": [_i, _i, _i, _sz, _sz, _sz, _i, _i, C.POINTER(_f)],
+    "coral_autotune_sgemm": [_h, _i, _i, _i, _sz, _sz, _sz, _vp, _sz, _vp, _sz, _vp, _sz, _i,
+                             C.POINTER(_f), C.POINTER(_i)],
+    "coral_mlp_create": [_h, _i, _i, _i, C.c_uint64, C.POINTER(_vp)],
+    "coral_mlp_destroy": [_vp],
+    "coral_mlp_param_count": [_vp],
+    "coral_mlp_get_params": [_vp, C.POINTER(_f), _sz],
+    "coral_mlp_set_params": [_vp, C.POINTER(_f), _sz],
+    "coral_mlp_forward": [_vp, _vp, _i, _vp],
+    "coral_mlp_gradients": [_vp, _vp, _vp, _i, _vp, C.POINTER(_f)],
+    "coral_mlp_train_step": [_vp, _vp, _vp, _i, _f, C.POINTER(_f)],
+    "coral_set_selector": [_h, _vp],
     "coral_strsv_batched": [_h, _sz, _vp],
     "coral_sgemm_bf16x3_noalloc": [_vp, _i, _i, _sz, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
     "coral_host_sgemm": [_i, _i, _sz, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
@@ -81,6 +95,7 @@ _RESTYPE = {
     "coral_last_cuda_error": C.c_char_p,
     "coral_abi_version": C.c_int,
     "coral_kernel_launches": C.c_uint64,
+    "coral_mlp_param_count": C.c_size_t,
 }
 
 

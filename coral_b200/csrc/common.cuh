@@ -28,6 +28,10 @@ struct Handle {
   uint64_t wait_limit = kDefaultWaitLimit;
   // K slabs (64 deep) per tensor-core accumulation chunk of the split GEMMs.
   int split_chunk_kb = 16;
+  // Explicit split-GEMM configuration (0 = not set): N tile width, split-K.
+  int cfg_bn = 0, cfg_splits = 0;
+  // Learned configuration selector (see selector.cu), or null.
+  struct Selector* selector = nullptr;
   int bad_arg = 0;
   std::string cuda_error;
 
@@ -115,6 +119,27 @@ inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 
 // Copies a scalar result produced at device address `src` to `dst` per the
 // pointer mode (host: waits on the stream).
 coral_status_t deliver_result(Handle* h, void* dst, const void* src, size_t bytes);
+
+// Split-BF16 GEMM configuration (tile width BN, split-K factor).
+struct SplitConfig {
+  int bn;
+  int splits;
+};
+// Shape of a split-BF16 GEMM call as the configuration policy sees it:
+// op(A) rows mr, B-rows nr (2n for complex), depth kd (2k for complex).
+struct SplitShape {
+  int mr, nr, kd;
+  int products;  // 3 or 6
+  int op_a, op_b;
+  int complex_;
+  int batch;
+};
+SplitConfig choose_split_config(Handle* h, const SplitShape& sh);
+// Asks the handle's selector for a configuration; false if it has none.
+bool select_split_config(Handle* h, const SplitShape& sh, SplitConfig* out);
+// Features of (shape, configuration) for the selector network.
+constexpr int kSelectorFeatures = 13;
+void selector_features(const SplitShape& sh, int bn, int splits, float* f);
 
 // Per-thread default handle for the coral_host_* entry points.
 Handle* thread_handle();

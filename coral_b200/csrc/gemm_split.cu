@@ -244,7 +244,8 @@ constexpr int kSplitThreads = 64 + 32 * kEpiWarps;
 template <int NP, int BN>
 __global__ void __launch_bounds__(kSplitThreads, 1)
 k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int n_tiles,
-             int chunk_kb, EpiParams ep, unsigned* status, uint64_t limit_ns) {
+             int chunk_kb, int splits, float* ws, int ws_cols, EpiParams ep, unsigned* status,
+             uint64_t limit_ns) {
   using Plan = SplitPlan<NP>;
   constexpr int kPieces = Plan::kPieces;
   constexpr uint32_t kATile = kBM * kBK * 2;  // bytes per A piece tile
@@ -262,8 +263,15 @@ k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int 
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nk = (kdim + kBK - 1) / kBK;
-  const int chunks_per_tile = (nk + chunk_kb - 1) / chunk_kb;
-  const int total_tiles = m_tiles * n_tiles;
+  // Work item = (output tile, K part); with splits > 1 each part covers
+  // ceil(nk / splits) slabs and its raw sums go to the workspace.
+  const int total_items = m_tiles * n_tiles * splits;
+  const int sk = (nk + splits - 1) / splits;
+  auto slab_range = [&](int item, int& lo, int& hi) {
+    const int part = item % splits;
+    lo = min(nk, part * sk);
+    hi = min(nk, lo + sk);
+  };
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
@@ -294,10 +302,11 @@ k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int 
         tc::prefetch_tmap(&maps.b[p]);
       }
       int it = 0;  // k-slab counter across tiles
-      for (int tile = blockIdx.x; tile < total_tiles && !abort_flag; tile += gridDim.x) {
-        int mt, nt;
-        tile_coords(tile, m_tiles, n_tiles, mt, nt);
-        for (int kb = 0; kb < nk; ++kb, ++it) {
+      for (int item = blockIdx.x; item < total_items && !abort_flag; item += gridDim.x) {
+        int mt, nt, kb_lo, kb_hi;
+        tile_coords(item / splits, m_tiles, n_tiles, mt, nt);
+        slab_range(item, kb_lo, kb_hi);
+        for (int kb = kb_lo; kb < kb_hi; ++kb, ++it) {
           const int s = it % kStages;
           if (it >= kStages && !tc::mbar_wait(&empty_bar[s], ((it / kStages) - 1) & 1, limit_ns)) {
             atomicOr(status, kStatusTimeout);
@@ -322,8 +331,11 @@ k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int 
       // ---- MMA issuer ----
       int it = 0, gc = 0;  // k-slab and chunk counters across tiles
       bool stop = false;
-      for (int tile = blockIdx.x; tile < total_tiles && !stop; tile += gridDim.x) {
-        for (int c = 0; c < chunks_per_tile && !stop; ++c, ++gc) {
+      for (int item = blockIdx.x; item < total_items && !stop; item += gridDim.x) {
+        int kb_lo, kb_hi;
+        slab_range(item, kb_lo, kb_hi);
+        const int chunks = (kb_hi - kb_lo + chunk_kb - 1) / chunk_kb;
+        for (int c = 0; c < chunks && !stop; ++c, ++gc) {
           const int b = gc & 1;
           if (gc >= 2 && !tc::mbar_wait(&chunk_empty[b], ((gc >> 1) - 1) & 1, limit_ns)) {
             atomicOr(status, kStatusTimeout);
@@ -333,7 +345,7 @@ k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int 
           }
           tc::tc_fence_after();
           const uint32_t acc = tmem + b * BN;
-          const int kb0 = c * chunk_kb, kb1 = min(nk, kb0 + chunk_kb);
+          const int kb0 = kb_lo + c * chunk_kb, kb1 = min(kb_hi, kb0 + chunk_kb);
           for (int kb = kb0; kb < kb1; ++kb, ++it) {
             const int s = it % kStages;
             if (!tc::mbar_wait(&full_bar[s], (it / kStages) & 1, limit_ns)) {
@@ -370,13 +382,15 @@ k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int 
     const bool beta1 = ep.beta_re == 1.f && ep.beta_im == 0.f;
     int gc = 0;
     bool stop = false;
-    for (int tile = blockIdx.x; tile < total_tiles && !stop; tile += gridDim.x) {
-      int mt, nt;
-      tile_coords(tile, m_tiles, n_tiles, mt, nt);
+    for (int item = blockIdx.x; item < total_items && !stop; item += gridDim.x) {
+      int mt, nt, kb_lo, kb_hi;
+      tile_coords(item / splits, m_tiles, n_tiles, mt, nt);
+      slab_range(item, kb_lo, kb_hi);
+      const int chunks = (kb_hi - kb_lo + chunk_kb - 1) / chunk_kb;
       float sum[kCols];
 #pragma unroll
       for (int j = 0; j < kCols; ++j) sum[j] = 0.f;
-      for (int c = 0; c < chunks_per_tile; ++c, ++gc) {
+      for (int c = 0; c < chunks; ++c, ++gc) {
         const int b = gc & 1;
         if (!tc::mbar_wait(&chunk_full[b], (gc >> 1) & 1, limit_ns)) {
           atomicOr(status, kStatusTimeout);
@@ -401,7 +415,12 @@ k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int 
       const int row = mt * kBM + quad * 32 + lane;
       if (row >= ep.m) continue;
       const int col0 = nt * BN + half * kCols;  // first accumulator column of this thread
-      if (!ep.complex_out) {
+      if (splits > 1) {  // raw partial sums; k_split_reduce applies the epilogue
+        float* wp = ws + ((size_t)(item % splits) * ws_cols) * ep.m + row;
+#pragma unroll
+        for (int j = 0; j < kCols; ++j)
+          if (col0 + j < ws_cols) wp[(size_t)(col0 + j) * ep.m] = sum[j];
+      } else if (!ep.complex_out) {
         float* crow = ep.C + row;
 #pragma unroll
         for (int j = 0; j < kCols; ++j) {
@@ -442,20 +461,55 @@ k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int 
   if (warp == 1) tc::tmem_dealloc(tmem, 2 * BN);
 }
 
-template <int NP> constexpr int tile_n() { return NP == 3 ? 256 : 128; }
+// Split-K combine: C = alpha * sum_p ws[p] + beta * C in a fixed part order.
+__global__ void k_split_reduce(const float* __restrict__ ws, int splits, int ws_cols, EpiParams ep) {
+  const size_t total = (size_t)ep.m * ep.n;
+  const bool beta0 = ep.beta_re == 0.f && ep.beta_im == 0.f;
+  const bool beta1 = ep.beta_re == 1.f && ep.beta_im == 0.f;
+  const size_t part = (size_t)ws_cols * ep.m;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int row = (int)(t % ep.m), col = (int)(t / ep.m);
+    if (!ep.complex_out) {
+      float s = 0.f;
+      for (int p = 0; p < splits; ++p) s += ws[p * part + (size_t)col * ep.m + row];
+      float* cp = ep.C + row + (size_t)col * ep.ldc;
+      const float v = ep.alpha_re * s;
+      if (beta0) *cp = v;
+      else if (beta1) *cp = *cp + v;
+      else *cp = ep.beta_re * *cp + v;
+    } else {
+      float ar = 0.f, ai = 0.f;
+      for (int p = 0; p < splits; ++p) {
+        ar += ws[p * part + (size_t)(2 * col) * ep.m + row];
+        ai += ws[p * part + (size_t)(2 * col + 1) * ep.m + row];
+      }
+      float2* cp = reinterpret_cast<float2*>(ep.C) + row + (size_t)col * ep.ldc;
+      float2 v = make_float2(ep.alpha_re * ar - ep.alpha_im * ai, ep.alpha_re * ai + ep.alpha_im * ar);
+      if (!beta0) {
+        const float2 cv = *cp;
+        if (beta1) { v.x += cv.x; v.y += cv.y; }
+        else {
+          v.x += ep.beta_re * cv.x - ep.beta_im * cv.y;
+          v.y += ep.beta_re * cv.y + ep.beta_im * cv.x;
+        }
+      }
+      *cp = v;
+    }
+  }
+}
 
-template <int NP>
+template <int NP, int BN>
 size_t gemm_smem_bytes() {
-  constexpr int BN = tile_n<NP>();
   return (size_t)kStages * SplitPlan<NP>::kPieces * (kBM * kBK * 2 + BN * kBK * 2) + 1024;
 }
 
-// Runs the GEMM kernel over prepared pieces: A pieces [mr][kp], B pieces [nr][kp].
-template <int NP>
+// Runs the GEMM kernel over prepared pieces: A pieces [mr][kp], B pieces [nr][kp];
+// with splits > 1, `ws` holds splits x nr x mr floats of partial sums.
+template <int NP, int BN>
 coral_status_t run_split_gemm(Handle* h, const __nv_bfloat16* ap, size_t a_piece, int mr,
                               const __nv_bfloat16* bp, size_t b_piece, int nr, int kd, size_t kp,
-                              const EpiParams& ep) {
-  constexpr int BN = tile_n<NP>();
+                              int splits, float* ws, const EpiParams& ep) {
   SplitMaps maps;
   std::memset(&maps, 0, sizeof(maps));
   for (int p = 0; p < SplitPlan<NP>::kPieces; ++p) {
@@ -463,7 +517,7 @@ coral_status_t run_split_gemm(Handle* h, const __nv_bfloat16* ap, size_t a_piece
         !encode_kmajor_map(&maps.b[p], bp + p * b_piece, 2, (uint64_t)kd, (uint64_t)nr, kp * 2, kBK, BN))
       return CORAL_ERR_NOT_SUPPORTED;
   }
-  const size_t smem = gemm_smem_bytes<NP>();
+  const size_t smem = gemm_smem_bytes<NP, BN>();
   static uint64_t attr_devices = 0;  // bit d: attribute set on device d
   const uint64_t bit = h->device < 64 ? (1ull << h->device) : 0;
   if (!(attr_devices & bit) || !bit) {
@@ -472,15 +526,63 @@ coral_status_t run_split_gemm(Handle* h, const __nv_bfloat16* ap, size_t a_piece
     attr_devices |= bit;
   }
   const int m_tiles = (mr + kBM - 1) / kBM, n_tiles = (nr + BN - 1) / BN;
-  const int tiles = m_tiles * n_tiles;
-  const int grid = tiles < h->sm_count ? tiles : h->sm_count;
+  const int items = m_tiles * n_tiles * splits;
+  const int grid = items < h->sm_count ? items : h->sm_count;
   const uint64_t limit_ns = h->wait_limit * 32ull;  // default 2^26 * 32 ns ~ 2.1 s
   timed_begin(h);
   k_gemm_split<NP, BN><<<grid, kSplitThreads, smem, h->stream>>>(
-      maps, kd, m_tiles, n_tiles, h->split_chunk_kb, ep, &h->words->status, limit_ns);
+      maps, kd, m_tiles, n_tiles, h->split_chunk_kb, splits, ws, nr, ep, &h->words->status,
+      limit_ns);
   coral_status_t s = launch_status(h);
   timed_end(h);
-  return s;
+  if (s != CORAL_OK || splits == 1) return s;
+  unsigned g = stream_grid((size_t)ep.m * ep.n, 256 * 4, h->sm_count, 8);
+  k_split_reduce<<<g, 256, 0, h->stream>>>(ws, splits, nr, ep);
+  return launch_status(h);
+}
+
+}  // namespace
+
+// Tile width and split-K factor for a split-BF16 GEMM of op(A) (mr x kd)
+// times B-rows (nr x kd): the handle's explicit choice, else its selector,
+// else the default rule (full-width tiles; split K when the output tiles
+// cannot fill the GPU and K is deep).
+SplitConfig choose_split_config(Handle* h, const SplitShape& sh) {
+  const int products = sh.products, mr = sh.mr, nr = sh.nr, kd = sh.kd;
+  SplitConfig c{products == 3 ? 256 : 128, 1};
+  const int nk = (kd + kBK - 1) / kBK;
+  if (h->cfg_bn > 0 || h->cfg_splits > 0) {
+    if (h->cfg_bn > 0) c.bn = h->cfg_bn;
+    if (h->cfg_splits > 0) c.splits = h->cfg_splits;
+  } else if (h->selector && select_split_config(h, sh, &c)) {
+    // selector decided
+  } else {
+    const int tiles = ((mr + kBM - 1) / kBM) * ((nr + c.bn - 1) / c.bn);
+    if (tiles * 2 <= h->sm_count && nk >= 16) {
+      int sp = h->sm_count / tiles;
+      sp = sp > 16 ? 16 : sp;
+      sp = sp > nk ? nk : sp;
+      int p2 = 1;  // largest power of two <= sp (the tuned candidate set)
+      while (p2 * 2 <= sp) p2 *= 2;
+      c.splits = p2;
+    }
+  }
+  if (products == 6) c.bn = 128;
+  if (c.bn != 128 && c.bn != 256) c.bn = 256;
+  if (c.splits > nk) c.splits = nk > 0 ? nk : 1;
+  if (c.splits < 1) c.splits = 1;
+  return c;
+}
+
+namespace {
+
+template <int NP>
+coral_status_t dispatch_split_gemm(Handle* h, const __nv_bfloat16* ap, size_t a_piece, int mr,
+                                   const __nv_bfloat16* bp, size_t b_piece, int nr, int kd,
+                                   size_t kp, const SplitConfig& c, float* ws, const EpiParams& ep) {
+  if (NP == 3 && c.bn == 256)
+    return run_split_gemm<NP, 256>(h, ap, a_piece, mr, bp, b_piece, nr, kd, kp, c.splits, ws, ep);
+  return run_split_gemm<NP, 128>(h, ap, a_piece, mr, bp, b_piece, nr, kd, kp, c.splits, ws, ep);
 }
 
 template <int NP>
@@ -491,8 +593,10 @@ coral_status_t sgemm_split_impl(Handle* h, int op_a, int op_b, size_t m, size_t 
   const size_t kp = (k + 7) & ~size_t(7);
   const size_t a_piece = m * kp, b_piece = n * kp;
   const size_t a_bytes = (NPC * a_piece * 2 + 255) & ~size_t(255);
-  const size_t b_bytes = NPC * b_piece * 2;
-  char* sc = static_cast<char*>(scratch(h, a_bytes + b_bytes));
+  const size_t b_bytes = (NPC * b_piece * 2 + 255) & ~size_t(255);
+  const SplitConfig cfg = choose_split_config(h, SplitShape{(int)m, (int)n, (int)k, NP, op_a, op_b, 0, 1});
+  const size_t ws_bytes = cfg.splits > 1 ? (size_t)cfg.splits * m * n * sizeof(float) : 0;
+  char* sc = static_cast<char*>(scratch(h, a_bytes + b_bytes + ws_bytes));
   if (!sc) return CORAL_ERR_ALLOC;
   __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(sc);
   __nv_bfloat16* bp = reinterpret_cast<__nv_bfloat16*>(sc + a_bytes);
@@ -513,7 +617,8 @@ coral_status_t sgemm_split_impl(Handle* h, int op_a, int op_b, size_t m, size_t 
   s = launch_status(h);
   if (s != CORAL_OK) return s;
   EpiParams ep{C, ldc, (int)m, (int)n, alpha, 0.f, beta, 0.f, 0};
-  return run_split_gemm<NP>(h, ap, a_piece, (int)m, bp, b_piece, (int)n, (int)k, kp, ep);
+  float* ws = reinterpret_cast<float*>(sc + a_bytes + b_bytes);
+  return dispatch_split_gemm<NP>(h, ap, a_piece, (int)m, bp, b_piece, (int)n, (int)k, kp, cfg, ws, ep);
 }
 
 template <int NP>
@@ -525,8 +630,11 @@ coral_status_t cgemm_split_impl(Handle* h, int op_a, int op_b, size_t m, size_t 
   const size_t kp = (k2 + 7) & ~size_t(7);
   const size_t a_piece = m * kp, b_piece = 2 * n * kp;
   const size_t a_bytes = (NPC * a_piece * 2 + 255) & ~size_t(255);
-  const size_t b_bytes = NPC * b_piece * 2;
-  char* sc = static_cast<char*>(scratch(h, a_bytes + b_bytes));
+  const size_t b_bytes = (NPC * b_piece * 2 + 255) & ~size_t(255);
+  const SplitConfig cfg =
+      choose_split_config(h, SplitShape{(int)m, (int)(2 * n), (int)k2, NP, op_a, op_b, 1, 1});
+  const size_t ws_bytes = cfg.splits > 1 ? (size_t)cfg.splits * m * 2 * n * sizeof(float) : 0;
+  char* sc = static_cast<char*>(scratch(h, a_bytes + b_bytes + ws_bytes));
   if (!sc) return CORAL_ERR_ALLOC;
   __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(sc);
   __nv_bfloat16* bp = reinterpret_cast<__nv_bfloat16*>(sc + a_bytes);
@@ -549,7 +657,9 @@ coral_status_t cgemm_split_impl(Handle* h, int op_a, int op_b, size_t m, size_t 
   s = launch_status(h);
   if (s != CORAL_OK) return s;
   EpiParams ep{reinterpret_cast<float*>(C), ldc, (int)m, (int)n, alpha.x, alpha.y, beta.x, beta.y, 1};
-  return run_split_gemm<NP>(h, ap, a_piece, (int)m, bp, b_piece, (int)(2 * n), (int)k2, kp, ep);
+  float* ws = reinterpret_cast<float*>(sc + a_bytes + b_bytes);
+  return dispatch_split_gemm<NP>(h, ap, a_piece, (int)m, bp, b_piece, (int)(2 * n), (int)k2, kp, cfg,
+                                 ws, ep);
 }
 
 }  // namespace
@@ -632,7 +742,7 @@ static coral_status_t noalloc_setup(NoAllocDevice** out) {
     e = cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return cuda_status(nullptr, e);
     e = cudaFuncSetAttribute(k_gemm_split<3, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)gemm_smem_bytes<3>());
+                             (int)gemm_smem_bytes<3, 256>());
     if (e != cudaSuccess) return cuda_status(nullptr, e);
     d.ready = true;
   }
@@ -697,7 +807,7 @@ extern "C" coral_status_t coral_sgemm_bf16x3_noalloc(void* stream, int op_a, int
   const int tiles = m_tiles * n_tiles;
   const int grid = tiles < d->sm_count ? tiles : d->sm_count;
   EpiParams ep{c, ldc, (int)m, (int)n, alpha, 0.f, beta, 0.f, 0};
-  k_gemm_split<3, 256><<<grid, kSplitThreads, gemm_smem_bytes<3>(), st>>>(
-      maps, (int)k, m_tiles, n_tiles, 16, ep, d->status, kDefaultWaitLimit * 32ull);
+  k_gemm_split<3, 256><<<grid, kSplitThreads, gemm_smem_bytes<3, 256>(), st>>>(
+      maps, (int)k, m_tiles, n_tiles, 16, 1, nullptr, (int)n, ep, d->status, kDefaultWaitLimit * 32ull);
   return launch_status(nullptr);
 }

@@ -97,9 +97,12 @@ void timed_end(Handle* h) {
   ++h->timing_used;
 }
 
+extern "C" coral_status_t coral_set_selector(coral_handle_t, coral_mlp_t);
+
 static void destroy_handle(Handle* h) {
   if (!h) return;
   cudaStreamSynchronize(h->stream);
+  if (h->selector) coral_set_selector(reinterpret_cast<coral_handle_t>(h), nullptr);
   for (auto& e : h->timing_events) {
     cudaEventDestroy(e.first);
     cudaEventDestroy(e.second);

@@ -210,6 +210,52 @@ typedef struct coral_strsv_problem {
 coral_status_t coral_strsv_batched(coral_handle_t h, size_t count,
                                    const coral_strsv_problem_t* problems);
 
+/* ---- configuration, autotuning and the learned selector ----------------- */
+/* (No reference counterpart.)  Split-BF16 GEMM configuration: N tile width
+ * (128 or 256) and split-K factor (1..64); 0 leaves the choice to the
+ * selector (when set) or to the default rule. */
+coral_status_t coral_set_gemm_config(coral_handle_t h, int tile_n, int split_k);
+/* The configuration a split-BF16 SGEMM of this shape would use now. */
+coral_status_t coral_get_gemm_config(coral_handle_t h, int products, int op_a, int op_b, size_t m,
+                                     size_t n, size_t k, int* tile_n, int* split_k);
+/* Features the selector network sees for (shape, configuration); 13 floats. */
+coral_status_t coral_selector_features(int products, int op_a, int op_b, size_t m, size_t n,
+                                       size_t k, int tile_n, int split_k, float* out);
+/* Exhaustive autotuning of one split-BF16 SGEMM shape on the given device
+ * buffers: times every (tile_n, split_k) candidate `reps` times (after one
+ * warm-up) with CUDA events; writes per-candidate milliseconds in the order
+ * tile_n in {256, 128} x split_k in {1, 2, 4, 8, 16} (10 values, products 6:
+ * only the 5 tile_n = 128 values) and the index of the fastest.  C is
+ * overwritten.  Restores the handle's previous configuration. */
+coral_status_t coral_autotune_sgemm(coral_handle_t h, int products, int op_a, int op_b, size_t m,
+                                    size_t n, size_t k, const float* a, size_t lda, const float* b,
+                                    size_t ldb, float* c, size_t ldc, int reps, float* ms_out,
+                                    int* best);
+
+/* A small MLP (in -> hidden -> hidden -> out, ReLU) trained and evaluated by
+ * the library's own kernels; used as the configuration selector (in = 13,
+ * out = 1: predicted log milliseconds). */
+typedef struct coral_mlp_s* coral_mlp_t;
+coral_status_t coral_mlp_create(coral_handle_t h, int in_dim, int hidden, int out_dim,
+                                uint64_t seed, coral_mlp_t* mlp);
+coral_status_t coral_mlp_destroy(coral_mlp_t mlp);
+size_t coral_mlp_param_count(coral_mlp_t mlp);
+coral_status_t coral_mlp_get_params(coral_mlp_t mlp, float* host, size_t count);
+coral_status_t coral_mlp_set_params(coral_mlp_t mlp, const float* host, size_t count);
+/* x: DEVICE [batch][in], y: DEVICE [batch][out]. */
+coral_status_t coral_mlp_forward(coral_mlp_t mlp, const float* x, int batch, float* y);
+/* Gradient of mean((y - target)^2) w.r.t. the packed parameters into the
+ * DEVICE array `grads` (may be NULL); loss to host memory (may be NULL). */
+coral_status_t coral_mlp_gradients(coral_mlp_t mlp, const float* x, const float* target, int batch,
+                                   float* grads, float* loss);
+/* One Adam step (beta1 0.9, beta2 0.999) on a batch; loss to host (may be NULL). */
+coral_status_t coral_mlp_train_step(coral_mlp_t mlp, const float* x, const float* target, int batch,
+                                    float lr, float* loss);
+/* Attach (or, with NULL, detach) a trained selector to a handle.  Decisions
+ * are cached per shape; the first call for a shape waits for one forward
+ * pass, so make it outside stream capture. */
+coral_status_t coral_set_selector(coral_handle_t h, coral_mlp_t mlp);
+
 /* ---- allocation-free split-BF16x3 SGEMM --------------------------------- */
 /* No counterpart in the reference (CORAL allocates its packing buffers on
  * every call).  Same arguments and result as coral_sgemm in
