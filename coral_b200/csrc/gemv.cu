@@ -131,9 +131,14 @@ k_gemv_t(int m, int n, const float* __restrict__ A, size_t lda, const float* __r
   const int r0 = blockIdx.y * rows_per_chunk;
   const int r1 = min(m, r0 + rows_per_chunk);
   const int nr = r1 - r0;
-  for (int i = threadIdx.x; i < nr; i += blockDim.x)
-    xs[i] = __fmul_rn(alpha, __ldg(x + (size_t)(r0 + i) * incx));
-  __syncthreads();
+  // alpha*x for this row chunk: staged in shared memory for strided x;
+  // unit-stride x is scaled on the fly from the read-only cache (xsc).
+  const bool direct = kVec && incx == 1 && ((reinterpret_cast<uintptr_t>(x + r0) & 15) == 0);
+  if (!direct) {
+    for (int i = threadIdx.x; i < nr; i += blockDim.x)
+      xs[i] = __fmul_rn(alpha, __ldg(x + (size_t)(r0 + i) * incx));
+    __syncthreads();
+  }
   const int g0 = blockIdx.x * cols_per_group;
   const int g1 = min(n, g0 + cols_per_group);
   for (int j = g0 + warp; j < g1; j += kGemvWarps) {
@@ -142,12 +147,20 @@ k_gemv_t(int m, int n, const float* __restrict__ A, size_t lda, const float* __r
     if (kVec) {
       const int n4 = nr >> 2;
       const float4* c4 = reinterpret_cast<const float4*>(col);
-      const float4* x4 = reinterpret_cast<const float4*>(xs);
+      const float4* x4 = reinterpret_cast<const float4*>(direct ? x + r0 : xs);
+      auto xsc = [&](int q) {
+        float4 v = direct ? __ldg(x4 + q) : x4[q];
+        if (direct) {
+          v.x = __fmul_rn(alpha, v.x); v.y = __fmul_rn(alpha, v.y);
+          v.z = __fmul_rn(alpha, v.z); v.w = __fmul_rn(alpha, v.w);
+        }
+        return v;
+      };
       int i = lane;
       for (; i + 96 < n4; i += 128) {
         float4 a0 = __ldcs(c4 + i), a1 = __ldcs(c4 + i + 32);
         float4 a2 = __ldcs(c4 + i + 64), a3 = __ldcs(c4 + i + 96);
-        float4 b0 = x4[i], b1 = x4[i + 32], b2 = x4[i + 64], b3 = x4[i + 96];
+        float4 b0 = xsc(i), b1 = xsc(i + 32), b2 = xsc(i + 64), b3 = xsc(i + 96);
         acc0 = fmaf(a0.x, b0.x, acc0); acc0 = fmaf(a0.y, b0.y, acc0);
         acc0 = fmaf(a0.z, b0.z, acc0); acc0 = fmaf(a0.w, b0.w, acc0);
         acc1 = fmaf(a1.x, b1.x, acc1); acc1 = fmaf(a1.y, b1.y, acc1);
@@ -158,11 +171,12 @@ k_gemv_t(int m, int n, const float* __restrict__ A, size_t lda, const float* __r
         acc1 = fmaf(a3.z, b3.z, acc1); acc1 = fmaf(a3.w, b3.w, acc1);
       }
       for (; i < n4; i += 32) {
-        float4 a = __ldcs(c4 + i), b = x4[i];
+        float4 a = __ldcs(c4 + i), b = xsc(i);
         acc0 = fmaf(a.x, b.x, acc0); acc0 = fmaf(a.y, b.y, acc0);
         acc0 = fmaf(a.z, b.z, acc0); acc0 = fmaf(a.w, b.w, acc0);
       }
-      for (int t = (n4 << 2) + lane; t < nr; t += 32) acc1 = fmaf(__ldcs(col + t), xs[t], acc1);
+      for (int t = (n4 << 2) + lane; t < nr; t += 32)
+        acc1 = fmaf(__ldcs(col + t), direct ? __fmul_rn(alpha, __ldg(x + r0 + t)) : xs[t], acc1);
     } else {
       int i = lane;
       for (; i + 32 < nr; i += 64) {

@@ -98,19 +98,30 @@ k_dot(size_t n, const float* __restrict__ x, size_t incx, const float* __restric
     const size_t n4 = n >> 2;
     const float4* x4 = reinterpret_cast<const float4*>(x);
     const float4* y4 = reinterpret_cast<const float4*>(y);
+    // 4 independent 128-bit loads per operand in flight per thread
     size_t i = tid;
-    for (; i + stride < n4; i += 2 * stride) {
-      float4 a = __ldcs(x4 + i), c = __ldcs(x4 + i + stride);
-      float4 b = kSquare ? a : __ldcs(y4 + i);
-      float4 d = kSquare ? c : __ldcs(y4 + i + stride);
-      acc += (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
-      acc += (double)c.x * d.x + (double)c.y * d.y + (double)c.z * d.z + (double)c.w * d.w;
+    double acc1 = 0.0;
+    for (; i + 3 * stride < n4; i += 4 * stride) {
+      float4 a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) a[u] = __ldcs(x4 + i + u * stride);
+      if (!kSquare) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) b[u] = __ldcs(y4 + i + u * stride);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const float4 c = kSquare ? a[u] : b[u];
+        double& t = (u & 1) ? acc1 : acc;
+        t += (double)a[u].x * c.x + (double)a[u].y * c.y + (double)a[u].z * c.z + (double)a[u].w * c.w;
+      }
     }
-    if (i < n4) {
+    for (; i < n4; i += stride) {
       float4 a = __ldcs(x4 + i);
       float4 b = kSquare ? a : __ldcs(y4 + i);
       acc += (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
     }
+    acc += acc1;
     for (size_t t = (n4 << 2) + tid; t < n; t += stride) {
       float a = x[t], b = kSquare ? a : y[t];
       acc += (double)a * b;
@@ -147,7 +158,20 @@ k_iamax(size_t n, const float* __restrict__ x, size_t incx, float* pv,
   if (kVec) {
     const size_t n4 = n >> 2;
     const float4* x4 = reinterpret_cast<const float4*>(x);
-    for (size_t i = tid; i < n4; i += stride) {
+    size_t i = tid;
+    for (; i + 3 * stride < n4; i += 4 * stride) {  // 4 loads in flight, scanned in index order
+      float4 a[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) a[u] = __ldcs(x4 + i + u * stride);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const float v[4] = {fabsf(a[u].x), fabsf(a[u].y), fabsf(a[u].z), fabsf(a[u].w)};
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (v[e] > best.v) { best.v = v[e]; best.i = ((i + u * stride) << 2) + e; }
+      }
+    }
+    for (; i < n4; i += stride) {
       float4 a = __ldcs(x4 + i);
       float v[4] = {fabsf(a.x), fabsf(a.y), fabsf(a.z), fabsf(a.w)};
 #pragma unroll

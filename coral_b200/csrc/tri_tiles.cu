@@ -66,7 +66,7 @@ template <typename T, int kMode>
 __global__ void __launch_bounds__(kTriThreads)
 k_tri_tiles(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x, size_t incx,
             T alpha, bool lower, bool unit, T* __restrict__ rowpart, T* __restrict__ colpart,
-            int max_seg) {
+            int max_seg, int diag_only) {
   constexpr bool kSym = kMode == kSymv || kMode == kHemv;
   constexpr bool kRow = kMode != kTrmvT;
   constexpr bool kCol = kMode == kSymv || kMode == kHemv || kMode == kTrmvT;
@@ -77,8 +77,8 @@ k_tri_tiles(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x,
   const int NT = (n + kT - 1) / kT;
   const int J = blockIdx.x, seg = blockIdx.y;
   // Stored tiles of tile-column J: upper I = 0..J, lower I = J..NT-1.
-  const int first = lower ? J : 0;
-  const int count = lower ? NT - J : J + 1;
+  const int first = diag_only ? J : (lower ? J : 0);
+  const int count = diag_only ? 1 : (lower ? NT - J : J + 1);
   const int t0 = seg * kSeg;
   if (t0 >= count) return;
   const int t1 = min(count, t0 + kSeg);
@@ -163,7 +163,7 @@ k_tri_tiles(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x,
     __syncthreads();
     if (kRow && tid < kT) {
       T s = Cx<T>::add(Cx<T>::add(red[0][tid], red[1][tid]), Cx<T>::add(red[2][tid], red[3][tid]));
-      rowpart[tri_index(I, J, lower) * kT + tid] = s;
+      rowpart[(diag_only ? (size_t)J : tri_index(I, J, lower)) * kT + tid] = s;
     }
   }
   if (kCol) {
@@ -172,7 +172,7 @@ k_tri_tiles(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x,
     __syncthreads();
     if (tid < kT) {
       T s = Cx<T>::add(Cx<T>::add(red[0][tid], red[1][tid]), Cx<T>::add(red[2][tid], red[3][tid]));
-      colpart[((size_t)J * max_seg + seg) * kT + tid] = s;
+      colpart[(diag_only ? (size_t)J : ((size_t)J * max_seg + seg)) * kT + tid] = s;
     }
   }
 }
@@ -224,11 +224,181 @@ coral_status_t run_tri(Handle* h, int n, const T* A, size_t lda, const T* x, siz
   dim3 grid(NT, max_seg);
   timed_begin(h);
   k_tri_tiles<T, kMode><<<grid, kTriThreads, 0, h->stream>>>(n, A, lda, x, incx, alpha, lower, unit,
-                                                             sc, sc + rp, max_seg);
+                                                             sc, sc + rp, max_seg, 0);
   coral_status_t s = launch_status(h);
   timed_end(h);
   if (s != CORAL_OK) return s;
   k_tri_combine<T, kMode><<<NT, kT, 0, h->stream>>>(n, beta, y, incy, lower, sc, sc + rp, max_seg);
+  return launch_status(h);
+}
+
+
+// ---- register-resident off-diagonal pass ----------------------------------------
+// Off-diagonal stored tiles, processed as 32-row strips of a kC-column tile
+// column J by one warp each (lane = row).  A strip's kC column values stay in
+// registers: the row part (A_strip * v_J) is complete per lane; the column
+// part (A_strip^T v_I) is accumulated per lane across every strip the warp
+// handles and reduced across lanes once at the end.  No shared-memory
+// staging, no barrier per tile, kC independent loads in flight per lane.
+template <typename T> struct StripCfg { static constexpr int kC = 64; };
+template <> struct StripCfg<float2> { static constexpr int kC = 32; };
+constexpr int kStripWarps = 4;
+
+template <typename T>
+__device__ __forceinline__ T shfl_xor_t(T v, int o);
+template <> __device__ __forceinline__ float shfl_xor_t<float>(float v, int o) {
+  return __shfl_xor_sync(0xffffffffu, v, o);
+}
+template <> __device__ __forceinline__ float2 shfl_xor_t<float2>(float2 v, int o) {
+  return make_float2(__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o));
+}
+
+template <int W, typename T, int N>
+__device__ __forceinline__ void butterfly(T (&acc)[N], int lane, int o) {
+  const bool up = (lane & o) != 0;
+#pragma unroll
+  for (int c = 0; c < W; ++c) {
+    const T mine = up ? acc[c + W] : acc[c];
+    const T theirs = shfl_xor_t(up ? acc[c] : acc[c + W], o);
+    acc[c] = Cx<T>::add(mine, theirs);
+  }
+}
+
+// Off-diagonal rows of column block J: upper [0, J*kC), lower [(J+1)*kC, n).
+template <typename T, int kMode>
+__global__ void __launch_bounds__(32 * kStripWarps)
+k_tri_strips(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x, size_t incx,
+             T alpha, bool lower, T* __restrict__ rowpart, T* __restrict__ colpart, int nstrip_rows) {
+  constexpr int kC = StripCfg<T>::kC;
+  constexpr bool kSym = kMode == kSymv || kMode == kHemv;
+  constexpr bool kRow = kMode != kTrmvT;
+  constexpr bool kCol = kMode == kSymv || kMode == kHemv || kMode == kTrmvT;
+  __shared__ T vJ[kC];
+  __shared__ T red[kStripWarps][kC];
+  const int J = blockIdx.x;
+  const int c0 = J * kC;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int row_lo = lower ? c0 + kC : 0;
+  const int row_hi = lower ? n : c0;
+  const int nstrip = row_hi > row_lo ? (row_hi - row_lo + 31) / 32 : 0;
+  if (threadIdx.x < kC) {
+    const int gc = c0 + threadIdx.x;
+    T v = gc < n ? x[(size_t)gc * incx] : Cx<T>::zero();
+    vJ[threadIdx.x] = kSym ? scale_x(alpha, v) : v;
+  }
+  __syncthreads();
+  T colacc[kC];
+#pragma unroll
+  for (int c = 0; c < kC; ++c) colacc[c] = Cx<T>::zero();
+  const int step = gridDim.y * kStripWarps;
+  for (int st = blockIdx.y * kStripWarps + warp; st < nstrip; st += step) {
+    const int r = row_lo + st * 32 + lane;
+    const bool rv = r < row_hi;
+    T a[kC];
+    const T* ap = A + r + (size_t)c0 * lda;
+#pragma unroll
+    for (int c = 0; c < kC; ++c) a[c] = (rv && c0 + c < n) ? __ldcs(ap + (size_t)c * lda) : Cx<T>::zero();
+    if (kRow) {
+      T acc = Cx<T>::zero();
+#pragma unroll
+      for (int c = 0; c < kC; ++c) Cx<T>::mac(acc, a[c], vJ[c]);
+      // row strip index within the whole matrix (32-row strips)
+      const int gstrip = (row_lo / 32) + st;
+      if (rv) rowpart[((size_t)gstrip * gridDim.x + J) * 32 + lane] = acc;
+      else rowpart[((size_t)gstrip * gridDim.x + J) * 32 + lane] = Cx<T>::zero();
+    }
+    if (kCol) {
+      T xi = rv ? x[(size_t)r * incx] : Cx<T>::zero();
+      if (kSym) xi = scale_x(alpha, xi);
+#pragma unroll
+      for (int c = 0; c < kC; ++c) Cx<T>::mac(colacc[c], kMode == kHemv ? Cx<T>::conj(a[c]) : a[c], xi);
+    }
+  }
+  if (!kCol) return;
+  // Cross-lane sum of colacc[c] for every c: a butterfly that halves the
+  // values per lane each step (lanes with bit o set keep the upper half).
+  // After the 5 steps, entry j of lane l holds the sum for column
+  // j + (kC / 32) * l.
+  butterfly<kC / 2>(colacc, lane, 16);
+  butterfly<kC / 4>(colacc, lane, 8);
+  butterfly<kC / 8>(colacc, lane, 4);
+  butterfly<kC / 16>(colacc, lane, 2);
+  butterfly<kC / 32>(colacc, lane, 1);
+  int col_of[kC / 32];
+#pragma unroll
+  for (int j = 0; j < kC / 32; ++j) col_of[j] = j + (kC / 32) * lane;
+#pragma unroll
+  for (int j = 0; j < kC / 32; ++j) red[warp][col_of[j]] = colacc[j];
+  __syncthreads();
+  if (threadIdx.x < kC) {
+    T s = red[0][threadIdx.x];
+#pragma unroll
+    for (int w2 = 1; w2 < kStripWarps; ++w2) s = Cx<T>::add(s, red[w2][threadIdx.x]);
+    colpart[((size_t)J * gridDim.y + blockIdx.y) * kC + threadIdx.x] = s;
+  }
+}
+
+// Per 32-row strip: y = beta*y (or 0 for TRMV) + row parts of every
+// off-diagonal column block + the diagonal block's parts + column parts.
+template <typename T, int kMode>
+__global__ void k_strip_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
+                                const T* __restrict__ rowpart, const T* __restrict__ colpart,
+                                int ncolblk, int nsplit, const T* __restrict__ drow,
+                                const T* __restrict__ dcol) {
+  constexpr int kC = StripCfg<T>::kC;
+  constexpr bool kRow = kMode != kTrmvT;
+  constexpr bool kCol = kMode == kSymv || kMode == kHemv || kMode == kTrmvT;
+  const int gr = blockIdx.x * 32 + threadIdx.x;
+  if (gr >= n) return;
+  const int gstrip = blockIdx.x;
+  const int Jr = gr / kC;  // column block containing this row
+  T s = Cx<T>::zero();
+  if (kRow) {
+    // off-diagonal column blocks J whose stored strips cover row gr
+    const int j0 = lower ? 0 : Jr + 1, j1 = lower ? Jr : ncolblk;
+    for (int J = j0; J < j1; ++J) s = Cx<T>::add(s, rowpart[((size_t)gstrip * ncolblk + J) * 32 + threadIdx.x]);
+    s = Cx<T>::add(s, drow[gr]);
+  }
+  if (kCol) {
+    for (int q = 0; q < nsplit; ++q) s = Cx<T>::add(s, colpart[((size_t)Jr * nsplit + q) * kC + gr % kC]);
+    if (kMode == kTrmvT) s = Cx<T>::add(s, dcol[gr]);
+  }
+  T* yp = y + (size_t)gr * incy;
+  if (kMode == kTrmvN || kMode == kTrmvT) *yp = s;
+  else *yp = Cx<T>::add(beta_apply(beta, *yp), s);
+}
+
+template <typename T, int kMode>
+coral_status_t run_tri_strips(Handle* h, int n, const T* A, size_t lda, const T* x, size_t incx,
+                              T alpha, T beta, T* y, size_t incy, bool lower, bool unit) {
+  constexpr int kC = StripCfg<T>::kC;
+  static_assert(kC == kT || kC == kT / 2, "diagonal tiles are kT wide");
+  const int ncol = (n + kC - 1) / kC;
+  const int nstrips = (n + 31) / 32;
+  // CTAs per column block: enough warps to cover the longest column with ~4 strips each
+  int nsplit = (nstrips / kStripWarps + 3) / 4;
+  nsplit = nsplit < 1 ? 1 : (nsplit > 64 ? 64 : nsplit);
+  const size_t rp = (size_t)nstrips * ncol * 32;
+  const size_t cp = (size_t)ncol * nsplit * kC;
+  // diagonal pass on kT-wide tiles: row parts and (TRMV T) column parts per row
+  const int NT = (n + kT - 1) / kT;
+  const size_t dlen = (size_t)NT * kT;
+  T* sc = static_cast<T*>(scratch(h, (rp + cp + 2 * dlen) * sizeof(T)));
+  if (!sc) return CORAL_ERR_ALLOC;
+  T* drow = sc + rp + cp;
+  T* dcol = drow + dlen;
+  if (kC != kT) return CORAL_ERR_NOT_SUPPORTED;
+  timed_begin(h);
+  k_tri_strips<T, kMode><<<dim3(ncol, nsplit), 32 * kStripWarps, 0, h->stream>>>(
+      n, A, lda, x, incx, alpha, lower, sc, sc + rp, nstrips);
+  coral_status_t s = launch_status(h);
+  timed_end(h);
+  if (s != CORAL_OK) return s;
+  k_tri_tiles<T, kMode><<<dim3(NT, 1), kTriThreads, 0, h->stream>>>(n, A, lda, x, incx, alpha, lower,
+                                                                    unit, drow, dcol, 1, 1);
+  if ((s = launch_status(h)) != CORAL_OK) return s;
+  k_strip_combine<T, kMode><<<nstrips, 32, 0, h->stream>>>(n, beta, y, incy, lower, sc, sc + rp, ncol,
+                                                           nsplit, drow, dcol);
   return launch_status(h);
 }
 
@@ -253,8 +423,8 @@ coral_status_t coral_ssymv(coral_handle_t hh, int uplo, size_t n, float alpha, c
   if (!y) return bad_arg(H, 9);
   if (incy == 0) return bad_arg(H, 10);
   if (n > (size_t)(1 << 20)) return CORAL_ERR_NOT_SUPPORTED;
-  return run_tri<float, kSymv>(H, (int)n, matrix, lda, x, incx, alpha, beta, y, incy,
-                               uplo == CORAL_LOWER, false);
+  return run_tri_strips<float, kSymv>(H, (int)n, matrix, lda, x, incx, alpha, beta, y, incy,
+                                      uplo == CORAL_LOWER, false);
 }
 
 coral_status_t coral_chemv(coral_handle_t hh, int uplo, size_t n, const float alpha[2],

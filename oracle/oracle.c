@@ -19,6 +19,7 @@
  * `a += b * c` in Rust is two roundings, and only explicit fmaf()/fma() may
  * fuse.
  */
+#include <immintrin.h>
 #include <math.h>
 #include <stddef.h>
 #include <stdint.h>
@@ -379,7 +380,8 @@ void or_gemm_sample(int dbl, int cplx, int op_a, int op_b, size_t m, size_t n, s
 
 /* level3/sgemm_nn.rs:10-99 with f32_packers.rs (MR x NR = 8 x 12 register
  * tile, MC/NC/KC = 384/576/256 from sgemm.rs:92-94) and the microkernel's
- * rank-1 update order (microkernel/f32_mrxnr.rs:46-95): NN only, fp32. */
+ * rank-1 update order (microkernel/f32_mrxnr.rs:46-95): NN only, fp32, with
+ * the NEON 4-wide FMAs restated as AVX2 8-wide FMAs (the host is x86-64). */
 #define P_MR 8
 #define P_NR 12
 #define P_MC 384
@@ -427,14 +429,35 @@ void port_sgemm_nn(size_t m, size_t n, size_t k, float alpha, const float* a, si
           for (size_t ir = 0; ir < mc; ir += P_MR) {
             size_t mr = mc - ir < P_MR ? mc - ir : P_MR;
             const float* apan = abuf + (ir / P_MR) * P_MR * kc;
+            /* 8 x 12 register tile: the 8 rows of one ymm per column, 12
+             * accumulators, one broadcast FMA per (k, column) -- the x86
+             * counterpart of the NEON vfmaq_laneq rank-1 update
+             * (microkernel/f32_mrxnr.rs:46-95). */
             float acc[P_NR][P_MR];
-            memset(acc, 0, sizeof(acc));
+            __m256 c0 = _mm256_setzero_ps(), c1 = c0, c2 = c0, c3 = c0, c4 = c0, c5 = c0;
+            __m256 c6 = c0, c7 = c0, c8 = c0, c9 = c0, c10 = c0, c11 = c0;
             for (size_t l = 0; l < kc; ++l) {
-              const float* av = apan + l * P_MR;
+              const __m256 av = _mm256_loadu_ps(apan + l * P_MR);
               const float* bv = bpan + l * P_NR;
-              for (int cc = 0; cc < P_NR; ++cc)
-                for (int r = 0; r < P_MR; ++r) acc[cc][r] = fmaf(av[r], bv[cc], acc[cc][r]);
+              c0 = _mm256_fmadd_ps(av, _mm256_broadcast_ss(bv + 0), c0);
+              c1 = _mm256_fmadd_ps(av, _mm256_broadcast_ss(bv + 1), c1);
+              c2 = _mm256_fmadd_ps(av, _mm256_broadcast_ss(bv + 2), c2);
+              c3 = _mm256_fmadd_ps(av, _mm256_broadcast_ss(bv + 3), c3);
+              c4 = _mm256_fmadd_ps(av, _mm256_broadcast_ss(bv + 4), c4);
+              c5 = _mm256_fmadd_ps(av, _mm256_broadcast_ss(bv + 5), c5);
+              c6 = _mm256_fmadd_ps(av, _mm256_broadcast_ss(bv + 6), c6);
+              c7 = _mm256_fmadd_ps(av, _mm256_broadcast_ss(bv + 7), c7);
+              c8 = _mm256_fmadd_ps(av, _mm256_broadcast_ss(bv + 8), c8);
+              c9 = _mm256_fmadd_ps(av, _mm256_broadcast_ss(bv + 9), c9);
+              c10 = _mm256_fmadd_ps(av, _mm256_broadcast_ss(bv + 10), c10);
+              c11 = _mm256_fmadd_ps(av, _mm256_broadcast_ss(bv + 11), c11);
             }
+            _mm256_storeu_ps(acc[0], c0); _mm256_storeu_ps(acc[1], c1);
+            _mm256_storeu_ps(acc[2], c2); _mm256_storeu_ps(acc[3], c3);
+            _mm256_storeu_ps(acc[4], c4); _mm256_storeu_ps(acc[5], c5);
+            _mm256_storeu_ps(acc[6], c6); _mm256_storeu_ps(acc[7], c7);
+            _mm256_storeu_ps(acc[8], c8); _mm256_storeu_ps(acc[9], c9);
+            _mm256_storeu_ps(acc[10], c10); _mm256_storeu_ps(acc[11], c11);
             for (size_t cc = 0; cc < nr; ++cc) {
               float* col = c + (i0 + ir) + (j0 + jr + cc) * ldc;
               for (size_t r = 0; r < mr; ++r) {
