@@ -240,8 +240,10 @@ coral_status_t run_tri(Handle* h, int n, const T* A, size_t lda, const T* x, siz
 // part (A_strip^T v_I) is accumulated per lane across every strip the warp
 // handles and reduced across lanes once at the end.  No shared-memory
 // staging, no barrier per tile, kC independent loads in flight per lane.
-template <typename T> struct StripCfg { static constexpr int kC = 64; };
-template <> struct StripCfg<float2> { static constexpr int kC = 32; };
+// kC columns per tile column (the diagonal tile width); kH columns loaded per
+// pass (complex values take two passes so a strip fits in registers).
+template <typename T> struct StripCfg { static constexpr int kC = 64, kH = 64; };
+template <> struct StripCfg<float2> { static constexpr int kC = 64, kH = 32; };
 constexpr int kStripWarps = 4;
 
 template <typename T>
@@ -269,7 +271,7 @@ template <typename T, int kMode>
 __global__ void __launch_bounds__(32 * kStripWarps)
 k_tri_strips(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x, size_t incx,
              T alpha, bool lower, T* __restrict__ rowpart, T* __restrict__ colpart, int nstrip_rows) {
-  constexpr int kC = StripCfg<T>::kC;
+  constexpr int kC = StripCfg<T>::kC, kH = StripCfg<T>::kH;
   constexpr bool kSym = kMode == kSymv || kMode == kHemv;
   constexpr bool kRow = kMode != kTrmvT;
   constexpr bool kCol = kMode == kSymv || kMode == kHemv || kMode == kTrmvT;
@@ -294,24 +296,33 @@ k_tri_strips(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x
   for (int st = blockIdx.y * kStripWarps + warp; st < nstrip; st += step) {
     const int r = row_lo + st * 32 + lane;
     const bool rv = r < row_hi;
-    T a[kC];
     const T* ap = A + r + (size_t)c0 * lda;
+    T xi = Cx<T>::zero();
+    if (kCol) {
+      xi = rv ? x[(size_t)r * incx] : Cx<T>::zero();
+      if (kSym) xi = scale_x(alpha, xi);
+    }
+    T racc = Cx<T>::zero();
 #pragma unroll
-    for (int c = 0; c < kC; ++c) a[c] = (rv && c0 + c < n) ? __ldcs(ap + (size_t)c * lda) : Cx<T>::zero();
+    for (int h0 = 0; h0 < kC; h0 += kH) {
+      T a[kH];
+#pragma unroll
+      for (int c = 0; c < kH; ++c)
+        a[c] = (rv && c0 + h0 + c < n) ? __ldcs(ap + (size_t)(h0 + c) * lda) : Cx<T>::zero();
+      if (kRow) {
+#pragma unroll
+        for (int c = 0; c < kH; ++c) Cx<T>::mac(racc, a[c], vJ[h0 + c]);
+      }
+      if (kCol) {
+#pragma unroll
+        for (int c = 0; c < kH; ++c)
+          Cx<T>::mac(colacc[h0 + c], kMode == kHemv ? Cx<T>::conj(a[c]) : a[c], xi);
+      }
+    }
     if (kRow) {
-      T acc = Cx<T>::zero();
-#pragma unroll
-      for (int c = 0; c < kC; ++c) Cx<T>::mac(acc, a[c], vJ[c]);
       // row strip index within the whole matrix (32-row strips)
       const int gstrip = (row_lo / 32) + st;
-      if (rv) rowpart[((size_t)gstrip * gridDim.x + J) * 32 + lane] = acc;
-      else rowpart[((size_t)gstrip * gridDim.x + J) * 32 + lane] = Cx<T>::zero();
-    }
-    if (kCol) {
-      T xi = rv ? x[(size_t)r * incx] : Cx<T>::zero();
-      if (kSym) xi = scale_x(alpha, xi);
-#pragma unroll
-      for (int c = 0; c < kC; ++c) Cx<T>::mac(colacc[c], kMode == kHemv ? Cx<T>::conj(a[c]) : a[c], xi);
+      rowpart[((size_t)gstrip * gridDim.x + J) * 32 + lane] = rv ? racc : Cx<T>::zero();
     }
   }
   if (!kCol) return;
@@ -444,7 +455,7 @@ coral_status_t coral_chemv(coral_handle_t hh, int uplo, size_t n, const float al
   if (incy == 0) return bad_arg(H, 10);
   if (((uintptr_t)matrix | (uintptr_t)x | (uintptr_t)y) & 7) return bad_arg(H, 4);
   if (n > (size_t)(1 << 20)) return CORAL_ERR_NOT_SUPPORTED;
-  return run_tri<float2, kHemv>(H, (int)n, reinterpret_cast<const float2*>(matrix), lda,
+  return run_tri_strips<float2, kHemv>(H, (int)n, reinterpret_cast<const float2*>(matrix), lda,
                                 reinterpret_cast<const float2*>(x), incx,
                                 make_float2(alpha[0], alpha[1]), make_float2(beta[0], beta[1]),
                                 reinterpret_cast<float2*>(y), incy, uplo == CORAL_LOWER, false);

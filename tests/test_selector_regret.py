@@ -1,0 +1,53 @@
+"""The trained selector (coral_b200/data/selector.npz) against exhaustive
+autotuning on the 2000 held-out shapes of coral_b200/data/timings_heldout.npz
+(every configuration timed on a B200 by coral_autotune_sgemm).
+
+CPU: predictions from the float64 restatement of the network (oracle);
+GPU: predictions from the library's own forward kernel.  Both must give a
+mean regret <= 5% and beat the default rule (the method without the network).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from coral_b200 import tuning
+from oracle import mlp_ref
+
+DATA = tuning.DATA_DIR
+
+
+def _load():
+    d = np.load(os.path.join(DATA, "timings_heldout.npz"))
+    w = np.load(os.path.join(DATA, "selector.npz"))
+    return d["shapes"], d["times"], w
+
+
+def test_selector_regret_cpu_oracle():
+    shapes, times, w = _load()
+    i, h, o = (int(v) for v in w["shape"])
+    X = tuning.feature_matrix(shapes)
+    y, _ = mlp_ref.forward(w["params"], X, i, h, o)
+    choice = y.reshape(len(shapes), len(tuning.CANDIDATES)).argmin(1)
+    r = tuning.regret(times, choice)
+    dflt = tuning.regret(times, np.array([tuning.default_choice(s) for s in shapes]))
+    assert r.mean() <= 0.05, r.mean()
+    assert r.mean() < 0.5 * dflt.mean(), (r.mean(), dflt.mean())
+
+
+def test_timing_db_is_exhaustive_and_positive():
+    shapes, times, _ = _load()
+    assert times.shape == (len(shapes), len(tuning.CANDIDATES)) and (times > 0).all()
+    train = np.load(os.path.join(DATA, "timings_train.npz"))
+    assert train["times"].shape == (20000, 10)
+    # held-out shapes come from a different seed than the training shapes
+    assert not np.array_equal(train["shapes"][2:12], shapes[2:12])
+
+
+@pytest.mark.gpu
+def test_selector_regret_gpu_kernels(cuda):
+    shapes, times, _ = _load()
+    net = tuning.Mlp.load(os.path.join(DATA, "selector.npz"))
+    choice = tuning.predict_choice(net, shapes)
+    r = tuning.regret(times, choice)
+    assert r.mean() <= 0.05, r.mean()

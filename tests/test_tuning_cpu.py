@@ -1,0 +1,37 @@
+"""Host-side logic of the autotuner/selector (no GPU): shape generation and the
+feature vector the library computes for (shape, configuration)."""
+import numpy as np
+
+from coral_b200 import tuning
+
+
+def test_generate_shapes_seeded_and_special():
+    a = tuning.generate_shapes(100, seed=1)
+    b = tuning.generate_shapes(100, seed=1)
+    np.testing.assert_array_equal(a, b)
+    assert tuple(a[0]) == (65536, 64, 4096, 0, 0)      # tall-skinny
+    assert tuple(a[1]) == (256, 256, 65536, 0, 0)      # split-K heavy
+    dims = a[2:, :3]
+    assert dims.min() >= 32 and dims.max() <= 16384
+    assert set(np.unique(a[:, 3:])) <= {0, 1}
+
+
+def test_features_shape_and_monotone():
+    f = tuning.features((1024, 2048, 4096, 1, 0), 256, 4)
+    assert f.shape == (tuning.N_FEATURES,) and np.isfinite(f).all()
+    np.testing.assert_allclose(f[:3], np.log2([1024, 2048, 4096]) / 16, rtol=1e-6)
+    assert f[3] == 1.0 and f[4] == 0.0
+    assert tuning.features((1024, 2048, 4096, 0, 0), 128, 4)[8] == 0.5
+    # more splits -> more work items -> larger occupancy feature
+    assert tuning.features((256, 256, 65536, 0, 0), 256, 16)[11] > \
+        tuning.features((256, 256, 65536, 0, 0), 256, 1)[11]
+
+
+def test_default_choice_splits_k_for_few_tiles():
+    assert tuning.CANDIDATES[tuning.default_choice((256, 256, 65536, 0, 0))] == (256, 16)
+    assert tuning.CANDIDATES[tuning.default_choice((8192, 8192, 8192, 0, 0))] == (256, 1)
+
+
+def test_regret_definition():
+    t = np.array([[1.0, 2.0], [4.0, 2.0]])
+    np.testing.assert_allclose(tuning.regret(t, np.array([0, 0])), [0.0, 1.0])
