@@ -23,6 +23,10 @@ struct Handle {
   int device = 0;
   int sm_count = kNumSMs;
   cudaStream_t stream = nullptr;
+  // Side stream and events for work that forks from and joins back into
+  // `stream` within one call (created with the handle).
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t fork_event = nullptr, join_event = nullptr;
   int pointer_mode = CORAL_POINTER_HOST;
   int gemm_mode = CORAL_GEMM_NATIVE;
   uint64_t wait_limit = kDefaultWaitLimit;

@@ -66,7 +66,10 @@ static coral_status_t create_handle(Handle** out) {
       cudaMemset(h->words, 0, sizeof(DeviceWords)) != cudaSuccess ||
       cudaMalloc(&h->counters, kCounterPool * sizeof(unsigned)) != cudaSuccess ||
       cudaMemset(h->counters, 0, kCounterPool * sizeof(unsigned)) != cudaSuccess ||
-      cudaMallocHost(&h->host_pinned, 64) != cudaSuccess) {
+      cudaMallocHost(&h->host_pinned, 64) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->fork_event, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->join_event, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
     if (h->words) cudaFree(h->words);
     if (h->counters) cudaFree(h->counters);
@@ -112,6 +115,12 @@ static void destroy_handle(Handle* h) {
   if (h->counters) cudaFree(h->counters);
   if (h->trsv_slots) cudaFree(h->trsv_slots);
   if (h->host_pinned) cudaFreeHost(h->host_pinned);
+  if (h->side_stream) {
+    cudaStreamSynchronize(h->side_stream);
+    cudaStreamDestroy(h->side_stream);
+  }
+  if (h->fork_event) cudaEventDestroy(h->fork_event);
+  if (h->join_event) cudaEventDestroy(h->join_event);
   delete h;
 }
 

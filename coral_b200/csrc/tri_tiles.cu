@@ -1,23 +1,21 @@
 // Level-2 routines that read one triangle of a square matrix: SSYMV, CHEMV
-// and STRMV (N and T), sharing one tile kernel.
+// and STRMV (N and T).  The stored triangle is read from HBM exactly once:
 //
-// The stored triangle is cut into 64 x 64 tiles; every stored tile is read
-// from HBM exactly once (128-bit loads when aligned), staged in shared memory
-// and used for up to two products:
-//   row part    tile * v_J        -> contribution to output rows of tile-row I
-//   column part tile^T * v_I      -> contribution to output rows of tile-row J
-// SYMV/HEMV use both (the unstored triangle is the (conjugate) transpose of
-// the stored one -- reading the triangle once, where CORAL's lda == n fast
-// path walks it column by column, ssymv.rs:144-211, chemv.rs:142-231);
-// TRMV N uses the row part, TRMV T the column part.  Diagonal tiles are
-// completed in shared memory (mirrored for SYMV/HEMV with Re(a_jj) for HEMV,
-// chemv.rs:179-182; masked to the triangle, unit diagonal = 1, for TRMV).
-//
-// A CTA handles a run of up to kSeg tiles of one tile-column J; row parts are
-// written per tile, column parts summed over the run.  A second kernel adds,
-// for each tile-row, its partials in a fixed order and applies beta (SYMV:
-// beta == 0 fills zeros, else multiplies, ssymv.rs:137-141) or writes x
-// (TRMV).  Results are deterministic.
+//   * off-diagonal part -- k_tri_strips: one warp per 32-row strip of a
+//     64-column tile column J, the strip held in registers (lane = row);
+//     it yields a row part (strip * v_J -> output rows of the strip) and a
+//     column part (strip^T v_I, accumulated per lane over the warp's strips,
+//     reduced across lanes once) -> output rows of block J.  SYMV/HEMV use
+//     both, the unstored triangle being the (conjugate) transpose of the
+//     stored one -- where CORAL's lda == n fast path walks the triangle column
+//     by column (ssymv.rs:144-211, chemv.rs:142-231); TRMV N uses the row
+//     part, TRMV T the column part;
+//   * diagonal 64 x 64 blocks -- k_tri_tiles: staged in shared memory and
+//     completed there (mirrored for SYMV/HEMV with Re(a_jj) for HEMV,
+//     chemv.rs:179-182; masked to the triangle, unit diagonal = 1, for TRMV);
+//   * k_strip_combine adds, per 32-row strip, its partials in a fixed order
+//     and applies beta (SYMV/HEMV: beta == 0 fills zeros, else multiplies,
+//     ssymv.rs:137-141) or writes x (TRMV).  Results are deterministic.
 #include "common.cuh"
 
 namespace coral {
@@ -186,64 +184,15 @@ __device__ __forceinline__ float2 beta_apply(float2 beta, float2 y) {
   return make_float2(y.x * beta.x - y.y * beta.y, y.x * beta.y + y.y * beta.x);
 }
 
-// Sums the partials of tile-row t in a fixed order.
-template <typename T, int kMode>
-__global__ void k_tri_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
-                              const T* __restrict__ rowpart, const T* __restrict__ colpart,
-                              int max_seg) {
-  constexpr bool kRow = kMode != kTrmvT;
-  constexpr bool kCol = kMode == kSymv || kMode == kHemv || kMode == kTrmvT;
-  const int NT = (n + kT - 1) / kT;
-  const int t = blockIdx.x, i = threadIdx.x;
-  const int gr = t * kT + i;
-  if (gr >= n) return;
-  T s = Cx<T>::zero();
-  if (kRow) {
-    const int j0 = lower ? 0 : t, j1 = lower ? t : NT - 1;
-    for (int J = j0; J <= j1; ++J) s = Cx<T>::add(s, rowpart[tri_index(t, J, lower) * kT + i]);
-  }
-  if (kCol) {
-    const int count = lower ? NT - t : t + 1;
-    const int nseg = (count + kSeg - 1) / kSeg;
-    for (int g = 0; g < nseg; ++g) s = Cx<T>::add(s, colpart[((size_t)t * max_seg + g) * kT + i]);
-  }
-  T* yp = y + (size_t)gr * incy;
-  if (kMode == kTrmvN || kMode == kTrmvT) *yp = s;
-  else *yp = Cx<T>::add(beta_apply(beta, *yp), s);
-}
-
-template <typename T, int kMode>
-coral_status_t run_tri(Handle* h, int n, const T* A, size_t lda, const T* x, size_t incx, T alpha,
-                       T beta, T* y, size_t incy, bool lower, bool unit) {
-  const int NT = (n + kT - 1) / kT;
-  const int max_seg = (NT + kSeg - 1) / kSeg;
-  const size_t rp = (size_t)NT * (NT + 1) / 2 * kT;
-  const size_t cp = (size_t)NT * max_seg * kT;
-  T* sc = static_cast<T*>(scratch(h, (rp + cp) * sizeof(T)));
-  if (!sc) return CORAL_ERR_ALLOC;
-  dim3 grid(NT, max_seg);
-  timed_begin(h);
-  k_tri_tiles<T, kMode><<<grid, kTriThreads, 0, h->stream>>>(n, A, lda, x, incx, alpha, lower, unit,
-                                                             sc, sc + rp, max_seg, 0);
-  coral_status_t s = launch_status(h);
-  timed_end(h);
-  if (s != CORAL_OK) return s;
-  k_tri_combine<T, kMode><<<NT, kT, 0, h->stream>>>(n, beta, y, incy, lower, sc, sc + rp, max_seg);
-  return launch_status(h);
-}
-
-
 // ---- register-resident off-diagonal pass ----------------------------------------
-// Off-diagonal stored tiles, processed as 32-row strips of a kC-column tile
-// column J by one warp each (lane = row).  A strip's kC column values stay in
-// registers: the row part (A_strip * v_J) is complete per lane; the column
-// part (A_strip^T v_I) is accumulated per lane across every strip the warp
-// handles and reduced across lanes once at the end.  No shared-memory
-// staging, no barrier per tile, kC independent loads in flight per lane.
-// kC columns per tile column (the diagonal tile width); kH columns loaded per
-// pass (complex values take two passes so a strip fits in registers).
-template <typename T> struct StripCfg { static constexpr int kC = 64, kH = 64; };
-template <> struct StripCfg<float2> { static constexpr int kC = 64, kH = 32; };
+// kC = 64 columns per tile column (the diagonal tile width).  A warp owns a
+// strip of 32*V rows: each lane V consecutive rows, loaded as one 16-byte
+// vector per column (V = 4 floats or 2 complex; V = 1 when lda or the base
+// are not 16-byte aligned), so a warp load covers a 512-byte contiguous
+// segment of a column.  Columns are taken kP per pass to bound registers.
+// Strips sit on a global grid of 32*V-row strips; rows outside this column
+// block's stored off-diagonal range [row_lo, row_hi) are masked out.
+constexpr int kC = 64;
 constexpr int kStripWarps = 4;
 
 template <typename T>
@@ -266,12 +215,22 @@ __device__ __forceinline__ void butterfly(T (&acc)[N], int lane, int o) {
   }
 }
 
-// Off-diagonal rows of column block J: upper [0, J*kC), lower [(J+1)*kC, n).
-template <typename T, int kMode>
-__global__ void __launch_bounds__(32 * kStripWarps)
+template <typename T, int V> struct Vec;
+template <> struct Vec<float, 4> {
+  using type = float4;
+  static __device__ __forceinline__ void split(const float4& v, float (&o)[4]) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; }
+};
+template <> struct Vec<float2, 2> {
+  using type = float4;
+  static __device__ __forceinline__ void split(const float4& v, float2 (&o)[2]) { o[0] = make_float2(v.x, v.y); o[1] = make_float2(v.z, v.w); }
+};
+
+template <typename T, int kMode, int V>
+__global__ void __launch_bounds__(32 * kStripWarps, 4)
 k_tri_strips(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x, size_t incx,
-             T alpha, bool lower, T* __restrict__ rowpart, T* __restrict__ colpart, int nstrip_rows) {
-  constexpr int kC = StripCfg<T>::kC, kH = StripCfg<T>::kH;
+             T alpha, bool lower, T* __restrict__ rowpart, T* __restrict__ colpart, int nsplit) {
+  constexpr int kS = 32 * V;                 // strip height
+  constexpr int kP = 16;                     // columns per pass
   constexpr bool kSym = kMode == kSymv || kMode == kHemv;
   constexpr bool kRow = kMode != kTrmvT;
   constexpr bool kCol = kMode == kSymv || kMode == kHemv || kMode == kTrmvT;
@@ -282,135 +241,197 @@ k_tri_strips(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int row_lo = lower ? c0 + kC : 0;
   const int row_hi = lower ? n : c0;
-  const int nstrip = row_hi > row_lo ? (row_hi - row_lo + 31) / 32 : 0;
+  const int s_lo = row_lo / kS;
+  const int s_hi = row_hi > row_lo ? (row_hi + kS - 1) / kS : s_lo;
   if (threadIdx.x < kC) {
     const int gc = c0 + threadIdx.x;
     T v = gc < n ? x[(size_t)gc * incx] : Cx<T>::zero();
     vJ[threadIdx.x] = kSym ? scale_x(alpha, v) : v;
   }
+  for (int i = threadIdx.x; i < kStripWarps * kC; i += blockDim.x) (&red[0][0])[i] = Cx<T>::zero();
   __syncthreads();
-  T colacc[kC];
+  // One strip per warp (the grid has enough warps for the longest column).
+  const int gs = s_lo + blockIdx.y * kStripWarps + warp;
+  if (gs < s_hi) {
+    const int r0 = gs * kS + lane * V;      // first row of this lane
+    bool rv[V];
+    T xi[V];
 #pragma unroll
-  for (int c = 0; c < kC; ++c) colacc[c] = Cx<T>::zero();
-  const int step = gridDim.y * kStripWarps;
-  for (int st = blockIdx.y * kStripWarps + warp; st < nstrip; st += step) {
-    const int r = row_lo + st * 32 + lane;
-    const bool rv = r < row_hi;
-    const T* ap = A + r + (size_t)c0 * lda;
-    T xi = Cx<T>::zero();
-    if (kCol) {
-      xi = rv ? x[(size_t)r * incx] : Cx<T>::zero();
-      if (kSym) xi = scale_x(alpha, xi);
+    for (int e = 0; e < V; ++e) {
+      const int r = r0 + e;
+      rv[e] = r >= row_lo && r < row_hi;
+      xi[e] = Cx<T>::zero();
+      if (kCol && rv[e]) {
+        xi[e] = x[(size_t)r * incx];
+        if (kSym) xi[e] = scale_x(alpha, xi[e]);
+      }
     }
-    T racc = Cx<T>::zero();
+    const bool all_in = V > 1 && rv[0] && rv[V - 1];
+    T racc[V];
 #pragma unroll
-    for (int h0 = 0; h0 < kC; h0 += kH) {
-      T a[kH];
+    for (int e = 0; e < V; ++e) racc[e] = Cx<T>::zero();
+#pragma unroll 1
+    for (int h0 = 0; h0 < kC; h0 += kP) {
+      T a[kP][V];
+      const T* base = A + r0 + (size_t)(c0 + h0) * lda;
+      if constexpr (V > 1) {
+        using VT = typename Vec<T, V>::type;
+        if (all_in) {
+          VT raw[kP];
 #pragma unroll
-      for (int c = 0; c < kH; ++c)
-        a[c] = (rv && c0 + h0 + c < n) ? __ldcs(ap + (size_t)(h0 + c) * lda) : Cx<T>::zero();
+          for (int c = 0; c < kP; ++c)
+            raw[c] = (c0 + h0 + c < n) ? __ldcs(reinterpret_cast<const VT*>(base + (size_t)c * lda)) : VT{};
+#pragma unroll
+          for (int c = 0; c < kP; ++c) Vec<T, V>::split(raw[c], a[c]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < kP; ++c)
+#pragma unroll
+            for (int e = 0; e < V; ++e)
+              a[c][e] = (rv[e] && c0 + h0 + c < n) ? __ldcs(base + (size_t)c * lda + e) : Cx<T>::zero();
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < kP; ++c)
+          a[c][0] = (rv[0] && c0 + h0 + c < n) ? __ldcs(base + (size_t)c * lda) : Cx<T>::zero();
+      }
       if (kRow) {
 #pragma unroll
-        for (int c = 0; c < kH; ++c) Cx<T>::mac(racc, a[c], vJ[h0 + c]);
+        for (int c = 0; c < kP; ++c)
+#pragma unroll
+          for (int e = 0; e < V; ++e) Cx<T>::mac(racc[e], a[c][e], vJ[h0 + c]);
       }
       if (kCol) {
+        // per-lane column partials of this pass, reduced across the warp now:
+        // butterfly 16 -> 1 values per lane, then a final pairwise add; lane l
+        // (even) ends with the sum for column h0 + (l >> 1).
+        T v[kP];
 #pragma unroll
-        for (int c = 0; c < kH; ++c)
-          Cx<T>::mac(colacc[h0 + c], kMode == kHemv ? Cx<T>::conj(a[c]) : a[c], xi);
+        for (int c = 0; c < kP; ++c) {
+          v[c] = Cx<T>::zero();
+#pragma unroll
+          for (int e = 0; e < V; ++e) Cx<T>::mac(v[c], kMode == kHemv ? Cx<T>::conj(a[c][e]) : a[c][e], xi[e]);
+        }
+        butterfly<8>(v, lane, 16);
+        butterfly<4>(v, lane, 8);
+        butterfly<2>(v, lane, 4);
+        butterfly<1>(v, lane, 2);
+        const T tot = Cx<T>::add(v[0], shfl_xor_t(v[0], 1));
+        if ((lane & 1) == 0) red[warp][h0 + (lane >> 1)] = tot;
       }
     }
     if (kRow) {
-      // row strip index within the whole matrix (32-row strips)
-      const int gstrip = (row_lo / 32) + st;
-      rowpart[((size_t)gstrip * gridDim.x + J) * 32 + lane] = rv ? racc : Cx<T>::zero();
+      T* rp = rowpart + ((size_t)gs * gridDim.x + J) * kS + lane * V;
+#pragma unroll
+      for (int e = 0; e < V; ++e) rp[e] = rv[e] ? racc[e] : Cx<T>::zero();
     }
   }
   if (!kCol) return;
-  // Cross-lane sum of colacc[c] for every c: a butterfly that halves the
-  // values per lane each step (lanes with bit o set keep the upper half).
-  // After the 5 steps, entry j of lane l holds the sum for column
-  // j + (kC / 32) * l.
-  butterfly<kC / 2>(colacc, lane, 16);
-  butterfly<kC / 4>(colacc, lane, 8);
-  butterfly<kC / 8>(colacc, lane, 4);
-  butterfly<kC / 16>(colacc, lane, 2);
-  butterfly<kC / 32>(colacc, lane, 1);
-  int col_of[kC / 32];
-#pragma unroll
-  for (int j = 0; j < kC / 32; ++j) col_of[j] = j + (kC / 32) * lane;
-#pragma unroll
-  for (int j = 0; j < kC / 32; ++j) red[warp][col_of[j]] = colacc[j];
   __syncthreads();
   if (threadIdx.x < kC) {
     T s = red[0][threadIdx.x];
 #pragma unroll
     for (int w2 = 1; w2 < kStripWarps; ++w2) s = Cx<T>::add(s, red[w2][threadIdx.x]);
-    colpart[((size_t)J * gridDim.y + blockIdx.y) * kC + threadIdx.x] = s;
+    colpart[((size_t)J * nsplit + blockIdx.y) * kC + threadIdx.x] = s;
   }
 }
 
-// Per 32-row strip: y = beta*y (or 0 for TRMV) + row parts of every
+// Per 32 output rows: y = beta*y (or 0 for TRMV) + row parts of every
 // off-diagonal column block + the diagonal block's parts + column parts.
-template <typename T, int kMode>
-__global__ void k_strip_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
-                                const T* __restrict__ rowpart, const T* __restrict__ colpart,
-                                int ncolblk, int nsplit, const T* __restrict__ drow,
-                                const T* __restrict__ dcol) {
-  constexpr int kC = StripCfg<T>::kC;
+// 8 groups of 32 threads (lane = row) split the column blocks, 4 loads in
+// flight each, then a fixed-order shared-memory sum.
+constexpr int kCombineGroups = 8;
+template <typename T, int kMode, int V>
+__global__ void __launch_bounds__(32 * kCombineGroups)
+k_strip_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
+                const T* __restrict__ rowpart, const T* __restrict__ colpart, int ncolblk,
+                int nsplit, const T* __restrict__ drow, const T* __restrict__ dcol) {
+  constexpr int kS = 32 * V;
   constexpr bool kRow = kMode != kTrmvT;
   constexpr bool kCol = kMode == kSymv || kMode == kHemv || kMode == kTrmvT;
-  const int gr = blockIdx.x * 32 + threadIdx.x;
-  if (gr >= n) return;
-  const int gstrip = blockIdx.x;
-  const int Jr = gr / kC;  // column block containing this row
+  __shared__ T part[kCombineGroups][32];
+  const int g = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gr = blockIdx.x * 32 + lane;
+  const int gs = gr / kS, li = gr % kS;   // strip and row within it
+  const int Jr = min(gr, n - 1) / kC;
   T s = Cx<T>::zero();
   if (kRow) {
-    // off-diagonal column blocks J whose stored strips cover row gr
+    // off-diagonal column blocks whose stored range covers row gr
     const int j0 = lower ? 0 : Jr + 1, j1 = lower ? Jr : ncolblk;
-    for (int J = j0; J < j1; ++J) s = Cx<T>::add(s, rowpart[((size_t)gstrip * ncolblk + J) * 32 + threadIdx.x]);
-    s = Cx<T>::add(s, drow[gr]);
+    const T* rp = rowpart + (size_t)gs * ncolblk * kS + li;
+    int J = j0 + g;
+    for (; J + 3 * kCombineGroups < j1; J += 4 * kCombineGroups) {
+      const T a0 = __ldcs(rp + (size_t)J * kS), a1 = __ldcs(rp + (size_t)(J + kCombineGroups) * kS);
+      const T a2 = __ldcs(rp + (size_t)(J + 2 * kCombineGroups) * kS);
+      const T a3 = __ldcs(rp + (size_t)(J + 3 * kCombineGroups) * kS);
+      s = Cx<T>::add(s, Cx<T>::add(Cx<T>::add(a0, a1), Cx<T>::add(a2, a3)));
+    }
+    for (; J < j1; J += kCombineGroups) s = Cx<T>::add(s, __ldcs(rp + (size_t)J * kS));
   }
   if (kCol) {
-    for (int q = 0; q < nsplit; ++q) s = Cx<T>::add(s, colpart[((size_t)Jr * nsplit + q) * kC + gr % kC]);
-    if (kMode == kTrmvT) s = Cx<T>::add(s, dcol[gr]);
+    for (int q = g; q < nsplit; q += kCombineGroups)
+      s = Cx<T>::add(s, colpart[((size_t)Jr * nsplit + q) * kC + gr % kC]);
   }
+  part[g][lane] = s;
+  __syncthreads();
+  if (g != 0 || gr >= n) return;
+  T t = part[0][lane];
+#pragma unroll
+  for (int q = 1; q < kCombineGroups; ++q) t = Cx<T>::add(t, part[q][lane]);
+  if (kRow) t = Cx<T>::add(t, drow[gr]);
+  if (kMode == kTrmvT) t = Cx<T>::add(t, dcol[gr]);
   T* yp = y + (size_t)gr * incy;
-  if (kMode == kTrmvN || kMode == kTrmvT) *yp = s;
-  else *yp = Cx<T>::add(beta_apply(beta, *yp), s);
+  if (kMode == kTrmvN || kMode == kTrmvT) *yp = t;
+  else *yp = Cx<T>::add(beta_apply(beta, *yp), t);
 }
 
-template <typename T, int kMode>
-coral_status_t run_tri_strips(Handle* h, int n, const T* A, size_t lda, const T* x, size_t incx,
-                              T alpha, T beta, T* y, size_t incy, bool lower, bool unit) {
-  constexpr int kC = StripCfg<T>::kC;
-  static_assert(kC == kT || kC == kT / 2, "diagonal tiles are kT wide");
+template <typename T, int kMode, int V>
+coral_status_t launch_strips(Handle* h, int n, const T* A, size_t lda, const T* x, size_t incx,
+                             T alpha, T beta, T* y, size_t incy, bool lower, bool unit) {
+  constexpr int kS = 32 * V;
   const int ncol = (n + kC - 1) / kC;
-  const int nstrips = (n + 31) / 32;
-  // CTAs per column block: enough warps to cover the longest column with ~4 strips each
-  int nsplit = (nstrips / kStripWarps + 3) / 4;
-  nsplit = nsplit < 1 ? 1 : (nsplit > 64 ? 64 : nsplit);
-  const size_t rp = (size_t)nstrips * ncol * 32;
+  const int nstrips = (n + kS - 1) / kS;
+  // CTAs per column block: one strip per warp in the longest column, so no
+  // warp streams more than one strip (CTAs past a short column's end exit)
+  int nsplit = (nstrips + kStripWarps - 1) / kStripWarps;
+  nsplit = nsplit < 1 ? 1 : (nsplit > 256 ? 256 : nsplit);
+  const size_t rp = (size_t)nstrips * ncol * kS;
   const size_t cp = (size_t)ncol * nsplit * kC;
-  // diagonal pass on kT-wide tiles: row parts and (TRMV T) column parts per row
-  const int NT = (n + kT - 1) / kT;
+  const int NT = (n + kT - 1) / kT;  // diagonal tiles (kT == kC)
   const size_t dlen = (size_t)NT * kT;
   T* sc = static_cast<T*>(scratch(h, (rp + cp + 2 * dlen) * sizeof(T)));
   if (!sc) return CORAL_ERR_ALLOC;
   T* drow = sc + rp + cp;
   T* dcol = drow + dlen;
-  if (kC != kT) return CORAL_ERR_NOT_SUPPORTED;
-  timed_begin(h);
-  k_tri_strips<T, kMode><<<dim3(ncol, nsplit), 32 * kStripWarps, 0, h->stream>>>(
-      n, A, lda, x, incx, alpha, lower, sc, sc + rp, nstrips);
+  // The diagonal tiles are independent of the strips: run them on the
+  // handle's side stream, forked from and joined back into the main stream.
+  CORAL_CUDA(h, cudaEventRecord(h->fork_event, h->stream));
+  CORAL_CUDA(h, cudaStreamWaitEvent(h->side_stream, h->fork_event, 0));
+  k_tri_tiles<T, kMode><<<dim3(NT, 1), kTriThreads, 0, h->side_stream>>>(n, A, lda, x, incx, alpha,
+                                                                         lower, unit, drow, dcol, 1, 1);
   coral_status_t s = launch_status(h);
+  if (s != CORAL_OK) return s;
+  CORAL_CUDA(h, cudaEventRecord(h->join_event, h->side_stream));
+  timed_begin(h);
+  k_tri_strips<T, kMode, V><<<dim3(ncol, nsplit), 32 * kStripWarps, 0, h->stream>>>(
+      n, A, lda, x, incx, alpha, lower, sc, sc + rp, nsplit);
+  s = launch_status(h);
   timed_end(h);
   if (s != CORAL_OK) return s;
-  k_tri_tiles<T, kMode><<<dim3(NT, 1), kTriThreads, 0, h->stream>>>(n, A, lda, x, incx, alpha, lower,
-                                                                    unit, drow, dcol, 1, 1);
-  if ((s = launch_status(h)) != CORAL_OK) return s;
-  k_strip_combine<T, kMode><<<nstrips, 32, 0, h->stream>>>(n, beta, y, incy, lower, sc, sc + rp, ncol,
-                                                           nsplit, drow, dcol);
+  CORAL_CUDA(h, cudaStreamWaitEvent(h->stream, h->join_event, 0));
+  k_strip_combine<T, kMode, V><<<(n + 31) / 32, 32 * kCombineGroups, 0, h->stream>>>(
+      n, beta, y, incy, lower, sc, sc + rp, ncol, nsplit, drow, dcol);
   return launch_status(h);
+}
+
+template <typename T, int kMode>
+coral_status_t run_tri_strips(Handle* h, int n, const T* A, size_t lda, const T* x, size_t incx,
+                              T alpha, T beta, T* y, size_t incy, bool lower, bool unit) {
+  static_assert(kC == kT, "diagonal tiles are as wide as the tile columns");
+  constexpr int V = sizeof(T) == 4 ? 4 : 2;
+  const bool vec = aligned16(A) && (lda * sizeof(T)) % 16 == 0;
+  if (vec) return launch_strips<T, kMode, V>(h, n, A, lda, x, incx, alpha, beta, y, incy, lower, unit);
+  return launch_strips<T, kMode, 1>(h, n, A, lda, x, incx, alpha, beta, y, incy, lower, unit);
 }
 
 }  // namespace
@@ -475,8 +496,8 @@ coral_status_t coral_strmv(coral_handle_t hh, int uplo, int trans, int diag, siz
   if (n > (size_t)(1 << 20)) return CORAL_ERR_NOT_SUPPORTED;
   const bool lower = uplo == CORAL_LOWER, unit = diag == CORAL_UNIT;
   if (trans == CORAL_NO_TRANSPOSE)
-    return run_tri<float, kTrmvN>(H, (int)n, matrix, lda, x, incx, 1.f, 0.f, x, incx, lower, unit);
-  return run_tri<float, kTrmvT>(H, (int)n, matrix, lda, x, incx, 1.f, 0.f, x, incx, lower, unit);
+    return run_tri_strips<float, kTrmvN>(H, (int)n, matrix, lda, x, incx, 1.f, 0.f, x, incx, lower, unit);
+  return run_tri_strips<float, kTrmvT>(H, (int)n, matrix, lda, x, incx, 1.f, 0.f, x, incx, lower, unit);
 }
 
 }  // extern "C"
