@@ -50,11 +50,9 @@ struct Handle {
   // Zeroed pool of per-tile arrival counters for single-launch multi-block
   // combines; every kernel returns the counters it used to zero.
   unsigned* counters = nullptr;
-  // TRSV: ready flags hold the epoch of the call that set them (never reset);
-  // tickets are handed out from a running counter starting at trsv_tickets.
-  unsigned trsv_epoch = 0;
-  unsigned long long trsv_tickets = 0;
-  // Epoch-tagged solution slots ((epoch << 32) | float bits), zeroed when
+  // TRSV block size (64 or 128 rows; 0 = by size)
+  int trsv_block = 0;
+  // TRSV epoch-tagged solution slots ((epoch << 32) | float bits), zeroed when
   // (re)allocated so stale memory never carries a live epoch.
   unsigned long long* trsv_slots = nullptr;
   size_t trsv_slots_len = 0;
@@ -82,8 +80,11 @@ struct DeviceWords {
   unsigned counters[30];           // arrival counters of single-launch reductions
   double dresult[4];               // scalar results (device pointer mode staging)
   unsigned long long uresult[4];
-  unsigned long long trsv_ticket;  // running ticket counter of the TRSV kernel
-  unsigned char reserved[1024 - 4 * 32 - 64 - 8];
+  unsigned trsv_ticket;   // TRSV: tickets handed out in the current call
+  unsigned trsv_done;     // TRSV: CTAs finished in the current call
+  unsigned trsv_epoch;    // TRSV: epoch of the last completed call
+  unsigned pad1;
+  unsigned char reserved[1024 - 4 * 32 - 64 - 16];
 };
 static_assert(sizeof(DeviceWords) == 1024, "DeviceWords layout");
 

@@ -1,25 +1,26 @@
 // STRSV: solve op(A) x = b in place, A triangular (strsv.rs:60-74 ->
 // strlsv.rs / strusv.rs).  ConjugateTranspose == Transpose.
 //
-// One launch.  op(A) is cut into 64-row blocks; each CTA takes a ticket from a
-// running counter, so block b is handled by the b-th CTA to start (in solve
+// One launch.  op(A) is cut into NB-row blocks (NB = 64, or 128 for large n or
+// when the handle asks for it); each CTA takes a ticket from a
+// per-call counter, so block b is handled by the b-th CTA to start (in solve
 // order: forward when op(A) is lower, backward when upper) and only ever
 // waits for blocks whose CTAs started earlier -- no dependency on scheduling
 // order, no deadlock.  A CTA
 //   1. stages its diagonal block of op(A) (triangle masked, unit diagonal
 //      applied) in shared memory and inverts it (independent of every other
 //      block, so it overlaps the solve of earlier blocks);
-//   2. streams its row panel of op(A), 4 tiles of 64 x 64 in flight, and
+//   2. streams its row panel of op(A), 256 KB of tiles in flight, and
 //      for each tile waits for the solution x_k of that block, then
 //      accumulates tile * x_k -- tiles of early blocks are ready long before
 //      the last one, so the panel streams while the solve front advances;
 //   3. forms x_b = inv(D_b) (b_b - acc), writes it over b, and publishes it
-//      as 64 epoch-tagged 64-bit slots ((epoch << 32) | float bits, store
+//      as NB epoch-tagged 64-bit slots ((epoch << 32) | float bits, store
 //      release).  A consumer polls the slots themselves: one round trip
 //      through L2 both signals readiness and delivers the values.
 // CORAL solves its diagonal blocks by substitution (strlsv.rs:66-140) with the
 // panel update through saxpyf/sdotf; here the blocked diagonal solve uses the
-// inverted 64 x 64 block as a small GEMV, which takes the serial substitution
+// inverted NB x NB block as a small GEMV, which takes the serial substitution
 // off the critical path.  Waits are bounded by the handle's wait limit and
 // abort early once any CTA has set the status word.
 #include "common.cuh"
@@ -27,10 +28,13 @@
 namespace coral {
 namespace {
 
-constexpr int kNB = 64;
-constexpr int kG = 4;          // panel tiles loaded per group
-constexpr int kTrsvThreads = 256;
-constexpr int kPer = kNB * kNB / kTrsvThreads;  // tile elements per thread (16)
+// Block size NB (64 or 128 rows); 4 threads per row.
+template <int NB> struct TrsvCfg {
+  static constexpr int kThreads = 4 * NB;
+  static constexpr int kPer = NB * NB / kThreads;  // tile elements per thread
+  static constexpr int kG = NB == 64 ? 4 : 2;     // panel tiles loaded per group
+  static constexpr int kQ = 4;                    // thread groups per row
+};
 
 __device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
   unsigned long long v;
@@ -46,32 +50,37 @@ __device__ __forceinline__ uint64_t gtimer() {
   return t;
 }
 
-__global__ void __launch_bounds__(kTrsvThreads)
+template <int kNB>
+__global__ void __launch_bounds__(4 * kNB, 1)
 k_trsv(int n, const float* __restrict__ A, size_t lda, float* x, size_t incx, bool lower_eff,
-       bool trans, bool unit, unsigned long long* slots, unsigned long long* ticket,
-       unsigned long long ticket_base, unsigned epoch, unsigned* status, uint64_t limit_ns) {
-  __shared__ float D[kNB][kNB + 1];    // D[r][c] = op(A)(r, c) of the diagonal block, then inv
-  __shared__ float T[kNB][kNB + 1];    // T[c][r] = stored block element (row r, col c)
+       bool trans, bool unit, unsigned long long* slots, unsigned* ticket, unsigned* done,
+       unsigned* epoch_word, unsigned* status, uint64_t limit_ns) {
+  constexpr int kTrsvThreads = TrsvCfg<kNB>::kThreads, kPer = TrsvCfg<kNB>::kPer;
+  constexpr int kG = TrsvCfg<kNB>::kG, kQ = TrsvCfg<kNB>::kQ;
+  extern __shared__ float smem_f[];
+  float (*D)[kNB + 1] = reinterpret_cast<float (*)[kNB + 1]>(smem_f);               // op(A) block, then inverse
+  float (*T)[kNB + 1] = reinterpret_cast<float (*)[kNB + 1]>(smem_f + kNB * (kNB + 1));  // panel tile / scratch
   __shared__ float xk[kNB];
-  __shared__ float red[4][kNB];
+  __shared__ float red[kQ][kNB];
   __shared__ float rhs[kNB];
   __shared__ int sblk;
   __shared__ int abort_flag;
 
   const int nblk = (n + kNB - 1) / kNB;
   const int tid = threadIdx.x;
+  __shared__ unsigned sepoch;
   if (tid == 0) {
-    unsigned long long t = atomicAdd(ticket, 1ull) - ticket_base;
+    // Tickets start at 0 in every call (the last CTA resets the counter);
+    // the call's epoch is one past the last completed call's, read before
+    // any CTA of this call can finish and advance it.
+    const unsigned t = atomicAdd(ticket, 1u);
+    sepoch = *(volatile unsigned*)epoch_word + 1u;
+    if (sepoch == 0u) sepoch = 1u;  // slots start at 0: never a live epoch
     abort_flag = 0;
-    if (t >= (unsigned long long)nblk) {  // ticket count out of step with the host
-      atomicOr(status, kStatusTimeout);
-      abort_flag = 1;
-      t = 0;
-    }
     sblk = lower_eff ? (int)t : nblk - 1 - (int)t;
   }
   __syncthreads();
-  if (abort_flag) return;
+  const unsigned epoch = sepoch;
   const int blk = sblk;
   const int b0 = blk * kNB;
 
@@ -80,39 +89,50 @@ k_trsv(int n, const float* __restrict__ A, size_t lda, float* x, size_t incx, bo
     const int rr = e % kNB, cc = e / kNB;       // stored element (b0+rr, b0+cc)
     const int gr = b0 + rr, gc = b0 + cc;
     float v = (gr < n && gc < n) ? __ldg(A + gr + (size_t)gc * lda) : 0.f;
-    // op(A)(r, c): stored (rr, cc) is op element (rr, cc) or (cc, rr).
-    const int r = trans ? cc : rr, c = trans ? rr : cc;
+    const int r = trans ? cc : rr, c = trans ? rr : cc;   // op(A)(r, c)
     const bool in_tri = lower_eff ? r >= c : r <= c;
     if (r == c) v = (unit || b0 + r >= n) ? 1.f : v;
     else if (!in_tri) v = 0.f;
     D[r][c] = v;
   }
   __syncthreads();
-  if (tid < kNB) {
-    // Column `c` of inv(D) by substitution on the unit vector e_c, kept in
-    // T[c][*] (T is free until the panel phase).
-    const int c = tid;
+  {
+    // Column c of inv(D) by substitution on e_c, 4 lanes per column (the 4
+    // share a warp and split each dot product); result kept in T[c][*].  A
+    // warp holds columns [8w, 8w + 8): every lane runs the warp's full
+    // iteration range so the full-mask shuffles always have all 32 lanes.
+    const int c = tid >> 2, part = tid & 3;
+    const int cw0 = (tid >> 5) * 8, cw1 = cw0 + 7;
     if (lower_eff) {
-      for (int i = 0; i < c; ++i) T[c][i] = 0.f;
-      T[c][c] = 1.f / D[c][c];
-      for (int i = c + 1; i < kNB; ++i) {
+      for (int i = part; i < c; i += 4) T[c][i] = 0.f;
+      if (part == 0) T[c][c] = 1.f / D[c][c];
+      __syncwarp();
+      for (int i = cw0 + 1; i < kNB; ++i) {
         float s = 0.f;
-        for (int j = c; j < i; ++j) s = fmaf(D[i][j], T[c][j], s);
-        T[c][i] = -s / D[i][i];
+        if (i > c)
+          for (int j = c + part; j < i; j += 4) s = fmaf(D[i][j], T[c][j], s);
+        s += __shfl_xor_sync(0xffffffffu, s, 1);
+        s += __shfl_xor_sync(0xffffffffu, s, 2);
+        if (i > c && part == 0) T[c][i] = -s / D[i][i];
+        __syncwarp();
       }
     } else {
-      for (int i = c + 1; i < kNB; ++i) T[c][i] = 0.f;
-      T[c][c] = 1.f / D[c][c];
-      for (int i = c - 1; i >= 0; --i) {
+      for (int i = c + 1 + part; i < kNB; i += 4) T[c][i] = 0.f;
+      if (part == 0) T[c][c] = 1.f / D[c][c];
+      __syncwarp();
+      for (int i = cw1 - 1; i >= 0; --i) {
         float s = 0.f;
-        for (int j = i + 1; j <= c; ++j) s = fmaf(D[i][j], T[c][j], s);
-        T[c][i] = -s / D[i][i];
+        if (i < c)
+          for (int j = i + 1 + part; j <= c; j += 4) s = fmaf(D[i][j], T[c][j], s);
+        s += __shfl_xor_sync(0xffffffffu, s, 1);
+        s += __shfl_xor_sync(0xffffffffu, s, 2);
+        if (i < c && part == 0) T[c][i] = -s / D[i][i];
+        __syncwarp();
       }
     }
   }
   __syncthreads();
-  // D <- inv(D) (D[r][c] = inv(r, c) = T[c][r])
-  for (int e = tid; e < kNB * kNB; e += kTrsvThreads) {
+  for (int e = tid; e < kNB * kNB; e += kTrsvThreads) {  // D <- inv(D)
     const int r = e % kNB, c = e / kNB;
     D[r][c] = T[c][r];
   }
@@ -167,18 +187,21 @@ k_trsv(int n, const float* __restrict__ A, size_t lda, float* x, size_t incx, bo
         xk[tid] = __uint_as_float((unsigned)v);
       }
       __syncthreads();
-      if (abort_flag) return;
+      if (abort_flag) break;
       // op(A)(r, c) = stored(r, c) = T[c][r], or stored(c, r) = T[r][c] when transposed
+      const int cq = q * (kNB / kQ);
       if (!trans) {
-#pragma unroll
-        for (int c = q * 16; c < q * 16 + 16; ++c) acc = fmaf(T[c][r], xk[c], acc);
+#pragma unroll 8
+        for (int c = cq; c < cq + kNB / kQ; ++c) acc = fmaf(T[c][r], xk[c], acc);
       } else {
-#pragma unroll
-        for (int c = q * 16; c < q * 16 + 16; ++c) acc = fmaf(T[r][c], xk[c], acc);
+#pragma unroll 8
+        for (int c = cq; c < cq + kNB / kQ; ++c) acc = fmaf(T[r][c], xk[c], acc);
       }
       __syncthreads();
     }
+    if (abort_flag) break;
   }
+  if (!abort_flag) {
   red[q][r] = acc;
   __syncthreads();
   if (tid < kNB) rhs[tid] -= (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
@@ -186,8 +209,9 @@ k_trsv(int n, const float* __restrict__ A, size_t lda, float* x, size_t incx, bo
 
   // ---- 3. x_b = inv(D) rhs, publish ----
   float s = 0.f;
-#pragma unroll
-  for (int c = q * 16; c < q * 16 + 16; ++c) s = fmaf(D[r][c], rhs[c], s);
+  const int cq = q * (kNB / kQ);
+#pragma unroll 8
+  for (int c = cq; c < cq + kNB / kQ; ++c) s = fmaf(D[r][c], rhs[c], s);
   red[q][r] = s;
   __syncthreads();
   if (tid < kNB) {
@@ -195,6 +219,19 @@ k_trsv(int n, const float* __restrict__ A, size_t lda, float* x, size_t incx, bo
     if (b0 + tid < n) x[(size_t)(b0 + tid) * incx] = v;
     st_release64(slots + (size_t)blk * kNB + tid,
                  ((unsigned long long)epoch << 32) | __float_as_uint(v));
+  }
+  }  // !abort_flag
+  // The last CTA to finish (aborted or not) resets the ticket counter and
+  // publishes this call's epoch for the next call.
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    if (atomicAdd(done, 1u) == (unsigned)nblk - 1) {
+      *ticket = 0u;
+      *done = 0u;
+      __threadfence();
+      atomicExch(epoch_word, epoch);
+    }
   }
 }
 
@@ -214,30 +251,45 @@ extern "C" coral_status_t coral_strsv(coral_handle_t hh, int uplo, int trans, in
   if (lda < n) return bad_arg(H, 6);
   if (!x) return bad_arg(H, 7);
   if (incx == 0) return bad_arg(H, 8);
-  const size_t nblk = (n + kNB - 1) / kNB;
+  const int nb = H->trsv_block == 128 || (H->trsv_block == 0 && n >= 8192) ? 128 : 64;
+  const size_t nblk = (n + nb - 1) / nb;
   if (n > (size_t)INT32_MAX) return CORAL_ERR_NOT_SUPPORTED;
-  if (H->trsv_slots_len < nblk * kNB) {
+  if (H->trsv_slots_len < nblk * nb) {
     if (H->trsv_slots) {
       CORAL_CUDA(H, cudaStreamSynchronize(H->stream));
       cudaFree(H->trsv_slots);
       H->trsv_slots = nullptr;
       H->trsv_slots_len = 0;
     }
-    const size_t len = ((nblk * kNB + 65535) / 65536) * 65536;
+    const size_t len = ((nblk * nb + 65535) / 65536) * 65536;
     CORAL_CUDA(H, cudaMalloc(&H->trsv_slots, len * sizeof(unsigned long long)));
     CORAL_CUDA(H, cudaMemsetAsync(H->trsv_slots, 0, len * sizeof(unsigned long long), H->stream));
     H->trsv_slots_len = len;
   }
   const bool t = trans != CORAL_NO_TRANSPOSE;
   const bool lower_eff = (uplo == CORAL_LOWER) != t;
-  H->trsv_epoch += 1;
-  if (H->trsv_epoch == 0) H->trsv_epoch = 1;  // flags start at 0: never a valid epoch
-  const unsigned long long base = H->trsv_tickets;
-  H->trsv_tickets += nblk;
+  const size_t smem = 2 * (size_t)nb * (nb + 1) * sizeof(float);
+  static uint64_t attr_devices[2] = {0, 0};  // bit d: attribute set on device d, per block size
+  const uint64_t bit = H->device < 64 ? (1ull << H->device) : 0;
+  uint64_t& mask = attr_devices[nb == 128];
+  if (!(mask & bit) || !bit) {
+    if (nb == 128)
+      CORAL_CUDA(H, cudaFuncSetAttribute(k_trsv<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    else
+      CORAL_CUDA(H, cudaFuncSetAttribute(k_trsv<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    mask |= bit;
+  }
   timed_begin(H);
-  k_trsv<<<(unsigned)nblk, kTrsvThreads, 0, H->stream>>>(
-      (int)n, matrix, lda, x, incx, lower_eff, t, diag == CORAL_UNIT, H->trsv_slots,
-      &H->words->trsv_ticket, base, H->trsv_epoch, &H->words->status, H->wait_limit * 32ull);
+  if (nb == 128)
+    k_trsv<128><<<(unsigned)nblk, 512, smem, H->stream>>>(
+        (int)n, matrix, lda, x, incx, lower_eff, t, diag == CORAL_UNIT, H->trsv_slots,
+        &H->words->trsv_ticket, &H->words->trsv_done, &H->words->trsv_epoch, &H->words->status,
+        H->wait_limit * 32ull);
+  else
+    k_trsv<64><<<(unsigned)nblk, 256, smem, H->stream>>>(
+        (int)n, matrix, lda, x, incx, lower_eff, t, diag == CORAL_UNIT, H->trsv_slots,
+        &H->words->trsv_ticket, &H->words->trsv_done, &H->words->trsv_epoch, &H->words->status,
+        H->wait_limit * 32ull);
   coral_status_t s = launch_status(H);
   timed_end(H);
   return s;

@@ -191,3 +191,48 @@ def test_strsv_wait_timeout_reports_status(cuda):
     cb.strsv(1, 0, 1, n, A, n, X, 1)
     h.sync()
     allclose_ref(host(X), oracle.strsv(1, 0, 1, n, a, n, x, 1), 1e-4, 1e-6)
+
+
+@pytest.mark.parametrize("rows", [64, 128])
+@pytest.mark.parametrize("n,uplo,trans", [(1000, 1, 0), (1000, 0, 1), (4097, 0, 0), (4097, 1, 1)])
+def test_strsv_block_sizes(cuda, rows, n, uplo, trans):
+    """Both diagonal-block sizes solve the same systems."""
+    a = tri_matrix(n, n, uplo, n + rows, diag_boost=float(n))
+    x = np.random.default_rng(rows).uniform(-1, 1, n).astype(np.float32)
+    h = cb.handle()
+    h.set_trsv_block(rows)
+    try:
+        X = dev(x)
+        cb.strsv(uplo, trans, 1, n, dev(a), n, X, 1)
+        got = host(X)
+    finally:
+        h.set_trsv_block(0)
+    allclose_ref(got, oracle.strsv(uplo, trans, 1, n, a, n, x, 1), 1e-4, 1e-6)
+
+
+def test_strsv_graph_replay(cuda):
+    """The solve keeps its per-call state (tickets, epoch) on the device, so a
+    captured solve replays correctly any number of times."""
+    n = 3000
+    a = tri_matrix(n, n, 1, 21, diag_boost=float(n))
+    A = dev(a)
+    x = np.random.default_rng(5).uniform(-1, 1, n).astype(np.float32)
+    B = dev(x)
+    X = B.clone()
+    cb.strsv(1, 0, 1, n, A, n, X, 1)  # first call sizes the slot array outside capture
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            X.copy_(B)
+            cb.strsv(1, 0, 1, n, A, n, X, 1)
+    torch.cuda.current_stream().wait_stream(s)
+    want = oracle.strsv(1, 0, 1, n, a, n, x, 1)
+    for _ in range(4):
+        X.fill_(float("nan"))
+        g.replay()
+        allclose_ref(host(X), want, 1e-4, 1e-6)
+    del g
+    cb.handle().sync()
