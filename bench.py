@@ -475,9 +475,6 @@ def level12_bandwidth(torch, cb, lib, h, dev, g):
         cb.strsv(1, 0, 1, nt, L, nt, xb, 1)
     # the 16 KB copy of b is inside the timed call; it is < 0.1% of the bytes
     rec("strsv_lower", 4 * (nt * (nt + 1) // 2 + 2 * nt), timed_calls(trsv_call, 10, True))
-    h.set_trsv_block(128)
-    rec("strsv_lower_nb128", 4 * (nt * (nt + 1) // 2 + 2 * nt), timed_calls(trsv_call, 10, True))
-    h.set_trsv_block(0)
     del L
     nc = 4096
     Hm = torch.empty(nc * nc, dtype=torch.complex64, device=dev)

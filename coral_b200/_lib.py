@@ -36,7 +36,6 @@ SIGNATURES = {
     "coral_get_gemm_mode": [_h, C.POINTER(_i)],
     "coral_set_wait_limit": [_h, C.c_uint64],
     "coral_set_split_chunk": [_h, _i],
-    "coral_set_trsv_block": [_h, _i],
     "coral_sync": [_h],
     "coral_set_kernel_timing": [_h, _i],
     "coral_get_kernel_timing": [_h, C.POINTER(_d), C.POINTER(C.c_uint64)],

@@ -105,10 +105,6 @@ class Handle:
     def set_split_chunk(self, slabs: int) -> None:
         self.check(self.lib.coral_set_split_chunk(self.h, slabs), "coral_set_split_chunk")
 
-    def set_trsv_block(self, rows: int) -> None:
-        """Rows per STRSV diagonal block: 64, 128, or 0 to choose by n."""
-        self.check(self.lib.coral_set_trsv_block(self.h, rows), "coral_set_trsv_block")
-
     def set_wait_limit(self, spins: int) -> None:
         self.check(self.lib.coral_set_wait_limit(self.h, spins), "coral_set_wait_limit")
 

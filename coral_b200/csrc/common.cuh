@@ -50,8 +50,6 @@ struct Handle {
   // Zeroed pool of per-tile arrival counters for single-launch multi-block
   // combines; every kernel returns the counters it used to zero.
   unsigned* counters = nullptr;
-  // TRSV block size (64 or 128 rows; 0 = by size)
-  int trsv_block = 0;
   // TRSV epoch-tagged solution slots ((epoch << 32) | float bits), zeroed when
   // (re)allocated so stale memory never carries a live epoch.
   unsigned long long* trsv_slots = nullptr;

@@ -218,13 +218,6 @@ coral_status_t coral_set_split_chunk(coral_handle_t handle, int slabs) {
   return CORAL_OK;
 }
 
-coral_status_t coral_set_trsv_block(coral_handle_t handle, int rows) {
-  CORAL_HANDLE(handle);
-  if (rows != 0 && rows != 64 && rows != 128) return bad_arg(H, 1);
-  H->trsv_block = rows;
-  return CORAL_OK;
-}
-
 coral_status_t coral_set_wait_limit(coral_handle_t handle, uint64_t spins) {
   CORAL_HANDLE(handle);
   H->wait_limit = spins ? spins : kDefaultWaitLimit;

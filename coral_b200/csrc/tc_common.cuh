@@ -191,9 +191,10 @@ __host__ __device__ constexpr uint32_t idesc_s8_s32(int M, int N) {
 
 }  // namespace tc
 
-// Host: encodes a 2-D K-major tensor map (inner dimension = K, contiguous)
-// for `elem_bytes`-byte elements with the given box, 128-byte swizzle and
-// zero fill outside [0, inner) x [0, outer).  Returns false on failure.
+// Host: encodes a 2-D tensor map (inner dimension contiguous) for
+// `elem_bytes`-byte elements (1: u8, 2: bf16, 4: f32) with the given box,
+// 128-, 64- or no (0) byte swizzle and zero fill outside [0, inner) x
+// [0, outer).  Returns false on failure.
 bool encode_kmajor_map(CUtensorMap* map, const void* base, int elem_bytes, uint64_t inner,
                        uint64_t outer, uint64_t row_stride_bytes, uint32_t box_inner,
                        uint32_t box_outer, int swizzle_bytes = 128);

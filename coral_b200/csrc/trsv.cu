@@ -1,8 +1,11 @@
 // STRSV: solve op(A) x = b in place, A triangular (strsv.rs:60-74 ->
 // strlsv.rs / strusv.rs).  ConjugateTranspose == Transpose.
 //
-// One launch.  op(A) is cut into NB-row blocks (NB = 64, or 128 for large n or
-// when the handle asks for it); each CTA takes a ticket from a
+// Two kernels.  k_trsv_cluster (below) is the path for any A that a tensor
+// map can describe; k_trsv, one CTA per block reading A with plain loads, is
+// the path for the rest (lda % 4 != 0 or A not 16-byte aligned).
+//
+// k_trsv: op(A) is cut into 64-row blocks; each CTA takes a ticket from a
 // per-call counter, so block b is handled by the b-th CTA to start (in solve
 // order: forward when op(A) is lower, backward when upper) and only ever
 // waits for blocks whose CTAs started earlier -- no dependency on scheduling
@@ -24,15 +27,16 @@
 // off the critical path.  Waits are bounded by the handle's wait limit and
 // abort early once any CTA has set the status word.
 #include "common.cuh"
+#include "tc_common.cuh"
 
 namespace coral {
 namespace {
 
-// Block size NB (64 or 128 rows); 4 threads per row.
+// Block size NB rows; 4 threads per row.
 template <int NB> struct TrsvCfg {
   static constexpr int kThreads = 4 * NB;
   static constexpr int kPer = NB * NB / kThreads;  // tile elements per thread
-  static constexpr int kG = NB == 64 ? 4 : 2;     // panel tiles loaded per group
+  static constexpr int kG = 4;                    // panel tiles loaded per group
   static constexpr int kQ = 4;                    // thread groups per row
 };
 
@@ -176,8 +180,11 @@ k_trsv(int n, const float* __restrict__ A, size_t lda, float* x, size_t incx, bo
           const uint64_t t0 = gtimer();
           unsigned spins = 0;
           while ((unsigned)((v = ld_acquire64(sp)) >> 32) != epoch) {
-            if (gtimer() - t0 > limit_ns ||
-                ((++spins & 15u) == 0 && *(volatile unsigned*)status != 0)) {
+            // the status word (another block gave up) is read only once the
+            // wait is long; a healthy wait never pays its round trip
+            const uint64_t el = gtimer() - t0;
+            if (el > limit_ns ||
+                ((++spins & 15u) == 0 && el > 20000ull && *(volatile unsigned*)status != 0)) {
               atomicOr(status, kStatusTimeout);
               abort_flag = 1;
               break;
@@ -235,6 +242,577 @@ k_trsv(int n, const float* __restrict__ A, size_t lda, float* x, size_t incx, bo
   }
 }
 
+
+// ---- cluster path ---------------------------------------------------------
+// Same block decomposition (64-row blocks in solve order), restructured so
+// that the chain from one block to the next is as short as the hardware
+// allows:
+//   * CTAs run in clusters of 16 (8 where the hardware cannot place 16) that
+//     take consecutive blocks.  A CTA pushes its solution straight into the
+//     shared memory of the later CTAs of its cluster (st.shared::cluster,
+//     epoch-tagged like the global slots), so 15 of every 16 hand-offs skip
+//     the L2 round trip; the global slots serve later clusters.
+//   * At setup each CTA inverts its diagonal block D and forms
+//     M1 = inv(D) op(A)(b, b-1) and M2 = inv(D) op(A)(b, b-2) in registers.
+//     With y = inv(D) (rhs - sum_{k <= b-3} op(A)(b, k) x_k), the solution is
+//     x_b = y - M2 x_{b-2} - M1 x_{b-1}: once x_{b-1} lands, each row costs 16
+//     FMAs and a 4-lane shuffle reduction -- no block-wide barrier.
+//   * The panel tiles op(A)(b, k), k <= b-3, stream through a 4-stage TMA ring
+//     (64 x 64 fp32 boxes, zero fill past n) fed by a producer warp, which
+//     also polls the solution slots of 8 tiles at once and stages ready ones
+//     in a shared-memory ring, so neither the tile nor the solution latency
+//     sits on the consumers' path.
+// Requires lda % 4 == 0 and a 16-byte aligned A (tensor-map rules).
+constexpr int kCB = 64;          // rows per block
+constexpr int kClMax = 16;       // CTAs per cluster: 16, or 8 where 16 cannot be placed
+constexpr int kCStages = 4;      // panel tile ring
+constexpr int kXRing = 32;       // staged solutions of panel tiles
+constexpr int kLook = 8;         // panel solutions polled at once
+constexpr int kCons = 256;       // consumer threads (8 warps)
+constexpr int kCThreads = kCons + 32;
+constexpr uint32_t kTileBytes = kCB * kCB * 4;
+constexpr int kLd = kCB + 4;     // row stride of the square work arrays (16-byte rows)
+
+struct ClusterSmem {
+  float ring[kCStages][kCB][kCB];     // panel tiles as loaded: [stored col][stored row]
+  float raw[3][kCB][kCB];             // diagonal block, tiles (b-1), (b-2) as loaded
+  float Dm[kCB][kLd];                 // op(D) masked (lower form), then inv(op(D)) transposed
+  float W[kCB][kLd];                  // inverse under construction, then op(tile b-2), then M2
+  float Top[kCB][kLd];                // inversion scratch, then op(tile b-1), then M1
+  float xs[kXRing][kCB];              // staged solutions of panel tiles
+  unsigned long long xin[kClMax][kCB];  // solutions pushed by earlier CTAs of the cluster
+  float part[8][kCB];
+  float v[kCB + 4];                   // v[vi(c)]: one pad word per 16 values
+  float rhs[kCB];
+  uint64_t full[kCStages];
+  uint64_t empty[kCStages];
+  uint64_t xfull[kXRing];
+  uint64_t xempty[kXRing];
+  uint64_t setup_bar;
+  unsigned ticket, epoch, my_ticket, my_epoch;
+  int abort_flag;
+  int issued;                         // panel tile loads the producer issued
+};
+
+// v keeps one pad word after every 16 values, so the four 16-value groups
+// read by a warp's lane quads start in different banks.
+__device__ __forceinline__ int vi(int c) { return c + (c >> 4); }
+
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t map_rank(const void* p, unsigned rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(tc::smem_u32(p)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ unsigned ld_cluster_u32(uint32_t addr) {
+  unsigned v;
+  asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_cluster_u64(uint32_t addr, unsigned long long v) {
+  asm volatile("st.relaxed.cluster.shared::cluster.u64 [%0], %1;" ::"r"(addr), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_local_tag(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.cluster.shared::cta.u64 %0, [%1];" : "=l"(v) : "r"(tc::smem_u32(p)) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void bar_consumers() {
+  asm volatile("bar.sync 1, %0;" ::"n"(kCons) : "memory");
+}
+__device__ __forceinline__ float quad_sum(float v) {
+  v += __shfl_xor_sync(0xffffffffu, v, 1);
+  v += __shfl_xor_sync(0xffffffffu, v, 2);
+  return v;
+}
+
+// Reads one block's 64 epoch-tagged solution values (global slots, or this
+// CTA's copies pushed by earlier CTAs of the cluster): lane l polls values 2l
+// and 2l + 1 (16 contiguous bytes) until the whole warp sees `epoch`, then
+// shuffles give each lane xv[j] = x[16 (lane & 3) + j], j < 16.  The poll
+// touches only the values, the timer and the CTA's abort flag; the global
+// status word (an L2 round trip) is read only after 20 us without the values.
+// False (warp-uniform) on timeout or abort.
+__device__ __forceinline__ bool fetch_x(const unsigned long long* src, bool local, unsigned epoch,
+                                        int lane, float (&xv)[16], const unsigned* status,
+                                        const int* abort_flag, uint64_t limit_ns) {
+  unsigned long long v0, v1;
+  uint64_t t0 = 0;
+  for (unsigned spins = 0;; ++spins) {
+    if (local) {
+      v0 = ld_local_tag(src + 2 * lane);
+      v1 = ld_local_tag(src + 2 * lane + 1);
+    } else {
+      v0 = ld_relaxed64(src + 2 * lane);
+      v1 = ld_relaxed64(src + 2 * lane + 1);
+    }
+    const bool ok = (unsigned)(v0 >> 32) == epoch && (unsigned)(v1 >> 32) == epoch;
+    if (__all_sync(0xffffffffu, ok)) break;
+    const uint64_t now = tc::globaltimer();
+    if (spins == 0) {
+      t0 = now;
+      continue;
+    }
+    const uint64_t el = now - t0;
+    bool quit = el > limit_ns;
+    if ((spins & 15u) == 0)
+      quit = quit || *(volatile const int*)abort_flag ||
+             (el > 20000ull && *(volatile const unsigned*)status != 0);
+    if (__any_sync(0xffffffffu, quit)) return false;
+  }
+  const float f0 = __uint_as_float((unsigned)v0), f1 = __uint_as_float((unsigned)v1);
+  const int base = 8 * (lane & 3);
+#pragma unroll
+  for (int j = 0; j < 16; ++j) xv[j] = __shfl_sync(0xffffffffu, (j & 1) ? f1 : f0, base + (j >> 1));
+  return true;
+}
+
+// Inverse of a 64 x 64 lower-triangular L into X by 8 x 8 blocks: the diagonal blocks are inverted by
+// substitution (one warp each), Lp = blockdiag(inv(L_II)) L is formed for the
+// blocks left of the diagonal, and then block diagonal d = 1..7 of the
+// inverse follows from X_IJ = -sum_{K=J}^{I-1} Lp_IK X_KJ, whose terms lie on
+// diagonals < d.  Seven short dependent stages instead of 63 substitution
+// steps.  Consumer threads only (tid < 256); rdiag holds 64 floats of
+// scratch.  All arrays have row stride kLd.
+__device__ __forceinline__ void invert_lower64(float (*L)[kLd], float (*X)[kLd], float (*Lp)[kLd],
+                                               float* rdiag, int tid) {
+  for (int e = tid; e < kCB * kLd; e += kCons) (&X[0][0])[e] = 0.f;
+  if (tid < kCB) rdiag[tid] = 1.f / L[tid][tid];
+  bar_consumers();
+  {
+    const int w = tid >> 5, c = tid & 31;
+    if (c < 8) {
+      const int o = 8 * w;
+      float xc[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        float a = (i == c) ? 1.f : 0.f;
+#pragma unroll
+        for (int j = 0; j < i; ++j) a = fmaf(-L[o + i][o + j], xc[j], a);
+        xc[i] = (i < c) ? 0.f : a * rdiag[o + i];
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) X[o + i][o + c] = xc[i];
+    }
+  }
+  bar_consumers();
+  for (int e = tid; e < kCB * kCB; e += kCons) {
+    const int R = e / kCB, k = e % kCB, I = R >> 3;
+    float a = 0.f;
+    if (k < 8 * I) {
+#pragma unroll
+      for (int m = 0; m < 8; ++m) a = fmaf(X[R][8 * I + m], L[8 * I + m][k], a);
+    }
+    Lp[R][k] = a;
+  }
+  bar_consumers();
+  for (int d = 1; d < 8; ++d) {
+    for (int o = tid; o < (8 - d) * 64; o += kCons) {
+      const int J = o >> 6, i = (o >> 3) & 7, j = o & 7, I = J + d;
+      const int R = 8 * I + i, C = 8 * J + j;
+      float a0 = 0.f, a1 = 0.f;
+      for (int K = J; K < I; ++K) {
+#pragma unroll
+        for (int m = 0; m < 8; m += 2) {
+          a0 = fmaf(Lp[R][8 * K + m], X[8 * K + m][C], a0);
+          a1 = fmaf(Lp[R][8 * K + m + 1], X[8 * K + m + 1][C], a1);
+        }
+      }
+      X[R][C] = -(a0 + a1);
+    }
+    bar_consumers();
+  }
+}
+
+__global__ void __launch_bounds__(kCThreads, 1)
+k_trsv_cluster(const __grid_constant__ CUtensorMap amap, int n, float* x, size_t incx,
+               bool lower_eff, bool trans, bool unit, unsigned long long* slots, unsigned* ticket,
+               unsigned* done, unsigned* epoch_word, unsigned* status, uint64_t limit_ns) {
+  // Offsetting the __shared__ array itself (not an integer address) keeps the
+  // accesses below in the shared window (LDS/STS rather than generic loads).
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  ClusterSmem& S = *reinterpret_cast<ClusterSmem*>(
+      smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u));
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned rank = cluster_rank();
+
+  unsigned ncl;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(ncl));
+  const int kCl = (int)ncl;
+  for (int i = tid; i < kCl * kCB; i += kCThreads) (&S.xin[0][0])[i] = 0ull;
+  if (tid == 0) {
+    for (int i = 0; i < kCStages; ++i) {
+      tc::mbar_init(&S.full[i], 1);
+      tc::mbar_init(&S.empty[i], 8);
+    }
+    for (int i = 0; i < kXRing; ++i) {
+      tc::mbar_init(&S.xfull[i], 32);
+      tc::mbar_init(&S.xempty[i], 8);
+    }
+    tc::mbar_init(&S.setup_bar, 1);
+    tc::fence_mbar_init();
+    S.abort_flag = 0;
+    S.issued = 0;
+    if (rank == 0) {
+      // Tickets start at 0 in every call (the last CTA resets the counter);
+      // the epoch is one past the last completed call's, read before any CTA
+      // of this call can finish and advance it.
+      S.ticket = atomicAdd(ticket, 1u);
+      unsigned e = *(volatile unsigned*)epoch_word + 1u;
+      S.epoch = e ? e : 1u;  // slots start at 0: never a live epoch
+    }
+  }
+  cluster_sync_all();
+  if (tid == 0) {
+    S.my_ticket = ld_cluster_u32(map_rank(&S.ticket, 0));
+    S.my_epoch = ld_cluster_u32(map_rank(&S.epoch, 0));
+  }
+  __syncthreads();
+  const unsigned epoch = S.my_epoch;
+  const int nblk = (n + kCB - 1) / kCB;
+  const int s_first = (int)S.my_ticket * kCl;        // first solve index of this cluster
+  const int s = s_first + (int)rank;                   // this CTA's solve index
+  const bool active = s < nblk;
+  auto blk_of = [&](int sp) { return lower_eff ? sp : nblk - 1 - sp; };
+  const int blk = active ? blk_of(s) : 0;
+  const int b0 = blk * kCB;
+  const int npanel = s >= 3 ? s - 2 : 0;              // panel tiles: solve indices 0 .. s-3
+  // TMA coordinates of tile op(A)(blk, kb): stored rows x, stored columns y
+  auto tile_x = [&](int kb) { return trans ? kb * kCB : b0; };
+  auto tile_y = [&](int kb) { return trans ? b0 : kb * kCB; };
+
+  if (active && warp == 8) {
+    // ---------------- producer warp ----------------
+    if (lane == 0) {
+      tc::prefetch_tmap(&amap);
+      uint32_t bytes = kTileBytes * (1 + (s >= 1) + (s >= 2));
+      tc::mbar_expect_tx(&S.setup_bar, bytes);
+      tc::tma_load_2d(S.raw[0], &amap, &S.setup_bar, b0, b0);
+      if (s >= 1) tc::tma_load_2d(S.raw[1], &amap, &S.setup_bar, tile_x(blk_of(s - 1)), tile_y(blk_of(s - 1)));
+      if (s >= 2) tc::tma_load_2d(S.raw[2], &amap, &S.setup_bar, tile_x(blk_of(s - 2)), tile_y(blk_of(s - 2)));
+    }
+    int tma_next = 0, x_next = 0;
+    uint64_t t_last = 0;  // start of the current stretch without progress (0: none)
+    unsigned iter = 0;
+    const int nstaged = npanel < s_first ? npanel : s_first;  // panel tiles of earlier clusters
+    while (x_next < nstaged || tma_next < npanel) {
+      if (lane == 0) {
+        while (tma_next < npanel) {
+          const int st = tma_next % kCStages;
+          if (tma_next >= kCStages && !tc::mbar_try_wait(&S.empty[st], ((tma_next / kCStages) - 1) & 1))
+            break;
+          const int kb = blk_of(tma_next);
+          tc::mbar_expect_tx(&S.full[st], kTileBytes);
+          tc::tma_load_2d(S.ring[st], &amap, &S.full[st], tile_x(kb), tile_y(kb));
+          ++tma_next;
+        }
+      }
+      tma_next = __shfl_sync(0xffffffffu, tma_next, 0);
+      // solutions of panel tiles x_next .. x_next + kLook - 1: load all, then
+      // publish the ready prefix in order
+      unsigned long long va[kLook], vb[kLook];
+#pragma unroll
+      for (int w = 0; w < kLook; ++w) {
+        const int i = x_next + w;
+        va[w] = vb[w] = 0ull;
+        if (i < nstaged) {
+          va[w] = ld_relaxed64(slots + (size_t)i * kCB + lane);
+          vb[w] = ld_relaxed64(slots + (size_t)i * kCB + lane + 32);
+        }
+      }
+      bool go = true;
+      const int x_start = x_next;
+#pragma unroll
+      for (int w = 0; w < kLook; ++w) {
+        const int i = x_start + w;
+        if (go && i < nstaged) {
+          const int j = i % kXRing;
+          bool ok = (unsigned)(va[w] >> 32) == epoch && (unsigned)(vb[w] >> 32) == epoch;
+          ok = __all_sync(0xffffffffu, ok);
+          if (ok && i >= kXRing) ok = tc::mbar_try_wait(&S.xempty[j], ((i / kXRing) - 1) & 1);
+          ok = __all_sync(0xffffffffu, ok);
+          if (ok) {
+            S.xs[j][lane] = __uint_as_float((unsigned)va[w]);
+            S.xs[j][lane + 32] = __uint_as_float((unsigned)vb[w]);
+            tc::mbar_arrive(&S.xfull[j]);
+            x_next = i + 1;
+          } else {
+            go = false;
+          }
+        }
+      }
+      // progress check every 16 idle rounds: timer and abort flag, and the
+      // global status word only after 20 us without progress
+      bool quit = false;
+      if (x_next != x_start) {
+        iter = 0;
+        t_last = 0;
+      } else if ((++iter & 15u) == 0) {
+        const uint64_t now = tc::globaltimer();
+        if (t_last == 0) t_last = now;
+        const uint64_t el = now - t_last;
+        quit = el > limit_ns || *(volatile int*)&S.abort_flag ||
+               (el > 20000ull && *(volatile unsigned*)status != 0);
+      }
+      quit = __any_sync(0xffffffffu, quit);
+      if (quit) {
+        if (lane == 0) {
+          atomicOr(status, kStatusTimeout);
+          S.abort_flag = 1;
+        }
+        break;
+      }
+    }
+    if (lane == 0) S.issued = tma_next;
+  } else if (active) {
+    // ---------------- consumer warps ----------------
+    // the right-hand side is read first so its latency hides behind the wait
+    const float rhs_v = (tid < kCB && b0 + tid < n) ? x[(size_t)(b0 + tid) * incx] : 0.f;
+    bool ok = tc::mbar_wait(&S.setup_bar, 0, limit_ns);
+    // op(D) masked: stored element (b0 + rr, b0 + cc) sits at raw[0][cc][rr].
+    // An upper op(D) is stored index-reversed (P op(D) P, P the reversal),
+    // which is lower triangular; its inverse is reversed back below.
+    for (int e = tid; e < kCB * kCB; e += kCons) {
+      const int rr = e % kCB, cc = e / kCB;
+      float v = S.raw[0][cc][rr];
+      const int r = trans ? cc : rr, c = trans ? rr : cc;
+      const bool in_tri = lower_eff ? r >= c : r <= c;
+      if (r == c) v = (unit || b0 + r >= n) ? 1.f : v;
+      else if (!in_tri) v = 0.f;
+      if (lower_eff) S.Dm[r][c] = v;
+      else S.Dm[kCB - 1 - r][kCB - 1 - c] = v;
+    }
+    if (tid < kCB) S.rhs[tid] = rhs_v;
+    bar_consumers();
+    invert_lower64(S.Dm, S.W, S.Top, S.v, tid);
+    // Dm <- inv(op(D)) transposed: Dm[i][r] = inv(op(D))[r][i]
+    for (int e = tid; e < kCB * kCB; e += kCons) {
+      const int i = e / kCB, r = e % kCB;
+      S.Dm[i][r] = lower_eff ? S.W[r][i] : S.W[kCB - 1 - r][kCB - 1 - i];
+    }
+    bar_consumers();
+    // op(tile) row-major for blocks b-1 (Top) and b-2 (W); zero where absent
+    for (int e = tid; e < kCB * kCB; e += kCons) {
+      const int i = trans ? e / kCB : e % kCB, c = trans ? e % kCB : e / kCB;
+      S.Top[i][c] = s >= 1 ? (trans ? S.raw[1][i][c] : S.raw[1][c][i]) : 0.f;
+      S.W[i][c] = s >= 2 ? (trans ? S.raw[2][i][c] : S.raw[2][c][i]) : 0.f;
+    }
+    bar_consumers();
+    const int r = tid >> 2, q = tid & 3, c0 = q * 16;
+    float inv[16], M1[16], M2[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) inv[j] = S.Dm[c0 + j][r];
+    if (s >= 1) {
+      // [M1 | M2] = inv(op(D)) [op(tile b-1) | op(tile b-2)] as 4 x 4 register
+      // outer products: rows 4 rg .. 4 rg + 3, columns 4 cg .. 4 cg + 3 of
+      // each; a quarter-warp reads 128 contiguous bytes of each tile row.
+      const int rg = 2 * warp + (lane >> 4), cg = lane & 15;
+      float a1[4][4], a2[4][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) a1[u][v] = a2[u][v] = 0.f;
+#pragma unroll 2
+      for (int i = 0; i < kCB; ++i) {
+        const float4 dv = *reinterpret_cast<const float4*>(&S.Dm[i][4 * rg]);
+        const float4 p = *reinterpret_cast<const float4*>(&S.Top[i][4 * cg]);
+        const float4 w2 = *reinterpret_cast<const float4*>(&S.W[i][4 * cg]);
+        const float d4[4] = {dv.x, dv.y, dv.z, dv.w};
+        const float p4[4] = {p.x, p.y, p.z, p.w};
+        const float w4[4] = {w2.x, w2.y, w2.z, w2.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            a1[u][v] = fmaf(d4[u], p4[v], a1[u][v]);
+            a2[u][v] = fmaf(d4[u], w4[v], a2[u][v]);
+          }
+      }
+      bar_consumers();
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        *reinterpret_cast<float4*>(&S.Top[4 * rg + u][4 * cg]) = make_float4(a1[u][0], a1[u][1], a1[u][2], a1[u][3]);
+        *reinterpret_cast<float4*>(&S.W[4 * rg + u][4 * cg]) = make_float4(a2[u][0], a2[u][1], a2[u][2], a2[u][3]);
+      }
+      bar_consumers();
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        M1[j] = S.Top[r][c0 + j];
+        M2[j] = S.W[r][c0 + j];
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) M1[j] = M2[j] = 0.f;
+    }
+
+    // panel: acc = sum over solve indices k <= s-3 of op(A)(b, k) x_k
+    float acc[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j] = 0.f;
+    for (int i = 0; i < npanel && ok; ++i) {
+      const int st = i % kCStages, j = i % kXRing;
+      const bool staged = i < s_first;  // earlier cluster: staged by the producer
+      ok = tc::mbar_wait(&S.full[st], (i / kCStages) & 1, limit_ns) &&
+           (!staged || tc::mbar_wait(&S.xfull[j], (i / kXRing) & 1, limit_ns));
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) break;
+      // solution values lane and lane + 32 of block i
+      float x0, x1;
+      if (staged) {
+        x0 = S.xs[j][lane];
+        x1 = S.xs[j][lane + 32];
+      } else {
+        // this cluster: read the pushed copy directly
+        const unsigned long long* src = S.xin[i - s_first];
+        unsigned long long v0, v1;
+        uint64_t t0 = 0;
+        for (unsigned spins = 0;; ++spins) {
+          v0 = ld_local_tag(src + lane);
+          v1 = ld_local_tag(src + lane + 32);
+          const bool got = (unsigned)(v0 >> 32) == epoch && (unsigned)(v1 >> 32) == epoch;
+          if (__all_sync(0xffffffffu, got)) break;
+          const uint64_t now = tc::globaltimer();
+          if (spins == 0) t0 = now;
+          bool quit = now - t0 > limit_ns;
+          if ((spins & 15u) == 0) quit = quit || *(volatile int*)&S.abort_flag;
+          if (__any_sync(0xffffffffu, quit)) {
+            ok = false;
+            break;
+          }
+        }
+        if (!ok) break;
+        x0 = __uint_as_float((unsigned)v0);
+        x1 = __uint_as_float((unsigned)v1);
+      }
+      const float (*T)[kCB] = S.ring[st];
+      if (!trans) {
+        // T[c][r]: rows lane, lane + 32; this warp's columns 8w .. 8w + 7,
+        // whose solution values sit in lanes (8w + u) mod 32 of x0 or x1
+        const float xsrc = warp < 4 ? x0 : x1;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const float xu = __shfl_sync(0xffffffffu, xsrc, (warp * 8 + u) & 31);
+          acc[0] = fmaf(T[warp * 8 + u][lane], xu, acc[0]);
+          acc[1] = fmaf(T[warp * 8 + u][lane + 32], xu, acc[1]);
+        }
+      } else {
+        // T[r][c]: this warp's rows 8w .. 8w + 7; columns lane, lane + 32
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          acc[u] = fmaf(T[warp * 8 + u][lane], x0, fmaf(T[warp * 8 + u][lane + 32], x1, acc[u]));
+      }
+      __syncwarp();
+      if (lane == 0) {
+        tc::mbar_arrive(&S.empty[st]);
+        if (staged) tc::mbar_arrive(&S.xempty[j]);
+      }
+    }
+    if (!ok && lane == 0) {
+      atomicOr(status, kStatusTimeout);
+      S.abort_flag = 1;
+    }
+    // v = rhs - acc
+    if (!trans) {
+      S.part[warp][lane] = acc[0];
+      S.part[warp][lane + 32] = acc[1];
+      bar_consumers();
+      if (tid < kCB) {
+        float a = 0.f;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) a += S.part[w][tid];
+        S.v[vi(tid)] = S.rhs[tid] - a;
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        float a = acc[u];
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == u) S.v[vi(warp * 8 + u)] = S.rhs[warp * 8 + u] - a;
+      }
+    }
+    bar_consumers();
+    // y = inv(D) v, then the two most recent blocks through M2 and M1
+    float y = 0.f;
+    {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) y = fmaf(inv[j], S.v[vi(c0 + j)], y);
+      y = quad_sum(y);
+    }
+    float xv[16];
+    if (s >= 2) {
+      const bool local = (int)rank >= 2;
+      const unsigned long long* src = local ? &S.xin[rank - 2][0] : slots + (size_t)(s - 2) * kCB;
+      bool got = ok && fetch_x(src, local, epoch, lane, xv, status, &S.abort_flag, limit_ns);
+      float d = 0.f;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) d = fmaf(M2[j], xv[j], d);
+      y -= quad_sum(d);
+      ok = __all_sync(0xffffffffu, got);
+    }
+    if (s >= 1) {
+      const bool local = (int)rank >= 1;
+      const unsigned long long* src = local ? &S.xin[rank - 1][0] : slots + (size_t)(s - 1) * kCB;
+      bool got = ok && fetch_x(src, local, epoch, lane, xv, status, &S.abort_flag, limit_ns);
+      float d = 0.f;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) d = fmaf(M1[j], xv[j], d);
+      y -= quad_sum(d);
+      ok = __all_sync(0xffffffffu, got);
+    }
+    if (ok) {
+      // rows past n solve to 0 (identity diagonal, zero-filled tiles)
+      const unsigned long long val = ((unsigned long long)epoch << 32) | __float_as_uint(y);
+      if (q == 3) st_relaxed64(slots + (size_t)s * kCB + r, val);
+      for (int d = (int)rank + 1 + q; d < kCl; d += 4) st_cluster_u64(map_rank(&S.xin[rank][r], d), val);
+      if (q == 1 && b0 + r < n) x[(size_t)(b0 + r) * incx] = y;
+    } else if (lane == 0) {
+      atomicOr(status, kStatusTimeout);
+      S.abort_flag = 1;
+    }
+  }
+  __syncthreads();
+  if (active && tid == kCons) {
+    // Every issued tile load lands before the CTA leaves (after an abort some
+    // may never have been consumed).  Loads of tiles before issued - stages
+    // were consumed, so only the last ring's worth can be in flight.  This
+    // wait is bounded by its own second, not the caller's wait limit, which
+    // may be far shorter than a copy.
+    const int issued = S.issued;
+    const int first = issued > kCStages ? issued - kCStages : 0;
+    const uint64_t drain_ns = limit_ns > 1000000000ull ? limit_ns : 1000000000ull;
+    for (int i = first; i < issued; ++i)
+      tc::mbar_wait(&S.full[i % kCStages], (i / kCStages) & 1, drain_ns);
+    tc::mbar_wait(&S.setup_bar, 0, drain_ns);
+  }
+  __syncthreads();
+  cluster_sync_all();
+  if (tid == 0) {
+    __threadfence();
+    if (atomicAdd(done, 1u) == gridDim.x - 1) {
+      *ticket = 0u;
+      *done = 0u;
+      __threadfence();
+      atomicExch(epoch_word, epoch);
+    }
+  }
+}
+
 }  // namespace
 }  // namespace coral
 
@@ -251,7 +829,7 @@ extern "C" coral_status_t coral_strsv(coral_handle_t hh, int uplo, int trans, in
   if (lda < n) return bad_arg(H, 6);
   if (!x) return bad_arg(H, 7);
   if (incx == 0) return bad_arg(H, 8);
-  const int nb = H->trsv_block == 128 || (H->trsv_block == 0 && n >= 8192) ? 128 : 64;
+  constexpr int nb = 64;
   const size_t nblk = (n + nb - 1) / nb;
   if (n > (size_t)INT32_MAX) return CORAL_ERR_NOT_SUPPORTED;
   if (H->trsv_slots_len < nblk * nb) {
@@ -268,28 +846,70 @@ extern "C" coral_status_t coral_strsv(coral_handle_t hh, int uplo, int trans, in
   }
   const bool t = trans != CORAL_NO_TRANSPOSE;
   const bool lower_eff = (uplo == CORAL_LOWER) != t;
-  const size_t smem = 2 * (size_t)nb * (nb + 1) * sizeof(float);
-  static uint64_t attr_devices[2] = {0, 0};  // bit d: attribute set on device d, per block size
+  const uint64_t limit_ns = H->wait_limit * 32ull;
+  static uint64_t attr_devices[2] = {0, 0};  // bit d: attribute set on device d, per kernel
   const uint64_t bit = H->device < 64 ? (1ull << H->device) : 0;
-  uint64_t& mask = attr_devices[nb == 128];
-  if (!(mask & bit) || !bit) {
-    if (nb == 128)
-      CORAL_CUDA(H, cudaFuncSetAttribute(k_trsv<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    else
-      CORAL_CUDA(H, cudaFuncSetAttribute(k_trsv<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    mask |= bit;
+  CUtensorMap map;
+  const bool tma_ok = (lda % 4) == 0 && aligned16(matrix) &&
+                      encode_kmajor_map(&map, matrix, 4, n, n, lda * 4, kCB, kCB, 0);
+  if (tma_ok) {
+    const size_t smem = sizeof(ClusterSmem) + 1024;
+    static int cluster_size[64] = {0};  // per device: 16 where the hardware places it, else 8
+    int& cl = cluster_size[H->device < 64 ? H->device : 63];
+    if (!(attr_devices[0] & bit) || !bit || cl == 0) {
+      CORAL_CUDA(H, cudaFuncSetAttribute(k_trsv_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      cl = 8;
+      if (cudaFuncSetAttribute(k_trsv_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+        cudaLaunchConfig_t q = {};
+        cudaLaunchAttribute qa[1];
+        qa[0].id = cudaLaunchAttributeClusterDimension;
+        qa[0].val.clusterDim.x = 16;
+        qa[0].val.clusterDim.y = qa[0].val.clusterDim.z = 1;
+        q.gridDim = dim3(16);
+        q.blockDim = dim3(kCThreads);
+        q.dynamicSmemBytes = smem;
+        q.attrs = qa;
+        q.numAttrs = 1;
+        int active = 0;
+        if (cudaOccupancyMaxActiveClusters(&active, k_trsv_cluster, &q) == cudaSuccess && active >= 1) cl = 16;
+      }
+      cudaGetLastError();  // a refused query leaves cl at 8, not an error
+      attr_devices[0] |= bit;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cl;
+    at[0].val.clusterDim.y = at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)(((nblk + cl - 1) / cl) * cl));
+    cfg.blockDim = dim3(kCThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = H->stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    timed_begin(H);
+    const cudaError_t le = cudaLaunchKernelEx(
+        &cfg, k_trsv_cluster, map, (int)n, x, incx, lower_eff, t, diag == CORAL_UNIT, H->trsv_slots,
+        &H->words->trsv_ticket, &H->words->trsv_done, &H->words->trsv_epoch, &H->words->status,
+        limit_ns);
+    if (le != cudaSuccess) {
+      timed_end(H);
+      count_launch();
+      cudaGetLastError();
+      return cuda_status(H, le);
+    }
+  } else {
+    const size_t smem = 2 * (size_t)nb * (nb + 1) * sizeof(float);
+    if (!(attr_devices[1] & bit) || !bit) {
+      CORAL_CUDA(H, cudaFuncSetAttribute(k_trsv<nb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr_devices[1] |= bit;
+    }
+    timed_begin(H);
+    k_trsv<nb><<<(unsigned)nblk, 4 * nb, smem, H->stream>>>(
+        (int)n, matrix, lda, x, incx, lower_eff, t, diag == CORAL_UNIT, H->trsv_slots,
+        &H->words->trsv_ticket, &H->words->trsv_done, &H->words->trsv_epoch, &H->words->status,
+        limit_ns);
   }
-  timed_begin(H);
-  if (nb == 128)
-    k_trsv<128><<<(unsigned)nblk, 512, smem, H->stream>>>(
-        (int)n, matrix, lda, x, incx, lower_eff, t, diag == CORAL_UNIT, H->trsv_slots,
-        &H->words->trsv_ticket, &H->words->trsv_done, &H->words->trsv_epoch, &H->words->status,
-        H->wait_limit * 32ull);
-  else
-    k_trsv<64><<<(unsigned)nblk, 256, smem, H->stream>>>(
-        (int)n, matrix, lda, x, incx, lower_eff, t, diag == CORAL_UNIT, H->trsv_slots,
-        &H->words->trsv_ticket, &H->words->trsv_done, &H->words->trsv_epoch, &H->words->status,
-        H->wait_limit * 32ull);
   coral_status_t s = launch_status(H);
   timed_end(H);
   return s;

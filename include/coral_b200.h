@@ -84,8 +84,6 @@ coral_status_t coral_get_gemm_mode(coral_handle_t handle, int* mode);
 /* K depth, in 64-element slabs, of each tensor-core accumulation chunk of the
  * split-BF16 GEMMs before it is added into fp32 registers (default 16). */
 coral_status_t coral_set_split_chunk(coral_handle_t handle, int slabs);
-/* Rows per diagonal block of the STRSV solve: 64 or 128 (0: chosen by n). */
-coral_status_t coral_set_trsv_block(coral_handle_t handle, int rows);
 /* Iteration limit of every bounded device wait (0 restores the default). */
 coral_status_t coral_set_wait_limit(coral_handle_t handle, uint64_t spins);
 /* Kernel timing: when enabled, the handle brackets the dominant kernel of each

@@ -193,21 +193,26 @@ def test_strsv_wait_timeout_reports_status(cuda):
     allclose_ref(host(X), oracle.strsv(1, 0, 1, n, a, n, x, 1), 1e-4, 1e-6)
 
 
-@pytest.mark.parametrize("rows", [64, 128])
-@pytest.mark.parametrize("n,uplo,trans", [(1000, 1, 0), (1000, 0, 1), (4097, 0, 0), (4097, 1, 1)])
-def test_strsv_block_sizes(cuda, rows, n, uplo, trans):
-    """Both diagonal-block sizes solve the same systems."""
-    a = tri_matrix(n, n, uplo, n + rows, diag_boost=float(n))
-    x = np.random.default_rng(rows).uniform(-1, 1, n).astype(np.float32)
-    h = cb.handle()
-    h.set_trsv_block(rows)
-    try:
-        X = dev(x)
-        cb.strsv(uplo, trans, 1, n, dev(a), n, X, 1)
-        got = host(X)
-    finally:
-        h.set_trsv_block(0)
-    allclose_ref(got, oracle.strsv(uplo, trans, 1, n, a, n, x, 1), 1e-4, 1e-6)
+@pytest.mark.parametrize("layout", ["tma", "odd_lda", "unaligned"])
+@pytest.mark.parametrize("n,uplo,trans,diag", [(1000, 1, 0, 1), (1000, 0, 1, 1), (4097, 0, 0, 0),
+                                               (4097, 1, 1, 1), (130, 1, 1, 0), (520, 0, 0, 1)])
+def test_strsv_both_paths(cuda, layout, n, uplo, trans, diag):
+    """The tensor-map path (lda % 4 == 0, 16-byte aligned A) and the plain-load
+    path (any other layout) solve the same systems; clusters of 8 blocks with
+    ragged last blocks and partial last clusters included."""
+    lda = n + (1 if layout == "odd_lda" else (4 - n % 4) % 4)
+    a = tri_matrix(n, lda, uplo, n + lda, diag_boost=float(n), garbage_diag=(diag == 0))
+    if diag == 0:
+        a = np.where(np.isnan(a), a, a / np.float32(n))
+    x = np.random.default_rng(lda).uniform(-1, 1, n).astype(np.float32)
+    if layout == "unaligned":
+        buf = dev(np.concatenate([np.zeros(1, np.float32), a]))
+        A = buf[1:]
+    else:
+        A = dev(a)
+    X = dev(x)
+    cb.strsv(uplo, trans, diag, n, A, lda, X, 1)
+    allclose_ref(host(X), oracle.strsv(uplo, trans, diag, n, a, lda, x, 1), 1e-4, 1e-6)
 
 
 def test_strsv_graph_replay(cuda):
