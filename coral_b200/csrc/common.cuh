@@ -94,6 +94,10 @@ void* scratch(Handle* h, size_t bytes);
 
 // Records the CUDA error text in the handle and maps it to a status.
 coral_status_t cuda_status(Handle* h, cudaError_t err);
+// GEMM argument check (gemm_simt.cu): 1-based position of the first bad
+// argument, -1 for sizes past INT32_MAX, 0 when all are valid.
+int gemm_bad_arg(int op_a, int op_b, size_t m, size_t n, size_t k, const void* a, size_t lda,
+                 const void* b, size_t ldb, const void* c, size_t ldc, bool complex_ops);
 // Every kernel launch site reports through launch_status(), which also
 // counts the launch (coral_kernel_launches()).
 void count_launch();

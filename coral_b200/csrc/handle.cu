@@ -124,13 +124,25 @@ static void destroy_handle(Handle* h) {
   delete h;
 }
 
-// Per-thread handle plus growable device staging for the host-slice wrappers.
+// Per-thread handle plus growable device staging for the host-slice wrappers,
+// and the copy streams / events of the pipelined host SGEMM.
+constexpr int kHostPanels = 8;
 struct ThreadState {
   Handle* h = nullptr;
   void* dev = nullptr;
   size_t dev_bytes = 0;
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaEvent_t ev_a = nullptr, ev_in[kHostPanels] = {}, ev_c[kHostPanels] = {}, ev_out = nullptr;
   ~ThreadState() {
     if (dev) cudaFree(dev);
+    if (s_in) cudaStreamDestroy(s_in);
+    if (s_out) cudaStreamDestroy(s_out);
+    if (ev_a) cudaEventDestroy(ev_a);
+    if (ev_out) cudaEventDestroy(ev_out);
+    for (int i = 0; i < kHostPanels; ++i) {
+      if (ev_in[i]) cudaEventDestroy(ev_in[i]);
+      if (ev_c[i]) cudaEventDestroy(ev_c[i]);
+    }
     destroy_handle(h);
   }
 };
@@ -302,11 +314,23 @@ coral_status_t coral_host_set_gemm_mode(int mode) {
   return coral_set_gemm_mode(hh, mode);
 }
 
+// Host-resident operands: for a large problem the PCIe transfers, not the
+// GEMM, bound the call.  A is copied first; then column panels of op(B) and C
+// (8 panels, widths a multiple of 256) stream in on one copy stream, the GEMM
+// of panel j runs on the handle's stream as soon as its inputs land, and C
+// panel j streams back on a second copy stream -- so host-to-device,
+// device-to-host and the compute overlap.  C is not copied in when beta == 0
+// (the GEMM does not read it then).  Small problems take one copy each way.
 coral_status_t coral_host_sgemm(int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
                                 const float* a, size_t lda, const float* b, size_t ldb,
                                 float beta, float* c, size_t ldc) {
   HOST_PROLOGUE();
   bool ta = op_a != CORAL_NO_TRANSPOSE, tb = op_b != CORAL_NO_TRANSPOSE;
+  // arguments are checked before any copy touches the caller's buffers
+  const int bad = gemm_bad_arg(op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, false);
+  if (bad > 0) return bad_arg(H, bad);
+  if (bad < 0) return CORAL_ERR_NOT_SUPPORTED;
+  if (m == 0 || n == 0) return CORAL_OK;
   size_t la = mat_len(ta ? k : m, ta ? m : k, lda);
   size_t lb = mat_len(tb ? n : k, tb ? k : n, ldb);
   size_t lc = mat_len(m, n, ldc);
@@ -316,12 +340,77 @@ coral_status_t coral_host_sgemm(int op_a, int op_b, size_t m, size_t n, size_t k
   float* da = reinterpret_cast<float*>(d + oa);
   float* db = reinterpret_cast<float*>(d + ob);
   float* dc = reinterpret_cast<float*>(d + oc);
-  if (la) CORAL_CUDA(H, cudaMemcpyAsync(da, a, la * 4, cudaMemcpyHostToDevice, H->stream));
-  if (lb) CORAL_CUDA(H, cudaMemcpyAsync(db, b, lb * 4, cudaMemcpyHostToDevice, H->stream));
-  if (lc) CORAL_CUDA(H, cudaMemcpyAsync(dc, c, lc * 4, cudaMemcpyHostToDevice, H->stream));
-  coral_status_t s = coral_sgemm(hh, op_a, op_b, m, n, k, alpha, da, lda, db, ldb, beta, dc, ldc);
-  if (s != CORAL_OK) return s;
-  if (lc) CORAL_CUDA(H, cudaMemcpyAsync(c, dc, lc * 4, cudaMemcpyDeviceToHost, H->stream));
+  const bool read_c = beta != 0.f;
+  const size_t bytes = (la + lb + lc) * 4;
+  if (n < 2 * 256 || m == 0 || k == 0 || bytes < (64u << 20)) {
+    if (la) CORAL_CUDA(H, cudaMemcpyAsync(da, a, la * 4, cudaMemcpyHostToDevice, H->stream));
+    if (lb) CORAL_CUDA(H, cudaMemcpyAsync(db, b, lb * 4, cudaMemcpyHostToDevice, H->stream));
+    if (lc) CORAL_CUDA(H, cudaMemcpyAsync(dc, c, lc * 4, cudaMemcpyHostToDevice, H->stream));
+    coral_status_t s = coral_sgemm(hh, op_a, op_b, m, n, k, alpha, da, lda, db, ldb, beta, dc, ldc);
+    if (s != CORAL_OK) return s;
+    if (lc) CORAL_CUDA(H, cudaMemcpyAsync(c, dc, lc * 4, cudaMemcpyDeviceToHost, H->stream));
+    return coral_sync(hh);
+  }
+  if (!tls.s_in) {
+    CORAL_CUDA(H, cudaStreamCreateWithFlags(&tls.s_in, cudaStreamNonBlocking));
+    CORAL_CUDA(H, cudaStreamCreateWithFlags(&tls.s_out, cudaStreamNonBlocking));
+    CORAL_CUDA(H, cudaEventCreateWithFlags(&tls.ev_a, cudaEventDisableTiming));
+    CORAL_CUDA(H, cudaEventCreateWithFlags(&tls.ev_out, cudaEventDisableTiming));
+    for (int i = 0; i < kHostPanels; ++i) {
+      CORAL_CUDA(H, cudaEventCreateWithFlags(&tls.ev_in[i], cudaEventDisableTiming));
+      CORAL_CUDA(H, cudaEventCreateWithFlags(&tls.ev_c[i], cudaEventDisableTiming));
+    }
+  }
+  // After the first asynchronous copy every early return first waits for the
+  // copy streams, so no transfer still touches the caller's buffers.
+  auto drain = [&](coral_status_t st) {
+    cudaStreamSynchronize(tls.s_in);
+    cudaStreamSynchronize(tls.s_out);
+    return st;
+  };
+#define PIPE_CUDA(call)                                        \
+  do {                                                         \
+    cudaError_t e__ = (call);                                  \
+    if (e__ != cudaSuccess) return drain(cuda_status(H, e__)); \
+  } while (0)
+  // the staging buffers may still be read by the previous call's stream
+  PIPE_CUDA(cudaEventRecord(tls.ev_out, H->stream));
+  PIPE_CUDA(cudaStreamWaitEvent(tls.s_in, tls.ev_out, 0));
+  PIPE_CUDA(cudaMemcpyAsync(da, a, la * 4, cudaMemcpyHostToDevice, tls.s_in));
+  PIPE_CUDA(cudaEventRecord(tls.ev_a, tls.s_in));
+  size_t nb = (n + kHostPanels - 1) / kHostPanels;
+  nb = (nb + 255) / 256 * 256;
+  int panels = 0;
+  for (size_t j0 = 0; j0 < n; j0 += nb, ++panels) {
+    const size_t nj = n - j0 < nb ? n - j0 : nb;
+    // op(B) columns j0 .. j0 + nj: stored columns (N) or stored rows (T)
+    if (!tb)
+      PIPE_CUDA(cudaMemcpy2DAsync(db + j0 * ldb, ldb * 4, b + j0 * ldb, ldb * 4, k * 4, nj,
+                                      cudaMemcpyHostToDevice, tls.s_in));
+    else
+      PIPE_CUDA(cudaMemcpy2DAsync(db + j0, ldb * 4, b + j0, ldb * 4, nj * 4, k,
+                                      cudaMemcpyHostToDevice, tls.s_in));
+    if (read_c)
+      PIPE_CUDA(cudaMemcpy2DAsync(dc + j0 * ldc, ldc * 4, c + j0 * ldc, ldc * 4, m * 4, nj,
+                                      cudaMemcpyHostToDevice, tls.s_in));
+    PIPE_CUDA(cudaEventRecord(tls.ev_in[panels], tls.s_in));
+  }
+  PIPE_CUDA(cudaStreamWaitEvent(H->stream, tls.ev_a, 0));
+  int p = 0;
+  for (size_t j0 = 0; j0 < n; j0 += nb, ++p) {
+    const size_t nj = n - j0 < nb ? n - j0 : nb;
+    PIPE_CUDA(cudaStreamWaitEvent(H->stream, tls.ev_in[p], 0));
+    coral_status_t s = coral_sgemm(hh, op_a, op_b, m, nj, k, alpha, da, lda,
+                                   tb ? db + j0 : db + j0 * ldb, ldb, beta, dc + j0 * ldc, ldc);
+    if (s != CORAL_OK) return drain(s);
+    PIPE_CUDA(cudaEventRecord(tls.ev_c[p], H->stream));
+    PIPE_CUDA(cudaStreamWaitEvent(tls.s_out, tls.ev_c[p], 0));
+    PIPE_CUDA(cudaMemcpy2DAsync(c + j0 * ldc, ldc * 4, dc + j0 * ldc, ldc * 4, m * 4, nj,
+                                    cudaMemcpyDeviceToHost, tls.s_out));
+  }
+  PIPE_CUDA(cudaEventRecord(tls.ev_out, tls.s_out));
+  PIPE_CUDA(cudaStreamWaitEvent(H->stream, tls.ev_out, 0));
+#undef PIPE_CUDA
   return coral_sync(hh);
 }
 
