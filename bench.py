@@ -370,7 +370,7 @@ def batched_set(torch, cb, dev):
     return out
 
 
-def level12_bandwidth(torch, cb, lib, h, dev, g):
+def level12_bandwidth(torch, cb, lib, h, dev, g, routines=None):
     """GB/s of algorithmic traffic for the level-1/2 bandwidth configuration
     (SGEMV N/T 8192^2, SSYMV upper 8192, STRSV lower non-unit 4096 with
     diag = n + U[0,1], CHEMV upper 4096, SDOT/SAXPY/ISAMAX/SNRM2 at 2^26).
@@ -432,6 +432,9 @@ def level12_bandwidth(torch, cb, lib, h, dev, g):
     hbm = peaks()[0]
     out = {}
 
+    def want(name):
+        return routines is None or name in routines
+
     def rec(name, nbytes, ms):
         gbs = nbytes / (ms * 1e-3) / 1e9
         out[name] = {"gbs": gbs, "frac": gbs / hbm, "us": ms * 1e3, "bytes": nbytes}
@@ -445,22 +448,29 @@ def level12_bandwidth(torch, cb, lib, h, dev, g):
     h.set_pointer_mode(1)
     try:
         rp = vp(res.data_ptr())
-        rec("sdot", 8 * n1, timed_calls(lambda: lib.coral_sdot(h.h, n1, vp(x.data_ptr()), 1,
-                                                                 vp(y.data_ptr()), 1, rp), 20, False))
-        rec("snrm2", 4 * n1, timed_calls(lambda: lib.coral_snrm2(h.h, n1, vp(x.data_ptr()), 1, rp), 20, False))
-        rec("isamax", 4 * n1, timed_calls(lambda: lib.coral_isamax(h.h, n1, vp(x.data_ptr()), 1, rp), 20, False))
+        if want("sdot"):
+            rec("sdot", 8 * n1, timed_calls(lambda: lib.coral_sdot(h.h, n1, vp(x.data_ptr()), 1,
+                                                                     vp(y.data_ptr()), 1, rp), 20, False))
+        if want("snrm2"):
+            rec("snrm2", 4 * n1, timed_calls(lambda: lib.coral_snrm2(h.h, n1, vp(x.data_ptr()), 1, rp), 20, False))
+        if want("isamax"):
+            rec("isamax", 4 * n1, timed_calls(lambda: lib.coral_isamax(h.h, n1, vp(x.data_ptr()), 1, rp), 20, False))
     finally:
         h.set_pointer_mode(0)
-    rec("saxpy", 12 * n1, timed_calls(lambda: cb.saxpy(n1, 0.5, x, 1, y, 1), 20, False))
+    if want("saxpy"):
+        rec("saxpy", 12 * n1, timed_calls(lambda: cb.saxpy(n1, 0.5, x, 1, y, 1), 20, False))
     del x, y
     m = 8192
     A = torch.empty(m * m, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
     xv = torch.empty(m, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
     yv = torch.empty(m, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
-    rec("sgemv_n", 4 * (m * m + m + 2 * m), timed_calls(lambda: cb.sgemv(0, m, m, 1.5, A, m, xv, 1, 0.5, yv, 1), 20, False))
-    rec("sgemv_t", 4 * (m * m + m + 2 * m), timed_calls(lambda: cb.sgemv(1, m, m, 1.5, A, m, xv, 1, 0.5, yv, 1), 20, False))
-    rec("ssymv_upper", 4 * (m * (m + 1) // 2 + 3 * m),
-        timed_calls(lambda: cb.ssymv(0, m, 1.5, A, m, xv, 1, 0.5, yv, 1), 20, False))
+    if want("sgemv_n"):
+        rec("sgemv_n", 4 * (m * m + m + 2 * m), timed_calls(lambda: cb.sgemv(0, m, m, 1.5, A, m, xv, 1, 0.5, yv, 1), 20, False))
+    if want("sgemv_t"):
+        rec("sgemv_t", 4 * (m * m + m + 2 * m), timed_calls(lambda: cb.sgemv(1, m, m, 1.5, A, m, xv, 1, 0.5, yv, 1), 20, False))
+    if want("ssymv_upper"):
+        rec("ssymv_upper", 4 * (m * (m + 1) // 2 + 3 * m),
+            timed_calls(lambda: cb.ssymv(0, m, 1.5, A, m, xv, 1, 0.5, yv, 1), 20, False))
     del A
     nt = 4096
     L = torch.empty(nt * nt, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
@@ -474,7 +484,8 @@ def level12_bandwidth(torch, cb, lib, h, dev, g):
         xb.copy_(b)
         cb.strsv(1, 0, 1, nt, L, nt, xb, 1)
     # the 16 KB copy of b is inside the timed call; it is < 0.1% of the bytes
-    rec("strsv_lower", 4 * (nt * (nt + 1) // 2 + 2 * nt), timed_calls(trsv_call, 10, True))
+    if want("strsv_lower"):
+        rec("strsv_lower", 4 * (nt * (nt + 1) // 2 + 2 * nt), timed_calls(trsv_call, 10, True))
     del L
     nc = 4096
     Hm = torch.empty(nc * nc, dtype=torch.complex64, device=dev)
@@ -482,8 +493,9 @@ def level12_bandwidth(torch, cb, lib, h, dev, g):
     Hm.imag.uniform_(-1, 1, generator=g)
     xc = torch.ones(nc, dtype=torch.complex64, device=dev)
     yc = torch.ones(nc, dtype=torch.complex64, device=dev)
-    rec("chemv_upper", 8 * (nc * (nc + 1) // 2 + 3 * nc),
-        timed_calls(lambda: cb.chemv(0, nc, 1.5 - 0.5j, Hm, nc, xc, 1, 0.25 + 0.0j, yc, 1), 10, True))
+    if want("chemv_upper"):
+        rec("chemv_upper", 8 * (nc * (nc + 1) // 2 + 3 * nc),
+            timed_calls(lambda: cb.chemv(0, nc, 1.5 - 0.5j, Hm, nc, xc, 1, 0.25 + 0.0j, yc, 1), 10, True))
     del flush_buf
     return out
 
@@ -548,7 +560,8 @@ def run_ours(args, world, rank, local):
         del A, B, C0, C
         torch.cuda.empty_cache()
         if rank == 0:
-            print(json.dumps({"level12": level12_bandwidth(torch, cb, lib, h, dev, g)}))
+            routines = args.routines.split(",") if args.routines else None
+            print(json.dumps({"level12": level12_bandwidth(torch, cb, lib, h, dev, g, routines)}))
         return
     # accuracy of the headline mode on sampled entries (single call from C0)
     import oracle
@@ -685,6 +698,7 @@ def main():
     ap.add_argument("--size", type=int, default=0, help="m = n = k (profiling cases; default 8192)")
     ap.add_argument("--only-gemm", action="store_true", help="run warmup+steps GEMMs, print nothing")
     ap.add_argument("--only-level12", action="store_true", help="run and print the level-1/2 set only")
+    ap.add_argument("--routines", default="", help="with --only-level12: comma list of routines to time")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_init(args)
