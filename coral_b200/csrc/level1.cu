@@ -98,19 +98,22 @@ k_dot(size_t n, const float* __restrict__ x, size_t incx, const float* __restric
     const size_t n4 = n >> 2;
     const float4* x4 = reinterpret_cast<const float4*>(x);
     const float4* y4 = reinterpret_cast<const float4*>(y);
-    // 4 independent 128-bit loads per operand in flight per thread
+    // 8 independent 128-bit loads in flight per thread: 4 per operand for
+    // sdot, 8 of x for snrm2 (one stream needs the deeper unroll to keep as
+    // many bytes in flight)
+    constexpr int U = kSquare ? 8 : 4;
     size_t i = tid;
     double acc1 = 0.0;
-    for (; i + 3 * stride < n4; i += 4 * stride) {
-      float4 a[4], b[4];
+    for (; i + (U - 1) * stride < n4; i += U * stride) {
+      float4 a[U], b[U];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) a[u] = __ldcs(x4 + i + u * stride);
+      for (int u = 0; u < U; ++u) a[u] = __ldcs(x4 + i + u * stride);
       if (!kSquare) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) b[u] = __ldcs(y4 + i + u * stride);
+        for (int u = 0; u < U; ++u) b[u] = __ldcs(y4 + i + u * stride);
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < U; ++u) {
         const float4 c = kSquare ? a[u] : b[u];
         double& t = (u & 1) ? acc1 : acc;
         t += (double)a[u].x * c.x + (double)a[u].y * c.y + (double)a[u].z * c.z + (double)a[u].w * c.w;
