@@ -468,6 +468,24 @@ def level12_bandwidth(torch, cb, lib, h, dev, g, routines=None):
         rec("sgemv_n", 4 * (m * m + m + 2 * m), timed_calls(lambda: cb.sgemv(0, m, m, 1.5, A, m, xv, 1, 0.5, yv, 1), 20, False))
     if want("sgemv_t"):
         rec("sgemv_t", 4 * (m * m + m + 2 * m), timed_calls(lambda: cb.sgemv(1, m, m, 1.5, A, m, xv, 1, 0.5, yv, 1), 20, False))
+    # double / complex GEMV at 8192 x 8192 (A: 512 MiB, 512 MiB, 1 GiB)
+    for dt, fn, nm, es in ((torch.float64, cb.dgemv, "dgemv", 8), (torch.complex64, cb.cgemv, "cgemv", 8),
+                           (torch.complex128, cb.zgemv, "zgemv", 16)):
+        ops = (("n", 0), ("t", 1)) if nm == "dgemv" else (("n", 0), ("c", 2))
+        if not any(want(f"{nm}_{o}") for o, _ in ops):
+            continue
+        Ax = torch.empty(m * m, dtype=dt, device=dev)
+        (Ax.real if dt.is_complex else Ax).uniform_(-1, 1, generator=g)
+        if dt.is_complex:
+            Ax.imag.uniform_(-1, 1, generator=g)
+        xx = torch.ones(m, dtype=dt, device=dev)
+        yx = torch.ones(m, dtype=dt, device=dev)
+        al, be = (1.5, 0.5) if nm == "dgemv" else (1.5 - 0.25j, 0.5 + 0.0j)
+        for o, tr in ops:
+            if want(f"{nm}_{o}"):
+                rec(f"{nm}_{o}", es * (m * m + m + 2 * m),
+                    timed_calls(lambda: fn(tr, m, m, al, Ax, m, xx, 1, be, yx, 1), 20, False))
+        del Ax, xx, yx
     if want("ssymv_upper"):
         rec("ssymv_upper", 4 * (m * (m + 1) // 2 + 3 * m),
             timed_calls(lambda: cb.ssymv(0, m, 1.5, A, m, xv, 1, 0.5, yv, 1), 20, False))

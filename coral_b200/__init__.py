@@ -9,7 +9,7 @@ from .blas import (  # noqa: F401
     CoralDiagonal, CoralError, CoralTranspose, CoralTriangular, GemmMode, Handle, cgemm,
     chemv, dgemm, gemm_mode, handle, isamax, saxpy, scopy, sdot, set_gemm_mode, sgemm, sgemv,
     sger, snrm2, sscal, sswap, ssymv, ssyr, ssyr2, strmv, strsv, zgemm, sgemm_grouped,
-    strsv_batched, sgemm_problem_dtype, strsv_problem_dtype,
+    strsv_batched, sgemm_problem_dtype, strsv_problem_dtype, dgemv, cgemv, zgemv,
 )
 
 __all__ = [
@@ -17,5 +17,5 @@ __all__ = [
     "cgemm", "chemv", "dgemm", "gemm_mode", "handle", "isamax", "saxpy", "scopy", "sdot",
     "set_gemm_mode", "sgemm", "sgemv", "sger", "snrm2", "sscal", "sswap", "ssymv", "ssyr",
     "ssyr2", "strmv", "strsv", "zgemm", "sgemm_grouped", "strsv_batched", "sgemm_problem_dtype",
-    "strsv_problem_dtype",
+    "strsv_problem_dtype", "dgemv", "cgemv", "zgemv",
 ]

@@ -52,6 +52,9 @@ SIGNATURES = {
     "coral_sswap": [_h, _sz, _vp, _sz, _vp, _sz],
     "coral_sscal": [_h, _sz, _f, _vp, _sz],
     "coral_sgemv": [_h, _i, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
+    "coral_dgemv": [_h, _i, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz],
+    "coral_cgemv": [_h, _i, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
+    "coral_zgemv": [_h, _i, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
     "coral_ssymv": [_h, _i, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
     "coral_chemv": [_h, _i, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
     "coral_strsv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],

@@ -226,6 +226,32 @@ def sgemv(trans, n_rows, n_cols, alpha, matrix, lda, x, incx, beta, y, incy) -> 
                   lda, _ptr(x, _f32(), "x"), incx, beta, _ptr(y, _f32(), "y"), incy)
 
 
+def dgemv(trans, n_rows, n_cols, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
+    """level2/dgemv.rs."""
+    handle().call("coral_dgemv", int(trans), n_rows, n_cols, float(alpha), _ptr(matrix, _f64(), "matrix"),
+                  lda, _ptr(x, _f64(), "x"), incx, float(beta), _ptr(y, _f64(), "y"), incy)
+
+
+def _cscalar(z):
+    return complex(z[0], z[1]) if isinstance(z, (list, tuple)) else complex(z)
+
+
+def cgemv(trans, n_rows, n_cols, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
+    """level2/cgemv.rs:60-80 (alpha/beta: complex or [re, im])."""
+    pa, ka = _pair(_cscalar(alpha), C.c_float)
+    pb, kb = _pair(_cscalar(beta), C.c_float)
+    handle().call("coral_cgemv", int(trans), n_rows, n_cols, pa, _ptr(matrix, _c64(), "matrix"), lda,
+                  _ptr(x, _c64(), "x"), incx, pb, _ptr(y, _c64(), "y"), incy)
+
+
+def zgemv(trans, n_rows, n_cols, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
+    """level2/zgemv.rs (alpha/beta: complex or [re, im])."""
+    pa, ka = _pair(_cscalar(alpha), C.c_double)
+    pb, kb = _pair(_cscalar(beta), C.c_double)
+    handle().call("coral_zgemv", int(trans), n_rows, n_cols, pa, _ptr(matrix, _c128(), "matrix"), lda,
+                  _ptr(x, _c128(), "x"), incx, pb, _ptr(y, _c128(), "y"), incy)
+
+
 def ssymv(uplo, n, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
     """level2/ssymv.rs:99-394."""
     handle().call("coral_ssymv", int(uplo), n, alpha, _ptr(matrix, _f32(), "matrix"), lda,

@@ -132,6 +132,23 @@ coral_status_t coral_sgemv(coral_handle_t h, int trans, size_t n_rows, size_t n_
                            float alpha, const float* matrix, size_t lda,
                            const float* x, size_t incx, float beta, float* y,
                            size_t incy);
+/* dgemv.rs (dgemv_notranspose.rs / dgemv_transpose.rs) -- same arguments as
+ * sgemv in double; ConjugateTranspose == Transpose */
+coral_status_t coral_dgemv(coral_handle_t h, int trans, size_t n_rows, size_t n_cols,
+                           double alpha, const double* matrix, size_t lda,
+                           const double* x, size_t incx, double beta, double* y,
+                           size_t incy);
+/* cgemv.rs:60-80 -- interleaved complex64, ld/inc in complex units; trans
+ * N, T or C (conjugate transpose) */
+coral_status_t coral_cgemv(coral_handle_t h, int trans, size_t n_rows, size_t n_cols,
+                           const float alpha[2], const float* matrix, size_t lda,
+                           const float* x, size_t incx, const float beta[2], float* y,
+                           size_t incy);
+/* zgemv.rs -- interleaved complex128, as cgemv */
+coral_status_t coral_zgemv(coral_handle_t h, int trans, size_t n_rows, size_t n_cols,
+                           const double alpha[2], const double* matrix, size_t lda,
+                           const double* x, size_t incx, const double beta[2], double* y,
+                           size_t incy);
 /* ssymv.rs:99-110 */
 coral_status_t coral_ssymv(coral_handle_t h, int uplo, size_t n, float alpha,
                            const float* matrix, size_t lda, const float* x,

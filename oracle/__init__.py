@@ -62,6 +62,9 @@ def _declare(L: C.CDLL) -> None:
     L.or_sgemv_f64.argtypes = [_i, _sz, _sz, C.c_float, _fp, _sz, _fp, _sz, C.c_float, _fp, _sz, _dp]
     L.or_ssymv_f64.argtypes = [_i, _sz, C.c_float, _fp, _sz, _fp, _sz, C.c_float, _fp, _sz, _dp]
     L.or_chemv_f64.argtypes = [_i, _sz, _fp, _fp, _sz, _fp, _sz, _fp, _fp, _sz, _dp]
+    L.or_dgemv_f64.argtypes = [_i, _sz, _sz, C.c_double, _dp, _sz, _dp, _sz, C.c_double, _dp, _sz, _dp]
+    L.or_cgemv_f64.argtypes = [_i, _sz, _sz, _fp, _fp, _sz, _fp, _sz, _fp, _fp, _sz, _dp]
+    L.or_zgemv_f64.argtypes = [_i, _sz, _sz, _dp, _dp, _sz, _dp, _sz, _dp, _dp, _sz, _dp]
     L.or_strsv_f64.argtypes = [_i, _i, _i, _sz, _fp, _sz, _fp, _sz, _dp]
     L.or_strmv_f64.argtypes = [_i, _i, _i, _sz, _fp, _sz, _fp, _sz, _dp]
     L.or_sger_exact.argtypes = [_sz, _sz, C.c_float, _fp, _sz, _fp, _sz, _fp, _sz]
@@ -133,6 +136,38 @@ def sgemv(trans, m, n, alpha, a, lda, x, incx, beta, y, incy) -> np.ndarray:
     out = np.zeros(max(ylen, 1), np.float64)
     lib().or_sgemv_f64(trans, m, n, alpha, _f(a), lda, _f(x), incx, beta, _f(y), incy, _d(out))
     return out[:ylen]
+
+
+def dgemv(trans, m, n, alpha, a, lda, x, incx, beta, y, incy) -> np.ndarray:
+    """dgemv result y (float64, contiguous length of y)."""
+    ylen = n if trans else m
+    out = np.zeros(max(ylen, 1), np.float64)
+    lib().or_dgemv_f64(trans, m, n, C.c_double(alpha), _d(np.ascontiguousarray(a, np.float64)), lda,
+                       _d(np.ascontiguousarray(x, np.float64)), incx, C.c_double(beta),
+                       _d(np.ascontiguousarray(y, np.float64)), incy, _d(out))
+    return out[:ylen]
+
+
+def cgemv(trans, m, n, alpha, a, lda, x, incx, beta, y, incy) -> np.ndarray:
+    """cgemv result y as complex128 (inputs complex64 or interleaved float32)."""
+    ylen = n if trans else m
+    out = np.zeros(2 * max(ylen, 1), np.float64)
+    al = np.array([complex(alpha).real, complex(alpha).imag], np.float32)
+    be = np.array([complex(beta).real, complex(beta).imag], np.float32)
+    f = lambda v: _f(np.ascontiguousarray(v, np.complex64).view(np.float32))  # noqa: E731
+    lib().or_cgemv_f64(trans, m, n, _f(al), f(a), lda, f(x), incx, _f(be), f(y), incy, _d(out))
+    return out.view(np.complex128)[:ylen]
+
+
+def zgemv(trans, m, n, alpha, a, lda, x, incx, beta, y, incy) -> np.ndarray:
+    """zgemv result y as complex128."""
+    ylen = n if trans else m
+    out = np.zeros(2 * max(ylen, 1), np.float64)
+    al = np.array([complex(alpha).real, complex(alpha).imag], np.float64)
+    be = np.array([complex(beta).real, complex(beta).imag], np.float64)
+    f = lambda v: _d(np.ascontiguousarray(v, np.complex128).view(np.float64))  # noqa: E731
+    lib().or_zgemv_f64(trans, m, n, _d(al), f(a), lda, f(x), incx, _d(be), f(y), incy, _d(out))
+    return out.view(np.complex128)[:ylen]
 
 
 def ssymv(uplo, n, alpha, a, lda, x, incx, beta, y, incy) -> np.ndarray:

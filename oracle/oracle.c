@@ -144,6 +144,89 @@ void or_sgemv_f64(int trans, size_t m, size_t n, float alpha, const float* A, si
   free(xs);
 }
 
+/* level2/dgemv_notranspose.rs, dgemv_transpose.rs: the sgemv order in
+ * double -- empty matrix or (alpha == 0 && beta == 1) -> no-op; beta != 1 ->
+ * y *= beta (dscal: a multiplication, so 0 * NaN stays NaN); alpha == 0 ->
+ * done; xs = alpha * x; y += op(A) xs, summed in double-double. */
+void or_dgemv_f64(int trans, size_t m, size_t n, double alpha, const double* A, size_t lda,
+                  const double* x, size_t incx, double beta, const double* y, size_t incy,
+                  double* y_out) {
+  const int t = trans != NOTRANS;
+  const size_t ylen = t ? n : m, xlen = t ? m : n;
+  for (size_t i = 0; i < ylen; ++i) y_out[i] = y[i * incy];
+  if (m == 0 || n == 0) return;
+  if (alpha == 0.0 && beta == 1.0) return;
+  if (beta != 1.0)
+    for (size_t i = 0; i < ylen; ++i) y_out[i] = y[i * incy] * beta;
+  if (alpha == 0.0) return;
+  double* xs = (double*)malloc(sizeof(double) * (xlen ? xlen : 1));
+  for (size_t j = 0; j < xlen; ++j) xs[j] = alpha * x[j * incx];
+  for (size_t i = 0; i < ylen; ++i) {
+    dd acc = {0.0, 0.0};
+    for (size_t j = 0; j < xlen; ++j) acc = dd_add_prod(acc, t ? A[j + i * lda] : A[i + j * lda], xs[j]);
+    y_out[i] += dd_val(acc);
+  }
+  free(xs);
+}
+
+/* level2/cgemv_*.rs and zgemv_*.rs (zgemv_notranspose.rs:76-101): empty or
+ * (alpha == 0 && beta == 1) -> no-op; beta != 1 -> y *= beta in the element
+ * precision, by csscal/zdscal when Im(beta) == 0 (both parts times Re(beta))
+ * and cscal/zscal otherwise; alpha == 0 -> done; xs = alpha * x in the
+ * element precision; y += op(A) xs with op N, T or C (conjugated A), summed
+ * in double-double.  Interleaved (re, im); ld and inc in complex units. */
+#define OR_CGEMV_BODY(R)                                                                     \
+  const int t = trans != NOTRANS, cj = trans == CONJTRANS;                                   \
+  const size_t ylen = t ? n : m, xlen = t ? m : n;                                           \
+  for (size_t i = 0; i < ylen; ++i) {                                                        \
+    y_out[2 * i] = y[2 * i * incy];                                                          \
+    y_out[2 * i + 1] = y[2 * i * incy + 1];                                                  \
+  }                                                                                          \
+  if (m == 0 || n == 0) return;                                                              \
+  if (alpha[0] == 0 && alpha[1] == 0 && beta[0] == 1 && beta[1] == 0) return;                \
+  if (!(beta[0] == 1 && beta[1] == 0))                                                       \
+    for (size_t i = 0; i < ylen; ++i) {                                                      \
+      R yr = y[2 * i * incy], yi = y[2 * i * incy + 1];                                      \
+      if (beta[1] == 0) { y_out[2 * i] = (R)(yr * beta[0]); y_out[2 * i + 1] = (R)(yi * beta[0]); } \
+      else {                                                                                 \
+        y_out[2 * i] = (R)(beta[0] * yr - beta[1] * yi);                                     \
+        y_out[2 * i + 1] = (R)(beta[0] * yi + beta[1] * yr);                                 \
+      }                                                                                      \
+    }                                                                                        \
+  if (alpha[0] == 0 && alpha[1] == 0) return;                                                \
+  R* xs = (R*)malloc(sizeof(R) * 2 * (xlen ? xlen : 1));                                     \
+  for (size_t j = 0; j < xlen; ++j) {                                                        \
+    R xr = x[2 * j * incx], xi = x[2 * j * incx + 1];                                        \
+    xs[2 * j] = alpha[0] * xr - alpha[1] * xi;                                               \
+    xs[2 * j + 1] = alpha[0] * xi + alpha[1] * xr;                                           \
+  }                                                                                          \
+  for (size_t i = 0; i < ylen; ++i) {                                                        \
+    dd re = {0.0, 0.0}, im = {0.0, 0.0};                                                     \
+    for (size_t j = 0; j < xlen; ++j) {                                                      \
+      size_t e = t ? j + i * lda : i + j * lda;                                              \
+      double ar = A[2 * e], ai = cj ? -(double)A[2 * e + 1] : (double)A[2 * e + 1];          \
+      re = dd_add_prod(re, ar, xs[2 * j]);                                                   \
+      re = dd_add_prod(re, -ai, xs[2 * j + 1]);                                              \
+      im = dd_add_prod(im, ar, xs[2 * j + 1]);                                               \
+      im = dd_add_prod(im, ai, xs[2 * j]);                                                   \
+    }                                                                                        \
+    y_out[2 * i] += dd_val(re);                                                              \
+    y_out[2 * i + 1] += dd_val(im);                                                          \
+  }                                                                                          \
+  free(xs);
+
+void or_cgemv_f64(int trans, size_t m, size_t n, const float alpha[2], const float* A, size_t lda,
+                  const float* x, size_t incx, const float beta[2], const float* y, size_t incy,
+                  double* y_out) {
+  OR_CGEMV_BODY(float)
+}
+
+void or_zgemv_f64(int trans, size_t m, size_t n, const double alpha[2], const double* A, size_t lda,
+                  const double* x, size_t incx, const double beta[2], const double* y, size_t incy,
+                  double* y_out) {
+  OR_CGEMV_BODY(double)
+}
+
 /* level2/ssymv.rs:99-394: n == 0 or (alpha == 0 && beta == 1) -> no-op;
  * x scaled by alpha in fp32; beta == 0 -> y = 0 (fill), beta != 1 -> y *= beta;
  * only the `uplo` triangle of A is referenced. */
