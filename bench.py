@@ -486,6 +486,23 @@ def level12_bandwidth(torch, cb, lib, h, dev, g, routines=None):
                 rec(f"{nm}_{o}", es * (m * m + m + 2 * m),
                     timed_calls(lambda: fn(tr, m, m, al, Ax, m, xx, 1, be, yx, 1), 20, False))
         del Ax, xx, yx
+    if want("dsymv_upper"):
+        Ad = torch.empty(m * m, dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
+        xd = torch.ones(m, dtype=torch.float64, device=dev)
+        yd = torch.ones(m, dtype=torch.float64, device=dev)
+        rec("dsymv_upper", 8 * (m * (m + 1) // 2 + 3 * m),
+            timed_calls(lambda: cb.dsymv(0, m, 1.5, Ad, m, xd, 1, 0.5, yd, 1), 20, False))
+        del Ad, xd, yd
+    if want("zhemv_upper"):
+        nz = 4096
+        Az = torch.empty(nz * nz, dtype=torch.complex128, device=dev)
+        Az.real.uniform_(-1, 1, generator=g)
+        Az.imag.uniform_(-1, 1, generator=g)
+        xz = torch.ones(nz, dtype=torch.complex128, device=dev)
+        yz = torch.ones(nz, dtype=torch.complex128, device=dev)
+        rec("zhemv_upper", 16 * (nz * (nz + 1) // 2 + 3 * nz),
+            timed_calls(lambda: cb.zhemv(0, nz, 1.5 - 0.5j, Az, nz, xz, 1, 0.25 + 0.0j, yz, 1), 20, False))
+        del Az, xz, yz
     if want("ssymv_upper"):
         rec("ssymv_upper", 4 * (m * (m + 1) // 2 + 3 * m),
             timed_calls(lambda: cb.ssymv(0, m, 1.5, A, m, xv, 1, 0.5, yv, 1), 20, False))

@@ -10,6 +10,7 @@ from .blas import (  # noqa: F401
     chemv, dgemm, gemm_mode, handle, isamax, saxpy, scopy, sdot, set_gemm_mode, sgemm, sgemv,
     sger, snrm2, sscal, sswap, ssymv, ssyr, ssyr2, strmv, strsv, zgemm, sgemm_grouped,
     strsv_batched, sgemm_problem_dtype, strsv_problem_dtype, dgemv, cgemv, zgemv,
+    dsymv, zhemv, dtrmv, ctrmv, ztrmv,
 )
 
 __all__ = [
@@ -18,4 +19,5 @@ __all__ = [
     "set_gemm_mode", "sgemm", "sgemv", "sger", "snrm2", "sscal", "sswap", "ssymv", "ssyr",
     "ssyr2", "strmv", "strsv", "zgemm", "sgemm_grouped", "strsv_batched", "sgemm_problem_dtype",
     "strsv_problem_dtype", "dgemv", "cgemv", "zgemv",
+    "dsymv", "zhemv", "dtrmv", "ctrmv", "ztrmv",
 ]

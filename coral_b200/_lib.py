@@ -55,6 +55,11 @@ SIGNATURES = {
     "coral_dgemv": [_h, _i, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz],
     "coral_cgemv": [_h, _i, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
     "coral_zgemv": [_h, _i, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
+    "coral_dsymv": [_h, _i, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz],
+    "coral_zhemv": [_h, _i, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
+    "coral_dtrmv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],
+    "coral_ctrmv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],
+    "coral_ztrmv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],
     "coral_ssymv": [_h, _i, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
     "coral_chemv": [_h, _i, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
     "coral_strsv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],

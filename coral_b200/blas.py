@@ -252,6 +252,38 @@ def zgemv(trans, n_rows, n_cols, alpha, matrix, lda, x, incx, beta, y, incy) -> 
                   _ptr(x, _c128(), "x"), incx, pb, _ptr(y, _c128(), "y"), incy)
 
 
+def dsymv(uplo, n, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
+    """level2/dsymv.rs:99-210."""
+    handle().call("coral_dsymv", int(uplo), n, float(alpha), _ptr(matrix, _f64(), "matrix"), lda,
+                  _ptr(x, _f64(), "x"), incx, float(beta), _ptr(y, _f64(), "y"), incy)
+
+
+def zhemv(uplo, n, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
+    """level2/zhemv.rs:96-230 (alpha/beta: complex or [re, im])."""
+    pa, ka = _pair(_cscalar(alpha), C.c_double)
+    pb, kb = _pair(_cscalar(beta), C.c_double)
+    handle().call("coral_zhemv", int(uplo), n, pa, _ptr(matrix, _c128(), "matrix"), lda,
+                  _ptr(x, _c128(), "x"), incx, pb, _ptr(y, _c128(), "y"), incy)
+
+
+def dtrmv(uplo, transpose, diagonal, n, matrix, lda, x, incx) -> None:
+    """level2/dtrmv.rs (x overwritten with op(A) x)."""
+    handle().call("coral_dtrmv", int(uplo), int(transpose), int(diagonal), n,
+                  _ptr(matrix, _f64(), "matrix"), lda, _ptr(x, _f64(), "x"), incx)
+
+
+def ctrmv(uplo, transpose, diagonal, n, matrix, lda, x, incx) -> None:
+    """level2/ctrmv.rs:58-72."""
+    handle().call("coral_ctrmv", int(uplo), int(transpose), int(diagonal), n,
+                  _ptr(matrix, _c64(), "matrix"), lda, _ptr(x, _c64(), "x"), incx)
+
+
+def ztrmv(uplo, transpose, diagonal, n, matrix, lda, x, incx) -> None:
+    """level2/ztrmv.rs."""
+    handle().call("coral_ztrmv", int(uplo), int(transpose), int(diagonal), n,
+                  _ptr(matrix, _c128(), "matrix"), lda, _ptr(x, _c128(), "x"), incx)
+
+
 def ssymv(uplo, n, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
     """level2/ssymv.rs:99-394."""
     handle().call("coral_ssymv", int(uplo), n, alpha, _ptr(matrix, _f32(), "matrix"), lda,

@@ -18,6 +18,8 @@
 //     ssymv.rs:137-141) or writes x (TRMV).  Results are deterministic.
 #include "common.cuh"
 
+#include <type_traits>
+
 namespace coral {
 namespace {
 
@@ -25,19 +27,50 @@ constexpr int kT = 64;        // tile edge
 constexpr int kSeg = 8;       // tiles per CTA run
 constexpr int kTriThreads = 256;
 
-enum TriMode { kSymv = 0, kHemv = 1, kTrmvN = 2, kTrmvT = 3 };
+enum TriMode { kSymv = 0, kHemv = 1, kTrmvN = 2, kTrmvT = 3, kTrmvC = 4 };
+// Mode traits: which parts a mode uses, and whether the column part (the
+// transposed use of a stored element) conjugates it.
+template <int kMode> struct ModeT {
+  static constexpr bool kSym = kMode == kSymv || kMode == kHemv;
+  static constexpr bool kTr = kMode == kTrmvN || kMode == kTrmvT || kMode == kTrmvC;
+  static constexpr bool kColOnly = kMode == kTrmvT || kMode == kTrmvC;
+  static constexpr bool kRow = !kColOnly;
+  static constexpr bool kCol = kSym || kColOnly;
+  static constexpr bool kConjCol = kMode == kHemv || kMode == kTrmvC;
+};
 
 template <typename T> struct Cx;
 template <> struct Cx<float> {
-  static __device__ __forceinline__ float zero() { return 0.f; }
+  static __host__ __device__ __forceinline__ float zero() { return 0.f; }
   static __device__ __forceinline__ float conj(float a) { return a; }
   static __device__ __forceinline__ float re(float a) { return a; }
   static __device__ __forceinline__ void mac(float& c, float a, float b) { c = fmaf(a, b, c); }
   static __device__ __forceinline__ float add(float a, float b) { return a + b; }
-  static __device__ __forceinline__ float one() { return 1.f; }
+  static __host__ __device__ __forceinline__ float one() { return 1.f; }
+};
+template <> struct Cx<double> {
+  static __host__ __device__ __forceinline__ double zero() { return 0.0; }
+  static __device__ __forceinline__ double conj(double a) { return a; }
+  static __device__ __forceinline__ double re(double a) { return a; }
+  static __device__ __forceinline__ void mac(double& c, double a, double b) { c = fma(a, b, c); }
+  static __device__ __forceinline__ double add(double a, double b) { return a + b; }
+  static __host__ __device__ __forceinline__ double one() { return 1.0; }
+};
+template <> struct Cx<double2> {
+  static __host__ __device__ __forceinline__ double2 zero() { return make_double2(0.0, 0.0); }
+  static __device__ __forceinline__ double2 conj(double2 a) { return make_double2(a.x, -a.y); }
+  static __device__ __forceinline__ double2 re(double2 a) { return make_double2(a.x, 0.0); }
+  static __device__ __forceinline__ void mac(double2& c, double2 a, double2 b) {
+    c.x = fma(a.x, b.x, c.x);
+    c.x = fma(-a.y, b.y, c.x);
+    c.y = fma(a.x, b.y, c.y);
+    c.y = fma(a.y, b.x, c.y);
+  }
+  static __device__ __forceinline__ double2 add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+  static __host__ __device__ __forceinline__ double2 one() { return make_double2(1.0, 0.0); }
 };
 template <> struct Cx<float2> {
-  static __device__ __forceinline__ float2 zero() { return make_float2(0.f, 0.f); }
+  static __host__ __device__ __forceinline__ float2 zero() { return make_float2(0.f, 0.f); }
   static __device__ __forceinline__ float2 conj(float2 a) { return make_float2(a.x, -a.y); }
   static __device__ __forceinline__ float2 re(float2 a) { return make_float2(a.x, 0.f); }
   static __device__ __forceinline__ void mac(float2& c, float2 a, float2 b) {
@@ -47,10 +80,14 @@ template <> struct Cx<float2> {
     c.y = fmaf(a.y, b.x, c.y);
   }
   static __device__ __forceinline__ float2 add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-  static __device__ __forceinline__ float2 one() { return make_float2(1.f, 0.f); }
+  static __host__ __device__ __forceinline__ float2 one() { return make_float2(1.f, 0.f); }
 };
 
 __device__ __forceinline__ float scale_x(float alpha, float x) { return alpha * x; }
+__device__ __forceinline__ double scale_x(double alpha, double x) { return alpha * x; }
+__device__ __forceinline__ double2 scale_x(double2 alpha, double2 x) {
+  return make_double2(alpha.x * x.x - alpha.y * x.y, alpha.x * x.y + alpha.y * x.x);
+}
 __device__ __forceinline__ float2 scale_x(float2 alpha, float2 x) {
   return make_float2(alpha.x * x.x - alpha.y * x.y, alpha.x * x.y + alpha.y * x.x);
 }
@@ -65,10 +102,12 @@ __global__ void __launch_bounds__(kTriThreads)
 k_tri_tiles(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x, size_t incx,
             T alpha, bool lower, bool unit, T* __restrict__ rowpart, T* __restrict__ colpart,
             int max_seg, int diag_only) {
-  constexpr bool kSym = kMode == kSymv || kMode == kHemv;
-  constexpr bool kRow = kMode != kTrmvT;
-  constexpr bool kCol = kMode == kSymv || kMode == kHemv || kMode == kTrmvT;
-  __shared__ T tile[kT][kT + 1];   // tile[c][r] = element (row r, col c)
+  constexpr bool kSym = ModeT<kMode>::kSym;
+  constexpr bool kRow = ModeT<kMode>::kRow;
+  constexpr bool kCol = ModeT<kMode>::kCol;
+  // tile[c][r] = element (row r, col c); dynamic, as complex128 tiles pass 48 KB
+  extern __shared__ __align__(16) unsigned char tile_raw[];
+  T(*tile)[kT + 1] = reinterpret_cast<T(*)[kT + 1]>(tile_raw);
   __shared__ T vJ[kT], vI[kT];
   __shared__ T red[4][kT];
 
@@ -128,7 +167,7 @@ k_tri_tiles(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x,
         const bool stored = lower ? rr >= cc : rr <= cc;
         if (rr == cc) {
           if (kMode == kHemv) tile[cc][rr] = Cx<T>::re(tile[cc][rr]);
-          if ((kMode == kTrmvN || kMode == kTrmvT) && unit) tile[cc][rr] = Cx<T>::one();
+          if (ModeT<kMode>::kTr && unit) tile[cc][rr] = Cx<T>::one();
         } else if (!stored) {
           if (kSym) {
             // unstored (rr, cc) = stored (cc, rr), conjugated for HEMV; read
@@ -151,11 +190,11 @@ k_tri_tiles(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x,
     }
     // Column part (off-diagonal tiles for SYMV/HEMV; every tile for TRMV T):
     // out[c = r] += sum_rr conj?(tile(rr, c)) * vI[rr], quarter q of the rows.
-    if (kCol && (!diag || kMode == kTrmvT)) {
+    if (kCol && (!diag || ModeT<kMode>::kColOnly)) {
 #pragma unroll
       for (int rr = q * 16; rr < q * 16 + 16; ++rr) {
         T a = tile[r][rr];
-        Cx<T>::mac(colacc, kMode == kHemv ? Cx<T>::conj(a) : a, vI[rr]);
+        Cx<T>::mac(colacc, ModeT<kMode>::kConjCol ? Cx<T>::conj(a) : a, vI[rr]);
       }
     }
     __syncthreads();
@@ -177,6 +216,14 @@ k_tri_tiles(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x,
 
 __device__ __forceinline__ float beta_apply(float beta, float y) {
   return beta == 0.f ? 0.f : (beta != 1.f ? y * beta : y);
+}
+__device__ __forceinline__ double beta_apply(double beta, double y) {
+  return beta == 0.0 ? 0.0 : (beta != 1.0 ? y * beta : y);
+}
+__device__ __forceinline__ double2 beta_apply(double2 beta, double2 y) {
+  if (beta.x == 0.0 && beta.y == 0.0) return make_double2(0.0, 0.0);
+  if (beta.x == 1.0 && beta.y == 0.0) return y;
+  return make_double2(y.x * beta.x - y.y * beta.y, y.x * beta.y + y.y * beta.x);
 }
 __device__ __forceinline__ float2 beta_apply(float2 beta, float2 y) {
   if (beta.x == 0.f && beta.y == 0.f) return make_float2(0.f, 0.f);
@@ -200,6 +247,12 @@ __device__ __forceinline__ T shfl_xor_t(T v, int o);
 template <> __device__ __forceinline__ float shfl_xor_t<float>(float v, int o) {
   return __shfl_xor_sync(0xffffffffu, v, o);
 }
+template <> __device__ __forceinline__ double shfl_xor_t<double>(double v, int o) {
+  return __shfl_xor_sync(0xffffffffu, v, o);
+}
+template <> __device__ __forceinline__ double2 shfl_xor_t<double2>(double2 v, int o) {
+  return make_double2(__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o));
+}
 template <> __device__ __forceinline__ float2 shfl_xor_t<float2>(float2 v, int o) {
   return make_float2(__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o));
 }
@@ -220,20 +273,24 @@ template <> struct Vec<float, 4> {
   using type = float4;
   static __device__ __forceinline__ void split(const float4& v, float (&o)[4]) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; }
 };
+template <> struct Vec<double, 2> {
+  using type = double2;
+  static __device__ __forceinline__ void split(const double2& v, double (&o)[2]) { o[0] = v.x; o[1] = v.y; }
+};
 template <> struct Vec<float2, 2> {
   using type = float4;
   static __device__ __forceinline__ void split(const float4& v, float2 (&o)[2]) { o[0] = make_float2(v.x, v.y); o[1] = make_float2(v.z, v.w); }
 };
 
 template <typename T, int kMode, int V>
-__global__ void __launch_bounds__(32 * kStripWarps, 4)
+__global__ void __launch_bounds__(32 * kStripWarps, sizeof(T) >= 16 ? 3 : 4)
 k_tri_strips(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x, size_t incx,
              T alpha, bool lower, T* __restrict__ rowpart, T* __restrict__ colpart, int nsplit) {
   constexpr int kS = 32 * V;                 // strip height
   constexpr int kP = 16;                     // columns per pass
-  constexpr bool kSym = kMode == kSymv || kMode == kHemv;
-  constexpr bool kRow = kMode != kTrmvT;
-  constexpr bool kCol = kMode == kSymv || kMode == kHemv || kMode == kTrmvT;
+  constexpr bool kSym = ModeT<kMode>::kSym;
+  constexpr bool kRow = ModeT<kMode>::kRow;
+  constexpr bool kCol = ModeT<kMode>::kCol;
   __shared__ T vJ[kC];
   __shared__ T red[kStripWarps][kC];
   const int J = blockIdx.x;
@@ -310,7 +367,8 @@ k_tri_strips(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x
         for (int c = 0; c < kP; ++c) {
           v[c] = Cx<T>::zero();
 #pragma unroll
-          for (int e = 0; e < V; ++e) Cx<T>::mac(v[c], kMode == kHemv ? Cx<T>::conj(a[c][e]) : a[c][e], xi[e]);
+          for (int e = 0; e < V; ++e)
+            Cx<T>::mac(v[c], ModeT<kMode>::kConjCol ? Cx<T>::conj(a[c][e]) : a[c][e], xi[e]);
         }
         butterfly<8>(v, lane, 16);
         butterfly<4>(v, lane, 8);
@@ -347,8 +405,8 @@ k_strip_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
                 const T* __restrict__ rowpart, const T* __restrict__ colpart, int ncolblk,
                 int nsplit, const T* __restrict__ drow, const T* __restrict__ dcol) {
   constexpr int kS = 32 * V;
-  constexpr bool kRow = kMode != kTrmvT;
-  constexpr bool kCol = kMode == kSymv || kMode == kHemv || kMode == kTrmvT;
+  constexpr bool kRow = ModeT<kMode>::kRow;
+  constexpr bool kCol = ModeT<kMode>::kCol;
   __shared__ T part[kCombineGroups][32];
   const int g = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gr = blockIdx.x * 32 + lane;
@@ -379,9 +437,9 @@ k_strip_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
 #pragma unroll
   for (int q = 1; q < kCombineGroups; ++q) t = Cx<T>::add(t, part[q][lane]);
   if (kRow) t = Cx<T>::add(t, drow[gr]);
-  if (kMode == kTrmvT) t = Cx<T>::add(t, dcol[gr]);
+  if (ModeT<kMode>::kColOnly) t = Cx<T>::add(t, dcol[gr]);
   T* yp = y + (size_t)gr * incy;
-  if (kMode == kTrmvN || kMode == kTrmvT) *yp = t;
+  if (ModeT<kMode>::kTr) *yp = t;
   else *yp = Cx<T>::add(beta_apply(beta, *yp), t);
 }
 
@@ -407,7 +465,17 @@ coral_status_t launch_strips(Handle* h, int n, const T* A, size_t lda, const T* 
   // handle's side stream, forked from and joined back into the main stream.
   CORAL_CUDA(h, cudaEventRecord(h->fork_event, h->stream));
   CORAL_CUDA(h, cudaStreamWaitEvent(h->side_stream, h->fork_event, 0));
-  k_tri_tiles<T, kMode><<<dim3(NT, 1), kTriThreads, 0, h->side_stream>>>(n, A, lda, x, incx, alpha,
+  constexpr size_t kTileSmem = (size_t)kT * (kT + 1) * sizeof(T);
+  if (kTileSmem > 48 * 1024) {
+    static uint64_t attr_devices = 0;  // bit d: attribute set on device d
+    const uint64_t bit = h->device < 64 ? (1ull << h->device) : 0;
+    if (!(attr_devices & bit) || !bit) {
+      CORAL_CUDA(h, cudaFuncSetAttribute(k_tri_tiles<T, kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTileSmem));
+      attr_devices |= bit;
+    }
+  }
+  k_tri_tiles<T, kMode><<<dim3(NT, 1), kTriThreads, kTileSmem, h->side_stream>>>(n, A, lda, x, incx, alpha,
                                                                          lower, unit, drow, dcol, 1, 1);
   coral_status_t s = launch_status(h);
   if (s != CORAL_OK) return s;
@@ -428,7 +496,7 @@ template <typename T, int kMode>
 coral_status_t run_tri_strips(Handle* h, int n, const T* A, size_t lda, const T* x, size_t incx,
                               T alpha, T beta, T* y, size_t incy, bool lower, bool unit) {
   static_assert(kC == kT, "diagonal tiles are as wide as the tile columns");
-  constexpr int V = sizeof(T) == 4 ? 4 : 2;
+  constexpr int V = (int)(16 / sizeof(T));  // one 16-byte vector per lane and column
   const bool vec = aligned16(A) && (lda * sizeof(T)) % 16 == 0;
   if (vec) return launch_strips<T, kMode, V>(h, n, A, lda, x, incx, alpha, beta, y, incy, lower, unit);
   return launch_strips<T, kMode, 1>(h, n, A, lda, x, incx, alpha, beta, y, incy, lower, unit);
@@ -500,4 +568,97 @@ coral_status_t coral_strmv(coral_handle_t hh, int uplo, int trans, int diag, siz
   return run_tri_strips<float, kTrmvT>(H, (int)n, matrix, lda, x, incx, 1.f, 0.f, x, incx, lower, unit);
 }
 
+// dsymv.rs:99-210: the ssymv order in double.
+coral_status_t coral_dsymv(coral_handle_t hh, int uplo, size_t n, double alpha, const double* matrix,
+                           size_t lda, const double* x, size_t incx, double beta, double* y,
+                           size_t incy) {
+  CORAL_HANDLE(hh);
+  if (uplo != CORAL_UPPER && uplo != CORAL_LOWER) return bad_arg(H, 1);
+  if (n == 0) return CORAL_OK;                          // dsymv.rs:112
+  if (alpha == 0.0 && beta == 1.0) return CORAL_OK;     // dsymv.rs:113
+  if (!matrix) return bad_arg(H, 4);
+  if (lda < n) return bad_arg(H, 5);
+  if (!x) return bad_arg(H, 6);
+  if (incx == 0) return bad_arg(H, 7);
+  if (!y) return bad_arg(H, 9);
+  if (incy == 0) return bad_arg(H, 10);
+  if (((uintptr_t)matrix | (uintptr_t)x | (uintptr_t)y) & 7) return bad_arg(H, 4);
+  if (n > (size_t)(1 << 20)) return CORAL_ERR_NOT_SUPPORTED;
+  return run_tri_strips<double, kSymv>(H, (int)n, matrix, lda, x, incx, alpha, beta, y, incy,
+                                       uplo == CORAL_LOWER, false);
+}
+
+// zhemv.rs:96-230: the chemv order in double (Re of the diagonal only; beta
+// == 0 fills zeros, beta != 1 multiplies by zscal, zhemv.rs:135-138).
+coral_status_t coral_zhemv(coral_handle_t hh, int uplo, size_t n, const double alpha[2],
+                           const double* matrix, size_t lda, const double* x, size_t incx,
+                           const double beta[2], double* y, size_t incy) {
+  CORAL_HANDLE(hh);
+  if (uplo != CORAL_UPPER && uplo != CORAL_LOWER) return bad_arg(H, 1);
+  if (!alpha) return bad_arg(H, 3);
+  if (!beta) return bad_arg(H, 8);
+  if (n == 0) return CORAL_OK;  // zhemv.rs:110
+  if (alpha[0] == 0.0 && alpha[1] == 0.0 && beta[0] == 1.0 && beta[1] == 0.0) return CORAL_OK;
+  if (!matrix) return bad_arg(H, 4);
+  if (lda < n) return bad_arg(H, 5);
+  if (!x) return bad_arg(H, 6);
+  if (incx == 0) return bad_arg(H, 7);
+  if (!y) return bad_arg(H, 9);
+  if (incy == 0) return bad_arg(H, 10);
+  if (((uintptr_t)matrix | (uintptr_t)x | (uintptr_t)y) & 15) return bad_arg(H, 4);
+  if (n > (size_t)(1 << 20)) return CORAL_ERR_NOT_SUPPORTED;
+  return run_tri_strips<double2, kHemv>(H, (int)n, reinterpret_cast<const double2*>(matrix), lda,
+                                        reinterpret_cast<const double2*>(x), incx,
+                                        make_double2(alpha[0], alpha[1]), make_double2(beta[0], beta[1]),
+                                        reinterpret_cast<double2*>(y), incy, uplo == CORAL_LOWER, false);
+}
+
+}  // extern "C"
+
+namespace coral {
+namespace {
+// x <- op(A) x for d/c/z TRMV (dtrmv.rs, ctrmv.rs:58-72, ztrmv.rs); for real
+// data ConjugateTranspose == Transpose.
+template <typename T>
+coral_status_t trmv_any(Handle* H, int uplo, int trans, int diag, size_t n, const void* matrix,
+                        size_t lda, void* x, size_t incx, size_t align) {
+  if (uplo != CORAL_UPPER && uplo != CORAL_LOWER) return bad_arg(H, 1);
+  if (trans < CORAL_NO_TRANSPOSE || trans > CORAL_CONJ_TRANSPOSE) return bad_arg(H, 2);
+  if (diag != CORAL_UNIT && diag != CORAL_NON_UNIT) return bad_arg(H, 3);
+  if (n == 0) return CORAL_OK;
+  if (!matrix) return bad_arg(H, 5);
+  if (lda < n) return bad_arg(H, 6);
+  if (!x) return bad_arg(H, 7);
+  if (incx == 0) return bad_arg(H, 8);
+  if (((uintptr_t)matrix | (uintptr_t)x) & (align - 1)) return bad_arg(H, 5);
+  if (n > (size_t)(1 << 20)) return CORAL_ERR_NOT_SUPPORTED;
+  const bool lower = uplo == CORAL_LOWER, unit = diag == CORAL_UNIT;
+  const T* A = static_cast<const T*>(matrix);
+  T* X = static_cast<T*>(x);
+  const T one = Cx<T>::one(), zero = Cx<T>::zero();
+  if (trans == CORAL_NO_TRANSPOSE)
+    return run_tri_strips<T, kTrmvN>(H, (int)n, A, lda, X, incx, one, zero, X, incx, lower, unit);
+  if (trans == CORAL_CONJ_TRANSPOSE && !std::is_same<T, double>::value)
+    return run_tri_strips<T, kTrmvC>(H, (int)n, A, lda, X, incx, one, zero, X, incx, lower, unit);
+  return run_tri_strips<T, kTrmvT>(H, (int)n, A, lda, X, incx, one, zero, X, incx, lower, unit);
+}
+}  // namespace
+}  // namespace coral
+
+extern "C" {
+coral_status_t coral_dtrmv(coral_handle_t hh, int uplo, int trans, int diag, size_t n,
+                           const double* matrix, size_t lda, double* x, size_t incx) {
+  CORAL_HANDLE(hh);
+  return trmv_any<double>(H, uplo, trans, diag, n, matrix, lda, x, incx, 8);
+}
+coral_status_t coral_ctrmv(coral_handle_t hh, int uplo, int trans, int diag, size_t n,
+                           const float* matrix, size_t lda, float* x, size_t incx) {
+  CORAL_HANDLE(hh);
+  return trmv_any<float2>(H, uplo, trans, diag, n, matrix, lda, x, incx, 8);
+}
+coral_status_t coral_ztrmv(coral_handle_t hh, int uplo, int trans, int diag, size_t n,
+                           const double* matrix, size_t lda, double* x, size_t incx) {
+  CORAL_HANDLE(hh);
+  return trmv_any<double2>(H, uplo, trans, diag, n, matrix, lda, x, incx, 16);
+}
 }  // extern "C"

@@ -157,6 +157,23 @@ coral_status_t coral_ssymv(coral_handle_t h, int uplo, size_t n, float alpha,
 coral_status_t coral_chemv(coral_handle_t h, int uplo, size_t n, const float alpha[2],
                            const float* matrix, size_t lda, const float* x,
                            size_t incx, const float beta[2], float* y, size_t incy);
+/* dsymv.rs:99-110 -- double */
+coral_status_t coral_dsymv(coral_handle_t h, int uplo, size_t n, double alpha,
+                           const double* matrix, size_t lda, const double* x,
+                           size_t incx, double beta, double* y, size_t incy);
+/* zhemv.rs:96-107 -- interleaved complex128 */
+coral_status_t coral_zhemv(coral_handle_t h, int uplo, size_t n, const double alpha[2],
+                           const double* matrix, size_t lda, const double* x,
+                           size_t incx, const double beta[2], double* y, size_t incy);
+/* dtrmv.rs -- double; ConjugateTranspose == Transpose */
+coral_status_t coral_dtrmv(coral_handle_t h, int uplo, int trans, int diag, size_t n,
+                           const double* matrix, size_t lda, double* x, size_t incx);
+/* ctrmv.rs:58-72 -- interleaved complex64; trans N, T or C */
+coral_status_t coral_ctrmv(coral_handle_t h, int uplo, int trans, int diag, size_t n,
+                           const float* matrix, size_t lda, float* x, size_t incx);
+/* ztrmv.rs -- interleaved complex128; trans N, T or C */
+coral_status_t coral_ztrmv(coral_handle_t h, int uplo, int trans, int diag, size_t n,
+                           const double* matrix, size_t lda, double* x, size_t incx);
 /* strsv.rs:60-74 */
 coral_status_t coral_strsv(coral_handle_t h, int uplo, int trans, int diag, size_t n,
                            const float* matrix, size_t lda, float* x, size_t incx);

@@ -65,6 +65,11 @@ def _declare(L: C.CDLL) -> None:
     L.or_dgemv_f64.argtypes = [_i, _sz, _sz, C.c_double, _dp, _sz, _dp, _sz, C.c_double, _dp, _sz, _dp]
     L.or_cgemv_f64.argtypes = [_i, _sz, _sz, _fp, _fp, _sz, _fp, _sz, _fp, _fp, _sz, _dp]
     L.or_zgemv_f64.argtypes = [_i, _sz, _sz, _dp, _dp, _sz, _dp, _sz, _dp, _dp, _sz, _dp]
+    L.or_dsymv_f64.argtypes = [_i, _sz, C.c_double, _dp, _sz, _dp, _sz, C.c_double, _dp, _sz, _dp]
+    L.or_zhemv_f64.argtypes = [_i, _sz, _dp, _dp, _sz, _dp, _sz, _dp, _dp, _sz, _dp]
+    L.or_dtrmv_f64.argtypes = [_i, _i, _i, _sz, _dp, _sz, _dp, _sz, _dp]
+    L.or_ctrmv_f64.argtypes = [_i, _i, _i, _sz, _fp, _sz, _fp, _sz, _dp]
+    L.or_ztrmv_f64.argtypes = [_i, _i, _i, _sz, _dp, _sz, _dp, _sz, _dp]
     L.or_strsv_f64.argtypes = [_i, _i, _i, _sz, _fp, _sz, _fp, _sz, _dp]
     L.or_strmv_f64.argtypes = [_i, _i, _i, _sz, _fp, _sz, _fp, _sz, _dp]
     L.or_sger_exact.argtypes = [_sz, _sz, C.c_float, _fp, _sz, _fp, _sz, _fp, _sz]
@@ -188,6 +193,50 @@ def strsv(uplo, trans, diag, n, a, lda, x, incx) -> np.ndarray:
     out = np.zeros(max(n, 1), np.float64)
     lib().or_strsv_f64(uplo, trans, diag, n, _f(a), lda, _f(x), incx, _d(out))
     return out[:n]
+
+
+def _c64f(v):
+    return _f(np.ascontiguousarray(v, np.complex64).view(np.float32))
+
+
+def _c128d(v):
+    return _d(np.ascontiguousarray(v, np.complex128).view(np.float64))
+
+
+def dsymv(uplo, n, alpha, a, lda, x, incx, beta, y, incy) -> np.ndarray:
+    out = np.zeros(max(n, 1), np.float64)
+    f = lambda v: _d(np.ascontiguousarray(v, np.float64))  # noqa: E731
+    lib().or_dsymv_f64(uplo, n, C.c_double(alpha), f(a), lda, f(x), incx, C.c_double(beta), f(y), incy,
+                       _d(out))
+    return out[:n]
+
+
+def zhemv(uplo, n, alpha, a, lda, x, incx, beta, y, incy) -> np.ndarray:
+    """zhemv result as complex128."""
+    out = np.zeros(2 * max(n, 1), np.float64)
+    al = np.array([complex(alpha).real, complex(alpha).imag], np.float64)
+    be = np.array([complex(beta).real, complex(beta).imag], np.float64)
+    lib().or_zhemv_f64(uplo, n, _d(al), _c128d(a), lda, _c128d(x), incx, _d(be), _c128d(y), incy, _d(out))
+    return out.view(np.complex128)[:n]
+
+
+def dtrmv(uplo, trans, diag, n, a, lda, x, incx) -> np.ndarray:
+    out = np.zeros(max(n, 1), np.float64)
+    f = lambda v: _d(np.ascontiguousarray(v, np.float64))  # noqa: E731
+    lib().or_dtrmv_f64(uplo, trans, diag, n, f(a), lda, f(x), incx, _d(out))
+    return out[:n]
+
+
+def ctrmv(uplo, trans, diag, n, a, lda, x, incx) -> np.ndarray:
+    out = np.zeros(2 * max(n, 1), np.float64)
+    lib().or_ctrmv_f64(uplo, trans, diag, n, _c64f(a), lda, _c64f(x), incx, _d(out))
+    return out.view(np.complex128)[:n]
+
+
+def ztrmv(uplo, trans, diag, n, a, lda, x, incx) -> np.ndarray:
+    out = np.zeros(2 * max(n, 1), np.float64)
+    lib().or_ztrmv_f64(uplo, trans, diag, n, _c128d(a), lda, _c128d(x), incx, _d(out))
+    return out.view(np.complex128)[:n]
 
 
 def strmv(uplo, trans, diag, n, a, lda, x, incx) -> np.ndarray:

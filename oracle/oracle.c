@@ -345,6 +345,120 @@ void or_strmv_f64(int uplo, int trans, int diag, size_t n, const float* A, size_
   }
 }
 
+/* level2/dsymv.rs:99-210: the ssymv order in double -- n == 0 or
+ * (alpha == 0 && beta == 1) -> no-op; xs = alpha * x; beta == 0 -> y = 0
+ * (fill), beta != 1 -> y *= beta; only the `uplo` triangle of A is read. */
+void or_dsymv_f64(int uplo, size_t n, double alpha, const double* A, size_t lda, const double* x,
+                  size_t incx, double beta, const double* y, size_t incy, double* y_out) {
+  for (size_t i = 0; i < n; ++i) y_out[i] = y[i * incy];
+  if (n == 0) return;
+  if (alpha == 0.0 && beta == 1.0) return;
+  double* xs = (double*)malloc(sizeof(double) * n);
+  for (size_t j = 0; j < n; ++j) xs[j] = alpha * x[j * incx];
+  for (size_t i = 0; i < n; ++i) {
+    double yb = beta == 0.0 ? 0.0 : (beta != 1.0 ? y[i * incy] * beta : y[i * incy]);
+    dd acc = {0.0, 0.0};
+    for (size_t j = 0; j < n; ++j) {
+      int stored = uplo == UPPER ? (i <= j) : (i >= j);
+      acc = dd_add_prod(acc, stored ? A[i + j * lda] : A[j + i * lda], xs[j]);
+    }
+    y_out[i] = yb + dd_val(acc);
+  }
+  free(xs);
+}
+
+/* level2/zhemv.rs:96-230: the chemv order in double -- Re of the diagonal
+ * only; the unstored triangle is the conjugate of the stored one; beta == 0
+ * -> y = 0, beta != 1 -> y *= beta (zscal). */
+void or_zhemv_f64(int uplo, size_t n, const double alpha[2], const double* A, size_t lda,
+                  const double* x, size_t incx, const double beta[2], const double* y, size_t incy,
+                  double* y_out) {
+  for (size_t i = 0; i < n; ++i) {
+    y_out[2 * i] = y[2 * i * incy];
+    y_out[2 * i + 1] = y[2 * i * incy + 1];
+  }
+  if (n == 0) return;
+  if (alpha[0] == 0.0 && alpha[1] == 0.0 && beta[0] == 1.0 && beta[1] == 0.0) return;
+  double* xs = (double*)malloc(sizeof(double) * 2 * n);
+  for (size_t j = 0; j < n; ++j) {
+    double xr = x[2 * j * incx], xi = x[2 * j * incx + 1];
+    xs[2 * j] = alpha[0] * xr - alpha[1] * xi;
+    xs[2 * j + 1] = alpha[0] * xi + alpha[1] * xr;
+  }
+  for (size_t i = 0; i < n; ++i) {
+    double yr = y[2 * i * incy], yi = y[2 * i * incy + 1], br, bi;
+    if (beta[0] == 0.0 && beta[1] == 0.0) { br = 0.0; bi = 0.0; }
+    else if (beta[0] == 1.0 && beta[1] == 0.0) { br = yr; bi = yi; }
+    else { br = yr * beta[0] - yi * beta[1]; bi = yr * beta[1] + yi * beta[0]; }
+    dd re = {0.0, 0.0}, im = {0.0, 0.0};
+    for (size_t j = 0; j < n; ++j) {
+      double ar, ai;
+      if (i == j) { ar = A[2 * (i + j * lda)]; ai = 0.0; }
+      else if (uplo == UPPER ? (i < j) : (i > j)) { ar = A[2 * (i + j * lda)]; ai = A[2 * (i + j * lda) + 1]; }
+      else { ar = A[2 * (j + i * lda)]; ai = -A[2 * (j + i * lda) + 1]; }
+      re = dd_add_prod(re, ar, xs[2 * j]);
+      re = dd_add_prod(re, -ai, xs[2 * j + 1]);
+      im = dd_add_prod(im, ar, xs[2 * j + 1]);
+      im = dd_add_prod(im, ai, xs[2 * j]);
+    }
+    y_out[2 * i] = br + dd_val(re);
+    y_out[2 * i + 1] = bi + dd_val(im);
+  }
+  free(xs);
+}
+
+/* level2/dtrmv.rs (dtrlmv.rs / dtrumv.rs): x <- op(A) x, A triangular in the
+ * `uplo` half, unit diagonal = 1; ConjugateTranspose == Transpose. */
+void or_dtrmv_f64(int uplo, int trans, int diag, size_t n, const double* A, size_t lda,
+                  const double* x, size_t incx, double* x_out) {
+  const int t = trans != NOTRANS;
+  for (size_t i = 0; i < n; ++i) {
+    dd acc = {0.0, 0.0};
+    for (size_t k = 0; k < n; ++k) {
+      size_t r = t ? k : i, c = t ? i : k;  /* element (r, c) of A */
+      double a;
+      if (r == c) a = diag == UNIT ? 1.0 : A[r + c * lda];
+      else if (uplo == UPPER ? (r < c) : (r > c)) a = A[r + c * lda];
+      else continue;
+      acc = dd_add_prod(acc, a, x[k * incx]);
+    }
+    x_out[i] = dd_val(acc);
+  }
+}
+
+/* level2/ctrmv.rs:58-72 / ztrmv.rs (c/z trlmv, trumv): x <- op(A) x with op
+ * N, T or C (conjugated elements), interleaved complex, unit diagonal = 1. */
+#define OR_CTRMV_BODY                                                                        \
+  const int t = trans != NOTRANS, cj = trans == CONJTRANS;                                   \
+  for (size_t i = 0; i < n; ++i) {                                                           \
+    dd re = {0.0, 0.0}, im = {0.0, 0.0};                                                     \
+    for (size_t k = 0; k < n; ++k) {                                                         \
+      size_t r = t ? k : i, c = t ? i : k;                                                   \
+      double ar, ai;                                                                         \
+      if (r == c && diag == UNIT) { ar = 1.0; ai = 0.0; }                                    \
+      else if (r == c || (uplo == UPPER ? (r < c) : (r > c))) {                             \
+        ar = A[2 * (r + c * lda)];                                                           \
+        ai = cj ? -(double)A[2 * (r + c * lda) + 1] : (double)A[2 * (r + c * lda) + 1];     \
+      } else continue;                                                                       \
+      double xr = x[2 * k * incx], xi = x[2 * k * incx + 1];                                 \
+      re = dd_add_prod(re, ar, xr);                                                          \
+      re = dd_add_prod(re, -ai, xi);                                                         \
+      im = dd_add_prod(im, ar, xi);                                                          \
+      im = dd_add_prod(im, ai, xr);                                                          \
+    }                                                                                        \
+    x_out[2 * i] = dd_val(re);                                                               \
+    x_out[2 * i + 1] = dd_val(im);                                                           \
+  }
+
+void or_ctrmv_f64(int uplo, int trans, int diag, size_t n, const float* A, size_t lda,
+                  const float* x, size_t incx, double* x_out) {
+  OR_CTRMV_BODY
+}
+void or_ztrmv_f64(int uplo, int trans, int diag, size_t n, const double* A, size_t lda,
+                  const double* x, size_t incx, double* x_out) {
+  OR_CTRMV_BODY
+}
+
 /* level2/sger.rs:68-132 (bit-exact): unit strides go through saxpy per
  * column (fused first m - m%8 rows, `+= a*x` for the rest), strided through
  * mul_add; a column whose coefficient alpha*y_j is 0 is skipped. */

@@ -84,3 +84,88 @@ def test_gemv_strides_and_beta_modes(cuda, dt, trans):
 def test_gemv_alpha_zero_and_quick_return(cuda, dt):
     run_gemv(dt, 0, 200, 100, 200, 1, 1, 0.0, 0.5, 21)      # beta step only
     run_gemv(dt, 1, 200, 100, 200, 1, 1, 0.0, 1.0, 22)      # no-op
+
+
+# ---- DSYMV / ZHEMV / d,c,z TRMV (dsymv.rs, zhemv.rs, dtrmv.rs, ctrmv.rs, ztrmv.rs) ----
+# The unstored triangle (and, for unit-diagonal TRMV, the diagonal) holds NaN:
+# any read of it would show up in the result.
+TRI_SIZES = [(1, 1), (7, 7), (64, 64), (65, 70), (127, 132), (300, 300), (1024, 1024), (2049, 2050)]
+
+
+def tri(rng, n, lda, uplo, dt, nan_diag=False):
+    a = rnd(rng, (n, lda), dt)                                   # [col][row]
+    jj, ii = np.meshgrid(np.arange(n), np.arange(lda), indexing="ij")
+    stored = (ii <= jj) if uplo == 0 else (ii >= jj)
+    a[~stored & (ii < n)] = np.nan
+    if nan_diag:
+        d = np.arange(n)
+        a[d, d] = np.nan
+    return a
+
+
+def check_scaled(got, want, scale, dt):
+    assert np.isfinite(got).all()
+    assert (np.abs(got - want) <= TOL[dt] * scale + 1e-30).all(), np.abs(got - want).max()
+
+
+def sym_mag(a, n, uplo, herm):
+    """|A| of the full symmetric / Hermitian matrix from the stored half."""
+    A = np.nan_to_num(np.abs(a[:, :n].T.astype(np.complex128)))
+    M = np.triu(A) if uplo == 0 else np.tril(A)
+    return M + M.T - np.diag(np.diag(M))
+
+
+@pytest.mark.parametrize("n,lda", TRI_SIZES)
+@pytest.mark.parametrize("uplo", [0, 1])
+def test_dsymv(cuda, n, lda, uplo):
+    rng = np.random.default_rng(n + 3 * uplo)
+    a = tri(rng, n, lda, uplo, np.float64)
+    x, y = rnd(rng, n, np.float64), rnd(rng, n, np.float64)
+    Y = torch.from_numpy(y.copy()).cuda()
+    cb.dsymv(uplo, n, 1.5, torch.from_numpy(a.ravel()).cuda(), lda, torch.from_numpy(x).cuda(), 1, 0.5, Y, 1)
+    torch.cuda.synchronize()
+    want = oracle.dsymv(uplo, n, 1.5, a.ravel(), lda, x, 1, 0.5, y, 1)
+    check_scaled(Y.cpu().numpy(), want, 1.5 * sym_mag(a, n, uplo, False) @ np.abs(x) + 0.5 * np.abs(y), np.float64)
+
+
+@pytest.mark.parametrize("n,lda", TRI_SIZES)
+@pytest.mark.parametrize("uplo", [0, 1])
+def test_zhemv(cuda, n, lda, uplo):
+    rng = np.random.default_rng(n + 5 * uplo)
+    a = tri(rng, n, lda, uplo, np.complex128)
+    x, y = rnd(rng, n, np.complex128), rnd(rng, n, np.complex128)
+    al, be = 1.5 - 0.5j, 0.25 + 0.5j
+    Y = torch.from_numpy(y.copy()).cuda()
+    cb.zhemv(uplo, n, al, torch.from_numpy(a.ravel()).cuda(), lda, torch.from_numpy(x).cuda(), 1, be, Y, 1)
+    torch.cuda.synchronize()
+    want = oracle.zhemv(uplo, n, al, a.ravel(), lda, x, 1, be, y, 1)
+    scale = abs(al) * sym_mag(a, n, uplo, True) @ np.abs(x) + abs(be) * np.abs(y)
+    check_scaled(Y.cpu().numpy(), want, scale, np.complex128)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.complex64, np.complex128], ids=["d", "c", "z"])
+@pytest.mark.parametrize("n,lda", [(1, 1), (65, 70), (300, 300), (2049, 2050)])
+@pytest.mark.parametrize("uplo", [0, 1])
+@pytest.mark.parametrize("trans", [0, 1, 2])
+@pytest.mark.parametrize("diag", [0, 1])
+def test_trmv_dcz(cuda, dt, n, lda, uplo, trans, diag):
+    rng = np.random.default_rng(n + 7 * uplo + 11 * trans + diag)
+    a = tri(rng, n, lda, uplo, dt, nan_diag=(diag == 0))
+    inc = 2 if n == 65 else 1
+    x = rnd(rng, (n - 1) * inc + 1, dt)
+    X = torch.from_numpy(x.copy()).cuda()
+    fn = {np.float64: cb.dtrmv, np.complex64: cb.ctrmv, np.complex128: cb.ztrmv}[dt]
+    fn(uplo, trans, diag, n, torch.from_numpy(a.ravel()).cuda(), lda, X, inc)
+    torch.cuda.synchronize()
+    got = X.cpu().numpy()
+    orc = {np.float64: oracle.dtrmv, np.complex64: oracle.ctrmv, np.complex128: oracle.ztrmv}[dt]
+    want = orc(uplo, trans, diag, n, a.ravel(), lda, x, inc)
+    A = np.nan_to_num(np.abs(a[:, :n].T.astype(np.complex128)))
+    M = np.triu(A) if uplo == 0 else np.tril(A)
+    if diag == 0:
+        np.fill_diagonal(M, 1.0)
+    scale = (M if trans == 0 else M.T) @ np.abs(x[::inc][:n])
+    check_scaled(got[::inc][:n], want, scale, dt)
+    if inc > 1:
+        holes = np.arange(x.size) % inc != 0
+        np.testing.assert_array_equal(got[holes], x[holes])
