@@ -10,7 +10,8 @@ from .blas import (  # noqa: F401
     chemv, dgemm, gemm_mode, handle, isamax, saxpy, scopy, sdot, set_gemm_mode, sgemm, sgemv,
     sger, snrm2, sscal, sswap, ssymv, ssyr, ssyr2, strmv, strsv, zgemm, sgemm_grouped,
     strsv_batched, sgemm_problem_dtype, strsv_problem_dtype, dgemv, cgemv, zgemv,
-    dsymv, zhemv, dtrmv, ctrmv, ztrmv,
+    dsymv, zhemv, dtrmv, ctrmv, ztrmv, dger, cgeru, cgerc, zgeru, zgerc, dsyr, dsyr2, cher, zher,
+    cher2, zher2,
 )
 
 __all__ = [
@@ -19,5 +20,6 @@ __all__ = [
     "set_gemm_mode", "sgemm", "sgemv", "sger", "snrm2", "sscal", "sswap", "ssymv", "ssyr",
     "ssyr2", "strmv", "strsv", "zgemm", "sgemm_grouped", "strsv_batched", "sgemm_problem_dtype",
     "strsv_problem_dtype", "dgemv", "cgemv", "zgemv",
-    "dsymv", "zhemv", "dtrmv", "ctrmv", "ztrmv",
+    "dsymv", "zhemv", "dtrmv", "ctrmv", "ztrmv", "dger", "cgeru", "cgerc", "zgeru", "zgerc", "dsyr",
+    "dsyr2", "cher", "zher", "cher2", "zher2",
 ]

@@ -60,6 +60,17 @@ SIGNATURES = {
     "coral_dtrmv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],
     "coral_ctrmv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],
     "coral_ztrmv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],
+    "coral_dger": [_h, _sz, _sz, _d, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_cgeru": [_h, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_cgerc": [_h, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_zgeru": [_h, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_zgerc": [_h, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_dsyr": [_h, _i, _sz, _d, _vp, _sz, _vp, _sz],
+    "coral_dsyr2": [_h, _i, _sz, _d, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_cher": [_h, _i, _sz, _f, _vp, _sz, _vp, _sz],
+    "coral_zher": [_h, _i, _sz, _d, _vp, _sz, _vp, _sz],
+    "coral_cher2": [_h, _i, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_zher2": [_h, _i, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _sz],
     "coral_ssymv": [_h, _i, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
     "coral_chemv": [_h, _i, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
     "coral_strsv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],

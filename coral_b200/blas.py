@@ -284,6 +284,80 @@ def ztrmv(uplo, transpose, diagonal, n, matrix, lda, x, incx) -> None:
                   _ptr(matrix, _c128(), "matrix"), lda, _ptr(x, _c128(), "x"), incx)
 
 
+def dger(n_rows, n_cols, alpha, x, incx, y, incy, matrix, lda) -> None:
+    """level2/dger.rs."""
+    handle().call("coral_dger", n_rows, n_cols, float(alpha), _ptr(x, _f64(), "x"), incx,
+                  _ptr(y, _f64(), "y"), incy, _ptr(matrix, _f64(), "matrix"), lda)
+
+
+def _cger(name, kind, n_rows, n_cols, alpha, x, incx, y, incy, matrix, lda):
+    pa, ka = _pair(_cscalar(alpha), C.c_float if kind == "c" else C.c_double)
+    dt = _c64() if kind == "c" else _c128()
+    handle().call(name, n_rows, n_cols, pa, _ptr(x, dt, "x"), incx, _ptr(y, dt, "y"), incy,
+                  _ptr(matrix, dt, "matrix"), lda)
+
+
+def cgeru(n_rows, n_cols, alpha, x, incx, y, incy, matrix, lda) -> None:
+    """level2/cgeru.rs: A += alpha x y^T."""
+    _cger("coral_cgeru", "c", n_rows, n_cols, alpha, x, incx, y, incy, matrix, lda)
+
+
+def cgerc(n_rows, n_cols, alpha, x, incx, y, incy, matrix, lda) -> None:
+    """level2/cgerc.rs: A += alpha x y^H."""
+    _cger("coral_cgerc", "c", n_rows, n_cols, alpha, x, incx, y, incy, matrix, lda)
+
+
+def zgeru(n_rows, n_cols, alpha, x, incx, y, incy, matrix, lda) -> None:
+    """level2/zgeru.rs."""
+    _cger("coral_zgeru", "z", n_rows, n_cols, alpha, x, incx, y, incy, matrix, lda)
+
+
+def zgerc(n_rows, n_cols, alpha, x, incx, y, incy, matrix, lda) -> None:
+    """level2/zgerc.rs."""
+    _cger("coral_zgerc", "z", n_rows, n_cols, alpha, x, incx, y, incy, matrix, lda)
+
+
+def dsyr(uplo, n, alpha, x, incx, matrix, lda) -> None:
+    """level2/dsyr.rs."""
+    handle().call("coral_dsyr", int(uplo), n, float(alpha), _ptr(x, _f64(), "x"), incx,
+                  _ptr(matrix, _f64(), "matrix"), lda)
+
+
+def dsyr2(uplo, n, alpha, x, incx, y, incy, matrix, lda) -> None:
+    """level2/dsyr2.rs."""
+    handle().call("coral_dsyr2", int(uplo), n, float(alpha), _ptr(x, _f64(), "x"), incx,
+                  _ptr(y, _f64(), "y"), incy, _ptr(matrix, _f64(), "matrix"), lda)
+
+
+def cher(uplo, n, alpha, x, incx, matrix, lda) -> None:
+    """level2/cher.rs (real alpha)."""
+    handle().call("coral_cher", int(uplo), n, float(alpha), _ptr(x, _c64(), "x"), incx,
+                  _ptr(matrix, _c64(), "matrix"), lda)
+
+
+def zher(uplo, n, alpha, x, incx, matrix, lda) -> None:
+    """level2/zher.rs (real alpha)."""
+    handle().call("coral_zher", int(uplo), n, float(alpha), _ptr(x, _c128(), "x"), incx,
+                  _ptr(matrix, _c128(), "matrix"), lda)
+
+
+def _cher2(name, kind, uplo, n, alpha, x, incx, y, incy, matrix, lda):
+    pa, ka = _pair(_cscalar(alpha), C.c_float if kind == "c" else C.c_double)
+    dt = _c64() if kind == "c" else _c128()
+    handle().call(name, int(uplo), n, pa, _ptr(x, dt, "x"), incx, _ptr(y, dt, "y"), incy,
+                  _ptr(matrix, dt, "matrix"), lda)
+
+
+def cher2(uplo, n, alpha, x, incx, y, incy, matrix, lda) -> None:
+    """level2/cher2.rs."""
+    _cher2("coral_cher2", "c", uplo, n, alpha, x, incx, y, incy, matrix, lda)
+
+
+def zher2(uplo, n, alpha, x, incx, y, incy, matrix, lda) -> None:
+    """level2/zher2.rs."""
+    _cher2("coral_zher2", "z", uplo, n, alpha, x, incx, y, incy, matrix, lda)
+
+
 def ssymv(uplo, n, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
     """level2/ssymv.rs:99-394."""
     handle().call("coral_ssymv", int(uplo), n, alpha, _ptr(matrix, _f32(), "matrix"), lda,

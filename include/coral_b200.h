@@ -191,6 +191,42 @@ coral_status_t coral_ssyr(coral_handle_t h, int uplo, size_t n, float alpha,
 coral_status_t coral_ssyr2(coral_handle_t h, int uplo, size_t n, float alpha,
                            const float* x, size_t incx, const float* y, size_t incy,
                            float* matrix, size_t lda);
+/* dger.rs -- A += alpha x y^T in double */
+coral_status_t coral_dger(coral_handle_t h, size_t n_rows, size_t n_cols, double alpha,
+                          const double* x, size_t incx, const double* y, size_t incy,
+                          double* matrix, size_t lda);
+/* cgeru.rs / cgerc.rs -- A += alpha x y^T / alpha x y^H, interleaved complex64 */
+coral_status_t coral_cgeru(coral_handle_t h, size_t n_rows, size_t n_cols, const float alpha[2],
+                           const float* x, size_t incx, const float* y, size_t incy,
+                           float* matrix, size_t lda);
+coral_status_t coral_cgerc(coral_handle_t h, size_t n_rows, size_t n_cols, const float alpha[2],
+                           const float* x, size_t incx, const float* y, size_t incy,
+                           float* matrix, size_t lda);
+/* zgeru.rs / zgerc.rs -- interleaved complex128 */
+coral_status_t coral_zgeru(coral_handle_t h, size_t n_rows, size_t n_cols, const double alpha[2],
+                           const double* x, size_t incx, const double* y, size_t incy,
+                           double* matrix, size_t lda);
+coral_status_t coral_zgerc(coral_handle_t h, size_t n_rows, size_t n_cols, const double alpha[2],
+                           const double* x, size_t incx, const double* y, size_t incy,
+                           double* matrix, size_t lda);
+/* dsyr.rs / dsyr2.rs -- double */
+coral_status_t coral_dsyr(coral_handle_t h, int uplo, size_t n, double alpha,
+                          const double* x, size_t incx, double* matrix, size_t lda);
+coral_status_t coral_dsyr2(coral_handle_t h, int uplo, size_t n, double alpha,
+                           const double* x, size_t incx, const double* y, size_t incy,
+                           double* matrix, size_t lda);
+/* cher.rs / zher.rs -- A += alpha x x^H, real alpha; diagonal stored real */
+coral_status_t coral_cher(coral_handle_t h, int uplo, size_t n, float alpha,
+                          const float* x, size_t incx, float* matrix, size_t lda);
+coral_status_t coral_zher(coral_handle_t h, int uplo, size_t n, double alpha,
+                          const double* x, size_t incx, double* matrix, size_t lda);
+/* cher2.rs / zher2.rs -- A += alpha x y^H + conj(alpha) y x^H */
+coral_status_t coral_cher2(coral_handle_t h, int uplo, size_t n, const float alpha[2],
+                           const float* x, size_t incx, const float* y, size_t incy,
+                           float* matrix, size_t lda);
+coral_status_t coral_zher2(coral_handle_t h, int uplo, size_t n, const double alpha[2],
+                           const double* x, size_t incx, const double* y, size_t incy,
+                           double* matrix, size_t lda);
 
 /* ---- level 3 (coral-aarch64/src/level3) --------------------------------- */
 /* sgemm.rs:106-130; arithmetic per coral_set_gemm_mode (NATIVE or SPLIT_BF16X3/X6) */

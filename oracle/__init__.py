@@ -70,6 +70,12 @@ def _declare(L: C.CDLL) -> None:
     L.or_dtrmv_f64.argtypes = [_i, _i, _i, _sz, _dp, _sz, _dp, _sz, _dp]
     L.or_ctrmv_f64.argtypes = [_i, _i, _i, _sz, _fp, _sz, _fp, _sz, _dp]
     L.or_ztrmv_f64.argtypes = [_i, _i, _i, _sz, _dp, _sz, _dp, _sz, _dp]
+    L.or_dger_f64.argtypes = [_sz, _sz, C.c_double, _dp, _sz, _dp, _sz, _dp, _sz]
+    L.or_cger_f64.argtypes = [_i, _sz, _sz, _fp, _fp, _sz, _fp, _sz, _dp, _sz]
+    L.or_zger_f64.argtypes = [_i, _sz, _sz, _dp, _dp, _sz, _dp, _sz, _dp, _sz]
+    L.or_dsyr_f64.argtypes = [_i, _sz, C.c_double, _dp, _sz, _dp, _sz, _i, _dp, _sz]
+    L.or_cher_f64.argtypes = [_i, _sz, _fp, _fp, _sz, _fp, _sz, _i, _dp, _sz]
+    L.or_zher_f64.argtypes = [_i, _sz, _dp, _dp, _sz, _dp, _sz, _i, _dp, _sz]
     L.or_strsv_f64.argtypes = [_i, _i, _i, _sz, _fp, _sz, _fp, _sz, _dp]
     L.or_strmv_f64.argtypes = [_i, _i, _i, _sz, _fp, _sz, _fp, _sz, _dp]
     L.or_sger_exact.argtypes = [_sz, _sz, C.c_float, _fp, _sz, _fp, _sz, _fp, _sz]
@@ -237,6 +243,52 @@ def ztrmv(uplo, trans, diag, n, a, lda, x, incx) -> np.ndarray:
     out = np.zeros(2 * max(n, 1), np.float64)
     lib().or_ztrmv_f64(uplo, trans, diag, n, _c128d(a), lda, _c128d(x), incx, _d(out))
     return out.view(np.complex128)[:n]
+
+
+def dger(m, n, alpha, x, incx, y, incy, a, lda) -> np.ndarray:
+    """dger: returns the updated A (float64)."""
+    a = np.array(a, dtype=np.float64, copy=True)
+    f = lambda v: _d(np.ascontiguousarray(v, np.float64))  # noqa: E731
+    lib().or_dger_f64(m, n, C.c_double(alpha), f(x), incx, f(y), incy, _d(a), lda)
+    return a
+
+
+def gerc_u(kind, conj, m, n, alpha, x, incx, y, incy, a, lda) -> np.ndarray:
+    """c/z geru (conj = 0) / gerc (conj = 1): returns the updated A as complex128."""
+    a = np.array(a, dtype=np.complex128, copy=True)
+    if kind == "c":
+        al = np.array([complex(alpha).real, complex(alpha).imag], np.float32)
+        lib().or_cger_f64(conj, m, n, _f(al), _c64f(x), incx, _c64f(y), incy, _d(a.view(np.float64)), lda)
+    else:
+        al = np.array([complex(alpha).real, complex(alpha).imag], np.float64)
+        lib().or_zger_f64(conj, m, n, _d(al), _c128d(x), incx, _c128d(y), incy, _d(a.view(np.float64)), lda)
+    return a
+
+
+def dsyr(uplo, n, alpha, x, incx, a, lda, y=None, incy=1) -> np.ndarray:
+    """dsyr (y None) or dsyr2: returns the updated A (float64)."""
+    a = np.array(a, dtype=np.float64, copy=True)
+    f = lambda v: _d(np.ascontiguousarray(v, np.float64))  # noqa: E731
+    two = y is not None
+    lib().or_dsyr_f64(uplo, n, C.c_double(alpha), f(x), incx, f(y if two else x), incy if two else incx,
+                      int(two), _d(a), lda)
+    return a
+
+
+def her(kind, uplo, n, alpha, x, incx, a, lda, y=None, incy=1) -> np.ndarray:
+    """c/z her (y None; real alpha) or her2: returns the updated A as complex128."""
+    a = np.array(a, dtype=np.complex128, copy=True)
+    two = y is not None
+    yy = y if two else x
+    if kind == "c":
+        al = np.array([complex(alpha).real, complex(alpha).imag], np.float32)
+        lib().or_cher_f64(uplo, n, _f(al), _c64f(x), incx, _c64f(yy), incy if two else incx, int(two),
+                          _d(a.view(np.float64)), lda)
+    else:
+        al = np.array([complex(alpha).real, complex(alpha).imag], np.float64)
+        lib().or_zher_f64(uplo, n, _d(al), _c128d(x), incx, _c128d(yy), incy if two else incx, int(two),
+                          _d(a.view(np.float64)), lda)
+    return a
 
 
 def strmv(uplo, trans, diag, n, a, lda, x, incx) -> np.ndarray:

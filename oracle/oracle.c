@@ -459,6 +459,101 @@ void or_ztrmv_f64(int uplo, int trans, int diag, size_t n, const double* A, size
   OR_CTRMV_BODY
 }
 
+/* level2/dger.rs: per column j, coeff = alpha * y_j (a zero coefficient
+ * leaves the column untouched); A_ij += x_i * coeff with one rounding (the
+ * reference's daxpy / mul_add).  A is updated in place. */
+void or_dger_f64(size_t m, size_t n, double alpha, const double* x, size_t incx, const double* y,
+                 size_t incy, double* A, size_t lda) {
+  if (m == 0 || n == 0 || alpha == 0.0) return;
+  for (size_t j = 0; j < n; ++j) {
+    double c = alpha * y[j * incy];
+    if (c == 0.0) continue;
+    for (size_t i = 0; i < m; ++i) A[i + j * lda] = fma(x[i * incx], c, A[i + j * lda]);
+  }
+}
+
+/* Complex rank updates, interleaved (re, im), A (double, interleaved) updated
+ * in place; coefficients are formed in the element precision R as the
+ * reference forms them, the update A_ij += x_i * c in double:
+ *   cgeru/zgeru (cj = 0): c = alpha * y_j;  cgerc/zgerc (cj = 1): alpha * conj(y_j)
+ *   (cgeru.rs / cgerc.rs: a zero coefficient leaves the column untouched). */
+#define OR_CGER(NAME, R)                                                                        \
+  void NAME(int cj, size_t m, size_t n, const R alpha[2], const R* x, size_t incx, const R* y,   \
+            size_t incy, double* A, size_t lda) {                                               \
+    if (m == 0 || n == 0 || (alpha[0] == 0 && alpha[1] == 0)) return;                           \
+    for (size_t j = 0; j < n; ++j) {                                                            \
+      R yr = y[2 * j * incy], yi = cj ? -y[2 * j * incy + 1] : y[2 * j * incy + 1];             \
+      R cr = alpha[0] * yr - alpha[1] * yi, ci = alpha[0] * yi + alpha[1] * yr;                 \
+      if (cr == 0 && ci == 0) continue;                                                         \
+      for (size_t i = 0; i < m; ++i) {                                                          \
+        double xr = x[2 * i * incx], xi = x[2 * i * incx + 1];                                  \
+        A[2 * (i + j * lda)] += xr * (double)cr - xi * (double)ci;                              \
+        A[2 * (i + j * lda) + 1] += xr * (double)ci + xi * (double)cr;                          \
+      }                                                                                         \
+    }                                                                                           \
+  }
+OR_CGER(or_cger_f64, float)
+OR_CGER(or_zger_f64, double)
+
+/* level2/dsyr.rs / dsyr2.rs: the `uplo` triangle of column j gets
+ * x_i * (alpha x_j)  (syr), or  x_i * (alpha y_j) + y_i * (alpha x_j)  (syr2),
+ * each term skipped when its coefficient is zero; one rounding per term. */
+void or_dsyr_f64(int uplo, size_t n, double alpha, const double* x, size_t incx, const double* y,
+                 size_t incy, int two, double* A, size_t lda) {
+  if (n == 0 || alpha == 0.0) return;
+  for (size_t j = 0; j < n; ++j) {
+    size_t lo = uplo == UPPER ? 0 : j, hi = uplo == UPPER ? j + 1 : n;
+    double c1 = two ? alpha * y[j * incy] : alpha * x[j * incx];
+    double c2 = two ? alpha * x[j * incx] : 0.0;
+    for (size_t i = lo; i < hi; ++i) {
+      double a = A[i + j * lda];
+      if (c1 != 0.0) a = fma(x[i * incx], c1, a);
+      if (c2 != 0.0) a = fma(y[i * incy], c2, a);
+      A[i + j * lda] = a;
+    }
+  }
+}
+
+/* level2/cher.rs, zher.rs (two = 0; real alpha): c = alpha * conj(x_j); the
+ * column's triangle gets x_i * c and, when updated, a real diagonal.
+ * cher2.rs, zher2.rs (two = 1): c1 = alpha * conj(y_j) on x,
+ * c2 = conj(alpha) * conj(x_j) on y, each skipped when zero; the diagonal is
+ * made real for every column. */
+#define OR_CHER(NAME, R)                                                                        \
+  void NAME(int uplo, size_t n, const R alpha[2], const R* x, size_t incx, const R* y,          \
+            size_t incy, int two, double* A, size_t lda) {                                      \
+    if (n == 0 || (alpha[0] == 0 && alpha[1] == 0)) return;                                     \
+    for (size_t j = 0; j < n; ++j) {                                                            \
+      size_t lo = uplo == UPPER ? 0 : j, hi = uplo == UPPER ? j + 1 : n;                        \
+      R c1r, c1i, c2r = 0, c2i = 0;                                                             \
+      R xjr = x[2 * j * incx], xji = x[2 * j * incx + 1];                                       \
+      if (!two) { c1r = alpha[0] * xjr; c1i = -alpha[0] * xji; }                                \
+      else {                                                                                    \
+        R yjr = y[2 * j * incy], yji = y[2 * j * incy + 1];                                     \
+        c1r = alpha[0] * yjr + alpha[1] * yji; c1i = -alpha[0] * yji + alpha[1] * yjr;          \
+        c2r = alpha[0] * xjr - alpha[1] * xji; c2i = -alpha[0] * xji - alpha[1] * xjr;          \
+      }                                                                                         \
+      int u1 = c1r != 0 || c1i != 0, u2 = c2r != 0 || c2i != 0;                                \
+      if (!u1 && !u2 && !two) continue;                                                         \
+      for (size_t i = lo; i < hi; ++i) {                                                        \
+        double* a = A + 2 * (i + j * lda);                                                      \
+        if (u1) {                                                                               \
+          double xr = x[2 * i * incx], xi = x[2 * i * incx + 1];                                \
+          a[0] += xr * (double)c1r - xi * (double)c1i;                                          \
+          a[1] += xr * (double)c1i + xi * (double)c1r;                                          \
+        }                                                                                       \
+        if (u2) {                                                                               \
+          double yr = y[2 * i * incy], yi = y[2 * i * incy + 1];                                \
+          a[0] += yr * (double)c2r - yi * (double)c2i;                                          \
+          a[1] += yr * (double)c2i + yi * (double)c2r;                                          \
+        }                                                                                       \
+        if (i == j) a[1] = 0.0;                                                                 \
+      }                                                                                         \
+    }                                                                                           \
+  }
+OR_CHER(or_cher_f64, float)
+OR_CHER(or_zher_f64, double)
+
 /* level2/sger.rs:68-132 (bit-exact): unit strides go through saxpy per
  * column (fused first m - m%8 rows, `+= a*x` for the rest), strided through
  * mul_add; a column whose coefficient alpha*y_j is 0 is skipped. */
