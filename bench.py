@@ -503,6 +503,25 @@ def level12_bandwidth(torch, cb, lib, h, dev, g, routines=None):
         rec("zhemv_upper", 16 * (nz * (nz + 1) // 2 + 3 * nz),
             timed_calls(lambda: cb.zhemv(0, nz, 1.5 - 0.5j, Az, nz, xz, 1, 0.25 + 0.0j, yz, 1), 20, False))
         del Az, xz, yz
+    for dt, fn, nm, es in ((torch.float64, cb.dtrsv, "dtrsv_lower", 8), (torch.complex64, cb.ctrsv, "ctrsv_lower", 8),
+                           (torch.complex128, cb.ztrsv, "ztrsv_lower", 16)):
+        if not want(nm):
+            continue
+        nq = 4096
+        Lq = torch.empty(nq * nq, dtype=dt, device=dev)
+        (Lq.real if dt.is_complex else Lq).uniform_(-1, 1, generator=g)
+        if dt.is_complex:
+            Lq.imag.uniform_(-1, 1, generator=g)
+        iq = torch.arange(nq, device=dev)
+        Lq.view(nq, nq)[iq, iq] += nq
+        bq = torch.ones(nq, dtype=dt, device=dev)
+        xq = bq.clone()
+
+        def solve(fn=fn, Lq=Lq, xq=xq, bq=bq):
+            xq.copy_(bq)
+            fn(1, 0, 1, nq, Lq, nq, xq, 1)
+        rec(nm, es * (nq * (nq + 1) // 2 + 2 * nq), timed_calls(solve, 10, True))
+        del Lq, xq, bq
     if want("ssymv_upper"):
         rec("ssymv_upper", 4 * (m * (m + 1) // 2 + 3 * m),
             timed_calls(lambda: cb.ssymv(0, m, 1.5, A, m, xv, 1, 0.5, yv, 1), 20, False))

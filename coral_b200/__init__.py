@@ -11,7 +11,7 @@ from .blas import (  # noqa: F401
     sger, snrm2, sscal, sswap, ssymv, ssyr, ssyr2, strmv, strsv, zgemm, sgemm_grouped,
     strsv_batched, sgemm_problem_dtype, strsv_problem_dtype, dgemv, cgemv, zgemv,
     dsymv, zhemv, dtrmv, ctrmv, ztrmv, dger, cgeru, cgerc, zgeru, zgerc, dsyr, dsyr2, cher, zher,
-    cher2, zher2,
+    cher2, zher2, dtrsv, ctrsv, ztrsv,
 )
 
 __all__ = [
@@ -21,5 +21,5 @@ __all__ = [
     "ssyr2", "strmv", "strsv", "zgemm", "sgemm_grouped", "strsv_batched", "sgemm_problem_dtype",
     "strsv_problem_dtype", "dgemv", "cgemv", "zgemv",
     "dsymv", "zhemv", "dtrmv", "ctrmv", "ztrmv", "dger", "cgeru", "cgerc", "zgeru", "zgerc", "dsyr",
-    "dsyr2", "cher", "zher", "cher2", "zher2",
+    "dsyr2", "cher", "zher", "cher2", "zher2", "dtrsv", "ctrsv", "ztrsv",
 ]

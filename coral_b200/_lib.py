@@ -71,6 +71,9 @@ SIGNATURES = {
     "coral_zher": [_h, _i, _sz, _d, _vp, _sz, _vp, _sz],
     "coral_cher2": [_h, _i, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _sz],
     "coral_zher2": [_h, _i, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_dtrsv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],
+    "coral_ctrsv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],
+    "coral_ztrsv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],
     "coral_ssymv": [_h, _i, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
     "coral_chemv": [_h, _i, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
     "coral_strsv": [_h, _i, _i, _i, _sz, _vp, _sz, _vp, _sz],

@@ -358,6 +358,24 @@ def zher2(uplo, n, alpha, x, incx, y, incy, matrix, lda) -> None:
     _cher2("coral_zher2", "z", uplo, n, alpha, x, incx, y, incy, matrix, lda)
 
 
+def dtrsv(uplo, transpose, diagonal, n, matrix, lda, x, incx) -> None:
+    """level2/dtrsv.rs (x solved in place)."""
+    handle().call("coral_dtrsv", int(uplo), int(transpose), int(diagonal), n,
+                  _ptr(matrix, _f64(), "matrix"), lda, _ptr(x, _f64(), "x"), incx)
+
+
+def ctrsv(uplo, transpose, diagonal, n, matrix, lda, x, incx) -> None:
+    """level2/ctrsv.rs (x solved in place)."""
+    handle().call("coral_ctrsv", int(uplo), int(transpose), int(diagonal), n,
+                  _ptr(matrix, _c64(), "matrix"), lda, _ptr(x, _c64(), "x"), incx)
+
+
+def ztrsv(uplo, transpose, diagonal, n, matrix, lda, x, incx) -> None:
+    """level2/ztrsv.rs (x solved in place)."""
+    handle().call("coral_ztrsv", int(uplo), int(transpose), int(diagonal), n,
+                  _ptr(matrix, _c128(), "matrix"), lda, _ptr(x, _c128(), "x"), incx)
+
+
 def ssymv(uplo, n, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
     """level2/ssymv.rs:99-394."""
     handle().call("coral_ssymv", int(uplo), n, alpha, _ptr(matrix, _f32(), "matrix"), lda,

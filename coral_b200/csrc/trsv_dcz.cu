@@ -1,0 +1,264 @@
+// DTRSV, CTRSV, ZTRSV: solve op(A) x = b in place, A triangular, op in
+// {N, T, C} (dtrsv.rs, ctrsv.rs, ztrsv.rs -> the *trlsv / *trusv files).
+// Complex data is interleaved (re, im) with lda / incx in complex units.
+//
+// One launch, one 64-row block of the solve per CTA.  Each CTA takes a
+// ticket, so block b is handled by the b-th CTA to start in solve order and
+// only waits for CTAs that started earlier -- no deadlock whatever the
+// scheduling.  A CTA
+//   1. stages its diagonal block of op(A) in shared memory (unstored triangle
+//      masked, unit diagonal applied, conjugated for op C) and reads its
+//      right-hand side;
+//   2. for every earlier block k in solve order: loads its panel tile of
+//      op(A) into registers, waits for block k's ready flag (epoch-tagged,
+//      acquire load, bounded), reads x_k back from x and accumulates
+//      op(A)(b, k) x_k -- four threads per row, 16 columns each;
+//   3. solves D x_b = rhs - acc by substitution in one warp (the diagonal
+//      block is never inverted: FP64 back-substitution as the reference does,
+//      dtrlsv.rs), with the reciprocals of the diagonal formed first;
+//   4. writes x_b over b and publishes its flag (release store).
+// The flags are the handle's epoch-tagged slot array (slot 64 k for block k);
+// the last CTA resets the ticket counter and publishes the call's epoch, so
+// no reset pass is needed.  Waits give up after the handle's wait limit and
+// set the status word.
+#include "common.cuh"
+#include "field.cuh"
+
+#include <type_traits>
+
+namespace coral {
+namespace {
+
+constexpr int kTB = 64;
+constexpr int kTThr = 256;
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t gtime() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+template <typename T, bool kConj>
+__global__ void __launch_bounds__(kTThr, 1)
+k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool lower_eff, bool trans,
+         bool unit, unsigned long long* slots, unsigned* ticket, unsigned* done, unsigned* epoch_word,
+         unsigned* status, uint64_t limit_ns) {
+  using F = Fld<T>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  T(*D)[kTB + 1] = reinterpret_cast<T(*)[kTB + 1]>(smem);   // op(A) diagonal block
+  __shared__ T xk[kTB];        // solution of the block being applied
+  __shared__ T rv[kTB];        // right-hand side, then this block's solution
+  __shared__ T rdiag[kTB];     // reciprocals of the diagonal
+  __shared__ int sblk, abort_flag;
+  __shared__ unsigned sepoch;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nblk = (n + kTB - 1) / kTB;
+  if (tid == 0) {
+    const unsigned t = atomicAdd(ticket, 1u);
+    unsigned e = *(volatile unsigned*)epoch_word + 1u;
+    sepoch = e ? e : 1u;   // slots start at 0: never a live epoch
+    abort_flag = 0;
+    sblk = lower_eff ? (int)t : nblk - 1 - (int)t;
+  }
+  __syncthreads();
+  const unsigned epoch = sepoch;
+  const int blk = sblk;
+  const int b0 = blk * kTB;
+  auto opv = [](T v) { return kConj ? F::conj(v) : v; };
+
+  // ---- 1. diagonal block and right-hand side ----
+  for (int e = tid; e < kTB * kTB; e += kTThr) {
+    const int rr = e % kTB, cc = e / kTB;          // stored element (b0 + rr, b0 + cc)
+    const int gr = b0 + rr, gc = b0 + cc;
+    T v = (gr < n && gc < n) ? A[gr + (size_t)gc * lda] : F::zero();
+    const int r = trans ? cc : rr, c = trans ? rr : cc;   // op(A)(r, c)
+    const bool in_tri = lower_eff ? r >= c : r <= c;
+    if (r == c) v = (unit || b0 + r >= n) ? F::one() : opv(v);
+    else v = in_tri ? opv(v) : F::zero();
+    D[r][c] = v;
+  }
+  if (tid < kTB) rv[tid] = (b0 + tid < n) ? x[(size_t)(b0 + tid) * incx] : F::zero();
+  __syncthreads();
+  if (tid < kTB) rdiag[tid] = F::div(F::one(), D[tid][tid]);
+
+  // ---- 2. panel: acc(r) = sum over earlier blocks k of op(A)(b, k) x_k ----
+  const int r = tid >> 2, q = tid & 3;
+  T acc = F::zero();
+  const int npanel = lower_eff ? blk : nblk - 1 - blk;
+  for (int idx = 0; idx < npanel; ++idx) {
+    const int k = lower_eff ? idx : blk + 1 + idx;
+    const int k0 = k * kTB;
+    T a[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int gr = b0 + r, gc = k0 + q * 16 + j;   // op(A)(gr, gc)
+      const bool in = gr < n && gc < n;
+      a[j] = in ? opv(trans ? A[gc + (size_t)gr * lda] : A[gr + (size_t)gc * lda]) : F::zero();
+    }
+    if (tid == 0) {
+      const unsigned long long* sp = slots + (size_t)k * kTB;
+      if ((unsigned)(ld_acquire_u64(sp) >> 32) != epoch) {
+        const uint64_t t0 = gtime();
+        for (unsigned spins = 1;; ++spins) {
+          if ((unsigned)(ld_acquire_u64(sp) >> 32) == epoch) break;
+          const uint64_t el = gtime() - t0;
+          if (el > limit_ns || ((spins & 15u) == 0 && el > 20000ull && *(volatile unsigned*)status != 0)) {
+            atomicOr(status, kStatusTimeout);
+            abort_flag = 1;
+            break;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (abort_flag) break;
+    if (tid < kTB) xk[tid] = (k0 + tid < n) ? __ldcg(x + (size_t)(k0 + tid) * incx) : F::zero();
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 16; ++j) F::mac(acc, a[j], xk[q * 16 + j]);
+    __syncthreads();
+  }
+  acc = F::add(acc, F::shfl_xor(acc, 1));
+  acc = F::add(acc, F::shfl_xor(acc, 2));
+  if (q == 0) rv[r] = F::sub(rv[r], acc);
+  __syncthreads();
+
+  // ---- 3. substitution on the diagonal block (one warp; lane owns rows
+  //         lane and lane + 32) ----
+  if (warp == 0 && !abort_flag) {
+    T v0 = rv[lane], v1 = rv[lane + 32];
+    for (int s = 0; s < kTB; ++s) {
+      const int j = lower_eff ? s : kTB - 1 - s;
+      const T src = j < 32 ? v0 : v1;
+      T xj;
+      if constexpr (F::kComplex) {
+        xj.x = __shfl_sync(0xffffffffu, src.x, j & 31);
+        xj.y = __shfl_sync(0xffffffffu, src.y, j & 31);
+      } else {
+        xj = __shfl_sync(0xffffffffu, src, j & 31);
+      }
+      xj = F::mul(xj, rdiag[j]);
+      if (lane == (j & 31)) {
+        if (j < 32) v0 = xj;
+        else v1 = xj;
+      }
+      // rows still to solve: after j in solve order
+      const int i0 = lane, i1 = lane + 32;
+      if (lower_eff ? i0 > j : i0 < j) v0 = F::sub(v0, F::mul(D[i0][j], xj));
+      if (lower_eff ? i1 > j : i1 < j) v1 = F::sub(v1, F::mul(D[i1][j], xj));
+    }
+    rv[lane] = v0;
+    rv[lane + 32] = v1;
+  }
+  __syncthreads();
+
+  // ---- 4. publish ----
+  if (!abort_flag) {
+    if (tid < kTB && b0 + tid < n) x[(size_t)(b0 + tid) * incx] = rv[tid];
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      st_release_u64(slots + (size_t)blk * kTB, (unsigned long long)epoch << 32);
+    }
+  }
+  // The last CTA to finish (aborted or not) resets the ticket counter and
+  // publishes this call's epoch for the next call.
+  if (tid == 0) {
+    __threadfence();
+    if (atomicAdd(done, 1u) == (unsigned)nblk - 1) {
+      *ticket = 0u;
+      *done = 0u;
+      __threadfence();
+      atomicExch(epoch_word, epoch);
+    }
+  }
+}
+
+template <typename T>
+coral_status_t trsv_g(Handle* H, int uplo, int trans, int diag, size_t n, const void* matrix, size_t lda,
+                      void* x, size_t incx, size_t align) {
+  if (uplo != CORAL_UPPER && uplo != CORAL_LOWER) return bad_arg(H, 1);
+  if (trans < CORAL_NO_TRANSPOSE || trans > CORAL_CONJ_TRANSPOSE) return bad_arg(H, 2);
+  if (diag != CORAL_UNIT && diag != CORAL_NON_UNIT) return bad_arg(H, 3);
+  if (n == 0) return CORAL_OK;
+  if (!matrix) return bad_arg(H, 5);
+  if (lda < n) return bad_arg(H, 6);
+  if (!x) return bad_arg(H, 7);
+  if (incx == 0) return bad_arg(H, 8);
+  if (((uintptr_t)matrix | (uintptr_t)x) & (align - 1)) return bad_arg(H, 5);
+  if (n > (size_t)INT32_MAX) return CORAL_ERR_NOT_SUPPORTED;
+  const size_t nblk = (n + kTB - 1) / kTB;
+  if (H->trsv_slots_len < nblk * kTB) {
+    if (H->trsv_slots) {
+      CORAL_CUDA(H, cudaStreamSynchronize(H->stream));
+      cudaFree(H->trsv_slots);
+      H->trsv_slots = nullptr;
+      H->trsv_slots_len = 0;
+    }
+    const size_t len = ((nblk * kTB + 65535) / 65536) * 65536;
+    CORAL_CUDA(H, cudaMalloc(&H->trsv_slots, len * sizeof(unsigned long long)));
+    CORAL_CUDA(H, cudaMemsetAsync(H->trsv_slots, 0, len * sizeof(unsigned long long), H->stream));
+    H->trsv_slots_len = len;
+  }
+  const bool t = trans != CORAL_NO_TRANSPOSE;
+  const bool cj = trans == CORAL_CONJ_TRANSPOSE && !std::is_same<T, double>::value;
+  const bool lower_eff = (uplo == CORAL_LOWER) != t;
+  const size_t smem = (size_t)kTB * (kTB + 1) * sizeof(T);
+  static uint64_t attr_devices[2] = {0, 0};
+  const uint64_t bit = H->device < 64 ? (1ull << H->device) : 0;
+  if (!(attr_devices[cj] & bit) || !bit) {
+    if (cj)
+      CORAL_CUDA(H, cudaFuncSetAttribute(k_trsv_g<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    else
+      CORAL_CUDA(H, cudaFuncSetAttribute(k_trsv_g<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_devices[cj] |= bit;
+  }
+  T* X = static_cast<T*>(x);
+  const T* Am = static_cast<const T*>(matrix);
+  timed_begin(H);
+#define CORAL_TRSV_G(CJ)                                                                                \
+  k_trsv_g<T, CJ><<<(unsigned)nblk, kTThr, smem, H->stream>>>(                                          \
+      (int)n, Am, lda, X, incx, lower_eff, t, diag == CORAL_UNIT, H->trsv_slots, &H->words->trsv_ticket, \
+      &H->words->trsv_done, &H->words->trsv_epoch, &H->words->status, H->wait_limit * 32ull)
+  if (cj) CORAL_TRSV_G(true);
+  else CORAL_TRSV_G(false);
+#undef CORAL_TRSV_G
+  coral_status_t s = launch_status(H);
+  timed_end(H);
+  return s;
+}
+
+}  // namespace
+}  // namespace coral
+
+using namespace coral;
+
+extern "C" {
+
+coral_status_t coral_dtrsv(coral_handle_t hh, int uplo, int trans, int diag, size_t n, const double* matrix,
+                           size_t lda, double* x, size_t incx) {
+  CORAL_HANDLE(hh);
+  return trsv_g<double>(H, uplo, trans, diag, n, matrix, lda, x, incx, 8);
+}
+
+coral_status_t coral_ctrsv(coral_handle_t hh, int uplo, int trans, int diag, size_t n, const float* matrix,
+                           size_t lda, float* x, size_t incx) {
+  CORAL_HANDLE(hh);
+  return trsv_g<float2>(H, uplo, trans, diag, n, matrix, lda, x, incx, 8);
+}
+
+coral_status_t coral_ztrsv(coral_handle_t hh, int uplo, int trans, int diag, size_t n, const double* matrix,
+                           size_t lda, double* x, size_t incx) {
+  CORAL_HANDLE(hh);
+  return trsv_g<double2>(H, uplo, trans, diag, n, matrix, lda, x, incx, 16);
+}
+
+}  // extern "C"

@@ -174,6 +174,15 @@ coral_status_t coral_ctrmv(coral_handle_t h, int uplo, int trans, int diag, size
 /* ztrmv.rs -- interleaved complex128; trans N, T or C */
 coral_status_t coral_ztrmv(coral_handle_t h, int uplo, int trans, int diag, size_t n,
                            const double* matrix, size_t lda, double* x, size_t incx);
+/* dtrsv.rs -- double; ConjugateTranspose == Transpose */
+coral_status_t coral_dtrsv(coral_handle_t h, int uplo, int trans, int diag, size_t n,
+                           const double* matrix, size_t lda, double* x, size_t incx);
+/* ctrsv.rs -- interleaved complex64; trans N, T or C */
+coral_status_t coral_ctrsv(coral_handle_t h, int uplo, int trans, int diag, size_t n,
+                           const float* matrix, size_t lda, float* x, size_t incx);
+/* ztrsv.rs -- interleaved complex128; trans N, T or C */
+coral_status_t coral_ztrsv(coral_handle_t h, int uplo, int trans, int diag, size_t n,
+                           const double* matrix, size_t lda, double* x, size_t incx);
 /* strsv.rs:60-74 */
 coral_status_t coral_strsv(coral_handle_t h, int uplo, int trans, int diag, size_t n,
                            const float* matrix, size_t lda, float* x, size_t incx);

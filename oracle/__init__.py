@@ -76,6 +76,9 @@ def _declare(L: C.CDLL) -> None:
     L.or_dsyr_f64.argtypes = [_i, _sz, C.c_double, _dp, _sz, _dp, _sz, _i, _dp, _sz]
     L.or_cher_f64.argtypes = [_i, _sz, _fp, _fp, _sz, _fp, _sz, _i, _dp, _sz]
     L.or_zher_f64.argtypes = [_i, _sz, _dp, _dp, _sz, _dp, _sz, _i, _dp, _sz]
+    L.or_dtrsv_f64.argtypes = [_i, _i, _i, _sz, _dp, _sz, _dp, _sz, _dp]
+    L.or_ctrsv_f64.argtypes = [_i, _i, _i, _sz, _fp, _sz, _fp, _sz, _dp]
+    L.or_ztrsv_f64.argtypes = [_i, _i, _i, _sz, _dp, _sz, _dp, _sz, _dp]
     L.or_strsv_f64.argtypes = [_i, _i, _i, _sz, _fp, _sz, _fp, _sz, _dp]
     L.or_strmv_f64.argtypes = [_i, _i, _i, _sz, _fp, _sz, _fp, _sz, _dp]
     L.or_sger_exact.argtypes = [_sz, _sz, C.c_float, _fp, _sz, _fp, _sz, _fp, _sz]
@@ -289,6 +292,21 @@ def her(kind, uplo, n, alpha, x, incx, a, lda, y=None, incy=1) -> np.ndarray:
         lib().or_zher_f64(uplo, n, _d(al), _c128d(x), incx, _c128d(yy), incy if two else incx, int(two),
                           _d(a.view(np.float64)), lda)
     return a
+
+
+def trsv_dcz(kind, uplo, trans, diag, n, a, lda, x, incx) -> np.ndarray:
+    """d/c/z TRSV solution (float64 or complex128), by long-double substitution."""
+    if kind == "d":
+        out = np.zeros(max(n, 1), np.float64)
+        f = lambda v: _d(np.ascontiguousarray(v, np.float64))  # noqa: E731
+        lib().or_dtrsv_f64(uplo, trans, diag, n, f(a), lda, f(x), incx, _d(out))
+        return out[:n]
+    out = np.zeros(2 * max(n, 1), np.float64)
+    if kind == "c":
+        lib().or_ctrsv_f64(uplo, trans, diag, n, _c64f(a), lda, _c64f(x), incx, _d(out))
+    else:
+        lib().or_ztrsv_f64(uplo, trans, diag, n, _c128d(a), lda, _c128d(x), incx, _d(out))
+    return out.view(np.complex128)[:n]
 
 
 def strmv(uplo, trans, diag, n, a, lda, x, incx) -> np.ndarray:

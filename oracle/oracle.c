@@ -554,6 +554,59 @@ void or_dsyr_f64(int uplo, size_t n, double alpha, const double* x, size_t incx,
 OR_CHER(or_cher_f64, float)
 OR_CHER(or_zher_f64, double)
 
+/* level2/dtrsv.rs, ctrsv.rs, ztrsv.rs (the *trlsv / *trusv files): solve
+ * op(A) x = b by substitution in long double (64-bit significand), op N, T
+ * or C, unit diagonal = 1; only the `uplo` triangle is read.  Complex data
+ * interleaved.  Output in double. */
+#define OR_TRSV_BODY(CPLX)                                                                      \
+  const int t = trans != NOTRANS, cj = trans == CONJTRANS;                                      \
+  const int lower_eff = (uplo == LOWER) != t;                                                   \
+  long double* vr = (long double*)malloc(sizeof(long double) * (n ? n : 1));                    \
+  long double* vi = (long double*)malloc(sizeof(long double) * (n ? n : 1));                    \
+  for (size_t i = 0; i < n; ++i) {                                                              \
+    vr[i] = CPLX ? x[2 * i * incx] : x[i * incx];                                               \
+    vi[i] = CPLX ? x[2 * i * incx + 1] : 0;                                                     \
+  }                                                                                             \
+  for (size_t s = 0; s < n; ++s) {                                                              \
+    size_t i = lower_eff ? s : n - 1 - s;                                                       \
+    long double sr = vr[i], si = vi[i];                                                         \
+    for (size_t s2 = 0; s2 < s; ++s2) {                                                         \
+      size_t k = lower_eff ? s2 : n - 1 - s2;                                                   \
+      size_t e = t ? k + i * lda : i + k * lda;                                                 \
+      long double ar = CPLX ? A[2 * e] : A[e];                                                  \
+      long double ai = CPLX ? (cj ? -(long double)A[2 * e + 1] : (long double)A[2 * e + 1]) : 0; \
+      sr -= ar * vr[k] - ai * vi[k];                                                            \
+      si -= ar * vi[k] + ai * vr[k];                                                            \
+    }                                                                                           \
+    if (diag != UNIT) {                                                                         \
+      size_t e = i + i * lda;                                                                   \
+      long double dr = CPLX ? A[2 * e] : A[e];                                                  \
+      long double di = CPLX ? (cj ? -(long double)A[2 * e + 1] : (long double)A[2 * e + 1]) : 0; \
+      long double den = dr * dr + di * di;                                                      \
+      long double qr = (sr * dr + si * di) / den, qi = (si * dr - sr * di) / den;               \
+      sr = qr; si = qi;                                                                         \
+    }                                                                                           \
+    vr[i] = sr; vi[i] = si;                                                                     \
+  }                                                                                             \
+  for (size_t i = 0; i < n; ++i) {                                                              \
+    if (CPLX) { x_out[2 * i] = (double)vr[i]; x_out[2 * i + 1] = (double)vi[i]; }               \
+    else x_out[i] = (double)vr[i];                                                              \
+  }                                                                                             \
+  free(vr); free(vi);
+
+void or_dtrsv_f64(int uplo, int trans, int diag, size_t n, const double* A, size_t lda,
+                  const double* x, size_t incx, double* x_out) {
+  OR_TRSV_BODY(0)
+}
+void or_ctrsv_f64(int uplo, int trans, int diag, size_t n, const float* A, size_t lda,
+                  const float* x, size_t incx, double* x_out) {
+  OR_TRSV_BODY(1)
+}
+void or_ztrsv_f64(int uplo, int trans, int diag, size_t n, const double* A, size_t lda,
+                  const double* x, size_t incx, double* x_out) {
+  OR_TRSV_BODY(1)
+}
+
 /* level2/sger.rs:68-132 (bit-exact): unit strides go through saxpy per
  * column (fused first m - m%8 rows, `+= a*x` for the rest), strided through
  * mul_add; a column whose coefficient alpha*y_j is 0 is skipped. */

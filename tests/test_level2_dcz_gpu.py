@@ -169,3 +169,74 @@ def test_trmv_dcz(cuda, dt, n, lda, uplo, trans, diag):
     if inc > 1:
         holes = np.arange(x.size) % inc != 0
         np.testing.assert_array_equal(got[holes], x[holes])
+
+
+# ---- D/C/Z TRSV (dtrsv.rs, ctrsv.rs, ztrsv.rs) --------------------------------
+# diag = n + U[0,1] (as the strsv configuration) keeps the systems well posed;
+# for a unit diagonal the off-diagonal is scaled by 1/n.  NaN fills the
+# unstored triangle and, for a unit diagonal, the diagonal.
+KIND = {np.float64: "d", np.complex64: "c", np.complex128: "z"}
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.complex64, np.complex128], ids=["d", "c", "z"])
+@pytest.mark.parametrize("n,lda", [(1, 1), (7, 7), (64, 64), (65, 70), (127, 132), (300, 300), (2049, 2050)])
+@pytest.mark.parametrize("uplo", [0, 1])
+@pytest.mark.parametrize("trans", [0, 1, 2])
+@pytest.mark.parametrize("diag", [0, 1])
+def test_trsv_dcz(cuda, dt, n, lda, uplo, trans, diag):
+    rng = np.random.default_rng(n * 13 + uplo + 3 * trans + 7 * diag)
+    a = tri(rng, n, lda, uplo, dt, nan_diag=(diag == 0))
+    if diag == 0:
+        a = np.where(np.isnan(a), a, a / dt(n).real)
+    else:
+        d = np.arange(n)
+        a[d, d] = a[d, d] + dt(n + rng.uniform(0, 1))
+    inc = 3 if n == 127 else 1
+    x = rnd(rng, (n - 1) * inc + 1, dt)
+    X = torch.from_numpy(x.copy()).cuda()
+    fn = {np.float64: cb.dtrsv, np.complex64: cb.ctrsv, np.complex128: cb.ztrsv}[dt]
+    fn(uplo, trans, diag, n, torch.from_numpy(a.ravel()).cuda(), lda, X, inc)
+    torch.cuda.synchronize()
+    got = X.cpu().numpy()
+    want = oracle.trsv_dcz(KIND[dt], uplo, trans, diag, n, a.ravel(), lda, x, inc)
+    g = got[::inc][:n]
+    assert np.isfinite(g).all()
+    tol = 1e-4 if dt == np.complex64 else 1e-12   # strsv_tests.rs:213-214 tolerance for fp32
+    assert (np.abs(g - want) <= tol * (np.abs(want) + 1e-3)).all(), np.abs(g - want).max()
+    if inc > 1:
+        holes = np.arange(x.size) % inc != 0
+        np.testing.assert_array_equal(got[holes], x[holes])
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.complex128], ids=["d", "z"])
+def test_trsv_dcz_repeated_and_timeout(cuda, dt):
+    """Back-to-back solves reuse the ready flags by epoch; a ~32 ns wait limit
+    makes blocks give up (status CORAL_ERR_TIMEOUT, no fault) and the next
+    solve with the default limit is correct."""
+    n = 2048
+    rng = np.random.default_rng(77)
+    a = tri(rng, n, n, 1, dt)
+    d = np.arange(n)
+    a[d, d] = a[d, d] + n
+    x = rnd(rng, n, dt)
+    A = torch.from_numpy(a.ravel()).cuda()
+    fn = cb.dtrsv if dt == np.float64 else cb.ztrsv
+    want = oracle.trsv_dcz(KIND[dt], 1, 0, 1, n, a.ravel(), n, x, 1)
+    for _ in range(3):
+        X = torch.from_numpy(x.copy()).cuda()
+        fn(1, 0, 1, n, A, n, X, 1)
+        torch.cuda.synchronize()
+        assert np.allclose(X.cpu().numpy(), want, rtol=1e-12, atol=1e-15)
+    h = cb.handle()
+    h.set_wait_limit(1)
+    try:
+        fn(1, 0, 1, n, A, n, torch.from_numpy(x.copy()).cuda(), 1)
+        with pytest.raises(cb.CoralError) as e:
+            h.sync()
+        assert e.value.status == 3
+    finally:
+        h.set_wait_limit(0)
+    X = torch.from_numpy(x.copy()).cuda()
+    fn(1, 0, 1, n, A, n, X, 1)
+    h.sync()
+    assert np.allclose(X.cpu().numpy(), want, rtol=1e-12, atol=1e-15)
