@@ -460,6 +460,54 @@ def level12_bandwidth(torch, cb, lib, h, dev, g, routines=None):
     if want("saxpy"):
         rec("saxpy", 12 * n1, timed_calls(lambda: cb.saxpy(n1, 0.5, x, 1, y, 1), 20, False))
     del x, y
+    # double / complex level 1 at 2^25 elements per vector (complex128: 512 MiB):
+    # (name, kind, vectors moved per element, call); reductions write their
+    # scalar to device memory (pointer mode 1) so the calls can be captured.
+    n2 = 1 << 25
+    P = lambda t: vp(t.data_ptr())  # noqa: E731
+    rq = vp(res.data_ptr())
+    l1_specs = [
+        ("ddot", "d", 2, lambda X, Y: lib.coral_ddot(h.h, n2, P(X), 1, P(Y), 1, rq)),
+        ("cdotc", "c", 2, lambda X, Y: lib.coral_cdotc(h.h, n2, P(X), 1, P(Y), 1, rq)),
+        ("zdotc", "z", 2, lambda X, Y: lib.coral_zdotc(h.h, n2, P(X), 1, P(Y), 1, rq)),
+        ("dasum", "d", 1, lambda X, Y: lib.coral_dasum(h.h, n2, P(X), 1, rq)),
+        ("dzasum", "z", 1, lambda X, Y: lib.coral_dzasum(h.h, n2, P(X), 1, rq)),
+        ("dnrm2", "d", 1, lambda X, Y: lib.coral_dnrm2(h.h, n2, P(X), 1, rq)),
+        ("dznrm2", "z", 1, lambda X, Y: lib.coral_dznrm2(h.h, n2, P(X), 1, rq)),
+        ("idamax", "d", 1, lambda X, Y: lib.coral_idamax(h.h, n2, P(X), 1, rq)),
+        ("izamax", "z", 1, lambda X, Y: lib.coral_izamax(h.h, n2, P(X), 1, rq)),
+        ("daxpy", "d", 3, lambda X, Y: cb.daxpy(n2, 0.5, X, 1, Y, 1)),
+        ("zaxpy", "z", 3, lambda X, Y: cb.zaxpy(n2, 0.5 - 0.25j, X, 1, Y, 1)),
+        ("dscal", "d", 2, lambda X, Y: cb.dscal(n2, 0.999, X, 1)),
+        ("zscal", "z", 2, lambda X, Y: cb.zscal(n2, 0.6 + 0.8j, X, 1)),
+        ("zdscal", "z", 2, lambda X, Y: cb.zdscal(n2, 0.999, X, 1)),
+        ("dcopy", "d", 2, lambda X, Y: cb.dcopy(n2, X, 1, Y, 1)),
+        ("zcopy", "z", 2, lambda X, Y: cb.zcopy(n2, X, 1, Y, 1)),
+        ("dswap", "d", 4, lambda X, Y: cb.dswap(n2, X, 1, Y, 1)),
+        ("zswap", "z", 4, lambda X, Y: cb.zswap(n2, X, 1, Y, 1)),
+        ("srot", "s", 4, lambda X, Y: cb.srot(n2, X, 1, Y, 1, 0.6, 0.8)),
+        ("drot", "d", 4, lambda X, Y: cb.drot(n2, X, 1, Y, 1, 0.6, 0.8)),
+        ("zdrot", "z", 4, lambda X, Y: cb.zdrot(n2, X, 1, Y, 1, 0.6, 0.8)),
+        ("drotm", "d", 4, lambda X, Y: cb.drotm(n2, X, 1, Y, 1, [-1.0, 0.6, -0.8, 0.8, 0.6])),
+    ]
+    l1_dtype = {"s": (torch.float32, 4), "d": (torch.float64, 8), "c": (torch.complex64, 8),
+                "z": (torch.complex128, 16)}
+    for kind in "sdcz":
+        specs = [s for s in l1_specs if s[1] == kind and want(s[0])]
+        if not specs:
+            continue
+        dt, es = l1_dtype[kind]
+        X = torch.empty(n2, dtype=dt, device=dev)
+        Y = torch.empty(n2, dtype=dt, device=dev)
+        for t in (X, Y):
+            (torch.view_as_real(t) if dt.is_complex else t).uniform_(-1, 1, generator=g)
+        h.set_pointer_mode(1)
+        try:
+            for name, _, vecs, call in specs:
+                rec(name, vecs * es * n2, timed_calls(lambda call=call: call(X, Y), 20, False))
+        finally:
+            h.set_pointer_mode(0)
+        del X, Y
     m = 8192
     A = torch.empty(m * m, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
     xv = torch.empty(m, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)

@@ -12,6 +12,9 @@ from .blas import (  # noqa: F401
     strsv_batched, sgemm_problem_dtype, strsv_problem_dtype, dgemv, cgemv, zgemv,
     dsymv, zhemv, dtrmv, ctrmv, ztrmv, dger, cgeru, cgerc, zgeru, zgerc, dsyr, dsyr2, cher, zher,
     cher2, zher2, dtrsv, ctrsv, ztrsv,
+    ddot, cdotu, cdotc, zdotu, zdotc, sasum, dasum, scasum, dzasum, dnrm2, scnrm2, dznrm2, idamax,
+    icamax, izamax, daxpy, caxpy, zaxpy, dscal, cscal, zscal, csscal, zdscal, dcopy, ccopy, zcopy,
+    dswap, cswap, zswap, srot, drot, csrot, zdrot, srotm, drotm, srotg, drotg, srotmg, drotmg,
 )
 
 __all__ = [
@@ -22,4 +25,7 @@ __all__ = [
     "strsv_problem_dtype", "dgemv", "cgemv", "zgemv",
     "dsymv", "zhemv", "dtrmv", "ctrmv", "ztrmv", "dger", "cgeru", "cgerc", "zgeru", "zgerc", "dsyr",
     "dsyr2", "cher", "zher", "cher2", "zher2", "dtrsv", "ctrsv", "ztrsv",
+    "ddot", "cdotu", "cdotc", "zdotu", "zdotc", "sasum", "dasum", "scasum", "dzasum", "dnrm2", "scnrm2", "dznrm2",
+    "idamax", "icamax", "izamax", "daxpy", "caxpy", "zaxpy", "dscal", "cscal", "zscal", "csscal", "zdscal", "dcopy",
+    "ccopy", "zcopy", "dswap", "cswap", "zswap", "srot", "drot", "csrot", "zdrot", "srotm", "drotm", "srotg", "drotg", "srotmg", "drotmg",
 ]

@@ -51,6 +51,45 @@ SIGNATURES = {
     "coral_scopy": [_h, _sz, _vp, _sz, _vp, _sz],
     "coral_sswap": [_h, _sz, _vp, _sz, _vp, _sz],
     "coral_sscal": [_h, _sz, _f, _vp, _sz],
+    "coral_ddot": [_h, _sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_cdotu": [_h, _sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_cdotc": [_h, _sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_zdotu": [_h, _sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_zdotc": [_h, _sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_sasum": [_h, _sz, _vp, _sz, _vp],
+    "coral_dasum": [_h, _sz, _vp, _sz, _vp],
+    "coral_scasum": [_h, _sz, _vp, _sz, _vp],
+    "coral_dzasum": [_h, _sz, _vp, _sz, _vp],
+    "coral_dnrm2": [_h, _sz, _vp, _sz, _vp],
+    "coral_scnrm2": [_h, _sz, _vp, _sz, _vp],
+    "coral_dznrm2": [_h, _sz, _vp, _sz, _vp],
+    "coral_idamax": [_h, _sz, _vp, _sz, _vp],
+    "coral_icamax": [_h, _sz, _vp, _sz, _vp],
+    "coral_izamax": [_h, _sz, _vp, _sz, _vp],
+    "coral_daxpy": [_h, _sz, _d, _vp, _sz, _vp, _sz],
+    "coral_caxpy": [_h, _sz, _vp, _vp, _sz, _vp, _sz],
+    "coral_zaxpy": [_h, _sz, _vp, _vp, _sz, _vp, _sz],
+    "coral_dscal": [_h, _sz, _d, _vp, _sz],
+    "coral_cscal": [_h, _sz, _vp, _vp, _sz],
+    "coral_zscal": [_h, _sz, _vp, _vp, _sz],
+    "coral_csscal": [_h, _sz, _f, _vp, _sz],
+    "coral_zdscal": [_h, _sz, _d, _vp, _sz],
+    "coral_dcopy": [_h, _sz, _vp, _sz, _vp, _sz],
+    "coral_ccopy": [_h, _sz, _vp, _sz, _vp, _sz],
+    "coral_zcopy": [_h, _sz, _vp, _sz, _vp, _sz],
+    "coral_dswap": [_h, _sz, _vp, _sz, _vp, _sz],
+    "coral_cswap": [_h, _sz, _vp, _sz, _vp, _sz],
+    "coral_zswap": [_h, _sz, _vp, _sz, _vp, _sz],
+    "coral_srot": [_h, _sz, _vp, _sz, _vp, _sz, _f, _f],
+    "coral_drot": [_h, _sz, _vp, _sz, _vp, _sz, _d, _d],
+    "coral_csrot": [_h, _sz, _vp, _sz, _vp, _sz, _f, _f],
+    "coral_zdrot": [_h, _sz, _vp, _sz, _vp, _sz, _d, _d],
+    "coral_srotm": [_h, _sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_drotm": [_h, _sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_srotg": [_h, _vp, _vp, _vp, _vp],
+    "coral_drotg": [_h, _vp, _vp, _vp, _vp],
+    "coral_srotmg": [_h, _vp, _vp, _vp, _f, _vp],
+    "coral_drotmg": [_h, _vp, _vp, _vp, _d, _vp],
     "coral_sgemv": [_h, _i, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
     "coral_dgemv": [_h, _i, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz],
     "coral_cgemv": [_h, _i, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],

@@ -219,6 +219,247 @@ def sscal(n, alpha, x, incx) -> None:
     handle().call("coral_sscal", n, alpha, _ptr(x, _f32(), "x"), incx)
 
 
+# Double and complex level 1: complex vectors are complex64 / complex128
+# tensors (or float32 / float64 interleaved), increments in complex elements.
+_L1_KIND = {"s": (_f32, C.c_float), "d": (_f64, C.c_double), "c": (_c64, C.c_float), "z": (_c128, C.c_double)}
+
+
+def _reduce_scalar(name, kind, n, x, incx, out_ctype):
+    dt = _L1_KIND[kind][0]
+    r = out_ctype()
+    handle().call(name, n, _ptr(x, dt(), "x"), incx, C.cast(C.byref(r), C.c_void_p))
+    return r.value
+
+
+def ddot(n, x, incx, y, incy) -> float:
+    """level1/ddot.rs:43-163."""
+    r = C.c_double()
+    handle().call("coral_ddot", n, _ptr(x, _f64(), "x"), incx, _ptr(y, _f64(), "y"), incy,
+                  C.cast(C.byref(r), C.c_void_p))
+    return r.value
+
+
+def _cdot(name, kind, n, x, incx, y, incy) -> complex:
+    dt, ct = _L1_KIND[kind]
+    r = (ct * 2)()
+    handle().call(name, n, _ptr(x, dt(), "x"), incx, _ptr(y, dt(), "y"), incy, C.cast(r, C.c_void_p))
+    return complex(r[0], r[1])
+
+
+def cdotu(n, x, incx, y, incy) -> complex:
+    """level1/cdotu.rs:46-178: sum x_i y_i."""
+    return _cdot("coral_cdotu", "c", n, x, incx, y, incy)
+
+
+def cdotc(n, x, incx, y, incy) -> complex:
+    """level1/cdotc.rs:46-176: sum conj(x_i) y_i."""
+    return _cdot("coral_cdotc", "c", n, x, incx, y, incy)
+
+
+def zdotu(n, x, incx, y, incy) -> complex:
+    """level1/zdotu.rs:45-176."""
+    return _cdot("coral_zdotu", "z", n, x, incx, y, incy)
+
+
+def zdotc(n, x, incx, y, incy) -> complex:
+    """level1/zdotc.rs:45-175."""
+    return _cdot("coral_zdotc", "z", n, x, incx, y, incy)
+
+
+def sasum(n, x, incx) -> float:
+    """level1/sasum.rs:40-107."""
+    return _reduce_scalar("coral_sasum", "s", n, x, incx, C.c_float)
+
+
+def dasum(n, x, incx) -> float:
+    """level1/dasum.rs:41-110."""
+    return _reduce_scalar("coral_dasum", "d", n, x, incx, C.c_double)
+
+
+def scasum(n, x, incx) -> float:
+    """level1/scasum.rs:40-108: sum |re| + |im|."""
+    return _reduce_scalar("coral_scasum", "c", n, x, incx, C.c_float)
+
+
+def dzasum(n, x, incx) -> float:
+    """level1/dzasum.rs:40-111."""
+    return _reduce_scalar("coral_dzasum", "z", n, x, incx, C.c_double)
+
+
+def dnrm2(n, x, incx) -> float:
+    """level1/dnrm2.rs:45-152."""
+    return _reduce_scalar("coral_dnrm2", "d", n, x, incx, C.c_double)
+
+
+def scnrm2(n, x, incx) -> float:
+    """level1/scnrm2.rs:44-155."""
+    return _reduce_scalar("coral_scnrm2", "c", n, x, incx, C.c_float)
+
+
+def dznrm2(n, x, incx) -> float:
+    """level1/dznrm2.rs:43-156."""
+    return _reduce_scalar("coral_dznrm2", "z", n, x, incx, C.c_double)
+
+
+def idamax(n, x, incx) -> int:
+    """level1/idamax.rs:43-159 (0-based index)."""
+    return _reduce_scalar("coral_idamax", "d", n, x, incx, C.c_size_t)
+
+
+def icamax(n, x, incx) -> int:
+    """level1/icamax.rs:48-166: first max |re| + |im| (0-based)."""
+    return _reduce_scalar("coral_icamax", "c", n, x, incx, C.c_size_t)
+
+
+def izamax(n, x, incx) -> int:
+    """level1/izamax.rs:33-163."""
+    return _reduce_scalar("coral_izamax", "z", n, x, incx, C.c_size_t)
+
+
+def daxpy(n, alpha, x, incx, y, incy) -> None:
+    """level1/daxpy.rs:42-133."""
+    handle().call("coral_daxpy", n, float(alpha), _ptr(x, _f64(), "x"), incx, _ptr(y, _f64(), "y"), incy)
+
+
+def caxpy(n, alpha, x, incx, y, incy) -> None:
+    """level1/caxpy.rs:45-172 (alpha: complex or [re, im])."""
+    pa, ka = _pair(_cscalar(alpha), C.c_float)
+    handle().call("coral_caxpy", n, pa, _ptr(x, _c64(), "x"), incx, _ptr(y, _c64(), "y"), incy)
+
+
+def zaxpy(n, alpha, x, incx, y, incy) -> None:
+    """level1/zaxpy.rs:44-172."""
+    pa, ka = _pair(_cscalar(alpha), C.c_double)
+    handle().call("coral_zaxpy", n, pa, _ptr(x, _c128(), "x"), incx, _ptr(y, _c128(), "y"), incy)
+
+
+def dscal(n, alpha, x, incx) -> None:
+    """level1/dscal.rs:30-66."""
+    handle().call("coral_dscal", n, float(alpha), _ptr(x, _f64(), "x"), incx)
+
+
+def cscal(n, alpha, x, incx) -> None:
+    """level1/cscal.rs:43-111."""
+    pa, ka = _pair(_cscalar(alpha), C.c_float)
+    handle().call("coral_cscal", n, pa, _ptr(x, _c64(), "x"), incx)
+
+
+def zscal(n, alpha, x, incx) -> None:
+    """level1/zscal.rs:41-109."""
+    pa, ka = _pair(_cscalar(alpha), C.c_double)
+    handle().call("coral_zscal", n, pa, _ptr(x, _c128(), "x"), incx)
+
+
+def csscal(n, alpha, x, incx) -> None:
+    """level1/csscal.rs:39-88: real alpha, complex64 x."""
+    handle().call("coral_csscal", n, float(alpha), _ptr(x, _c64(), "x"), incx)
+
+
+def zdscal(n, alpha, x, incx) -> None:
+    """level1/zdscal.rs:38-88: real alpha, complex128 x."""
+    handle().call("coral_zdscal", n, float(alpha), _ptr(x, _c128(), "x"), incx)
+
+
+def _xy(name, kind, n, x, incx, y, incy, *extra) -> None:
+    dt = _L1_KIND[kind][0]
+    handle().call(name, n, _ptr(x, dt(), "x"), incx, _ptr(y, dt(), "y"), incy, *extra)
+
+
+def dcopy(n, x, incx, y, incy) -> None:
+    """level1/dcopy.rs:28-57."""
+    _xy("coral_dcopy", "d", n, x, incx, y, incy)
+
+
+def ccopy(n, x, incx, y, incy) -> None:
+    """level1/ccopy.rs:29-58."""
+    _xy("coral_ccopy", "c", n, x, incx, y, incy)
+
+
+def zcopy(n, x, incx, y, incy) -> None:
+    """level1/zcopy.rs:28-61."""
+    _xy("coral_zcopy", "z", n, x, incx, y, incy)
+
+
+def dswap(n, x, incx, y, incy) -> None:
+    """level1/dswap.rs:35-119."""
+    _xy("coral_dswap", "d", n, x, incx, y, incy)
+
+
+def cswap(n, x, incx, y, incy) -> None:
+    """level1/cswap.rs:36-120."""
+    _xy("coral_cswap", "c", n, x, incx, y, incy)
+
+
+def zswap(n, x, incx, y, incy) -> None:
+    """level1/zswap.rs:35-120."""
+    _xy("coral_zswap", "z", n, x, incx, y, incy)
+
+
+def srot(n, x, incx, y, incy, c, s) -> None:
+    """level1/srot.rs:51-180."""
+    _xy("coral_srot", "s", n, x, incx, y, incy, float(c), float(s))
+
+
+def drot(n, x, incx, y, incy, c, s) -> None:
+    """level1/drot.rs:48-178."""
+    _xy("coral_drot", "d", n, x, incx, y, incy, float(c), float(s))
+
+
+def csrot(n, x, incx, y, incy, c, s) -> None:
+    """level1/csrot.rs:50-166: real c, s on complex64 vectors."""
+    _xy("coral_csrot", "c", n, x, incx, y, incy, float(c), float(s))
+
+
+def zdrot(n, x, incx, y, incy, c, s) -> None:
+    """level1/zdrot.rs:51-166."""
+    _xy("coral_zdrot", "z", n, x, incx, y, incy, float(c), float(s))
+
+
+def srotm(n, x, incx, y, incy, param) -> None:
+    """level1/srotm.rs:47-412: param = [flag, h11, h21, h12, h22]."""
+    p = (C.c_float * 5)(*[float(v) for v in param])
+    _xy("coral_srotm", "s", n, x, incx, y, incy, C.cast(p, C.c_void_p))
+
+
+def drotm(n, x, incx, y, incy, param) -> None:
+    """level1/drotm.rs:47-410."""
+    p = (C.c_double * 5)(*[float(v) for v in param])
+    _xy("coral_drotm", "d", n, x, incx, y, incy, C.cast(p, C.c_void_p))
+
+
+def _rotg(name, ct, a, b):
+    v = [ct(a), ct(b), ct(), ct()]
+    handle().call(name, *[C.cast(C.byref(t), C.c_void_p) for t in v])
+    return tuple(t.value for t in v)
+
+
+def srotg(a, b):
+    """level1/srotg.rs:40-75: returns (r, z, c, s) -- the updated a, b and c, s."""
+    return _rotg("coral_srotg", C.c_float, a, b)
+
+
+def drotg(a, b):
+    """level1/drotg.rs:40-71: returns (r, z, c, s)."""
+    return _rotg("coral_drotg", C.c_double, a, b)
+
+
+def _rotmg(name, ct, d1, d2, x1, y1):
+    v = [ct(d1), ct(d2), ct(x1)]
+    p = (ct * 5)()
+    handle().call(name, *[C.cast(C.byref(t), C.c_void_p) for t in v], ct(y1), C.cast(p, C.c_void_p))
+    return v[0].value, v[1].value, v[2].value, list(p)
+
+
+def srotmg(d1, d2, x1, y1):
+    """level1/srotmg.rs:42-199: returns (d1, d2, x1, param)."""
+    return _rotmg("coral_srotmg", C.c_float, d1, d2, x1, y1)
+
+
+def drotmg(d1, d2, x1, y1):
+    """level1/drotmg.rs:41-195: returns (d1, d2, x1, param)."""
+    return _rotmg("coral_drotmg", C.c_double, d1, d2, x1, y1)
+
+
 # ---------------------------------------------------------------- level 2 ----
 def sgemv(trans, n_rows, n_cols, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
     """level2/sgemv.rs:63-80."""

@@ -82,7 +82,8 @@ struct DeviceWords {
   unsigned trsv_done;     // TRSV: CTAs finished in the current call
   unsigned trsv_epoch;    // TRSV: epoch of the last completed call
   unsigned pad1;
-  unsigned char reserved[1024 - 4 * 32 - 64 - 16];
+  double stage[8];        // scalar arguments of the rotation constructors
+  unsigned char reserved[1024 - 4 * 32 - 64 - 16 - 64];
 };
 static_assert(sizeof(DeviceWords) == 1024, "DeviceWords layout");
 

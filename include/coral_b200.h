@@ -126,6 +126,109 @@ coral_status_t coral_sswap(coral_handle_t h, size_t n, float* x, size_t incx,
 coral_status_t coral_sscal(coral_handle_t h, size_t n, float alpha, float* x,
                            size_t incx);
 
+/* Double and complex level 1.  Complex vectors are interleaved (re, im) and
+ * increments count complex elements; complex scalars are [re, im] arrays.
+ * Scalar results follow the pointer mode like coral_sdot; complex results
+ * are written as two words. */
+/* ddot.rs:43-163 */
+coral_status_t coral_ddot(coral_handle_t h, size_t n, const double* x, size_t incx,
+                          const double* y, size_t incy, double* result);
+/* cdotu.rs:46-178 -- sum x_i y_i */
+coral_status_t coral_cdotu(coral_handle_t h, size_t n, const float* x, size_t incx,
+                           const float* y, size_t incy, float result[2]);
+/* cdotc.rs:46-176 -- sum conj(x_i) y_i */
+coral_status_t coral_cdotc(coral_handle_t h, size_t n, const float* x, size_t incx,
+                           const float* y, size_t incy, float result[2]);
+/* zdotu.rs:45-176 */
+coral_status_t coral_zdotu(coral_handle_t h, size_t n, const double* x, size_t incx,
+                           const double* y, size_t incy, double result[2]);
+/* zdotc.rs:45-175 */
+coral_status_t coral_zdotc(coral_handle_t h, size_t n, const double* x, size_t incx,
+                           const double* y, size_t incy, double result[2]);
+/* sasum.rs:40-107, dasum.rs:41-110 -- sum |x_i| */
+coral_status_t coral_sasum(coral_handle_t h, size_t n, const float* x, size_t incx,
+                           float* result);
+coral_status_t coral_dasum(coral_handle_t h, size_t n, const double* x, size_t incx,
+                           double* result);
+/* scasum.rs:40-108, dzasum.rs:40-111 -- sum |re| + |im| */
+coral_status_t coral_scasum(coral_handle_t h, size_t n, const float* x, size_t incx,
+                            float* result);
+coral_status_t coral_dzasum(coral_handle_t h, size_t n, const double* x, size_t incx,
+                            double* result);
+/* dnrm2.rs:45-152, scnrm2.rs:44-155, dznrm2.rs:43-156 */
+coral_status_t coral_dnrm2(coral_handle_t h, size_t n, const double* x, size_t incx,
+                           double* result);
+coral_status_t coral_scnrm2(coral_handle_t h, size_t n, const float* x, size_t incx,
+                            float* result);
+coral_status_t coral_dznrm2(coral_handle_t h, size_t n, const double* x, size_t incx,
+                            double* result);
+/* idamax.rs:43-159, icamax.rs:48-166, izamax.rs:33-163 -- 0-based index of
+ * the first max |x_i| (|re| + |im| for complex) */
+coral_status_t coral_idamax(coral_handle_t h, size_t n, const double* x, size_t incx,
+                            size_t* index);
+coral_status_t coral_icamax(coral_handle_t h, size_t n, const float* x, size_t incx,
+                            size_t* index);
+coral_status_t coral_izamax(coral_handle_t h, size_t n, const double* x, size_t incx,
+                            size_t* index);
+/* daxpy.rs:42-133, caxpy.rs:45-172, zaxpy.rs:44-172 */
+coral_status_t coral_daxpy(coral_handle_t h, size_t n, double alpha, const double* x,
+                           size_t incx, double* y, size_t incy);
+coral_status_t coral_caxpy(coral_handle_t h, size_t n, const float alpha[2],
+                           const float* x, size_t incx, float* y, size_t incy);
+coral_status_t coral_zaxpy(coral_handle_t h, size_t n, const double alpha[2],
+                           const double* x, size_t incx, double* y, size_t incy);
+/* dscal.rs:30-66, cscal.rs:43-111, zscal.rs:41-109, csscal.rs:39-88 and
+ * zdscal.rs:38-88 (real alpha on complex x) */
+coral_status_t coral_dscal(coral_handle_t h, size_t n, double alpha, double* x,
+                           size_t incx);
+coral_status_t coral_cscal(coral_handle_t h, size_t n, const float alpha[2], float* x,
+                           size_t incx);
+coral_status_t coral_zscal(coral_handle_t h, size_t n, const double alpha[2], double* x,
+                           size_t incx);
+coral_status_t coral_csscal(coral_handle_t h, size_t n, float alpha, float* x,
+                            size_t incx);
+coral_status_t coral_zdscal(coral_handle_t h, size_t n, double alpha, double* x,
+                            size_t incx);
+/* dcopy.rs:28-57, ccopy.rs:29-58, zcopy.rs:28-61 */
+coral_status_t coral_dcopy(coral_handle_t h, size_t n, const double* x, size_t incx,
+                           double* y, size_t incy);
+coral_status_t coral_ccopy(coral_handle_t h, size_t n, const float* x, size_t incx,
+                           float* y, size_t incy);
+coral_status_t coral_zcopy(coral_handle_t h, size_t n, const double* x, size_t incx,
+                           double* y, size_t incy);
+/* dswap.rs:35-119, cswap.rs:36-120, zswap.rs:35-120 */
+coral_status_t coral_dswap(coral_handle_t h, size_t n, double* x, size_t incx,
+                           double* y, size_t incy);
+coral_status_t coral_cswap(coral_handle_t h, size_t n, float* x, size_t incx,
+                           float* y, size_t incy);
+coral_status_t coral_zswap(coral_handle_t h, size_t n, double* x, size_t incx,
+                           double* y, size_t incy);
+/* srot.rs:51-180, drot.rs:48-178, csrot.rs:50-166, zdrot.rs:51-166 --
+ * x' = c x + s y, y' = c y - s x with real c, s */
+coral_status_t coral_srot(coral_handle_t h, size_t n, float* x, size_t incx, float* y,
+                          size_t incy, float c, float s);
+coral_status_t coral_drot(coral_handle_t h, size_t n, double* x, size_t incx, double* y,
+                          size_t incy, double c, double s);
+coral_status_t coral_csrot(coral_handle_t h, size_t n, float* x, size_t incx, float* y,
+                           size_t incy, float c, float s);
+coral_status_t coral_zdrot(coral_handle_t h, size_t n, double* x, size_t incx, double* y,
+                           size_t incy, double c, double s);
+/* srotm.rs:47-412, drotm.rs:47-410 -- param = [flag, h11, h21, h12, h22] in
+ * host memory */
+coral_status_t coral_srotm(coral_handle_t h, size_t n, float* x, size_t incx, float* y,
+                           size_t incy, const float param[5]);
+coral_status_t coral_drotm(coral_handle_t h, size_t n, double* x, size_t incx, double* y,
+                           size_t incy, const double param[5]);
+/* srotg.rs:40-75, drotg.rs:40-71 -- a, b, c, s follow the pointer mode */
+coral_status_t coral_srotg(coral_handle_t h, float* a, float* b, float* c, float* s);
+coral_status_t coral_drotg(coral_handle_t h, double* a, double* b, double* c, double* s);
+/* srotmg.rs:42-199, drotmg.rs:41-195 -- d1, d2, x1 and param follow the
+ * pointer mode; y1 by value */
+coral_status_t coral_srotmg(coral_handle_t h, float* d1, float* d2, float* x1, float y1,
+                            float param[5]);
+coral_status_t coral_drotmg(coral_handle_t h, double* d1, double* d2, double* x1,
+                            double y1, double param[5]);
+
 /* ---- level 2 (coral-aarch64/src/level2) --------------------------------- */
 /* sgemv.rs:63-80 */
 coral_status_t coral_sgemv(coral_handle_t h, int trans, size_t n_rows, size_t n_cols,

@@ -92,6 +92,20 @@ def _declare(L: C.CDLL) -> None:
     L.port_sgemv_t.argtypes = [_sz, _sz, C.c_float, _fp, _sz, _fp, C.c_float, _fp]
     L.port_sdot.argtypes = [_sz, _fp, _fp]
     L.port_sdot.restype = C.c_float
+    _vp = C.c_void_p
+    L.or_axpy_exact.argtypes = [_i, _sz, _dp, _vp, _sz, _vp, _sz]
+    L.or_scal_exact.argtypes = [_i, _sz, _dp, _vp, _sz]
+    L.or_rot_exact.argtypes = [_i, _sz, _vp, _sz, _vp, _sz, C.c_double, C.c_double]
+    L.or_rotm_exact.argtypes = [_i, _sz, _vp, _sz, _vp, _sz, _dp]
+    L.or_rotg_exact.argtypes = [_i, _dp]
+    L.or_rotmg_exact.argtypes = [_i, _dp, _dp]
+    L.or_iamax_exact.argtypes = [_i, _sz, _vp, _sz]
+    L.or_iamax_exact.restype = _sz
+    L.or_dot_f64.argtypes = [_i, _i, _sz, _vp, _sz, _vp, _sz, _dp]
+    L.or_asum_f64.argtypes = [_i, _sz, _vp, _sz]
+    L.or_asum_f64.restype = C.c_double
+    L.or_nrm2_f64.argtypes = [_i, _sz, _vp, _sz]
+    L.or_nrm2_f64.restype = C.c_double
 
 
 def _f(a: np.ndarray):
@@ -141,6 +155,113 @@ def sdot(n, x, incx, y, incy) -> float:
 
 def snrm2(n, x, incx) -> float:
     return float(lib().or_snrm2_f64(n, _f(x), incx))
+
+
+# ---- double and complex level 1 ----------------------------------------------
+# kind letters: s float32, d float64, c complex64, z complex128 (numpy arrays
+# of those dtypes, increments in elements).
+_KIND = {"s": (0, np.float32), "d": (1, np.float64), "c": (2, np.complex64), "z": (3, np.complex128)}
+
+
+def _vec(kind, a, copy=False):
+    dt = _KIND[kind][1]
+    a = np.array(a, dtype=dt, copy=True) if copy else np.ascontiguousarray(a, dt)
+    return a, C.c_void_p(a.ctypes.data)
+
+
+def axpy(kind, n, alpha, x, incx, y, incy):
+    """d/c/z axpy (bit-exact restatement) on a copy of y; returns it."""
+    al = np.array([complex(alpha).real, complex(alpha).imag], np.float64)
+    x, px = _vec(kind, x)
+    y, py = _vec(kind, y, copy=True)
+    lib().or_axpy_exact(_KIND[kind][0], n, _d(al), px, incx, py, incy)
+    return y
+
+
+def scal(kind, n, alpha, x, incx, real_alpha=False):
+    """d/c/z scal, or csscal / zdscal with real_alpha (bit-exact); returns a copy."""
+    al = np.array([complex(alpha).real, complex(alpha).imag], np.float64)
+    x, px = _vec(kind, x, copy=True)
+    k = _KIND[kind][0]
+    if real_alpha:
+        k = 4 if kind == "c" else 5
+    lib().or_scal_exact(k, n, _d(al), px, incx)
+    return x
+
+
+def copy(n, x, incx, y, incy):
+    """Any dtype: y[i*incy] = x[i*incx]; returns a copy of y."""
+    y = np.array(y, copy=True)
+    if n:
+        y[: (n - 1) * incy + 1: incy] = x[: (n - 1) * incx + 1: incx]
+    return y
+
+
+def swap(n, x, incx, y, incy):
+    x = np.array(x, copy=True)
+    y = np.array(y, copy=True)
+    if n:
+        sx, sy = slice(0, (n - 1) * incx + 1, incx), slice(0, (n - 1) * incy + 1, incy)
+        t = x[sx].copy()
+        x[sx] = y[sy]
+        y[sy] = t
+    return x, y
+
+
+def rot(kind, n, x, incx, y, incy, c, s):
+    """srot / drot / csrot / zdrot (bit-exact); returns (x', y') copies."""
+    x, px = _vec(kind, x, copy=True)
+    y, py = _vec(kind, y, copy=True)
+    lib().or_rot_exact(_KIND[kind][0], n, px, incx, py, incy, float(c), float(s))
+    return x, y
+
+
+def rotm(kind, n, x, incx, y, incy, param):
+    """srotm / drotm (bit-exact); returns (x', y') copies."""
+    p = np.asarray(param, np.float64)
+    x, px = _vec(kind, x, copy=True)
+    y, py = _vec(kind, y, copy=True)
+    lib().or_rotm_exact(_KIND[kind][0], n, px, incx, py, incy, _d(p))
+    return x, y
+
+
+def rotg(kind, a, b):
+    """srotg / drotg: returns (r, z, c, s) in the routine's precision."""
+    v = np.array([a, b, 0, 0], np.float64)
+    lib().or_rotg_exact(int(kind == "d"), _d(v))
+    return tuple(float(t) for t in v)
+
+
+def rotmg(kind, d1, d2, x1, y1):
+    """srotmg / drotmg: returns (d1, d2, x1, param)."""
+    v = np.array([d1, d2, x1, y1], np.float64)
+    p = np.zeros(5, np.float64)
+    lib().or_rotmg_exact(int(kind == "d"), _d(v), _d(p))
+    return float(v[0]), float(v[1]), float(v[2]), [float(t) for t in p]
+
+
+def iamax(kind, n, x, incx) -> int:
+    x, px = _vec(kind, x)
+    return int(lib().or_iamax_exact(_KIND[kind][0], n, px, incx))
+
+
+def dot(kind, conj, n, x, incx, y, incy) -> complex:
+    """ddot / cdotu / cdotc / zdotu / zdotc in double-double (complex result)."""
+    x, px = _vec(kind, x)
+    y, py = _vec(kind, y)
+    out = np.zeros(2, np.float64)
+    lib().or_dot_f64(_KIND[kind][0], int(conj), n, px, incx, py, incy, _d(out))
+    return complex(out[0], out[1])
+
+
+def asum(kind, n, x, incx) -> float:
+    x, px = _vec(kind, x)
+    return float(lib().or_asum_f64(_KIND[kind][0], n, px, incx))
+
+
+def nrm2(kind, n, x, incx) -> float:
+    x, px = _vec(kind, x)
+    return float(lib().or_nrm2_f64(_KIND[kind][0], n, px, incx))
 
 
 # ---- level 2 -----------------------------------------------------------------

@@ -114,6 +114,304 @@ double or_snrm2_f64(size_t n, const float* x, size_t incx) {
   return sqrt(dd_val(acc));
 }
 
+/* ---------------- double and complex level 1 ------------------------------
+ * kind: 0 = s (float), 1 = d (double), 2 = c (complex64), 3 = z (complex128);
+ * complex data interleaved, increments in complex elements.  The reference's
+ * unit-stride loops run a NEON body over the first n - n % W elements and a
+ * scalar tail; the body fuses where the tail rounds every product, so the
+ * exact restatements take `nf` = n - n % W (unit strides) or 0. */
+#define L1_LOAD(kind, p, i, re, im)                                           \
+  do {                                                                        \
+    if ((kind) == 0) { re = ((const float*)(p))[i]; im = 0; }                 \
+    else if ((kind) == 1) { re = ((const double*)(p))[i]; im = 0; }           \
+    else if ((kind) == 2) { re = ((const float*)(p))[2 * (i)]; im = ((const float*)(p))[2 * (i) + 1]; } \
+    else { re = ((const double*)(p))[2 * (i)]; im = ((const double*)(p))[2 * (i) + 1]; } \
+  } while (0)
+
+static size_t nf_of(size_t n, size_t incx, size_t incy, size_t w) {
+  return (incx == 1 && incy == 1) ? n - n % w : 0;
+}
+
+/* daxpy.rs:42-133 (W 4), caxpy.rs:45-172 (W 4), zaxpy.rs:44-172 (W 2):
+ * body y += a x fused (complex: yr = fma(ar, xr, yr), yr = fma(-ai, xi, yr),
+ * yi = fma(ar, xi, yi), yi = fma(ai, xr, yi)); tail y += a x /
+ * yr += ar xr - ai xi, yi += ar xi + ai xr.  n == 0 or alpha == 0 returns. */
+#define OR_AXPY_C(T, FMA)                                                       \
+  {                                                                           \
+    const T ar = (T)alpha[0], ai = (T)alpha[1];                               \
+    if (ar == 0 && ai == 0) return;                                           \
+    T* xx = (T*)x; T* yy = (T*)y;                                             \
+    for (size_t i = 0; i < n; ++i) {                                          \
+      T xr = xx[2 * i * incx], xi = xx[2 * i * incx + 1];                     \
+      T* yp = yy + 2 * i * incy;                                              \
+      if (i < nf) {                                                           \
+        yp[0] = FMA(ar, xr, yp[0]); yp[0] = FMA(-ai, xi, yp[0]);              \
+        yp[1] = FMA(ar, xi, yp[1]); yp[1] = FMA(ai, xr, yp[1]);               \
+      } else {                                                                \
+        yp[0] += ar * xr - ai * xi;                                           \
+        yp[1] += ar * xi + ai * xr;                                           \
+      }                                                                       \
+    }                                                                         \
+  }
+void or_axpy_exact(int kind, size_t n, const double alpha[2], const void* x, size_t incx, void* y,
+                   size_t incy) {
+  if (n == 0) return;
+  const size_t nf = nf_of(n, incx, incy, kind == 3 ? 2 : 4);
+  if (kind == 1) {
+    const double a = alpha[0];
+    if (a == 0.0) return;
+    const double* xx = (const double*)x;
+    double* yy = (double*)y;
+    for (size_t i = 0; i < n; ++i)
+      yy[i * incy] = i < nf ? fma(a, xx[i * incx], yy[i * incy]) : yy[i * incy] + a * xx[i * incx];
+  } else if (kind == 2) OR_AXPY_C(float, fmaf)
+  else OR_AXPY_C(double, fma)
+}
+
+/* dscal.rs:30-66 (kind 1), cscal.rs:43-111 (kind 2, W 4), zscal.rs:41-109
+ * (kind 3, W 2), csscal.rs:39-88 (kind 4: real alpha, complex64) and
+ * zdscal.rs:38-88 (kind 5: real alpha, complex128).  Complex body:
+ * re = fma(-xi, ai, xr ar), im = fma(xr, ai, xi ar); tail re = ar xr - ai xi,
+ * im = ar xi + ai xr.  Real alpha multiplies each part.  n == 0 or incx == 0
+ * returns; alpha == 0 still multiplies. */
+#define OR_SCAL_C(T, FMA, W)                                                    \
+  {                                                                           \
+    const T ar = (T)alpha[0], ai = (T)alpha[1];                               \
+    T* xx = (T*)x;                                                            \
+    const size_t nf = nf_of(n, incx, 1, W);                                   \
+    for (size_t i = 0; i < n; ++i) {                                          \
+      T* p = xx + 2 * i * incx;                                               \
+      T re, im;                                                               \
+      if (i < nf) { re = FMA(-p[1], ai, p[0] * ar); im = FMA(p[0], ai, p[1] * ar); } \
+      else { re = ar * p[0] - ai * p[1]; im = ar * p[1] + ai * p[0]; }        \
+      p[0] = re; p[1] = im;                                                   \
+    }                                                                         \
+  }
+void or_scal_exact(int kind, size_t n, const double alpha[2], void* x, size_t incx) {
+  if (n == 0 || incx == 0) return;
+  if (kind == 1) {
+    double* xx = (double*)x;
+    for (size_t i = 0; i < n; ++i) xx[i * incx] = xx[i * incx] * alpha[0];
+  } else if (kind == 2) OR_SCAL_C(float, fmaf, 4)
+  else if (kind == 3) OR_SCAL_C(double, fma, 2)
+  else if (kind == 4) {
+    float* xx = (float*)x;
+    const float a = (float)alpha[0];
+    for (size_t i = 0; i < n; ++i) { xx[2 * i * incx] *= a; xx[2 * i * incx + 1] *= a; }
+  } else {
+    double* xx = (double*)x;
+    for (size_t i = 0; i < n; ++i) { xx[2 * i * incx] *= alpha[0]; xx[2 * i * incx + 1] *= alpha[0]; }
+  }
+}
+
+/* srot.rs:51-180 (kind 0, W 4), drot.rs:48-178 (kind 1, W 2), csrot.rs:50-166
+ * (kind 2, W 2 complex) and zdrot.rs:51-166 (kind 3, every unit-stride
+ * element in the body): x' = c x + s y, y' = c y - s x per real part.  Body:
+ * x' = fma(y, s, c x); real kinds y' = fma(-s, x, c y), complex kinds round
+ * both products of y'.  n == 0 returns. */
+#define OR_ROT_PART(T, FMA, FUSEY, xp, yp, fused)                               \
+  do {                                                                        \
+    T xv = *(xp), yv = *(yp), xn, yn;                                         \
+    if (fused) {                                                              \
+      xn = FMA(yv, s, c * xv);                                                \
+      yn = (FUSEY) ? FMA(-s, xv, c * yv) : c * yv - s * xv;                   \
+    } else { xn = c * xv + s * yv; yn = c * yv - s * xv; }                    \
+    *(xp) = xn; *(yp) = yn;                                                   \
+  } while (0)
+void or_rot_exact(int kind, size_t n, void* x, size_t incx, void* y, size_t incy, double cc, double ss) {
+  if (n == 0) return;
+  static const size_t W[4] = {4, 2, 2, 1};
+  const size_t nf = nf_of(n, incx, incy, W[kind]);
+  if (kind == 0 || kind == 2) {
+    const float c = (float)cc, s = (float)ss;
+    float* xx = (float*)x; float* yy = (float*)y;
+    for (size_t i = 0; i < n; ++i) {
+      if (kind == 0) OR_ROT_PART(float, fmaf, 1, xx + i * incx, yy + i * incy, i < nf);
+      else for (int h = 0; h < 2; ++h) OR_ROT_PART(float, fmaf, 0, xx + 2 * i * incx + h, yy + 2 * i * incy + h, i < nf);
+    }
+  } else {
+    const double c = cc, s = ss;
+    double* xx = (double*)x; double* yy = (double*)y;
+    for (size_t i = 0; i < n; ++i) {
+      if (kind == 1) OR_ROT_PART(double, fma, 1, xx + i * incx, yy + i * incy, i < nf);
+      else for (int h = 0; h < 2; ++h) OR_ROT_PART(double, fma, 0, xx + 2 * i * incx + h, yy + 2 * i * incy + h, i < nf);
+    }
+  }
+}
+
+/* srotm.rs:47-412 (kind 0, W 4) and drotm.rs:47-410 (kind 1, W 2):
+ * param = [flag, h11, h21, h12, h22]; flag == -2 or n == 0 returns; flag < 0
+ * full H (body x' = fma(y, h12, h11 x), y' = fma(x, h21, h22 y); tail
+ * h11 x + h12 y, h21 x + h22 y); flag == 0 (body fma(y, h12, x),
+ * fma(x, h21, y); tail x + h12 y, h21 x + y); otherwise (body fma(x, h11, y),
+ * h22 y - x; tail h11 x + y, -x + h22 y). */
+#define OR_ROTM(T, FMA)                                                         \
+  {                                                                           \
+    const T flag = (T)param[0], h11 = (T)param[1], h21 = (T)param[2],         \
+            h12 = (T)param[3], h22 = (T)param[4];                             \
+    if (flag == (T)-2) return;                                                \
+    T* xx = (T*)x; T* yy = (T*)y;                                             \
+    for (size_t i = 0; i < n; ++i) {                                          \
+      const T a = xx[i * incx], b = yy[i * incy];                             \
+      const int f = i < nf;                                                   \
+      T xn, yn;                                                               \
+      if (flag < 0) {                                                         \
+        xn = f ? FMA(b, h12, h11 * a) : h11 * a + h12 * b;                    \
+        yn = f ? FMA(a, h21, h22 * b) : h21 * a + h22 * b;                    \
+      } else if (flag == 0) {                                                 \
+        xn = f ? FMA(b, h12, a) : a + h12 * b;                                \
+        yn = f ? FMA(a, h21, b) : h21 * a + b;                                \
+      } else {                                                                \
+        xn = f ? FMA(a, h11, b) : h11 * a + b;                                \
+        yn = f ? h22 * b - a : -a + h22 * b;                                  \
+      }                                                                       \
+      xx[i * incx] = xn; yy[i * incy] = yn;                                   \
+    }                                                                         \
+  }
+void or_rotm_exact(int kind, size_t n, void* x, size_t incx, void* y, size_t incy, const double param[5]) {
+  if (n == 0) return;
+  const size_t nf = nf_of(n, incx, incy, kind == 0 ? 4 : 2);
+  if (kind == 0) OR_ROTM(float, fmaf)
+  else OR_ROTM(double, fma)
+}
+
+/* srotg.rs:40-75 / drotg.rs:40-71: r = scale sqrt((a/scale)^2 + (b/scale)^2)
+ * with the sign of the larger of a, b; c = a / r, s = b / r; z = s when
+ * |a| > |b|, 1 / c when |b| >= |a| and c != 0, else 1; a <- r, b <- z.
+ * scale == 0 gives c = 1, s = 0, a = b = 0.  v = {a, b, c, s}. */
+#define OR_ROTG(T, FABS, SQRT)                                                  \
+  {                                                                           \
+    T a = (T)v[0], b = (T)v[1];                                               \
+    T roe = FABS(a) > FABS(b) ? a : b, scale = FABS(a) + FABS(b);             \
+    if (scale == 0) { v[0] = 0; v[1] = 0; v[2] = 1; v[3] = 0; return; }       \
+    T qa = a / scale, qb = b / scale;                                         \
+    T r = scale * SQRT(qa * qa + qb * qb);                                    \
+    if (roe < 0) r = -r;                                                      \
+    T c = a / r, s = b / r, z = 1;                                            \
+    if (FABS(a) > FABS(b)) z = s;                                             \
+    if (FABS(b) >= FABS(a) && c != 0) z = (T)1 / c;                           \
+    v[0] = r; v[1] = z; v[2] = c; v[3] = s;                                   \
+  }
+void or_rotg_exact(int dbl, double v[4]) {
+  if (dbl) OR_ROTG(double, fabs, sqrt)
+  else OR_ROTG(float, fabsf, sqrtf)
+}
+
+/* srotmg.rs:42-199 / drotmg.rs:41-195: modified Givens construction with
+ * rescaling by gam = 4096 (the loops stop after 256 steps, which finite
+ * inputs never reach).  v = {d1, d2, x1, y1}; param[5] written (param[0] = -2
+ * only when d2 y1 == 0, leaving v untouched). */
+#define OR_ROTMG(T, FABS)                                                       \
+  {                                                                           \
+    const T gam = 4096, gamsq = gam * gam, rgamsq = (T)1 / gamsq;             \
+    T d1 = (T)v[0], d2 = (T)v[1], x1 = (T)v[2], y1 = (T)v[3];                 \
+    T flag, h11 = 0, h12 = 0, h21 = 0, h22 = 0;                               \
+    if (d1 < 0) { flag = -1; d1 = 0; d2 = 0; x1 = 0; }                        \
+    else {                                                                    \
+      T p2 = d2 * y1;                                                         \
+      if (p2 == 0) { param[0] = -2; return; }                                 \
+      T p1 = d1 * x1, q2 = p2 * y1, q1 = p1 * x1;                             \
+      if (FABS(q1) > FABS(q2)) {                                              \
+        h21 = -y1 / x1; h12 = p2 / p1;                                        \
+        T u = 1 - h12 * h21;                                                  \
+        if (u <= 0) { flag = -1; d1 = d2 = x1 = 0; h11 = h12 = h21 = h22 = 0; } \
+        else { flag = 0; d1 /= u; d2 /= u; x1 *= u; }                         \
+      } else if (q2 < 0) { flag = -1; d1 = d2 = x1 = 0; h11 = h12 = h21 = h22 = 0; } \
+      else {                                                                  \
+        flag = 1; h11 = p1 / p2; h22 = x1 / y1;                               \
+        T u = 1 + h11 * h22, t = d2 / u;                                      \
+        d2 = d1 / u; d1 = t; x1 = y1 * u;                                     \
+      }                                                                       \
+      if (d1 != 0)                                                            \
+        for (int it = 0; it < 256 && (d1 <= rgamsq || d1 >= gamsq); ++it) {   \
+          if (flag == 0) { h11 = 1; h22 = 1; } else { h21 = -1; h12 = 1; }    \
+          flag = -1;                                                          \
+          if (d1 <= rgamsq) { d1 *= gamsq; x1 /= gam; h11 /= gam; h12 /= gam; } \
+          else { d1 /= gamsq; x1 *= gam; h11 *= gam; h12 *= gam; }            \
+        }                                                                     \
+      if (d2 != 0)                                                            \
+        for (int it = 0; it < 256 && (FABS(d2) <= rgamsq || FABS(d2) >= gamsq); ++it) { \
+          if (flag == 0) { h11 = 1; h22 = 1; } else { h21 = -1; h12 = 1; }    \
+          flag = -1;                                                          \
+          if (FABS(d2) <= rgamsq) { d2 *= gamsq; h21 /= gam; h22 /= gam; }    \
+          else { d2 /= gamsq; h21 *= gam; h22 *= gam; }                       \
+        }                                                                     \
+    }                                                                         \
+    param[1] = param[2] = param[3] = param[4] = 0;                            \
+    if (flag < 0) { param[1] = h11; param[2] = h21; param[3] = h12; param[4] = h22; } \
+    else if (flag == 0) { param[2] = h21; param[3] = h12; }                   \
+    else { param[1] = h11; param[4] = h22; }                                  \
+    param[0] = flag;                                                          \
+    v[0] = d1; v[1] = d2; v[2] = x1;                                          \
+  }
+void or_rotmg_exact(int dbl, double v[4], double param[5]) {
+  if (dbl) OR_ROTMG(double, fabs)
+  else OR_ROTMG(float, fabsf)
+}
+
+/* idamax.rs:43-159, icamax.rs:48-166, izamax.rs:33-163: first index of the
+ * largest |x| (|re| + |im| summed in the element precision); NaN never wins;
+ * n == 0 or incx == 0 -> 0. */
+size_t or_iamax_exact(int kind, size_t n, const void* x, size_t incx) {
+  if (n == 0 || incx == 0) return 0;
+  double best = -INFINITY;
+  size_t idx = 0;
+  for (size_t i = 0; i < n; ++i) {
+    double v;
+    if (kind == 1) v = fabs(((const double*)x)[i * incx]);
+    else if (kind == 2) v = (double)(fabsf(((const float*)x)[2 * i * incx]) + fabsf(((const float*)x)[2 * i * incx + 1]));
+    else v = fabs(((const double*)x)[2 * i * incx]) + fabs(((const double*)x)[2 * i * incx + 1]);
+    if (v > best) { best = v; idx = i; }
+  }
+  return idx;
+}
+
+/* ddot.rs:43-163, cdotu.rs / cdotc.rs / zdotu.rs / zdotc.rs (conj: sum
+ * conj(x_i) y_i) in double-double; n == 0 -> 0. */
+void or_dot_f64(int kind, int conj, size_t n, const void* x, size_t incx, const void* y, size_t incy,
+                double out[2]) {
+  dd re = {0, 0}, im = {0, 0};
+  for (size_t i = 0; i < n; ++i) {
+    double xr, xi, yr, yi;
+    L1_LOAD(kind, x, i * incx, xr, xi);
+    L1_LOAD(kind, y, i * incy, yr, yi);
+    if (conj) xi = -xi;
+    re = dd_add_prod(re, xr, yr);
+    re = dd_add_prod(re, -xi, yi);
+    im = dd_add_prod(im, xr, yi);
+    im = dd_add_prod(im, xi, yr);
+  }
+  out[0] = dd_val(re);
+  out[1] = dd_val(im);
+}
+
+/* sasum.rs:40-107, dasum.rs:41-110, scasum.rs:40-108, dzasum.rs:40-111:
+ * sum of |re| + |im| in long double; n == 0 or incx == 0 -> 0. */
+double or_asum_f64(int kind, size_t n, const void* x, size_t incx) {
+  if (n == 0 || incx == 0) return 0.0;
+  long double s = 0;
+  for (size_t i = 0; i < n; ++i) {
+    double r, m;
+    L1_LOAD(kind, x, i * incx, r, m);
+    s += fabsl((long double)r) + fabsl((long double)m);
+  }
+  return (double)s;
+}
+
+/* dnrm2.rs:45-152, scnrm2.rs:44-155, dznrm2.rs:43-156: ||x||_2 with the sum
+ * of squares in long double (no overflow or underflow for double data);
+ * n == 0 or incx == 0 -> 0. */
+double or_nrm2_f64(int kind, size_t n, const void* x, size_t incx) {
+  if (n == 0 || incx == 0) return 0.0;
+  long double s = 0;
+  for (size_t i = 0; i < n; ++i) {
+    double r, m;
+    L1_LOAD(kind, x, i * incx, r, m);
+    s += (long double)r * r + (long double)m * m;
+  }
+  return (double)sqrtl(s);
+}
+
 /* ============================ level 2 ==================================== */
 
 /* level2/sgemv_notranspose.rs:63-177, sgemv_transpose.rs:64-182:

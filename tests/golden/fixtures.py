@@ -141,3 +141,156 @@ CGEMM_DOCTEST = dict(
     c=np.array([1 + 1j, 3 + 0j, 0 + 2j, 4 + 1j], np.complex64),
     alpha=2 + 1j, beta=1 - 1j,
     expect=np.array([-50 + 99j, -69 + 276j, -78 + 92j, -163 + 223j], np.complex64))
+
+
+# ---- double and complex level 1 (coral-aarch64/tests/level1/*.rs) -------------
+# Every vector there is a linear ramp a + b k (complex: (a + b k, c + d k)),
+# sometimes with alternating signs and one planted element; the generators
+# below rebuild them in the element precision.  Each case names its source.
+_DT = {"s": np.float32, "d": np.float64, "c": np.complex64, "z": np.complex128}
+
+
+def ramp(kind: str, n: int, inc: int, g, alt: bool = False, plant=None) -> np.ndarray:
+    """Strided vector of n ramp elements (make_strided_vec / make_strided_cvec)."""
+    dt = _DT[kind]
+    real = np.float32 if kind in "sc" else np.float64
+    v = np.zeros((n - 1) * inc + 1 if n else 1, dt)
+    if n == 0:
+        return v
+    k = np.arange(n).astype(real)
+    re = real(g[0]) + real(g[1]) * k
+    val = re if kind in "sd" else re + 1j * (real(g[2]) + real(g[3]) * k)
+    if alt:
+        val = np.where(np.arange(n) % 2 == 0, val, -val)
+    val = val.astype(dt)
+    if plant is not None:
+        val[plant[0]] = plant[1]
+    v[np.arange(n) * inc] = val
+    return v
+
+
+L1_CASES = [
+    # axpy_tests.rs
+    dict(fn="axpy", kind="d", n=1536, incx=1, incy=1, alpha=-2.5, x=(0.25, 0.125), y=(-0.75, 0.05),
+         src="axpy_tests.rs:216-226"),
+    dict(fn="axpy", kind="d", n=1023, incx=4, incy=3, alpha=0.333333333333, x=(1.0, -1e-3), y=(-0.5, 2e-3),
+         src="axpy_tests.rs:252-264"),
+    dict(fn="axpy", kind="c", n=800, incx=1, incy=1, alpha=0.75 - 0.2j, x=(0.1, 0.01, -0.05, 0.002),
+         y=(-0.2, 0.001, 0.3, -0.003), src="axpy_tests.rs:321-331"),
+    dict(fn="axpy", kind="c", n=513, incx=2, incy=3, alpha=-1.1 + 0.4j, x=(0.0, 0.02, 0.03, -0.001),
+         y=(0.0, -0.01, 0.04, 0.002), src="axpy_tests.rs:357-369"),
+    dict(fn="axpy", kind="c", n=300, incx=1, incy=1, alpha=1j, x=(0.1, 0.001, -0.2, 0.002),
+         y=(-0.05, 0.0015, 0.03, -0.001), src="axpy_tests.rs:431-441"),
+    dict(fn="axpy", kind="z", n=640, incx=1, incy=1, alpha=1.25 - 0.75j, x=(0.05, 0.002, 0.1, -0.001),
+         y=(-0.2, 0.0005, 0.3, 0.0003), src="axpy_tests.rs:468-478"),
+    dict(fn="axpy", kind="z", n=511, incx=3, incy=2, alpha=-0.2 + 0.9j, x=(0.0, 0.001, 0.0, -0.002),
+         y=(0.4, -0.003, -0.1, 0.004), src="axpy_tests.rs:504-516"),
+    dict(fn="axpy", kind="z", n=333, incx=1, incy=1, alpha=2.0, x=(0.3, -0.001, 0.25, 0.002),
+         y=(-0.15, 0.0005, 0.07, -0.0003), src="axpy_tests.rs:578-588"),
+    # scal_tests.rs (csscal / zdscal reuse the complex ramps with a real alpha)
+    dict(fn="scal", kind="d", n=1536, incx=1, alpha=-2.5, x=(0.25, 0.125), src="scal_tests.rs:261-266"),
+    dict(fn="scal", kind="d", n=1023, incx=4, alpha=1.0 / 3.0, x=(1.0, -1e-3), src="scal_tests.rs:291-297"),
+    dict(fn="scal", kind="d", n=512, incx=1, alpha=0.0, x=(0.2, -0.02), src="scal_tests.rs:322-327"),
+    dict(fn="scal", kind="c", n=800, incx=1, alpha=0.75 - 0.2j, x=(0.1, 0.01, -0.05, 0.002),
+         src="scal_tests.rs:411-416"),
+    dict(fn="scal", kind="c", n=513, incx=3, alpha=-1.1 + 0.4j, x=(0.0, 0.02, 0.03, -0.001),
+         src="scal_tests.rs:441-447"),
+    dict(fn="scal", kind="c", n=300, incx=1, alpha=1j, x=(0.1, 0.001, -0.2, 0.002), src="scal_tests.rs:532-537"),
+    dict(fn="scal", kind="z", n=640, incx=1, alpha=1.25 - 0.75j, x=(0.05, 0.002, 0.1, -0.001),
+         src="scal_tests.rs:592-597"),
+    dict(fn="scal", kind="z", n=511, incx=2, alpha=-0.2 + 0.9j, x=(0.0, 0.001, 0.0, -0.002),
+         src="scal_tests.rs:622-628"),
+    dict(fn="scal", kind="z", n=333, incx=1, alpha=2.0, x=(-0.15, 0.0005, 0.07, -0.0003), src="scal_tests.rs:683-688"),
+    dict(fn="sscal_r", kind="c", n=513, incx=3, alpha=-1.1, x=(0.0, 0.02, 0.03, -0.001), src="scal_tests.rs:441-447"),
+    dict(fn="sscal_r", kind="z", n=640, incx=1, alpha=1.25, x=(0.05, 0.002, 0.1, -0.001), src="scal_tests.rs:592-597"),
+    # dot_tests.rs
+    dict(fn="dotu", kind="d", n=1536, incx=1, incy=1, x=(0.25, 0.125), y=(-0.75, 0.05), src="dot_tests.rs:305-314"),
+    dict(fn="dotu", kind="d", n=1023, incx=4, incy=3, x=(1.0, -1e-3), xalt=True, y=(-0.5, 2e-3),
+         src="dot_tests.rs:336-347"),
+    dict(fn="dotu", kind="c", n=800, incx=1, incy=1, x=(0.1, 0.01, -0.05, 0.002), y=(-0.2, 0.001, 0.3, -0.003),
+         src="dot_tests.rs:429-438"),
+    dict(fn="dotu", kind="c", n=513, incx=2, incy=3, x=(0.0, 0.02, 0.03, -0.001), y=(0.0, -0.01, 0.04, 0.002),
+         src="dot_tests.rs:462-473"),
+    dict(fn="dotc", kind="c", n=800, incx=1, incy=1, x=(0.1, 0.01, -0.05, 0.002), y=(-0.2, 0.001, 0.3, -0.003),
+         src="dot_tests.rs:566-575"),
+    dict(fn="dotc", kind="c", n=513, incx=2, incy=3, x=(0.0, 0.02, 0.03, -0.001), y=(0.0, -0.01, 0.04, 0.002),
+         src="dot_tests.rs:599-610"),
+    dict(fn="dotu", kind="z", n=640, incx=1, incy=1, x=(0.05, 0.002, 0.1, -0.001), y=(-0.2, 0.0005, 0.3, 0.0003),
+         src="dot_tests.rs:635-644"),
+    dict(fn="dotc", kind="z", n=511, incx=3, incy=2, x=(0.0, 0.001, 0.0, -0.002), y=(0.4, -0.003, -0.1, 0.004),
+         src="dot_tests.rs:668-674"),
+    # asum_tests.rs
+    dict(fn="asum", kind="s", n=1024, incx=1, x=(0.05, 0.03), xalt=True, src="asum_tests.rs:114-118"),
+    dict(fn="asum", kind="d", n=1536, incx=1, x=(0.25, 0.125), xalt=True, src="asum_tests.rs:217-221"),
+    dict(fn="asum", kind="d", n=1023, incx=4, x=(1.0, -1e-3), xalt=True, src="asum_tests.rs:243-248"),
+    dict(fn="asum", kind="c", n=800, incx=1, x=(0.1, 0.01, -0.05, 0.002), xalt=True, src="asum_tests.rs:323-330"),
+    dict(fn="asum", kind="c", n=513, incx=2, x=(0.0, 0.02, 0.03, -0.001), xalt=True, src="asum_tests.rs:353-361"),
+    dict(fn="asum", kind="z", n=640, incx=1, x=(0.05, 0.002, 0.1, -0.001), xalt=True, src="asum_tests.rs:438-445"),
+    dict(fn="asum", kind="z", n=511, incx=3, x=(0.0, 0.001, 0.0, -0.002), xalt=True, src="asum_tests.rs:468-476"),
+    # nrm2_tests.rs
+    dict(fn="nrm2", kind="d", n=1536, incx=1, x=(0.25, 0.125), src="nrm2_tests.rs:205-209"),
+    dict(fn="nrm2", kind="d", n=1023, incx=4, x=(1.0, -1e-3), xalt=True, src="nrm2_tests.rs:228-233"),
+    dict(fn="nrm2", kind="c", n=800, incx=1, x=(0.1, 0.01, -0.05, 0.002), src="nrm2_tests.rs:299-305"),
+    dict(fn="nrm2", kind="c", n=513, incx=2, x=(0.0, 0.02, 0.03, -0.001), src="nrm2_tests.rs:326-333"),
+    dict(fn="nrm2", kind="z", n=640, incx=1, x=(0.05, 0.002, 0.1, -0.001), src="nrm2_tests.rs:402-408"),
+    dict(fn="nrm2", kind="z", n=511, incx=3, x=(0.0, 0.001, 0.0, -0.002), src="nrm2_tests.rs:429-436"),
+    # iamax_tests.rs
+    dict(fn="iamax", kind="d", n=1023, incx=4, x=(1.0, -1e-3), xalt=True, src="iamax_tests.rs:207-215"),
+    dict(fn="iamax", kind="c", n=800, incx=1, x=(0.1, 0.01, -0.05, 0.002), xalt=True, plant=(400, 999 - 999j),
+         src="iamax_tests.rs:282-295"),
+    dict(fn="iamax", kind="c", n=513, incx=2, x=(0.0, 0.02, 0.03, -0.001), xalt=True, src="iamax_tests.rs:313-325"),
+    dict(fn="iamax", kind="z", n=640, incx=1, x=(0.05, 0.002, 0.1, -0.001), xalt=True, plant=(333, 7777 - 8888j),
+         src="iamax_tests.rs:393-405"),
+    dict(fn="iamax", kind="z", n=511, incx=3, x=(0.0, 0.001, 0.0, -0.002), xalt=True, src="iamax_tests.rs:424-436"),
+    # rot_tests.rs (csrot / zdrot reuse the complex ramps)
+    dict(fn="rot", kind="s", n=1024, incx=1, incy=1, theta=0.375, x=(0.05, 0.03), y=(-0.3, 0.002),
+         src="rot_tests.rs:86-101"),
+    dict(fn="rot", kind="s", n=777, incx=3, incy=2, theta=-0.91, x=(0.2, -0.001), y=(-0.3, 0.002),
+         src="rot_tests.rs:135-150"),
+    dict(fn="rot", kind="d", n=1536, incx=1, incy=1, theta=0.22, x=(0.25, 0.125), y=(-0.75, 0.05),
+         src="rot_tests.rs:271-284"),
+    dict(fn="rot", kind="d", n=1023, incx=4, incy=3, theta=-0.61, x=(1.0, -1e-3), y=(-0.5, 2e-3),
+         src="rot_tests.rs:318-333"),
+    dict(fn="rot", kind="c", n=801, incx=1, incy=1, theta=0.375, x=(0.1, 0.01, -0.05, 0.002),
+         y=(-0.2, 0.001, 0.3, -0.003), src="dot_tests.rs:429-438 ramps"),
+    dict(fn="rot", kind="z", n=511, incx=3, incy=2, theta=-0.61, x=(0.0, 0.001, 0.0, -0.002),
+         y=(0.4, -0.003, -0.1, 0.004), src="dot_tests.rs:668-674 ramps"),
+    dict(fn="rotm", kind="s", n=320, incx=1, incy=1, param=(-1.0, 1.1, -0.4, 0.7, 0.9), x=(-0.5, 0.03),
+         y=(0.1, 0.002), src="rot_tests.rs:761-772"),
+    dict(fn="rotm", kind="s", n=300, incx=1, incy=1, param=(0.0, 0.0, -0.6, 0.8, 0.0), x=(0.2, -0.001),
+         y=(-0.3, 0.002), src="rot_tests.rs:804-815"),
+    dict(fn="rotm", kind="s", n=300, incx=1, incy=1, param=(1.0, 1.2, 0.0, 0.0, -0.75), x=(0.0, 0.01),
+         y=(1.0, -0.005), src="rot_tests.rs:847-858"),
+    dict(fn="rotm", kind="s", n=257, incx=2, incy=3, param=(-1.0, -0.3, 0.5, -0.9, 0.4), x=(0.05, 0.01),
+         y=(-0.2, 0.003), src="rot_tests.rs:890-903"),
+    dict(fn="rotm", kind="d", n=320, incx=1, incy=1, param=(-1.0, 1.05, -0.6, 0.8, 0.95), x=(-1.0, 0.1),
+         y=(0.2, 0.004), src="rot_tests.rs:1052-1063"),
+    dict(fn="rotm", kind="d", n=300, incx=1, incy=1, param=(0.0, 0.0, -0.25, 0.33, 0.0), x=(1.0, -1e-3),
+         y=(-0.5, 2e-3), src="rot_tests.rs:1095-1106"),
+    dict(fn="rotm", kind="d", n=300, incx=1, incy=1, param=(1.0, 0.75, 0.0, 0.0, -1.2), x=(0.25, 0.125),
+         y=(-0.75, 0.05), src="rot_tests.rs:1138-1149"),
+    dict(fn="rotm", kind="d", n=257, incx=2, incy=3, param=(-1.0, -0.8, 0.2, -0.1, 1.3), x=(0.25, 0.125),
+         y=(-0.75, 0.05), src="rot_tests.rs:1181-1194"),
+]
+
+# rot_tests.rs:455-715: (a, b) of the srotg (first four) and drotg (last four)
+# cases; both precisions run all eight here
+ROTG_CASES = [(3.5, -2.25), (0.0, 5.0), (-4.0, 0.0), (-1.25, -7.5), (12.0, -0.75), (0.0, 3.0), (-5.0, 0.0),
+              (-2.0, 9.0)]
+# rot_tests.rs:936-999 (srotmg) and 1227-1290 (drotmg): (kind, d1, d2, x1, y1)
+ROTMG_CASES = [("s", 1.5, 2.0, 0.75, -1.25), ("s", 1e-3, 3e2, -4.5, 7.25), ("d", 5.0, 0.75, -2.0, 3.0),
+               ("d", 1e4, 1e-5, 8.0, -6.0)]
+
+
+def l1_vectors(case):
+    """(x, y) of a L1_CASES entry (y None when the routine has one vector)."""
+    x = ramp(case["kind"], case["n"], case["incx"], case["x"], case.get("xalt", False), case.get("plant"))
+    y = ramp(case["kind"], case["n"], case["incy"], case["y"]) if "y" in case else None
+    return x, y
+
+
+def rot_cs(case):
+    """(c, s) of a rot case: cos / sin of theta in the element precision."""
+    real = np.float32 if case["kind"] in "sc" else np.float64
+    t = real(case["theta"])
+    return real(np.cos(t)), real(np.sin(t))

@@ -25,6 +25,42 @@ def logical(buf, rows, cols, ld):
     return np.asfortranarray(buf.reshape(cols, ld).T[:rows, :])
 
 
+def l1_reference(case) -> np.ndarray:
+    """OpenBLAS result of one L1_CASES entry: the updated vector(s) or the
+    scalar, as a flat array."""
+    kind, n, fn = case["kind"], case["n"], case["fn"]
+    x, y = fx.l1_vectors(case)
+    incx, incy = case["incx"], case.get("incy", 1)
+    pre = {"s": "s", "d": "d", "c": "c", "z": "z"}[kind]
+    if fn == "axpy":
+        return getattr(blas, pre + "axpy")(x, y.copy(), n=n, a=case["alpha"], incx=incx, incy=incy)
+    if fn == "scal":
+        return getattr(blas, pre + "scal")(case["alpha"], x.copy(), n=n, incx=incx)
+    if fn == "sscal_r":
+        return getattr(blas, {"c": "csscal", "z": "zdscal"}[kind])(case["alpha"], x.copy(), n=n, incx=incx)
+    if fn in ("dotu", "dotc"):
+        name = pre + "dot" if kind in "sd" else pre + fn
+        return np.atleast_1d(np.asarray(getattr(blas, name)(x, y, n=n, incx=incx, incy=incy), np.complex128))
+    if fn == "asum":
+        name = {"s": "sasum", "d": "dasum", "c": "scasum", "z": "dzasum"}[kind]
+        return np.array([getattr(blas, name)(x, n=n, incx=incx)], np.float64)
+    if fn == "nrm2":
+        name = {"s": "snrm2", "d": "dnrm2", "c": "scnrm2", "z": "dznrm2"}[kind]
+        return np.array([getattr(blas, name)(x, n=n, incx=incx)], np.float64)
+    if fn == "iamax":
+        return np.array([getattr(blas, "i" + pre + "amax")(x, n=n, incx=incx)], np.int64)
+    if fn == "rot":
+        c, s = fx.rot_cs(case)
+        name = {"s": "srot", "d": "drot", "c": "csrot", "z": "zdrot"}[kind]
+        xo, yo = getattr(blas, name)(x.copy(), y.copy(), c, s, n=n, incx=incx, incy=incy)
+        return np.concatenate([xo, yo])
+    if fn == "rotm":
+        p = np.asarray(case["param"], x.dtype)
+        xo, yo = getattr(blas, pre + "rotm")(x.copy(), y.copy(), p, n=n, incx=incx, incy=incy)
+        return np.concatenate([xo, yo])
+    raise ValueError(fn)
+
+
 def main() -> None:
     g: dict[str, np.ndarray] = {}
     # ---- SGEMM: small fixture shapes x ops x (alpha, beta), + ConjugateTranspose cases.
@@ -69,6 +105,15 @@ def main() -> None:
     for ci, (n, inc, x) in enumerate(fx.isamax_cases()):
         idx = 0 if n == 0 else int(blas.isamax(x, n=n, incx=inc))
         g[f"isamax_c{ci}"] = np.array([idx], np.int64)
+    # ---- double and complex level 1 (tests/level1/*.rs fixture ramps)
+    for ci, case in enumerate(fx.L1_CASES):
+        g[f"l1_c{ci}"] = l1_reference(case)
+    for ci, (a, b) in enumerate(fx.ROTG_CASES):
+        for kind in "sd":
+            c, s = getattr(blas, kind + "rotg")(a, b)
+            g[f"rotg_{kind}{ci}"] = np.array([c, s], np.float64)
+    for ci, (kind, d1, d2, x1, y1) in enumerate(fx.ROTMG_CASES):
+        g[f"rotmg_c{ci}"] = np.asarray(getattr(blas, kind + "rotmg")(d1, d2, x1, y1), np.float64)
     np.savez_compressed(OUT, **g)
     print(f"wrote {len(g)} arrays to {OUT} ({os.path.getsize(OUT)} bytes)")
 

@@ -135,3 +135,113 @@ def test_gemm_sample_scale_only():
     vals, absb = oracle.gemm_sample(0, 0, 2, 3, 0, 1.0, np.zeros(1, np.float32), 2,
                                     np.zeros(1, np.float32), 1, 0.5, c, 2, [0, 1], [2, 2])
     np.testing.assert_array_equal(vals, [2.0, 2.5])
+
+
+# ---- double and complex level 1 ------------------------------------------------
+def oracle_l1(case) -> np.ndarray:
+    """The oracle's result for one fx.L1_CASES entry, shaped like the golden
+    entry (updated vectors concatenated, or the scalar)."""
+    kind, n, fn = case["kind"], case["n"], case["fn"]
+    x, y = fx.l1_vectors(case)
+    incx, incy = case["incx"], case.get("incy", 1)
+    if fn == "axpy":
+        return oracle.axpy(kind, n, case["alpha"], x, incx, y, incy)
+    if fn == "scal":
+        return oracle.scal(kind, n, case["alpha"], x, incx)
+    if fn == "sscal_r":
+        return oracle.scal(kind, n, case["alpha"], x, incx, real_alpha=True)
+    if fn in ("dotu", "dotc"):
+        return np.array([oracle.dot(kind, fn == "dotc", n, x, incx, y, incy)])
+    if fn == "asum":
+        return np.array([oracle.asum(kind, n, x, incx)])
+    if fn == "nrm2":
+        return np.array([oracle.nrm2(kind, n, x, incx)])
+    if fn == "iamax":
+        return np.array([oracle.iamax(kind, n, x, incx)])
+    if fn == "rot":
+        c, s = fx.rot_cs(case)
+        return np.concatenate(oracle.rot(kind, n, x, incx, y, incy, c, s))
+    if fn == "rotm":
+        return np.concatenate(oracle.rotm(kind, n, x, incx, y, incy, case["param"]))
+    raise ValueError(fn)
+
+
+# the reference tests' tolerances: dot_tests.rs:176-179, the other level-1
+# test files' RTOL/ATOL (asum_tests.rs:106-109, rot_tests.rs:80-83, ...)
+def l1_tol(case):
+    if case["kind"] in "sc":
+        return (4e-6, 4e-6) if case["fn"].startswith("dot") else (1e-6, 1e-6)
+    return 1e-12, 1e-12
+
+
+@pytest.mark.parametrize("ci", range(len(fx.L1_CASES)))
+def test_l1_dcz_fixtures(golden, ci):
+    case = fx.L1_CASES[ci]
+    got, want = oracle_l1(case), golden[f"l1_c{ci}"]
+    if case["fn"] == "iamax":
+        assert int(got[0]) == int(want[0]), case["src"]
+        return
+    rtol, atol = l1_tol(case)
+    got = np.asarray(got, np.complex128)
+    want = np.asarray(want, np.complex128)
+    assert got.shape == want.shape
+    d = np.abs(got - want)
+    assert (d <= atol + rtol * np.maximum(np.abs(got), np.abs(want))).all(), (case["src"], d.max())
+
+
+@pytest.mark.parametrize("kind", "sd")
+@pytest.mark.parametrize("ci", range(len(fx.ROTG_CASES)))
+def test_rotg_fixtures(golden, kind, ci):
+    a, b = fx.ROTG_CASES[ci]
+    r, z, c, s = oracle.rotg(kind, a, b)
+    tol = 1e-6 if kind == "s" else 1e-12
+    np.testing.assert_allclose([c, s], golden[f"rotg_{kind}{ci}"], rtol=tol, atol=tol)
+    # r = c a + s b and [c s; -s c] [a; b] = [r; 0]
+    assert abs(r - (c * a + s * b)) <= 4 * tol * max(1.0, abs(r))
+    assert abs(-s * a + c * b) <= 4 * tol * max(1.0, abs(r))
+
+
+@pytest.mark.parametrize("ci", range(len(fx.ROTMG_CASES)))
+def test_rotmg_fixtures(golden, ci):
+    kind, d1, d2, x1, y1 = fx.ROTMG_CASES[ci]
+    _, _, _, param = oracle.rotmg(kind, d1, d2, x1, y1)
+    tol = 1e-6 if kind == "s" else 1e-12
+    want = golden[f"rotmg_c{ci}"]
+    assert param[0] == want[0]
+    # only the entries the flag makes meaningful (rotmg.rs param packing)
+    used = {-1.0: [1, 2, 3, 4], 0.0: [2, 3], 1.0: [1, 4]}.get(param[0], [])
+    np.testing.assert_allclose(np.array(param)[used], want[used], rtol=tol, atol=tol)
+
+
+def test_l1_dcz_rounding_paths():
+    """Unit-stride body fused, tail and strided paths rounded per product."""
+    rng = np.random.default_rng(11)
+    n = 11
+    x = (rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)).astype(np.complex64)
+    y = (rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)).astype(np.complex64)
+    a = np.complex64(0.3 - 0.7j)
+    got = oracle.axpy("c", n, a, x, 1, y, 1)
+    f32 = np.float32
+    for i in range(n):
+        xr, xi, yr, yi = f32(x[i].real), f32(x[i].imag), f32(y[i].real), f32(y[i].imag)
+        ar, ai = f32(a.real), f32(a.imag)
+        if i < 8:   # fused: exact product-sums rounded once per step
+            r = f32(np.float64(ar) * xr + yr)
+            r = f32(-np.float64(ai) * xi + r)
+            m = f32(np.float64(ar) * xi + yi)
+            m = f32(np.float64(ai) * xr + m)
+        else:
+            r = yr + (ar * xr - ai * xi)
+            m = yi + (ar * xi + ai * xr)
+        assert got[i] == np.complex64(complex(r, m)), i
+    # idamax / icamax / izamax: first index, NaN never wins, all NaN -> 0
+    v = np.array([np.nan, -3.0, 3.0, np.nan, -3.0])
+    assert oracle.iamax("d", 5, v, 1) == 1
+    c = np.array([1 + 2j, np.nan, -2 - 1j, 3 + 0j], np.complex64)
+    assert oracle.iamax("c", 4, c, 1) == 0
+    assert oracle.iamax("z", 3, np.full(3, np.nan, np.complex128), 1) == 0
+    # rotm flag -2 and n == 0 leave the vectors alone
+    xd, yd = rng.uniform(-1, 1, 5), rng.uniform(-1, 1, 5)
+    xo, yo = oracle.rotm("d", 5, xd, 1, yd, 1, [-2, 1, 2, 3, 4])
+    np.testing.assert_array_equal(xo, xd)
+    np.testing.assert_array_equal(yo, yd)
