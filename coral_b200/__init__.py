@@ -15,6 +15,7 @@ from .blas import (  # noqa: F401
     ddot, cdotu, cdotc, zdotu, zdotc, sasum, dasum, scasum, dzasum, dnrm2, scnrm2, dznrm2, idamax,
     icamax, izamax, daxpy, caxpy, zaxpy, dscal, cscal, zscal, csscal, zdscal, dcopy, ccopy, zcopy,
     dswap, cswap, zswap, srot, drot, csrot, zdrot, srotm, drotm, srotg, drotg, srotmg, drotmg,
+    saxpyf, daxpyf, caxpyf, zaxpyf, sdotf, ddotf, cdotuf, cdotcf, zdotuf, zdotcf,
 )
 
 __all__ = [
@@ -28,4 +29,5 @@ __all__ = [
     "ddot", "cdotu", "cdotc", "zdotu", "zdotc", "sasum", "dasum", "scasum", "dzasum", "dnrm2", "scnrm2", "dznrm2",
     "idamax", "icamax", "izamax", "daxpy", "caxpy", "zaxpy", "dscal", "cscal", "zscal", "csscal", "zdscal", "dcopy",
     "ccopy", "zcopy", "dswap", "cswap", "zswap", "srot", "drot", "csrot", "zdrot", "srotm", "drotm", "srotg", "drotg", "srotmg", "drotmg",
+    "saxpyf", "daxpyf", "caxpyf", "zaxpyf", "sdotf", "ddotf", "cdotuf", "cdotcf", "zdotuf", "zdotcf",
 ]

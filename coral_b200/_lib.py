@@ -90,6 +90,16 @@ SIGNATURES = {
     "coral_drotg": [_h, _vp, _vp, _vp, _vp],
     "coral_srotmg": [_h, _vp, _vp, _vp, _f, _vp],
     "coral_drotmg": [_h, _vp, _vp, _vp, _d, _vp],
+    "coral_saxpyf": [_h, _sz, _sz, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_daxpyf": [_h, _sz, _sz, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_caxpyf": [_h, _sz, _sz, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_zaxpyf": [_h, _sz, _sz, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_sdotf": [_h, _sz, _sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_ddotf": [_h, _sz, _sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_cdotuf": [_h, _sz, _sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_cdotcf": [_h, _sz, _sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_zdotuf": [_h, _sz, _sz, _vp, _sz, _vp, _sz, _vp],
+    "coral_zdotcf": [_h, _sz, _sz, _vp, _sz, _vp, _sz, _vp],
     "coral_sgemv": [_h, _i, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
     "coral_dgemv": [_h, _i, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz],
     "coral_cgemv": [_h, _i, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],

@@ -460,6 +460,72 @@ def drotmg(d1, d2, x1, y1):
     return _rotmg("coral_drotmg", C.c_double, d1, d2, x1, y1)
 
 
+# ------------------------------------------------------- fused level 1.5 ----
+_FUSED_DT = {"s": _f32, "d": _f64, "c": _c64, "z": _c128}
+
+
+def _axpyf(kind, n_rows, n_cols, x, incx, matrix, lda, y, incy) -> None:
+    dt = _FUSED_DT[kind]
+    handle().call(f"coral_{kind}axpyf", n_rows, n_cols, _ptr(x, dt(), "x"), incx, _ptr(matrix, dt(), "matrix"),
+                  lda, _ptr(y, dt(), "y"), incy)
+
+
+def _dotf(name, kind, n_rows, n_cols, matrix, lda, x, incx, out) -> None:
+    dt = _FUSED_DT[kind]
+    handle().call(name, n_rows, n_cols, _ptr(matrix, dt(), "matrix"), lda, _ptr(x, dt(), "x"), incx,
+                  _ptr(out, dt(), "out"))
+
+
+def saxpyf(n_rows, n_cols, x, incx, matrix, lda, y, incy) -> None:
+    """level1_special/saxpyf.rs:36-513: y += A x."""
+    _axpyf("s", n_rows, n_cols, x, incx, matrix, lda, y, incy)
+
+
+def daxpyf(n_rows, n_cols, x, incx, matrix, lda, y, incy) -> None:
+    """level1_special/daxpyf.rs:45-518."""
+    _axpyf("d", n_rows, n_cols, x, incx, matrix, lda, y, incy)
+
+
+def caxpyf(n_rows, n_cols, x, incx, matrix, lda, y, incy) -> None:
+    """level1_special/caxpyf.rs:48-696."""
+    _axpyf("c", n_rows, n_cols, x, incx, matrix, lda, y, incy)
+
+
+def zaxpyf(n_rows, n_cols, x, incx, matrix, lda, y, incy) -> None:
+    """level1_special/zaxpyf.rs:49-697."""
+    _axpyf("z", n_rows, n_cols, x, incx, matrix, lda, y, incy)
+
+
+def sdotf(n_rows, n_cols, matrix, lda, x, incx, out) -> None:
+    """level1_special/sdotf.rs:37-600: out += A^T x."""
+    _dotf("coral_sdotf", "s", n_rows, n_cols, matrix, lda, x, incx, out)
+
+
+def ddotf(n_rows, n_cols, matrix, lda, x, incx, out) -> None:
+    """level1_special/ddotf.rs:37-596."""
+    _dotf("coral_ddotf", "d", n_rows, n_cols, matrix, lda, x, incx, out)
+
+
+def cdotuf(n_rows, n_cols, matrix, lda, x, incx, out) -> None:
+    """level1_special/cdotuf.rs:41-764: out += A^T x."""
+    _dotf("coral_cdotuf", "c", n_rows, n_cols, matrix, lda, x, incx, out)
+
+
+def cdotcf(n_rows, n_cols, matrix, lda, x, incx, out) -> None:
+    """level1_special/cdotcf.rs:42-765: out += A^H x."""
+    _dotf("coral_cdotcf", "c", n_rows, n_cols, matrix, lda, x, incx, out)
+
+
+def zdotuf(n_rows, n_cols, matrix, lda, x, incx, out) -> None:
+    """level1_special/zdotuf.rs:41-665."""
+    _dotf("coral_zdotuf", "z", n_rows, n_cols, matrix, lda, x, incx, out)
+
+
+def zdotcf(n_rows, n_cols, matrix, lda, x, incx, out) -> None:
+    """level1_special/zdotcf.rs:41-1000."""
+    _dotf("coral_zdotcf", "z", n_rows, n_cols, matrix, lda, x, incx, out)
+
+
 # ---------------------------------------------------------------- level 2 ----
 def sgemv(trans, n_rows, n_cols, alpha, matrix, lda, x, incx, beta, y, incy) -> None:
     """level2/sgemv.rs:63-80."""

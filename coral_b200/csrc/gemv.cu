@@ -271,6 +271,34 @@ coral_status_t enqueue_gemv(Handle* h, bool trans, size_t m, size_t n, float alp
 
 using namespace coral;
 
+// Fused level-1.5 updates in fp32 (level1_special/saxpyf.rs:36-513,
+// sdotf.rs:37-600): y += A x and out += A^T x on the SGEMV kernels with
+// alpha = beta = 1.  Argument positions follow the reference's lists.
+extern "C" coral_status_t coral_saxpyf(coral_handle_t hh, size_t n_rows, size_t n_cols, const float* x,
+                                       size_t incx, const float* matrix, size_t lda, float* y, size_t incy) {
+  CORAL_HANDLE(hh);
+  if (n_rows == 0 || n_cols == 0) return CORAL_OK;   // saxpyf.rs:46-47
+  if (!x) return bad_arg(H, 3);
+  if (incx == 0) return bad_arg(H, 4);
+  if (!matrix) return bad_arg(H, 5);
+  if (lda < n_rows) return bad_arg(H, 6);
+  if (!y) return bad_arg(H, 7);
+  if (incy == 0) return bad_arg(H, 8);
+  return enqueue_gemv(H, false, n_rows, n_cols, 1.0f, matrix, lda, x, incx, 1.0f, y, incy);
+}
+
+extern "C" coral_status_t coral_sdotf(coral_handle_t hh, size_t n_rows, size_t n_cols, const float* matrix,
+                                      size_t lda, const float* x, size_t incx, float* out) {
+  CORAL_HANDLE(hh);
+  if (n_rows == 0 || n_cols == 0) return CORAL_OK;   // sdotf.rs:46-47
+  if (!matrix) return bad_arg(H, 3);
+  if (lda < n_rows) return bad_arg(H, 4);
+  if (!x) return bad_arg(H, 5);
+  if (incx == 0) return bad_arg(H, 6);
+  if (!out) return bad_arg(H, 7);
+  return enqueue_gemv(H, true, n_rows, n_cols, 1.0f, matrix, lda, x, incx, 1.0f, out, 1);
+}
+
 extern "C" coral_status_t coral_sgemv(coral_handle_t hh, int trans, size_t n_rows, size_t n_cols,
                                       float alpha, const float* matrix, size_t lda,
                                       const float* x, size_t incx, float beta, float* y,

@@ -360,12 +360,83 @@ coral_status_t complex_gemv(Handle* H, int trans, size_t n_rows, size_t n_cols, 
                    reinterpret_cast<T*>(y), incy);
 }
 
+// Fused level-1.5 updates (level1_special/*axpyf.rs, *dotf.rs): y += A x
+// (axpyf, op 0) or out += op(A) x with op T (dotf / dotuf) or C (dotcf), on
+// the GEMV kernels with alpha = beta = 1 (the beta step then leaves y alone).
+// Argument positions follow the reference's lists: axpyf (n_rows 1, n_cols 2,
+// x 3, incx 4, matrix 5, lda 6, y 7, incy 8); dotf (matrix 3, lda 4, x 5,
+// incx 6, out 7; out is contiguous).
+template <typename T>
+coral_status_t fused_g(Handle* H, int op, size_t n_rows, size_t n_cols, const void* matrix, size_t lda,
+                       const void* x, size_t incx, void* y, size_t incy) {
+  const bool axpy = op == 0;
+  if (n_rows == 0 || n_cols == 0) return CORAL_OK;   // saxpyf.rs:46-47, sdotf.rs:46-47
+  if (axpy) {
+    if (!x) return bad_arg(H, 3);
+    if (incx == 0) return bad_arg(H, 4);
+    if (!matrix) return bad_arg(H, 5);
+    if (lda < n_rows) return bad_arg(H, 6);
+    if (!y) return bad_arg(H, 7);
+    if (incy == 0) return bad_arg(H, 8);
+  } else {
+    if (!matrix) return bad_arg(H, 3);
+    if (lda < n_rows) return bad_arg(H, 4);
+    if (!x) return bad_arg(H, 5);
+    if (incx == 0) return bad_arg(H, 6);
+    if (!y) return bad_arg(H, 7);
+  }
+  if (((uintptr_t)matrix | (uintptr_t)x | (uintptr_t)y) % sizeof(T)) return bad_arg(H, axpy ? 5 : 3);
+  return gemv_g<T>(H, op, n_rows, n_cols, Fld<T>::one(), false, Fld<T>::one(), 0, static_cast<const T*>(matrix),
+                   lda, static_cast<const T*>(x), incx, static_cast<T*>(y), axpy ? incy : 1);
+}
+
 }  // namespace
 }  // namespace coral
 
 using namespace coral;
 
 extern "C" {
+
+coral_status_t coral_daxpyf(coral_handle_t hh, size_t n_rows, size_t n_cols, const double* x, size_t incx,
+                            const double* matrix, size_t lda, double* y, size_t incy) {
+  CORAL_HANDLE(hh);
+  return fused_g<double>(H, 0, n_rows, n_cols, matrix, lda, x, incx, y, incy);
+}
+coral_status_t coral_caxpyf(coral_handle_t hh, size_t n_rows, size_t n_cols, const float* x, size_t incx,
+                            const float* matrix, size_t lda, float* y, size_t incy) {
+  CORAL_HANDLE(hh);
+  return fused_g<float2>(H, 0, n_rows, n_cols, matrix, lda, x, incx, y, incy);
+}
+coral_status_t coral_zaxpyf(coral_handle_t hh, size_t n_rows, size_t n_cols, const double* x, size_t incx,
+                            const double* matrix, size_t lda, double* y, size_t incy) {
+  CORAL_HANDLE(hh);
+  return fused_g<double2>(H, 0, n_rows, n_cols, matrix, lda, x, incx, y, incy);
+}
+coral_status_t coral_ddotf(coral_handle_t hh, size_t n_rows, size_t n_cols, const double* matrix, size_t lda,
+                           const double* x, size_t incx, double* out) {
+  CORAL_HANDLE(hh);
+  return fused_g<double>(H, 1, n_rows, n_cols, matrix, lda, x, incx, out, 1);
+}
+coral_status_t coral_cdotuf(coral_handle_t hh, size_t n_rows, size_t n_cols, const float* matrix, size_t lda,
+                            const float* x, size_t incx, float* out) {
+  CORAL_HANDLE(hh);
+  return fused_g<float2>(H, 1, n_rows, n_cols, matrix, lda, x, incx, out, 1);
+}
+coral_status_t coral_cdotcf(coral_handle_t hh, size_t n_rows, size_t n_cols, const float* matrix, size_t lda,
+                            const float* x, size_t incx, float* out) {
+  CORAL_HANDLE(hh);
+  return fused_g<float2>(H, 2, n_rows, n_cols, matrix, lda, x, incx, out, 1);
+}
+coral_status_t coral_zdotuf(coral_handle_t hh, size_t n_rows, size_t n_cols, const double* matrix, size_t lda,
+                            const double* x, size_t incx, double* out) {
+  CORAL_HANDLE(hh);
+  return fused_g<double2>(H, 1, n_rows, n_cols, matrix, lda, x, incx, out, 1);
+}
+coral_status_t coral_zdotcf(coral_handle_t hh, size_t n_rows, size_t n_cols, const double* matrix, size_t lda,
+                            const double* x, size_t incx, double* out) {
+  CORAL_HANDLE(hh);
+  return fused_g<double2>(H, 2, n_rows, n_cols, matrix, lda, x, incx, out, 1);
+}
 
 coral_status_t coral_dgemv(coral_handle_t hh, int trans, size_t n_rows, size_t n_cols, double alpha,
                            const double* matrix, size_t lda, const double* x, size_t incx,

@@ -229,6 +229,33 @@ coral_status_t coral_srotmg(coral_handle_t h, float* d1, float* d2, float* x1, f
 coral_status_t coral_drotmg(coral_handle_t h, double* d1, double* d2, double* x1,
                             double y1, double param[5]);
 
+/* ---- fused level 1.5 (coral-aarch64/src/level1_special) ------------------ */
+/* y[0..n_rows) += A x (x: n_cols elements), the reference's argument lists:
+ * saxpyf.rs:36-513, daxpyf.rs:45-518, caxpyf.rs:48-696, zaxpyf.rs:49-697 */
+coral_status_t coral_saxpyf(coral_handle_t h, size_t n_rows, size_t n_cols, const float* x,
+                            size_t incx, const float* matrix, size_t lda, float* y, size_t incy);
+coral_status_t coral_daxpyf(coral_handle_t h, size_t n_rows, size_t n_cols, const double* x,
+                            size_t incx, const double* matrix, size_t lda, double* y, size_t incy);
+coral_status_t coral_caxpyf(coral_handle_t h, size_t n_rows, size_t n_cols, const float* x,
+                            size_t incx, const float* matrix, size_t lda, float* y, size_t incy);
+coral_status_t coral_zaxpyf(coral_handle_t h, size_t n_rows, size_t n_cols, const double* x,
+                            size_t incx, const double* matrix, size_t lda, double* y, size_t incy);
+/* out[0..n_cols) += A^T x (x: n_rows elements, out contiguous): sdotf.rs:37-600,
+ * ddotf.rs:37-596, cdotuf.rs:41-764, zdotuf.rs:41-665; out += A^H x:
+ * cdotcf.rs:42-765, zdotcf.rs:41-1000 */
+coral_status_t coral_sdotf(coral_handle_t h, size_t n_rows, size_t n_cols, const float* matrix,
+                           size_t lda, const float* x, size_t incx, float* out);
+coral_status_t coral_ddotf(coral_handle_t h, size_t n_rows, size_t n_cols, const double* matrix,
+                           size_t lda, const double* x, size_t incx, double* out);
+coral_status_t coral_cdotuf(coral_handle_t h, size_t n_rows, size_t n_cols, const float* matrix,
+                            size_t lda, const float* x, size_t incx, float* out);
+coral_status_t coral_cdotcf(coral_handle_t h, size_t n_rows, size_t n_cols, const float* matrix,
+                            size_t lda, const float* x, size_t incx, float* out);
+coral_status_t coral_zdotuf(coral_handle_t h, size_t n_rows, size_t n_cols, const double* matrix,
+                            size_t lda, const double* x, size_t incx, double* out);
+coral_status_t coral_zdotcf(coral_handle_t h, size_t n_rows, size_t n_cols, const double* matrix,
+                            size_t lda, const double* x, size_t incx, double* out);
+
 /* ---- level 2 (coral-aarch64/src/level2) --------------------------------- */
 /* sgemv.rs:63-80 */
 coral_status_t coral_sgemv(coral_handle_t h, int trans, size_t n_rows, size_t n_cols,
