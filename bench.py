@@ -460,10 +460,10 @@ def level12_bandwidth(torch, cb, lib, h, dev, g, routines=None):
     if want("saxpy"):
         rec("saxpy", 12 * n1, timed_calls(lambda: cb.saxpy(n1, 0.5, x, 1, y, 1), 20, False))
     del x, y
-    # double / complex level 1 at 2^25 elements per vector (complex128: 512 MiB):
+    # double / complex level 1 at 2^26 elements per vector, as sdot (complex128: 1 GiB):
     # (name, kind, vectors moved per element, call); reductions write their
     # scalar to device memory (pointer mode 1) so the calls can be captured.
-    n2 = 1 << 25
+    n2 = 1 << 26
     P = lambda t: vp(t.data_ptr())  # noqa: E731
     rq = vp(res.data_ptr())
     l1_specs = [

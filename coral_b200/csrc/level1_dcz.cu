@@ -19,6 +19,8 @@
 #include "common.cuh"
 
 #include <cfloat>
+#include <mutex>
+#include <unordered_map>
 
 namespace coral {
 namespace {
@@ -649,7 +651,33 @@ __global__ void k_rotmg(R* d1, R* d2, R* x1, R y1, R* param) {
 }
 
 // ---- host helpers ------------------------------------------------------------------
-unsigned l1_grid(Handle* h, size_t n) { return stream_grid(n, (size_t)kL1 * 8, h->sm_count, 8); }
+// Resident blocks of 256 threads per SM of a kernel, queried once per kernel.
+int resident_blocks(const void* kernel) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto it = cache.find(kernel);
+  if (it != cache.end()) return it->second;
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kL1, 0) != cudaSuccess || b < 1) {
+    cudaGetLastError();
+    b = 1;
+  }
+  cache.emplace(kernel, b);
+  return b;
+}
+
+// Most blocks a level-1 launch uses (256 threads: at most 8 resident per SM);
+// the reductions size their per-block partials for it.
+size_t max_l1_blocks(Handle* h) { return (size_t)h->sm_count * 8; }
+
+// Launches a streaming level-1 kernel on at most one wave of its resident
+// blocks, each with at least 8 x 256 elements.
+template <typename... P, typename... A>
+void l1_launch(Handle* h, size_t n, void (*kernel)(P...), A&&... args) {
+  const unsigned g = stream_grid(n, (size_t)kL1 * 8, h->sm_count, resident_blocks((const void*)kernel));
+  kernel<<<g, kL1, 0, h->stream>>>(std::forward<A>(args)...);
+}
 
 template <typename Out>
 coral_status_t finish(Handle* H, Out* result, const void* dres, size_t bytes) {
@@ -688,16 +716,15 @@ coral_status_t dot_entry(coral_handle_t hh, size_t n, const void* x, size_t incx
   if (!y) return bad_arg(H, 4);
   if (incy == 0) return bad_arg(H, 5);
   if (((uintptr_t)x | (uintptr_t)y) & (align - 1)) return bad_arg(H, 2);
-  const unsigned g = l1_grid(H, n);
-  double* part = static_cast<double*>(scratch(H, (size_t)g * 2 * sizeof(double)));
+  double* part = static_cast<double*>(scratch(H, max_l1_blocks(H) * 2 * sizeof(double)));
   if (!part) return CORAL_ERR_ALLOC;
   const T* xx = static_cast<const T*>(x);
   const T* yy = static_cast<const T*>(y);
   unsigned* ctr = &H->words->counters[kCtrMisc];
   if (unit_ok(incx, incy, x, y))
-    k_dot_x<T, kConj, true><<<g, kL1, 0, H->stream>>>(n, xx, 1, yy, 1, part, ctr, dres);
+    l1_launch(H, n, k_dot_x<T, kConj, true>, n, xx, 1, yy, 1, part, ctr, dres);
   else
-    k_dot_x<T, kConj, false><<<g, kL1, 0, H->stream>>>(n, xx, incx, yy, incy, part, ctr, dres);
+    l1_launch(H, n, k_dot_x<T, kConj, false>, n, xx, incx, yy, incy, part, ctr, dres);
   return finish(H, result, dres, sizeof(T));
 }
 
@@ -712,15 +739,14 @@ coral_status_t asum_entry(coral_handle_t hh, size_t n, const void* x, size_t inc
   }
   if (!x) return bad_arg(H, 2);
   if ((uintptr_t)x & (align - 1)) return bad_arg(H, 2);
-  const unsigned g = l1_grid(H, n);
-  double* part = static_cast<double*>(scratch(H, (size_t)g * sizeof(double)));
+  double* part = static_cast<double*>(scratch(H, max_l1_blocks(H) * sizeof(double)));
   if (!part) return CORAL_ERR_ALLOC;
   const T* xx = static_cast<const T*>(x);
   unsigned* ctr = &H->words->counters[kCtrMisc];
   if (unit_ok(incx, 1, x, x))
-    k_asum_x<T, R, true><<<g, kL1, 0, H->stream>>>(n, xx, 1, part, ctr, dres);
+    l1_launch(H, n, k_asum_x<T, R, true>, n, xx, 1, part, ctr, dres);
   else
-    k_asum_x<T, R, false><<<g, kL1, 0, H->stream>>>(n, xx, incx, part, ctr, dres);
+    l1_launch(H, n, k_asum_x<T, R, false>, n, xx, incx, part, ctr, dres);
   return finish(H, result, dres, sizeof(R));
 }
 
@@ -735,8 +761,7 @@ coral_status_t nrm2_entry(coral_handle_t hh, size_t n, const void* x, size_t inc
   }
   if (!x) return bad_arg(H, 2);
   if ((uintptr_t)x & (align - 1)) return bad_arg(H, 2);
-  const unsigned g = l1_grid(H, n);
-  double* part = static_cast<double*>(scratch(H, (size_t)g * 2 * sizeof(double)));
+  double* part = static_cast<double*>(scratch(H, max_l1_blocks(H) * 2 * sizeof(double)));
   if (!part) return CORAL_ERR_ALLOC;
   unsigned* flag = &H->words->counters[kCtrMisc + 1];
   double* dmx = &H->words->dresult[3];
@@ -744,16 +769,16 @@ coral_status_t nrm2_entry(coral_handle_t hh, size_t n, const void* x, size_t inc
   unsigned* ctr = &H->words->counters[kCtrMisc];
   const bool unit = unit_ok(incx, 1, x, x);
   if (unit)
-    k_nrm2_x<T, R, true><<<g, kL1, 0, H->stream>>>(n, xx, 1, part, ctr, flag, dmx, dres);
+    l1_launch(H, n, k_nrm2_x<T, R, true>, n, xx, 1, part, ctr, flag, dmx, dres);
   else
-    k_nrm2_x<T, R, false><<<g, kL1, 0, H->stream>>>(n, xx, incx, part, ctr, flag, dmx, dres);
+    l1_launch(H, n, k_nrm2_x<T, R, false>, n, xx, incx, part, ctr, flag, dmx, dres);
   coral_status_t s = launch_status(H);
   if (s != CORAL_OK) return s;
   if (sizeof(R) == 8) {   // fp64 data: rescaling pass (returns at once unless asked)
     if (unit)
-      k_nrm2_scaled<T, R, true><<<g, kL1, 0, H->stream>>>(n, xx, 1, part, ctr, flag, dmx, dres);
+      l1_launch(H, n, k_nrm2_scaled<T, R, true>, n, xx, 1, part, ctr, flag, dmx, dres);
     else
-      k_nrm2_scaled<T, R, false><<<g, kL1, 0, H->stream>>>(n, xx, incx, part, ctr, flag, dmx, dres);
+      l1_launch(H, n, k_nrm2_scaled<T, R, false>, n, xx, incx, part, ctr, flag, dmx, dres);
   }
   return finish(H, result, dres, sizeof(R));
 }
@@ -769,17 +794,16 @@ coral_status_t iamax_entry(coral_handle_t hh, size_t n, const void* x, size_t in
   }
   if (!x) return bad_arg(H, 2);
   if ((uintptr_t)x & (align - 1)) return bad_arg(H, 2);
-  const unsigned g = l1_grid(H, n);
-  char* sc = static_cast<char*>(scratch(H, (size_t)g * 16));
+  char* sc = static_cast<char*>(scratch(H, max_l1_blocks(H) * 16));
   if (!sc) return CORAL_ERR_ALLOC;
   double* pv = reinterpret_cast<double*>(sc);
-  unsigned long long* pi = reinterpret_cast<unsigned long long*>(sc + (size_t)g * 8);
+  unsigned long long* pi = reinterpret_cast<unsigned long long*>(sc + max_l1_blocks(H) * 8);
   const T* xx = static_cast<const T*>(x);
   unsigned* ctr = &H->words->counters[kCtrMisc];
   if (unit_ok(incx, 1, x, x))
-    k_iamax_x<T, true><<<g, kL1, 0, H->stream>>>(n, xx, 1, pv, pi, ctr, dres);
+    l1_launch(H, n, k_iamax_x<T, true>, n, xx, 1, pv, pi, ctr, dres);
   else
-    k_iamax_x<T, false><<<g, kL1, 0, H->stream>>>(n, xx, incx, pv, pi, ctr, dres);
+    l1_launch(H, n, k_iamax_x<T, false>, n, xx, incx, pv, pi, ctr, dres);
   return finish(H, index, dres, sizeof(size_t));
 }
 
@@ -802,9 +826,9 @@ coral_status_t axpy_entry(coral_handle_t hh, size_t n, T alpha, bool alpha_zero,
   const T* xx = static_cast<const T*>(x);
   T* yy = static_cast<T*>(y);
   if (unit_ok(incx, incy, x, y))
-    k_axpy_x<T, true><<<l1_grid(H, n), kL1, 0, H->stream>>>(n, nf, alpha, xx, 1, yy, 1);
+    l1_launch(H, n, k_axpy_x<T, true>, n, nf, alpha, xx, 1, yy, 1);
   else
-    k_axpy_x<T, false><<<l1_grid(H, n), kL1, 0, H->stream>>>(n, nf, alpha, xx, incx, yy, incy);
+    l1_launch(H, n, k_axpy_x<T, false>, n, nf, alpha, xx, incx, yy, incy);
   return launch_status(H);
 }
 
@@ -817,9 +841,9 @@ coral_status_t scal_entry(coral_handle_t hh, size_t n, T alpha, void* x, size_t 
   const size_t nf = fused_len(n, incx, 1, w);
   T* xx = static_cast<T*>(x);
   if (unit_ok(incx, 1, x, x))
-    k_scal_x<T, kReal, true><<<l1_grid(H, n), kL1, 0, H->stream>>>(n, nf, alpha, xx, 1);
+    l1_launch(H, n, k_scal_x<T, kReal, true>, n, nf, alpha, xx, 1);
   else
-    k_scal_x<T, kReal, false><<<l1_grid(H, n), kL1, 0, H->stream>>>(n, nf, alpha, xx, incx);
+    l1_launch(H, n, k_scal_x<T, kReal, false>, n, nf, alpha, xx, incx);
   return launch_status(H);
 }
 
@@ -835,14 +859,13 @@ coral_status_t copy_entry(coral_handle_t hh, size_t n, const void* x, size_t inc
   if (((uintptr_t)x | (uintptr_t)y) & (alignof(E) - 1)) return bad_arg(H, 2);
   E* xx = static_cast<E*>(const_cast<void*>(x));
   E* yy = static_cast<E*>(y);
-  const unsigned g = l1_grid(H, n);
   const bool unit = unit_ok(incx, incy, x, y);
   if (swap) {
-    if (unit) k_swap_x<E, true><<<g, kL1, 0, H->stream>>>(n, xx, 1, yy, 1);
-    else k_swap_x<E, false><<<g, kL1, 0, H->stream>>>(n, xx, incx, yy, incy);
+    if (unit) l1_launch(H, n, k_swap_x<E, true>, n, xx, 1, yy, 1);
+    else l1_launch(H, n, k_swap_x<E, false>, n, xx, incx, yy, incy);
   } else {
-    if (unit) k_copy_x<E, true><<<g, kL1, 0, H->stream>>>(n, xx, 1, yy, 1);
-    else k_copy_x<E, false><<<g, kL1, 0, H->stream>>>(n, xx, incx, yy, incy);
+    if (unit) l1_launch(H, n, k_copy_x<E, true>, n, xx, 1, yy, 1);
+    else l1_launch(H, n, k_copy_x<E, false>, n, xx, incx, yy, incy);
   }
   return launch_status(H);
 }
@@ -861,9 +884,9 @@ coral_status_t rot_entry(coral_handle_t hh, size_t n, void* x, size_t incx, void
   T* xx = static_cast<T*>(x);
   T* yy = static_cast<T*>(y);
   if (unit_ok(incx, incy, x, y))
-    k_rot_x<T, R, true><<<l1_grid(H, n), kL1, 0, H->stream>>>(n, nf, xx, 1, yy, 1, c, s);
+    l1_launch(H, n, k_rot_x<T, R, true>, n, nf, xx, 1, yy, 1, c, s);
   else
-    k_rot_x<T, R, false><<<l1_grid(H, n), kL1, 0, H->stream>>>(n, nf, xx, incx, yy, incy, c, s);
+    l1_launch(H, n, k_rot_x<T, R, false>, n, nf, xx, incx, yy, incy, c, s);
   return launch_status(H);
 }
 
@@ -881,10 +904,10 @@ coral_status_t rotm_entry(coral_handle_t hh, size_t n, R* x, size_t incx, R* y, 
   if (((uintptr_t)x | (uintptr_t)y) & (sizeof(R) - 1)) return bad_arg(H, 2);
   const size_t nf = fused_len(n, incx, incy, w);
   if (unit_ok(incx, incy, x, y))
-    k_rotm_x<R, true><<<l1_grid(H, n), kL1, 0, H->stream>>>(n, nf, x, 1, y, 1, param[0], param[1], param[2],
+    l1_launch(H, n, k_rotm_x<R, true>, n, nf, x, 1, y, 1, param[0], param[1], param[2],
                                                              param[3], param[4]);
   else
-    k_rotm_x<R, false><<<l1_grid(H, n), kL1, 0, H->stream>>>(n, nf, x, incx, y, incy, param[0], param[1],
+    l1_launch(H, n, k_rotm_x<R, false>, n, nf, x, incx, y, incy, param[0], param[1],
                                                               param[2], param[3], param[4]);
   return launch_status(H);
 }
