@@ -16,8 +16,8 @@
 //      2j, 2j+1 of B'' = [Re B_j | -Im B_j], [Im B_j | Re B_j], so that
 //      columns 2j, 2j+1 of A'' B''^T are Re and Im of C_j.
 //   2. GEMM kernel: one CTA per 128 x BN tile of C.  Warp 0 lane 0 issues
-//      TMA loads of all pieces of a 64-deep K slab into a 2-stage ring
-//      (128-byte swizzle, full/empty mbarriers); warp 1 lane 0 issues the
+//      TMA loads of all pieces of a 32-deep K slab into a 4-stage ring
+//      (64-byte swizzle, full/empty mbarriers); warp 1 lane 0 issues the
 //      tcgen05.mma products (M=128, N=BN, K=16 per instruction) into one
 //      fp32 TMEM accumulator of BN columns and commits each stage back to
 //      the producer; then all 4 warps read the accumulator row by row
@@ -79,8 +79,15 @@ bool encode_kmajor_map(CUtensorMap* map, const void* base, int elem_bytes, uint6
 namespace {
 
 constexpr int kBM = 128;
-constexpr int kBK = 64;  // bf16 elements per 128-byte swizzled row
-constexpr int kStages = 2;
+constexpr int kBK = 32;   // bf16 elements per 64-byte swizzled row of a K slab
+constexpr int kStages = 4;
+constexpr int kSwizzle = kBK * 2;   // bytes: the TMA swizzle span of a slab row
+// K slabs of kBK per 64-deep unit of the handle's chunk setting
+constexpr int kSlabsPer64 = 64 / kBK;
+
+__device__ __forceinline__ uint64_t slab_desc(uint32_t saddr) {
+  return kSwizzle == 128 ? tc::desc_k_sw128(saddr) : tc::desc_k_sw64(saddr);
+}
 
 template <int P> struct SplitPlan;
 // pairs (i, j): product A_i * B_j, smallest terms first
@@ -231,7 +238,7 @@ __device__ __forceinline__ void tile_coords(int tile, int m_tiles, int n_tiles, 
 }
 
 // Persistent kernel, 2 + 8 warps:
-//   warp 0 lane 0: TMA producer over a 2-stage ring of K slabs (all pieces);
+//   warp 0 lane 0: TMA producer over a 4-stage ring of K slabs (all pieces);
 //   warp 1 lane 0: tcgen05.mma issuer.  The K loop of a tile is cut into
 //     chunks of `chunk_kb` slabs; chunk c accumulates (from zero) into TMEM
 //     buffer c % 2 and is committed to chunk_full[c % 2];
@@ -364,8 +371,8 @@ k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int 
             for (int kk = 0; kk < kBK / 16; ++kk) {
 #pragma unroll
               for (int q = 0; q < Plan::kProducts; ++q) {
-                const uint64_t ad = tc::desc_k_sw128(sa + Plan::a(q) * kATile + kk * 32);
-                const uint64_t bd = tc::desc_k_sw128(sb + Plan::b(q) * kBTile + kk * 32);
+                const uint64_t ad = slab_desc(sa + Plan::a(q) * kATile + kk * 32);
+                const uint64_t bd = slab_desc(sb + Plan::b(q) * kBTile + kk * 32);
                 tc::mma_f16(acc, ad, bd, kIdesc, ((kb - kb0) | kk | q) != 0);
               }
             }
@@ -516,8 +523,10 @@ coral_status_t run_split_gemm(Handle* h, const __nv_bfloat16* ap, size_t a_piece
   SplitMaps maps;
   std::memset(&maps, 0, sizeof(maps));
   for (int p = 0; p < SplitPlan<NP>::kPieces; ++p) {
-    if (!encode_kmajor_map(&maps.a[p], ap + p * a_piece, 2, (uint64_t)kd, (uint64_t)mr, kp * 2, kBK, kBM) ||
-        !encode_kmajor_map(&maps.b[p], bp + p * b_piece, 2, (uint64_t)kd, (uint64_t)nr, kp * 2, kBK, BN))
+    if (!encode_kmajor_map(&maps.a[p], ap + p * a_piece, 2, (uint64_t)kd, (uint64_t)mr, kp * 2, kBK, kBM,
+                           kSwizzle) ||
+        !encode_kmajor_map(&maps.b[p], bp + p * b_piece, 2, (uint64_t)kd, (uint64_t)nr, kp * 2, kBK, BN,
+                           kSwizzle))
       return CORAL_ERR_NOT_SUPPORTED;
   }
   const size_t smem = gemm_smem_bytes<NP, BN>();
@@ -534,7 +543,7 @@ coral_status_t run_split_gemm(Handle* h, const __nv_bfloat16* ap, size_t a_piece
   const uint64_t limit_ns = h->wait_limit * 32ull;  // default 2^26 * 32 ns ~ 2.1 s
   timed_begin(h);
   k_gemm_split<NP, BN><<<grid, kSplitThreads, smem, h->stream>>>(
-      maps, kd, m_tiles, n_tiles, h->split_chunk_kb, splits, ws, nr, ep, &h->words->status,
+      maps, kd, m_tiles, n_tiles, h->split_chunk_kb * kSlabsPer64, splits, ws, nr, ep, &h->words->status,
       limit_ns);
   coral_status_t s = launch_status(h);
   timed_end(h);
@@ -553,7 +562,7 @@ coral_status_t run_split_gemm(Handle* h, const __nv_bfloat16* ap, size_t a_piece
 SplitConfig choose_split_config(Handle* h, const SplitShape& sh) {
   const int products = sh.products, mr = sh.mr, nr = sh.nr, kd = sh.kd;
   SplitConfig c{products == 3 ? 256 : 128, 1};
-  const int nk = (kd + kBK - 1) / kBK;
+  const int nk = (kd + 63) / 64;   // 64-deep K units (independent of the kernel's slab depth)
   if (h->cfg_bn > 0 || h->cfg_splits > 0) {
     if (h->cfg_bn > 0) c.bn = h->cfg_bn;
     if (h->cfg_splits > 0) c.splits = h->cfg_splits;
@@ -802,8 +811,8 @@ extern "C" coral_status_t coral_sgemm_bf16x3_noalloc(void* stream, int op_a, int
   SplitMaps maps;
   std::memset(&maps, 0, sizeof(maps));
   for (int p = 0; p < 2; ++p) {
-    if (!encode_kmajor_map(&maps.a[p], ap + p * a_piece, 2, k, m, kp * 2, kBK, kBM) ||
-        !encode_kmajor_map(&maps.b[p], bp + p * b_piece, 2, k, n, kp * 2, kBK, 256))
+    if (!encode_kmajor_map(&maps.a[p], ap + p * a_piece, 2, k, m, kp * 2, kBK, kBM, kSwizzle) ||
+        !encode_kmajor_map(&maps.b[p], bp + p * b_piece, 2, k, n, kp * 2, kBK, 256, kSwizzle))
       return CORAL_ERR_NOT_SUPPORTED;
   }
   const int m_tiles = (int)((m + kBM - 1) / kBM), n_tiles = (int)((n + 255) / 256);
@@ -811,6 +820,7 @@ extern "C" coral_status_t coral_sgemm_bf16x3_noalloc(void* stream, int op_a, int
   const int grid = tiles < d->sm_count ? tiles : d->sm_count;
   EpiParams ep{c, ldc, (int)m, (int)n, alpha, 0.f, beta, 0.f, 0};
   k_gemm_split<3, 256><<<grid, kSplitThreads, gemm_smem_bytes<3, 256>(), st>>>(
-      maps, (int)k, m_tiles, n_tiles, 16, 1, nullptr, (int)n, ep, d->status, kDefaultWaitLimit * 32ull);
+      maps, (int)k, m_tiles, n_tiles, 16 * kSlabsPer64, 1, nullptr, (int)n, ep, d->status,
+      kDefaultWaitLimit * 32ull);
   return launch_status(nullptr);
 }

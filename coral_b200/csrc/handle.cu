@@ -126,7 +126,7 @@ static void destroy_handle(Handle* h) {
 
 // Per-thread handle plus growable device staging for the host-slice wrappers,
 // and the copy streams / events of the pipelined host SGEMM.
-constexpr int kHostPanels = 8;
+constexpr int kHostPanels = 16;
 struct ThreadState {
   Handle* h = nullptr;
   void* dev = nullptr;
@@ -316,7 +316,7 @@ coral_status_t coral_host_set_gemm_mode(int mode) {
 
 // Host-resident operands: for a large problem the PCIe transfers, not the
 // GEMM, bound the call.  A is copied first; then column panels of op(B) and C
-// (8 panels, widths a multiple of 256) stream in on one copy stream, the GEMM
+// (16 panels, widths a multiple of 256) stream in on one copy stream, the GEMM
 // of panel j runs on the handle's stream as soon as its inputs land, and C
 // panel j streams back on a second copy stream -- so host-to-device,
 // device-to-host and the compute overlap.  C is not copied in when beta == 0
