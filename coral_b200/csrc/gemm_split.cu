@@ -160,6 +160,119 @@ k_split_real(const float* __restrict__ X, size_t ld, int R, int Kd, __nv_bfloat1
   }
 }
 
+// Eight consecutive K values of one row split into NPC pieces, each piece's
+// eight bf16 stored with one 16-byte store at dst + i * piece_stride + o.
+template <int NPC>
+__device__ __forceinline__ void split_store8(const float (&v)[8], __nv_bfloat16* __restrict__ dst,
+                                             size_t piece_stride, size_t o) {
+  __align__(16) __nv_bfloat16 q[3][8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    __nv_bfloat16 p[3];
+    split_value<NPC>(v[j], p);
+#pragma unroll
+    for (int i = 0; i < NPC; ++i) q[i][j] = p[i];
+  }
+#pragma unroll
+  for (int i = 0; i < NPC; ++i)
+    __stcs(reinterpret_cast<uint4*>(dst + i * piece_stride + o), *reinterpret_cast<const uint4*>(q[i]));
+}
+
+// Vector forms of k_split_real, for a 16-byte-aligned X with ld % 4 == 0
+// (dst rows are 16-byte multiples: kp % 8 == 0).
+// K-major storage (src(r, l) = X[l + r*ld]): a thread converts 8 consecutive
+// K values of a row -- two 16-byte loads, one 16-byte store per piece; a
+// block covers 2048 K values of one row, rows strided over grid.y.
+template <int NPC>
+__global__ void __launch_bounds__(256)
+k_split_rows(const float* __restrict__ X, size_t ld, int R, int Kd, __nv_bfloat16* __restrict__ dst, size_t kp,
+             size_t piece_stride) {
+  const size_t l = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * 8;
+  if (l >= kp) return;
+  for (int r = blockIdx.y; r < R; r += gridDim.y) {
+    const float* src = X + (size_t)r * ld + l;
+    float v[8];
+    if (l + 8 <= (size_t)Kd) {
+      const float4 a = __ldcs(reinterpret_cast<const float4*>(src));
+      const float4 b = __ldcs(reinterpret_cast<const float4*>(src) + 1);
+      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+      v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[j] = l + j < (size_t)Kd ? src[j] : 0.f;
+    }
+    split_store8<NPC>(v, dst, piece_stride, (size_t)r * kp + l);
+  }
+}
+
+// Storage contiguous along r (src(r, l) = X[r + l*ld]): 64 x 64 tiles read
+// as 16-byte column segments, transposed through shared memory (pitch 65:
+// at most 2-way bank conflicts on the column reads), written as 16-byte
+// row segments of 8 K values; a warp writes 4 rows x 128 contiguous bytes
+// per piece.  Tiles along r are strided over grid.y.
+template <int NPC>
+__global__ void __launch_bounds__(256)
+k_split_cols(const float* __restrict__ X, size_t ld, int R, int Kd, __nv_bfloat16* __restrict__ dst, size_t kp,
+             size_t piece_stride) {
+  __shared__ float tile[64][65];   // [l][r]
+  const int t = threadIdx.x;
+  const int l0 = blockIdx.x * 64;
+  for (int r0 = blockIdx.y * 64; r0 < R; r0 += gridDim.y * 64) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int ll = t / 16 + 16 * q, r4 = t % 16;
+      const int l = l0 + ll, r = r0 + 4 * r4;
+      float e[4] = {0.f, 0.f, 0.f, 0.f};
+      if (l < Kd) {
+        const float* src = X + r + (size_t)l * ld;
+        if (r + 3 < R) {
+          const float4 a = __ldcs(reinterpret_cast<const float4*>(src));
+          e[0] = a.x; e[1] = a.y; e[2] = a.z; e[3] = a.w;
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) e[j] = r + j < R ? src[j] : 0.f;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) tile[ll][4 * r4 + j] = e[j];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int task = t + 256 * q, c = task % 8, rl = task / 8;
+      const int r = r0 + rl;
+      const size_t l = (size_t)l0 + 8 * c;
+      if (r < R && l < kp) {
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = tile[8 * c + j][rl];
+        split_store8<NPC>(v, dst, piece_stride, (size_t)r * kp + l);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Splits op(X)'s R x Kd block into NPC pieces [R][kp]: the vector kernels
+// when X is 16-byte aligned with ld % 4 == 0, else k_split_real.
+template <int NPC>
+void launch_split_real(cudaStream_t st, const float* X, size_t ld, int R, int Kd, bool kmajor,
+                       __nv_bfloat16* dst, size_t kp, size_t piece_stride) {
+  const bool vec = aligned16(X) && ld % 4 == 0;
+  if (vec && kmajor) {
+    const dim3 g((unsigned)((kp / 8 + 255) / 256), (unsigned)(R < 65535 ? R : 65535));
+    k_split_rows<NPC><<<g, 256, 0, st>>>(X, ld, R, Kd, dst, kp, piece_stride);
+  } else if (vec) {
+    const int rt = (R + 63) / 64;
+    const dim3 g((unsigned)((kp + 63) / 64), (unsigned)(rt < 65535 ? rt : 65535));
+    k_split_cols<NPC><<<g, 256, 0, st>>>(X, ld, R, Kd, dst, kp, piece_stride);
+  } else {
+    const dim3 g((unsigned)((kp + 31) / 32), (unsigned)((R + 31) / 32));
+    if (kmajor) k_split_real<NPC, true><<<g, 256, 0, st>>>(X, ld, R, Kd, dst, kp, piece_stride);
+    else k_split_real<NPC, false><<<g, 256, 0, st>>>(X, ld, R, Kd, dst, kp, piece_stride);
+  }
+}
+
 // Complex operand, 4M layout.  src(r, l) is the complex element of op(X)
 // (conjugated when `conj`), storage K-major (X[l + r*ld]) or not (X[r + l*ld]).
 //   kIsB == false: dst row r = [Re src(r, :) | Im src(r, :)]          (k' = 2k)
@@ -613,19 +726,11 @@ coral_status_t sgemm_split_impl(Handle* h, int op_a, int op_b, size_t m, size_t 
   __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(sc);
   __nv_bfloat16* bp = reinterpret_cast<__nv_bfloat16*>(sc + a_bytes);
   // op(A) rows are i: storage K-major iff op_a is (conjugate) transpose.
-  dim3 ga((unsigned)((kp + 31) / 32), (unsigned)((m + 31) / 32));
-  if (op_a == CORAL_NO_TRANSPOSE)
-    k_split_real<NPC, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ap, kp, a_piece);
-  else
-    k_split_real<NPC, true><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ap, kp, a_piece);
+  launch_split_real<NPC>(h->stream, A, lda, (int)m, (int)k, op_a != CORAL_NO_TRANSPOSE, ap, kp, a_piece);
   coral_status_t s = launch_status(h);
   if (s != CORAL_OK) return s;
   // op(B)^T rows are j: storage K-major iff op_b is NoTranspose.
-  dim3 gb((unsigned)((kp + 31) / 32), (unsigned)((n + 31) / 32));
-  if (op_b == CORAL_NO_TRANSPOSE)
-    k_split_real<NPC, true><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, bp, kp, b_piece);
-  else
-    k_split_real<NPC, false><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, bp, kp, b_piece);
+  launch_split_real<NPC>(h->stream, B, ldb, (int)n, (int)k, op_b == CORAL_NO_TRANSPOSE, bp, kp, b_piece);
   s = launch_status(h);
   if (s != CORAL_OK) return s;
   EpiParams ep{C, ldc, (int)m, (int)n, alpha, 0.f, beta, 0.f, 0};
@@ -796,17 +901,9 @@ extern "C" coral_status_t coral_sgemm_bf16x3_noalloc(void* stream, int op_a, int
   __nv_bfloat16* bp = reinterpret_cast<__nv_bfloat16*>(d->scratch + a_bytes);
   // Every piece element the GEMM reads is rewritten here, so stale contents
   // of the shared array from an earlier call never leak into this one.
-  dim3 ga((unsigned)((kp + 31) / 32), (unsigned)((m + 31) / 32));
-  if (op_a == CORAL_NO_TRANSPOSE)
-    k_split_real<2, false><<<ga, 256, 0, st>>>(a, lda, (int)m, (int)k, ap, kp, a_piece);
-  else
-    k_split_real<2, true><<<ga, 256, 0, st>>>(a, lda, (int)m, (int)k, ap, kp, a_piece);
+  launch_split_real<2>(st, a, lda, (int)m, (int)k, op_a != CORAL_NO_TRANSPOSE, ap, kp, a_piece);
   if ((s = launch_status(nullptr)) != CORAL_OK) return s;
-  dim3 gb((unsigned)((kp + 31) / 32), (unsigned)((n + 31) / 32));
-  if (op_b == CORAL_NO_TRANSPOSE)
-    k_split_real<2, true><<<gb, 256, 0, st>>>(b, ldb, (int)n, (int)k, bp, kp, b_piece);
-  else
-    k_split_real<2, false><<<gb, 256, 0, st>>>(b, ldb, (int)n, (int)k, bp, kp, b_piece);
+  launch_split_real<2>(st, b, ldb, (int)n, (int)k, op_b == CORAL_NO_TRANSPOSE, bp, kp, b_piece);
   if ((s = launch_status(nullptr)) != CORAL_OK) return s;
   SplitMaps maps;
   std::memset(&maps, 0, sizeof(maps));
