@@ -396,9 +396,21 @@ k_tri_strips(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x
 
 // Per 32 output rows: y = beta*y (or 0 for TRMV) + row parts of every
 // off-diagonal column block + the diagonal block's parts + column parts.
-// 8 groups of 32 threads (lane = row) split the column blocks, 4 loads in
-// flight each, then a fixed-order shared-memory sum.
+// 8 groups of 32 threads (lane = row) split the column blocks; a group loads
+// up to 16 of its partials at once (one L2 round trip covers 128 column
+// blocks, n = 8192) and adds them in a fixed tree order, then a fixed-order
+// shared-memory sum across the groups.
 constexpr int kCombineGroups = 8;
+constexpr int kCombineBatch = 16;
+
+template <typename T, int N>
+__device__ __forceinline__ T tree_sum(T (&a)[N]) {
+#pragma unroll
+  for (int w = N / 2; w >= 1; w /= 2)
+#pragma unroll
+    for (int u = 0; u < w; ++u) a[u] = Cx<T>::add(a[u], a[u + w]);
+  return a[0];
+}
 template <typename T, int kMode, int V>
 __global__ void __launch_bounds__(32 * kCombineGroups)
 k_strip_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
@@ -417,18 +429,27 @@ k_strip_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
     // off-diagonal column blocks whose stored range covers row gr
     const int j0 = lower ? 0 : Jr + 1, j1 = lower ? Jr : ncolblk;
     const T* rp = rowpart + (size_t)gs * ncolblk * kS + li;
-    int J = j0 + g;
-    for (; J + 3 * kCombineGroups < j1; J += 4 * kCombineGroups) {
-      const T a0 = __ldcs(rp + (size_t)J * kS), a1 = __ldcs(rp + (size_t)(J + kCombineGroups) * kS);
-      const T a2 = __ldcs(rp + (size_t)(J + 2 * kCombineGroups) * kS);
-      const T a3 = __ldcs(rp + (size_t)(J + 3 * kCombineGroups) * kS);
-      s = Cx<T>::add(s, Cx<T>::add(Cx<T>::add(a0, a1), Cx<T>::add(a2, a3)));
+    for (int Jb = j0 + g; Jb < j1; Jb += kCombineBatch * kCombineGroups) {
+      T a[kCombineBatch];
+#pragma unroll
+      for (int u = 0; u < kCombineBatch; ++u) {
+        const int J = Jb + u * kCombineGroups;
+        a[u] = J < j1 ? __ldcs(rp + (size_t)J * kS) : Cx<T>::zero();
+      }
+      s = Cx<T>::add(s, tree_sum(a));
     }
-    for (; J < j1; J += kCombineGroups) s = Cx<T>::add(s, __ldcs(rp + (size_t)J * kS));
   }
   if (kCol) {
-    for (int q = g; q < nsplit; q += kCombineGroups)
-      s = Cx<T>::add(s, colpart[((size_t)Jr * nsplit + q) * kC + gr % kC]);
+    const T* cp = colpart + (size_t)Jr * nsplit * kC + gr % kC;
+    for (int qb = g; qb < nsplit; qb += kCombineBatch * kCombineGroups) {
+      T a[kCombineBatch];
+#pragma unroll
+      for (int u = 0; u < kCombineBatch; ++u) {
+        const int q = qb + u * kCombineGroups;
+        a[u] = q < nsplit ? cp[(size_t)q * kC] : Cx<T>::zero();
+      }
+      s = Cx<T>::add(s, tree_sum(a));
+    }
   }
   part[g][lane] = s;
   __syncthreads();
