@@ -384,14 +384,18 @@ k_tri_strips(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x
       for (int e = 0; e < V; ++e) rp[e] = rv[e] ? racc[e] : Cx<T>::zero();
     }
   }
-  if (!kCol) return;
-  __syncthreads();
-  if (threadIdx.x < kC) {
-    T s = red[0][threadIdx.x];
+  if (kCol) {
+    __syncthreads();
+    if (threadIdx.x < kC) {
+      T s = red[0][threadIdx.x];
 #pragma unroll
-    for (int w2 = 1; w2 < kStripWarps; ++w2) s = Cx<T>::add(s, red[w2][threadIdx.x]);
-    colpart[((size_t)J * nsplit + blockIdx.y) * kC + threadIdx.x] = s;
+      for (int w2 = 1; w2 < kStripWarps; ++w2) s = Cx<T>::add(s, red[w2][threadIdx.x]);
+      colpart[((size_t)J * nsplit + blockIdx.y) * kC + threadIdx.x] = s;
+    }
   }
+  // This CTA's share is written: the combine grid may start launching (its
+  // griddepcontrol.wait still waits for the whole of this grid).
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 // Per 32 output rows: y = beta*y (or 0 for TRMV) + row parts of every
@@ -420,6 +424,10 @@ k_strip_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
   constexpr bool kRow = ModeT<kMode>::kRow;
   constexpr bool kCol = ModeT<kMode>::kCol;
   __shared__ T part[kCombineGroups][32];
+  // Launched as a programmatic dependent of k_tri_strips: wait until that
+  // grid has completed and its writes are visible (a no-op when launched
+  // without the dependency).
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   const int g = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gr = blockIdx.x * 32 + lane;
   const int gs = gr / kS, li = gr % kS;   // strip and row within it
@@ -508,8 +516,21 @@ coral_status_t launch_strips(Handle* h, int n, const T* A, size_t lda, const T* 
   timed_end(h);
   if (s != CORAL_OK) return s;
   CORAL_CUDA(h, cudaStreamWaitEvent(h->stream, h->join_event, 0));
-  k_strip_combine<T, kMode, V><<<(n + 31) / 32, 32 * kCombineGroups, 0, h->stream>>>(
-      n, beta, y, incy, lower, sc, sc + rp, ncol, nsplit, drow, dcol);
+  // Programmatic dependent launch: the combine's CTAs are scheduled as the
+  // strips grid drains instead of after it has fully retired.
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((n + 31) / 32);
+  cfg.blockDim = dim3(32 * kCombineGroups);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CORAL_CUDA(h, cudaLaunchKernelEx(&cfg, k_strip_combine<T, kMode, V>, n, beta, y, incy, lower,
+                                   static_cast<const T*>(sc), static_cast<const T*>(sc + rp), ncol, nsplit,
+                                   static_cast<const T*>(drow), static_cast<const T*>(dcol)));
   return launch_status(h);
 }
 
