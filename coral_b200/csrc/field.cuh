@@ -25,6 +25,8 @@ template <> struct Fld<double> {
   static __device__ __forceinline__ double shfl_xor(double v, int o) {
     return __shfl_xor_sync(0xffffffffu, v, o);
   }
+  static __device__ __forceinline__ double shfl(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+  static __device__ __forceinline__ double neg(double a) { return -a; }
 };
 
 template <> struct Fld<float2> {
@@ -57,6 +59,10 @@ template <> struct Fld<float2> {
   static __device__ __forceinline__ float2 shfl_xor(float2 v, int o) {
     return make_float2(__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o));
   }
+  static __device__ __forceinline__ float2 shfl(float2 v, int src) {
+    return make_float2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+  }
+  static __device__ __forceinline__ float2 neg(float2 a) { return make_float2(-a.x, -a.y); }
 };
 
 template <> struct Fld<double2> {
@@ -88,6 +94,10 @@ template <> struct Fld<double2> {
   static __device__ __forceinline__ double2 shfl_xor(double2 v, int o) {
     return make_double2(__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o));
   }
+  static __device__ __forceinline__ double2 shfl(double2 v, int src) {
+    return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+  }
+  static __device__ __forceinline__ double2 neg(double2 a) { return make_double2(-a.x, -a.y); }
 };
 
 // y <- beta * y the way the reference's scal routines do it: mode 0 leaves y

@@ -7,20 +7,23 @@
 // only waits for CTAs that started earlier -- no deadlock whatever the
 // scheduling.  A CTA
 //   1. stages its diagonal block of op(A) in shared memory (unstored triangle
-//      masked, unit diagonal applied, conjugated for op C) and reads its
-//      right-hand side;
+//      masked, unit diagonal applied, conjugated for op C), forms the
+//      reciprocals of its diagonal and scales each row by its reciprocal
+//      (negated, ready for the updates), and reads its right-hand side;
 //   2. for every earlier block k in solve order: loads its panel tile of
-//      op(A) into registers, waits for block k's ready flag (epoch-tagged,
-//      acquire load, bounded), reads x_k back from x and accumulates
-//      op(A)(b, k) x_k -- four threads per row, 16 columns each;
-//   3. solves D x_b = rhs - acc by substitution in one warp (the diagonal
-//      block is never inverted: FP64 back-substitution as the reference does,
-//      dtrlsv.rs), with the reciprocals of the diagonal formed first;
-//   4. writes x_b over b and publishes its flag (release store).
-// The flags are the handle's epoch-tagged slot array (slot 64 k for block k);
-// the last CTA resets the ticket counter and publishes the call's epoch, so
-// no reset pass is needed.  Waits give up after the handle's wait limit and
-// set the status word.
+//      op(A) into registers, then reads x_k from block k's published slots
+//      and accumulates op(A)(b, k) x_k -- four threads per row, 16 columns
+//      each;
+//   3. solves the row-scaled system by forward (backward) substitution in
+//      one warp, fully unrolled (the diagonal block is never inverted: FP64
+//      substitution as the reference does, dtrlsv.rs);
+//   4. writes x_b over b and publishes it in its slots.
+// Slots: every 32-bit word of a block's solution is published as one 64-bit
+// slot (epoch << 32) | word, so a single load delivers both the readiness of
+// that word and its value (aligned 64-bit accesses are single-copy atomic):
+// a consumer's poll is its data load.  The last CTA resets the ticket counter
+// and publishes the call's epoch, so no reset pass is needed.  Waits give up
+// after the handle's wait limit and set the status word.
 #include "common.cuh"
 #include "field.cuh"
 
@@ -32,13 +35,33 @@ namespace {
 constexpr int kTB = 64;
 constexpr int kTThr = 256;
 
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
   unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// 32-bit words per element (slots per element).
+template <typename T> constexpr int kWords = (int)(sizeof(T) / 4);
+
+// Substitution on the row-scaled diagonal block in one warp, fully unrolled:
+// lane owns rows lane and lane + 32; D holds -op(A)(i, j) / op(A)(i, i) off
+// the diagonal, v the scaled right-hand side.  At step j the owner's value
+// is x_j; it is broadcast and every later row i takes v_i += D[i][j] x_j.
+template <typename T, bool kLower>
+__device__ __forceinline__ void substitute(const T (*D)[kTB + 1], T& v0, T& v1, int lane) {
+  using F = Fld<T>;
+#pragma unroll
+  for (int s = 0; s < kTB; ++s) {
+    const int j = kLower ? s : kTB - 1 - s;
+    const T xj = F::shfl(j < 32 ? v0 : v1, j & 31);
+    const int i0 = lane, i1 = lane + 32;
+    if (kLower ? i0 > j : i0 < j) F::mac(v0, D[i0][j], xj);
+    if (kLower ? i1 > j : i1 < j) F::mac(v1, D[i1][j], xj);
+  }
 }
 __device__ __forceinline__ uint64_t gtime() {
   uint64_t t;
@@ -74,7 +97,7 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
   const int b0 = blk * kTB;
   auto opv = [](T v) { return kConj ? F::conj(v) : v; };
 
-  // ---- 1. diagonal block and right-hand side ----
+  // ---- 1. diagonal block, its reciprocals, the row scaling; right-hand side ----
   for (int e = tid; e < kTB * kTB; e += kTThr) {
     const int rr = e % kTB, cc = e / kTB;          // stored element (b0 + rr, b0 + cc)
     const int gr = b0 + rr, gc = b0 + cc;
@@ -88,8 +111,16 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
   if (tid < kTB) rv[tid] = (b0 + tid < n) ? x[(size_t)(b0 + tid) * incx] : F::zero();
   __syncthreads();
   if (tid < kTB) rdiag[tid] = F::div(F::one(), D[tid][tid]);
+  __syncthreads();
+  for (int e = tid; e < kTB * kTB; e += kTThr) {
+    const int r = e / kTB, c = e % kTB;
+    if (r != c) D[r][c] = F::neg(F::mul(D[r][c], rdiag[r]));
+  }
 
   // ---- 2. panel: acc(r) = sum over earlier blocks k of op(A)(b, k) x_k ----
+  constexpr int W = kWords<T>;
+  constexpr int kSlotWords = kTB * W;   // slots per block (<= kTThr)
+  uint32_t* xkw = reinterpret_cast<uint32_t*>(xk);
   const int r = tid >> 2, q = tid & 3;
   T acc = F::zero();
   const int npanel = lower_eff ? blk : nblk - 1 - blk;
@@ -103,12 +134,14 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
       const bool in = gr < n && gc < n;
       a[j] = in ? opv(trans ? A[gc + (size_t)gr * lda] : A[gr + (size_t)gc * lda]) : F::zero();
     }
-    if (tid == 0) {
-      const unsigned long long* sp = slots + (size_t)k * kTB;
-      if ((unsigned)(ld_acquire_u64(sp) >> 32) != epoch) {
+    if (tid < kSlotWords) {
+      const unsigned long long* sp = slots + (size_t)k * kSlotWords + tid;
+      unsigned long long w = ld_relaxed_u64(sp);
+      if ((unsigned)(w >> 32) != epoch) {
         const uint64_t t0 = gtime();
         for (unsigned spins = 1;; ++spins) {
-          if ((unsigned)(ld_acquire_u64(sp) >> 32) == epoch) break;
+          w = ld_relaxed_u64(sp);
+          if ((unsigned)(w >> 32) == epoch) break;
           const uint64_t el = gtime() - t0;
           if (el > limit_ns || ((spins & 15u) == 0 && el > 20000ull && *(volatile unsigned*)status != 0)) {
             atomicOr(status, kStatusTimeout);
@@ -117,57 +150,35 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
           }
         }
       }
+      xkw[tid] = (uint32_t)w;
     }
     __syncthreads();
     if (abort_flag) break;
-    if (tid < kTB) xk[tid] = (k0 + tid < n) ? __ldcg(x + (size_t)(k0 + tid) * incx) : F::zero();
-    __syncthreads();
 #pragma unroll
     for (int j = 0; j < 16; ++j) F::mac(acc, a[j], xk[q * 16 + j]);
     __syncthreads();
   }
   acc = F::add(acc, F::shfl_xor(acc, 1));
   acc = F::add(acc, F::shfl_xor(acc, 2));
-  if (q == 0) rv[r] = F::sub(rv[r], acc);
+  if (q == 0) rv[r] = F::mul(F::sub(rv[r], acc), rdiag[r]);
   __syncthreads();
 
-  // ---- 3. substitution on the diagonal block (one warp; lane owns rows
-  //         lane and lane + 32) ----
+  // ---- 3. substitution on the row-scaled diagonal block (one warp) ----
   if (warp == 0 && !abort_flag) {
     T v0 = rv[lane], v1 = rv[lane + 32];
-    for (int s = 0; s < kTB; ++s) {
-      const int j = lower_eff ? s : kTB - 1 - s;
-      const T src = j < 32 ? v0 : v1;
-      T xj;
-      if constexpr (F::kComplex) {
-        xj.x = __shfl_sync(0xffffffffu, src.x, j & 31);
-        xj.y = __shfl_sync(0xffffffffu, src.y, j & 31);
-      } else {
-        xj = __shfl_sync(0xffffffffu, src, j & 31);
-      }
-      xj = F::mul(xj, rdiag[j]);
-      if (lane == (j & 31)) {
-        if (j < 32) v0 = xj;
-        else v1 = xj;
-      }
-      // rows still to solve: after j in solve order
-      const int i0 = lane, i1 = lane + 32;
-      if (lower_eff ? i0 > j : i0 < j) v0 = F::sub(v0, F::mul(D[i0][j], xj));
-      if (lower_eff ? i1 > j : i1 < j) v1 = F::sub(v1, F::mul(D[i1][j], xj));
-    }
+    if (lower_eff) substitute<T, true>(D, v0, v1, lane);
+    else substitute<T, false>(D, v0, v1, lane);
     rv[lane] = v0;
     rv[lane + 32] = v1;
   }
   __syncthreads();
 
-  // ---- 4. publish ----
+  // ---- 4. publish: x_b over b, and every word of it in the block's slots ----
   if (!abort_flag) {
     if (tid < kTB && b0 + tid < n) x[(size_t)(b0 + tid) * incx] = rv[tid];
-    __syncthreads();
-    if (tid == 0) {
-      __threadfence();
-      st_release_u64(slots + (size_t)blk * kTB, (unsigned long long)epoch << 32);
-    }
+    if (tid < kSlotWords)
+      st_relaxed_u64(slots + (size_t)blk * kSlotWords + tid,
+                     ((unsigned long long)epoch << 32) | reinterpret_cast<const uint32_t*>(rv)[tid]);
   }
   // The last CTA to finish (aborted or not) resets the ticket counter and
   // publishes this call's epoch for the next call.
@@ -196,14 +207,15 @@ coral_status_t trsv_g(Handle* H, int uplo, int trans, int diag, size_t n, const 
   if (((uintptr_t)matrix | (uintptr_t)x) & (align - 1)) return bad_arg(H, 5);
   if (n > (size_t)INT32_MAX) return CORAL_ERR_NOT_SUPPORTED;
   const size_t nblk = (n + kTB - 1) / kTB;
-  if (H->trsv_slots_len < nblk * kTB) {
+  const size_t nslots = nblk * kTB * kWords<T>;   // one slot per 32-bit word of x
+  if (H->trsv_slots_len < nslots) {
     if (H->trsv_slots) {
       CORAL_CUDA(H, cudaStreamSynchronize(H->stream));
       cudaFree(H->trsv_slots);
       H->trsv_slots = nullptr;
       H->trsv_slots_len = 0;
     }
-    const size_t len = ((nblk * kTB + 65535) / 65536) * 65536;
+    const size_t len = ((nslots + 65535) / 65536) * 65536;
     CORAL_CUDA(H, cudaMalloc(&H->trsv_slots, len * sizeof(unsigned long long)));
     CORAL_CUDA(H, cudaMemsetAsync(H->trsv_slots, 0, len * sizeof(unsigned long long), H->stream));
     H->trsv_slots_len = len;
