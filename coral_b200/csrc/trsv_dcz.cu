@@ -32,8 +32,12 @@
 namespace coral {
 namespace {
 
-constexpr int kTB = 64;
-constexpr int kTThr = 256;
+// Block edge: 64 rows for every element type, four threads per block row.
+// 128-row blocks halve the serial hand-offs but double each block's
+// substitution chain; at n = 4096 they measured slower (dtrsv 253 against
+// 200 us, ctrsv 250 against 187 us), and a complex128 block of 128 rows
+// would not fit in shared memory.
+template <typename T> constexpr int kTBOf = 64;
 
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
   unsigned long long v;
@@ -48,19 +52,22 @@ __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned l
 template <typename T> constexpr int kWords = (int)(sizeof(T) / 4);
 
 // Substitution on the row-scaled diagonal block in one warp, fully unrolled:
-// lane owns rows lane and lane + 32; D holds -op(A)(i, j) / op(A)(i, i) off
-// the diagonal, v the scaled right-hand side.  At step j the owner's value
-// is x_j; it is broadcast and every later row i takes v_i += D[i][j] x_j.
-template <typename T, bool kLower>
-__device__ __forceinline__ void substitute(const T (*D)[kTB + 1], T& v0, T& v1, int lane) {
+// lane owns rows lane + 32 m (m < TB / 32); D holds -op(A)(i, j) / op(A)(i, i)
+// off the diagonal, v the scaled right-hand side.  At step j the owner's
+// value is x_j; it is broadcast and every later row i takes
+// v_i += D[i][j] x_j.
+template <typename T, int TB, bool kLower>
+__device__ __forceinline__ void substitute(const T (*D)[TB + 1], T (&v)[TB / 32], int lane) {
   using F = Fld<T>;
 #pragma unroll
-  for (int s = 0; s < kTB; ++s) {
-    const int j = kLower ? s : kTB - 1 - s;
-    const T xj = F::shfl(j < 32 ? v0 : v1, j & 31);
-    const int i0 = lane, i1 = lane + 32;
-    if (kLower ? i0 > j : i0 < j) F::mac(v0, D[i0][j], xj);
-    if (kLower ? i1 > j : i1 < j) F::mac(v1, D[i1][j], xj);
+  for (int s = 0; s < TB; ++s) {
+    const int j = kLower ? s : TB - 1 - s;
+    const T xj = F::shfl(v[j / 32], j & 31);
+#pragma unroll
+    for (int m = 0; m < TB / 32; ++m) {
+      const int i = lane + 32 * m;
+      if (kLower ? i > j : i < j) F::mac(v[m], D[i][j], xj);
+    }
   }
 }
 __device__ __forceinline__ uint64_t gtime() {
@@ -69,7 +76,7 @@ __device__ __forceinline__ uint64_t gtime() {
   return t;
 }
 
-template <typename T, bool kConj>
+template <typename T, bool kConj, int kTB = kTBOf<T>, int kTThr = 4 * kTBOf<T>>
 __global__ void __launch_bounds__(kTThr, 1)
 k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool lower_eff, bool trans,
          bool unit, unsigned long long* slots, unsigned* ticket, unsigned* done, unsigned* epoch_word,
@@ -120,6 +127,8 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
   // ---- 2. panel: acc(r) = sum over earlier blocks k of op(A)(b, k) x_k ----
   constexpr int W = kWords<T>;
   constexpr int kSlotWords = kTB * W;   // slots per block (<= kTThr)
+  constexpr int kQ = kTB / 4;           // columns per thread of a panel tile
+  static_assert(kSlotWords <= kTThr, "one slot per thread");
   uint32_t* xkw = reinterpret_cast<uint32_t*>(xk);
   const int r = tid >> 2, q = tid & 3;
   T acc = F::zero();
@@ -127,10 +136,10 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
   for (int idx = 0; idx < npanel; ++idx) {
     const int k = lower_eff ? idx : blk + 1 + idx;
     const int k0 = k * kTB;
-    T a[16];
+    T a[kQ];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int gr = b0 + r, gc = k0 + q * 16 + j;   // op(A)(gr, gc)
+    for (int j = 0; j < kQ; ++j) {
+      const int gr = b0 + r, gc = k0 + q * kQ + j;   // op(A)(gr, gc)
       const bool in = gr < n && gc < n;
       a[j] = in ? opv(trans ? A[gc + (size_t)gr * lda] : A[gr + (size_t)gc * lda]) : F::zero();
     }
@@ -155,7 +164,7 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
     __syncthreads();
     if (abort_flag) break;
 #pragma unroll
-    for (int j = 0; j < 16; ++j) F::mac(acc, a[j], xk[q * 16 + j]);
+    for (int j = 0; j < kQ; ++j) F::mac(acc, a[j], xk[q * kQ + j]);
     __syncthreads();
   }
   acc = F::add(acc, F::shfl_xor(acc, 1));
@@ -165,11 +174,13 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
 
   // ---- 3. substitution on the row-scaled diagonal block (one warp) ----
   if (warp == 0 && !abort_flag) {
-    T v0 = rv[lane], v1 = rv[lane + 32];
-    if (lower_eff) substitute<T, true>(D, v0, v1, lane);
-    else substitute<T, false>(D, v0, v1, lane);
-    rv[lane] = v0;
-    rv[lane + 32] = v1;
+    T v[kTB / 32];
+#pragma unroll
+    for (int m = 0; m < kTB / 32; ++m) v[m] = rv[lane + 32 * m];
+    if (lower_eff) substitute<T, kTB, true>(D, v, lane);
+    else substitute<T, kTB, false>(D, v, lane);
+#pragma unroll
+    for (int m = 0; m < kTB / 32; ++m) rv[lane + 32 * m] = v[m];
   }
   __syncthreads();
 
@@ -206,6 +217,7 @@ coral_status_t trsv_g(Handle* H, int uplo, int trans, int diag, size_t n, const 
   if (incx == 0) return bad_arg(H, 8);
   if (((uintptr_t)matrix | (uintptr_t)x) & (align - 1)) return bad_arg(H, 5);
   if (n > (size_t)INT32_MAX) return CORAL_ERR_NOT_SUPPORTED;
+  constexpr int kTB = kTBOf<T>, kTThr = 4 * kTBOf<T>;
   const size_t nblk = (n + kTB - 1) / kTB;
   const size_t nslots = nblk * kTB * kWords<T>;   // one slot per 32-bit word of x
   if (H->trsv_slots_len < nslots) {
