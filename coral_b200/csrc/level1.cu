@@ -81,12 +81,13 @@ __device__ bool last_block(unsigned* counter) {
   return is_last;
 }
 
-// ---- sdot / snrm2 ---------------------------------------------------------
-// Each product of two fp32 values is exact in fp64, and an fp64 sum of fp32
-// squares can neither overflow nor underflow, so one fp64 accumulation gives
-// snrm2 the overflow safety that the reference obtains with its running
-// (scale, ssq) pair (nrm2_helpers.rs:15-38) in a single pass.
-template <bool kSquare, bool kVec>
+// ---- sdot --------------------------------------------------------------------
+// Each product of two fp32 values is exact in fp64; the sum is accumulated in
+// fp64.  (snrm2 runs on the streaming reduction of level1_dcz.cu: an fp64 sum
+// of fp32 squares can neither overflow nor underflow, which gives it the
+// overflow safety of the reference's running (scale, ssq) pair,
+// nrm2_helpers.rs:15-38, in a single pass.)
+template <bool kVec>
 __global__ void __launch_bounds__(kRedThreads)
 k_dot(size_t n, const float* __restrict__ x, size_t incx, const float* __restrict__ y,
       size_t incy, double* partials, unsigned* counter, float* out) {
@@ -98,42 +99,31 @@ k_dot(size_t n, const float* __restrict__ x, size_t incx, const float* __restric
     const size_t n4 = n >> 2;
     const float4* x4 = reinterpret_cast<const float4*>(x);
     const float4* y4 = reinterpret_cast<const float4*>(y);
-    // 8 independent 128-bit loads in flight per thread: 4 per operand for
-    // sdot, 8 of x for snrm2 (one stream needs the deeper unroll to keep as
-    // many bytes in flight)
-    constexpr int U = kSquare ? 8 : 4;
+    // 8 independent 128-bit loads in flight per thread, 4 per operand
+    constexpr int U = 4;
     size_t i = tid;
     double acc1 = 0.0;
     for (; i + (U - 1) * stride < n4; i += U * stride) {
       float4 a[U], b[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) a[u] = __ldcs(x4 + i + u * stride);
-      if (!kSquare) {
 #pragma unroll
-        for (int u = 0; u < U; ++u) b[u] = __ldcs(y4 + i + u * stride);
-      }
+      for (int u = 0; u < U; ++u) b[u] = __ldcs(y4 + i + u * stride);
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const float4 c = kSquare ? a[u] : b[u];
         double& t = (u & 1) ? acc1 : acc;
-        t += (double)a[u].x * c.x + (double)a[u].y * c.y + (double)a[u].z * c.z + (double)a[u].w * c.w;
+        t += (double)a[u].x * b[u].x + (double)a[u].y * b[u].y + (double)a[u].z * b[u].z +
+             (double)a[u].w * b[u].w;
       }
     }
     for (; i < n4; i += stride) {
-      float4 a = __ldcs(x4 + i);
-      float4 b = kSquare ? a : __ldcs(y4 + i);
+      const float4 a = __ldcs(x4 + i), b = __ldcs(y4 + i);
       acc += (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
     }
     acc += acc1;
-    for (size_t t = (n4 << 2) + tid; t < n; t += stride) {
-      float a = x[t], b = kSquare ? a : y[t];
-      acc += (double)a * b;
-    }
+    for (size_t t = (n4 << 2) + tid; t < n; t += stride) acc += (double)x[t] * y[t];
   } else {
-    for (size_t t = tid; t < n; t += stride) {
-      float a = x[t * incx], b = kSquare ? a : y[t * incy];
-      acc += (double)a * b;
-    }
+    for (size_t t = tid; t < n; t += stride) acc += (double)x[t * incx] * y[t * incy];
   }
   double bs = block_sum(acc, sh);
   if (threadIdx.x == 0) partials[blockIdx.x] = bs;
@@ -142,7 +132,7 @@ k_dot(size_t n, const float* __restrict__ x, size_t incx, const float* __restric
   for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) s += __ldcg(partials + b);
   s = block_sum(s, sh);
   if (threadIdx.x == 0) {
-    *out = kSquare ? (float)sqrt(s) : (float)s;
+    *out = (float)s;
     *counter = 0;
   }
 }
@@ -329,33 +319,9 @@ coral_status_t coral_sdot(coral_handle_t hh, size_t n, const float* x, size_t in
   double* part = static_cast<double*>(scratch(H, g * sizeof(double)));
   if (!part) return CORAL_ERR_ALLOC;
   if (vec)
-    k_dot<false, true><<<g, kRedThreads, 0, H->stream>>>(n, x, 1, y, 1, part, &w->counters[kCtrDot], dres);
+    k_dot<true><<<g, kRedThreads, 0, H->stream>>>(n, x, 1, y, 1, part, &w->counters[kCtrDot], dres);
   else
-    k_dot<false, false><<<g, kRedThreads, 0, H->stream>>>(n, x, incx, y, incy, part, &w->counters[kCtrDot], dres);
-  coral_status_t s = launch_status(H);
-  if (s != CORAL_OK) return s;
-  return deliver_result(H, result, dres, sizeof(float));
-}
-
-coral_status_t coral_snrm2(coral_handle_t hh, size_t n, const float* x, size_t incx,
-                           float* result) {
-  CORAL_HANDLE(hh);
-  if (!result) return bad_arg(H, 4);
-  DeviceWords* w = H->words;
-  float* dres = reinterpret_cast<float*>(&w->dresult[1]);
-  if (n == 0 || incx == 0) {  // snrm2.rs:53-55
-    CORAL_CUDA(H, cudaMemsetAsync(dres, 0, sizeof(float), H->stream));
-    return deliver_result(H, result, dres, sizeof(float));
-  }
-  if (!x) return bad_arg(H, 2);
-  bool vec = incx == 1 && aligned16(x);
-  unsigned g = stream_grid(n, (size_t)kRedThreads * 8, H->sm_count, 4);
-  double* part = static_cast<double*>(scratch(H, g * sizeof(double)));
-  if (!part) return CORAL_ERR_ALLOC;
-  if (vec)
-    k_dot<true, true><<<g, kRedThreads, 0, H->stream>>>(n, x, 1, x, 1, part, &w->counters[kCtrNrm2], dres);
-  else
-    k_dot<true, false><<<g, kRedThreads, 0, H->stream>>>(n, x, incx, x, incx, part, &w->counters[kCtrNrm2], dres);
+    k_dot<false><<<g, kRedThreads, 0, H->stream>>>(n, x, incx, y, incy, part, &w->counters[kCtrDot], dres);
   coral_status_t s = launch_status(H);
   if (s != CORAL_OK) return s;
   return deliver_result(H, result, dres, sizeof(float));

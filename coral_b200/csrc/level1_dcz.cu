@@ -304,10 +304,15 @@ k_nrm2_x(size_t n, const T* __restrict__ x, size_t incx, double* part, unsigned*
   __shared__ double sh[32];
   double s = 0.0, m = 0.0;
   visit<T, kUnit>(n, x, incx, nullptr, 0, [&](T u, T, size_t) {
-    const double r = re_of(u), im = im_of(u);
+    const double r = re_of(u);
     s = fma(r, r, s);
-    s = fma(im, im, s);
-    m = fmax(m, fmax(fabs(r), fabs(im)));
+    if constexpr (IsCx<T>::v) {
+      const double im = im_of(u);
+      s = fma(im, im, s);
+      if constexpr (sizeof(R) == 8) m = fmax(m, fmax(fabs(r), fabs(im)));
+    } else if constexpr (sizeof(R) == 8) {
+      m = fmax(m, fabs(r));
+    }
   });
   const double bs = bsum(s, sh), bm = bmax(m, sh);
   if (threadIdx.x == 0) {
@@ -344,9 +349,12 @@ k_nrm2_scaled(size_t n, const T* __restrict__ x, size_t incx, double* part, unsi
   const double inv = 1.0 / *dmx;
   double s = 0.0;
   visit<T, kUnit>(n, x, incx, nullptr, 0, [&](T u, T, size_t) {
-    const double r = re_of(u) * inv, im = im_of(u) * inv;
+    const double r = re_of(u) * inv;
     s = fma(r, r, s);
-    s = fma(im, im, s);
+    if constexpr (IsCx<T>::v) {
+      const double im = im_of(u) * inv;
+      s = fma(im, im, s);
+    }
   });
   const double bs = bsum(s, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = bs;
@@ -1008,6 +1016,11 @@ coral_status_t coral_scnrm2(coral_handle_t h, size_t n, const float* x, size_t i
 }
 coral_status_t coral_dznrm2(coral_handle_t h, size_t n, const double* x, size_t incx, double* result) {
   return nrm2_entry<double2, double>(h, n, x, incx, result, 16);
+}
+// snrm2.rs:45-149: the fp32 norm on the same streaming reduction (fp64 sum
+// of squares of the fp32 values, which cannot overflow, then sqrt).
+coral_status_t coral_snrm2(coral_handle_t h, size_t n, const float* x, size_t incx, float* result) {
+  return nrm2_entry<float, float>(h, n, x, incx, result, 4);
 }
 
 // ---- i?amax ----
