@@ -376,8 +376,9 @@ def level12_bandwidth(torch, cb, lib, h, dev, g, routines=None):
     diag = n + U[0,1], CHEMV upper 4096, SDOT/SAXPY/ISAMAX/SNRM2 at 2^26).
     Each routine is captured in a CUDA graph and timed by replay, so host
     launch gaps are not in the figure.  Operands that fit in L2 (STRSV, CHEMV)
-    are timed one replay of one call at a time with L2 flushed (256 MiB
-    written) before each; the others as one replay of 20 calls."""
+    are timed with L2 flushed (256 MiB written) before every call: a graph of
+    10 x [flush, call] against a graph of 10 x [flush], the difference per
+    call, three times; the others as one replay of 20 calls."""
     import ctypes
     vp = ctypes.c_void_p
     stream = torch.cuda.current_stream()
@@ -415,19 +416,25 @@ def level12_bandwidth(torch, cb, lib, h, dev, g, routines=None):
             torch.cuda.synchronize()
             del cg
             return e0.elapsed_time(e1) / iters
-        cg = capture(fn, 1)
-        cg.replay()
-        torch.cuda.synchronize()
-        for _ in range(iters):
-            flush_buf.fill_(1.0)
+        # cold L2 for every call: one graph of `iters` x [flush, call] and one
+        # of `iters` x [flush]; the call's time is the difference per call, so
+        # the host-side submission of a graph stays out of the figure
+        both = capture(lambda: (flush_buf.fill_(1.0), fn()), iters)
+        only = capture(lambda: flush_buf.fill_(1.0), iters)
+
+        def replay_ms(cg):
+            cg.replay()
+            torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             cg.replay()
             e1.record(stream)
             torch.cuda.synchronize()
-            total += e0.elapsed_time(e1)
-        del cg
-        return total / iters
+            return e0.elapsed_time(e1)
+        for _ in range(3):
+            total += replay_ms(both) - replay_ms(only)
+        del both, only
+        return total / (3 * iters)
 
     hbm = peaks()[0]
     out = {}
