@@ -319,6 +319,9 @@ k_nrm2_x(size_t n, const T* __restrict__ x, size_t incx, double* part, unsigned*
     part[2 * blockIdx.x] = bs;
     part[2 * blockIdx.x + 1] = bm;
   }
+  // the rescaling pass (a programmatic dependent) may start launching; it
+  // waits for this whole grid before it reads anything
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if (!last_block_l1(counter)) return;
   double ts = 0.0, tm = 0.0;
   for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
@@ -345,6 +348,7 @@ __global__ void __launch_bounds__(kL1)
 k_nrm2_scaled(size_t n, const T* __restrict__ x, size_t incx, double* part, unsigned* counter,
               unsigned* flag, const double* dmx, R* out) {
   __shared__ double sh[32];
+  asm volatile("griddepcontrol.wait;" ::: "memory");   // pass 1 complete and visible
   if (*(volatile unsigned*)flag == 0u) return;   // every block sees the same word
   const double inv = 1.0 / *dmx;
   double s = 0.0;
@@ -687,6 +691,24 @@ void l1_launch(Handle* h, size_t n, void (*kernel)(P...), A&&... args) {
   kernel<<<g, kL1, 0, h->stream>>>(std::forward<A>(args)...);
 }
 
+// The same as a programmatic dependent of the previous kernel on the stream:
+// its blocks are scheduled as that grid drains and must wait for it with
+// griddepcontrol.wait before reading its results.
+template <typename... P, typename... A>
+cudaError_t l1_launch_dependent(Handle* h, size_t n, void (*kernel)(P...), A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(stream_grid(n, (size_t)kL1 * 8, h->sm_count, resident_blocks((const void*)kernel)));
+  cfg.blockDim = dim3(kL1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
+
 template <typename Out>
 coral_status_t finish(Handle* H, Out* result, const void* dres, size_t bytes) {
   coral_status_t s = launch_status(H);
@@ -783,10 +805,13 @@ coral_status_t nrm2_entry(coral_handle_t hh, size_t n, const void* x, size_t inc
   coral_status_t s = launch_status(H);
   if (s != CORAL_OK) return s;
   if (sizeof(R) == 8) {   // fp64 data: rescaling pass (returns at once unless asked)
+    const double* cmx = dmx;
     if (unit)
-      l1_launch(H, n, k_nrm2_scaled<T, R, true>, n, xx, 1, part, ctr, flag, dmx, dres);
+      CORAL_CUDA(H, l1_launch_dependent(H, n, k_nrm2_scaled<T, R, true>, n, xx, (size_t)1, part, ctr, flag, cmx,
+                                        dres));
     else
-      l1_launch(H, n, k_nrm2_scaled<T, R, false>, n, xx, incx, part, ctr, flag, dmx, dres);
+      CORAL_CUDA(H, l1_launch_dependent(H, n, k_nrm2_scaled<T, R, false>, n, xx, incx, part, ctr, flag, cmx,
+                                        dres));
   }
   return finish(H, result, dres, sizeof(R));
 }
