@@ -665,6 +665,12 @@ def run_ours(args, world, rank, local):
             step(mode)
         torch.cuda.synchronize()
         return
+    if args.only_precision:  # profiling case: the precision-GEMM set alone
+        del A, B, C0, C
+        torch.cuda.empty_cache()
+        if rank == 0:
+            print(json.dumps({"precision_gemm": precision_set(torch, cb, h, dev, g)}))
+        return
     if args.only_level12:  # profiling case: the level-1/2 set alone
         del A, B, C0, C
         torch.cuda.empty_cache()
@@ -807,6 +813,7 @@ def main():
     ap.add_argument("--size", type=int, default=0, help="m = n = k (profiling cases; default 8192)")
     ap.add_argument("--only-gemm", action="store_true", help="run warmup+steps GEMMs, print nothing")
     ap.add_argument("--only-level12", action="store_true", help="run and print the level-1/2 set only")
+    ap.add_argument("--only-precision", action="store_true", help="run and print the precision-GEMM set only")
     ap.add_argument("--routines", default="", help="with --only-level12: comma list of routines to time")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
