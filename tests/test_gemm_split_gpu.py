@@ -46,6 +46,23 @@ def test_sgemm_split_random(cuda, mode, tol, shape, ops):
         gemm_case(cb.sgemm, np.float32, *ops, m, n, k, alpha, beta, tol, sample=sample)
 
 
+# Shapes whose dimensions share a residue mod 4, with the pad that makes every
+# leading dimension a multiple of 4: the split pre-pass then takes its
+# 16-byte kernels (k_split_rows / k_split_cols) with ragged M/N and K edges
+# (K not a multiple of 8, M/N not multiples of 4 or 64).
+ALIGNED_RAGGED = [((127, 131, 63), 1), ((301, 77, 513), 3), ((66, 70, 10), 2), ((1000, 8, 12), 4)]
+
+
+@pytest.mark.parametrize("mode,tol", MODES)
+@pytest.mark.parametrize("shape,pad", ALIGNED_RAGGED)
+@pytest.mark.parametrize("ops", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_sgemm_split_vector_prepass_edges(cuda, mode, tol, shape, pad, ops):
+    cb.set_gemm_mode(mode)
+    m, n, k = shape
+    assert all((d + pad) % 4 == 0 for d in shape)
+    gemm_case(cb.sgemm, np.float32, *ops, m, n, k, 1.25, 0.5, tol, pad=pad)
+
+
 @pytest.mark.parametrize("mode,tol", MODES)
 @pytest.mark.parametrize("shape", [(1, 1, 1), (5, 7, 4), (127, 129, 65), (64, 200, 301)])
 @pytest.mark.parametrize("ops", [(a, b) for a in (0, 1, 2) for b in (0, 1, 2)])
