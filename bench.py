@@ -373,7 +373,9 @@ def batched_set(torch, cb, dev):
 def level12_bandwidth(torch, cb, lib, h, dev, g, routines=None):
     """GB/s of algorithmic traffic for the level-1/2 bandwidth configuration
     (SGEMV N/T 8192^2, SSYMV upper 8192, STRSV lower non-unit 4096 with
-    diag = n + U[0,1], CHEMV upper 4096, SDOT/SAXPY/ISAMAX/SNRM2 at 2^26).
+    diag = n + U[0,1], CHEMV upper 4096, SDOT/SAXPY/ISAMAX/SNRM2 at 2^26),
+    the rest of level 1 at 2^26, the d/c/z GEMV/SYMV/HEMV/TRSV, and the rank
+    updates (GER, SYR, SYR2, HER, HER2) at n = 8192.
     Each routine is captured in a CUDA graph and timed by replay, so host
     launch gaps are not in the figure.  Operands that fit in L2 (STRSV, CHEMV)
     are timed with L2 flushed (256 MiB written) before every call: a graph of
@@ -492,6 +494,10 @@ def level12_bandwidth(torch, cb, lib, h, dev, g, routines=None):
         ("zcopy", "z", 2, lambda X, Y: cb.zcopy(n2, X, 1, Y, 1)),
         ("dswap", "d", 4, lambda X, Y: cb.dswap(n2, X, 1, Y, 1)),
         ("zswap", "z", 4, lambda X, Y: cb.zswap(n2, X, 1, Y, 1)),
+        ("sasum", "s", 1, lambda X, Y: lib.coral_sasum(h.h, n2, P(X), 1, rq)),
+        ("sscal", "s", 2, lambda X, Y: cb.sscal(n2, 0.999, X, 1)),
+        ("scopy", "s", 2, lambda X, Y: cb.scopy(n2, X, 1, Y, 1)),
+        ("sswap", "s", 4, lambda X, Y: cb.sswap(n2, X, 1, Y, 1)),
         ("srot", "s", 4, lambda X, Y: cb.srot(n2, X, 1, Y, 1, 0.6, 0.8)),
         ("drot", "d", 4, lambda X, Y: cb.drot(n2, X, 1, Y, 1, 0.6, 0.8)),
         ("zdrot", "z", 4, lambda X, Y: cb.zdrot(n2, X, 1, Y, 1, 0.6, 0.8)),
@@ -605,6 +611,55 @@ def level12_bandwidth(torch, cb, lib, h, dev, g, routines=None):
     if want("chemv_upper"):
         rec("chemv_upper", 8 * (nc * (nc + 1) // 2 + 3 * nc),
             timed_calls(lambda: cb.chemv(0, nc, 1.5 - 0.5j, Hm, nc, xc, 1, 0.25 + 0.0j, yc, 1), 10, True))
+    del Hm, xc, yc
+    # Rank updates at n = 8192 (the matrix, or its stored triangle, is read and
+    # written once; x and y are read once). alpha is small so that repeated
+    # in-place updates stay in range.
+    nr = 8192
+    tri = nr * (nr + 1) // 2
+    rank_specs = [
+        # (name, dtype, bytes, call(A, x, y))
+        ("sger", torch.float32, 4 * (2 * nr * nr + 2 * nr),
+         lambda A_, x_, y_: cb.sger(nr, nr, 1e-3, x_, 1, y_, 1, A_, nr)),
+        ("ssyr_upper", torch.float32, 4 * (2 * tri + nr),
+         lambda A_, x_, y_: cb.ssyr(0, nr, 1e-3, x_, 1, A_, nr)),
+        ("ssyr2_upper", torch.float32, 4 * (2 * tri + 2 * nr),
+         lambda A_, x_, y_: cb.ssyr2(0, nr, 1e-3, x_, 1, y_, 1, A_, nr)),
+        ("dger", torch.float64, 8 * (2 * nr * nr + 2 * nr),
+         lambda A_, x_, y_: cb.dger(nr, nr, 1e-3, x_, 1, y_, 1, A_, nr)),
+        ("dsyr_upper", torch.float64, 8 * (2 * tri + nr),
+         lambda A_, x_, y_: cb.dsyr(0, nr, 1e-3, x_, 1, A_, nr)),
+        ("dsyr2_upper", torch.float64, 8 * (2 * tri + 2 * nr),
+         lambda A_, x_, y_: cb.dsyr2(0, nr, 1e-3, x_, 1, y_, 1, A_, nr)),
+        ("cgeru", torch.complex64, 8 * (2 * nr * nr + 2 * nr),
+         lambda A_, x_, y_: cb.cgeru(nr, nr, 1e-3 - 1e-3j, x_, 1, y_, 1, A_, nr)),
+        ("cgerc", torch.complex64, 8 * (2 * nr * nr + 2 * nr),
+         lambda A_, x_, y_: cb.cgerc(nr, nr, 1e-3 - 1e-3j, x_, 1, y_, 1, A_, nr)),
+        ("cher_upper", torch.complex64, 8 * (2 * tri + nr),
+         lambda A_, x_, y_: cb.cher(0, nr, 1e-3, x_, 1, A_, nr)),
+        ("cher2_upper", torch.complex64, 8 * (2 * tri + 2 * nr),
+         lambda A_, x_, y_: cb.cher2(0, nr, 1e-3 - 1e-3j, x_, 1, y_, 1, A_, nr)),
+        ("zgeru", torch.complex128, 16 * (2 * nr * nr + 2 * nr),
+         lambda A_, x_, y_: cb.zgeru(nr, nr, 1e-3 - 1e-3j, x_, 1, y_, 1, A_, nr)),
+        ("zgerc", torch.complex128, 16 * (2 * nr * nr + 2 * nr),
+         lambda A_, x_, y_: cb.zgerc(nr, nr, 1e-3 - 1e-3j, x_, 1, y_, 1, A_, nr)),
+        ("zher_upper", torch.complex128, 16 * (2 * tri + nr),
+         lambda A_, x_, y_: cb.zher(0, nr, 1e-3, x_, 1, A_, nr)),
+        ("zher2_upper", torch.complex128, 16 * (2 * tri + 2 * nr),
+         lambda A_, x_, y_: cb.zher2(0, nr, 1e-3 - 1e-3j, x_, 1, y_, 1, A_, nr)),
+    ]
+    for dt in (torch.float32, torch.float64, torch.complex64, torch.complex128):
+        specs = [s for s in rank_specs if s[1] == dt and want(s[0])]
+        if not specs:
+            continue
+        Ar = torch.empty(nr * nr, dtype=dt, device=dev)
+        xr = torch.empty(nr, dtype=dt, device=dev)
+        yr = torch.empty(nr, dtype=dt, device=dev)
+        for t in (Ar, xr, yr):
+            (torch.view_as_real(t) if dt.is_complex else t).uniform_(-1, 1, generator=g)
+        for name, _, nbytes, call in specs:
+            rec(name, nbytes, timed_calls(lambda call=call: call(Ar, xr, yr), 20, False))
+        del Ar, xr, yr
     del flush_buf
     return out
 
@@ -670,6 +725,12 @@ def run_ours(args, world, rank, local):
         torch.cuda.empty_cache()
         if rank == 0:
             print(json.dumps({"precision_gemm": precision_set(torch, cb, h, dev, g)}))
+        return
+    if args.only_batched:  # profiling case: the batched set alone
+        del A, B, C0, C
+        torch.cuda.empty_cache()
+        if rank == 0:
+            print(json.dumps({"batched": batched_set(torch, cb, dev)}))
         return
     if args.only_level12:  # profiling case: the level-1/2 set alone
         del A, B, C0, C
@@ -814,6 +875,7 @@ def main():
     ap.add_argument("--only-gemm", action="store_true", help="run warmup+steps GEMMs, print nothing")
     ap.add_argument("--only-level12", action="store_true", help="run and print the level-1/2 set only")
     ap.add_argument("--only-precision", action="store_true", help="run and print the precision-GEMM set only")
+    ap.add_argument("--only-batched", action="store_true", help="run and print the batched set only")
     ap.add_argument("--routines", default="", help="with --only-level12: comma list of routines to time")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -81,11 +81,130 @@ k_rank(int m, int n, float alpha, const float* __restrict__ x, size_t incx,
   }
 }
 
+// Vector form of the unit-stride path, for A, x (and y for SSYR2) on 16-byte
+// boundaries with lda % 4 == 0. A thread owns 4 consecutive rows: it loads
+// their x (and y) once and updates them in kVCols columns. All of those
+// columns' A vectors are loaded, together with the columns' coefficients,
+// before the first is written back, so 16 * kVCols bytes of A are in flight
+// per thread instead of 4. A column whose coefficient is zero is loaded but
+// not written, so it is left untouched as before. Each element gets exactly
+// the roundings of k_rank's unit path. A vector that straddles the edge of a
+// column's triangle, or the last row, is read and written element by
+// element, in-range elements only.
+constexpr int kVCols = 8;
+
+template <int kKind>
+__global__ void __launch_bounds__(kRankThreads, 3)
+k_rank_vec(int m, int n, float alpha, const float* __restrict__ x, const float* __restrict__ y,
+           float* __restrict__ A, size_t lda, bool lower) {
+  const int rows = kKind == kGer ? m : n;
+  // rows [lo, hi) of column j that the update touches
+  auto range = [&](int j, int& lo, int& hi) {
+    lo = kKind == kGer ? 0 : (lower ? j : 0);
+    hi = kKind == kGer ? m : (lower ? n : j + 1);
+  };
+  // rows i0 .. i0+3 of columns jg .. jg+kVCols-1
+  auto block = [&](int i0, int jg) {
+    const bool full_rows = i0 + 4 <= rows;
+    float xv[4], yv[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      xv[e] = full_rows || i0 + e < rows ? x[i0 + e] : 0.0f;
+      yv[e] = kKind == kSyr2 && (full_rows || i0 + e < rows) ? y[i0 + e] : 0.0f;
+    }
+    float4 a[kVCols];
+    float c1[kVCols], c2[kVCols];
+    unsigned on_mask = 0, whole_mask = 0;
+#pragma unroll
+    for (int c = 0; c < kVCols; ++c) {
+      const int j = jg + c;
+      int l, h;
+      range(j, l, h);
+      const bool on = j < n && i0 < h && i0 + 4 > l;
+      const bool whole = on && i0 >= l && i0 + 4 <= h;
+      on_mask |= on ? 1u << c : 0u;
+      whole_mask |= whole ? 1u << c : 0u;
+      c1[c] = c2[c] = 0.0f;
+      if (on) {
+        if (kKind == kGer) c1[c] = __fmul_rn(alpha, y[j]);
+        if (kKind == kSyr) c1[c] = __fmul_rn(alpha, x[j]);
+        if (kKind == kSyr2) {
+          c1[c] = __fmul_rn(alpha, y[j]);  // coefficient of x
+          c2[c] = __fmul_rn(alpha, x[j]);  // coefficient of y
+        }
+      }
+      const float* col = A + (size_t)(on ? j : 0) * lda + i0;
+      if (whole) {
+        a[c] = *reinterpret_cast<const float4*>(col);
+      } else {
+        a[c].x = on && i0 >= l && i0 < h ? col[0] : 0.0f;
+        a[c].y = on && i0 + 1 >= l && i0 + 1 < h ? col[1] : 0.0f;
+        a[c].z = on && i0 + 2 >= l && i0 + 2 < h ? col[2] : 0.0f;
+        a[c].w = on && i0 + 3 >= l && i0 + 3 < h ? col[3] : 0.0f;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < kVCols; ++c) {
+      if (!(on_mask & (1u << c))) continue;
+      if (c1[c] == 0.0f && c2[c] == 0.0f) continue;  // column left untouched
+      const int j = jg + c;
+      int l, h;
+      range(j, l, h);
+      const int len = h - l, nfused = len - (len & 7);
+      float* av = &a[c].x;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const bool fused = (i0 + e - l) < nfused;
+        float v = av[e];
+        if (c1[c] != 0.0f) v = axpy_elem(v, c1[c], xv[e], fused);
+        if (kKind == kSyr2 && c2[c] != 0.0f) v = axpy_elem(v, c2[c], yv[e], fused);
+        av[e] = v;
+      }
+      float* col = A + (size_t)j * lda + i0;
+      if (whole_mask & (1u << c)) {
+        *reinterpret_cast<float4*>(col) = a[c];
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (i0 + e >= l && i0 + e < h) col[e] = av[e];
+      }
+    }
+  };
+  if (kKind == kGer) {
+    // grid: x = 1024-row chunks, y = column groups
+    const int i0 = (blockIdx.x * kRankThreads + threadIdx.x) * 4;
+    if (i0 >= rows) return;
+    for (int jg = blockIdx.y * kVCols; jg < n; jg += gridDim.y * kVCols) block(i0, jg);
+  } else {
+    // grid: x = column groups, each walking only the row chunks its
+    // triangle columns touch; upper takes the longest groups first
+    const int ngroups = (n + kVCols - 1) / kVCols;
+    for (int gi = blockIdx.x; gi < ngroups; gi += gridDim.x) {
+      const int jg = (lower ? gi : ngroups - 1 - gi) * kVCols;
+      const int jl = min(n, jg + kVCols) - 1;
+      const int r_lo = lower ? jg : 0, r_hi = lower ? n : jl + 1;
+      for (int rb = r_lo / (4 * kRankThreads); rb * 4 * kRankThreads < r_hi; ++rb) {
+        const int i0 = (rb * kRankThreads + threadIdx.x) * 4;
+        if (i0 < r_hi && i0 + 4 > r_lo) block(i0, jg);
+      }
+    }
+  }
+}
+
 template <int kKind>
 coral_status_t launch_rank(Handle* h, size_t m, size_t n, float alpha, const float* x, size_t incx,
                            const float* y, size_t incy, float* A, size_t lda, bool lower, bool unit) {
   if (m > INT32_MAX || n > INT32_MAX) return CORAL_ERR_NOT_SUPPORTED;
   const size_t rows = kKind == kGer ? m : n;
+  if (unit && aligned16(A) && lda % 4 == 0 && aligned16(x) && (kKind != kSyr2 || aligned16(y))) {
+    const size_t groups = (n + kVCols - 1) / kVCols;
+    const dim3 vgrid = kKind == kGer
+        ? dim3((unsigned)((rows + 4 * kRankThreads - 1) / (4 * kRankThreads)),
+               (unsigned)(groups < 65535 ? groups : 65535))
+        : dim3((unsigned)(groups < (1u << 30) ? groups : (1u << 30)));
+    k_rank_vec<kKind><<<vgrid, kRankThreads, 0, h->stream>>>((int)m, (int)n, alpha, x, y, A, lda, lower);
+    return launch_status(h);
+  }
   dim3 grid((unsigned)((rows + kRowsPerBlock - 1) / kRowsPerBlock),
             (unsigned)(n < 65535 ? n : 65535));
   k_rank<kKind><<<grid, kRankThreads, 0, h->stream>>>((int)m, (int)n, alpha, x, incx, y, incy, A,

@@ -94,7 +94,8 @@ def test_sgemv_bad_args(cuda):
     assert e.value.bad_arg == 1
 
 
-@pytest.mark.parametrize("m,n,lda", [(1, 1, 1), (7, 9, 8), (37, 29, 40), (1000, 300, 1001), (2048, 2048, 2048)])
+@pytest.mark.parametrize("m,n,lda", [(1, 1, 1), (7, 9, 8), (37, 29, 40), (1000, 300, 1001), (2048, 2048, 2048),
+                                     (1001, 77, 1004)])
 @pytest.mark.parametrize("incs", [(1, 1), (2, 3)])
 def test_sger_bit_exact(cuda, m, n, lda, incs):
     incx, incy = incs
@@ -107,7 +108,7 @@ def test_sger_bit_exact(cuda, m, n, lda, incs):
     np.testing.assert_array_equal(host(A), oracle.sger(m, n, 0.75, x, incx, y, incy, a, lda))
 
 
-@pytest.mark.parametrize("n,lda", [(1, 1), (9, 9), (37, 41), (1000, 1000)])
+@pytest.mark.parametrize("n,lda", [(1, 1), (9, 9), (37, 41), (1000, 1000), (37, 40), (1001, 1004)])
 @pytest.mark.parametrize("uplo", [0, 1])
 @pytest.mark.parametrize("inc", [1, 2])
 def test_ssyr_ssyr2_bit_exact(cuda, n, lda, uplo, inc):

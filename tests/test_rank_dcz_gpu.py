@@ -40,7 +40,8 @@ def check(got, want, a0, terms, kind):
 
 
 @pytest.mark.parametrize("kind,conj", [("d", 0), ("c", 0), ("c", 1), ("z", 0), ("z", 1)])
-@pytest.mark.parametrize("m,n,lda,inc", [(1, 1, 1, 1), (300, 211, 305, 1), (1500, 1100, 1500, 1), (257, 129, 260, 3)])
+@pytest.mark.parametrize("m,n,lda,inc", [(1, 1, 1, 1), (300, 211, 305, 1), (1500, 1100, 1500, 1), (257, 129, 260, 3),
+                                          (301, 211, 304, 1), (33, 17, 36, 1)])
 def test_ger(cuda, kind, conj, m, n, lda, inc):
     rng = np.random.default_rng(m + n + conj)
     a = rnd(rng, (n, lda), kind)
@@ -66,7 +67,8 @@ def test_ger(cuda, kind, conj, m, n, lda, inc):
 
 @pytest.mark.parametrize("kind,two", [("d", 0), ("d", 1), ("c", 0), ("c", 1), ("z", 0), ("z", 1)])
 @pytest.mark.parametrize("uplo", [0, 1])
-@pytest.mark.parametrize("n,lda,inc", [(1, 1, 1), (7, 9, 1), (300, 300, 1), (1030, 1035, 1), (129, 130, 2)])
+@pytest.mark.parametrize("n,lda,inc", [(1, 1, 1), (7, 9, 1), (300, 300, 1), (1030, 1035, 1), (129, 130, 2),
+                                       (1031, 1032, 1), (13, 16, 1)])
 def test_syr_her(cuda, kind, two, uplo, n, lda, inc):
     rng = np.random.default_rng(n * 3 + uplo + 7 * two)
     a = rnd(rng, (n, lda), kind)
