@@ -94,13 +94,34 @@ __global__ void k_mlp_gemm(int M, int N, int K, const float* __restrict__ A, int
   }
 }
 
-// out[c] = sum_r X[r][c] (column sums, fixed order per column).
-__global__ void k_col_sum(int R, int Cn, const float* __restrict__ X, float* __restrict__ out) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= Cn) return;
+// out[c] = sum_r X[r][c] (column sums). A block takes 32 columns (lane =
+// column, so a warp reads 128 contiguous bytes of a row); warp w sums rows
+// w, w + 32, ... with 8 loads in flight, and the 32 warp sums are added in
+// warp order. The order is fixed, so the result is deterministic.
+constexpr int kColSumWarps = 32;
+__global__ void __launch_bounds__(32 * kColSumWarps)
+k_col_sum(int R, int Cn, const float* __restrict__ X, float* __restrict__ out) {
+  __shared__ float part[kColSumWarps][33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int c = blockIdx.x * 32 + lane;
   float s = 0.f;
-  for (int r = 0; r < R; ++r) s += X[(size_t)r * Cn + c];
-  out[c] = s;
+  if (c < Cn) {
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int r = w;
+    for (; r + 7 * kColSumWarps < R; r += 8 * kColSumWarps) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc[u] += X[(size_t)(r + u * kColSumWarps) * Cn + c];
+    }
+    for (; r < R; r += kColSumWarps) acc[0] += X[(size_t)r * Cn + c];
+    s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+  }
+  part[w][lane] = s;
+  __syncthreads();
+  if (w != 0 || c >= Cn) return;
+  float t = 0.f;
+#pragma unroll 8
+  for (int k = 0; k < kColSumWarps; ++k) t += part[k][lane];
+  out[c] = t;
 }
 
 // dY = 2 (y - t) / (batch * out); loss partial sums via a single-block reduction.
@@ -211,7 +232,7 @@ coral_status_t backward(Mlp* n, const float* x, const float* t, int batch) {
   float* gb3 = const_cast<float*>(g.b3);
   // layer 3: dW3 = dY^T A2, db3 = colsum(dY), dA2 = dY W3
   if ((s = gemm(n, n->out, n->hid, batch, dY, 1, A2, 0, gW3, 0.f, nullptr, 0)) != CORAL_OK) return s;
-  k_col_sum<<<(n->out + 127) / 128, 128, 0, n->h->stream>>>(batch, n->out, dY, gb3);
+  k_col_sum<<<(n->out + 31) / 32, 32 * kColSumWarps, 0, n->h->stream>>>(batch, n->out, dY, gb3);
   if ((s = launch_status(n->h)) != CORAL_OK) return s;
   if ((s = gemm(n, batch, n->hid, n->out, dY, 0, w.W3, 0, dA2, 0.f, nullptr, 0)) != CORAL_OK) return s;
   const size_t bh = (size_t)batch * n->hid;
@@ -220,14 +241,14 @@ coral_status_t backward(Mlp* n, const float* x, const float* t, int batch) {
   if ((s = launch_status(n->h)) != CORAL_OK) return s;
   // layer 2
   if ((s = gemm(n, n->hid, n->hid, batch, dA2, 1, A1, 0, gW2, 0.f, nullptr, 0)) != CORAL_OK) return s;
-  k_col_sum<<<(n->hid + 127) / 128, 128, 0, n->h->stream>>>(batch, n->hid, dA2, gb2);
+  k_col_sum<<<(n->hid + 31) / 32, 32 * kColSumWarps, 0, n->h->stream>>>(batch, n->hid, dA2, gb2);
   if ((s = launch_status(n->h)) != CORAL_OK) return s;
   if ((s = gemm(n, batch, n->hid, n->hid, dA2, 0, w.W2, 0, dA1, 0.f, nullptr, 0)) != CORAL_OK) return s;
   k_relu_back<<<gr, 256, 0, n->h->stream>>>(bh, A1, dA1);
   if ((s = launch_status(n->h)) != CORAL_OK) return s;
   // layer 1
   if ((s = gemm(n, n->hid, n->in, batch, dA1, 1, x, 0, gW1, 0.f, nullptr, 0)) != CORAL_OK) return s;
-  k_col_sum<<<(n->hid + 127) / 128, 128, 0, n->h->stream>>>(batch, n->hid, dA1, gb1);
+  k_col_sum<<<(n->hid + 31) / 32, 32 * kColSumWarps, 0, n->h->stream>>>(batch, n->hid, dA1, gb1);
   return launch_status(n->h);
 }
 

@@ -40,42 +40,81 @@ constexpr int kOzEpiWarps = 8;
 constexpr int kOzThreads = 64 + 32 * kOzEpiWarps;
 
 // ---- 1. exponents ---------------------------------------------------------------
-// Per-row maximum exponent of op(X) for a 32 x 32 tile; atomicMax into e[row].
-// Complex: magnitude max(|re|, |im|) covers every real entry the 4M folding makes.
+// e[r] = max over l of the exponent of |op(X)(r, l)| (frexp: |v| 2^-e < 1),
+// combined across column chunks with atomicMax, which is exact in any order.
+// Complex: magnitude max(|re|, |im|) covers every real entry the 4M folding
+// makes. Column-major rows (element (r, l) at X[r + l ld]): a thread owns a
+// row and streams kExpChunkN columns with 8 loads in flight, so a warp reads
+// 32 consecutive elements per column. K-major rows (element (r, l) at
+// X[l + r ld]): a warp owns a row and streams kExpChunkK contiguous columns.
+constexpr int kExpChunkN = 64, kExpChunkK = 256;
+
+template <typename T>
+__device__ __forceinline__ double mag(const T& a) {
+  if constexpr (sizeof(T) == 16)
+    return fmax(fabs(reinterpret_cast<const double2&>(a).x), fabs(reinterpret_cast<const double2&>(a).y));
+  else
+    return fabs(reinterpret_cast<const double&>(a));
+}
+
 template <typename T, bool kKMajorSrc>
 __global__ void __launch_bounds__(256)
 k_row_exponent(const T* __restrict__ X, size_t ld, int R, int Kd, int* __restrict__ e) {
-  __shared__ double tile[32][33];
-  const int r0 = blockIdx.y * 32, l0 = blockIdx.x * 32;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  double m = 0.0;
+  int r;
+  if constexpr (!kKMajorSrc) {
+    r = blockIdx.y * 256 + threadIdx.x;
+    if (r >= R) return;
+    const int l0 = blockIdx.x * kExpChunkN, l1 = min(Kd, l0 + kExpChunkN);
+    const T* p = X + r;
+    int l = l0;
+    for (; l + 8 <= l1; l += 8) {
+      T a[8];
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    int r, l;
-    if (kKMajorSrc) { r = r0 + ty + 8 * q; l = l0 + tx; }
-    else            { l = l0 + ty + 8 * q; r = r0 + tx; }
-    double v = 0.0;
-    if (r < R && l < Kd) {
-      T a = __ldg(kKMajorSrc ? X + l + (size_t)r * ld : X + r + (size_t)l * ld);
-      if constexpr (sizeof(T) == 16) v = fmax(fabs(reinterpret_cast<double2&>(a).x), fabs(reinterpret_cast<double2&>(a).y));
-      else v = fabs(reinterpret_cast<double&>(a));
+      for (int u = 0; u < 8; ++u) a[u] = __ldg(p + (size_t)(l + u) * ld);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) m = fmax(m, mag(a[u]));
     }
-    if (kKMajorSrc) tile[ty + 8 * q][tx] = v;
-    else tile[tx][ty + 8 * q] = v;
-  }
-  __syncthreads();
-  // warp ty reduces rows ty, ty+8, ty+16, ty+24 across the 32 columns
+    for (; l < l1; ++l) m = fmax(m, mag(__ldg(p + (size_t)l * ld)));
+  } else {
+    const int lane = threadIdx.x & 31;
+    r = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (r >= R) return;
+    const int l0 = blockIdx.x * kExpChunkK;
+    const T* p = X + (size_t)r * ld;
+    T a[kExpChunkK / 32];
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int rr = ty + 8 * q;
-    double v = tile[rr][tx];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if (tx == 0 && r0 + rr < R && v > 0.0) {
-      int ex;
-      frexp(v, &ex);  // v = m 2^ex, m in [0.5, 1) -> v 2^-ex < 1
-      atomicMax(e + r0 + rr, ex);
+    for (int u = 0; u < kExpChunkK / 32; ++u) {
+      const int l = l0 + lane + 32 * u;
+      a[u] = l < Kd ? __ldg(p + l) : T{};
     }
+#pragma unroll
+    for (int u = 0; u < kExpChunkK / 32; ++u) m = fmax(m, mag(a[u]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane != 0) return;
   }
+  if (m > 0.0) {
+    int ex;
+    frexp(m, &ex);  // m = f 2^ex, f in [0.5, 1) -> m 2^-ex < 1
+    atomicMax(e + r, ex);
+  }
+}
+
+// Launches k_row_exponent over R rows of Kd columns (e must hold INT_MIN-like
+// starting values).
+template <typename T>
+coral_status_t launch_row_exponent(Handle* h, const T* X, size_t ld, int R, int Kd, bool kmajor, int* e) {
+  if (kmajor) {
+    const dim3 g((unsigned)((Kd + kExpChunkK - 1) / kExpChunkK), (unsigned)((R + 7) / 8));
+    if (g.y > 65535) return CORAL_ERR_NOT_SUPPORTED;
+    k_row_exponent<T, true><<<g, 256, 0, h->stream>>>(X, ld, R, Kd, e);
+  } else {
+    const dim3 g((unsigned)((Kd + kExpChunkN - 1) / kExpChunkN), (unsigned)((R + 255) / 256));
+    if (g.y > 65535) return CORAL_ERR_NOT_SUPPORTED;
+    k_row_exponent<T, false><<<g, 256, 0, h->stream>>>(X, ld, R, Kd, e);
+  }
+  return launch_status(h);
 }
 
 // ---- 2. slicing ----------------------------------------------------------------
@@ -453,16 +492,10 @@ coral_status_t dgemm_ozaki_impl(Handle* h, int op_a, int op_b, size_t m, size_t 
   int* ea = reinterpret_cast<int*>(sc + a_bytes + b_bytes);
   int* eb = ea + m;
   CORAL_CUDA(h, cudaMemsetAsync(ea, 0x80, (m + n) * sizeof(int), h->stream));  // INT_MIN-ish
-  dim3 ga((unsigned)((k + 31) / 32), (unsigned)((m + 31) / 32));
-  dim3 gb((unsigned)((k + 31) / 32), (unsigned)((n + 31) / 32));
   const bool a_km = op_a != CORAL_NO_TRANSPOSE, b_km = op_b == CORAL_NO_TRANSPOSE;
-  if (a_km) k_row_exponent<double, true><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ea);
-  else k_row_exponent<double, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ea);
-  coral_status_t s = launch_status(h);
+  coral_status_t s = launch_row_exponent(h, A, lda, (int)m, (int)k, a_km, ea);
   if (s != CORAL_OK) return s;
-  if (b_km) k_row_exponent<double, true><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, eb);
-  else k_row_exponent<double, false><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, eb);
-  if ((s = launch_status(h)) != CORAL_OK) return s;
+  if ((s = launch_row_exponent(h, B, ldb, (int)n, (int)k, b_km, eb)) != CORAL_OK) return s;
   dim3 gsa((unsigned)((kp + 31) / 32), (unsigned)((m + 31) / 32));
   dim3 gsb((unsigned)((kp + 31) / 32), (unsigned)((n + 31) / 32));
   if (a_km) k_slice_real<S, true><<<gsa, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ea, ap, kp, a_piece);
@@ -493,16 +526,10 @@ coral_status_t zgemm_ozaki_impl(Handle* h, int op_a, int op_b, size_t m, size_t 
   int* ebs = ea + m;          // per source column j of op(B) (length n)
   int* eb2 = ebs + n;         // per B'' row (length 2n)
   CORAL_CUDA(h, cudaMemsetAsync(ea, 0x80, (m + n) * sizeof(int), h->stream));
-  dim3 ga((unsigned)((k + 31) / 32), (unsigned)((m + 31) / 32));
-  dim3 gb((unsigned)((k + 31) / 32), (unsigned)((n + 31) / 32));
   const bool a_km = op_a != CORAL_NO_TRANSPOSE, b_km = op_b == CORAL_NO_TRANSPOSE;
-  if (a_km) k_row_exponent<double2, true><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ea);
-  else k_row_exponent<double2, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ea);
-  coral_status_t s = launch_status(h);
+  coral_status_t s = launch_row_exponent(h, A, lda, (int)m, (int)k, a_km, ea);
   if (s != CORAL_OK) return s;
-  if (b_km) k_row_exponent<double2, true><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, ebs);
-  else k_row_exponent<double2, false><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, ebs);
-  if ((s = launch_status(h)) != CORAL_OK) return s;
+  if ((s = launch_row_exponent(h, B, ldb, (int)n, (int)k, b_km, ebs)) != CORAL_OK) return s;
   // B'' rows 2j and 2j+1 share column j's exponent.
   CORAL_CUDA(h, cudaMemcpy2DAsync(eb2, 2 * sizeof(int), ebs, sizeof(int), sizeof(int), n,
                                   cudaMemcpyDeviceToDevice, h->stream));
@@ -510,6 +537,8 @@ coral_status_t zgemm_ozaki_impl(Handle* h, int op_a, int op_b, size_t m, size_t 
                                   cudaMemcpyDeviceToDevice, h->stream));
   if (kp != k2) CORAL_CUDA(h, cudaMemsetAsync(sc, 0, a_bytes + b_bytes, h->stream));
   const bool ca = op_a == CORAL_CONJ_TRANSPOSE, cbj = op_b == CORAL_CONJ_TRANSPOSE;
+  const dim3 ga((unsigned)((k + 31) / 32), (unsigned)((m + 31) / 32));  // 32 x 32 slicing tiles
+  const dim3 gb((unsigned)((k + 31) / 32), (unsigned)((n + 31) / 32));
   if (a_km) k_slice_cplx<S, true, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ca, ea, ap, kp, a_piece);
   else k_slice_cplx<S, false, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ca, ea, ap, kp, a_piece);
   if ((s = launch_status(h)) != CORAL_OK) return s;
