@@ -261,29 +261,6 @@ __global__ void k_scopy_strided(size_t n, const float* __restrict__ x, size_t in
     y[t * incy] = x[t * incx];
 }
 
-__global__ void k_sswap(size_t n, float* __restrict__ x, size_t incx, float* __restrict__ y,
-                        size_t incy, bool vec) {
-  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const size_t stride = (size_t)gridDim.x * blockDim.x;
-  size_t done = 0;
-  if (vec) {
-    const size_t n4 = n >> 2;
-    float4* x4 = reinterpret_cast<float4*>(x);
-    float4* y4 = reinterpret_cast<float4*>(y);
-    for (size_t i = tid; i < n4; i += stride) {
-      float4 a = __ldcs(x4 + i), b = __ldcs(y4 + i);
-      __stcs(x4 + i, b);
-      __stcs(y4 + i, a);
-    }
-    done = n4 << 2;
-  }
-  for (size_t t = done + tid; t < n; t += stride) {
-    float a = x[t * incx];
-    x[t * incx] = y[t * incy];
-    y[t * incy] = a;
-  }
-}
-
 }  // namespace
 
 // Enqueue helpers shared with level 2 (GEMV's beta step is sscal).
@@ -396,18 +373,5 @@ coral_status_t coral_scopy(coral_handle_t hh, size_t n, const float* x, size_t i
   return launch_status(H);
 }
 
-coral_status_t coral_sswap(coral_handle_t hh, size_t n, float* x, size_t incx, float* y,
-                           size_t incy) {
-  CORAL_HANDLE(hh);
-  if (n == 0) return CORAL_OK;  // sswap.rs:43
-  if (!x) return bad_arg(H, 2);
-  if (incx == 0) return bad_arg(H, 3);
-  if (!y) return bad_arg(H, 4);
-  if (incy == 0) return bad_arg(H, 5);
-  bool vec = incx == 1 && incy == 1 && aligned16(x) && aligned16(y);
-  unsigned g = stream_grid(n, 256 * 4 * 4, H->sm_count, 8);
-  k_sswap<<<g, 256, 0, H->stream>>>(n, x, incx, y, incy, vec);
-  return launch_status(H);
-}
 
 }  // extern "C"

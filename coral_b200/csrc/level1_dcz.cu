@@ -1115,6 +1115,11 @@ coral_status_t coral_cswap(coral_handle_t h, size_t n, float* x, size_t incx, fl
 coral_status_t coral_zswap(coral_handle_t h, size_t n, double* x, size_t incx, double* y, size_t incy) {
   return copy_entry<double2>(h, n, x, incx, y, incy, true);
 }
+// sswap.rs:35: the fp32 swap on the same streaming kernel (a pure
+// exchange, so bit-exact).
+coral_status_t coral_sswap(coral_handle_t h, size_t n, float* x, size_t incx, float* y, size_t incy) {
+  return copy_entry<float>(h, n, x, incx, y, incy, true);
+}
 
 // ---- rotations ----
 coral_status_t coral_srot(coral_handle_t h, size_t n, float* x, size_t incx, float* y, size_t incy, float c,
