@@ -152,13 +152,25 @@ k_rank_vec(int m, int n, float alpha, const float* __restrict__ x, const float* 
       range(j, l, h);
       const int len = h - l, nfused = len - (len & 7);
       float* av = &a[c].x;
+      const float k1 = c1[c], k2 = c2[c];
+      if (i0 + 3 - l < nfused) {
+        // all four elements in the fused part (the common case)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const bool fused = (i0 + e - l) < nfused;
-        float v = av[e];
-        if (c1[c] != 0.0f) v = axpy_elem(v, c1[c], xv[e], fused);
-        if (kKind == kSyr2 && c2[c] != 0.0f) v = axpy_elem(v, c2[c], yv[e], fused);
-        av[e] = v;
+        for (int e = 0; e < 4; ++e) {
+          float v = av[e];
+          if (k1 != 0.0f) v = fmaf(xv[e], k1, v);
+          if (kKind == kSyr2 && k2 != 0.0f) v = fmaf(yv[e], k2, v);
+          av[e] = v;
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const bool fused = (i0 + e - l) < nfused;
+          float v = av[e];
+          if (k1 != 0.0f) v = axpy_elem(v, k1, xv[e], fused);
+          if (kKind == kSyr2 && k2 != 0.0f) v = axpy_elem(v, k2, yv[e], fused);
+          av[e] = v;
+        }
       }
       float* col = A + (size_t)j * lda + i0;
       if (whole_mask & (1u << c)) {
