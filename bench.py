@@ -41,9 +41,12 @@ M = N = K = 8192  # overridden by --size (small profiling cases only)
 ALPHA, BETA = 1.5, 0.5
 GEMV_BYTES = 4 * (M * N + N + 2 * M)  # A once, x once, y read + written
 FP32_FMA_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal: SMs x FP32 lanes x 2 x max clock
-# DRAM bytes (read + write) of one 8192^3 launch of the split GEMM kernel, from
-# the ncu capture summarised in profiles/ (None until captured).
-SPLIT_GEMM_TRAFFIC_PER_LAUNCH: dict = {}
+# DRAM bytes (read + write) of one launch of the split GEMM kernel, keyed by
+# (products, m = n = k), from a one-pass ncu launch list of
+# `bench.py --only-gemm --steps 3 --warmup 3`: 2553.4 MB read + 258.3 MB
+# written (median of 6 launches). The bf16 pieces (536 MB) do not fit in the
+# 126 MB L2, and the kernel reads them about 4.8 times over.
+SPLIT_GEMM_TRAFFIC_PER_LAUNCH: dict = {(3, 8192): 2811.68e6}
 
 
 def peaks():
@@ -825,7 +828,7 @@ def run_ours(args, world, rank, local):
     else:
         products = 3 if mode == cb.GemmMode.SPLIT_BF16X3 else 6
         roof = {"bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
-                "frac": ach / bf16, "traffic": SPLIT_GEMM_TRAFFIC_PER_LAUNCH.get(products),
+                "frac": ach / bf16, "traffic": SPLIT_GEMM_TRAFFIC_PER_LAUNCH.get((products, M)),
                 "kernel": f"k_gemm_split<{products}>", "kernel_ms": kernel_ms,
                 "tensor_issue_frac": products * ach / bf16,
                 "peak_source": ("measured bf16 dense burst (MEASURED_PEAKS.json)" if src == "measured"
