@@ -161,7 +161,7 @@ def test_gemm_bad_args(cuda):
 
 
 def test_sgemm_8192_sampled(cuda):
-    """BASELINE precision config shape (plain FP32), sampled entries."""
+    """The 8192^3 precision-set shape in plain FP32, checked on sampled entries."""
     m = n = k = 8192
     rng = np.random.default_rng(1)
     A = torch.empty(m * k, dtype=torch.float32, device="cuda").uniform_(-1, 1)
