@@ -206,17 +206,19 @@ coral_status_t launch_rank_g(Handle* h, size_t m, size_t n, T alpha, const T* x,
   // measured 68% of HBM on the element kernel against 48% on this one
   // (n = 8192, upper).
   constexpr bool kVecOk = sizeof(T) < 16 && !(kKind == kHer2G && sizeof(T) == 8);
-  if (kVecOk && incx == 1 && (!kTwo || incy == 1) && aligned16(A) && (lda * sizeof(T)) % 16 == 0 &&
-      aligned16(x) && (!kTwo || aligned16(y))) {
-    constexpr int kV = Pack16<T>::kV;
-    const size_t groups = (n + kGCols - 1) / kGCols;
-    const dim3 vgrid = kKind < kSyrG
-        ? dim3((unsigned)((rows + (size_t)kV * kRThreads - 1) / ((size_t)kV * kRThreads)),
-               (unsigned)(groups < 65535 ? groups : 65535))
-        : dim3((unsigned)(groups < (1u << 30) ? groups : (1u << 30)));
-    k_rank_g_vec<T, kKind><<<vgrid, kRThreads, 0, h->stream>>>((int)m, (int)n, alpha, x, y, incy, A, lda,
-                                                                 lower);
-    return launch_status(h);
+  if constexpr (kVecOk) {  // the vector kernel is only instantiated where it is used
+    if (incx == 1 && (!kTwo || incy == 1) && aligned16(A) && (lda * sizeof(T)) % 16 == 0 && aligned16(x) &&
+        (!kTwo || aligned16(y))) {
+      constexpr int kV = Pack16<T>::kV;
+      const size_t groups = (n + kGCols - 1) / kGCols;
+      const dim3 vgrid = kKind < kSyrG
+          ? dim3((unsigned)((rows + (size_t)kV * kRThreads - 1) / ((size_t)kV * kRThreads)),
+                 (unsigned)(groups < 65535 ? groups : 65535))
+          : dim3((unsigned)(groups < (1u << 30) ? groups : (1u << 30)));
+      k_rank_g_vec<T, kKind><<<vgrid, kRThreads, 0, h->stream>>>((int)m, (int)n, alpha, x, y, incy, A, lda,
+                                                                   lower);
+      return launch_status(h);
+    }
   }
   const dim3 grid((unsigned)((rows + kRRows - 1) / kRRows), (unsigned)(n < 65535 ? n : 65535));
   k_rank_g<T, kKind><<<grid, kRThreads, 0, h->stream>>>((int)m, (int)n, alpha, x, incx, y, incy, A, lda,
