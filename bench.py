@@ -18,7 +18,9 @@ is the sum of work over that time.
 --impl reference times CORAL's own CPU algorithm for the same metric (its
 sgemm_nn blocking and microkernel order restated in C, oracle/oracle.c
 port_sgemm_nn; the Rust crate cannot be built on this host) on a bounded
-sample of the workload, single-threaded as the reference is.
+sample of the workload: one independent 1024^3 problem per host thread on
+every host thread (the reference is single-threaded per call but
+re-entrant), with the single-thread figure printed beside it.
 """
 from __future__ import annotations
 
@@ -187,6 +189,7 @@ def run_reference(args, world, rank):
         vals.append(v)
         secs += el
     value = float(np.mean(vals))
+    v1, reps1, el1, _ = cpu_sample_tflops(2.0, size, threads=1)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -199,7 +202,10 @@ def run_reference(args, world, rank):
                          "sample": f"sgemm NN {size}^3 problems, one per thread for 2 s per step; "
                                    f"CORAL sgemm_nn blocking (MC/NC/KC 384/576/256) and 8x12 "
                                    f"microkernel restated in C with AVX2 FMAs (Rust crate not "
-                                   f"buildable here; the reference has no threading of its own)"},
+                                   f"buildable here; the reference has no threading of its own)",
+                         "single_core": {"value": v1, "unit": "TFLOP/s", "cores": 1,
+                                         "sample": f"{reps1} problems of {size}^3 in {el1:.1f} s "
+                                                   f"on one host thread"}},
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -326,6 +332,8 @@ def batched_set(torch, cb, dev):
     dims = np.exp(rng.uniform(np.log(16), np.log(512), (count, 3))).astype(np.int64)
     ops = np.where(rng.uniform(size=count) < 0.5, 0, 1)
     flops = float(2 * (dims[:, 0] * dims[:, 1] * dims[:, 2]).sum())
+    h = cb.handle()
+    saved_mode = h.gemm_mode()
     for bf16 in (False, True):
         rec = np.zeros(count, dtype=cb.sgemm_problem_dtype())
         sizes = [(int(m) * int(k), int(k) * int(n), int(m) * int(n)) for m, n, k in dims]
@@ -343,10 +351,30 @@ def batched_set(torch, cb, dev):
                       pc.data_ptr() + oc * 4, m if op_a == 0 else k, k, m)
             oa += m * k; ob += k * n; oc += m * n
         desc = torch.from_numpy(rec.view(np.uint8)).to(dev)
-        ms = graph_time(lambda: cb.sgemm_grouped(1 if bf16 else 0, count, desc))
-        out["grouped_sgemm_4096_" + ("bf16in" if bf16 else "fp32")] = {
-            "ms": ms, "tflops": flops / (ms * 1e-3) / 1e12, "instances": count}
+        it = 1 if bf16 else 0
+        # fp32 inputs: exact FP32 FMA tiles (NATIVE) and tensor-core
+        # split-BF16x3; bf16 inputs: tensor cores.  Tensor-core variants are
+        # timed with the default tile-width policy and with the policy the
+        # autotuner picks on this batch.
+        variants = ([] if bf16 else [("fp32_native", cb.GemmMode.NATIVE)]) + [
+            ("bf16in" if bf16 else "fp32_split_bf16x3", cb.GemmMode.SPLIT_BF16X3)]
+        for name, gm in variants:
+            h.set_gemm_mode(gm)
+            ms = graph_time(lambda: cb.sgemm_grouped(it, count, desc))
+            entry = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12, "instances": count,
+                     "kernel": "k_gemm_simt-style FMA tiles" if gm == cb.GemmMode.NATIVE
+                     else "k_gemm_grouped_tc (tcgen05)"}
+            if gm == cb.GemmMode.SPLIT_BF16X3:
+                entry["policy_default"] = cb.grouped_config()
+                tune_ms, best, tile_n = cb.autotune_sgemm_grouped(it, count, desc, reps=2)
+                ms_t = graph_time(lambda: cb.sgemm_grouped(it, count, desc))
+                entry.update({"policy_tuned": tile_n, "ms_tuned": ms_t,
+                              "tflops_tuned": flops / (ms_t * 1e-3) / 1e12,
+                              "autotune_candidates": len(tune_ms)})
+                cb.set_grouped_config(None)
+            out["grouped_sgemm_4096_" + name] = entry
         del pa, pb, pc, desc
+    h.set_gemm_mode(saved_mode)
     count = 1024
     ns = np.exp(rng.uniform(np.log(32), np.log(1024), count)).astype(np.int64)
     rec = np.zeros(count, dtype=cb.strsv_problem_dtype())
@@ -742,25 +770,39 @@ def run_ours(args, world, rank, local):
             routines = args.routines.split(",") if args.routines else None
             print(json.dumps({"level12": level12_bandwidth(torch, cb, lib, h, dev, g, routines)}))
         return
-    # accuracy of the headline mode on sampled entries (single call from C0)
+    # accuracy on the same 4096 sampled entries (each mode: one call from C0)
+    # for the headline mode, the plain FP32 kernel and the 3-piece split
     import oracle
-    C.copy_(C0)
-    step(mode)
-    torch.cuda.synchronize()
     rng = np.random.default_rng(7)
     ns = 4096
     ii, jj = rng.integers(0, M, ns), rng.integers(0, N, ns)
     idx = torch.from_numpy(ii + jj * M).to(dev)
-    got = C[idx].double().cpu().numpy()
     sub_a = A.cpu().numpy()
     sub_b = B.cpu().numpy()
     want, bound = oracle.gemm_sample(0, 0, M, N, K, ALPHA, sub_a, M, sub_b, K, BETA,
                                      C0.cpu().numpy(), M, ii, jj)
     del sub_a, sub_b
-    err = np.abs(got - want)
-    acc = {"samples": ns, "max_rel_componentwise": float((err / bound).max()),
-           "max_rel_normwise": float(err.max() / np.abs(want).max()),
-           "max_rel_elementwise_p50": float(np.median(err / np.abs(want)))}
+
+    def accuracy_of(m_):
+        C.copy_(C0)
+        step(m_)
+        torch.cuda.synchronize()
+        got = C[idx].double().cpu().numpy()
+        err = np.abs(got - want)
+        rel = err / np.abs(want)
+        return {"max_rel_componentwise": float((err / bound).max()),
+                "max_rel_normwise": float(err.max() / np.abs(want).max()),
+                "max_rel_elementwise": float(rel.max()),
+                "rel_elementwise_p50": float(np.median(rel)),
+                "rel_elementwise_p99": float(np.quantile(rel, 0.99))}
+    mode_names = {cb.GemmMode.NATIVE: "native", cb.GemmMode.SPLIT_BF16X3: "split_bf16x3",
+                  cb.GemmMode.SPLIT_BF16X6: "split_bf16x6"}
+    acc = {"samples": ns, "definitions": (
+        "componentwise: |err| / (|alpha| (|A||B|)_ij + |beta| |C_ij|); normwise: max |err| / "
+        "max |C_exact| over the samples; elementwise: |err| / |C_exact_ij|")}
+    acc.update(accuracy_of(mode))
+    acc["by_mode"] = {mode_names[m_]: accuracy_of(m_) for m_ in
+                      (cb.GemmMode.SPLIT_BF16X3, cb.GemmMode.NATIVE, cb.GemmMode.SPLIT_BF16X6)}
 
     with ClockSampler(local) as clocks:
         # keep the GPU under load ~0.6 s before the timed steps so the clock
@@ -775,9 +817,11 @@ def run_ours(args, world, rank, local):
     flops = 2.0 * M * N * K
     value = world * flops / (ms * 1e-3) / 1e12
 
-    native_ms = None
+    native_ms = x6_ms = None
     if mode != cb.GemmMode.NATIVE:
         native_ms, _ = timed(lambda: step(cb.GemmMode.NATIVE), max(2, args.steps // 2), 1)
+    if mode != cb.GemmMode.SPLIT_BF16X6:
+        x6_ms, _ = timed(lambda: step(cb.GemmMode.SPLIT_BF16X6), max(2, args.steps // 2), 1)
     h.set_gemm_mode(mode)
 
     # e2e through the host-slice C ABI: pinned host operands, H2D + compute + D2H per step
@@ -838,10 +882,15 @@ def run_ours(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         v, reps, el, threads = cpu_sample_tflops(10.0)
+        v1, reps1, el1, _ = cpu_sample_tflops(4.0, threads=1)
         cpu = {"value": v, "unit": "TFLOP/s", "cores": threads, "kind": "port",
                "sample": f"{reps} sgemm NN 1024^3 problems in {el:.1f} s on {threads} host threads "
                          f"(one independent problem per thread), CORAL sgemm_nn blocking and 8x12 "
-                         f"microkernel restated in C with AVX2 FMAs"}
+                         f"microkernel restated in C with AVX2 FMAs",
+               "single_core": {"value": v1, "unit": "TFLOP/s", "cores": 1,
+                               "sample": f"{reps1} sgemm NN 1024^3 problems in {el1:.1f} s on one "
+                                         f"host thread (the reference is single-threaded)"},
+               "host_cores": os.cpu_count()}
 
     if rank == 0:
         line = {
@@ -854,6 +903,7 @@ def run_ours(args, world, rank, local):
                        "l2": "inputs 768 MiB > L2, no flush", "parallelism": f"replicas x{world}"},
             "accuracy": acc,
             "plain_fp32_tflops": (world * flops / (native_ms * 1e-3) / 1e12) if native_ms else value,
+            "split_bf16x6_tflops": (world * flops / (x6_ms * 1e-3) / 1e12) if x6_ms else value,
             "gemv_gbs": {"n": gemv["n"], "t": gemv["t"], "peak": hbm,
                          "frac_n": gemv["n"] / hbm, "frac_t": gemv["t"] / hbm},
             "level12": l12,

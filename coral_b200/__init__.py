@@ -16,6 +16,7 @@ from .blas import (  # noqa: F401
     icamax, izamax, daxpy, caxpy, zaxpy, dscal, cscal, zscal, csscal, zdscal, dcopy, ccopy, zcopy,
     dswap, cswap, zswap, srot, drot, csrot, zdrot, srotm, drotm, srotg, drotg, srotmg, drotmg,
     saxpyf, daxpyf, caxpyf, zaxpyf, sdotf, ddotf, cdotuf, cdotcf, zdotuf, zdotcf,
+    set_grouped_config, grouped_config, autotune_sgemm_grouped,
 )
 
 __all__ = [
@@ -30,4 +31,5 @@ __all__ = [
     "idamax", "icamax", "izamax", "daxpy", "caxpy", "zaxpy", "dscal", "cscal", "zscal", "csscal", "zdscal", "dcopy",
     "ccopy", "zcopy", "dswap", "cswap", "zswap", "srot", "drot", "csrot", "zdrot", "srotm", "drotm", "srotg", "drotg", "srotmg", "drotmg",
     "saxpyf", "daxpyf", "caxpyf", "zaxpyf", "sdotf", "ddotf", "cdotuf", "cdotcf", "zdotuf", "zdotcf",
+    "set_grouped_config", "grouped_config", "autotune_sgemm_grouped",
 ]

@@ -36,6 +36,7 @@ SIGNATURES = {
     "coral_get_gemm_mode": [_h, C.POINTER(_i)],
     "coral_set_wait_limit": [_h, C.c_uint64],
     "coral_set_split_chunk": [_h, _i],
+    "coral_set_complex_mapping": [_h, _i],
     "coral_sync": [_h],
     "coral_set_kernel_timing": [_h, _i],
     "coral_get_kernel_timing": [_h, C.POINTER(_d), C.POINTER(C.c_uint64)],
@@ -135,6 +136,9 @@ SIGNATURES = {
     "coral_cgemm": [_h, _i, _i, _sz, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
     "coral_zgemm": [_h, _i, _i, _sz, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
     "coral_sgemm_grouped": [_h, _i, _sz, _vp],
+    "coral_set_grouped_config": [_h, _vp],
+    "coral_get_grouped_config": [_h, _vp],
+    "coral_autotune_sgemm_grouped": [_h, _i, _sz, _vp, _i, _vp, C.POINTER(_i), _vp],
     "coral_set_gemm_config": [_h, _i, _i],
     "coral_get_gemm_config": [_h, _i, _i, _i, _sz, _sz, _sz, C.POINTER(_i), C.POINTER(_i)],
     "coral_selector_features": [_i, _i, _i, _sz, _sz, _sz, _i, _i, C.POINTER(_f)],
@@ -151,6 +155,7 @@ SIGNATURES = {
     "coral_set_selector": [_h, _vp],
     "coral_strsv_batched": [_h, _sz, _vp],
     "coral_sgemm_bf16x3_noalloc": [_vp, _i, _i, _sz, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
+    "coral_sgemm_bf16x3_noalloc_status": [_vp],
     "coral_host_sgemm": [_i, _i, _sz, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
     "coral_host_sgemv": [_i, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
     "coral_host_sdot": [_sz, _vp, _sz, _vp, _sz, _vp],
@@ -158,6 +163,19 @@ SIGNATURES = {
     "coral_host_isamax": [_sz, _vp, _sz, _vp],
     "coral_host_strsv": [_i, _i, _i, _sz, _vp, _sz, _vp, _sz],
     "coral_host_set_gemm_mode": [_i],
+    "coral_host_ssymv": [_i, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
+    "coral_host_chemv": [_i, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
+    "coral_host_strmv": [_i, _i, _i, _sz, _vp, _sz, _vp, _sz],
+    "coral_host_sger": [_sz, _sz, _f, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_host_ssyr": [_i, _sz, _f, _vp, _sz, _vp, _sz],
+    "coral_host_ssyr2": [_i, _sz, _f, _vp, _sz, _vp, _sz, _vp, _sz],
+    "coral_host_snrm2": [_sz, _vp, _sz, _vp],
+    "coral_host_scopy": [_sz, _vp, _sz, _vp, _sz],
+    "coral_host_sswap": [_sz, _vp, _sz, _vp, _sz],
+    "coral_host_sscal": [_sz, _f, _vp, _sz],
+    "coral_host_dgemm": [_i, _i, _sz, _sz, _sz, _d, _vp, _sz, _vp, _sz, _d, _vp, _sz],
+    "coral_host_cgemm": [_i, _i, _sz, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
+    "coral_host_zgemm": [_i, _i, _sz, _sz, _sz, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _sz],
 }
 
 _RESTYPE = {

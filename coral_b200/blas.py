@@ -105,6 +105,10 @@ class Handle:
     def set_split_chunk(self, slabs: int) -> None:
         self.check(self.lib.coral_set_split_chunk(self.h, slabs), "coral_set_split_chunk")
 
+    def set_complex_mapping(self, mapping: int) -> None:
+        """0: 4M (default), 1: 3M, for coral_cgemm in the split-BF16 modes."""
+        self.check(self.lib.coral_set_complex_mapping(self.h, mapping), "coral_set_complex_mapping")
+
     def set_wait_limit(self, spins: int) -> None:
         self.check(self.lib.coral_set_wait_limit(self.h, spins), "coral_set_wait_limit")
 
@@ -809,3 +813,30 @@ def sgemm_grouped(input_type, count, problems) -> None:
 def strsv_batched(count, problems) -> None:
     """Batched STRSV over `count` descriptors held in the CUDA tensor `problems`."""
     handle().call("coral_strsv_batched", count, C.c_void_p(problems.data_ptr()))
+
+
+def set_grouped_config(tile_n=None) -> None:
+    """N tile widths of the tensor-core grouped GEMM for the instance classes
+    n <= 64, <= 128, <= 256, > 256 (None restores the default)."""
+    if tile_n is None:
+        handle().call("coral_set_grouped_config", None)
+    else:
+        arr = (C.c_int * 4)(*[int(t) for t in tile_n])
+        handle().call("coral_set_grouped_config", arr)
+
+
+def grouped_config() -> list:
+    arr = (C.c_int * 4)()
+    handle().call("coral_get_grouped_config", arr)
+    return list(arr)
+
+
+def autotune_sgemm_grouped(input_type, count, problems, reps=3):
+    """Exhaustive tuning of the grouped policy on one batch; returns
+    (ms per candidate [36], best index, tile widths) and installs the best."""
+    ms = (C.c_float * 36)()
+    best = C.c_int()
+    tn = (C.c_int * 4)()
+    handle().call("coral_autotune_sgemm_grouped", int(input_type), count,
+                  C.c_void_p(problems.data_ptr()), int(reps), ms, C.byref(best), tn)
+    return list(ms), best.value, list(tn)

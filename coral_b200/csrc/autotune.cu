@@ -62,3 +62,61 @@ extern "C" coral_status_t coral_autotune_sgemm(coral_handle_t hh, int products, 
   H->cfg_splits = saved_sp;
   return st;
 }
+
+// Exhaustive tuning of the tensor-core grouped GEMM's tile-width policy on one
+// batch: every assignment of N tile widths to the four instance classes
+// (n <= 64: {64, 128}; n <= 128: {64, 128}; n <= 256 and n > 256:
+// {64, 128, 256}) -- 36 candidates, class 0 varying slowest -- runs once
+// untimed and `reps` times between CUDA events.  Installs the fastest policy
+// on the handle and returns it in `tile_n`.  The instances' C is overwritten.
+extern "C" coral_status_t coral_autotune_sgemm_grouped(coral_handle_t hh, int input_type, size_t count,
+                                                       const coral_sgemm_problem_t* problems, int reps,
+                                                       float* ms_out, int* best, int tile_n[4]) {
+  CORAL_HANDLE(hh);
+  if (input_type != CORAL_INPUT_F32 && input_type != CORAL_INPUT_BF16) return bad_arg(H, 1);
+  if (!problems) return bad_arg(H, 3);
+  if (reps < 1) return bad_arg(H, 4);
+  if (!ms_out) return bad_arg(H, 5);
+  if (!best) return bad_arg(H, 6);
+  if (!tile_n) return bad_arg(H, 7);
+  static const int kC01[2] = {64, 128};
+  static const int kC23[3] = {64, 128, 256};
+  std::vector<GroupedPolicy> cands;
+  for (int a : kC01)
+    for (int b : kC01)
+      for (int c : kC23)
+        for (int d : kC23) cands.push_back(GroupedPolicy{{a, b, c, d}});
+  const GroupedPolicy saved = H->grouped_policy;
+  const int saved_mode = H->gemm_mode;
+  if (input_type == CORAL_INPUT_F32) H->gemm_mode = CORAL_GEMM_SPLIT_BF16X3;
+  std::vector<cudaEvent_t> ev(2 * cands.size(), nullptr);
+  coral_status_t st = CORAL_OK;
+  for (auto& e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) st = CORAL_ERR_CUDA;
+  for (size_t i = 0; i < cands.size() && st == CORAL_OK; ++i) {
+    H->grouped_policy = cands[i];
+    st = coral_sgemm_grouped(hh, input_type, count, problems);
+    if (st != CORAL_OK) break;
+    cudaEventRecord(ev[2 * i], H->stream);
+    for (int r = 0; r < reps && st == CORAL_OK; ++r) st = coral_sgemm_grouped(hh, input_type, count, problems);
+    cudaEventRecord(ev[2 * i + 1], H->stream);
+  }
+  if (st == CORAL_OK && cudaStreamSynchronize(H->stream) != cudaSuccess) st = CORAL_ERR_CUDA;
+  H->gemm_mode = saved_mode;
+  H->grouped_policy = saved;
+  if (st == CORAL_OK) {
+    int bi = 0;
+    for (size_t i = 0; i < cands.size(); ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
+      ms_out[i] = ms / (float)reps;
+      if (ms_out[i] < ms_out[bi]) bi = (int)i;
+    }
+    *best = bi;
+    H->grouped_policy = cands[bi];
+    for (int c = 0; c < 4; ++c) tile_n[c] = cands[bi].bn[c];
+  }
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  return st;
+}

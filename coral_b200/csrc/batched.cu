@@ -7,7 +7,11 @@
 // work per instance and can be captured in a CUDA graph (size the handle's
 // scratch with one uncaptured call first).
 //
-// Grouped GEMM: k_tile_prefix (one CTA) turns the descriptors into an
+// Grouped GEMM on the tensor cores (bf16 inputs, or fp32 inputs in
+// split-BF16x3 mode): grouped_tc.cu.  The FP32 FMA form below serves fp32
+// inputs in the NATIVE and SPLIT_BF16X6 modes.
+//
+// Grouped GEMM (FMA form): k_tile_prefix (one CTA) turns the descriptors into an
 // exclusive prefix sum of 64 x 64 output tiles; k_gemm_grouped (persistent,
 // 4 CTAs per SM) walks the global tile index space with a grid stride, finds
 // each tile's instance by binary search over the prefix array and computes
@@ -289,6 +293,11 @@ coral_status_t coral_sgemm_grouped(coral_handle_t hh, int input_type, size_t cou
   if (count == 0) return CORAL_OK;
   if (!problems) return bad_arg(H, 3);
   if (count > (size_t)INT32_MAX / 2) return CORAL_ERR_NOT_SUPPORTED;
+  // Tensor cores for bf16 inputs and for fp32 inputs in split-BF16x3 mode;
+  // exact FP32 FMA tiles otherwise (NATIVE, and SPLIT_BF16X6, whose error
+  // bound the two-piece split does not meet).
+  if (input_type == CORAL_INPUT_BF16 || H->gemm_mode == CORAL_GEMM_SPLIT_BF16X3)
+    return enqueue_grouped_tc(H, input_type == CORAL_INPUT_BF16, count, problems);
   int* prefix = static_cast<int*>(scratch(H, (count + 1) * sizeof(int)));
   if (!prefix) return CORAL_ERR_ALLOC;
   const GemmProblem* pr = reinterpret_cast<const GemmProblem*>(problems);
@@ -304,6 +313,25 @@ coral_status_t coral_sgemm_grouped(coral_handle_t hh, int input_type, size_t cou
   s = launch_status(H);
   timed_end(H);
   return s;
+}
+
+coral_status_t coral_set_grouped_config(coral_handle_t hh, const int tile_n[4]) {
+  CORAL_HANDLE(hh);
+  if (!tile_n) {
+    H->grouped_policy = GroupedPolicy{{64, 128, 128, 256}};
+    return CORAL_OK;
+  }
+  for (int i = 0; i < 4; ++i)
+    if (tile_n[i] != 64 && tile_n[i] != 128 && tile_n[i] != 256) return bad_arg(H, 1);
+  for (int i = 0; i < 4; ++i) H->grouped_policy.bn[i] = tile_n[i];
+  return CORAL_OK;
+}
+
+coral_status_t coral_get_grouped_config(coral_handle_t hh, int tile_n[4]) {
+  CORAL_HANDLE(hh);
+  if (!tile_n) return bad_arg(H, 1);
+  for (int i = 0; i < 4; ++i) tile_n[i] = H->grouped_policy.bn[i];
+  return CORAL_OK;
 }
 
 coral_status_t coral_strsv_batched(coral_handle_t hh, size_t count,

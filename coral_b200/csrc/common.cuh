@@ -19,6 +19,12 @@ constexpr uint64_t kDefaultWaitLimit = 1ull << 26;  // ~1 s of 20-ns spins
 // Device status word bits (written by bounded waits, read by coral_sync).
 constexpr unsigned kStatusTimeout = 1u;
 
+// Tile width policy of the tensor-core grouped GEMM: N tile width (64, 128
+// or 256) per instance class by n (<= 64, <= 128, <= 256, > 256).
+struct GroupedPolicy {
+  int bn[4];
+};
+
 struct Handle {
   int device = 0;
   int sm_count = kNumSMs;
@@ -34,6 +40,10 @@ struct Handle {
   int split_chunk_kb = 16;
   // Explicit split-GEMM configuration (0 = not set): N tile width, split-K.
   int cfg_bn = 0, cfg_splits = 0;
+  // Complex GEMM mapping onto real tensor-core products (CORAL_COMPLEX_4M or 3M).
+  int complex_mapping = CORAL_COMPLEX_4M;
+  // Tile widths of the tensor-core grouped GEMM per instance class.
+  GroupedPolicy grouped_policy{{64, 128, 128, 256}};
   // Learned configuration selector (see selector.cu), or null.
   struct Selector* selector = nullptr;
   int bad_arg = 0;
@@ -148,6 +158,11 @@ bool select_split_config(Handle* h, const SplitShape& sh, SplitConfig* out);
 // Features of (shape, configuration) for the selector network.
 constexpr int kSelectorFeatures = 13;
 void selector_features(const SplitShape& sh, int bn, int splits, float* f);
+
+// Tensor-core grouped GEMM (grouped_tc.cu): bf16 inputs, or fp32 inputs as
+// split-BF16x3; descriptors in device memory.
+coral_status_t enqueue_grouped_tc(Handle* h, bool bf16_inputs, size_t count,
+                                  const coral_sgemm_problem_t* probs);
 
 // Per-thread default handle for the coral_host_* entry points.
 Handle* thread_handle();

@@ -328,6 +328,74 @@ k_split_cplx(const float2* __restrict__ X, size_t ld, int R, int Kd, bool conj,
   }
 }
 
+// Complex operand, 3M layout: three real matrices of op(X) (conjugated when
+// `conj`), each [R][kp] with NPC pieces: part 0 Re, part 1 Im, part 2 Re + Im
+// (the sum rounded in fp32 before it is split).  K past Kd is written as zero.
+template <int NPC, bool kKMajorSrc>
+__global__ void __launch_bounds__(256)
+k_split_cplx3(const float2* __restrict__ X, size_t ld, int R, int Kd, bool conj,
+              __nv_bfloat16* __restrict__ dst, size_t kp, size_t piece_stride, size_t part_stride) {
+  __shared__ float2 tile[32][33];
+  const int r0 = blockIdx.y * 32, l0 = blockIdx.x * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  if (kKMajorSrc) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int r = r0 + ty + 8 * q, l = l0 + tx;
+      tile[ty + 8 * q][tx] = (r < R && l < Kd) ? __ldg(X + l + (size_t)r * ld) : make_float2(0.f, 0.f);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int l = l0 + ty + 8 * q, r = r0 + tx;
+      tile[tx][ty + 8 * q] = (r < R && l < Kd) ? __ldg(X + r + (size_t)l * ld) : make_float2(0.f, 0.f);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    int r = r0 + ty + 8 * q, l = l0 + tx;
+    if (r >= R || l >= (int)kp) continue;
+    float2 v = tile[ty + 8 * q][tx];  // zero past Kd
+    if (conj) v.y = -v.y;
+    const float vals[3] = {v.x, v.y, v.x + v.y};
+    const size_t o = (size_t)r * kp + l;
+#pragma unroll
+    for (int part = 0; part < 3; ++part) {
+      __nv_bfloat16 p[3];
+      split_value<NPC>(vals[part], p);
+#pragma unroll
+      for (int i = 0; i < NPC; ++i) dst[part * part_stride + i * piece_stride + o] = p[i];
+    }
+  }
+}
+
+// 3M combine: with T1 = Re A Re B, T2 = Im A Im B, T3 = (Re A + Im A)(Re B + Im B)
+// (m x n, column-major, ld m), C = alpha (T1 - T2 + i (T3 - T1 - T2)) + beta C.
+__global__ void k_combine_3m(const float* __restrict__ t1, const float* __restrict__ t2,
+                             const float* __restrict__ t3, int m, int n, float2 alpha, float2 beta,
+                             float2* __restrict__ C, size_t ldc) {
+  const size_t total = (size_t)m * n;
+  const bool beta0 = beta.x == 0.f && beta.y == 0.f;
+  const bool beta1 = beta.x == 1.f && beta.y == 0.f;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const float a = t1[t], b = t2[t], c3 = t3[t];
+    const float re = a - b, im = c3 - a - b;
+    float2 v = make_float2(alpha.x * re - alpha.y * im, alpha.x * im + alpha.y * re);
+    float2* cp = C + t % m + (t / m) * ldc;
+    if (!beta0) {
+      const float2 cv = *cp;
+      if (beta1) { v.x += cv.x; v.y += cv.y; }
+      else {
+        v.x += beta.x * cv.x - beta.y * cv.y;
+        v.y += beta.x * cv.y + beta.y * cv.x;
+      }
+    }
+    *cp = v;
+  }
+}
+
 // ---- 2. tcgen05 GEMM ---------------------------------------------------------
 struct EpiParams {
   float* C;          // real: float column-major; complex: float2 column-major
@@ -738,10 +806,63 @@ coral_status_t sgemm_split_impl(Handle* h, int op_a, int op_b, size_t m, size_t 
   return dispatch_split_gemm<NP>(h, ap, a_piece, (int)m, bp, b_piece, (int)n, (int)k, kp, cfg, ws, ep);
 }
 
+// 3M mapping: three real split GEMMs of m x n x k (Re A Re B, Im A Im B and
+// (Re A + Im A)(Re B + Im B)) into fp32 workspace, then k_combine_3m.  Three
+// quarters of the 4M mapping's tensor work; the imaginary part is formed as
+// T3 - T1 - T2, so its error is bounded by (|Re A| + |Im A|)(|Re B| + |Im B|)
+// rather than |A| |B| per term.
+template <int NP>
+coral_status_t cgemm_split_3m(Handle* h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                              float2 alpha, const float2* A, size_t lda, const float2* B, size_t ldb,
+                              float2 beta, float2* C, size_t ldc) {
+  constexpr int NPC = SplitPlan<NP>::kPieces;
+  const size_t kp = (k + 7) & ~size_t(7);
+  const size_t a_piece = m * kp, b_piece = n * kp;
+  const size_t a_part = NPC * a_piece, b_part = NPC * b_piece;
+  const size_t a_bytes = (3 * a_part * 2 + 255) & ~size_t(255);
+  const size_t b_bytes = (3 * b_part * 2 + 255) & ~size_t(255);
+  const size_t t_bytes = (m * n * sizeof(float) + 255) & ~size_t(255);
+  const SplitConfig cfg = choose_split_config(h, SplitShape{(int)m, (int)n, (int)k, NP, op_a, op_b, 1, 1});
+  const size_t ws_bytes = cfg.splits > 1 ? (size_t)cfg.splits * m * n * sizeof(float) : 0;
+  char* sc = static_cast<char*>(scratch(h, a_bytes + b_bytes + 3 * t_bytes + ws_bytes));
+  if (!sc) return CORAL_ERR_ALLOC;
+  __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(sc);
+  __nv_bfloat16* bp = reinterpret_cast<__nv_bfloat16*>(sc + a_bytes);
+  float* t[3];
+  for (int i = 0; i < 3; ++i) t[i] = reinterpret_cast<float*>(sc + a_bytes + b_bytes + i * t_bytes);
+  float* ws = reinterpret_cast<float*>(sc + a_bytes + b_bytes + 3 * t_bytes);
+  const bool ca = op_a == CORAL_CONJ_TRANSPOSE, cbj = op_b == CORAL_CONJ_TRANSPOSE;
+  dim3 ga((unsigned)((kp + 31) / 32), (unsigned)((m + 31) / 32));
+  if (op_a == CORAL_NO_TRANSPOSE)
+    k_split_cplx3<NPC, false><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ca, ap, kp, a_piece, a_part);
+  else
+    k_split_cplx3<NPC, true><<<ga, 256, 0, h->stream>>>(A, lda, (int)m, (int)k, ca, ap, kp, a_piece, a_part);
+  coral_status_t s = launch_status(h);
+  if (s != CORAL_OK) return s;
+  // op(B)^T rows are j: storage K-major iff op_b is NoTranspose
+  dim3 gb((unsigned)((kp + 31) / 32), (unsigned)((n + 31) / 32));
+  if (op_b == CORAL_NO_TRANSPOSE)
+    k_split_cplx3<NPC, true><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, cbj, bp, kp, b_piece, b_part);
+  else
+    k_split_cplx3<NPC, false><<<gb, 256, 0, h->stream>>>(B, ldb, (int)n, (int)k, cbj, bp, kp, b_piece, b_part);
+  if ((s = launch_status(h)) != CORAL_OK) return s;
+  for (int part = 0; part < 3; ++part) {
+    EpiParams ep{t[part], m, (int)m, (int)n, 1.f, 0.f, 0.f, 0.f, 0};
+    s = dispatch_split_gemm<NP>(h, ap + part * a_part, a_piece, (int)m, bp + part * b_part, b_piece, (int)n,
+                                (int)k, kp, cfg, ws, ep);
+    if (s != CORAL_OK) return s;
+  }
+  unsigned g = stream_grid(m * n, 256 * 4, h->sm_count, 8);
+  k_combine_3m<<<g, 256, 0, h->stream>>>(t[0], t[1], t[2], (int)m, (int)n, alpha, beta, C, ldc);
+  return launch_status(h);
+}
+
 template <int NP>
 coral_status_t cgemm_split_impl(Handle* h, int op_a, int op_b, size_t m, size_t n, size_t k,
                                 float2 alpha, const float2* A, size_t lda, const float2* B,
                                 size_t ldb, float2 beta, float2* C, size_t ldc) {
+  if (h->complex_mapping == CORAL_COMPLEX_3M)
+    return cgemm_split_3m<NP>(h, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
   constexpr int NPC = SplitPlan<NP>::kPieces;
   const size_t k2 = 2 * k;
   const size_t kp = (k2 + 7) & ~size_t(7);
@@ -876,27 +997,29 @@ extern "C" coral_status_t coral_sgemm_bf16x3_noalloc(void* stream, int op_a, int
   using namespace coral;
   if (gemm_bad_arg(op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, false) > 0)
     return CORAL_ERR_INVALID_ARG;
-  const size_t kp = (k + 7) & ~size_t(7);
-  const size_t a_piece = m * kp, b_piece = n * kp;
-  const size_t a_bytes = (2 * a_piece * 2 + 255) & ~size_t(255);
-  const size_t b_bytes = 2 * b_piece * 2;
-  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX || k > (size_t)INT32_MAX ||
-      a_bytes + b_bytes > kNoAllocScratchBytes)
-    return CORAL_ERR_NOT_SUPPORTED;  // the pieces do not fit the fixed scratch
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX || k > (size_t)INT32_MAX)
+    return CORAL_ERR_NOT_SUPPORTED;
   if (m == 0 || n == 0) return CORAL_OK;
   NoAllocDevice* d = nullptr;
   coral_status_t s = noalloc_setup(&d);
   if (s != CORAL_OK) return s;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  if (alpha == 0.0f || k == 0) {  // scale-only (sgemm_nn.rs:29-45)
+  if (alpha == 0.0f || k == 0) {  // scale-only, no scratch used (sgemm_nn.rs:29-45)
     if (beta == 1.0f) return CORAL_OK;
     unsigned g = stream_grid(m * n, 256 * 4, d->sm_count, 8);
     k_noalloc_scale<<<g, 256, 0, st>>>((int)m, (int)n, beta, c, ldc);
     return launch_status(nullptr);
   }
-  // The status word keeps the previous call's value: clear it first.
-  cudaError_t e = cudaMemsetAsync(d->status, 0, sizeof(unsigned), st);
-  if (e != cudaSuccess) return cuda_status(nullptr, e);
+  // The two pieces of each operand need 4 * (m + n) * kp bytes plus the
+  // 256-byte rounding of A's part.  Compared by division: with m, n, k up to
+  // 2^31 the product itself could wrap around 64 bits.
+  const size_t kp = (k + 7) & ~size_t(7);
+  if (m + n > ((kNoAllocScratchBytes - 256) / 4) / kp)
+    return CORAL_ERR_NOT_SUPPORTED;  // the pieces do not fit the fixed scratch
+  const size_t a_piece = m * kp, b_piece = n * kp;
+  const size_t a_bytes = (2 * a_piece * 2 + 255) & ~size_t(255);
+  // The status word is not cleared here: it collects the give-ups of every
+  // call until coral_sgemm_bf16x3_noalloc_status reads and clears it.
   __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(d->scratch);
   __nv_bfloat16* bp = reinterpret_cast<__nv_bfloat16*>(d->scratch + a_bytes);
   // Every piece element the GEMM reads is rewritten here, so stale contents
@@ -920,4 +1043,28 @@ extern "C" coral_status_t coral_sgemm_bf16x3_noalloc(void* stream, int op_a, int
       maps, (int)k, m_tiles, n_tiles, 16 * kSlabsPer64, 1, nullptr, (int)n, ep, d->status,
       kDefaultWaitLimit * 32ull);
   return launch_status(nullptr);
+}
+
+// The GEMM's bounded waits report a give-up in the fixed status word of the
+// device, not in a return value (the call returns before the kernel runs).
+// This waits for `stream`, then reads and clears that word for the current
+// device: CORAL_ERR_TIMEOUT means a C written since the last query may be
+// incomplete.  No allocation: the word is copied into a host variable.
+extern "C" coral_status_t coral_sgemm_bf16x3_noalloc_status(void* stream) {
+  using namespace coral;
+  NoAllocDevice* d = nullptr;
+  coral_status_t s = noalloc_setup(&d);
+  if (s != CORAL_OK) return s;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  unsigned word = 0;
+  cudaError_t e = cudaMemcpyAsync(&word, d->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_status(nullptr, e);
+  if (word) {
+    e = cudaMemsetAsync(d->status, 0, sizeof(unsigned), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_status(nullptr, e);
+    if (word & kStatusTimeout) return CORAL_ERR_TIMEOUT;
+  }
+  return CORAL_OK;
 }

@@ -223,6 +223,13 @@ coral_status_t coral_get_gemm_mode(coral_handle_t handle, int* mode) {
   return CORAL_OK;
 }
 
+coral_status_t coral_set_complex_mapping(coral_handle_t handle, int mapping) {
+  CORAL_HANDLE(handle);
+  if (mapping != CORAL_COMPLEX_4M && mapping != CORAL_COMPLEX_3M) return bad_arg(H, 1);
+  H->complex_mapping = mapping;
+  return CORAL_OK;
+}
+
 coral_status_t coral_set_split_chunk(coral_handle_t handle, int slabs) {
   CORAL_HANDLE(handle);
   if (slabs < 1 || slabs > 1 << 20) return bad_arg(H, 1);
@@ -505,5 +512,262 @@ coral_status_t coral_host_strsv(int uplo, int trans, int diag, size_t n, const f
   if (lx) CORAL_CUDA(H, cudaMemcpyAsync(x, dx, lx * 4, cudaMemcpyDeviceToHost, H->stream));
   return coral_sync(hh);
 }
+
+
+}  // extern "C"
+
+// ---- host-slice drop-ins built on one staging helper ---------------------
+// Each operand is a host span: copied to the thread's device staging before
+// the call when `in`, back after it when `out`.  Arguments are checked first
+// (the same positions the device entry points report), so no copy ever reads
+// past what the reference's own length checks would allow.
+namespace {
+struct Span {
+  const void* host;
+  size_t bytes;
+  bool in, out;
+  void* dev;
+};
+
+template <typename F>
+coral_status_t host_stage_call(Span* spans, int count, F&& call) {
+  HOST_PROLOGUE();
+  size_t total = 0;
+  for (int i = 0; i < count; ++i) total += up256(spans[i].bytes);
+  char* d = static_cast<char*>(thread_staging(total + 256));
+  if (!d) return CORAL_ERR_ALLOC;
+  for (int i = 0; i < count; ++i) {
+    spans[i].dev = d;
+    d += up256(spans[i].bytes);
+    if (spans[i].in && spans[i].bytes)
+      CORAL_CUDA(H, cudaMemcpyAsync(spans[i].dev, spans[i].host, spans[i].bytes,
+                                    cudaMemcpyHostToDevice, H->stream));
+  }
+  const int mode = H->pointer_mode;
+  H->pointer_mode = CORAL_POINTER_HOST;  // scalar results land in host memory
+  coral_status_t s = call(hh);
+  H->pointer_mode = mode;
+  if (s != CORAL_OK) {
+    cudaStreamSynchronize(H->stream);  // no copy in flight may outlive the call
+    return s;
+  }
+  for (int i = 0; i < count; ++i)
+    if (spans[i].out && spans[i].bytes)
+      CORAL_CUDA(H, cudaMemcpyAsync(const_cast<void*>(spans[i].host), spans[i].dev, spans[i].bytes,
+                                    cudaMemcpyDeviceToHost, H->stream));
+  return coral_sync(hh);
+}
+
+bool bad_uplo(int u) { return u != CORAL_UPPER && u != CORAL_LOWER; }
+bool bad_trans(int t) { return t < CORAL_NO_TRANSPOSE || t > CORAL_CONJ_TRANSPOSE; }
+bool bad_diag(int d) { return d != CORAL_UNIT && d != CORAL_NON_UNIT; }
+
+// GEMM operands of any element size (es bytes); arguments already checked.
+template <typename T, typename F>
+coral_status_t host_gemm(int op_a, int op_b, size_t m, size_t n, size_t k, const T* a, size_t lda,
+                         const T* b, size_t ldb, bool read_c, T* c, size_t ldc, bool complex_ops,
+                         F&& call) {
+  const int bad = gemm_bad_arg(op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, complex_ops);
+  if (bad > 0) { Handle* H = thread_handle(); if (H) H->bad_arg = bad; return CORAL_ERR_INVALID_ARG; }
+  if (bad < 0) return CORAL_ERR_NOT_SUPPORTED;
+  if (m == 0 || n == 0) return CORAL_OK;
+  const bool ta = op_a != CORAL_NO_TRANSPOSE, tb = op_b != CORAL_NO_TRANSPOSE;
+  const bool use_ab = k != 0;
+  Span sp[3] = {{a, use_ab ? mat_len(ta ? k : m, ta ? m : k, lda) * sizeof(T) : 0, true, false, nullptr},
+                {b, use_ab ? mat_len(tb ? n : k, tb ? k : n, ldb) * sizeof(T) : 0, true, false, nullptr},
+                // C is uploaded when read, and when ldc > m: the rows between its
+                // columns must come back to the caller unchanged
+                {c, mat_len(m, n, ldc) * sizeof(T), read_c || ldc > m, true, nullptr}};
+  return host_stage_call(sp, 3, [&](coral_handle_t hh) {
+    return call(hh, static_cast<const T*>(sp[0].dev), static_cast<const T*>(sp[1].dev),
+                static_cast<T*>(sp[2].dev));
+  });
+}
+}  // namespace
+
+extern "C" {
+
+#define HOST_ARG(cond, pos)                                                  \
+  do {                                                                      \
+    if (cond) {                                                             \
+      Handle* H__ = thread_handle();                                        \
+      if (H__) H__->bad_arg = (pos);                                        \
+      return CORAL_ERR_INVALID_ARG;                                         \
+    }                                                                       \
+  } while (0)
+
+coral_status_t coral_host_ssymv(int uplo, size_t n, float alpha, const float* matrix, size_t lda,
+                                const float* x, size_t incx, float beta, float* y, size_t incy) {
+  HOST_ARG(bad_uplo(uplo), 1);
+  if (n == 0) return CORAL_OK;
+  HOST_ARG(!matrix, 4); HOST_ARG(lda < n, 5); HOST_ARG(!x, 6); HOST_ARG(incx == 0, 7);
+  HOST_ARG(!y, 9); HOST_ARG(incy == 0, 10);
+  Span sp[3] = {{matrix, mat_len(n, n, lda) * 4, true, false, nullptr},
+                {x, vec_len(n, incx) * 4, true, false, nullptr},
+                {y, vec_len(n, incy) * 4, true, true, nullptr}};
+  return host_stage_call(sp, 3, [&](coral_handle_t hh) {
+    return coral_ssymv(hh, uplo, n, alpha, static_cast<const float*>(sp[0].dev), lda,
+                       static_cast<const float*>(sp[1].dev), incx, beta, static_cast<float*>(sp[2].dev),
+                       incy);
+  });
+}
+
+coral_status_t coral_host_chemv(int uplo, size_t n, const float alpha[2], const float* matrix,
+                                size_t lda, const float* x, size_t incx, const float beta[2],
+                                float* y, size_t incy) {
+  HOST_ARG(bad_uplo(uplo), 1);
+  HOST_ARG(!alpha, 3); HOST_ARG(!beta, 8);
+  if (n == 0) return CORAL_OK;
+  HOST_ARG(!matrix, 4); HOST_ARG(lda < n, 5); HOST_ARG(!x, 6); HOST_ARG(incx == 0, 7);
+  HOST_ARG(!y, 9); HOST_ARG(incy == 0, 10);
+  Span sp[3] = {{matrix, mat_len(n, n, lda) * 8, true, false, nullptr},
+                {x, vec_len(n, incx) * 8, true, false, nullptr},
+                {y, vec_len(n, incy) * 8, true, true, nullptr}};
+  return host_stage_call(sp, 3, [&](coral_handle_t hh) {
+    return coral_chemv(hh, uplo, n, alpha, static_cast<const float*>(sp[0].dev), lda,
+                       static_cast<const float*>(sp[1].dev), incx, beta, static_cast<float*>(sp[2].dev),
+                       incy);
+  });
+}
+
+coral_status_t coral_host_strmv(int uplo, int trans, int diag, size_t n, const float* matrix,
+                                size_t lda, float* x, size_t incx) {
+  HOST_ARG(bad_uplo(uplo), 1); HOST_ARG(bad_trans(trans), 2); HOST_ARG(bad_diag(diag), 3);
+  if (n == 0) return CORAL_OK;
+  HOST_ARG(!matrix, 5); HOST_ARG(lda < n, 6); HOST_ARG(!x, 7); HOST_ARG(incx == 0, 8);
+  Span sp[2] = {{matrix, mat_len(n, n, lda) * 4, true, false, nullptr},
+                {x, vec_len(n, incx) * 4, true, true, nullptr}};
+  return host_stage_call(sp, 2, [&](coral_handle_t hh) {
+    return coral_strmv(hh, uplo, trans, diag, n, static_cast<const float*>(sp[0].dev), lda,
+                       static_cast<float*>(sp[1].dev), incx);
+  });
+}
+
+coral_status_t coral_host_sger(size_t n_rows, size_t n_cols, float alpha, const float* x,
+                               size_t incx, const float* y, size_t incy, float* matrix, size_t lda) {
+  if (n_rows == 0 || n_cols == 0) return CORAL_OK;
+  HOST_ARG(!x, 4); HOST_ARG(incx == 0, 5); HOST_ARG(!y, 6); HOST_ARG(incy == 0, 7);
+  HOST_ARG(!matrix, 8); HOST_ARG(lda < n_rows, 9);
+  Span sp[3] = {{x, vec_len(n_rows, incx) * 4, true, false, nullptr},
+                {y, vec_len(n_cols, incy) * 4, true, false, nullptr},
+                {matrix, mat_len(n_rows, n_cols, lda) * 4, true, true, nullptr}};
+  return host_stage_call(sp, 3, [&](coral_handle_t hh) {
+    return coral_sger(hh, n_rows, n_cols, alpha, static_cast<const float*>(sp[0].dev), incx,
+                      static_cast<const float*>(sp[1].dev), incy, static_cast<float*>(sp[2].dev), lda);
+  });
+}
+
+coral_status_t coral_host_ssyr(int uplo, size_t n, float alpha, const float* x, size_t incx,
+                               float* matrix, size_t lda) {
+  HOST_ARG(bad_uplo(uplo), 1);
+  if (n == 0) return CORAL_OK;
+  HOST_ARG(!x, 4); HOST_ARG(incx == 0, 5); HOST_ARG(!matrix, 6); HOST_ARG(lda < n, 7);
+  Span sp[2] = {{x, vec_len(n, incx) * 4, true, false, nullptr},
+                {matrix, mat_len(n, n, lda) * 4, true, true, nullptr}};
+  return host_stage_call(sp, 2, [&](coral_handle_t hh) {
+    return coral_ssyr(hh, uplo, n, alpha, static_cast<const float*>(sp[0].dev), incx,
+                      static_cast<float*>(sp[1].dev), lda);
+  });
+}
+
+coral_status_t coral_host_ssyr2(int uplo, size_t n, float alpha, const float* x, size_t incx,
+                                const float* y, size_t incy, float* matrix, size_t lda) {
+  HOST_ARG(bad_uplo(uplo), 1);
+  if (n == 0) return CORAL_OK;
+  HOST_ARG(!x, 4); HOST_ARG(incx == 0, 5); HOST_ARG(!y, 6); HOST_ARG(incy == 0, 7);
+  HOST_ARG(!matrix, 8); HOST_ARG(lda < n, 9);
+  Span sp[3] = {{x, vec_len(n, incx) * 4, true, false, nullptr},
+                {y, vec_len(n, incy) * 4, true, false, nullptr},
+                {matrix, mat_len(n, n, lda) * 4, true, true, nullptr}};
+  return host_stage_call(sp, 3, [&](coral_handle_t hh) {
+    return coral_ssyr2(hh, uplo, n, alpha, static_cast<const float*>(sp[0].dev), incx,
+                       static_cast<const float*>(sp[1].dev), incy, static_cast<float*>(sp[2].dev), lda);
+  });
+}
+
+coral_status_t coral_host_snrm2(size_t n, const float* x, size_t incx, float* result) {
+  HOST_ARG(!result, 4);
+  if (n == 0 || incx == 0) { *result = 0.0f; return CORAL_OK; }
+  HOST_ARG(!x, 2);
+  Span sp[1] = {{x, vec_len(n, incx) * 4, true, false, nullptr}};
+  return host_stage_call(sp, 1, [&](coral_handle_t hh) {
+    return coral_snrm2(hh, n, static_cast<const float*>(sp[0].dev), incx, result);
+  });
+}
+
+coral_status_t coral_host_scopy(size_t n, const float* x, size_t incx, float* y, size_t incy) {
+  if (n == 0) return CORAL_OK;
+  HOST_ARG(!x, 2); HOST_ARG(incx == 0, 3); HOST_ARG(!y, 4); HOST_ARG(incy == 0, 5);
+  // y is read too: the stride holes between its elements keep the caller's values
+  Span sp[2] = {{x, vec_len(n, incx) * 4, true, false, nullptr},
+                {y, vec_len(n, incy) * 4, incy > 1, true, nullptr}};
+  return host_stage_call(sp, 2, [&](coral_handle_t hh) {
+    return coral_scopy(hh, n, static_cast<const float*>(sp[0].dev), incx, static_cast<float*>(sp[1].dev),
+                       incy);
+  });
+}
+
+coral_status_t coral_host_sswap(size_t n, float* x, size_t incx, float* y, size_t incy) {
+  if (n == 0) return CORAL_OK;
+  HOST_ARG(!x, 2); HOST_ARG(incx == 0, 3); HOST_ARG(!y, 4); HOST_ARG(incy == 0, 5);
+  Span sp[2] = {{x, vec_len(n, incx) * 4, true, true, nullptr},
+                {y, vec_len(n, incy) * 4, true, true, nullptr}};
+  return host_stage_call(sp, 2, [&](coral_handle_t hh) {
+    return coral_sswap(hh, n, static_cast<float*>(sp[0].dev), incx, static_cast<float*>(sp[1].dev), incy);
+  });
+}
+
+coral_status_t coral_host_sscal(size_t n, float alpha, float* x, size_t incx) {
+  if (n == 0 || incx == 0) return CORAL_OK;
+  HOST_ARG(!x, 3);
+  Span sp[1] = {{x, vec_len(n, incx) * 4, true, true, nullptr}};
+  return host_stage_call(sp, 1, [&](coral_handle_t hh) {
+    return coral_sscal(hh, n, alpha, static_cast<float*>(sp[0].dev), incx);
+  });
+}
+
+coral_status_t coral_host_dgemm(int op_a, int op_b, size_t m, size_t n, size_t k, double alpha,
+                                const double* a, size_t lda, const double* b, size_t ldb,
+                                double beta, double* c, size_t ldc) {
+  return host_gemm<double>(op_a, op_b, m, n, k, a, lda, b, ldb, beta != 0.0, c, ldc, false,
+                           [&](coral_handle_t hh, const double* da, const double* db, double* dc) {
+                             return coral_dgemm(hh, op_a, op_b, m, n, k, alpha, da, lda, db, ldb,
+                                                beta, dc, ldc);
+                           });
+}
+
+coral_status_t coral_host_cgemm(int op_a, int op_b, size_t m, size_t n, size_t k,
+                                const float alpha[2], const float* a, size_t lda, const float* b,
+                                size_t ldb, const float beta[2], float* c, size_t ldc) {
+  HOST_ARG(!alpha, 6); HOST_ARG(!beta, 11);
+  struct C64 { float re, im; };
+  return host_gemm<C64>(op_a, op_b, m, n, k, reinterpret_cast<const C64*>(a), lda,
+                        reinterpret_cast<const C64*>(b), ldb, beta[0] != 0.f || beta[1] != 0.f,
+                        reinterpret_cast<C64*>(c), ldc, true,
+                        [&](coral_handle_t hh, const C64* da, const C64* db, C64* dc) {
+                          return coral_cgemm(hh, op_a, op_b, m, n, k, alpha,
+                                             reinterpret_cast<const float*>(da), lda,
+                                             reinterpret_cast<const float*>(db), ldb, beta,
+                                             reinterpret_cast<float*>(dc), ldc);
+                        });
+}
+
+coral_status_t coral_host_zgemm(int op_a, int op_b, size_t m, size_t n, size_t k,
+                                const double alpha[2], const double* a, size_t lda, const double* b,
+                                size_t ldb, const double beta[2], double* c, size_t ldc) {
+  HOST_ARG(!alpha, 6); HOST_ARG(!beta, 11);
+  struct C128 { double re, im; };
+  return host_gemm<C128>(op_a, op_b, m, n, k, reinterpret_cast<const C128*>(a), lda,
+                         reinterpret_cast<const C128*>(b), ldb, beta[0] != 0.0 || beta[1] != 0.0,
+                         reinterpret_cast<C128*>(c), ldc, true,
+                         [&](coral_handle_t hh, const C128* da, const C128* db, C128* dc) {
+                           return coral_zgemm(hh, op_a, op_b, m, n, k, alpha,
+                                              reinterpret_cast<const double*>(da), lda,
+                                              reinterpret_cast<const double*>(db), ldb, beta,
+                                              reinterpret_cast<double*>(dc), ldc);
+                         });
+}
+
+#undef HOST_ARG
 
 }  // extern "C"

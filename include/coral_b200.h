@@ -70,6 +70,15 @@ enum {
   CORAL_GEMM_SPLIT_BF16X6 = 3  /* s/c: 3-way BF16 split, 6 tcgen05 products */
 };
 
+/* How the emulated complex GEMMs (coral_cgemm in the split-BF16 modes) map
+ * onto real tensor-core products. */
+enum {
+  CORAL_COMPLEX_4M = 0, /* one real GEMM of m x 2n x 2k: Re and Im exact per term */
+  CORAL_COMPLEX_3M = 1  /* three real GEMMs of m x n x k (3/4 of the work); the
+                           imaginary part is T3 - T1 - T2, with its error bounded
+                           by (|Re A| + |Im A|)(|Re B| + |Im B|) */
+};
+
 typedef struct coral_handle_s* coral_handle_t;
 
 /* ---- handle ------------------------------------------------------------ */
@@ -84,6 +93,8 @@ coral_status_t coral_get_gemm_mode(coral_handle_t handle, int* mode);
 /* K depth, in 64-element slabs, of each tensor-core accumulation chunk of the
  * split-BF16 GEMMs before it is added into fp32 registers (default 16). */
 coral_status_t coral_set_split_chunk(coral_handle_t handle, int slabs);
+/* Complex mapping of the split-BF16 CGEMM: CORAL_COMPLEX_4M (default) or 3M. */
+coral_status_t coral_set_complex_mapping(coral_handle_t handle, int mapping);
 /* Iteration limit of every bounded device wait (0 restores the default). */
 coral_status_t coral_set_wait_limit(coral_handle_t handle, uint64_t spins);
 /* Kernel timing: when enabled, the handle brackets the dominant kernel of each
@@ -405,9 +416,29 @@ enum { CORAL_INPUT_F32 = 0, CORAL_INPUT_BF16 = 1 };
 /* Computes every instance of `problems` (an array of `count` descriptors in
  * DEVICE memory) with coral_sgemm's semantics; bf16 inputs accumulate in
  * fp32.  A fixed number of kernels, no host work per instance: capturable in
- * a CUDA graph once a first uncaptured call has sized the handle's scratch. */
+ * a CUDA graph once a first uncaptured call has sized the handle's scratch.
+ * bf16 inputs, and fp32 inputs when the handle's GEMM mode is
+ * CORAL_GEMM_SPLIT_BF16X3, run on the tensor cores (fp32 as split-BF16x3);
+ * fp32 inputs in the other modes run on FP32 FMA tiles.  On the tensor-core
+ * path each instance's N tile width comes from the handle's grouped policy
+ * (coral_set_grouped_config), unless its `reserved` field is 64, 128 or 256. */
 coral_status_t coral_sgemm_grouped(coral_handle_t h, int input_type, size_t count,
                                    const coral_sgemm_problem_t* problems);
+/* Tensor-core grouped GEMM tile widths (64, 128 or 256) for the instance
+ * classes n <= 64, n <= 128, n <= 256, n > 256; NULL restores the default
+ * {64, 128, 128, 256}. */
+coral_status_t coral_set_grouped_config(coral_handle_t h, const int tile_n[4]);
+coral_status_t coral_get_grouped_config(coral_handle_t h, int tile_n[4]);
+/* Exhaustive tuning of that policy on one batch (descriptors in DEVICE
+ * memory): all 36 assignments (class 0 and 1 in {64, 128}, class 2 and 3 in
+ * {64, 128, 256}; class 0 varies slowest) run once untimed and `reps` times
+ * between CUDA events; per-candidate milliseconds go to ms_out[36], the
+ * fastest index to `best` and its widths to tile_n, and that policy is
+ * installed on the handle.  fp32 inputs are tuned in split-BF16x3 mode.  The
+ * instances' C is overwritten. */
+coral_status_t coral_autotune_sgemm_grouped(coral_handle_t h, int input_type, size_t count,
+                                            const coral_sgemm_problem_t* problems, int reps,
+                                            float* ms_out, int* best, int tile_n[4]);
 /* One instance of a batched STRSV: the arguments of coral_strsv. */
 typedef struct coral_strsv_problem {
   int32_t uplo, trans, diag, n;
@@ -485,11 +516,21 @@ coral_status_t coral_set_selector(coral_handle_t h, coral_mlp_t mlp);
  *   - All calls share the one array: calls whose work can overlap on the GPU
  *     (different streams, or other host threads) race on it and must be
  *     serialised by the caller.
+ *   - alpha == 0 or k == 0 only scales C by beta and uses no scratch, so it
+ *     is accepted at any size; m == 0 or n == 0 returns at once.
+ *   - The kernel's bounded waits cannot report through the return value (the
+ *     call returns before the kernel runs): a give-up sets a fixed device
+ *     status word, read by coral_sgemm_bf16x3_noalloc_status.
  * Device pointers; asynchronous on `stream`. */
 coral_status_t coral_sgemm_bf16x3_noalloc(void* stream, int op_a, int op_b, size_t m, size_t n,
                                           size_t k, float alpha, const float* a, size_t lda,
                                           const float* b, size_t ldb, float beta, float* c,
                                           size_t ldc);
+/* Waits for `stream`, then reads and clears the current device's status word
+ * of coral_sgemm_bf16x3_noalloc: CORAL_ERR_TIMEOUT when a call since the last
+ * query gave up a bounded wait (its C may be incomplete), else CORAL_OK.
+ * Allocates nothing. */
+coral_status_t coral_sgemm_bf16x3_noalloc_status(void* stream);
 
 /* ---- host-slice drop-ins: the reference's exact argument lists ---------- */
 /* Pointers are HOST memory.  Return value as above; scalar-returning routines
@@ -508,6 +549,46 @@ coral_status_t coral_host_saxpy(size_t n, float alpha, const float* x, size_t in
 coral_status_t coral_host_isamax(size_t n, const float* x, size_t incx, size_t* index);
 coral_status_t coral_host_strsv(int uplo, int trans, int diag, size_t n,
                                 const float* matrix, size_t lda, float* x, size_t incx);
+/* level2/ssymv.rs:99-110 */
+coral_status_t coral_host_ssymv(int uplo, size_t n, float alpha, const float* matrix, size_t lda,
+                                const float* x, size_t incx, float beta, float* y, size_t incy);
+/* level2/chemv.rs:96-107 -- interleaved complex64, complex scalars [re, im] */
+coral_status_t coral_host_chemv(int uplo, size_t n, const float alpha[2], const float* matrix,
+                                size_t lda, const float* x, size_t incx, const float beta[2],
+                                float* y, size_t incy);
+/* level2/strmv.rs:59-73 */
+coral_status_t coral_host_strmv(int uplo, int trans, int diag, size_t n, const float* matrix,
+                                size_t lda, float* x, size_t incx);
+/* level2/sger.rs:68-78 */
+coral_status_t coral_host_sger(size_t n_rows, size_t n_cols, float alpha, const float* x,
+                               size_t incx, const float* y, size_t incy, float* matrix, size_t lda);
+/* level2/ssyr.rs:63-71 */
+coral_status_t coral_host_ssyr(int uplo, size_t n, float alpha, const float* x, size_t incx,
+                               float* matrix, size_t lda);
+/* level2/ssyr2.rs:59-69 */
+coral_status_t coral_host_ssyr2(int uplo, size_t n, float alpha, const float* x, size_t incx,
+                                const float* y, size_t incy, float* matrix, size_t lda);
+/* level1/snrm2.rs:45-149 -- result through the out-pointer */
+coral_status_t coral_host_snrm2(size_t n, const float* x, size_t incx, float* result);
+/* level1/scopy.rs:28-58 */
+coral_status_t coral_host_scopy(size_t n, const float* x, size_t incx, float* y, size_t incy);
+/* level1/sswap.rs:35-118 */
+coral_status_t coral_host_sswap(size_t n, float* x, size_t incx, float* y, size_t incy);
+/* level1/sscal.rs:30-66 */
+coral_status_t coral_host_sscal(size_t n, float alpha, float* x, size_t incx);
+/* level3/dgemm.rs:107 -- arithmetic per coral_host_set_gemm_mode */
+coral_status_t coral_host_dgemm(int op_a, int op_b, size_t m, size_t n, size_t k, double alpha,
+                                const double* a, size_t lda, const double* b, size_t ldb,
+                                double beta, double* c, size_t ldc);
+/* level3/cgemm.rs:127-157 -- interleaved complex64 */
+coral_status_t coral_host_cgemm(int op_a, int op_b, size_t m, size_t n, size_t k,
+                                const float alpha[2], const float* a, size_t lda, const float* b,
+                                size_t ldb, const float beta[2], float* c, size_t ldc);
+/* level3/zgemm.rs:123 -- interleaved complex128 */
+coral_status_t coral_host_zgemm(int op_a, int op_b, size_t m, size_t n, size_t k,
+                                const double alpha[2], const double* a, size_t lda,
+                                const double* b, size_t ldb, const double beta[2], double* c,
+                                size_t ldc);
 /* Select the GEMM arithmetic of this thread's internal handle. */
 coral_status_t coral_host_set_gemm_mode(int mode);
 

@@ -114,3 +114,23 @@ def test_sgemm_bf16x3_8192_meets_1e6(cuda, ill):
 
 def test_sgemm_bf16x3_8192_tt(cuda):
     assert _headline(cb.GemmMode.SPLIT_BF16X3, False, ops=(1, 1)) <= 1e-6
+
+
+@pytest.mark.parametrize("mode,tol", MODES)
+@pytest.mark.parametrize("shape", [(1, 1, 1), (5, 7, 4), (127, 129, 65), (64, 200, 301), (300, 260, 700)])
+@pytest.mark.parametrize("ops", [(a, b) for a in (0, 1, 2) for b in (0, 1, 2)])
+def test_cgemm_split_3m(cuda, mode, tol, shape, ops):
+    """3M mapping: Re = T1 - T2, Im = T3 - T1 - T2 from three real split
+    GEMMs.  Against the same component-wise bound as 4M, with three times
+    the 4M tolerance: the Im error is bounded by
+    (|Re A| + |Im A|)(|Re B| + |Im B|) <= 2 |A||B| plus the T1, T2 terms."""
+    h = cb.handle()
+    cb.set_gemm_mode(mode)
+    h.set_complex_mapping(1)
+    try:
+        m, n, k = shape
+        sample = 4096 if m * n > 50000 else None
+        gemm_case(cb.cgemm, np.complex64, *ops, m, n, k, 1.5 - 0.5j, 0.25 + 1j, 6 * tol, sample=sample)
+        gemm_case(cb.cgemm, np.complex64, *ops, m, n, k, 1.0, 0.0, 6 * tol, sample=sample)
+    finally:
+        h.set_complex_mapping(0)

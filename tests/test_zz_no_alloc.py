@@ -73,6 +73,55 @@ def test_noalloc_matches_existing_entry_point_twice(cuda):
     _run_pair(1, 1, 129, 77, 1000, -0.75, 0.0, seed=2)
 
 
+def _call(lib, m, n, k, alpha, A, B, beta, Cd, stream=None):
+    return lib.coral_sgemm_bf16x3_noalloc(stream, 0, 0, m, n, k, alpha, C.c_void_p(A.data_ptr()),
+                                          max(m, 1), C.c_void_p(B.data_ptr()), max(k, 1), beta,
+                                          C.c_void_p(Cd.data_ptr()), max(m, 1))
+
+
+@pytest.mark.parametrize("m,n,k", [(300, 200, 0), (4096, 4096, 4096)])
+@pytest.mark.parametrize("beta", [0.0, 1.0, -0.5])
+def test_noalloc_scale_only(cuda, m, n, k, beta):
+    """alpha == 0 or k == 0 only scales C (sgemm_nn.rs:29-45) and uses no
+    scratch, so it succeeds even where the pieces would not fit: beta == 0
+    writes zeros, beta == 1 leaves C as it was, other beta scale C."""
+    lib = _lib.load()
+    A = torch.ones(max(m * k, 1), device="cuda")
+    B = torch.ones(max(k * n, 1), device="cuda")
+    c = np.random.default_rng(3).uniform(-1, 1, m * n).astype(np.float32)
+    Cd = torch.from_numpy(c).cuda()
+    alpha = 0.0 if k else 2.0
+    assert _call(lib, m, n, k, alpha, A, B, beta, Cd) == 0
+    torch.cuda.synchronize()
+    got = Cd.cpu().numpy()
+    want = np.zeros_like(c) if beta == 0.0 else (c if beta == 1.0 else c * np.float32(beta))
+    np.testing.assert_array_equal(got, want)
+
+
+def test_noalloc_empty_and_huge_sizes(cuda):
+    """m == 0 returns at once whatever k is; sizes whose byte count would
+    wrap 64 bits are rejected by the size check, not let through."""
+    lib = _lib.load()
+    assert lib.coral_sgemm_bf16x3_noalloc(None, 0, 0, 0, 4096, 1 << 30, 1.0, None, 1, None,
+                                          1 << 30, 0.0, None, 1) == 0
+    buf = torch.zeros(4, device="cuda")
+    p = C.c_void_p(buf.data_ptr())
+    big = (1 << 31) - 1
+    # m = n = 2^31 - 1, k = 2^31 - 1: 4 (m + n) kp is about 2^66 bytes
+    assert lib.coral_sgemm_bf16x3_noalloc(None, 0, 0, big, big, big, 1.0, p, big, p, big, 0.0, p,
+                                          big) == 5
+    torch.cuda.synchronize()
+    assert float(buf.abs().sum()) == 0.0
+
+
+def test_noalloc_status_reads_clear_after_normal_calls(cuda):
+    lib = _lib.load()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _run_pair(0, 1, 64, 96, 40, 1.0, 1.0, seed=4)
+    assert lib.coral_sgemm_bf16x3_noalloc_status(stream) == 0
+    assert lib.coral_sgemm_bf16x3_noalloc_status(None) == 0
+
+
 def test_noalloc_rejects_sizes_beyond_fixed_scratch(cuda):
     lib = _lib.load()
     m = n = k = 4096  # pieces need 4 * 8192 * 4096 bytes = 128 MiB > 32 MiB
