@@ -274,13 +274,34 @@ def precision_set(torch, cb, h, dev, g):
     C0 = torch.empty(m * m, dtype=torch.complex128, device=dev)
     C0.real.uniform_(-1, 1, generator=g); C0.imag.uniform_(-1, 1, generator=g)
     Cm = C0.clone()
-    for mode, name in ((cb.GemmMode.NATIVE, "native"), (cb.GemmMode.OZAKI_INT8, "ozaki_int8")):
+    for mode, name, mapping in ((cb.GemmMode.NATIVE, "native", 0), (cb.GemmMode.OZAKI_INT8, "ozaki_int8", 0),
+                                (cb.GemmMode.OZAKI_INT8, "ozaki_int8_3m", 1)):
         h.set_gemm_mode(mode)
+        h.set_complex_mapping(mapping)
         f = lambda: cb.zgemm(2, 2, m, m, m, 1.5 - 0.5j, A, m, B, m, 0.25 + 1j, Cm, m)  # noqa: E731
         err = sample_err(f, 2, m, m, m, 1.5 - 0.5j, A, m, B, m, 0.25 + 1j, C0, Cm, m, True)
         ms = run(f)
         out[f"zgemm_cc_2048_{name}"] = {"ms": ms, "tflops": 8.0 * m ** 3 / (ms * 1e-3) / 1e12,
                                         "max_rel_componentwise": err}
+    h.set_complex_mapping(0)
+    del A, B, C0, Cm
+    # CGEMM CC 2048^3 complex64, split-BF16x3 through the 4M and the 3M mapping
+    A = torch.empty(m * m, dtype=torch.complex64, device=dev)
+    A.real.uniform_(-1, 1, generator=g); A.imag.uniform_(-1, 1, generator=g)
+    B = torch.empty(m * m, dtype=torch.complex64, device=dev)
+    B.real.uniform_(-1, 1, generator=g); B.imag.uniform_(-1, 1, generator=g)
+    C0 = torch.empty(m * m, dtype=torch.complex64, device=dev)
+    C0.real.uniform_(-1, 1, generator=g); C0.imag.uniform_(-1, 1, generator=g)
+    Cm = C0.clone()
+    h.set_gemm_mode(cb.GemmMode.SPLIT_BF16X3)
+    for name, mapping in (("split_bf16x3_4m", 0), ("split_bf16x3_3m", 1)):
+        h.set_complex_mapping(mapping)
+        f = lambda: cb.cgemm(2, 2, m, m, m, 1.5 - 0.5j, A, m, B, m, 0.25 + 1j, Cm, m)  # noqa: E731
+        err = sample_err(f, 2, m, m, m, 1.5 - 0.5j, A, m, B, m, 0.25 + 1j, C0, Cm, m, True)
+        ms = run(f)
+        out[f"cgemm_cc_2048_{name}"] = {"ms": ms, "tflops": 8.0 * m ** 3 / (ms * 1e-3) / 1e12,
+                                        "max_rel_componentwise": err}
+    h.set_complex_mapping(0)
     del A, B, C0, Cm
     # SGEMM TT 8192^3 split-BF16x3
     m = 8192

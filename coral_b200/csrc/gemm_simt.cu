@@ -19,6 +19,7 @@
 #include "common.cuh"
 
 #include <cuComplex.h>
+#include <type_traits>
 
 namespace coral {
 
@@ -246,6 +247,14 @@ int gemm_bad_arg(int op_a, int op_b, size_t m, size_t n, size_t k, const void* a
 }
 
 template <typename T>
+coral_status_t enqueue_gemm_tma_fma(Handle* h, int op_a, int op_b, size_t m, size_t n, size_t k, T alpha,
+                                    const T* A, size_t lda, const T* B, size_t ldb, T beta, T* C,
+                                    size_t ldc);
+
+// Real types take the TMA-fed kernel (gemm_tma_fma.cu) whenever tensor maps
+// can describe the operands, the register-staged kernel below otherwise;
+// complex types always take the register-staged kernel.
+template <typename T>
 coral_status_t enqueue_gemm_simt(Handle* h, int op_a, int op_b, size_t m, size_t n, size_t k,
                                  T alpha, const T* A, size_t lda, const T* B, size_t ldb, T beta,
                                  T* C, size_t ldc) {
@@ -255,6 +264,10 @@ coral_status_t enqueue_gemm_simt(Handle* h, int op_a, int op_b, size_t m, size_t
     unsigned g = stream_grid(m * n, 256 * 4, h->sm_count, 8);
     k_scale_c<T><<<g, 256, 0, h->stream>>>((int)m, (int)n, beta, C, ldc);
     return launch_status(h);
+  }
+  if constexpr (std::is_same<T, float>::value || std::is_same<T, double>::value) {
+    const coral_status_t s = enqueue_gemm_tma_fma<T>(h, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    if (s != CORAL_ERR_NOT_SUPPORTED) return s;
   }
   constexpr int BM = 16 * SimtCfg<T>::TM, BN = 16 * SimtCfg<T>::TN;
   dim3 grid((unsigned)((m + BM - 1) / BM), (unsigned)((n + BN - 1) / BN));

@@ -64,7 +64,8 @@ bool encode_kmajor_map(CUtensorMap* map, const void* base, int elem_bytes, uint6
   cuuint64_t strides[1] = {row_stride_bytes};
   cuuint32_t box[2] = {box_inner, box_outer};
   cuuint32_t estr[2] = {1, 1};
-  CUtensorMapDataType dt = elem_bytes == 4   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+  CUtensorMapDataType dt = elem_bytes == 8   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                           : elem_bytes == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                            : elem_bytes == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
                                              : CU_TENSOR_MAP_DATA_TYPE_UINT8;
   CUresult r = fn(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
@@ -90,17 +91,42 @@ __device__ __forceinline__ uint64_t slab_desc(uint32_t saddr) {
 }
 
 template <int P> struct SplitPlan;
-// pairs (i, j): product A_i * B_j, smallest terms first
+// Products A_a(q) * B_b(q), small terms first, with the products that share an
+// A piece adjacent so the tensor core keeps that piece in its A collector
+// buffer (collect(q): fill, use, last use) instead of reading it again.
 template <> struct SplitPlan<3> {
   static constexpr int kPieces = 2, kProducts = 3;
+  // A1 B0, A0 B1 (fill A0), A0 B0 (last use of A0)
   __host__ __device__ static constexpr int a(int q) { return q == 0 ? 1 : 0; }
   __host__ __device__ static constexpr int b(int q) { return q == 1 ? 1 : 0; }
+  __host__ __device__ static constexpr int collect(int q) {
+    return q == 1 ? tc::kCollectFill : q == 2 ? tc::kCollectLastUse : tc::kCollectNone;
+  }
 };
 template <> struct SplitPlan<6> {
   static constexpr int kPieces = 3, kProducts = 6;
-  __host__ __device__ static constexpr int a(int q) { return q == 0 ? 2 : (q == 2 || q == 3) ? 1 : 0; }
-  __host__ __device__ static constexpr int b(int q) { return q == 1 ? 2 : (q == 2 || q == 4) ? 1 : 0; }
+  // A2 B0, A1 B1 (fill A1), A1 B0 (last use), A0 B2 (fill A0), A0 B1, A0 B0 (last use)
+  __host__ __device__ static constexpr int a(int q) { return q == 0 ? 2 : q <= 2 ? 1 : 0; }
+  __host__ __device__ static constexpr int b(int q) { return q == 3 ? 2 : (q == 1 || q == 4) ? 1 : 0; }
+  __host__ __device__ static constexpr int collect(int q) {
+    return (q == 1 || q == 3) ? tc::kCollectFill
+           : q == 4           ? tc::kCollectUse
+           : (q == 2 || q == 5) ? tc::kCollectLastUse
+                              : tc::kCollectNone;
+  }
 };
+
+// Issues product q of a split plan with its collector usage.
+template <typename Plan>
+__device__ __forceinline__ void mma_plan(int q, uint32_t acc, uint64_t ad, uint64_t bd, uint32_t idesc,
+                                         uint32_t accumulate) {
+  switch (Plan::collect(q)) {
+    case tc::kCollectFill: tc::mma_f16_ca<tc::kCollectFill>(acc, ad, bd, idesc, accumulate); break;
+    case tc::kCollectUse: tc::mma_f16_ca<tc::kCollectUse>(acc, ad, bd, idesc, accumulate); break;
+    case tc::kCollectLastUse: tc::mma_f16_ca<tc::kCollectLastUse>(acc, ad, bd, idesc, accumulate); break;
+    default: tc::mma_f16(acc, ad, bd, idesc, accumulate); break;
+  }
+}
 
 struct SplitMaps {
   CUtensorMap a[3];
@@ -554,7 +580,7 @@ k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int 
               for (int q = 0; q < Plan::kProducts; ++q) {
                 const uint64_t ad = slab_desc(sa + Plan::a(q) * kATile + kk * 32);
                 const uint64_t bd = slab_desc(sb + Plan::b(q) * kBTile + kk * 32);
-                tc::mma_f16(acc, ad, bd, kIdesc, ((kb - kb0) | kk | q) != 0);
+                mma_plan<Plan>(q, acc, ad, bd, kIdesc, ((kb - kb0) | kk | q) != 0);
               }
             }
             tc::mma_commit(&empty_bar[s]);

@@ -62,14 +62,19 @@ constexpr uint32_t kBPieceBytes = kMaxBN * kTK * 2;    // 16 KiB
 template <int NPC> struct TcCfg;
 template <> struct TcCfg<2> {
   static constexpr int kStages = 4, kProducts = 3;
-  // (A piece, B piece) per product, smallest terms first: A1 B0, A0 B1, A0 B0
+  // (A piece, B piece) per product, smallest terms first: A1 B0, A0 B1, A0 B0;
+  // A0 stays in the tensor core's A collector between its two products
   __device__ static constexpr int a(int q) { return q == 0 ? 1 : 0; }
   __device__ static constexpr int b(int q) { return q == 1 ? 1 : 0; }
+  __device__ static constexpr int collect(int q) {
+    return q == 1 ? tc::kCollectFill : q == 2 ? tc::kCollectLastUse : tc::kCollectNone;
+  }
 };
 template <> struct TcCfg<1> {
   static constexpr int kStages = 8, kProducts = 1;
   __device__ static constexpr int a(int) { return 0; }
   __device__ static constexpr int b(int) { return 0; }
+  __device__ static constexpr int collect(int) { return tc::kCollectNone; }
 };
 
 template <int NPC>
@@ -393,7 +398,14 @@ k_gemm_grouped_tc(const coral_sgemm_problem_t* __restrict__ probs, int count,
               for (int q = 0; q < Cfg::kProducts; ++q) {
                 const uint64_t ad = tc::desc_k_sw64(sa + Cfg::a(q) * kAPieceBytes + kk * 32);
                 const uint64_t bd = tc::desc_k_sw64(sb + Cfg::b(q) * kBPieceBytes + kk * 32);
-                tc::mma_f16(acc, ad, bd, idesc, ((kb - kb0) | kk | q) != 0);
+                const uint32_t accum = ((kb - kb0) | kk | q) != 0;
+                switch (Cfg::collect(q)) {
+                  case tc::kCollectFill: tc::mma_f16_ca<tc::kCollectFill>(acc, ad, bd, idesc, accum); break;
+                  case tc::kCollectLastUse:
+                    tc::mma_f16_ca<tc::kCollectLastUse>(acc, ad, bd, idesc, accum);
+                    break;
+                  default: tc::mma_f16(acc, ad, bd, idesc, accum); break;
+                }
               }
             }
             tc::mma_commit(&empty_bar[s]);

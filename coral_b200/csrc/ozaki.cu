@@ -20,7 +20,9 @@
 //   4. Epilogue: C = alpha * 2^(e_i + f_j) * acc + beta * C in FP64 (beta == 0
 //      does not read C, as f64_edge / f32_edge.rs:37-58 do).
 // Complex operands (ZGEMM) use the same 4M folding as the split-BF16 CGEMM:
-// A'' = [Re A | Im A], B'' rows (2j, 2j+1) = ([Re B_j | -Im B_j], [Im B_j | Re B_j]).
+// A'' = [Re A | Im A], B'' rows (2j, 2j+1) = ([Re B_j | -Im B_j], [Im B_j | Re B_j]);
+// or, with the handle's complex mapping set to 3M, three real Ozaki GEMMs
+// combined as Re = T1 - T2, Im = T3 - T1 - T2 (zgemm_ozaki_3m).
 //
 // Pipeline: warp 0 lane 0 = TMA producer (2 stages of S slices of A and B,
 // 64-byte K slabs, 64-byte swizzle); warp 1 lane 0 = MMA issuer (kind::i8,
@@ -476,7 +478,19 @@ coral_status_t run_ozaki_gemm(Handle* h, const int8_t* ap, size_t a_piece, int m
 
 constexpr int kOzSlices = 7;
 
-coral_status_t dgemm_ozaki_impl(Handle* h, int op_a, int op_b, size_t m, size_t n, size_t k,
+// Device bytes the real Ozaki GEMM needs for its slices and exponents.
+size_t dgemm_ozaki_bytes(size_t m, size_t n, size_t k) {
+  constexpr int S = kOzSlices;
+  const size_t kp = (k + 15) & ~size_t(15);
+  const size_t a_bytes = (S * m * kp + 1023) & ~size_t(1023);
+  const size_t b_bytes = (S * n * kp + 1023) & ~size_t(1023);
+  const size_t e_bytes = ((m + n) * sizeof(int) + 255) & ~size_t(255);
+  return a_bytes + b_bytes + e_bytes;
+}
+
+// The real Ozaki GEMM with its slices and exponents in `sc`
+// (dgemm_ozaki_bytes(m, n, k) bytes, 1024-byte aligned).
+coral_status_t dgemm_ozaki_core(Handle* h, char* sc, int op_a, int op_b, size_t m, size_t n, size_t k,
                                 double alpha, const double* A, size_t lda, const double* B,
                                 size_t ldb, double beta, double* C, size_t ldc) {
   constexpr int S = kOzSlices;
@@ -484,9 +498,6 @@ coral_status_t dgemm_ozaki_impl(Handle* h, int op_a, int op_b, size_t m, size_t 
   const size_t a_piece = m * kp, b_piece = n * kp;
   const size_t a_bytes = (S * a_piece + 1023) & ~size_t(1023);
   const size_t b_bytes = (S * b_piece + 1023) & ~size_t(1023);
-  const size_t e_bytes = ((m + n) * sizeof(int) + 255) & ~size_t(255);
-  char* sc = static_cast<char*>(scratch(h, a_bytes + b_bytes + e_bytes));
-  if (!sc) return CORAL_ERR_ALLOC;
   int8_t* ap = reinterpret_cast<int8_t*>(sc);
   int8_t* bp = reinterpret_cast<int8_t*>(sc + a_bytes);
   int* ea = reinterpret_cast<int*>(sc + a_bytes + b_bytes);
@@ -506,6 +517,116 @@ coral_status_t dgemm_ozaki_impl(Handle* h, int op_a, int op_b, size_t m, size_t 
   if ((s = launch_status(h)) != CORAL_OK) return s;
   OzEpi ep{C, ldc, (int)m, (int)n, ea, eb, alpha, 0.0, beta, 0.0, 0};
   return run_ozaki_gemm<S>(h, ap, a_piece, (int)m, bp, b_piece, (int)n, (int)k, kp, ep);
+}
+
+coral_status_t dgemm_ozaki_impl(Handle* h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                                double alpha, const double* A, size_t lda, const double* B,
+                                size_t ldb, double beta, double* C, size_t ldc) {
+  char* sc = static_cast<char*>(scratch(h, dgemm_ozaki_bytes(m, n, k)));
+  if (!sc) return CORAL_ERR_ALLOC;
+  return dgemm_ozaki_core(h, sc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+// 3M operands: the real matrices Re, Im and Re + Im of op(X) (conjugated when
+// `conj`), R x L, column-major with leading dimension R.  Element (r, l) of
+// op(X) is X[r + l * ld] (trans == false) or X[l + r * ld]; 32 x 32 tiles
+// through shared memory so both the loads and the stores are coalesced.
+__global__ void __launch_bounds__(256)
+k_cplx_parts(const double2* __restrict__ X, size_t ld, bool trans, bool conj, int R, int L,
+             double* __restrict__ re, double* __restrict__ im, double* __restrict__ sum) {
+  __shared__ double2 tile[32][33];
+  const int r0 = blockIdx.y * 32, l0 = blockIdx.x * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    if (trans) {  // contiguous along l
+      const int r = r0 + ty + 8 * q, l = l0 + tx;
+      if (r < R && l < L) tile[ty + 8 * q][tx] = X[l + (size_t)r * ld];
+    } else {      // contiguous along r
+      const int l = l0 + ty + 8 * q, r = r0 + tx;
+      if (r < R && l < L) tile[tx][ty + 8 * q] = X[r + (size_t)l * ld];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int l = l0 + ty + 8 * q, r = r0 + tx;
+    if (r < R && l < L) {
+      double2 v = tile[tx][ty + 8 * q];
+      if (conj) v.y = -v.y;
+      const size_t o = r + (size_t)l * R;
+      re[o] = v.x;
+      im[o] = v.y;
+      sum[o] = v.x + v.y;
+    }
+  }
+}
+
+// C = alpha (T1 - T2 + i (T3 - T1 - T2)) + beta C, T* m x n with ld m.
+__global__ void k_combine_3m_z(const double* __restrict__ t1, const double* __restrict__ t2,
+                               const double* __restrict__ t3, int m, int n, double2 alpha, double2 beta,
+                               double2* __restrict__ C, size_t ldc) {
+  const size_t total = (size_t)m * n;
+  const bool beta0 = beta.x == 0.0 && beta.y == 0.0;
+  const bool beta1 = beta.x == 1.0 && beta.y == 0.0;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const double a = t1[t], b = t2[t], c3 = t3[t];
+    const double re = a - b, im = c3 - a - b;
+    double2 v = make_double2(alpha.x * re - alpha.y * im, alpha.x * im + alpha.y * re);
+    double2* cp = C + t % m + (t / m) * ldc;
+    if (!beta0) {
+      const double2 cv = *cp;
+      if (beta1) { v.x += cv.x; v.y += cv.y; }
+      else {
+        v.x += beta.x * cv.x - beta.y * cv.y;
+        v.y += beta.x * cv.y + beta.y * cv.x;
+      }
+    }
+    *cp = v;
+  }
+}
+
+// ZGEMM by the 3M mapping: three real Ozaki GEMMs of m x n x k (Re A Re B,
+// Im A Im B, (Re A + Im A)(Re B + Im B)) into fp64 workspace, then the
+// combine.  Three quarters of the 4M work; Im C = T3 - T1 - T2, whose error is
+// bounded by (|Re A| + |Im A|)(|Re B| + |Im B|) instead of |A| |B| per term.
+coral_status_t zgemm_ozaki_3m(Handle* h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                              double2 alpha, const double2* A, size_t lda, const double2* B,
+                              size_t ldb, double2 beta, double2* C, size_t ldc) {
+  auto up = [](size_t b) { return (b + 1023) & ~size_t(1023); };
+  const size_t pa = up(m * k * sizeof(double)), pb = up(k * n * sizeof(double));
+  const size_t pt = up(m * n * sizeof(double));
+  const size_t oz = dgemm_ozaki_bytes(m, n, k);
+  char* sc = static_cast<char*>(scratch(h, 3 * pa + 3 * pb + 3 * pt + oz));
+  if (!sc) return CORAL_ERR_ALLOC;
+  double* ar[3];
+  double* br[3];
+  double* t[3];
+  for (int i = 0; i < 3; ++i) {
+    ar[i] = reinterpret_cast<double*>(sc + i * pa);
+    br[i] = reinterpret_cast<double*>(sc + 3 * pa + i * pb);
+    t[i] = reinterpret_cast<double*>(sc + 3 * pa + 3 * pb + i * pt);
+  }
+  char* ozs = sc + 3 * pa + 3 * pb + 3 * pt;
+  // op(A): m x k; op(B): k x n
+  const dim3 ga((unsigned)((k + 31) / 32), (unsigned)((m + 31) / 32));
+  k_cplx_parts<<<ga, 256, 0, h->stream>>>(A, lda, op_a != CORAL_NO_TRANSPOSE, op_a == CORAL_CONJ_TRANSPOSE,
+                                          (int)m, (int)k, ar[0], ar[1], ar[2]);
+  coral_status_t s = launch_status(h);
+  if (s != CORAL_OK) return s;
+  const dim3 gb((unsigned)((n + 31) / 32), (unsigned)((k + 31) / 32));
+  k_cplx_parts<<<gb, 256, 0, h->stream>>>(B, ldb, op_b != CORAL_NO_TRANSPOSE, op_b == CORAL_CONJ_TRANSPOSE,
+                                          (int)k, (int)n, br[0], br[1], br[2]);
+  if ((s = launch_status(h)) != CORAL_OK) return s;
+  for (int i = 0; i < 3; ++i) {
+    s = dgemm_ozaki_core(h, ozs, CORAL_NO_TRANSPOSE, CORAL_NO_TRANSPOSE, m, n, k, 1.0, ar[i], m, br[i], k,
+                         0.0, t[i], m);
+    if (s != CORAL_OK) return s;
+  }
+  const unsigned g = stream_grid(m * n, 256 * 4, h->sm_count, 8);
+  k_combine_3m_z<<<g, 256, 0, h->stream>>>(t[0], t[1], t[2], (int)m, (int)n, alpha, beta, C, ldc);
+  return launch_status(h);
 }
 
 coral_status_t zgemm_ozaki_impl(Handle* h, int op_a, int op_b, size_t m, size_t n, size_t k,
@@ -565,6 +686,8 @@ coral_status_t enqueue_zgemm_ozaki(Handle* h, int op_a, int op_b, size_t m, size
                                    size_t ldb, double2 beta, double2* C, size_t ldc) {
   if (m > (size_t)INT32_MAX / 4 || n > (size_t)INT32_MAX / 4 || k > (size_t)INT32_MAX / 4)
     return CORAL_ERR_NOT_SUPPORTED;
+  if (h->complex_mapping == CORAL_COMPLEX_3M)
+    return zgemm_ozaki_3m(h, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
   return zgemm_ozaki_impl(h, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 

@@ -119,6 +119,40 @@ __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_
       : "memory");
 }
 
+// Same, with the A operand kept in the tensor core's collector buffer:
+// kFill loads A and keeps it, kUse reuses the kept A (the descriptor must name
+// the same tile), kLastUse reuses it and releases the buffer.  Consecutive
+// products that share A then read it from shared memory once.
+enum CollectorA { kCollectNone = 0, kCollectFill = 1, kCollectUse = 2, kCollectLastUse = 3 };
+template <int kCollect>
+__device__ __forceinline__ void mma_f16_ca(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                           uint32_t idesc, uint32_t accumulate) {
+  if constexpr (kCollect == kCollectFill) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16.collector::a::fill [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+  } else if constexpr (kCollect == kCollectUse) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16.collector::a::use [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+  } else if constexpr (kCollect == kCollectLastUse) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16.collector::a::lastuse [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+  } else {
+    mma_f16(tmem_d, adesc, bdesc, idesc, accumulate);
+  }
+}
+
 // D[tmem] (+)= A * B^T, kind::i8 (signed 8-bit operands, s32 accumulate).
 __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
                                        uint32_t idesc, uint32_t accumulate) {
@@ -199,7 +233,7 @@ __host__ __device__ constexpr uint32_t idesc_s8_s32(int M, int N) {
 }  // namespace tc
 
 // Host: encodes a 2-D tensor map (inner dimension contiguous) for
-// `elem_bytes`-byte elements (1: u8, 2: bf16, 4: f32) with the given box,
+// `elem_bytes`-byte elements (1: u8, 2: bf16, 4: f32, 8: f64) with the given box,
 // 128-, 64- or no (0) byte swizzle and zero fill outside [0, inner) x
 // [0, outer).  Returns false on failure.
 bool encode_kmajor_map(CUtensorMap* map, const void* base, int elem_bytes, uint64_t inner,

@@ -93,3 +93,21 @@ def test_dgemm_ozaki_4096_accuracy(cuda, ill):
     err_oz = _dgemm_4096(cb.GemmMode.OZAKI_INT8, ill)
     err_native = _dgemm_4096(cb.GemmMode.NATIVE, ill)
     assert err_oz <= 4e-15, (err_oz, err_native)
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (5, 7, 4), (127, 129, 65), (64, 200, 301), (300, 260, 500)])
+@pytest.mark.parametrize("ops", [(a, b) for a in (0, 1, 2) for b in (0, 1, 2)])
+def test_zgemm_ozaki_3m(cuda, shape, ops):
+    """3M mapping: three real Ozaki GEMMs, Re = T1 - T2, Im = T3 - T1 - T2.
+    Same component-wise bound as 4M with three times the tolerance (the Im
+    error is bounded by (|Re A| + |Im A|)(|Re B| + |Im B|) <= 2 |A||B| plus the
+    T1, T2 terms)."""
+    h = cb.handle()
+    h.set_complex_mapping(1)
+    try:
+        m, n, k = shape
+        sample = 4096 if m * n > 50000 else None
+        gemm_case(cb.zgemm, np.complex128, *ops, m, n, k, 1.5 - 0.5j, 0.25 + 1j, 3e-13, sample=sample)
+        gemm_case(cb.zgemm, np.complex128, *ops, m, n, k, 1.0, 0.0, 3e-13, sample=sample)
+    finally:
+        h.set_complex_mapping(0)
