@@ -153,6 +153,8 @@ SIGNATURES = {
     "coral_mlp_gradients": [_vp, _vp, _vp, _i, _vp, C.POINTER(_f)],
     "coral_mlp_train_step": [_vp, _vp, _vp, _i, _f, C.POINTER(_f)],
     "coral_set_selector": [_h, _vp],
+    "coral_grouped_features": [_i, _i, _i, _sz, _sz, _sz, _sz, _i, C.POINTER(_f)],
+    "coral_select_grouped_config": [_h, _vp, _i, _sz, _vp, _vp],
     "coral_strsv_batched": [_h, _sz, _vp],
     "coral_sgemm_bf16x3_noalloc": [_vp, _i, _i, _sz, _sz, _sz, _f, _vp, _sz, _vp, _sz, _f, _vp, _sz],
     "coral_sgemm_bf16x3_noalloc_status": [_vp],

@@ -523,7 +523,13 @@ k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int 
         int mt, nt, kb_lo, kb_hi;
         tile_coords(item / splits, m_tiles, n_tiles, mt, nt);
         slab_range(item, kb_lo, kb_hi);
-        for (int kb = kb_lo; kb < kb_hi; ++kb, ++it) {
+        // K-serpentine: items of odd waves walk their slabs downwards, so a
+        // wave starts on the slabs the previous wave read last, which are
+        // the ones still in L2.  The MMA side consumes stages in order and
+        // does not depend on the direction.
+        const bool down = ((item / (int)gridDim.x) & 1) != 0;
+        for (int j = 0; j < kb_hi - kb_lo; ++j, ++it) {
+          const int kb = down ? kb_hi - 1 - j : kb_lo + j;
           const int s = it % kStages;
           if (it >= kStages && !tc::mbar_wait(&empty_bar[s], ((it / kStages) - 1) & 1, limit_ns)) {
             atomicOr(status, kStatusTimeout);

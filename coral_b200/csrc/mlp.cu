@@ -13,6 +13,8 @@
 // (cached per shape, so only the first call for a shape waits for it).
 #include "common.cuh"
 
+#include <algorithm>
+
 #include <cmath>
 #include <mutex>
 #include <random>
@@ -330,11 +332,116 @@ void selector_features(const SplitShape& sh, int bn, int splits, float* f) {
   f[12] = std::log2(std::max(1.f, std::ceil(k / 64.f) / (float)splits)) / 12.f;
 }
 
+// Features of a batch of `batch` instances of one shape under grouped tile
+// width bn, in the layout of selector_features: log2 m, n, k; transpose flags;
+// data type (3 products for fp32 inputs, 1 for bf16); log2 batch; tile width;
+// log2 tiles per instance, resident waves of the batch's tiles, log2 K slabs.
+void grouped_features(int input_type, int op_a, int op_b, int mi, int ni, int ki, int batch, int bn, float* f) {
+  const float m = (float)(mi > 0 ? mi : 1), n = (float)(ni > 0 ? ni : 1), k = (float)(ki > 0 ? ki : 1);
+  const float b = (float)(batch > 0 ? batch : 1);
+  f[0] = std::log2(m) / 16.f;
+  f[1] = std::log2(n) / 16.f;
+  f[2] = std::log2(k) / 16.f;
+  f[3] = op_a != 0 ? 1.f : 0.f;
+  f[4] = op_b != 0 ? 1.f : 0.f;
+  f[5] = (input_type == CORAL_INPUT_BF16 ? 1.f : 3.f) / 6.f;
+  f[6] = 0.f;
+  f[7] = std::log2(b) / 12.f;
+  f[8] = (float)bn / 256.f;
+  f[9] = 0.f;
+  const float tiles = std::ceil(m / 128.f) * std::ceil(n / (float)bn);
+  f[10] = std::log2(tiles) / 16.f;
+  f[11] = std::min(tiles * b / 148.f, 8.f) / 8.f;
+  f[12] = std::log2(std::max(1.f, std::ceil(k / 32.f))) / 12.f;
+}
+
 }  // namespace coral
 
 using namespace coral;
 
 extern "C" {
+
+coral_status_t coral_grouped_features(int input_type, int op_a, int op_b, size_t m, size_t n, size_t k,
+                                      size_t batch, int tile_n, float* out) {
+  if (!out) return CORAL_ERR_INVALID_ARG;
+  grouped_features(input_type, op_a, op_b, (int)m, (int)n, (int)k,
+                   (int)(batch < (size_t)INT32_MAX ? batch : INT32_MAX), tile_n, out);
+  return CORAL_OK;
+}
+
+// Learned choice of the grouped tile-width policy: for each instance class
+// (n <= 64, <= 128, <= 256, > 256) present in the host copy of the
+// descriptors, the class's median m, n, k, majority operations and instance
+// count describe a uniform batch; the network predicts its log time under each
+// allowed width (64 or 128 for the two small classes, 64, 128 or 256 for the
+// others) and the class takes the argmin.  Classes without instances keep the
+// handle's width.  Synchronises with the handle's stream.
+coral_status_t coral_select_grouped_config(coral_handle_t hh, coral_mlp_t mlp, int input_type, size_t count,
+                                           const coral_sgemm_problem_t* problems_host, int tile_n[4]) {
+  CORAL_HANDLE(hh);
+  Mlp* net = reinterpret_cast<Mlp*>(mlp);
+  if (!net || net->in != kSelectorFeatures || net->out != 1) return bad_arg(H, 1);
+  if (input_type != CORAL_INPUT_F32 && input_type != CORAL_INPUT_BF16) return bad_arg(H, 2);
+  if (count && !problems_host) return bad_arg(H, 4);
+  if (!tile_n) return bad_arg(H, 5);
+  std::vector<int> ms[4], ns[4], ks[4];
+  int ta[4] = {0, 0, 0, 0}, tb[4] = {0, 0, 0, 0};
+  for (size_t i = 0; i < count; ++i) {
+    const coral_sgemm_problem_t& p = problems_host[i];
+    if (p.m <= 0 || p.n <= 0) continue;
+    const int c = p.n <= 64 ? 0 : p.n <= 128 ? 1 : p.n <= 256 ? 2 : 3;
+    ms[c].push_back(p.m);
+    ns[c].push_back(p.n);
+    ks[c].push_back(p.k);
+    ta[c] += p.op_a != 0;
+    tb[c] += p.op_b != 0;
+  }
+  auto median = [](std::vector<int>& v) {
+    std::nth_element(v.begin(), v.begin() + v.size() / 2, v.end());
+    return v[v.size() / 2];
+  };
+  float feats[12 * kSelectorFeatures];
+  int cls[12], width[12], rows = 0;
+  for (int c = 0; c < 4; ++c) {
+    if (ms[c].empty()) continue;
+    const int b = (int)ms[c].size();
+    const int m = median(ms[c]), n = median(ns[c]), k = median(ks[c]);
+    for (int bn : {64, 128, 256}) {
+      if (c < 2 && bn == 256) continue;
+      grouped_features(input_type, 2 * ta[c] > b, 2 * tb[c] > b, m, n, k, b, bn, feats + rows * kSelectorFeatures);
+      cls[rows] = c;
+      width[rows] = bn;
+      ++rows;
+    }
+  }
+  GroupedPolicy pol = H->grouped_policy;
+  if (rows > 0) {
+    char* d = static_cast<char*>(scratch(H, 16 * kSelectorFeatures * sizeof(float) + 256));
+    if (!d) return CORAL_ERR_ALLOC;
+    float* fx = reinterpret_cast<float*>(d);
+    float* py = reinterpret_cast<float*>(d + 12 * kSelectorFeatures * sizeof(float));
+    CORAL_CUDA(H, cudaMemcpyAsync(fx, feats, sizeof(float) * rows * kSelectorFeatures, cudaMemcpyHostToDevice,
+                                  H->stream));
+    Handle* owner = net->h;
+    cudaStream_t saved = owner->stream;
+    owner->stream = H->stream;
+    coral_status_t s = forward(net, fx, rows, py);
+    owner->stream = saved;
+    if (s != CORAL_OK) return s;
+    float pred[12];
+    CORAL_CUDA(H, cudaMemcpyAsync(pred, py, sizeof(float) * rows, cudaMemcpyDeviceToHost, H->stream));
+    CORAL_CUDA(H, cudaStreamSynchronize(H->stream));
+    float best[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+    for (int r = 0; r < rows; ++r)
+      if (pred[r] < best[cls[r]]) {
+        best[cls[r]] = pred[r];
+        pol.bn[cls[r]] = width[r];
+      }
+  }
+  H->grouped_policy = pol;
+  for (int c = 0; c < 4; ++c) tile_n[c] = pol.bn[c];
+  return CORAL_OK;
+}
 
 coral_status_t coral_mlp_create(coral_handle_t hh, int in_dim, int hidden, int out_dim,
                                 uint64_t seed, coral_mlp_t* out) {

@@ -19,6 +19,13 @@ CLI (runs on a B200):
     python -m coral_b200.tuning collect --count 2000 --seed 2 --out heldout.npz
     python -m coral_b200.tuning train --db train.npz --out selector.npz
     python -m coral_b200.tuning evaluate --db heldout.npz --weights selector.npz
+
+The tensor-core grouped GEMM's tile-width policy has its own network and
+pipeline (uniform batches of varied data type and instance count; live
+regret on held-out uneven batches against all 36 policies):
+    python -m coral_b200.tuning grouped-collect --count 6000 --out grouped_train.npz
+    python -m coral_b200.tuning grouped-train --db grouped_train.npz --out grouped_selector.npz
+    python -m coral_b200.tuning grouped-evaluate --weights grouped_selector.npz
 """
 from __future__ import annotations
 
@@ -249,6 +256,243 @@ def summarize(r: np.ndarray) -> dict:
             "max": float(r.max()), "frac_optimal": float((r <= 1e-9).mean())}
 
 
+# ----------------------------------------------- grouped GEMM tile policy --
+# The tensor-core grouped GEMM takes one N tile width per instance class
+# (n <= 64, <= 128, <= 256, > 256).  A second network of the same shape
+# predicts the log time of a uniform batch (one shape, `batch` instances) under
+# each width, from features whose data type (fp32 split / bf16 inputs) and
+# batch count vary over the training set; coral_select_grouped_config applies
+# it per class of a real batch.
+GROUPED_WIDTHS = (64, 128, 256)
+GROUPED_CLASS_WIDTHS = ((64, 128), (64, 128), (64, 128, 256), (64, 128, 256))
+
+
+def grouped_policies() -> list:
+    """The 36 policies in coral_autotune_sgemm_grouped's order (class 0 slowest)."""
+    return [(a, b, c, d) for a in GROUPED_CLASS_WIDTHS[0] for b in GROUPED_CLASS_WIDTHS[1]
+            for c in GROUPED_CLASS_WIDTHS[2] for d in GROUPED_CLASS_WIDTHS[3]]
+
+
+def grouped_samples(count: int, seed: int) -> np.ndarray:
+    """[count, 7] int64: input_type, op_a, op_b, m, n, k, batch.  m, n, k
+    log-uniform in [16, 1024]; batch log-uniform in [1, 4096], capped so the
+    batch holds at most 2^25 output elements and 2^34 multiply-adds."""
+    rng = np.random.default_rng(seed)
+    dims = np.exp(rng.uniform(np.log(16), np.log(1024), (count, 3))).astype(np.int64)
+    batch = np.exp(rng.uniform(0, np.log(4096), count)).astype(np.int64)
+    mn = dims[:, 0] * dims[:, 1]
+    batch = np.minimum(batch, np.maximum(1, (1 << 25) // mn))
+    batch = np.minimum(batch, np.maximum(1, (1 << 34) // (mn * dims[:, 2])))
+    it = rng.integers(0, 2, count)
+    op_a = rng.integers(0, 2, count)
+    op_b = (rng.uniform(size=count) < 0.25).astype(np.int64)
+    return np.stack([it, op_a, op_b, dims[:, 0], dims[:, 1], dims[:, 2], batch], axis=1)
+
+
+def grouped_feature(sample, bn: int) -> np.ndarray:
+    it, op_a, op_b, m, n, k, b = (int(v) for v in sample)
+    out = (C.c_float * N_FEATURES)()
+    st = _lib.load().coral_grouped_features(it, op_a, op_b, m, n, k, b, bn, out)
+    if st != 0:
+        raise RuntimeError(f"coral_grouped_features: {st}")
+    return np.frombuffer(out, dtype=np.float32).copy()
+
+
+def grouped_feature_matrix(samples: np.ndarray) -> np.ndarray:
+    """[len(samples) * 3, 13], sample-major, width-minor."""
+    return np.stack([grouped_feature(s, bn) for s in samples for bn in GROUPED_WIDTHS])
+
+
+def uniform_records(b, op_a, op_b, m, n, k, ptr_a, ptr_b, ptr_c):
+    """Descriptor records of b instances of one shape sharing A and B, each
+    with its own m x n block of C."""
+    from .blas import sgemm_problem_dtype
+    rec = np.zeros(b, dtype=sgemm_problem_dtype())
+    for f, v in (("op_a", op_a), ("op_b", op_b), ("m", m), ("n", n), ("k", k), ("alpha", 1.0), ("a", ptr_a),
+                 ("b", ptr_b), ("lda", m if op_a == 0 else k), ("ldb", k if op_b == 0 else n), ("ldc", m)):
+        rec[f] = v
+    rec["c"] = ptr_c + 4 * m * n * np.arange(b, dtype=np.uint64)
+    return rec
+
+
+def collect_grouped(samples: np.ndarray, reps: int = 3, log_every: int = 1000) -> np.ndarray:
+    """Times each uniform batch under every width: [len(samples), 3] ms."""
+    import torch
+    h = handle()
+    h.bind_current_stream()
+    lib = _lib.load()
+    need_ab = int(max(max(s[3] * s[5], s[5] * s[4]) for s in samples))
+    need_c = int(max(s[3] * s[4] * s[6] for s in samples))
+    A32 = torch.empty(need_ab, dtype=torch.float32, device="cuda").uniform_(-1, 1)
+    B32 = torch.empty(need_ab, dtype=torch.float32, device="cuda").uniform_(-1, 1)
+    A16, B16 = A32.to(torch.bfloat16), B32.to(torch.bfloat16)
+    Cd = torch.zeros(need_c, dtype=torch.float32, device="cuda")
+    times = np.zeros((len(samples), len(GROUPED_WIDTHS)), np.float32)
+    saved_mode = h.gemm_mode()
+    h.set_gemm_mode(1)   # SPLIT_BF16X3: fp32 inputs on the tensor cores
+    t0 = time.time()
+    try:
+        for i, (it, op_a, op_b, m, n, k, b) in enumerate(samples):
+            it, op_a, op_b, m, n, k, b = (int(v) for v in (it, op_a, op_b, m, n, k, b))
+            A, B = (A16, B16) if it == 1 else (A32, B32)
+            rec = uniform_records(b, op_a, op_b, m, n, k, A.data_ptr(), B.data_ptr(), Cd.data_ptr())
+            desc = torch.from_numpy(rec.view(np.uint8)).cuda()
+            evs = []
+            for bn in GROUPED_WIDTHS:
+                lib.coral_set_grouped_config(h.h, (C.c_int * 4)(bn, bn, bn, bn))
+                h.check(lib.coral_sgemm_grouped(h.h, it, b, C.c_void_p(desc.data_ptr())), "grouped")
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(reps):
+                    h.check(lib.coral_sgemm_grouped(h.h, it, b, C.c_void_p(desc.data_ptr())), "grouped")
+                e1.record()
+                evs.append((e0, e1))
+            torch.cuda.synchronize()
+            times[i] = [e0.elapsed_time(e1) / reps for e0, e1 in evs]
+            if log_every and (i + 1) % log_every == 0:
+                print(f"  {i + 1}/{len(samples)} batches, {time.time() - t0:.0f} s", flush=True)
+    finally:
+        lib.coral_set_grouped_config(h.h, None)
+        h.set_gemm_mode(saved_mode)
+    return times
+
+
+def train_grouped(samples: np.ndarray, times: np.ndarray, epochs: int = 400, batch: int = 2048,
+                  lr: float = 2e-3, seed: int = 0) -> tuple[Mlp, list]:
+    """Fits log(ms) of every (uniform batch, width) pair with the library's kernels."""
+    import torch
+    X = torch.from_numpy(grouped_feature_matrix(samples)).cuda()
+    y = torch.from_numpy(np.log(np.maximum(times.reshape(-1, 1), 1e-4)).astype(np.float32)).cuda()
+    net = Mlp(seed=seed)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    history = []
+    n = X.shape[0]
+    for ep in range(epochs):
+        perm = torch.randperm(n, device="cuda", generator=g)
+        tot, steps = 0.0, 0
+        lr_ep = lr * (0.5 * (1 + np.cos(np.pi * ep / epochs)) * 0.95 + 0.05)
+        for s0 in range(0, n, batch):
+            idx = perm[s0:s0 + batch]
+            tot += net.train_step(X[idx].contiguous(), y[idx].contiguous(), float(lr_ep))
+            steps += 1
+        history.append(tot / max(steps, 1))
+    return net, history
+
+
+def predict_grouped_choice(predict, samples: np.ndarray) -> np.ndarray:
+    """Index into GROUPED_WIDTHS of the predicted fastest width per sample;
+    `predict` maps a feature matrix to predicted log times."""
+    pred = np.asarray(predict(grouped_feature_matrix(samples))).reshape(len(samples), len(GROUPED_WIDTHS))
+    return pred.argmin(1)
+
+
+def uneven_batches(count: int, seed: int, max_elems: int = 1 << 27) -> list:
+    """Held-out uneven batches: [(input_type, [(op_a, op_b, m, n, k), ...])].
+    Each batch draws its instance count log-uniform in [64, 4096], one of
+    several dimension ranges and an operation mix, up to max_elems operand
+    elements in total."""
+    rng = np.random.default_rng(seed)
+    ranges = [(16, 512), (16, 128), (32, 256), (64, 1024), (128, 2048), (16, 2048)]
+    out = []
+    for _ in range(count):
+        it = int(rng.integers(0, 2))
+        lo, hi = ranges[int(rng.integers(0, len(ranges)))]
+        want = int(np.exp(rng.uniform(np.log(64), np.log(4096))))
+        p_t = float(rng.uniform(0, 1))
+        insts, elems = [], 0
+        for _ in range(want):
+            m, n, k = (int(v) for v in np.exp(rng.uniform(np.log(lo), np.log(hi), 3)))
+            e = m * k + k * n + m * n
+            if elems + e > max_elems:
+                break
+            elems += e
+            insts.append((int(rng.uniform() < p_t), int(rng.uniform() < 0.25), m, n, k))
+        out.append((it, insts))
+    return out
+
+
+def _default_policy(h, lib):
+    lib.coral_set_grouped_config(h.h, None)
+    tn = (C.c_int * 4)()
+    lib.coral_get_grouped_config(h.h, tn)
+    return tuple(int(v) for v in tn)
+
+
+def evaluate_grouped_live(net: Mlp, batches: list, reps: int = 3) -> dict:
+    """For every held-out batch, on this GPU: all 36 policies timed by
+    coral_autotune_sgemm_grouped, the network's choice
+    (coral_select_grouped_config) and the exhaustive best re-timed on their
+    own, and the default policy.  Returns per-batch records and the regret
+    summaries t(choice) / t(exhaustive best) - 1."""
+    import torch
+    from .blas import sgemm_problem_dtype
+    h = handle()
+    h.bind_current_stream()
+    lib = _lib.load()
+    pols = grouped_policies()
+    default = _default_policy(h, lib)
+    rows = []
+    saved_mode = h.gemm_mode()
+    h.set_gemm_mode(1)
+    try:
+        for it, insts in batches:
+            dt = torch.bfloat16 if it == 1 else torch.float32
+            na = sum(m * k for _, _, m, n, k in insts)
+            nb = sum(k * n for _, _, m, n, k in insts)
+            nc = sum(m * n for _, _, m, n, k in insts)
+            A = torch.empty(na, dtype=torch.float32, device="cuda").uniform_(-1, 1).to(dt)
+            B = torch.empty(nb, dtype=torch.float32, device="cuda").uniform_(-1, 1).to(dt)
+            Cd = torch.zeros(nc, dtype=torch.float32, device="cuda")
+            es = A.element_size()
+            rec = np.zeros(len(insts), dtype=sgemm_problem_dtype())
+            oa = ob = oc = 0
+            for i, (op_a, op_b, m, n, k) in enumerate(insts):
+                rec[i] = (op_a, op_b, m, n, k, 1.0, 0.0, 0, A.data_ptr() + oa * es, B.data_ptr() + ob * es,
+                          Cd.data_ptr() + oc * 4, m if op_a == 0 else k, k if op_b == 0 else n, m)
+                oa += m * k
+                ob += k * n
+                oc += m * n
+            desc = torch.from_numpy(rec.view(np.uint8)).cuda()
+            ms = (C.c_float * 36)()
+            best = C.c_int()
+            tn = (C.c_int * 4)()
+            h.check(lib.coral_autotune_sgemm_grouped(h.h, it, len(insts), C.c_void_p(desc.data_ptr()), reps, ms,
+                                                     C.byref(best), tn), "autotune grouped")
+            table = np.frombuffer(ms, dtype=np.float32).copy()
+            sel = (C.c_int * 4)()
+            h.check(lib.coral_select_grouped_config(h.h, net.p, it, len(insts), rec.ctypes.data_as(C.c_void_p),
+                                                    sel), "select grouped")
+            choice = tuple(int(v) for v in sel)
+
+            def time_policy(pol):
+                lib.coral_set_grouped_config(h.h, (C.c_int * 4)(*pol))
+                h.check(lib.coral_sgemm_grouped(h.h, it, len(insts), C.c_void_p(desc.data_ptr())), "grouped")
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(reps):
+                    lib.coral_sgemm_grouped(h.h, it, len(insts), C.c_void_p(desc.data_ptr()))
+                e1.record()
+                torch.cuda.synchronize()
+                return e0.elapsed_time(e1) / reps
+            t_sel = time_policy(choice)
+            t_best = time_policy(pols[int(best.value)])
+            rows.append({"input": "bf16" if it == 1 else "fp32", "instances": len(insts),
+                         "best_ms": float(table.min()), "choice_ms": float(table[pols.index(choice)]),
+                         "default_ms": float(table[pols.index(default)]),
+                         "choice_ms_retimed": t_sel, "best_ms_retimed": t_best,
+                         "choice": list(choice), "best": list(pols[int(best.value)])})
+            del A, B, Cd, desc
+    finally:
+        lib.coral_set_grouped_config(h.h, None)
+        h.set_gemm_mode(saved_mode)
+    r_sel = np.array([x["choice_ms"] / x["best_ms"] - 1 for x in rows])
+    r_def = np.array([x["default_ms"] / x["best_ms"] - 1 for x in rows])
+    r_live = np.array([x["choice_ms_retimed"] / x["best_ms_retimed"] - 1 for x in rows])
+    return {"batches": rows, "selector": summarize(r_sel), "default_policy": summarize(r_def),
+            "selector_retimed": summarize(r_live)}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m coral_b200.tuning")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -263,6 +507,19 @@ def main(argv=None):
     e = sub.add_parser("evaluate")
     e.add_argument("--db", required=True)
     e.add_argument("--weights", required=True)
+    gc = sub.add_parser("grouped-collect")
+    gc.add_argument("--count", type=int, default=6000)
+    gc.add_argument("--seed", type=int, default=11)
+    gc.add_argument("--out", required=True)
+    gt = sub.add_parser("grouped-train")
+    gt.add_argument("--db", required=True)
+    gt.add_argument("--out", required=True)
+    gt.add_argument("--epochs", type=int, default=400)
+    ge = sub.add_parser("grouped-evaluate")
+    ge.add_argument("--weights", required=True)
+    ge.add_argument("--batches", type=int, default=40)
+    ge.add_argument("--seed", type=int, default=12)
+    ge.add_argument("--out", default="")
     args = ap.parse_args(argv)
     if args.cmd == "collect":
         shapes = generate_shapes(args.count, args.seed)
@@ -290,6 +547,31 @@ def main(argv=None):
                           "selector": summarize(regret(d["times"], choice)),
                           "default_rule": summarize(regret(d["times"], dflt)),
                           "fixed_256x1": summarize(regret(d["times"], fixed))}))
+    elif args.cmd == "grouped-collect":
+        samples = grouped_samples(args.count, args.seed)
+        t0 = time.time()
+        times = collect_grouped(samples)
+        np.savez_compressed(args.out, samples=samples, times=times, widths=np.array(GROUPED_WIDTHS),
+                            seed=args.seed)
+        print(json.dumps({"collected": len(samples), "seconds": time.time() - t0, "out": args.out}))
+    elif args.cmd == "grouped-train":
+        import torch
+        d = np.load(args.db)
+        t0 = time.time()
+        net, hist = train_grouped(d["samples"], d["times"], epochs=args.epochs)
+        net.save(args.out, {"db": os.path.basename(args.db), "epochs": args.epochs,
+                            "final_mse": hist[-1], "seconds": time.time() - t0})
+        choice = predict_grouped_choice(lambda X: net.forward(torch.from_numpy(X).cuda()).cpu().numpy(),
+                                        d["samples"])
+        print(json.dumps({"train_mse": hist[-1], "train_regret": summarize(regret(d["times"], choice)),
+                          "seconds": time.time() - t0}))
+    elif args.cmd == "grouped-evaluate":
+        net = Mlp.load(args.weights)
+        res = evaluate_grouped_live(net, uneven_batches(args.batches, args.seed))
+        if args.out:
+            with open(args.out, "w") as f:
+                json.dump(res, f)
+        print(json.dumps({k: v for k, v in res.items() if k != "batches"}))
 
 
 if __name__ == "__main__":

@@ -70,8 +70,8 @@ enum {
   CORAL_GEMM_SPLIT_BF16X6 = 3  /* s/c: 3-way BF16 split, 6 tcgen05 products */
 };
 
-/* How the emulated complex GEMMs (coral_cgemm in the split-BF16 modes) map
- * onto real tensor-core products. */
+/* How the emulated complex GEMMs (coral_cgemm in the split-BF16 modes,
+ * coral_zgemm in the Ozaki mode) map onto real tensor-core products. */
 enum {
   CORAL_COMPLEX_4M = 0, /* one real GEMM of m x 2n x 2k: Re and Im exact per term */
   CORAL_COMPLEX_3M = 1  /* three real GEMMs of m x n x k (3/4 of the work); the
@@ -93,7 +93,7 @@ coral_status_t coral_get_gemm_mode(coral_handle_t handle, int* mode);
 /* K depth, in 64-element slabs, of each tensor-core accumulation chunk of the
  * split-BF16 GEMMs before it is added into fp32 registers (default 16). */
 coral_status_t coral_set_split_chunk(coral_handle_t handle, int slabs);
-/* Complex mapping of the split-BF16 CGEMM: CORAL_COMPLEX_4M (default) or 3M. */
+/* Complex mapping of the emulated CGEMM / ZGEMM: CORAL_COMPLEX_4M (default) or 3M. */
 coral_status_t coral_set_complex_mapping(coral_handle_t handle, int mapping);
 /* Iteration limit of every bounded device wait (0 restores the default). */
 coral_status_t coral_set_wait_limit(coral_handle_t handle, uint64_t spins);
@@ -491,6 +491,18 @@ coral_status_t coral_mlp_gradients(coral_mlp_t mlp, const float* x, const float*
 /* One Adam step (beta1 0.9, beta2 0.999) on a batch; loss to host (may be NULL). */
 coral_status_t coral_mlp_train_step(coral_mlp_t mlp, const float* x, const float* target, int batch,
                                     float lr, float* loss);
+/* Features (13 floats) of a uniform batch of `batch` instances of one shape
+ * in the tensor-core grouped GEMM under N tile width tile_n, for training a
+ * network that predicts the batch's log time. */
+coral_status_t coral_grouped_features(int input_type, int op_a, int op_b, size_t m, size_t n, size_t k,
+                                      size_t batch, int tile_n, float* out);
+/* Learned grouped tile-width policy: for each instance class present in
+ * `problems_host` (a HOST copy of the descriptors), the network (trained on
+ * coral_grouped_features) scores the allowed widths for the class's median
+ * shape and instance count; the argmin per class is installed on the handle
+ * and returned in tile_n.  Synchronises with the handle's stream. */
+coral_status_t coral_select_grouped_config(coral_handle_t h, coral_mlp_t mlp, int input_type, size_t count,
+                                           const coral_sgemm_problem_t* problems_host, int tile_n[4]);
 /* Attach (or, with NULL, detach) a trained selector to a handle.  Decisions
  * are cached per shape; the first call for a shape waits for one forward
  * pass, so make it outside stream capture. */
