@@ -24,16 +24,18 @@
 // overrides it), instances are ordered by decreasing K bucket (longest tiles
 // first), and the exclusive prefix sum of 128 x BN output tiles is formed.
 //
-// GEMM (k_gemm_grouped_tc, persistent, one CTA per SM, 10 warps):
+// GEMM (k_gemm_grouped_tc, persistent, one CTA per SM, 14 warps):
 //   warp 0      scheduler: takes tile indices from a global atomic counter
 //               (dynamic load balance), decodes (instance, m0, n0, BN) and
 //               publishes them through a 16-deep shared queue;
-//   warps 1-4   producers: stage the K slabs of each tile into a ring of
-//               shared-memory stages (4 for fp32 pieces, 8 for bf16);
-//   warp 5      MMA issuer (lane 0): tcgen05.mma M=128, N=BN, K=16 into one of
+//   warps 1-8   producers: stage the K slabs of each tile into a ring of
+//               shared-memory stages (4 for fp32 pieces, 8 for bf16), each
+//               thread issuing the loads of all its items of a slab before
+//               converting any;
+//   warp 9      MMA issuer (lane 0): tcgen05.mma M=128, N=BN, K=16 into one of
 //               two TMEM accumulators of 256 columns, in chunks of at most
 //               32 slabs (1024 K) per accumulation;
-//   warps 6-9   epilogue: tcgen05.ld the accumulator (thread = row), apply
+//   warps 10-13 epilogue: tcgen05.ld the accumulator (thread = row), apply
 //               alpha / beta to C with coalesced column accesses; chunks after
 //               the first add alpha * partial into C.
 // Every wait is bounded: a wait that gives up sets the handle's status word
@@ -49,11 +51,11 @@ namespace {
 constexpr int kTM = 128;          // tile rows (TMEM lanes)
 constexpr int kTK = 32;           // K slab: one 64-byte swizzled row of bf16
 constexpr int kMaxBN = 256;
-constexpr int kProdWarps = 4;
+constexpr int kProdWarps = 8;
 constexpr int kEpiWarps = 4;
 constexpr int kMmaWarp = 1 + kProdWarps;
 constexpr int kEpiWarp0 = kMmaWarp + 1;
-constexpr int kTcThreads = 32 * (kEpiWarp0 + kEpiWarps);  // 320
+constexpr int kTcThreads = 32 * (kEpiWarp0 + kEpiWarps);  // 448
 constexpr int kQueue = 16;
 constexpr int kChunkSlabs = 32;
 constexpr uint32_t kAPieceBytes = kTM * kTK * 2;       // 8 KiB
@@ -191,45 +193,76 @@ __device__ __forceinline__ void load8_kcontig(const TIn* p, int avail, float (&v
   for (int j = 0; j < 8; ++j) v[j] = j < avail ? ld_val<TIn>(p + j) : 0.f;
 }
 
-// Stages rows [row0, row0 + rows) x K [k0, k0 + 32) of an operand (element
-// (r, k) at X[k + r * ld] when kcontig, else X[r + k * ld]; zero outside
-// R x Kd) as NPC bf16 piece tiles at dst + i * piece_bytes, 64-byte swizzled.
+// Operand views of one tile's K slab for the producers.
+template <typename TIn>
+struct SlabSrc {
+  const TIn* a;
+  const TIn* b;
+  long long lda, ldb;
+  bool a_kc, b_kc;  // stored contiguous along K
+  int m, n, k;      // valid rows of A, of B, and K
+  int m0, n0, bn;
+};
+
+// Stages one 32-deep K slab of a tile: A rows [m0, m0 + 128) and B rows
+// [n0, n0 + bn) (element (r, k) at X[k + r ld] when stored contiguous along K,
+// else X[r + k ld]; zero outside the matrix) as NPC bf16 piece tiles, A pieces
+// at st + i * kAPieceBytes and B pieces after them, 64-byte swizzled.  A thread
+// handles up to kMaxItems items of 8 K values; it issues the loads of all of
+// them before converting any, so a slab costs one memory round trip rather
+// than one per item.
 template <typename TIn, int NPC>
-__device__ __forceinline__ void stage_rows(const TIn* __restrict__ X, long long ld, bool kcontig, int R,
-                                           int Kd, int row0, int k0, int rows, uint8_t* dst,
-                                           uint32_t piece_bytes, int ptid) {
-  const int items = rows * 4;
-  for (int e = ptid; e < items; e += 32 * kProdWarps) {
+__device__ __forceinline__ void stage_slab(const SlabSrc<TIn>& src, int k0, uint8_t* st, int ptid) {
+  constexpr int kPT = 32 * kProdWarps;
+  constexpr int kMaxItems = (kTM + kMaxBN) * 4 / kPT;
+  const int a_items = kTM * 4;
+  const int total = (kTM + src.bn) * 4;
+  float v[kMaxItems][8];
+  uint32_t off[kMaxItems];
+#pragma unroll
+  for (int i = 0; i < kMaxItems; ++i) {
+    const int e = ptid + i * kPT;
+    off[i] = 0xffffffffu;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[i][j] = 0.f;
+    if (e >= total) continue;
+    const bool is_a = e < a_items;
+    const int el = is_a ? e : e - a_items;
+    const int rows = is_a ? kTM : src.bn;
+    const bool kc = is_a ? src.a_kc : src.b_kc;
     int r, c;
-    if (kcontig) { r = e >> 2; c = e & 3; }
-    else { r = e % rows; c = e / rows; }
-    const int gr = row0 + r, gk = k0 + 8 * c;
-    float v[8];
-    const int avail = Kd - gk;
-    if (gr < R && avail > 0) {
-      if (kcontig) {
-        load8_kcontig<TIn>(X + (size_t)gr * ld + gk, avail, v);
-      } else {
-        const TIn* p = X + gr + (size_t)gk * ld;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) v[j] = j < avail ? ld_val<TIn>(p + (size_t)j * ld) : 0.f;
-      }
+    if (kc) { r = el >> 2; c = el & 3; }
+    else { r = el % rows; c = el / rows; }
+    off[i] = (is_a ? 0u : (uint32_t)(NPC * kAPieceBytes)) + (uint32_t)(r >> 3) * 512u + (uint32_t)(r & 7) * 64u +
+             (uint32_t)((c ^ ((r >> 1) & 3)) * 16);
+    const int gr = (is_a ? src.m0 : src.n0) + r, gk = k0 + 8 * c;
+    const int avail = src.k - gk;
+    if (gr >= (is_a ? src.m : src.n) || avail <= 0) continue;
+    const TIn* X = is_a ? src.a : src.b;
+    const long long ld = is_a ? src.lda : src.ldb;
+    if (kc) {
+      load8_kcontig<TIn>(X + (size_t)gr * ld + gk, avail, v[i]);
     } else {
+      const TIn* p = X + gr + (size_t)gk * ld;
 #pragma unroll
-      for (int j = 0; j < 8; ++j) v[j] = 0.f;
+      for (int j = 0; j < 8; ++j)
+        if (j < avail) v[i][j] = ld_val<TIn>(p + (size_t)j * ld);
     }
+  }
+#pragma unroll
+  for (int i = 0; i < kMaxItems; ++i) {
+    if (off[i] == 0xffffffffu) continue;
     __align__(16) __nv_bfloat16 q[NPC][8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      const __nv_bfloat16 h0 = __float2bfloat16_rn(v[j]);
+      const __nv_bfloat16 h0 = __float2bfloat16_rn(v[i][j]);
       q[0][j] = h0;
-      if constexpr (NPC == 2) q[1][j] = __float2bfloat16_rn(v[j] - __bfloat162float(h0));
+      if constexpr (NPC == 2) q[1][j] = __float2bfloat16_rn(v[i][j] - __bfloat162float(h0));
     }
-    const uint32_t off = (uint32_t)(r >> 3) * 512u + (uint32_t)(r & 7) * 64u +
-                         (uint32_t)((c ^ ((r >> 1) & 3)) * 16);
+    const uint32_t piece = off[i] < (uint32_t)(NPC * kAPieceBytes) ? kAPieceBytes : kBPieceBytes;
 #pragma unroll
-    for (int i = 0; i < NPC; ++i)
-      *reinterpret_cast<uint4*>(dst + i * piece_bytes + off) = *reinterpret_cast<const uint4*>(q[i]);
+    for (int pc = 0; pc < NPC; ++pc)
+      *reinterpret_cast<uint4*>(st + pc * piece + off[i]) = *reinterpret_cast<const uint4*>(q[pc]);
   }
 }
 
@@ -341,9 +374,9 @@ k_gemm_grouped_tc(const coral_sgemm_problem_t* __restrict__ probs, int count,
     for (int j = 0; next_tile(j, ti, false); ++j) {
       if (ti.nslabs == 0) continue;
       const coral_sgemm_problem_t p = probs[ti.inst];
-      const TIn* A = static_cast<const TIn*>(p.a);
-      const TIn* B = static_cast<const TIn*>(p.b);
-      const bool a_kc = p.op_a != CORAL_NO_TRANSPOSE, b_kc = p.op_b == CORAL_NO_TRANSPOSE;
+      const SlabSrc<TIn> src{static_cast<const TIn*>(p.a), static_cast<const TIn*>(p.b), p.lda, p.ldb,
+                             p.op_a != CORAL_NO_TRANSPOSE, p.op_b == CORAL_NO_TRANSPOSE, p.m, p.n, p.k,
+                             ti.m0, ti.n0, ti.bn};
       bool stop = false;
       for (int kb = 0; kb < ti.nslabs; ++kb, ++it) {
         const int s = it % S;
@@ -353,9 +386,7 @@ k_gemm_grouped_tc(const coral_sgemm_problem_t* __restrict__ probs, int count,
           break;
         }
         uint8_t* st = smem + (size_t)s * kStage;
-        stage_rows<TIn, NPC>(A, p.lda, a_kc, p.m, p.k, ti.m0, kb * kTK, kTM, st, kAPieceBytes, ptid);
-        stage_rows<TIn, NPC>(B, p.ldb, b_kc, p.n, p.k, ti.n0, kb * kTK, ti.bn, st + NPC * kAPieceBytes,
-                             kBPieceBytes, ptid);
+        stage_slab<TIn, NPC>(src, kb * kTK, st, ptid);
         tc::fence_proxy_async_smem();
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&full_bar[s]);
