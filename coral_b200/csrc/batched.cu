@@ -181,23 +181,28 @@ k_gemm_grouped(const GemmProblem* __restrict__ probs, int count, const int* __re
     }
     const bool beta0 = p.beta == 0.f, beta1 = p.beta == 1.f;
     const bool scale_only = p.alpha == 0.f || p.k == 0;  // sgemm_nn.rs:29-45
+    // the four C loads of a column before its stores (no round trip per element)
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int gc = n0 + tx * 4 + j;
       if (gc >= p.n) continue;
+      if (scale_only && beta1) continue;
+      float cv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int gr = m0 + ty * 4 + i;
+        cv[i] = (!beta0 && gr < p.m) ? p.c[gr + (size_t)gc * p.ldc] : 0.f;
+      }
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int gr = m0 + ty * 4 + i;
         if (gr >= p.m) continue;
         float* cp = p.c + gr + (size_t)gc * p.ldc;
         if (scale_only) {
-          if (beta0) *cp = 0.f;
-          else if (!beta1) *cp = *cp * p.beta;
+          *cp = beta0 ? 0.f : cv[i] * p.beta;
         } else {
           const float v = p.alpha * acc[i][j];
-          if (beta0) *cp = v;
-          else if (beta1) *cp = *cp + v;
-          else *cp = p.beta * *cp + v;
+          *cp = beta0 ? v : beta1 ? cv[i] + v : p.beta * cv[i] + v;
         }
       }
     }

@@ -193,19 +193,25 @@ k_gemm_simt(int m, int n, int k, T alpha, const T* __restrict__ A, size_t lda, i
   }
 
   const bool beta0 = Arith<T>::is_zero(beta), beta1 = Arith<T>::is_one(beta);
+  // every C load of a column before its stores: a load behind a store the
+  // compiler cannot prove disjoint would cost a memory round trip each
 #pragma unroll
   for (int j = 0; j < TN; ++j) {
     const int gc = n0 + (j < HN ? tx * HN + j : BN / 2 + tx * HN + (j - HN));
     if (gc >= n) continue;
+    T cv[TM];
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+      const int gr = m0 + (i < HM ? ty * HM + i : BM / 2 + ty * HM + (i - HM));
+      cv[i] = (!beta0 && gr < m) ? C[gr + (size_t)gc * ldc] : Arith<T>::zero();
+    }
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
       const int gr = m0 + (i < HM ? ty * HM + i : BM / 2 + ty * HM + (i - HM));
       if (gr >= m) continue;
-      T* cp = C + gr + (size_t)gc * ldc;
-      T v = Arith<T>::mul(alpha, acc[i][j]);
-      if (beta0) *cp = v;
-      else if (beta1) *cp = Arith<T>::add(*cp, v);
-      else *cp = Arith<T>::add(Arith<T>::mul(beta, *cp), v);
+      const T v = Arith<T>::mul(alpha, acc[i][j]);
+      C[gr + (size_t)gc * ldc] =
+          beta0 ? v : beta1 ? Arith<T>::add(cv[i], v) : Arith<T>::add(Arith<T>::mul(beta, cv[i]), v);
     }
   }
 }

@@ -457,6 +457,7 @@ __device__ __forceinline__ void tile_coords(int tile, int m_tiles, int n_tiles, 
 // partial sum goes through; the register adds round to nearest.
 constexpr int kEpiWarps = 8;
 constexpr int kSplitThreads = 64 + 32 * kEpiWarps;
+constexpr int kCGroup = 8;  // C columns loaded together by the epilogue
 
 template <int NP, int BN>
 __global__ void __launch_bounds__(kSplitThreads, 1)
@@ -644,36 +645,50 @@ k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int 
         for (int j = 0; j < kCols; ++j)
           if (col0 + j < ws_cols) wp[(size_t)(col0 + j) * ep.m] = sum[j];
       } else if (!ep.complex_out) {
+        // C is read in groups of kCGroup columns, all loads of a group before
+        // any store: a store followed by a load the compiler cannot prove
+        // disjoint would otherwise cost a memory round trip per column.
         float* crow = ep.C + row;
 #pragma unroll
-        for (int j = 0; j < kCols; ++j) {
-          const int col = col0 + j;
-          if (col < ep.n) {
-            float v = ep.alpha_re * sum[j];
-            float* cp = crow + (size_t)col * ep.ldc;
-            if (beta0) *cp = v;
-            else if (beta1) *cp = *cp + v;
-            else *cp = ep.beta_re * *cp + v;
+        for (int g = 0; g < kCols; g += kCGroup) {
+          float cv[kCGroup];
+#pragma unroll
+          for (int j = 0; j < kCGroup; ++j)
+            cv[j] = (!beta0 && col0 + g + j < ep.n) ? crow[(size_t)(col0 + g + j) * ep.ldc] : 0.f;
+#pragma unroll
+          for (int j = 0; j < kCGroup; ++j) {
+            const int col = col0 + g + j;
+            if (col < ep.n) {
+              const float v = ep.alpha_re * sum[g + j];
+              crow[(size_t)col * ep.ldc] = beta0 ? v : beta1 ? cv[j] + v : ep.beta_re * cv[j] + v;
+            }
           }
         }
       } else {
         float2* crow = reinterpret_cast<float2*>(ep.C) + row;
 #pragma unroll
-        for (int j = 0; j < kCols / 2; ++j) {
-          const int col = col0 / 2 + j;
-          if (col < ep.n) {
-            const float ar = sum[2 * j], ai = sum[2 * j + 1];
-            float2 v = make_float2(ep.alpha_re * ar - ep.alpha_im * ai, ep.alpha_re * ai + ep.alpha_im * ar);
-            float2* cp = crow + (size_t)col * ep.ldc;
-            if (!beta0) {
-              float2 cv = *cp;
-              if (beta1) { v.x += cv.x; v.y += cv.y; }
-              else {
-                v.x += ep.beta_re * cv.x - ep.beta_im * cv.y;
-                v.y += ep.beta_re * cv.y + ep.beta_im * cv.x;
+        for (int g = 0; g < kCols / 2; g += kCGroup / 2) {
+          float2 cvs[kCGroup / 2];
+#pragma unroll
+          for (int j = 0; j < kCGroup / 2; ++j)
+            cvs[j] = (!beta0 && col0 / 2 + g + j < ep.n) ? crow[(size_t)(col0 / 2 + g + j) * ep.ldc]
+                                                          : make_float2(0.f, 0.f);
+#pragma unroll
+          for (int j = 0; j < kCGroup / 2; ++j) {
+            const int col = col0 / 2 + g + j;
+            if (col < ep.n) {
+              const float ar = sum[2 * (g + j)], ai = sum[2 * (g + j) + 1];
+              float2 v = make_float2(ep.alpha_re * ar - ep.alpha_im * ai, ep.alpha_re * ai + ep.alpha_im * ar);
+              if (!beta0) {
+                const float2 cv = cvs[j];
+                if (beta1) { v.x += cv.x; v.y += cv.y; }
+                else {
+                  v.x += ep.beta_re * cv.x - ep.beta_im * cv.y;
+                  v.y += ep.beta_re * cv.y + ep.beta_im * cv.x;
+                }
               }
+              crow[(size_t)col * ep.ldc] = v;
             }
-            *cp = v;
           }
         }
       }

@@ -175,19 +175,24 @@ k_gemm_tma_fma(const __grid_constant__ TfMaps maps, int m, int n, int k, T alpha
     }
     if (!*(volatile int*)&abort_flag) {
       const bool beta0 = beta == T(0), beta1 = beta == T(1);
+      // every C load of a column before its stores: a load behind a store
+      // the compiler cannot prove disjoint would cost a round trip each
 #pragma unroll
       for (int j = 0; j < TN; ++j) {
         const int gc = n0 + tile_row<TN, V, BK_>(tx, j);
         if (gc >= n) continue;
+        T cv[TM];
+#pragma unroll
+        for (int i = 0; i < TM; ++i) {
+          const int gr = m0 + tile_row<TM, V, AK>(ty, i);
+          cv[i] = (!beta0 && gr < m) ? C[gr + (size_t)gc * ldc] : T(0);
+        }
 #pragma unroll
         for (int i = 0; i < TM; ++i) {
           const int gr = m0 + tile_row<TM, V, AK>(ty, i);
           if (gr >= m) continue;
-          T* cp = C + gr + (size_t)gc * ldc;
           const T v = alpha * acc[i][j];
-          if (beta0) *cp = v;
-          else if (beta1) *cp = *cp + v;
-          else *cp = beta * *cp + v;
+          C[gr + (size_t)gc * ldc] = beta0 ? v : beta1 ? cv[i] + v : beta * cv[i] + v;
         }
       }
     }

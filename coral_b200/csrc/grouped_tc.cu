@@ -36,8 +36,10 @@
 //               two TMEM accumulators of 256 columns, in chunks of at most
 //               32 slabs (1024 K) per accumulation;
 //   warps 10-13 epilogue: tcgen05.ld the accumulator (thread = row), apply
-//               alpha / beta to C with coalesced column accesses; chunks after
-//               the first add alpha * partial into C.
+//               alpha / beta to C with coalesced column accesses (the C loads
+//               of 16 columns issued together before their stores, so a tile
+//               costs a few memory round trips, not one per column); chunks
+//               after the first add alpha * partial into C.
 // Every wait is bounded: a wait that gives up sets the handle's status word
 // (reported by coral_sync) and the CTA winds down.
 #include "common.cuh"
@@ -484,15 +486,22 @@ k_gemm_grouped_tc(const coral_sgemm_problem_t* __restrict__ probs, int count,
           tc::tmem_ld32(tmem + b * kMaxBN + col0 + lane_base, r);
           tc::tmem_wait_ld();
           if (row < p.m) {
+            // every C load of the 32 columns before any store (see below)
             const int lim = min(32, ncols - col0);
+            const bool read_c = c > 0 || !beta0;
 #pragma unroll
-            for (int jj = 0; jj < 32; ++jj) {
-              if (jj >= lim) break;
-              float* cp = crow + (size_t)(ti.n0 + col0 + jj) * p.ldc;
-              const float v = p.alpha * __uint_as_float(r[jj]);
-              if (c > 0 || beta1) *cp = *cp + v;
-              else if (beta0) *cp = v;
-              else *cp = p.beta * *cp + v;
+            for (int h = 0; h < 32; h += 16) {
+              float cv[16];
+#pragma unroll
+              for (int jj = 0; jj < 16; ++jj)
+                cv[jj] = (read_c && h + jj < lim) ? crow[(size_t)(ti.n0 + col0 + h + jj) * p.ldc] : 0.f;
+#pragma unroll
+              for (int jj = 0; jj < 16; ++jj) {
+                if (h + jj >= lim) break;
+                const float v = p.alpha * __uint_as_float(r[h + jj]);
+                crow[(size_t)(ti.n0 + col0 + h + jj) * p.ldc] =
+                    (c > 0 || beta1) ? cv[jj] + v : beta0 ? v : p.beta * cv[jj] + v;
+              }
             }
           }
         }

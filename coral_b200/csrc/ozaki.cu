@@ -396,37 +396,58 @@ k_gemm_ozaki(const __grid_constant__ OzMaps maps, int kdim, int m_tiles, int n_t
       if (row >= ep.m) continue;
       const int ei = max(ep.ea[row], -4000);  // all-zero rows keep the INT_MIN-like fill
       const int col0 = nt * kOzBN + half * kCols;
+      // All C loads (and column exponents) of the tile row before any store:
+      // a store followed by a load the compiler cannot prove disjoint would
+      // cost a memory round trip per column.
+      constexpr int G = 8;  // columns per group of loads
       if (!ep.complex_out) {
         double* crow = ep.C + row;
 #pragma unroll
-        for (int j = 0; j < kCols; ++j) {
-          const int col = col0 + j;
-          if (col >= ep.n) continue;
-          const double v = ep.alpha_re * ldexp(sum[j], ei + max(ep.eb[col], -4000));
-          double* cp = crow + (size_t)col * ep.ldc;
-          if (beta0) *cp = v;
-          else if (beta1) *cp = *cp + v;
-          else *cp = ep.beta_re * *cp + v;
+        for (int g = 0; g < kCols; g += G) {
+          double cv[G];
+          int ej[G];
+#pragma unroll
+          for (int j = 0; j < G; ++j) {
+            const int col = col0 + g + j;
+            cv[j] = (!beta0 && col < ep.n) ? crow[(size_t)col * ep.ldc] : 0.0;
+            ej[j] = col < ep.n ? max(ep.eb[col], -4000) : 0;
+          }
+#pragma unroll
+          for (int j = 0; j < G; ++j) {
+            const int col = col0 + g + j;
+            if (col >= ep.n) continue;
+            const double v = ep.alpha_re * ldexp(sum[g + j], ei + ej[j]);
+            crow[(size_t)col * ep.ldc] = beta0 ? v : beta1 ? cv[j] + v : ep.beta_re * cv[j] + v;
+          }
         }
       } else {
         double2* crow = reinterpret_cast<double2*>(ep.C) + row;
 #pragma unroll
-        for (int j = 0; j < kCols / 2; ++j) {
+        for (int g = 0; g < kCols / 2; g += G / 2) {
+        double2 cvs[G / 2];
+#pragma unroll
+        for (int j0 = 0; j0 < G / 2; ++j0) {
+          const int col = col0 / 2 + g + j0;
+          cvs[j0] = (!beta0 && col < ep.n) ? crow[(size_t)col * ep.ldc] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int j0 = 0; j0 < G / 2; ++j0) {
+          const int j = g + j0;
           const int col = col0 / 2 + j;
           if (col >= ep.n) continue;
           const double ar = ldexp(sum[2 * j], ei + max(ep.eb[2 * col], -4000));
           const double ai = ldexp(sum[2 * j + 1], ei + max(ep.eb[2 * col + 1], -4000));
           double2 v = make_double2(ep.alpha_re * ar - ep.alpha_im * ai, ep.alpha_re * ai + ep.alpha_im * ar);
-          double2* cp = crow + (size_t)col * ep.ldc;
           if (!beta0) {
-            const double2 cv = *cp;
+            const double2 cv = cvs[j0];
             if (beta1) { v.x += cv.x; v.y += cv.y; }
             else {
               v.x += ep.beta_re * cv.x - ep.beta_im * cv.y;
               v.y += ep.beta_re * cv.y + ep.beta_im * cv.x;
             }
           }
-          *cp = v;
+          crow[(size_t)col * ep.ldc] = v;
+        }
         }
       }
     }
