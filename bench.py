@@ -716,6 +716,63 @@ def level12_bandwidth(torch, cb, lib, h, dev, g, routines=None):
     return out
 
 
+def profile_case(torch, cb, case):
+    """Small cases for ncu captures (a few GB on the device at most):
+    `grouped` -- the 4096-instance batch of the batched configuration, bf16
+    then fp32 inputs, two tensor-core grouped calls each; `native` -- SGEMM
+    4096^3 NN and DGEMM 2048^3 NN on the TMA-fed FMA kernel, two calls each;
+    `split` -- SGEMM 4096^3 NN split-BF16x3, two calls."""
+    h = cb.handle()
+    if case == "grouped":
+        rng = np.random.default_rng(2024)
+        count = 4096
+        dims = np.exp(rng.uniform(np.log(16), np.log(512), (count, 3))).astype(np.int64)
+        ops = np.where(rng.uniform(size=count) < 0.5, 0, 1)
+        for bf16 in (True, False):
+            dt = torch.bfloat16 if bf16 else torch.float32
+            ta = int(sum(int(m) * int(k) for m, n, k in dims))
+            tb = int(sum(int(k) * int(n) for m, n, k in dims))
+            tc = int(sum(int(m) * int(n) for m, n, k in dims))
+            pa = torch.empty(ta, device="cuda").uniform_(-1, 1).to(dt)
+            pb = torch.empty(tb, device="cuda").uniform_(-1, 1).to(dt)
+            pc = torch.zeros(tc, device="cuda")
+            rec = np.zeros(count, dtype=cb.sgemm_problem_dtype())
+            oa = ob = oc = 0
+            es = pa.element_size()
+            for i, (m, n, k) in enumerate(dims):
+                m, n, k, op = int(m), int(n), int(k), int(ops[i])
+                rec[i] = (op, 0, m, n, k, 1.5, 0.5, 0, pa.data_ptr() + oa * es, pb.data_ptr() + ob * es,
+                          pc.data_ptr() + oc * 4, m if op == 0 else k, k, m)
+                oa += m * k
+                ob += k * n
+                oc += m * n
+            desc = torch.from_numpy(rec.view(np.uint8)).cuda()
+            h.set_gemm_mode(cb.GemmMode.SPLIT_BF16X3)
+            for _ in range(2):
+                cb.sgemm_grouped(1 if bf16 else 0, count, desc)
+            torch.cuda.synchronize()
+            h.set_gemm_mode(cb.GemmMode.NATIVE)
+    elif case == "native":
+        for dt, n, fn in ((torch.float32, 4096, cb.sgemm), (torch.float64, 2048, cb.dgemm)):
+            A = torch.empty(n * n, dtype=dt, device="cuda").uniform_(-1, 1)
+            B = torch.empty(n * n, dtype=dt, device="cuda").uniform_(-1, 1)
+            C = torch.empty(n * n, dtype=dt, device="cuda").uniform_(-1, 1)
+            for _ in range(2):
+                fn(0, 0, n, n, n, 1.5, A, n, B, n, 0.5, C, n)
+            torch.cuda.synchronize()
+    elif case == "split":
+        n = 4096
+        A = torch.empty(n * n, device="cuda").uniform_(-1, 1)
+        B = torch.empty(n * n, device="cuda").uniform_(-1, 1)
+        C = torch.empty(n * n, device="cuda").uniform_(-1, 1)
+        h.set_gemm_mode(cb.GemmMode.SPLIT_BF16X3)
+        for _ in range(2):
+            cb.sgemm(0, 0, n, n, n, 1.5, A, n, B, n, 0.5, C, n)
+        torch.cuda.synchronize()
+        h.set_gemm_mode(cb.GemmMode.NATIVE)
+    print(json.dumps({"profile_case": case, "ok": True}))
+
+
 def run_ours(args, world, rank, local):
     import torch
     global M, N, K
@@ -730,6 +787,9 @@ def run_ours(args, world, rank, local):
     lib = _lib.load()
     mode = {"native": cb.GemmMode.NATIVE, "split_bf16x3": cb.GemmMode.SPLIT_BF16X3,
             "split_bf16x6": cb.GemmMode.SPLIT_BF16X6}[args.mode]
+    if args.profile_case:  # small ncu cases
+        profile_case(torch, cb, args.profile_case)
+        return
     g = torch.Generator(device=dev)
     g.manual_seed(1234 + rank)
     A = torch.empty(M * K, dtype=torch.float32, device=dev).uniform_(-1, 1, generator=g)
@@ -952,6 +1012,8 @@ def main():
     ap.add_argument("--only-precision", action="store_true", help="run and print the precision-GEMM set only")
     ap.add_argument("--only-batched", action="store_true", help="run and print the batched set only")
     ap.add_argument("--routines", default="", help="with --only-level12: comma list of routines to time")
+    ap.add_argument("--profile-case", choices=["grouped", "native", "split"], default="",
+                    help="run one small case for an ncu capture and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_init(args)
