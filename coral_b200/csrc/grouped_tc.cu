@@ -268,6 +268,34 @@ __device__ __forceinline__ void stage_slab(const SlabSrc<TIn>& src, int k0, uint
   }
 }
 
+// One warp asks the TMA engine to pull a tile's operand panels into L2: the
+// rows (stored contiguous along K) or K columns (stored contiguous along M/N)
+// that the tile's first 1024 K values touch, each as the 16-byte aligned
+// interior of its range, so nothing outside the instance's matrices is named.
+// The producers' slab loads then hit L2 instead of waiting on DRAM.
+template <typename TIn>
+__device__ __forceinline__ void prefetch_tile(const coral_sgemm_problem_t& p, const TileInfo& ti, int lane) {
+  if (ti.nslabs <= 0) return;
+  const int kmax = min(p.k, kChunkSlabs * kTK);
+  for (int op = 0; op < 2; ++op) {
+    const TIn* X = static_cast<const TIn*>(op == 0 ? p.a : p.b);
+    const long long ld = op == 0 ? p.lda : p.ldb;
+    const bool kc = op == 0 ? p.op_a != CORAL_NO_TRANSPOSE : p.op_b == CORAL_NO_TRANSPOSE;
+    const int r0 = op == 0 ? ti.m0 : ti.n0;
+    const int rows = min(op == 0 ? kTM : ti.bn, (op == 0 ? p.m : p.n) - r0);
+    // segment s: a row r0 + s of kmax elements, or a K column s of `rows` elements
+    const int segs = kc ? rows : kmax;
+    const int len = kc ? kmax : rows;
+    for (int sgi = lane; sgi < segs; sgi += 32) {
+      const TIn* base = kc ? X + (size_t)(r0 + sgi) * ld : X + r0 + (size_t)sgi * ld;
+      const uintptr_t a0 = reinterpret_cast<uintptr_t>(base);
+      const uintptr_t s16 = (a0 + 15) & ~uintptr_t(15);
+      const uintptr_t e16 = (a0 + (uintptr_t)len * sizeof(TIn)) & ~uintptr_t(15);
+      if (e16 > s16) tc::prefetch_l2_bulk(reinterpret_cast<const void*>(s16), (uint32_t)(e16 - s16));
+    }
+  }
+}
+
 template <typename TIn, int NPC>
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_gemm_grouped_tc(const coral_sgemm_problem_t* __restrict__ probs, int count,
@@ -374,6 +402,17 @@ k_gemm_grouped_tc(const coral_sgemm_problem_t* __restrict__ probs, int count,
     int it = 0;
     TileInfo ti;
     for (int j = 0; next_tile(j, ti, false); ++j) {
+      if (warp == 1) {
+        // L2 prefetch: this tile's panels on the first tile, then the next
+        // tile's as soon as the scheduler has published it (peeked, not
+        // consumed: its slot cannot be reused before this warp consumes it)
+        if (j == 0 && ti.nslabs > 0) prefetch_tile<TIn>(probs[ti.inst], ti, lane);
+        const int qn = (j + 1) % kQueue;
+        if (tc::mbar_try_wait(&tq_full[qn], ((j + 1) / kQueue) & 1)) {
+          const TileInfo nx = tq[qn];
+          if (nx.inst >= 0 && nx.nslabs > 0) prefetch_tile<TIn>(probs[nx.inst], nx, lane);
+        }
+      }
       if (ti.nslabs == 0) continue;
       const coral_sgemm_problem_t p = probs[ti.inst];
       const SlabSrc<TIn> src{static_cast<const TIn*>(p.a), static_cast<const TIn*>(p.b), p.lda, p.ldb,

@@ -51,3 +51,39 @@ def test_selector_regret_gpu_kernels(cuda):
     choice = tuning.predict_choice(net, shapes)
     r = tuning.regret(times, choice)
     assert r.mean() <= 0.05, r.mean()
+
+
+# ---- grouped GEMM tile-width network ------------------------------------------
+def _load_grouped():
+    d = np.load(os.path.join(DATA, "grouped_timings_heldout.npz"))
+    w = np.load(os.path.join(DATA, "grouped_selector.npz"))
+    return d["samples"], d["times"], w
+
+
+def _default_width(sample):
+    n = int(sample[4])
+    return (64, 128, 128, 256)[0 if n <= 64 else 1 if n <= 128 else 2 if n <= 256 else 3]
+
+
+def test_grouped_selector_regret_cpu_oracle():
+    """The grouped network on 1000 held-out uniform batches (seed 13; every
+    width timed on a B200): the width it predicts fastest against the measured
+    best, from the float64 restatement of the network.  It must stay within 5%
+    on average and beat the default per-class widths."""
+    samples, times, w = _load_grouped()
+    i, h, o = (int(v) for v in w["shape"])
+    choice = tuning.predict_grouped_choice(lambda X: mlp_ref.forward(w["params"], X, i, h, o)[0], samples)
+    r = tuning.regret(times, choice)
+    dflt = tuning.regret(times, np.array([tuning.GROUPED_WIDTHS.index(_default_width(s)) for s in samples]))
+    assert r.mean() <= 0.05, r.mean()
+    assert r.mean() < dflt.mean(), (r.mean(), dflt.mean())
+
+
+def test_grouped_timing_db_shape():
+    samples, times, _ = _load_grouped()
+    assert times.shape == (len(samples), len(tuning.GROUPED_WIDTHS)) and (times > 0).all()
+    train = np.load(os.path.join(DATA, "grouped_timings_train.npz"))
+    assert train["times"].shape == (6000, 3)
+    # both data types and a range of instance counts are present
+    assert set(np.unique(train["samples"][:, 0])) == {0, 1}
+    assert train["samples"][:, 6].min() == 1 and train["samples"][:, 6].max() > 1000
