@@ -44,11 +44,11 @@ ALPHA, BETA = 1.5, 0.5
 GEMV_BYTES = 4 * (M * N + N + 2 * M)  # A once, x once, y read + written
 FP32_FMA_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal: SMs x FP32 lanes x 2 x max clock
 # DRAM bytes (read + write) of one launch of the split GEMM kernel, keyed by
-# (products, m = n = k), from a one-pass ncu launch list of
-# `bench.py --only-gemm --steps 3 --warmup 3`: 2553.4 MB read + 258.3 MB
-# written (median of 6 launches). The bf16 pieces (536 MB) do not fit in the
-# 126 MB L2, and the kernel reads them about 4.8 times over.
-SPLIT_GEMM_TRAFFIC_PER_LAUNCH: dict = {(3, 8192): 2811.68e6}
+# (products, m = n = k), from a one-pass ncu capture of three launches of
+# `bench.py --only-gemm --steps 3 --warmup 3`: 2330 MB read + 260 MB written
+# per launch. The bf16 pieces (536 MB) do not fit in the 126 MB L2, and the
+# kernel reads them about 4.3 times over.
+SPLIT_GEMM_TRAFFIC_PER_LAUNCH: dict = {(3, 8192): 2590.5e6}
 
 
 def peaks():
