@@ -10,10 +10,11 @@
 //
 // The instances' operands have arbitrary leading dimensions and alignments,
 // which tensor maps cannot describe without per-instance host work, so the
-// operands are staged by producer warps instead of TMA: plain loads (16-byte
-// when aligned) coalesced along whichever dimension the instance stores
-// contiguously, conversion to bf16 pieces in registers, and 16-byte shared
-// stores into the K-major 64-byte-swizzled layout that a TMA
+// operands are staged by producer warps instead of TMA: plain loads coalesced
+// along whichever dimension the instance stores contiguously (for an operand
+// stored along K, one warp load covers 32
+// consecutive K values of a row), conversion to bf16 pieces in registers, and
+// shared stores into the K-major 64-byte-swizzled layout that a TMA
 // CU_TENSOR_MAP_SWIZZLE_64B load would write (rows of 32 bf16, 8-row / 512-byte
 // atoms, 16-byte chunk c of row r at chunk c ^ ((r >> 1) & 3)), so the MMA
 // descriptors are the same as the TMA-fed kernels'.
@@ -24,18 +25,17 @@
 // overrides it), instances are ordered by decreasing K bucket (longest tiles
 // first), and the exclusive prefix sum of 128 x BN output tiles is formed.
 //
-// GEMM (k_gemm_grouped_tc, persistent, one CTA per SM, 14 warps):
+// GEMM (k_gemm_grouped_tc, persistent, one CTA per SM, 22 warps):
 //   warp 0      scheduler: takes tile indices from a global atomic counter
 //               (dynamic load balance), decodes (instance, m0, n0, BN) and
 //               publishes them through a 16-deep shared queue;
-//   warps 1-8   producers: stage the K slabs of each tile into a ring of
+//   warps 1-16  producers: stage the K slabs of each tile into a ring of
 //               shared-memory stages (4 for fp32 pieces, 8 for bf16), each
-//               thread issuing the loads of all its items of a slab before
-//               converting any;
-//   warp 9      MMA issuer (lane 0): tcgen05.mma M=128, N=BN, K=16 into one of
+//               thread issuing all its loads of a slab before converting any;
+//   warp 17     MMA issuer (lane 0): tcgen05.mma M=128, N=BN, K=16 into one of
 //               two TMEM accumulators of 256 columns, in chunks of at most
 //               32 slabs (1024 K) per accumulation;
-//   warps 10-13 epilogue: tcgen05.ld the accumulator (thread = row), apply
+//   warps 18-21 epilogue: tcgen05.ld the accumulator (thread = row), apply
 //               alpha / beta to C with coalesced column accesses (the C loads
 //               of 16 columns issued together before their stores, so a tile
 //               costs a few memory round trips, not one per column); chunks
@@ -53,11 +53,11 @@ namespace {
 constexpr int kTM = 128;          // tile rows (TMEM lanes)
 constexpr int kTK = 32;           // K slab: one 64-byte swizzled row of bf16
 constexpr int kMaxBN = 256;
-constexpr int kProdWarps = 8;
+constexpr int kProdWarps = 16;
 constexpr int kEpiWarps = 4;
 constexpr int kMmaWarp = 1 + kProdWarps;
 constexpr int kEpiWarp0 = kMmaWarp + 1;
-constexpr int kTcThreads = 32 * (kEpiWarp0 + kEpiWarps);  // 448
+constexpr int kTcThreads = 32 * (kEpiWarp0 + kEpiWarps);  // 704
 constexpr int kQueue = 16;
 constexpr int kChunkSlabs = 32;
 constexpr uint32_t kAPieceBytes = kTM * kTK * 2;       // 8 KiB
@@ -169,32 +169,6 @@ template <> __device__ __forceinline__ float ld_val<__nv_bfloat16>(const __nv_bf
   return __bfloat162float(__ldg(p));
 }
 
-// Eight consecutive K values (k0 .. k0 + 7) of stored row r of a K-contiguous
-// operand: X[k + r * ld]; zero past Kd.
-template <typename TIn>
-__device__ __forceinline__ void load8_kcontig(const TIn* p, int avail, float (&v)[8]) {
-  if (avail >= 8 && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
-    if constexpr (sizeof(TIn) == 4) {
-      const float4 a = __ldg(reinterpret_cast<const float4*>(p));
-      const float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
-      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-      v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-    } else {
-      const uint4 u = __ldg(reinterpret_cast<const uint4*>(p));
-      const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const float2 f = __bfloat1622float2(h[j]);
-        v[2 * j] = f.x;
-        v[2 * j + 1] = f.y;
-      }
-    }
-    return;
-  }
-#pragma unroll
-  for (int j = 0; j < 8; ++j) v[j] = j < avail ? ld_val<TIn>(p + j) : 0.f;
-}
-
 // Operand views of one tile's K slab for the producers.
 template <typename TIn>
 struct SlabSrc {
@@ -206,94 +180,107 @@ struct SlabSrc {
   int m0, n0, bn;
 };
 
-// Stages one 32-deep K slab of a tile: A rows [m0, m0 + 128) and B rows
-// [n0, n0 + bn) (element (r, k) at X[k + r ld] when stored contiguous along K,
-// else X[r + k ld]; zero outside the matrix) as NPC bf16 piece tiles, A pieces
-// at st + i * kAPieceBytes and B pieces after them, 64-byte swizzled.  A thread
-// handles up to kMaxItems items of 8 K values; it issues the loads of all of
-// them before converting any, so a slab costs one memory round trip rather
-// than one per item.
-template <typename TIn, int NPC>
-__device__ __forceinline__ void stage_slab(const SlabSrc<TIn>& src, int k0, uint8_t* st, int ptid) {
+// Byte offset of element (row r, K position kk) of a slab tile in the
+// 64-byte-swizzled K-major layout (rows of 32 bf16, 8-row / 512-byte atoms,
+// 16-byte chunk c of row r at chunk c ^ ((r >> 1) & 3)).
+__device__ __forceinline__ uint32_t sw64_offset(int r, int kk) {
+  return (uint32_t)(r >> 3) * 512u + (uint32_t)(r & 7) * 64u + (uint32_t)((((kk >> 3) ^ ((r >> 1) & 3)) << 4) +
+                                                                           (kk & 7) * 2);
+}
+
+// Loads one operand's share of a 32-deep slab for this producer thread into
+// v[0 .. kVals): rows [row0, row0 + rows) of an operand stored contiguous
+// along K (element (r, k) at X[k + r ld]) or along the rows (X[r + k ld]).
+//   along K: producer warp pw takes rows pw, pw + 8, ...; lane l holds K
+//     position l, so one warp load reads 32 consecutive elements of a row;
+//   along the rows: item e = (row e % rows, K chunk e / rows) of 8 K values,
+//     lanes on consecutive rows, so each of the 8 loads is one coalesced row
+//     segment.
+// Everything outside R x Kd (and rows past `rows`) reads as zero.
+template <typename TIn, int kVals>
+__device__ __forceinline__ void load_share(const TIn* __restrict__ X, long long ld, bool kc, int R, int Kd,
+                                           int row0, int rows, int k0, int ptid, float (&v)[kVals]) {
   constexpr int kPT = 32 * kProdWarps;
-  constexpr int kMaxItems = (kTM + kMaxBN) * 4 / kPT;
-  const int a_items = kTM * 4;
-  const int total = (kTM + src.bn) * 4;
-  float v[kMaxItems][8];
-  uint32_t off[kMaxItems];
+  const int pw = ptid >> 5, lane = ptid & 31;
 #pragma unroll
-  for (int i = 0; i < kMaxItems; ++i) {
-    const int e = ptid + i * kPT;
-    off[i] = 0xffffffffu;
+  for (int i = 0; i < kVals; ++i) v[i] = 0.f;
+  if (kc) {
+    const int gk = k0 + lane;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) v[i][j] = 0.f;
-    if (e >= total) continue;
-    const bool is_a = e < a_items;
-    const int el = is_a ? e : e - a_items;
-    const int rows = is_a ? kTM : src.bn;
-    const bool kc = is_a ? src.a_kc : src.b_kc;
-    int r, c;
-    if (kc) { r = el >> 2; c = el & 3; }
-    else { r = el % rows; c = el / rows; }
-    off[i] = (is_a ? 0u : (uint32_t)(NPC * kAPieceBytes)) + (uint32_t)(r >> 3) * 512u + (uint32_t)(r & 7) * 64u +
-             (uint32_t)((c ^ ((r >> 1) & 3)) * 16);
-    const int gr = (is_a ? src.m0 : src.n0) + r, gk = k0 + 8 * c;
-    const int avail = src.k - gk;
-    if (gr >= (is_a ? src.m : src.n) || avail <= 0) continue;
-    const TIn* X = is_a ? src.a : src.b;
-    const long long ld = is_a ? src.lda : src.ldb;
-    if (kc) {
-      load8_kcontig<TIn>(X + (size_t)gr * ld + gk, avail, v[i]);
-    } else {
+    for (int i = 0; i < kVals; ++i) {
+      const int r = pw + kProdWarps * i;
+      if (r < rows && row0 + r < R && gk < Kd) v[i] = ld_val<TIn>(X + (size_t)(row0 + r) * ld + gk);
+    }
+  } else {
+#pragma unroll
+    for (int it = 0; it < kVals / 8; ++it) {
+      const int e = ptid + it * kPT;
+      if (e >= rows * 4) continue;
+      const int r = e % rows, c = e / rows;
+      const int gr = row0 + r, gk = k0 + 8 * c;
+      if (gr >= R) continue;
       const TIn* p = X + gr + (size_t)gk * ld;
 #pragma unroll
       for (int j = 0; j < 8; ++j)
-        if (j < avail) v[i][j] = ld_val<TIn>(p + (size_t)j * ld);
+        if (gk + j < Kd) v[it * 8 + j] = ld_val<TIn>(p + (size_t)j * ld);
     }
-  }
-#pragma unroll
-  for (int i = 0; i < kMaxItems; ++i) {
-    if (off[i] == 0xffffffffu) continue;
-    __align__(16) __nv_bfloat16 q[NPC][8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const __nv_bfloat16 h0 = __float2bfloat16_rn(v[i][j]);
-      q[0][j] = h0;
-      if constexpr (NPC == 2) q[1][j] = __float2bfloat16_rn(v[i][j] - __bfloat162float(h0));
-    }
-    const uint32_t piece = off[i] < (uint32_t)(NPC * kAPieceBytes) ? kAPieceBytes : kBPieceBytes;
-#pragma unroll
-    for (int pc = 0; pc < NPC; ++pc)
-      *reinterpret_cast<uint4*>(st + pc * piece + off[i]) = *reinterpret_cast<const uint4*>(q[pc]);
   }
 }
 
-// One warp asks the TMA engine to pull a tile's operand panels into L2: the
-// rows (stored contiguous along K) or K columns (stored contiguous along M/N)
-// that the tile's first 1024 K values touch, each as the 16-byte aligned
-// interior of its range, so nothing outside the instance's matrices is named.
-// The producers' slab loads then hit L2 instead of waiting on DRAM.
-template <typename TIn>
-__device__ __forceinline__ void prefetch_tile(const coral_sgemm_problem_t& p, const TileInfo& ti, int lane) {
-  if (ti.nslabs <= 0) return;
-  const int kmax = min(p.k, kChunkSlabs * kTK);
-  for (int op = 0; op < 2; ++op) {
-    const TIn* X = static_cast<const TIn*>(op == 0 ? p.a : p.b);
-    const long long ld = op == 0 ? p.lda : p.ldb;
-    const bool kc = op == 0 ? p.op_a != CORAL_NO_TRANSPOSE : p.op_b == CORAL_NO_TRANSPOSE;
-    const int r0 = op == 0 ? ti.m0 : ti.n0;
-    const int rows = min(op == 0 ? kTM : ti.bn, (op == 0 ? p.m : p.n) - r0);
-    // segment s: a row r0 + s of kmax elements, or a K column s of `rows` elements
-    const int segs = kc ? rows : kmax;
-    const int len = kc ? kmax : rows;
-    for (int sgi = lane; sgi < segs; sgi += 32) {
-      const TIn* base = kc ? X + (size_t)(r0 + sgi) * ld : X + r0 + (size_t)sgi * ld;
-      const uintptr_t a0 = reinterpret_cast<uintptr_t>(base);
-      const uintptr_t s16 = (a0 + 15) & ~uintptr_t(15);
-      const uintptr_t e16 = (a0 + (uintptr_t)len * sizeof(TIn)) & ~uintptr_t(15);
-      if (e16 > s16) tc::prefetch_l2_bulk(reinterpret_cast<const void*>(s16), (uint32_t)(e16 - s16));
+// Converts and stores what load_share loaded: NPC bf16 pieces of each value
+// at dst + pc * piece_bytes (2-byte stores for the along-K layout, one 16-byte
+// store per item and piece for the along-rows layout).
+template <int NPC, int kVals>
+__device__ __forceinline__ void store_share(uint8_t* dst, uint32_t piece_bytes, bool kc, int rows, int ptid,
+                                            const float (&v)[kVals]) {
+  constexpr int kPT = 32 * kProdWarps;
+  const int pw = ptid >> 5, lane = ptid & 31;
+  if (kc) {
+#pragma unroll
+    for (int i = 0; i < kVals; ++i) {
+      const int r = pw + kProdWarps * i;
+      if (r >= rows) continue;
+      const uint32_t off = sw64_offset(r, lane);
+      const __nv_bfloat16 h0 = __float2bfloat16_rn(v[i]);
+      *reinterpret_cast<__nv_bfloat16*>(dst + off) = h0;
+      if constexpr (NPC == 2)
+        *reinterpret_cast<__nv_bfloat16*>(dst + piece_bytes + off) = __float2bfloat16_rn(v[i] - __bfloat162float(h0));
+    }
+  } else {
+#pragma unroll
+    for (int it = 0; it < kVals / 8; ++it) {
+      const int e = ptid + it * kPT;
+      if (e >= rows * 4) continue;
+      const int r = e % rows, c = e / rows;
+      __align__(16) __nv_bfloat16 q[NPC][8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const __nv_bfloat16 h0 = __float2bfloat16_rn(v[it * 8 + j]);
+        q[0][j] = h0;
+        if constexpr (NPC == 2) q[1][j] = __float2bfloat16_rn(v[it * 8 + j] - __bfloat162float(h0));
+      }
+      const uint32_t off = sw64_offset(r, 8 * c);
+#pragma unroll
+      for (int pc = 0; pc < NPC; ++pc)
+        *reinterpret_cast<uint4*>(dst + pc * piece_bytes + off) = *reinterpret_cast<const uint4*>(q[pc]);
     }
   }
+}
+
+// Stages one 32-deep K slab of a tile: A rows [m0, m0 + 128) and B rows
+// [n0, n0 + bn) as NPC bf16 piece tiles, A pieces at st + i * kAPieceBytes
+// and B pieces after them, 64-byte swizzled.  Every load of the thread's share
+// of both operands is issued before any value is converted, so a slab costs
+// one memory round trip.
+template <typename TIn, int NPC>
+__device__ __forceinline__ void stage_slab(const SlabSrc<TIn>& src, int k0, uint8_t* st, int ptid) {
+  constexpr int kAVals = kTM / kProdWarps;       // 16: along-K rows per warp, or 2 items of 8
+  constexpr int kBVals = kMaxBN / kProdWarps;    // 32: along-K rows per warp, or 4 items of 8
+  float va[kAVals], vb[kBVals];
+  load_share<TIn, kAVals>(src.a, src.lda, src.a_kc, src.m, src.k, src.m0, kTM, k0, ptid, va);
+  load_share<TIn, kBVals>(src.b, src.ldb, src.b_kc, src.n, src.k, src.n0, src.bn, k0, ptid, vb);
+  store_share<NPC, kAVals>(st, kAPieceBytes, src.a_kc, kTM, ptid, va);
+  store_share<NPC, kBVals>(st + NPC * kAPieceBytes, kBPieceBytes, src.b_kc, src.bn, ptid, vb);
 }
 
 template <typename TIn, int NPC>
@@ -402,17 +389,6 @@ k_gemm_grouped_tc(const coral_sgemm_problem_t* __restrict__ probs, int count,
     int it = 0;
     TileInfo ti;
     for (int j = 0; next_tile(j, ti, false); ++j) {
-      if (warp == 1) {
-        // L2 prefetch: this tile's panels on the first tile, then the next
-        // tile's as soon as the scheduler has published it (peeked, not
-        // consumed: its slot cannot be reused before this warp consumes it)
-        if (j == 0 && ti.nslabs > 0) prefetch_tile<TIn>(probs[ti.inst], ti, lane);
-        const int qn = (j + 1) % kQueue;
-        if (tc::mbar_try_wait(&tq_full[qn], ((j + 1) / kQueue) & 1)) {
-          const TileInfo nx = tq[qn];
-          if (nx.inst >= 0 && nx.nslabs > 0) prefetch_tile<TIn>(probs[nx.inst], nx, lane);
-        }
-      }
       if (ti.nslabs == 0) continue;
       const coral_sgemm_problem_t p = probs[ti.inst];
       const SlabSrc<TIn> src{static_cast<const TIn*>(p.a), static_cast<const TIn*>(p.b), p.lda, p.ldb,
@@ -502,11 +478,16 @@ k_gemm_grouped_tc(const coral_sgemm_problem_t* __restrict__ probs, int count,
       const bool beta0 = p.beta == 0.f, beta1 = p.beta == 1.f;
       const int ncols = min(ti.bn, p.n - ti.n0);
       float* crow = p.c + row;
-      if (ti.nslabs == 0) {  // scale-only (sgemm_nn.rs:29-45)
+      if (ti.nslabs == 0) {  // scale-only (sgemm_nn.rs:29-45), 16 C loads before their stores
         if (!beta1 && row < p.m)
-          for (int jj = 0; jj < ncols; ++jj) {
-            float* cp = crow + (size_t)(ti.n0 + jj) * p.ldc;
-            *cp = beta0 ? 0.f : p.beta * *cp;
+          for (int g = 0; g < ncols; g += 16) {
+            float cv[16];
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj)
+              cv[jj] = (!beta0 && g + jj < ncols) ? crow[(size_t)(ti.n0 + g + jj) * p.ldc] : 0.f;
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj)
+              if (g + jj < ncols) crow[(size_t)(ti.n0 + g + jj) * p.ldc] = beta0 ? 0.f : p.beta * cv[jj];
           }
         continue;
       }
@@ -520,27 +501,24 @@ k_gemm_grouped_tc(const coral_sgemm_problem_t* __restrict__ probs, int count,
           break;
         }
         tc::tc_fence_after();
-        for (int col0 = 0; col0 < ncols; col0 += 32) {
-          uint32_t r[32];
-          tc::tmem_ld32(tmem + b * kMaxBN + col0 + lane_base, r);
+        const bool read_c = c > 0 || !beta0;
+        for (int col0 = 0; col0 < ncols; col0 += 16) {
+          // 16 accumulator columns, then every C load of them before any store
+          uint32_t r[16];
+          tc::tmem_ld16(tmem + b * kMaxBN + col0 + lane_base, r);
           tc::tmem_wait_ld();
           if (row < p.m) {
-            // every C load of the 32 columns before any store (see below)
-            const int lim = min(32, ncols - col0);
-            const bool read_c = c > 0 || !beta0;
+            const int lim = min(16, ncols - col0);
+            float cv[16];
 #pragma unroll
-            for (int h = 0; h < 32; h += 16) {
-              float cv[16];
+            for (int jj = 0; jj < 16; ++jj)
+              cv[jj] = (read_c && jj < lim) ? crow[(size_t)(ti.n0 + col0 + jj) * p.ldc] : 0.f;
 #pragma unroll
-              for (int jj = 0; jj < 16; ++jj)
-                cv[jj] = (read_c && h + jj < lim) ? crow[(size_t)(ti.n0 + col0 + h + jj) * p.ldc] : 0.f;
-#pragma unroll
-              for (int jj = 0; jj < 16; ++jj) {
-                if (h + jj >= lim) break;
-                const float v = p.alpha * __uint_as_float(r[h + jj]);
-                crow[(size_t)(ti.n0 + col0 + h + jj) * p.ldc] =
-                    (c > 0 || beta1) ? cv[jj] + v : beta0 ? v : p.beta * cv[jj] + v;
-              }
+            for (int jj = 0; jj < 16; ++jj) {
+              if (jj >= lim) break;
+              const float v = p.alpha * __uint_as_float(r[jj]);
+              crow[(size_t)(ti.n0 + col0 + jj) * p.ldc] =
+                  (c > 0 || beta1) ? cv[jj] + v : beta0 ? v : p.beta * cv[jj] + v;
             }
           }
         }
