@@ -37,6 +37,7 @@ SIGNATURES = {
     "coral_set_wait_limit": [_h, C.c_uint64],
     "coral_set_split_chunk": [_h, _i],
     "coral_set_complex_mapping": [_h, _i],
+    "coral_set_strip_form": [_h, _i],
     "coral_sync": [_h],
     "coral_set_kernel_timing": [_h, _i],
     "coral_get_kernel_timing": [_h, C.POINTER(_d), C.POINTER(C.c_uint64)],

@@ -109,6 +109,10 @@ class Handle:
         """0: 4M (default), 1: 3M, for coral_cgemm in the split-BF16 modes."""
         self.check(self.lib.coral_set_complex_mapping(self.h, mapping), "coral_set_complex_mapping")
 
+    def set_strip_form(self, form: int) -> None:
+        """0: register-streaming SYMV/HEMV/TRMV (default), 1: the TMA-fed single pass when the matrix allows."""
+        self.check(self.lib.coral_set_strip_form(self.h, form), "coral_set_strip_form")
+
     def set_wait_limit(self, spins: int) -> None:
         self.check(self.lib.coral_set_wait_limit(self.h, spins), "coral_set_wait_limit")
 

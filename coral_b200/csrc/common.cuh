@@ -42,6 +42,9 @@ struct Handle {
   int cfg_bn = 0, cfg_splits = 0;
   // Complex GEMM mapping onto real tensor-core products (CORAL_COMPLEX_4M or 3M).
   int complex_mapping = CORAL_COMPLEX_4M;
+  // SYMV / HEMV / TRMV: the TMA-fed single pass (when the matrix allows)
+  // instead of the register-streaming strips.
+  bool tri_tma = false;
   // Tile widths of the tensor-core grouped GEMM per instance class.
   GroupedPolicy grouped_policy{{64, 128, 128, 256}};
   // Learned configuration selector (see selector.cu), or null.

@@ -230,6 +230,13 @@ coral_status_t coral_set_complex_mapping(coral_handle_t handle, int mapping) {
   return CORAL_OK;
 }
 
+coral_status_t coral_set_strip_form(coral_handle_t handle, int form) {
+  CORAL_HANDLE(handle);
+  if (form != CORAL_STRIPS_REGISTER && form != CORAL_STRIPS_TMA) return bad_arg(H, 1);
+  H->tri_tma = form == CORAL_STRIPS_TMA;
+  return CORAL_OK;
+}
+
 coral_status_t coral_set_split_chunk(coral_handle_t handle, int slabs) {
   CORAL_HANDLE(handle);
   if (slabs < 1 || slabs > 1 << 20) return bad_arg(H, 1);

@@ -16,8 +16,16 @@
 //   * k_strip_combine adds, per 32-row strip, its partials in a fixed order
 //     and applies beta (SYMV/HEMV: beta == 0 fills zeros, else multiplies,
 //     ssymv.rs:137-141) or writes x (TRMV).  Results are deterministic.
+//
+// With coral_set_strip_form(CORAL_STRIPS_TMA) an aligned matrix instead takes
+// k_tri_strips_tma, one TMA-fed persistent pass over the whole stored triangle
+// (diagonal blocks included), then the combine: two launches instead of three.
+// On the measured sizes (SSYMV n = 8192, CHEMV n = 4096) it is not faster than
+// the register form, which stays the default.
 #include "common.cuh"
+#include "tc_common.cuh"
 
+#include <cstring>
 #include <type_traits>
 
 namespace coral {
@@ -257,6 +265,16 @@ template <> __device__ __forceinline__ float2 shfl_xor_t<float2>(float2 v, int o
   return make_float2(__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o));
 }
 
+// The value of lane `src`, for each type.
+__device__ __forceinline__ float shfl_idx_t(float v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+__device__ __forceinline__ double shfl_idx_t(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+__device__ __forceinline__ float2 shfl_idx_t(float2 v, int src) {
+  return make_float2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+__device__ __forceinline__ double2 shfl_idx_t(double2 v, int src) {
+  return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
 template <int W, typename T, int N>
 __device__ __forceinline__ void butterfly(T (&acc)[N], int lane, int o) {
   const bool up = (lane & o) != 0;
@@ -398,6 +416,334 @@ k_tri_strips(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// ---- TMA-fed persistent pass ------------------------------------------------------
+// One launch for the whole stored triangle (off-diagonal strips and diagonal
+// blocks), for matrices a tensor map can describe.  A unit is the kS x 64 block of rows
+// [s*kS, s*kS + kS) and columns [J*64, J*64 + 64), kS = 32 * (16 / sizeof(T)):
+// 32 KB for every type.  One CTA per SM takes an equal share of the units,
+// numbered in column-block order (equal-sized units, so the static share is
+// balanced to one unit); its producer thread loads each unit with
+// TMA into a kTsStages-deep ring.  Two groups of four consumer warps take
+// alternate units, so one group's reductions overlap the other's; in a group,
+// warp w reduces columns [16w, 16w + 16): lane l holds rows l*V .. l*V + V - 1
+// of each column (one conflict-free 16-byte shared load per column), forms the
+// row part over its 16 columns and the column part of its 16 columns
+// (butterfly across the lanes, as in k_tri_strips); the four warps' row parts
+// are added in shared memory in warp order.  The x values of a group's next
+// unit are loaded while it reduces the current one.  Column block J's units
+// are the strips meeting its stored rows including its diagonal block (upper:
+// rows [0, J*64 + 64); lower: rows [J*64, n)).  Each stored element (r, c)
+// with r != c adds A(r, c) x(c) to the row part of r and, for SYMV / HEMV,
+// conj?(A(r, c)) x(r) to the column part of c; the diagonal element adds once
+// (a_jj, Re(a_jj) for HEMV, 1 for a unit TRMV), to the row part or, for TRMV
+// T / C, to the column part.  Unstored elements are masked with a select (the
+// unstored triangle may hold NaN); rows and columns past n are zero-filled by
+// TMA.  Column parts are kept per (J, s) unit.  Every wait is bounded: a
+// give-up sets the status word and the CTA drains.
+constexpr int kTsStages = 4;
+constexpr int kTsConsumers = 4;   // warps per consumer group
+constexpr int kTsGroups = 2;
+constexpr int kTsThreads = 32 * (1 + kTsGroups * kTsConsumers);
+constexpr int kTsCtasPerSm = 1;
+constexpr int kTsBoxCols = 64;   // columns per TMA copy (a unit takes kC / kTsBoxCols copies)
+// 1: each CTA takes a contiguous run of units (it streams its column blocks
+// top to bottom); 0: units are dealt round-robin across the CTAs.
+constexpr int kTsContiguous = 1;
+
+// The units of CTA b of g: count, and the i-th one.
+struct UnitShare {
+  int first, count, stride;
+  __device__ __forceinline__ UnitShare(int total, int b, int g) {
+    if (kTsContiguous) {
+      const int per = total / g, rem = total % g;
+      first = b * per + min(b, rem);
+      count = per + (b < rem ? 1 : 0);
+      stride = 1;
+    } else {
+      first = b;
+      count = b < total ? (total - b + g - 1) / g : 0;
+      stride = g;
+    }
+  }
+  __device__ __forceinline__ int unit(int i) const { return first + i * stride; }
+};
+
+// Strips [s_lo, s_hi) holding column block J's stored rows, its diagonal
+// block included: the units of block J in the TMA-fed pass.
+__host__ __device__ __forceinline__ void strip_range_fold(int J, int n, int kS, bool lower, int& s_lo,
+                                                          int& s_hi) {
+  const int c0 = J * kC;
+  const int row_lo = lower ? c0 : 0;
+  const int row_hi = lower ? n : min(c0 + kC, n);
+  s_lo = row_lo / kS;
+  s_hi = row_hi > row_lo ? (row_hi + kS - 1) / kS : s_lo;
+}
+
+// Walks the units of one CTA (or consumer group) in increasing order: unit u
+// lies in column block J, whose units are base .. base + cnt - 1 and start at
+// strip s_lo.  Each walker passes over the column blocks once in all.
+struct UnitWalk {
+  int J = 0, base = 0, cnt = 0, s_lo = 0;
+  __device__ __forceinline__ void start(int n, int kS, bool lower) {
+    int hi;
+    strip_range_fold(0, n, kS, lower, s_lo, hi);
+    cnt = hi - s_lo;
+  }
+  // -> strip of unit u; J names its column block
+  __device__ __forceinline__ int seek(int u, int n, int kS, bool lower) {
+    while (u >= base + cnt) {
+      base += cnt;
+      ++J;
+      int hi;
+      strip_range_fold(J, n, kS, lower, s_lo, hi);
+      cnt = hi - s_lo;
+    }
+    return s_lo + (u - base);
+  }
+};
+
+template <typename T> struct TsVec { using type = T; };
+template <> struct TsVec<float> { using type = float4; };
+template <> struct TsVec<double> { using type = double2; };
+template <> struct TsVec<float2> { using type = float4; };
+
+template <typename T, int V>
+__device__ __forceinline__ void ts_split(const typename TsVec<T>::type& raw, T (&o)[V]) {
+  if constexpr (V == 1) {
+    o[0] = raw;
+  } else {
+    Vec<T, V>::split(raw, o);
+  }
+}
+
+// One consumer lane's view of a unit: where it is and the x values it needs.
+template <typename T, int V>
+struct UnitX {
+  int J, gs;
+  int row_lo, row_hi;   // the block's stored rows, its diagonal block included
+  bool diag;            // the strip meets the diagonal block: classify each element
+  bool rv[V];           // lane's row is a stored off-diagonal row (the rule when !diag)
+  T xi[V];              // x of the lane's rows (column part)
+  T vj;                 // x of column cw * 16 + lane (row part), lanes 0..15
+};
+
+template <typename T, int kMode, int V>
+__device__ __forceinline__ void unit_x(UnitWalk& w, int u, int n, bool lower, const T* __restrict__ x,
+                                       size_t incx, int cw, int lane, UnitX<T, V>& o) {
+  constexpr int kS = 32 * V;
+  constexpr int kP = kC / kTsConsumers;
+  o.gs = w.seek(u, n, kS, lower);
+  o.J = w.J;
+  const int c0 = o.J * kC;
+  o.row_lo = lower ? c0 : 0;
+  o.row_hi = lower ? n : min(c0 + kC, n);
+  o.diag = o.gs * kS < c0 + kC && o.gs * kS + kS > c0;
+  const int off_lo = lower ? c0 + kC : 0, off_hi = lower ? n : c0;
+  const int r0 = o.gs * kS + lane * V;
+#pragma unroll
+  for (int e = 0; e < V; ++e) {
+    const int r = r0 + e;
+    o.rv[e] = r >= off_lo && r < off_hi;
+    o.xi[e] = Cx<T>::zero();
+    if (ModeT<kMode>::kCol && r >= o.row_lo && r < o.row_hi) o.xi[e] = x[(size_t)r * incx];
+  }
+  o.vj = Cx<T>::zero();
+  if (ModeT<kMode>::kRow && lane < kP) {
+    const int gc = c0 + cw * kP + lane;
+    if (gc < n) o.vj = x[(size_t)gc * incx];
+  }
+}
+
+// Element weights of a unit: what element (row rb + e, column cb + c) with
+// value a adds to the row part (row) and to the column part (col).
+// Off-diagonal strips: the stored off-diagonal rows, others masked.
+template <typename T, int V>
+struct PlainWeight {
+  const bool (&rv)[V];
+  __device__ __forceinline__ T row(int, int e, T a) const { return rv[e] ? a : Cx<T>::zero(); }
+  __device__ __forceinline__ T col(int, int e, T a) const { return rv[e] ? a : Cx<T>::zero(); }
+};
+// Strips meeting the diagonal block: the strict triangle (r < c upper, r > c
+// lower) adds to both parts; the diagonal adds a_jj (Re(a_jj) for HEMV, 1 for
+// a unit TRMV) once, to the column part for TRMV T / C, else to the row part.
+template <typename T, int kMode>
+struct DiagWeight {
+  int rb, cb, n;
+  bool lower, unit;
+  __device__ __forceinline__ bool strict(int r, int c) const { return lower ? (r > c && r < n) : r < c; }
+  __device__ __forceinline__ T dval(T a) const {
+    if (kMode == kHemv) return Cx<T>::re(a);
+    if (ModeT<kMode>::kTr && unit) return Cx<T>::one();
+    return a;
+  }
+  __device__ __forceinline__ T row(int c, int e, T a) const {
+    const int r = rb + e, cc = cb + c;
+    return strict(r, cc) ? a : (r == cc && !ModeT<kMode>::kColOnly) ? dval(a) : Cx<T>::zero();
+  }
+  __device__ __forceinline__ T col(int c, int e, T a) const {
+    const int r = rb + e, cc = cb + c;
+    return strict(r, cc) ? a : (r == cc && ModeT<kMode>::kColOnly) ? dval(a) : Cx<T>::zero();
+  }
+};
+
+// A warp's share of a unit: row part into racc (this lane's V rows over the
+// warp's kP columns), column part of the kP columns into colpart.
+template <typename T, int kMode, int V, int kP, typename W>
+__device__ __forceinline__ void reduce_unit(const T (&a)[kP][V], const W& w, const UnitX<T, V>& cur,
+                                            T alpha, int lane, T (&racc)[V], T* __restrict__ colpart, int nstrips,
+                                            int cw) {
+  constexpr bool kSym = ModeT<kMode>::kSym;
+  if (ModeT<kMode>::kRow) {
+    const T vjs = kSym ? scale_x(alpha, cur.vj) : cur.vj;
+#pragma unroll
+    for (int c = 0; c < kP; ++c) {
+      const T vc = shfl_idx_t(vjs, c);
+#pragma unroll
+      for (int e = 0; e < V; ++e) Cx<T>::mac(racc[e], w.row(c, e, a[c][e]), vc);
+    }
+  }
+  if (ModeT<kMode>::kCol) {
+    T xs[V];
+#pragma unroll
+    for (int e = 0; e < V; ++e) xs[e] = kSym ? scale_x(alpha, cur.xi[e]) : cur.xi[e];
+    T v[kP];
+#pragma unroll
+    for (int c = 0; c < kP; ++c) {
+      v[c] = Cx<T>::zero();
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const T wa = w.col(c, e, a[c][e]);
+        Cx<T>::mac(v[c], ModeT<kMode>::kConjCol ? Cx<T>::conj(wa) : wa, xs[e]);
+      }
+    }
+    butterfly<8>(v, lane, 16);
+    butterfly<4>(v, lane, 8);
+    butterfly<2>(v, lane, 4);
+    butterfly<1>(v, lane, 2);
+    const T tot = Cx<T>::add(v[0], shfl_xor_t(v[0], 1));
+    if ((lane & 1) == 0) colpart[((size_t)cur.J * nstrips + cur.gs) * kC + cw * kP + (lane >> 1)] = tot;
+  }
+}
+
+template <typename T, int kMode>
+__global__ void __launch_bounds__(kTsThreads, kTsCtasPerSm)
+k_tri_strips_tma(const __grid_constant__ CUtensorMap map, int n, const T* __restrict__ x, size_t incx,
+                 T alpha, bool lower, bool unit, int total, T* __restrict__ rowpart, T* __restrict__ colpart,
+                 unsigned* status, uint64_t limit_ns) {
+  constexpr int V = 16 / (int)sizeof(T);
+  constexpr int kS = 32 * V;
+  constexpr int kP = kC / kTsConsumers;              // columns per consumer warp
+  constexpr uint32_t kUnitBytes = kS * kC * sizeof(T);
+  constexpr int kMapPerElem = sizeof(T) > 8 ? 2 : 1;   // map elements per T
+  constexpr bool kRow = ModeT<kMode>::kRow;
+  using VT = typename TsVec<T>::type;
+  extern __shared__ __align__(128) uint8_t ts_raw[];
+  uint8_t* ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(ts_raw) + 127) & ~uintptr_t(127));
+  __shared__ __align__(8) uint64_t full_bar[kTsStages], empty_bar[kTsStages];
+  __shared__ __align__(16) T red[kTsGroups][2][kTsConsumers][kS];
+  __shared__ int abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ncol = (n + kC - 1) / kC;
+  const int nstrips = (n + kS - 1) / kS;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kTsStages; ++s) {
+      tc::mbar_init(&full_bar[s], 1);
+      tc::mbar_init(&empty_bar[s], kTsConsumers);
+    }
+    abort_flag = 0;
+    tc::fence_mbar_init();
+  }
+  __syncthreads();
+  UnitWalk walk;
+  walk.start(n, kS, lower);
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- TMA producer ----
+      tc::prefetch_tmap(&map);
+      const UnitShare share(total, blockIdx.x, gridDim.x);
+      int i = 0;
+      for (; i < share.count; ++i) {
+        const int u = share.unit(i);
+        const int st = i % kTsStages;
+        if (i >= kTsStages && !tc::mbar_wait(&empty_bar[st], ((i / kTsStages) - 1) & 1, limit_ns)) {
+          atomicOr(status, kStatusTimeout);
+          atomicExch(&abort_flag, 1);
+          break;
+        }
+        if (*(volatile int*)&abort_flag) break;
+        const int gs = walk.seek(u, n, kS, lower);
+        tc::mbar_expect_tx(&full_bar[st], kUnitBytes);
+#pragma unroll
+        for (int b = 0; b < kC / kTsBoxCols; ++b)
+          tc::tma_load_2d(ring + (size_t)st * kUnitBytes + (size_t)b * kS * kTsBoxCols * sizeof(T), &map,
+                          &full_bar[st], gs * kS * kMapPerElem, walk.J * kC + b * kTsBoxCols);
+      }
+      // every issued copy lands before the CTA may exit
+      for (int j = (i > kTsStages ? i - kTsStages : 0); j < i; ++j)
+        tc::mbar_wait(&full_bar[j % kTsStages], (j / kTsStages) & 1, 1000000000ull);
+    }
+  } else {
+    // ---- consumers: group cg takes the CTA's units cg, cg + 2, ...; warp cw
+    // of the group takes columns [cw * kP, cw * kP + kP) of each ----
+    const int cg = (warp - 1) / kTsConsumers;
+    const int cw = (warp - 1) % kTsConsumers;
+    const int ct = (warp - 1 - cg * kTsConsumers) * 32 + lane;  // 0 .. 127 within the group
+    const UnitShare share(total, blockIdx.x, gridDim.x);
+    UnitX<T, V> nx;
+    if (cg < share.count) unit_x<T, kMode, V>(walk, share.unit(cg), n, lower, x, incx, cw, lane, nx);
+    for (int i = cg, k = 0; i < share.count; i += kTsGroups, ++k) {
+      const UnitX<T, V> cur = nx;
+      if (i + kTsGroups < share.count)
+        unit_x<T, kMode, V>(walk, share.unit(i + kTsGroups), n, lower, x, incx, cw, lane, nx);
+      const int st = i % kTsStages;
+      bool ok = !*(volatile int*)&abort_flag;
+      if (ok && !tc::mbar_wait(&full_bar[st], (i / kTsStages) & 1, limit_ns)) {
+        atomicOr(status, kStatusTimeout);
+        atomicExch(&abort_flag, 1);
+        ok = false;
+      }
+      T racc[V];
+#pragma unroll
+      for (int e = 0; e < V; ++e) racc[e] = Cx<T>::zero();
+      if (ok) {
+        const T* tile = reinterpret_cast<const T*>(ring + (size_t)st * kUnitBytes);
+        T a[kP][V];
+#pragma unroll
+        for (int c = 0; c < kP; ++c) {
+          const VT raw = *reinterpret_cast<const VT*>(tile + (size_t)(cw * kP + c) * kS + lane * V);
+          ts_split<T, V>(raw, a[c]);
+        }
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&empty_bar[st]);
+        if (cur.diag) {
+          const DiagWeight<T, kMode> w{cur.gs * kS + lane * V, cur.J * kC + cw * kP, n, lower, unit};
+          reduce_unit<T, kMode, V, kP>(a, w, cur, alpha, lane, racc, colpart, nstrips, cw);
+        } else {
+          const PlainWeight<T, V> w{cur.rv};
+          reduce_unit<T, kMode, V, kP>(a, w, cur, alpha, lane, racc, colpart, nstrips, cw);
+        }
+      }
+      if (kRow) {
+        // row part: the group's four partials added in warp order (the buffer
+        // alternates with the unit, so one barrier per unit suffices)
+#pragma unroll
+        for (int e = 0; e < V; ++e) red[cg][k & 1][cw][lane * V + e] = racc[e];
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + cg), "n"(32 * kTsConsumers) : "memory");
+        if (ok && ct < kS) {
+          T t = Cx<T>::add(Cx<T>::add(red[cg][k & 1][0][ct], red[cg][k & 1][1][ct]),
+                           Cx<T>::add(red[cg][k & 1][2][ct], red[cg][k & 1][3][ct]));
+          const int r = cur.gs * kS + ct;
+          if (r < cur.row_lo || r >= cur.row_hi) t = Cx<T>::zero();
+          rowpart[((size_t)cur.gs * ncol + cur.J) * kS + ct] = t;
+        }
+      }
+    }
+  }
+  // this CTA's share is written: the combine grid may start launching
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Per 32 output rows: y = beta*y (or 0 for TRMV) + row parts of every
 // off-diagonal column block + the diagonal block's parts + column parts.
 // 8 groups of 32 threads (lane = row) split the column blocks; a group loads
@@ -419,7 +765,7 @@ template <typename T, int kMode, int V>
 __global__ void __launch_bounds__(32 * kCombineGroups)
 k_strip_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
                 const T* __restrict__ rowpart, const T* __restrict__ colpart, int ncolblk,
-                int nsplit, const T* __restrict__ drow, const T* __restrict__ dcol) {
+                int nsplit, int folded, const T* __restrict__ drow, const T* __restrict__ dcol) {
   constexpr int kS = 32 * V;
   constexpr bool kRow = ModeT<kMode>::kRow;
   constexpr bool kCol = ModeT<kMode>::kCol;
@@ -434,8 +780,9 @@ k_strip_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
   const int Jr = min(gr, n - 1) / kC;
   T s = Cx<T>::zero();
   if (kRow) {
-    // off-diagonal column blocks whose stored range covers row gr
-    const int j0 = lower ? 0 : Jr + 1, j1 = lower ? Jr : ncolblk;
+    // column blocks whose stored range covers row gr: the off-diagonal ones,
+    // and with the layout of k_tri_strips_tma (folded) block Jr itself
+    const int j0 = lower ? 0 : (folded ? Jr : Jr + 1), j1 = lower ? (folded ? Jr + 1 : Jr) : ncolblk;
     const T* rp = rowpart + (size_t)gs * ncolblk * kS + li;
     for (int Jb = j0 + g; Jb < j1; Jb += kCombineBatch * kCombineGroups) {
       T a[kCombineBatch];
@@ -448,13 +795,18 @@ k_strip_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
     }
   }
   if (kCol) {
+    // column parts of block Jr: one per CTA split (k_tri_strips), or one per
+    // stored strip [q_lo, q_hi) of the block, its diagonal block included
+    // (k_tri_strips_tma, nsplit = strips)
+    int q_lo = 0, q_hi = nsplit;
+    if (folded) strip_range_fold(Jr, n, kS, lower, q_lo, q_hi);
     const T* cp = colpart + (size_t)Jr * nsplit * kC + gr % kC;
-    for (int qb = g; qb < nsplit; qb += kCombineBatch * kCombineGroups) {
+    for (int qb = q_lo + g; qb < q_hi; qb += kCombineBatch * kCombineGroups) {
       T a[kCombineBatch];
 #pragma unroll
       for (int u = 0; u < kCombineBatch; ++u) {
         const int q = qb + u * kCombineGroups;
-        a[u] = q < nsplit ? cp[(size_t)q * kC] : Cx<T>::zero();
+        a[u] = q < q_hi ? cp[(size_t)q * kC] : Cx<T>::zero();
       }
       s = Cx<T>::add(s, tree_sum(a));
     }
@@ -465,8 +817,10 @@ k_strip_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
   T t = part[0][lane];
 #pragma unroll
   for (int q = 1; q < kCombineGroups; ++q) t = Cx<T>::add(t, part[q][lane]);
-  if (kRow) t = Cx<T>::add(t, drow[gr]);
-  if (ModeT<kMode>::kColOnly) t = Cx<T>::add(t, dcol[gr]);
+  if (!folded) {
+    if (kRow) t = Cx<T>::add(t, drow[gr]);
+    if (ModeT<kMode>::kColOnly) t = Cx<T>::add(t, dcol[gr]);
+  }
   T* yp = y + (size_t)gr * incy;
   if (ModeT<kMode>::kTr) *yp = t;
   else *yp = Cx<T>::add(beta_apply(beta, *yp), t);
@@ -529,8 +883,71 @@ coral_status_t launch_strips(Handle* h, int n, const T* A, size_t lda, const T* 
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   CORAL_CUDA(h, cudaLaunchKernelEx(&cfg, k_strip_combine<T, kMode, V>, n, beta, y, incy, lower,
-                                   static_cast<const T*>(sc), static_cast<const T*>(sc + rp), ncol, nsplit,
+                                   static_cast<const T*>(sc), static_cast<const T*>(sc + rp), ncol, nsplit, 0,
                                    static_cast<const T*>(drow), static_cast<const T*>(dcol)));
+  return launch_status(h);
+}
+
+// TMA-fed form, one launch over the whole stored triangle plus the combine:
+// returns CORAL_ERR_NOT_SUPPORTED, having enqueued nothing, when the matrix
+// cannot be described by a tensor map (the caller then takes the
+// register-streaming form).
+template <typename T, int kMode>
+coral_status_t launch_strips_tma(Handle* h, int n, const T* A, size_t lda, const T* x, size_t incx,
+                                 T alpha, T beta, T* y, size_t incy, bool lower, bool unit) {
+  constexpr int V = 16 / (int)sizeof(T);
+  constexpr int kS = 32 * V;
+  constexpr int kMapElem = sizeof(T) > 8 ? 8 : (int)sizeof(T);
+  constexpr int kMapPerElem = (int)sizeof(T) / kMapElem;
+  constexpr size_t kSmem = (size_t)kTsStages * kS * kC * sizeof(T) + 128;
+  if (!aligned16(A) || (lda * sizeof(T)) % 16) return CORAL_ERR_NOT_SUPPORTED;
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  if (!encode_kmajor_map(&map, A, kMapElem, (uint64_t)n * kMapPerElem, (uint64_t)n, lda * sizeof(T),
+                         (uint32_t)(kS * kMapPerElem), (uint32_t)kTsBoxCols, 0))
+    return CORAL_ERR_NOT_SUPPORTED;
+  const int ncol = (n + kC - 1) / kC;
+  const int nstrips = (n + kS - 1) / kS;
+  int total = 0;
+  for (int J = 0; J < ncol; ++J) {
+    int lo, hi;
+    strip_range_fold(J, n, kS, lower, lo, hi);
+    total += hi - lo;
+  }
+  const size_t rp = (size_t)nstrips * ncol * kS;
+  const size_t cp = (size_t)ncol * nstrips * kC;
+  T* sc = static_cast<T*>(scratch(h, (rp + cp) * sizeof(T)));
+  if (!sc) return CORAL_ERR_ALLOC;
+  static uint64_t attr_devices = 0;  // bit d: attribute set on device d
+  const uint64_t bit = h->device < 64 ? (1ull << h->device) : 0;
+  if (!(attr_devices & bit) || !bit) {
+    CORAL_CUDA(h, cudaFuncSetAttribute(k_tri_strips_tma<T, kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kSmem));
+    attr_devices |= bit;
+  }
+  const int slots = h->sm_count * kTsCtasPerSm;
+  const int grid = total < slots ? total : slots;   // n >= 1: every block has its diagonal unit
+  timed_begin(h);
+  k_tri_strips_tma<T, kMode><<<grid, kTsThreads, kSmem, h->stream>>>(
+      map, n, x, incx, alpha, lower, unit, total, sc, sc + rp, &h->words->status, h->wait_limit * 32ull);
+  coral_status_t s = launch_status(h);
+  timed_end(h);
+  if (s != CORAL_OK) return s;
+  // Programmatic dependent launch: the combine's CTAs are scheduled as the
+  // pass drains instead of after it has fully retired.
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((n + 31) / 32);
+  cfg.blockDim = dim3(32 * kCombineGroups);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CORAL_CUDA(h, cudaLaunchKernelEx(&cfg, k_strip_combine<T, kMode, V>, n, beta, y, incy, lower,
+                                   static_cast<const T*>(sc), static_cast<const T*>(sc + rp), ncol, nstrips, 1,
+                                   static_cast<const T*>(nullptr), static_cast<const T*>(nullptr)));
   return launch_status(h);
 }
 
@@ -540,6 +957,10 @@ coral_status_t run_tri_strips(Handle* h, int n, const T* A, size_t lda, const T*
   static_assert(kC == kT, "diagonal tiles are as wide as the tile columns");
   constexpr int V = (int)(16 / sizeof(T));  // one 16-byte vector per lane and column
   const bool vec = aligned16(A) && (lda * sizeof(T)) % 16 == 0;
+  if (vec && h->tri_tma) {
+    const coral_status_t s = launch_strips_tma<T, kMode>(h, n, A, lda, x, incx, alpha, beta, y, incy, lower, unit);
+    if (s != CORAL_ERR_NOT_SUPPORTED) return s;
+  }
   if (vec) return launch_strips<T, kMode, V>(h, n, A, lda, x, incx, alpha, beta, y, incy, lower, unit);
   return launch_strips<T, kMode, 1>(h, n, A, lda, x, incx, alpha, beta, y, incy, lower, unit);
 }

@@ -79,6 +79,12 @@ enum {
                            by (|Re A| + |Im A|)(|Re B| + |Im B|) */
 };
 
+/* Kernel form of SYMV / HEMV / TRMV (coral_set_strip_form). */
+enum {
+  CORAL_STRIPS_REGISTER = 0, /* register-streaming strips, diagonal tiles on a side stream, combine */
+  CORAL_STRIPS_TMA = 1       /* one TMA-fed persistent pass over the whole triangle, combine */
+};
+
 typedef struct coral_handle_s* coral_handle_t;
 
 /* ---- handle ------------------------------------------------------------ */
@@ -95,6 +101,12 @@ coral_status_t coral_get_gemm_mode(coral_handle_t handle, int* mode);
 coral_status_t coral_set_split_chunk(coral_handle_t handle, int slabs);
 /* Complex mapping of the emulated CGEMM / ZGEMM: CORAL_COMPLEX_4M (default) or 3M. */
 coral_status_t coral_set_complex_mapping(coral_handle_t handle, int mapping);
+/* Kernel form of the SYMV / HEMV / TRMV family: CORAL_STRIPS_REGISTER
+ * (default, the faster on the measured sizes) or CORAL_STRIPS_TMA (used when
+ * the matrix is 16-byte aligned with a leading dimension of a multiple of 16
+ * bytes, else the register form runs). Results agree to rounding; the two
+ * forms add the partials of a row in different orders. */
+coral_status_t coral_set_strip_form(coral_handle_t handle, int form);
 /* Iteration limit of every bounded device wait (0 restores the default). */
 coral_status_t coral_set_wait_limit(coral_handle_t handle, uint64_t spins);
 /* Kernel timing: when enabled, the handle brackets the dominant kernel of each
