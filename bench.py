@@ -44,11 +44,13 @@ ALPHA, BETA = 1.5, 0.5
 GEMV_BYTES = 4 * (M * N + N + 2 * M)  # A once, x once, y read + written
 FP32_FMA_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal: SMs x FP32 lanes x 2 x max clock
 # DRAM bytes (read + write) of one launch of the split GEMM kernel, keyed by
-# (products, m = n = k), from a one-pass ncu capture of three launches of
-# `bench.py --only-gemm --steps 3 --warmup 3`: 2330 MB read + 260 MB written
-# per launch. The bf16 pieces (536 MB) do not fit in the 126 MB L2, and the
-# kernel reads them about 4.3 times over.
-SPLIT_GEMM_TRAFFIC_PER_LAUNCH: dict = {(3, 8192): 2590.5e6}
+# (products, m = n = k, tile height), from one-pass ncu captures of
+# `bench.py --only-gemm`: the 128 x 256 single-CTA tiles 2330 MB read + 260 MB
+# written per launch; the 256 x 256 CTA-pair tiles 2464 MB read + 265 MB
+# written (one launch, `-k regex:k_gemm_split_pair -c 1`). The bf16 pieces
+# (536 MB) do not fit in the 126 MB L2, and the kernels read them 4.3-4.6
+# times over.
+SPLIT_GEMM_TRAFFIC_PER_LAUNCH: dict = {(3, 8192, 128): 2590.5e6, (3, 8192, 256): 2729.0e6}
 
 
 def peaks():
@@ -952,9 +954,12 @@ def run_ours(args, world, rank, local):
                 "peak_source": "nominal FP32 FMA pipe at max clock (no measured figure)"}
     else:
         products = 3 if mode == cb.GemmMode.SPLIT_BF16X3 else 6
+        tile_m, tile_n, _ = h.gemm_tile(products, 0, 0, M, N, K)
+        kname = (f"k_gemm_split_pair<{products}> (256 x 256 tile on a CTA pair)" if tile_m == 256
+                 else f"k_gemm_split<{products}, {tile_n}>")
         roof = {"bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
-                "frac": ach / bf16, "traffic": SPLIT_GEMM_TRAFFIC_PER_LAUNCH.get((products, M)),
-                "kernel": f"k_gemm_split<{products}>", "kernel_ms": kernel_ms,
+                "frac": ach / bf16, "traffic": SPLIT_GEMM_TRAFFIC_PER_LAUNCH.get((products, M, tile_m)),
+                "kernel": kname, "kernel_ms": kernel_ms,
                 "tensor_issue_frac": products * ach / bf16,
                 "peak_source": ("measured bf16 dense burst (MEASURED_PEAKS.json)" if src == "measured"
                                 else "fallback bf16 dense burst (1.59 PFLOP/s; no MEASURED_PEAKS.json)"),

@@ -141,6 +141,12 @@ SIGNATURES = {
     "coral_get_grouped_config": [_h, _vp],
     "coral_autotune_sgemm_grouped": [_h, _i, _sz, _vp, _i, _vp, C.POINTER(_i), _vp],
     "coral_set_gemm_config": [_h, _i, _i],
+    "coral_set_gemm_tile": [_h, _i, _i, _i],
+    "coral_get_gemm_tile": [_h, _i, _i, _i, _sz, _sz, _sz, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)],
+    "coral_set_pair_raster": [_h, _i],
+    "coral_autotune_sgemm_tiles": [_h, _i, _i, _i, _sz, _sz, _sz, _vp, _sz, _vp, _sz, _vp, _sz, _i,
+                                   C.POINTER(_f), _i, C.POINTER(_i), C.POINTER(_i)],
+    "coral_selector_features_tile": [_i, _i, _i, _sz, _sz, _sz, _i, _i, _i, C.POINTER(_f)],
     "coral_get_gemm_config": [_h, _i, _i, _i, _sz, _sz, _sz, C.POINTER(_i), C.POINTER(_i)],
     "coral_selector_features": [_i, _i, _i, _sz, _sz, _sz, _i, _i, C.POINTER(_f)],
     "coral_autotune_sgemm": [_h, _i, _i, _i, _sz, _sz, _sz, _vp, _sz, _vp, _sz, _vp, _sz, _i,

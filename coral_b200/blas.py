@@ -113,6 +113,20 @@ class Handle:
         """0: register-streaming SYMV/HEMV/TRMV (default), 1: the TMA-fed single pass when the matrix allows."""
         self.check(self.lib.coral_set_strip_form(self.h, form), "coral_set_strip_form")
 
+    def set_gemm_tile(self, tile_m: int, tile_n: int, split_k: int) -> None:
+        """Split-GEMM tile: (128, 128 | 256) one CTA per tile, (256, 256) a CTA pair; zeros: policy."""
+        self.check(self.lib.coral_set_gemm_tile(self.h, tile_m, tile_n, split_k), "coral_set_gemm_tile")
+
+    def gemm_tile(self, products: int, op_a: int, op_b: int, m: int, n: int, k: int) -> tuple[int, int, int]:
+        """(tile_m, tile_n, split_k) a split GEMM of this shape would use now."""
+        tm, tn, sk = C.c_int(), C.c_int(), C.c_int()
+        self.check(self.lib.coral_get_gemm_tile(self.h, products, op_a, op_b, m, n, k, C.byref(tm),
+                                                C.byref(tn), C.byref(sk)), "coral_get_gemm_tile")
+        return tm.value, tn.value, sk.value
+
+    def set_pair_raster(self, group: int) -> None:
+        self.check(self.lib.coral_set_pair_raster(self.h, group), "coral_set_pair_raster")
+
     def set_wait_limit(self, spins: int) -> None:
         self.check(self.lib.coral_set_wait_limit(self.h, spins), "coral_set_wait_limit")
 
@@ -787,6 +801,10 @@ def set_gemm_mode(mode: int) -> None:
 
 def gemm_mode() -> int:
     return handle().gemm_mode()
+
+
+def set_gemm_tile(tile_m: int, tile_n: int, split_k: int = 0) -> None:
+    handle().set_gemm_tile(tile_m, tile_n, split_k)
 
 
 # ------------------------------------------------------- batched (no reference) --

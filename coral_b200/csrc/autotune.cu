@@ -1,5 +1,5 @@
 // Exhaustive autotuning of the split-BF16 SGEMM configuration for one shape
-// (no reference counterpart).  Every candidate (tile width x split-K) runs
+// (no reference counterpart).  Every candidate (tile shape x split-K) runs
 // once untimed and `reps` times between CUDA events on the handle's stream;
 // all candidates are enqueued before the single synchronisation, so the
 // measurement does not include host round trips.
@@ -34,6 +34,8 @@ extern "C" coral_status_t coral_autotune_sgemm(coral_handle_t hh, int products, 
   coral_status_t st = CORAL_OK;
   for (auto& e : ev)
     if (cudaEventCreate(&e) != cudaSuccess) st = CORAL_ERR_CUDA;
+  const int saved_bm = H->cfg_bm;
+  H->cfg_bm = 128;
   for (size_t i = 0; i < cands.size() && st == CORAL_OK; ++i) {
     H->cfg_bn = cands[i].bn;
     H->cfg_splits = cands[i].sp;
@@ -60,6 +62,62 @@ extern "C" coral_status_t coral_autotune_sgemm(coral_handle_t hh, int products, 
   H->gemm_mode = saved_mode;
   H->cfg_bn = saved_bn;
   H->cfg_splits = saved_sp;
+  H->cfg_bm = saved_bm;
+  return st;
+}
+
+// Exhaustive tuning over the tile shapes as well: the configurations of
+// split_candidates() (CTA-pair 256 x 256, 128 x 256 and 128 x 128 tiles, each
+// with split-K 1..16), timed like coral_autotune_sgemm.
+extern "C" coral_status_t coral_autotune_sgemm_tiles(coral_handle_t hh, int products, int op_a, int op_b,
+                                                     size_t m, size_t n, size_t k, const float* a,
+                                                     size_t lda, const float* b, size_t ldb, float* c,
+                                                     size_t ldc, int reps, float* ms_out, int capacity,
+                                                     int* count, int* best) {
+  CORAL_HANDLE(hh);
+  if (products != 3 && products != 6) return bad_arg(H, 1);
+  if (reps < 1) return bad_arg(H, 14);
+  if (!ms_out) return bad_arg(H, 15);
+  if (!count) return bad_arg(H, 17);
+  if (!best) return bad_arg(H, 18);
+  SplitConfig cands[15];
+  const int nc = split_candidates(products, cands);
+  if (capacity < nc) return bad_arg(H, 16);
+  const int saved_mode = H->gemm_mode, saved_bn = H->cfg_bn, saved_sp = H->cfg_splits, saved_bm = H->cfg_bm;
+  H->gemm_mode = products == 6 ? CORAL_GEMM_SPLIT_BF16X6 : CORAL_GEMM_SPLIT_BF16X3;
+  std::vector<cudaEvent_t> ev(2 * nc, nullptr);
+  coral_status_t st = CORAL_OK;
+  for (auto& e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) st = CORAL_ERR_CUDA;
+  for (int i = 0; i < nc && st == CORAL_OK; ++i) {
+    H->cfg_bm = cands[i].pair ? 256 : 128;
+    H->cfg_bn = cands[i].bn;
+    H->cfg_splits = cands[i].splits;
+    st = coral_sgemm(hh, op_a, op_b, m, n, k, 1.0f, a, lda, b, ldb, 0.0f, c, ldc);
+    if (st != CORAL_OK) break;
+    cudaEventRecord(ev[2 * i], H->stream);
+    for (int r = 0; r < reps && st == CORAL_OK; ++r)
+      st = coral_sgemm(hh, op_a, op_b, m, n, k, 1.0f, a, lda, b, ldb, 0.0f, c, ldc);
+    cudaEventRecord(ev[2 * i + 1], H->stream);
+  }
+  if (st == CORAL_OK && cudaStreamSynchronize(H->stream) != cudaSuccess) st = CORAL_ERR_CUDA;
+  if (st == CORAL_OK) {
+    int bi = 0;
+    for (int i = 0; i < nc; ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
+      ms_out[i] = ms / (float)reps;
+      if (ms_out[i] < ms_out[bi]) bi = i;
+    }
+    *best = bi;
+    *count = nc;
+  }
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  H->gemm_mode = saved_mode;
+  H->cfg_bn = saved_bn;
+  H->cfg_splits = saved_sp;
+  H->cfg_bm = saved_bm;
   return st;
 }
 

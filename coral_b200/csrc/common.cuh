@@ -38,8 +38,11 @@ struct Handle {
   uint64_t wait_limit = kDefaultWaitLimit;
   // K slabs (64 deep) per tensor-core accumulation chunk of the split GEMMs.
   int split_chunk_kb = 16;
-  // Explicit split-GEMM configuration (0 = not set): N tile width, split-K.
-  int cfg_bn = 0, cfg_splits = 0;
+  // Explicit split-GEMM configuration (0 = not set): N tile width, split-K,
+  // and tile height (128: one CTA per tile; 256: a CTA pair per 256 x 256 tile).
+  int cfg_bn = 0, cfg_splits = 0, cfg_bm = 0;
+  // M-tiles per raster group of the CTA-pair split GEMM (0: the default, 8).
+  int pair_group = 0;
   // Complex GEMM mapping onto real tensor-core products (CORAL_COMPLEX_4M or 3M).
   int complex_mapping = CORAL_COMPLEX_4M;
   // SYMV / HEMV / TRMV: the TMA-fed single pass (when the matrix allows)
@@ -141,10 +144,12 @@ inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 
 // pointer mode (host: waits on the stream).
 coral_status_t deliver_result(Handle* h, void* dst, const void* src, size_t bytes);
 
-// Split-BF16 GEMM configuration (tile width BN, split-K factor).
+// Split-BF16 GEMM configuration (tile width BN, split-K factor, and whether a
+// CTA pair computes a 256 x 256 tile).
 struct SplitConfig {
   int bn;
   int splits;
+  int pair = 0;
 };
 // Shape of a split-BF16 GEMM call as the configuration policy sees it:
 // op(A) rows mr, B-rows nr (2n for complex), depth kd (2k for complex).
@@ -160,7 +165,12 @@ SplitConfig choose_split_config(Handle* h, const SplitShape& sh);
 bool select_split_config(Handle* h, const SplitShape& sh, SplitConfig* out);
 // Features of (shape, configuration) for the selector network.
 constexpr int kSelectorFeatures = 13;
-void selector_features(const SplitShape& sh, int bn, int splits, float* f);
+void selector_features(const SplitShape& sh, int bm, int bn, int splits, float* f);
+// Split-GEMM configurations the selector and the exhaustive tile autotuner
+// consider, in their documented order: tiles (256 x 256 CTA pair, 128 x 256,
+// 128 x 128) x split-K (1, 2, 4, 8, 16); the 3-piece mode has no 128 x 256
+// tile.  Writes up to 15 configurations; returns the count.
+int split_candidates(int products, SplitConfig* out);
 
 // Tensor-core grouped GEMM (grouped_tc.cu): bf16 inputs, or fp32 inputs as
 // split-BF16x3; descriptors in device memory.

@@ -699,6 +699,301 @@ k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int 
   if (warp == 1) tc::tmem_dealloc(tmem, 2 * BN);
 }
 
+// ---- 2b. CTA-pair tcgen05 GEMM (cta_group::2) ---------------------------------
+// A 256 x 256 tile of C per cluster of two CTAs on two SMs.  For each 32-deep
+// K slab, CTA r (r = 0, 1) stages rows [128 r, 128 r + 128) of the tile's A
+// pieces and of its B pieces; the even CTA issues tcgen05.mma.cta_group::2
+// (M = 256, N = 256, K = 16), which reads A and B from both CTAs' shared
+// memory and accumulates rows [128 r, 128 r + 128) x 256 columns into CTA r's
+// TMEM.  Per SM an instruction reads 128 rows of B where the single-CTA
+// 128 x 256 tile reads 256, so the B operand's shared-memory traffic per flop
+// halves, and each CTA's ring slot is 32 KB instead of 48 KB (6 stages).
+// Barriers:
+//   full_bar[s]   even CTA only: armed by its producer with both CTAs' bytes;
+//                 both CTAs' TMA loads count on it (.cta_group::2 loads);
+//   empty_bar[s]  both CTAs: the MMA commit multicast to the pair;
+//   chunk_full[b] both CTAs: likewise, after a chunk's last MMA;
+//   chunk_empty[b] even CTA only: 2 x kEpiWarps arrivals, the odd CTA's
+//                 epilogue warps arriving through the cluster window.
+// Epilogue, split-K and the K-serpentine order follow k_gemm_split.  Every
+// wait is bounded; a CTA that gives up sets the status word, and its partner's
+// waits then run out too, so both CTAs reach the closing cluster barrier.
+constexpr int kPairHalf = 128;  // rows of A and of B staged per CTA
+constexpr int kPairTile = 256;  // tile edge in M and N
+
+template <int NP>
+struct PairRing {
+  static constexpr int kPieces = SplitPlan<NP>::kPieces;
+  static constexpr uint32_t kPieceTile = kPairHalf * kBK * 2;            // 8 KB
+  static constexpr uint32_t kStageBytes = 2 * kPieces * kPieceTile;      // this CTA's A and B pieces
+  static constexpr int kStages = NP == 3 ? 6 : 4;
+};
+
+// Tile order for the pair kernel: groups of `group` M-tiles sweep all N-tiles.
+__device__ __forceinline__ void tile_coords_g(int tile, int m_tiles, int group, int& mt, int& nt,
+                                              int n_tiles) {
+  const int per_group = group * n_tiles;
+  const int g = tile / per_group;
+  const int gm0 = g * group;
+  const int gsz = min(group, m_tiles - gm0);
+  const int within = tile - g * per_group;
+  mt = gm0 + within % gsz;
+  nt = within / gsz;
+}
+
+template <typename Plan>
+__device__ __forceinline__ void mma_plan_pair(int q, uint32_t acc, uint64_t ad, uint64_t bd,
+                                              uint32_t idesc, uint32_t accumulate) {
+  switch (Plan::collect(q)) {
+    case tc::kCollectFill: tc::mma_f16_pair<tc::kCollectFill>(acc, ad, bd, idesc, accumulate); break;
+    case tc::kCollectUse: tc::mma_f16_pair<tc::kCollectUse>(acc, ad, bd, idesc, accumulate); break;
+    case tc::kCollectLastUse: tc::mma_f16_pair<tc::kCollectLastUse>(acc, ad, bd, idesc, accumulate); break;
+    default: tc::mma_f16_pair<tc::kCollectNone>(acc, ad, bd, idesc, accumulate); break;
+  }
+}
+
+template <int NP>
+__global__ void __launch_bounds__(kSplitThreads, 1)
+k_gemm_split_pair(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int n_tiles, int group,
+                  int chunk_kb, int splits, float* ws, int ws_cols, EpiParams ep, unsigned* status,
+                  uint64_t limit_ns) {
+  using Plan = SplitPlan<NP>;
+  using Ring = PairRing<NP>;
+  constexpr int kPieces = Ring::kPieces;
+  constexpr int kS = Ring::kStages;
+  constexpr uint32_t kPieceTile = Ring::kPieceTile;
+  constexpr uint32_t kStageBytes = Ring::kStageBytes;
+  constexpr uint32_t kIdesc = tc::idesc_bf16_f32(kPairTile, kPairTile);
+  constexpr int kCols = kPairTile / 2;  // accumulator columns per epilogue thread
+  constexpr uint16_t kPairMask = 3;
+
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ __align__(8) uint64_t full_bar[kS], empty_bar[kS];
+  __shared__ __align__(8) uint64_t chunk_full[2], chunk_empty[2];
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = tc::cluster_ctarank();
+  const int cluster = (int)(blockIdx.x >> 1), nclusters = (int)(gridDim.x >> 1);
+  const int nk = (kdim + kBK - 1) / kBK;
+  const int total_items = m_tiles * n_tiles * splits;
+  const int sk = (nk + splits - 1) / splits;
+  auto slab_range = [&](int item, int& lo, int& hi) {
+    const int part = item % splits;
+    lo = min(nk, part * sk);
+    hi = min(nk, lo + sk);
+  };
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kS; ++s) {
+      tc::mbar_init(&full_bar[s], 1);
+      tc::mbar_init(&empty_bar[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(&chunk_full[b], 1);
+      tc::mbar_init(&chunk_empty[b], 2 * kEpiWarps);
+    }
+    abort_flag = 0;
+    tc::fence_mbar_init();
+  }
+  if (warp == 1) {
+    tc::tmem_alloc_pair(&tmem_slot, 2 * kPairTile);
+    tc::tmem_relinquish_pair();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::cluster_sync();  // both CTAs' barriers exist before any remote use
+  tc::tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- TMA producer (both CTAs) ----
+      for (int p = 0; p < kPieces; ++p) {
+        tc::prefetch_tmap(&maps.a[p]);
+        tc::prefetch_tmap(&maps.b[p]);
+      }
+      int it = 0;
+      for (int item = cluster; item < total_items && !abort_flag; item += nclusters) {
+        int mt, nt, kb_lo, kb_hi;
+        tile_coords_g(item / splits, m_tiles, group, mt, nt, n_tiles);
+        slab_range(item, kb_lo, kb_hi);
+        const bool down = ((item / nclusters) & 1) != 0;
+        const int row_a = mt * kPairTile + (int)rank * kPairHalf;
+        const int row_b = nt * kPairTile + (int)rank * kPairHalf;
+        for (int j = 0; j < kb_hi - kb_lo; ++j, ++it) {
+          const int kb = down ? kb_hi - 1 - j : kb_lo + j;
+          const int s = it % kS;
+          if (it >= kS && !tc::mbar_wait(&empty_bar[s], ((it / kS) - 1) & 1, limit_ns)) {
+            atomicOr(status, kStatusTimeout);
+            atomicExch(&abort_flag, 1);
+            break;
+          }
+          if (*(volatile int*)&abort_flag) break;
+          uint8_t* st = smem + (size_t)s * kStageBytes;
+          if (rank == 0) tc::mbar_expect_tx(&full_bar[s], 2 * kStageBytes);
+          const uint32_t fb = tc::mapa_shared(tc::smem_u32(&full_bar[s]), 0);
+          for (int p = 0; p < kPieces; ++p) {
+            tc::tma_load_2d_pair(st + p * kPieceTile, &maps.a[p], fb, kb * kBK, row_a);
+            tc::tma_load_2d_pair(st + (kPieces + p) * kPieceTile, &maps.b[p], fb, kb * kBK, row_b);
+          }
+        }
+      }
+      // Drain: a slab's loads have landed once the MMA that read it released
+      // the slot, so wait for the last slots' releases before exiting.
+      for (int j = (it > kS ? it - kS : 0); j < it; ++j)
+        tc::mbar_wait(&empty_bar[j % kS], (j / kS) & 1, limit_ns);
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && rank == 0) {
+      // ---- MMA issuer (even CTA) ----
+      int it = 0, gc = 0;
+      bool stop = false;
+      for (int item = cluster; item < total_items && !stop; item += nclusters) {
+        int kb_lo, kb_hi;
+        slab_range(item, kb_lo, kb_hi);
+        const int chunks = (kb_hi - kb_lo + chunk_kb - 1) / chunk_kb;
+        for (int c = 0; c < chunks && !stop; ++c, ++gc) {
+          const int b = gc & 1;
+          if (gc >= 2 && !tc::mbar_wait(&chunk_empty[b], ((gc >> 1) - 1) & 1, limit_ns)) {
+            atomicOr(status, kStatusTimeout);
+            atomicExch(&abort_flag, 1);
+            stop = true;
+            break;
+          }
+          tc::tc_fence_after();
+          const uint32_t acc = tmem + b * kPairTile;
+          const int kb0 = kb_lo + c * chunk_kb, kb1 = min(kb_hi, kb0 + chunk_kb);
+          for (int kb = kb0; kb < kb1; ++kb, ++it) {
+            const int s = it % kS;
+            if (!tc::mbar_wait(&full_bar[s], (it / kS) & 1, limit_ns)) {
+              atomicOr(status, kStatusTimeout);
+              atomicExch(&abort_flag, 1);
+              stop = true;
+              break;
+            }
+            tc::tc_fence_after();
+            const uint32_t sa = tc::smem_u32(smem + (size_t)s * kStageBytes);
+            const uint32_t sb = sa + kPieces * kPieceTile;
+#pragma unroll
+            for (int kk = 0; kk < kBK / 16; ++kk) {
+#pragma unroll
+              for (int q = 0; q < Plan::kProducts; ++q) {
+                const uint64_t ad = slab_desc(sa + Plan::a(q) * kPieceTile + kk * 32);
+                const uint64_t bd = slab_desc(sb + Plan::b(q) * kPieceTile + kk * 32);
+                mma_plan_pair<Plan>(q, acc, ad, bd, kIdesc, ((kb - kb0) | kk | q) != 0);
+              }
+            }
+            tc::mma_commit_pair(&empty_bar[s], kPairMask);
+          }
+          tc::mma_commit_pair(&chunk_full[b], kPairMask);
+        }
+      }
+    }
+  } else {
+    // ---- epilogue warps (both CTAs): rows [128 r, 128 r + 128) of the tile ----
+    const int ew = warp - 2;
+    const int quad = warp & 3;
+    const int half = ew >> 2;
+    const uint32_t lane_base = (uint32_t)(quad * 32) << 16;
+    const bool beta0 = ep.beta_re == 0.f && ep.beta_im == 0.f;
+    const bool beta1 = ep.beta_re == 1.f && ep.beta_im == 0.f;
+    int gc = 0;
+    bool stop = false;
+    for (int item = cluster; item < total_items && !stop; item += nclusters) {
+      int mt, nt, kb_lo, kb_hi;
+      tile_coords_g(item / splits, m_tiles, group, mt, nt, n_tiles);
+      slab_range(item, kb_lo, kb_hi);
+      const int chunks = (kb_hi - kb_lo + chunk_kb - 1) / chunk_kb;
+      float sum[kCols];
+#pragma unroll
+      for (int j = 0; j < kCols; ++j) sum[j] = 0.f;
+      for (int c = 0; c < chunks; ++c, ++gc) {
+        const int b = gc & 1;
+        if (!tc::mbar_wait(&chunk_full[b], (gc >> 1) & 1, limit_ns)) {
+          atomicOr(status, kStatusTimeout);
+          stop = true;
+          break;
+        }
+        tc::tc_fence_after();
+        const uint32_t acc = tmem + b * kPairTile + half * kCols + lane_base;
+#pragma unroll
+        for (int c0 = 0; c0 < kCols; c0 += 32) {
+          uint32_t r[32];
+          tc::tmem_ld32(acc + c0, r);
+          tc::tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 32; ++j) sum[c0 + j] += __uint_as_float(r[j]);
+        }
+        tc::tc_fence_before();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive_cluster(tc::mapa_shared(tc::smem_u32(&chunk_empty[b]), 0));
+      }
+      if (stop || *(volatile int*)&abort_flag) break;
+      const int row = mt * kPairTile + (int)rank * kPairHalf + quad * 32 + lane;
+      if (row >= ep.m) continue;
+      const int col0 = nt * kPairTile + half * kCols;
+      if (splits > 1) {
+        float* wp = ws + ((size_t)(item % splits) * ws_cols) * ep.m + row;
+#pragma unroll
+        for (int j = 0; j < kCols; ++j)
+          if (col0 + j < ws_cols) wp[(size_t)(col0 + j) * ep.m] = sum[j];
+      } else if (!ep.complex_out) {
+        float* crow = ep.C + row;
+#pragma unroll
+        for (int g = 0; g < kCols; g += kCGroup) {
+          float cv[kCGroup];
+#pragma unroll
+          for (int j = 0; j < kCGroup; ++j)
+            cv[j] = (!beta0 && col0 + g + j < ep.n) ? crow[(size_t)(col0 + g + j) * ep.ldc] : 0.f;
+#pragma unroll
+          for (int j = 0; j < kCGroup; ++j) {
+            const int col = col0 + g + j;
+            if (col < ep.n) {
+              const float v = ep.alpha_re * sum[g + j];
+              crow[(size_t)col * ep.ldc] = beta0 ? v : beta1 ? cv[j] + v : ep.beta_re * cv[j] + v;
+            }
+          }
+        }
+      } else {
+        float2* crow = reinterpret_cast<float2*>(ep.C) + row;
+#pragma unroll
+        for (int g = 0; g < kCols / 2; g += kCGroup / 2) {
+          float2 cvs[kCGroup / 2];
+#pragma unroll
+          for (int j = 0; j < kCGroup / 2; ++j)
+            cvs[j] = (!beta0 && col0 / 2 + g + j < ep.n) ? crow[(size_t)(col0 / 2 + g + j) * ep.ldc]
+                                                          : make_float2(0.f, 0.f);
+#pragma unroll
+          for (int j = 0; j < kCGroup / 2; ++j) {
+            const int col = col0 / 2 + g + j;
+            if (col < ep.n) {
+              const float ar = sum[2 * (g + j)], ai = sum[2 * (g + j) + 1];
+              float2 v = make_float2(ep.alpha_re * ar - ep.alpha_im * ai, ep.alpha_re * ai + ep.alpha_im * ar);
+              if (!beta0) {
+                const float2 cv = cvs[j];
+                if (beta1) { v.x += cv.x; v.y += cv.y; }
+                else {
+                  v.x += ep.beta_re * cv.x - ep.beta_im * cv.y;
+                  v.y += ep.beta_re * cv.y + ep.beta_im * cv.x;
+                }
+              }
+              crow[(size_t)col * ep.ldc] = v;
+            }
+          }
+        }
+      }
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::cluster_sync();  // no CTA leaves while its partner may still signal or read it
+  tc::tc_fence_after();
+  if (warp == 1) tc::tmem_dealloc_pair(tmem, 2 * kPairTile);
+}
+
 // Split-K combine: C = alpha * sum_p ws[p] + beta * C in a fixed part order.
 __global__ void k_split_reduce(const float* __restrict__ ws, int splits, int ws_cols, EpiParams ep) {
   const size_t total = (size_t)ep.m * ep.n;
@@ -781,6 +1076,91 @@ coral_status_t run_split_gemm(Handle* h, const __nv_bfloat16* ap, size_t a_piece
   return launch_status(h);
 }
 
+template <int NP>
+size_t pair_smem_bytes() {
+  return (size_t)PairRing<NP>::kStages * PairRing<NP>::kStageBytes + 1024;
+}
+
+// Clusters of two that can be resident at once (per device, queried once).
+template <int NP>
+int pair_cluster_capacity(Handle* h, size_t smem) {
+  static int cap[64] = {0};
+  const int d = h->device < 64 ? h->device : 0;
+  if (cap[d] > 0) return cap[d];
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)h->sm_count, 1, 1);
+  cfg.blockDim = dim3(kSplitThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k_gemm_split_pair<NP>, &cfg) != cudaSuccess || n < 1) {
+    cudaGetLastError();
+    n = h->sm_count / 2;
+  }
+  cap[d] = n;
+  return n;
+}
+
+// The pair kernel over prepared pieces (same operands and workspace as
+// run_split_gemm); `group` M-tiles per raster group.
+template <int NP>
+coral_status_t run_split_gemm_pair(Handle* h, const __nv_bfloat16* ap, size_t a_piece, int mr,
+                                   const __nv_bfloat16* bp, size_t b_piece, int nr, int kd, size_t kp,
+                                   int splits, float* ws, const EpiParams& ep) {
+  SplitMaps maps;
+  std::memset(&maps, 0, sizeof(maps));
+  for (int p = 0; p < SplitPlan<NP>::kPieces; ++p) {
+    if (!encode_kmajor_map(&maps.a[p], ap + p * a_piece, 2, (uint64_t)kd, (uint64_t)mr, kp * 2, kBK,
+                           kPairHalf, kSwizzle) ||
+        !encode_kmajor_map(&maps.b[p], bp + p * b_piece, 2, (uint64_t)kd, (uint64_t)nr, kp * 2, kBK,
+                           kPairHalf, kSwizzle))
+      return CORAL_ERR_NOT_SUPPORTED;
+  }
+  const size_t smem = pair_smem_bytes<NP>();
+  static uint64_t attr_devices = 0;
+  const uint64_t bit = h->device < 64 ? (1ull << h->device) : 0;
+  if (!(attr_devices & bit) || !bit) {
+    CORAL_CUDA(h, cudaFuncSetAttribute(k_gemm_split_pair<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    attr_devices |= bit;
+  }
+  const int m_tiles = (mr + kPairTile - 1) / kPairTile, n_tiles = (nr + kPairTile - 1) / kPairTile;
+  const int items = m_tiles * n_tiles * splits;
+  const int cap = pair_cluster_capacity<NP>(h, smem);
+  const int clusters = items < cap ? items : cap;
+  const int group = h->pair_group > 0 ? h->pair_group : 8;
+  const uint64_t limit_ns = h->wait_limit * 32ull;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(2 * clusters), 1, 1);
+  cfg.blockDim = dim3(kSplitThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  timed_begin(h);
+  cudaError_t e = cudaLaunchKernelEx(&cfg, k_gemm_split_pair<NP>, maps, kd, m_tiles, n_tiles, group,
+                                     h->split_chunk_kb * kSlabsPer64, splits, ws, nr, ep,
+                                     &h->words->status, limit_ns);
+  count_launch();
+  coral_status_t s = cuda_status(h, e != cudaSuccess ? e : cudaGetLastError());
+  timed_end(h);
+  if (s != CORAL_OK || splits == 1) return s;
+  unsigned g = stream_grid((size_t)ep.m * ep.n, 256 * 4, h->sm_count, 8);
+  k_split_reduce<<<g, 256, 0, h->stream>>>(ws, splits, nr, ep);
+  return launch_status(h);
+}
+
 }  // namespace
 
 // Tile width and split-K factor for a split-BF16 GEMM of op(A) (mr x kd)
@@ -791,14 +1171,24 @@ SplitConfig choose_split_config(Handle* h, const SplitShape& sh) {
   const int products = sh.products, mr = sh.mr, nr = sh.nr, kd = sh.kd;
   SplitConfig c{products == 3 ? 256 : 128, 1};
   const int nk = (kd + 63) / 64;   // 64-deep K units (independent of the kernel's slab depth)
-  if (h->cfg_bn > 0 || h->cfg_splits > 0) {
+  if (h->cfg_bn > 0 || h->cfg_splits > 0 || h->cfg_bm > 0) {
     if (h->cfg_bn > 0) c.bn = h->cfg_bn;
     if (h->cfg_splits > 0) c.splits = h->cfg_splits;
+    if (h->cfg_bm == 256) {
+      c.pair = 1;
+      c.bn = 256;
+    }
   } else if (h->selector && select_split_config(h, sh, &c)) {
     // selector decided
   } else {
     const int tiles = ((mr + kBM - 1) / kBM) * ((nr + c.bn - 1) / c.bn);
-    if (tiles * 2 <= h->sm_count && nk >= 16) {
+    const int pair_tiles = ((mr + kPairTile - 1) / kPairTile) * ((nr + kPairTile - 1) / kPairTile);
+    if (pair_tiles >= h->sm_count) {
+      // At least two waves of 256 x 256 tiles over the resident CTA pairs:
+      // the pair tiles read half as much of B per flop from shared memory.
+      c.pair = 1;
+      c.bn = 256;
+    } else if (tiles * 2 <= h->sm_count && nk >= 16) {
       int sp = h->sm_count / tiles;
       sp = sp > 16 ? 16 : sp;
       sp = sp > nk ? nk : sp;
@@ -807,7 +1197,7 @@ SplitConfig choose_split_config(Handle* h, const SplitShape& sh) {
       c.splits = p2;
     }
   }
-  if (products == 6) c.bn = 128;
+  if (products == 6 && !c.pair) c.bn = 128;
   if (c.bn != 128 && c.bn != 256) c.bn = 256;
   if (c.splits > nk) c.splits = nk > 0 ? nk : 1;
   if (c.splits < 1) c.splits = 1;
@@ -820,6 +1210,8 @@ template <int NP>
 coral_status_t dispatch_split_gemm(Handle* h, const __nv_bfloat16* ap, size_t a_piece, int mr,
                                    const __nv_bfloat16* bp, size_t b_piece, int nr, int kd,
                                    size_t kp, const SplitConfig& c, float* ws, const EpiParams& ep) {
+  if (c.pair)
+    return run_split_gemm_pair<NP>(h, ap, a_piece, mr, bp, b_piece, nr, kd, kp, c.splits, ws, ep);
   if (NP == 3 && c.bn == 256)
     return run_split_gemm<NP, 256>(h, ap, a_piece, mr, bp, b_piece, nr, kd, kp, c.splits, ws, ep);
   return run_split_gemm<NP, 128>(h, ap, a_piece, mr, bp, b_piece, nr, kd, kp, c.splits, ws, ep);

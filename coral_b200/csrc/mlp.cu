@@ -273,20 +273,11 @@ bool select_split_config(Handle* h, const SplitShape& sh, SplitConfig* out) {
     *out = it->second;
     return true;
   }
-  static const int kBn[2] = {256, 128};
-  static const int kSp[5] = {1, 2, 4, 8, 16};
-  float feats[10 * kSelectorFeatures];
-  (void)products;
-  SplitConfig cand[10];
-  int nc = 0;
-  for (int b = 0; b < 2; ++b) {
-    if (products == 6 && kBn[b] == 256) continue;
-    for (int s = 0; s < 5; ++s) {
-      cand[nc] = SplitConfig{kBn[b], kSp[s]};
-      selector_features(sh, kBn[b], kSp[s], feats + nc * kSelectorFeatures);
-      ++nc;
-    }
-  }
+  float feats[15 * kSelectorFeatures];
+  SplitConfig cand[15];
+  const int nc = split_candidates(products, cand);
+  for (int i = 0; i < nc; ++i)
+    selector_features(sh, cand[i].pair ? 256 : 128, cand[i].bn, cand[i].splits, feats + i * kSelectorFeatures);
   if (cudaMemcpyAsync(sel->feat_dev, feats, sizeof(float) * nc * kSelectorFeatures,
                       cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
     return false;
@@ -295,7 +286,7 @@ bool select_split_config(Handle* h, const SplitShape& sh, SplitConfig* out) {
   saved->stream = h->stream;
   coral_status_t s = forward(sel->mlp, sel->feat_dev, nc, sel->pred_dev);
   saved->stream = saved_stream;
-  float pred[10];
+  float pred[15];
   if (s != CORAL_OK ||
       cudaMemcpyAsync(pred, sel->pred_dev, sizeof(float) * nc, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
       cudaStreamSynchronize(h->stream) != cudaSuccess)
@@ -308,11 +299,27 @@ bool select_split_config(Handle* h, const SplitShape& sh, SplitConfig* out) {
   return true;
 }
 
+int split_candidates(int products, SplitConfig* out) {
+  static const int kSp[5] = {1, 2, 4, 8, 16};
+  int nc = 0;
+  for (int t = 0; t < 3; ++t) {
+    if (products == 6 && t == 1) continue;  // 3 pieces: no 128 x 256 single-CTA tile
+    for (int s = 0; s < 5; ++s) {
+      SplitConfig c{t == 2 ? 128 : 256, kSp[s]};
+      c.pair = t == 0 ? 1 : 0;
+      out[nc++] = c;
+    }
+  }
+  return nc;
+}
+
 // Feature vector of (shape, configuration) for the selector network:
 // log2 m, n, k; transpose flags; data type (products, complex); log2 batch;
-// tile width and log2 split-K; and the occupancy the pair implies (log2 of
-// output tiles, resident waves of work items, log2 K slabs per split).
-void selector_features(const SplitShape& sh, int bn, int splits, float* f) {
+// tile area (bm x bn over 128 x 256: 0.5, 1, or 2 for the CTA-pair tile) and
+// log2 split-K; and the occupancy the configuration implies (log2 of output
+// tiles, resident waves of work items -- 148 single CTAs or 74 pairs --, log2
+// K slabs per split).
+void selector_features(const SplitShape& sh, int bm, int bn, int splits, float* f) {
   const float m = (float)(sh.mr > 0 ? sh.mr : 1), n = (float)(sh.nr > 0 ? sh.nr : 1);
   const float k = (float)(sh.kd > 0 ? sh.kd : 1);
   f[0] = std::log2(m) / 16.f;
@@ -323,12 +330,13 @@ void selector_features(const SplitShape& sh, int bn, int splits, float* f) {
   f[5] = (float)sh.products / 6.f;
   f[6] = sh.complex_ ? 1.f : 0.f;
   f[7] = std::log2((float)(sh.batch > 0 ? sh.batch : 1)) / 12.f;
-  f[8] = (float)bn / 256.f;
+  f[8] = (float)(bm * bn) / (128.f * 256.f);
   f[9] = std::log2((float)splits) / 4.f;
-  const float tiles = std::ceil(m / 128.f) * std::ceil(n / (float)bn);
+  const float tiles = std::ceil(m / (float)bm) * std::ceil(n / (float)bn);
   const float items = tiles * (float)splits;
+  const float resident = bm == 256 ? 74.f : 148.f;
   f[10] = std::log2(tiles) / 16.f;
-  f[11] = std::min(items / 148.f, 8.f) / 8.f;
+  f[11] = std::min(items / resident, 8.f) / 8.f;
   f[12] = std::log2(std::max(1.f, std::ceil(k / 64.f) / (float)splits)) / 12.f;
 }
 
@@ -600,6 +608,40 @@ coral_status_t coral_set_gemm_config(coral_handle_t hh, int tile_n, int split_k)
   if (split_k < 0 || split_k > 64) return bad_arg(H, 2);
   H->cfg_bn = tile_n;
   H->cfg_splits = split_k;
+  H->cfg_bm = 0;
+  return CORAL_OK;
+}
+
+coral_status_t coral_set_gemm_tile(coral_handle_t hh, int tile_m, int tile_n, int split_k) {
+  CORAL_HANDLE(hh);
+  if (tile_m != 0 && tile_m != 128 && tile_m != 256) return bad_arg(H, 1);
+  if (tile_n != 0 && tile_n != 128 && tile_n != 256) return bad_arg(H, 2);
+  if (tile_m == 256 && tile_n != 256) return bad_arg(H, 2);
+  if (split_k < 0 || split_k > 64) return bad_arg(H, 3);
+  H->cfg_bm = tile_m;
+  H->cfg_bn = tile_n;
+  H->cfg_splits = split_k;
+  return CORAL_OK;
+}
+
+coral_status_t coral_get_gemm_tile(coral_handle_t hh, int products, int op_a, int op_b, size_t m,
+                                   size_t n, size_t k, int* tile_m, int* tile_n, int* split_k) {
+  CORAL_HANDLE(hh);
+  if (products != 3 && products != 6) return bad_arg(H, 1);
+  if (!tile_m) return bad_arg(H, 7);
+  if (!tile_n) return bad_arg(H, 8);
+  if (!split_k) return bad_arg(H, 9);
+  SplitConfig c = choose_split_config(H, SplitShape{(int)m, (int)n, (int)k, products, op_a, op_b, 0, 1});
+  *tile_m = c.pair ? 256 : 128;
+  *tile_n = c.bn;
+  *split_k = c.splits;
+  return CORAL_OK;
+}
+
+coral_status_t coral_set_pair_raster(coral_handle_t hh, int group) {
+  CORAL_HANDLE(hh);
+  if (group < 0 || group > 64) return bad_arg(H, 1);
+  H->pair_group = group;
   return CORAL_OK;
 }
 
@@ -618,7 +660,16 @@ coral_status_t coral_get_gemm_config(coral_handle_t hh, int products, int op_a, 
 coral_status_t coral_selector_features(int products, int op_a, int op_b, size_t m, size_t n, size_t k,
                                        int tile_n, int split_k, float* out) {
   if (!out) return CORAL_ERR_INVALID_ARG;
-  selector_features(SplitShape{(int)m, (int)n, (int)k, products, op_a, op_b, 0, 1}, tile_n, split_k, out);
+  selector_features(SplitShape{(int)m, (int)n, (int)k, products, op_a, op_b, 0, 1}, 128, tile_n, split_k, out);
+  return CORAL_OK;
+}
+
+coral_status_t coral_selector_features_tile(int products, int op_a, int op_b, size_t m, size_t n, size_t k,
+                                            int tile_m, int tile_n, int split_k, float* out) {
+  if (!out) return CORAL_ERR_INVALID_ARG;
+  if (tile_m != 128 && tile_m != 256) return CORAL_ERR_INVALID_ARG;
+  selector_features(SplitShape{(int)m, (int)n, (int)k, products, op_a, op_b, 0, 1}, tile_m, tile_n, split_k,
+                    out);
   return CORAL_OK;
 }
 

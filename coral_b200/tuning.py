@@ -1,12 +1,16 @@
 """Autotuning database and the learned configuration selector.
 
-The split-BF16 SGEMM has ten configurations per shape: N tile width
-{256, 128} x split-K {1, 2, 4, 8, 16}.  This module
+The split-BF16 SGEMM has fifteen configurations per shape: tile
+{256 x 256 on a CTA pair (tcgen05 cta_group::2, cluster of 2), 128 x 256,
+128 x 128} x split-K {1, 2, 4, 8, 16}; the 3-piece (x6) mode has no 128 x 256
+tile.  This module
 
 * draws seeded shapes (dims log-uniform in [32, 16384], plus the tall-skinny
-  65536 x 64 x 4096 and split-K-heavy 256 x 256 x 65536 shapes),
+  65536 x 64 x 4096 and split-K-heavy 256 x 256 x 65536 shapes; a quarter of
+  them in the 3-piece mode, so the data-type feature varies),
 * times every configuration of every shape on the GPU with the library's
-  exhaustive autotuner (``coral_autotune_sgemm``) into a timing database,
+  exhaustive autotuner (``coral_autotune_sgemm_tiles``) into a timing database
+  (configurations a mode does not have are stored as +inf),
 * trains the selector network -- 13 features -> 128 -> 128 -> 1 (ReLU),
   predicting log(ms) -- with the library's own CUDA forward/backward/Adam
   kernels (``coral_mlp_*``),
@@ -19,6 +23,7 @@ CLI (runs on a B200):
     python -m coral_b200.tuning collect --count 2000 --seed 2 --out heldout.npz
     python -m coral_b200.tuning train --db train.npz --out selector.npz
     python -m coral_b200.tuning evaluate --db heldout.npz --weights selector.npz
+    python -m coral_b200.tuning evaluate-live --db heldout.npz --weights selector.npz --count 300
 
 The tensor-core grouped GEMM's tile-width policy has its own network and
 pipeline (uniform batches of varied data type and instance count; live
@@ -40,56 +45,78 @@ import numpy as np
 from . import _lib
 from .blas import handle
 
-CANDIDATES = [(bn, sp) for bn in (256, 128) for sp in (1, 2, 4, 8, 16)]
+TILES = ((256, 256), (128, 256), (128, 128))
+CANDIDATES = [(tm, tn, sp) for (tm, tn) in TILES for sp in (1, 2, 4, 8, 16)]
+X6_FRACTION = 0.25
 N_FEATURES = 13
 HIDDEN = 128
 DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 
 
 # ------------------------------------------------------------------- shapes --
-def generate_shapes(count: int, seed: int, lo: int = 32, hi: int = 16384) -> np.ndarray:
-    """[count, 5] int64: m, n, k, op_a, op_b.  The first two rows are the
-    tall-skinny and split-K-heavy shapes when count >= 2."""
+def generate_shapes(count: int, seed: int, lo: int = 32, hi: int = 16384,
+                    x6_fraction: float = X6_FRACTION) -> np.ndarray:
+    """[count, 6] int64: m, n, k, op_a, op_b, products (3 or 6).  The first two
+    rows are the tall-skinny and split-K-heavy shapes when count >= 2."""
     rng = np.random.default_rng(seed)
     dims = np.exp(rng.uniform(np.log(lo), np.log(hi), (count, 3))).astype(np.int64)
     ops = rng.integers(0, 2, (count, 2))
-    shapes = np.concatenate([dims, ops], axis=1)
+    products = np.where(rng.uniform(size=(count, 1)) < x6_fraction, 6, 3)
+    shapes = np.concatenate([dims, ops, products], axis=1)
     if count >= 2:
-        shapes[0] = (65536, 64, 4096, 0, 0)
-        shapes[1] = (256, 256, 65536, 0, 0)
+        shapes[0] = (65536, 64, 4096, 0, 0, 3)
+        shapes[1] = (256, 256, 65536, 0, 0, 3)
     return shapes
 
 
-def features(shape, bn: int, sp: int, products: int = 3) -> np.ndarray:
+def shape_products(shape) -> int:
+    return int(shape[5]) if len(shape) > 5 else 3
+
+
+def valid(shape, cand) -> bool:
+    """Whether the shape's mode has this configuration (x6: no 128 x 256 tile)."""
+    return not (shape_products(shape) == 6 and cand[:2] == (128, 256))
+
+
+def features(shape, tm: int, tn: int, sp: int) -> np.ndarray:
     """The selector's 13 features for (shape, configuration), computed by the library."""
-    m, n, k, op_a, op_b = (int(v) for v in shape)
+    m, n, k, op_a, op_b = (int(v) for v in shape[:5])
     out = (C.c_float * N_FEATURES)()
-    st = _lib.load().coral_selector_features(products, op_a, op_b, m, n, k, bn, sp, out)
+    st = _lib.load().coral_selector_features_tile(shape_products(shape), op_a, op_b, m, n, k, tm, tn, sp, out)
     if st != 0:
-        raise RuntimeError(f"coral_selector_features: {st}")
+        raise RuntimeError(f"coral_selector_features_tile: {st}")
     return np.frombuffer(out, dtype=np.float32).copy()
 
 
 def feature_matrix(shapes: np.ndarray) -> np.ndarray:
-    """[len(shapes) * 10, 13] in shape-major, candidate-minor order."""
-    return np.stack([features(s, bn, sp) for s in shapes for (bn, sp) in CANDIDATES])
+    """[len(shapes) * 15, 13] in shape-major, candidate-minor order."""
+    return np.stack([features(s, *c) for s in shapes for c in CANDIDATES])
+
+
+def valid_mask(shapes: np.ndarray) -> np.ndarray:
+    """[len(shapes), 15] bool."""
+    return np.array([[valid(s, c) for c in CANDIDATES] for s in shapes])
 
 
 def default_choice(shape, sm_count: int = 148) -> int:
     """Index in CANDIDATES of the library's default rule (no selector)."""
     m, n, k = (int(v) for v in shape[:3])
+    if -(-m // 256) * -(-n // 256) >= sm_count:
+        return CANDIDATES.index((256, 256, 1))
+    tn = 256 if shape_products(shape) == 3 else 128
     tiles = -(-m // 128) * -(-n // 256)
     sp = 1
     if tiles * 2 <= sm_count and -(-k // 64) >= 16:
         sp = min(16, max(1, sm_count // tiles))
     sp = min(sp, max(1, -(-k // 64)))
     best = max([s for s in (1, 2, 4, 8, 16) if s <= sp])
-    return CANDIDATES.index((256, best))
+    return CANDIDATES.index((128, tn, best))
 
 
 # ------------------------------------------------------------ autotune DB --
 def collect(shapes: np.ndarray, reps_small: int = 3, log_every: int = 500) -> np.ndarray:
-    """Exhaustively times every candidate of every shape: [len(shapes), 10] ms."""
+    """Exhaustively times every candidate of every shape: [len(shapes), 15] ms
+    (+inf where the shape's mode has no such configuration)."""
     import torch
     lib = _lib.load()
     h = handle()
@@ -100,24 +127,34 @@ def collect(shapes: np.ndarray, reps_small: int = 3, log_every: int = 500) -> np
     A = torch.empty(need_a, dtype=torch.float32, device="cuda").uniform_(-1, 1)
     B = torch.empty(need_b, dtype=torch.float32, device="cuda").uniform_(-1, 1)
     Cm = torch.empty(need_c, dtype=torch.float32, device="cuda")
-    times = np.zeros((len(shapes), len(CANDIDATES)), np.float32)
-    ms = (C.c_float * len(CANDIDATES))()
-    best = C.c_int()
+    times = np.full((len(shapes), len(CANDIDATES)), np.inf, np.float32)
     t0 = time.time()
-    for i, (m, n, k, op_a, op_b) in enumerate(shapes):
-        m, n, k, op_a, op_b = int(m), int(n), int(k), int(op_a), int(op_b)
-        lda = m if op_a == 0 else k
-        ldb = k if op_b == 0 else n
-        reps = reps_small if 2.0 * m * n * k < 2e10 else 1
-        st = lib.coral_autotune_sgemm(h.h, 3, op_a, op_b, m, n, k, C.c_void_p(A.data_ptr()), lda,
-                                      C.c_void_p(B.data_ptr()), ldb, C.c_void_p(Cm.data_ptr()), m,
-                                      reps, ms, C.byref(best))
-        if st != 0:
-            raise RuntimeError(f"coral_autotune_sgemm failed on {m}x{n}x{k}: {st}")
-        times[i] = np.frombuffer(ms, dtype=np.float32)
+    for i, s in enumerate(shapes):
+        times[i] = time_all(lib, h, s, A, B, Cm, reps_small)
         if log_every and (i + 1) % log_every == 0:
             print(f"  {i + 1}/{len(shapes)} shapes, {time.time() - t0:.0f} s", flush=True)
     return times
+
+
+def time_all(lib, h, shape, A, B, Cm, reps_small: int = 3) -> np.ndarray:
+    """[15] ms of every configuration of one shape (coral_autotune_sgemm_tiles),
+    +inf where the mode has none."""
+    m, n, k, op_a, op_b = (int(v) for v in shape[:5])
+    prod = shape_products(shape)
+    lda = m if op_a == 0 else k
+    ldb = k if op_b == 0 else n
+    reps = reps_small if 2.0 * m * n * k * prod / 3 < 2e10 else 1
+    ms = (C.c_float * len(CANDIDATES))()
+    count, best = C.c_int(), C.c_int()
+    st = lib.coral_autotune_sgemm_tiles(h.h, prod, op_a, op_b, m, n, k, C.c_void_p(A.data_ptr()), lda,
+                                        C.c_void_p(B.data_ptr()), ldb, C.c_void_p(Cm.data_ptr()), m, reps, ms,
+                                        len(CANDIDATES), C.byref(count), C.byref(best))
+    if st != 0:
+        raise RuntimeError(f"coral_autotune_sgemm_tiles failed on {m}x{n}x{k}: {st}")
+    got = np.frombuffer(ms, dtype=np.float32)[:count.value]
+    out = np.full(len(CANDIDATES), np.inf, np.float32)
+    out[[j for j, c in enumerate(CANDIDATES) if valid(shape, c)]] = got
+    return out
 
 
 # --------------------------------------------------------------------- MLP --
@@ -215,8 +252,9 @@ def train(db_shapes: np.ndarray, db_times: np.ndarray, epochs: int = 300, batch:
           lr: float = 2e-3, seed: int = 0, log_every: int = 50) -> tuple[Mlp, list]:
     """Fits log(ms) of every (shape, configuration) pair on the GPU."""
     import torch
-    X = torch.from_numpy(feature_matrix(db_shapes)).cuda()
-    y = torch.from_numpy(np.log(np.maximum(db_times.reshape(-1, 1), 1e-4)).astype(np.float32)).cuda()
+    ok = np.isfinite(db_times.reshape(-1))
+    X = torch.from_numpy(feature_matrix(db_shapes)[ok]).cuda()
+    y = torch.from_numpy(np.log(np.maximum(db_times.reshape(-1, 1)[ok], 1e-4)).astype(np.float32)).cuda()
     net = Mlp(seed=seed)
     g = torch.Generator(device="cuda")
     g.manual_seed(seed)
@@ -239,16 +277,80 @@ def train(db_shapes: np.ndarray, db_times: np.ndarray, epochs: int = 300, batch:
     return net, history
 
 
+def choose(pred: np.ndarray, shapes: np.ndarray) -> np.ndarray:
+    """Argmin of predicted log ms over each shape's valid configurations."""
+    pred = np.asarray(pred, np.float64).reshape(len(shapes), len(CANDIDATES))
+    return np.where(valid_mask(shapes), pred, np.inf).argmin(axis=1)
+
+
 def predict_choice(net: Mlp, shapes: np.ndarray) -> np.ndarray:
     import torch
     X = torch.from_numpy(feature_matrix(shapes)).cuda()
-    pred = net.forward(X).cpu().numpy().reshape(len(shapes), len(CANDIDATES))
-    return pred.argmin(axis=1)
+    return choose(net.forward(X).cpu().numpy(), shapes)
 
 
 def regret(times: np.ndarray, choice: np.ndarray) -> np.ndarray:
     best = times.min(axis=1)
     return times[np.arange(len(times)), choice] / best - 1.0
+
+
+def evaluate_live(net: Mlp, shapes: np.ndarray, reps_small: int = 3) -> dict:
+    """Regret measured on the GPU, not read from a table: for each shape, every
+    configuration is timed (exhaustive autotune), then coral_sgemm is timed
+    with the configuration the library itself picks -- once with the network
+    attached to the handle as its selector, once with the default rule."""
+    import torch
+    lib = _lib.load()
+    h = handle()
+    h.bind_current_stream()
+    need_a = int(max(s[0] * s[2] for s in shapes))
+    need_b = int(max(s[2] * s[1] for s in shapes))
+    need_c = int(max(s[0] * s[1] for s in shapes))
+    A = torch.empty(need_a, dtype=torch.float32, device="cuda").uniform_(-1, 1)
+    B = torch.empty(need_b, dtype=torch.float32, device="cuda").uniform_(-1, 1)
+    Cm = torch.empty(need_c, dtype=torch.float32, device="cuda")
+
+    def time_policy(s, reps, trials=3):
+        """Median over `trials` of the per-call time of `reps` back-to-back calls."""
+        m, n, k, op_a, op_b = (int(v) for v in s[:5])
+        lda, ldb = (m if op_a == 0 else k), (k if op_b == 0 else n)
+        h.set_gemm_mode(3 if shape_products(s) == 6 else 1)  # SPLIT_BF16X6 / SPLIT_BF16X3
+        h.set_gemm_tile(0, 0, 0)
+        args = (h.h, op_a, op_b, m, n, k, C.c_float(1.0), C.c_void_p(A.data_ptr()), lda,
+                C.c_void_p(B.data_ptr()), ldb, C.c_float(0.0), C.c_void_p(Cm.data_ptr()), m)
+        h.check(lib.coral_sgemm(*args), "coral_sgemm")
+        out = []
+        for _ in range(trials):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                lib.coral_sgemm(*args)
+            e1.record()
+            torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1) / reps)
+        return float(np.median(out))
+
+    rows = []
+    for s in shapes:
+        m, n, k = (int(v) for v in s[:3])
+        reps = reps_small if 2.0 * m * n * k * shape_products(s) / 3 < 2e10 else 1
+        t_all = time_all(lib, h, s, A, B, Cm, reps_small)
+        net.attach(h)
+        t_sel = time_policy(s, reps)
+        tm, tn, sk = h.gemm_tile(shape_products(s), int(s[3]), int(s[4]), m, n, k)
+        lib.coral_set_selector(h.h, None)
+        t_def = time_policy(s, reps)
+        rows.append({"shape": [int(v) for v in s], "best_ms": float(t_all.min()),
+                     "best": list(CANDIDATES[int(t_all.argmin())]), "selector_ms": t_sel,
+                     "selector_choice": [tm, tn, sk], "default_ms": t_def,
+                     "selector_table_ms": float(t_all[CANDIDATES.index((tm, tn, sk))])
+                     if (tm, tn, sk) in CANDIDATES else None})
+    h.set_gemm_mode(0)
+    r_sel = np.array([x["selector_ms"] / x["best_ms"] - 1 for x in rows])
+    r_def = np.array([x["default_ms"] / x["best_ms"] - 1 for x in rows])
+    return {"shapes": len(rows), "selector": summarize(r_sel), "default_rule": summarize(r_def),
+            "pair_chosen": float(np.mean([x["selector_choice"][0] == 256 for x in rows])),
+            "pair_best": float(np.mean([x["best"][0] == 256 for x in rows])), "rows": rows}
 
 
 def summarize(r: np.ndarray) -> dict:
@@ -507,6 +609,11 @@ def main(argv=None):
     e = sub.add_parser("evaluate")
     e.add_argument("--db", required=True)
     e.add_argument("--weights", required=True)
+    el = sub.add_parser("evaluate-live")
+    el.add_argument("--db", required=True)
+    el.add_argument("--weights", required=True)
+    el.add_argument("--count", type=int, default=300)
+    el.add_argument("--out", default="")
     gc = sub.add_parser("grouped-collect")
     gc.add_argument("--count", type=int, default=6000)
     gc.add_argument("--seed", type=int, default=11)
@@ -542,11 +649,20 @@ def main(argv=None):
         net = Mlp.load(args.weights)
         choice = predict_choice(net, d["shapes"])
         dflt = np.array([default_choice(s) for s in d["shapes"]])
-        fixed = np.full(len(d["shapes"]), CANDIDATES.index((256, 1)))
+        fixed = np.array([CANDIDATES.index((128, 256 if shape_products(s) == 3 else 128, 1))
+                          for s in d["shapes"]])
         print(json.dumps({"shapes": int(len(d["shapes"])),
                           "selector": summarize(regret(d["times"], choice)),
                           "default_rule": summarize(regret(d["times"], dflt)),
-                          "fixed_256x1": summarize(regret(d["times"], fixed))}))
+                          "fixed_single_cta_no_split": summarize(regret(d["times"], fixed))}))
+    elif args.cmd == "evaluate-live":
+        d = np.load(args.db)
+        net = Mlp.load(args.weights)
+        res = evaluate_live(net, d["shapes"][:args.count])
+        if args.out:
+            with open(args.out, "w") as f:
+                json.dump(res, f)
+        print(json.dumps({k: v for k, v in res.items() if k != "rows"}))
     elif args.cmd == "grouped-collect":
         samples = grouped_samples(args.count, args.seed)
         t0 = time.time()

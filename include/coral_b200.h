@@ -467,6 +467,16 @@ coral_status_t coral_strsv_batched(coral_handle_t h, size_t count,
  * (128 or 256) and split-K factor (1..64); 0 leaves the choice to the
  * selector (when set) or to the default rule. */
 coral_status_t coral_set_gemm_config(coral_handle_t h, int tile_n, int split_k);
+/* Same, with the tile height: tile_m 128 runs one CTA per 128 x tile_n tile;
+ * tile_m 256 (with tile_n 256) runs a cluster of two CTAs per 256 x 256 tile,
+ * whose tensor-core products read each CTA's half of A and of B
+ * (tcgen05 cta_group::2).  All zero leaves the choice to the policy. */
+coral_status_t coral_set_gemm_tile(coral_handle_t h, int tile_m, int tile_n, int split_k);
+/* The tile a split-BF16 SGEMM of this shape would use now. */
+coral_status_t coral_get_gemm_tile(coral_handle_t h, int products, int op_a, int op_b, size_t m,
+                                   size_t n, size_t k, int* tile_m, int* tile_n, int* split_k);
+/* M-tiles per raster group of the CTA-pair tiles (1..64; 0 restores 8). */
+coral_status_t coral_set_pair_raster(coral_handle_t h, int group);
 /* The configuration a split-BF16 SGEMM of this shape would use now. */
 coral_status_t coral_get_gemm_config(coral_handle_t h, int products, int op_a, int op_b, size_t m,
                                      size_t n, size_t k, int* tile_n, int* split_k);
@@ -483,6 +493,20 @@ coral_status_t coral_autotune_sgemm(coral_handle_t h, int products, int op_a, in
                                     size_t n, size_t k, const float* a, size_t lda, const float* b,
                                     size_t ldb, float* c, size_t ldc, int reps, float* ms_out,
                                     int* best);
+
+/* Exhaustive autotuning over tile shapes too: the configurations
+ * (tile_m x tile_n) in {256 x 256 (a CTA pair, cta_group::2), 128 x 256,
+ * 128 x 128} x split_k in {1, 2, 4, 8, 16}, in that order (15 values;
+ * products 6: 10, without 128 x 256).  `capacity` is the length of ms_out;
+ * the number written goes to *count and the fastest index to *best.  C is
+ * overwritten; the handle's configuration is restored. */
+coral_status_t coral_autotune_sgemm_tiles(coral_handle_t h, int products, int op_a, int op_b, size_t m,
+                                          size_t n, size_t k, const float* a, size_t lda, const float* b,
+                                          size_t ldb, float* c, size_t ldc, int reps, float* ms_out,
+                                          int capacity, int* count, int* best);
+/* Selector features of (shape, tile_m x tile_n, split_k); 13 floats. */
+coral_status_t coral_selector_features_tile(int products, int op_a, int op_b, size_t m, size_t n,
+                                            size_t k, int tile_m, int tile_n, int split_k, float* out);
 
 /* A small MLP (in -> hidden -> hidden -> out, ReLU) trained and evaluated by
  * the library's own kernels; used as the configuration selector (in = 13,

@@ -25,20 +25,20 @@ pytestmark = pytest.mark.gpu
 def restore():
     yield
     h = cb.handle()
-    h.lib.coral_set_gemm_config(h.h, 0, 0)
+    h.lib.coral_set_gemm_tile(h.h, 0, 0, 0)
     h.lib.coral_set_selector(h.h, None)
     cb.set_gemm_mode(cb.GemmMode.NATIVE)
 
 
-@pytest.mark.parametrize("bn,sp", tuning.CANDIDATES)
-def test_split_configs_correct(cuda, bn, sp):
+@pytest.mark.parametrize("tm,tn,sp", tuning.CANDIDATES)
+def test_split_configs_correct(cuda, tm, tn, sp):
     h = cb.handle()
-    assert h.lib.coral_set_gemm_config(h.h, bn, sp) == 0
+    assert h.lib.coral_set_gemm_tile(h.h, tm, tn, sp) == 0
     cb.set_gemm_mode(cb.GemmMode.SPLIT_BF16X3)
     gemm_case(cb.sgemm, np.float32, 0, 0, 200, 300, 2000, 1.5, 0.5, 4e-5, sample=2048)
     gemm_case(cb.sgemm, np.float32, 1, 1, 129, 65, 777, 1.0, 0.0, 4e-5)
     gemm_case(cb.cgemm, np.complex64, 2, 1, 70, 90, 333, 1.5 - 0.5j, 0.25 + 1j, 8e-5)
-    if bn == 128:
+    if (tm, tn) != (128, 256):
         cb.set_gemm_mode(cb.GemmMode.SPLIT_BF16X6)
         gemm_case(cb.sgemm, np.float32, 0, 1, 150, 140, 900, -0.5, 1.0, 1e-5)
 
@@ -67,6 +67,32 @@ def test_autotune_and_config_restore(cuda):
     bn, sp = C.c_int(), C.c_int()
     assert h.lib.coral_get_gemm_config(h.h, 3, 0, 0, 256, 256, 65536, C.byref(bn), C.byref(sp)) == 0
     assert (bn.value, sp.value) == (256, 16)   # default rule: split K to fill the GPU
+    # default rule: CTA-pair tiles once they fill two waves of resident pairs
+    assert h.gemm_tile(3, 0, 0, 8192, 8192, 8192) == (256, 256, 1)
+    assert h.gemm_tile(3, 0, 0, 2048, 2048, 2048)[0] == 128
+
+
+def test_autotune_tiles_covers_pair(cuda):
+    h = cb.handle()
+    m, n, k = 600, 700, 900
+    A = torch.empty(m * k, device="cuda").uniform_(-1, 1)
+    B = torch.empty(k * n, device="cuda").uniform_(-1, 1)
+    Cm = torch.empty(m * n, device="cuda")
+    h.bind_current_stream()
+    for products, expect in ((3, 15), (6, 10)):
+        ms = (C.c_float * 15)()
+        count, best = C.c_int(), C.c_int()
+        st = h.lib.coral_autotune_sgemm_tiles(h.h, products, 0, 0, m, n, k, C.c_void_p(A.data_ptr()), m,
+                                              C.c_void_p(B.data_ptr()), k, C.c_void_p(Cm.data_ptr()), m, 1,
+                                              ms, 15, C.byref(count), C.byref(best))
+        assert st == 0 and count.value == expect
+        t = np.frombuffer(ms, np.float32)[:expect]
+        assert (t > 0).all() and t[best.value] == t.min()
+    # too small an output array is an argument error, nothing is run
+    assert h.lib.coral_autotune_sgemm_tiles(h.h, 3, 0, 0, m, n, k, C.c_void_p(A.data_ptr()), m,
+                                            C.c_void_p(B.data_ptr()), k, C.c_void_p(Cm.data_ptr()), m, 1,
+                                            ms, 10, C.byref(count), C.byref(best)) == 1
+    assert h.gemm_tile(3, 0, 0, 8192, 8192, 8192) == (256, 256, 1)  # configuration restored
 
 
 def _net_and_batch(seed, batch=64):
@@ -110,8 +136,6 @@ def test_selector_attached_drives_configuration(cuda):
     h = cb.handle()
     net = tuning.Mlp(seed=4)
     net.attach(h)
-    bn, sp = C.c_int(), C.c_int()
-    assert h.lib.coral_get_gemm_config(h.h, 3, 0, 0, 1000, 1000, 1000, C.byref(bn), C.byref(sp)) == 0
-    assert (bn.value, sp.value) in tuning.CANDIDATES
+    assert h.gemm_tile(3, 0, 0, 1000, 1000, 1000) in tuning.CANDIDATES
     cb.set_gemm_mode(cb.GemmMode.SPLIT_BF16X3)
     gemm_case(cb.sgemm, np.float32, 0, 0, 300, 200, 1500, 1.5, 0.5, 4e-5, sample=2048)

@@ -1,6 +1,8 @@
 """The trained selector (coral_b200/data/selector.npz) against exhaustive
 autotuning on the 2000 held-out shapes of coral_b200/data/timings_heldout.npz
-(every configuration timed on a B200 by coral_autotune_sgemm).
+(every configuration -- CTA-pair 256 x 256, 128 x 256 and 128 x 128 tiles,
+each with split-K 1..16 -- timed on a B200 by coral_autotune_sgemm_tiles; a
+quarter of the shapes in the 3-piece mode, which has no 128 x 256 tile).
 
 CPU: predictions from the float64 restatement of the network (oracle);
 GPU: predictions from the library's own forward kernel.  Both must give a
@@ -28,7 +30,7 @@ def test_selector_regret_cpu_oracle():
     i, h, o = (int(v) for v in w["shape"])
     X = tuning.feature_matrix(shapes)
     y, _ = mlp_ref.forward(w["params"], X, i, h, o)
-    choice = y.reshape(len(shapes), len(tuning.CANDIDATES)).argmin(1)
+    choice = tuning.choose(y, shapes)
     r = tuning.regret(times, choice)
     dflt = tuning.regret(times, np.array([tuning.default_choice(s) for s in shapes]))
     assert r.mean() <= 0.05, r.mean()
@@ -38,8 +40,14 @@ def test_selector_regret_cpu_oracle():
 def test_timing_db_is_exhaustive_and_positive():
     shapes, times, _ = _load()
     assert times.shape == (len(shapes), len(tuning.CANDIDATES)) and (times > 0).all()
+    # exactly the configurations a shape's mode lacks are +inf
+    assert (np.isfinite(times) == tuning.valid_mask(shapes)).all()
     train = np.load(os.path.join(DATA, "timings_train.npz"))
-    assert train["times"].shape == (20000, 10)
+    assert train["times"].shape == (20000, 15)
+    # both modes occur, and the pair tiles win on a share of the shapes
+    assert set(np.unique(train["shapes"][:, 5])) == {3, 6}
+    best = np.array(tuning.CANDIDATES)[train["times"].argmin(1)]
+    assert 0.05 < (best[:, 0] == 256).mean() < 0.95
     # held-out shapes come from a different seed than the training shapes
     assert not np.array_equal(train["shapes"][2:12], shapes[2:12])
 
