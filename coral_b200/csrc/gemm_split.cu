@@ -473,7 +473,7 @@ k_gemm_split(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles, int 
   constexpr int kCols = BN / 2;  // accumulator columns per epilogue thread
 
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* smem = tc::align1024_shared(smem_raw);
   __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages];
   __shared__ __align__(8) uint64_t chunk_full[2], chunk_empty[2];
   __shared__ uint32_t tmem_slot;
@@ -768,7 +768,7 @@ k_gemm_split_pair(const __grid_constant__ SplitMaps maps, int kdim, int m_tiles,
   constexpr uint16_t kPairMask = 3;
 
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* smem = tc::align1024_shared(smem_raw);
   __shared__ __align__(8) uint64_t full_bar[kS], empty_bar[kS];
   __shared__ __align__(8) uint64_t chunk_full[2], chunk_empty[2];
   __shared__ uint32_t tmem_slot;

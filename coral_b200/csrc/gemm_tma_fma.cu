@@ -97,7 +97,7 @@ k_gemm_tma_fma(const __grid_constant__ TfMaps maps, int m, int n, int k, T alpha
   using S = TfShape<T>;
   constexpr int TM = S::TM, TN = S::TN, V = S::V, BKd = S::BK;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* smem = tc::align1024_shared(smem_raw);
   __shared__ __align__(8) uint64_t full_bar[kTfStages], empty_bar[kTfStages];
   __shared__ int abort_flag;
 

@@ -294,7 +294,7 @@ k_gemm_grouped_tc(const coral_sgemm_problem_t* __restrict__ probs, int count,
   constexpr uint32_t kStage = tc_stage_bytes<NPC>();
 
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* smem = tc::align1024_shared(smem_raw);
   __shared__ __align__(8) uint64_t full_bar[S], empty_bar[S];
   __shared__ __align__(8) uint64_t acc_full[2], acc_empty[2];
   __shared__ __align__(8) uint64_t tq_full[kQueue], tq_empty[kQueue];

@@ -253,7 +253,7 @@ k_gemm_ozaki(const __grid_constant__ OzMaps maps, int kdim, int m_tiles, int n_t
   constexpr int kCols = kOzBN / 2;  // columns per epilogue thread
 
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* smem = tc::align1024_shared(smem_raw);
   __shared__ __align__(8) uint64_t full_bar[kOzStages], empty_bar[kOzStages];
   __shared__ __align__(8) uint64_t acc_full, acc_empty;
   __shared__ uint32_t tmem_slot;

@@ -16,6 +16,14 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// First 1024-byte boundary at or after the start of a dynamic shared-memory
+// array.  The offset is applied to the array itself, not to an integer, so the
+// result stays in the shared window: accesses through it compile to shared
+// loads and stores, where a pointer rebuilt from an integer would be generic.
+__device__ __forceinline__ uint8_t* align1024_shared(uint8_t* raw) {
+  return raw + ((1024u - (smem_u32(raw) & 1023u)) & 1023u);
+}
+
 __device__ __forceinline__ uint64_t globaltimer() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

@@ -638,7 +638,7 @@ k_tri_strips_tma(const __grid_constant__ CUtensorMap map, int n, const T* __rest
   constexpr bool kRow = ModeT<kMode>::kRow;
   using VT = typename TsVec<T>::type;
   extern __shared__ __align__(128) uint8_t ts_raw[];
-  uint8_t* ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(ts_raw) + 127) & ~uintptr_t(127));
+  uint8_t* ring = ts_raw + ((128u - (tc::smem_u32(ts_raw) & 127u)) & 127u);  // stays in the shared window
   __shared__ __align__(8) uint64_t full_bar[kTsStages], empty_bar[kTsStages];
   __shared__ __align__(16) T red[kTsGroups][2][kTsConsumers][kS];
   __shared__ int abort_flag;
