@@ -158,10 +158,10 @@ k_gemm_tma_fma(const __grid_constant__ TfMaps maps, int m, int n, int k, T alpha
       }
       const uint8_t* ta = smem + (size_t)s * S::kStage;
       const uint8_t* tb = ta + S::kABytes;
-      // measured per type: fp32 runs fastest with the K-group loop rolled
-      // (register pressure), fp64 with it fully unrolled
-      constexpr int kUnroll = sizeof(T) == 4 ? 1 : BKd / V;
-#pragma unroll kUnroll
+      // fully unrolled for both types: with the tiles addressed in the
+      // shared window the fp32 kernel fits it (NN 8192^3: 47.9 TFLOP/s
+      // rolled, 50.9 unrolled)
+#pragma unroll
       for (int kq = 0; kq < BKd / V; ++kq) {
         T a[TM][V], b[TN][V];
         load_block<T, TM, S::BM, AK>(ta, ty, kq, a);
