@@ -276,9 +276,10 @@ constexpr int kLd = kCB + 4;     // row stride of the square work arrays (16-byt
 struct ClusterSmem {
   float ring[kCStages][kCB][kCB];     // panel tiles as loaded: [stored col][stored row]
   float raw[3][kCB][kCB];             // diagonal block, tiles (b-1), (b-2) as loaded
-  float Dm[kCB][kLd];                 // op(D) masked (lower form), then inv(op(D)) transposed
-  float W[kCB][kLd];                  // inverse under construction, then op(tile b-2), then M2
-  float Top[kCB][kLd];                // inversion scratch, then op(tile b-1), then M1
+  float Dm[kCB][kLd];                 // op(D) masked, in lower form
+  float W[kCB][kLd];                  // op(tile b-2), rows in the order of Dm
+  float Top[kCB][kLd];                // op(tile b-1), rows in the order of Dm
+  float rdiag[kCB];                   // reciprocals of Dm's diagonal
   float xs[kXRing][kCB];              // staged solutions of panel tiles
   unsigned long long xin[kClMax][kCB];  // solutions pushed by earlier CTAs of the cluster
   float part[8][kCB];
@@ -382,61 +383,35 @@ __device__ __forceinline__ bool fetch_x(const unsigned long long* src, bool loca
   return true;
 }
 
-// Inverse of a 64 x 64 lower-triangular L into X by 8 x 8 blocks: the diagonal blocks are inverted by
-// substitution (one warp each), Lp = blockdiag(inv(L_II)) L is formed for the
-// blocks left of the diagonal, and then block diagonal d = 1..7 of the
-// inverse follows from X_IJ = -sum_{K=J}^{I-1} Lp_IK X_KJ, whose terms lie on
-// diagonals < d.  Seven short dependent stages instead of 63 substitution
-// steps.  Consumer threads only (tid < 256); rdiag holds 64 floats of
-// scratch.  All arrays have row stride kLd.
-__device__ __forceinline__ void invert_lower64(float (*L)[kLd], float (*X)[kLd], float (*Lp)[kLd],
-                                               float* rdiag, int tid) {
-  for (int e = tid; e < kCB * kLd; e += kCons) (&X[0][0])[e] = 0.f;
-  if (tid < kCB) rdiag[tid] = 1.f / L[tid][tid];
-  bar_consumers();
-  {
-    const int w = tid >> 5, c = tid & 31;
-    if (c < 8) {
-      const int o = 8 * w;
-      float xc[8];
+// Column `col` of X = inv(L) B for the 64 x 64 lower-triangular L in Dm
+// (reciprocal diagonal in rdiag), B = [I | Top | W] (192 columns), by forward
+// substitution with the column in registers: x_i = (b_i - sum_{j<i} L_ij x_j)
+// / L_ii, the sum over j split four ways.  Each thread solves its column with
+// no barrier; L's rows are read as broadcast 16-byte shared loads.  Column c
+// of X goes to out[c / 64] at row i, position (c % 64) ^ (4 (i % 8)): the
+// swizzle keeps both this column-wise store and the row-wise 16-byte reads of
+// the later register loads free of bank conflicts.
+__device__ __forceinline__ void solve_column(const ClusterSmem& S, int col, float (*out)[kCB][kCB]) {
+  const int part = col >> 6, c = col & 63;
+  float xc[kCB];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        float a = (i == c) ? 1.f : 0.f;
+  for (int i = 0; i < kCB; ++i) {
+    float a0 = part == 0 ? (i == c ? 1.f : 0.f) : part == 1 ? S.Top[i][c] : S.W[i][c];
+    float a1 = 0.f, a2 = 0.f, a3 = 0.f;
 #pragma unroll
-        for (int j = 0; j < i; ++j) a = fmaf(-L[o + i][o + j], xc[j], a);
-        xc[i] = (i < c) ? 0.f : a * rdiag[o + i];
-      }
-#pragma unroll
-      for (int i = 0; i < 8; ++i) X[o + i][o + c] = xc[i];
+    for (int j = 0; j + 4 <= i; j += 4) {
+      const float4 l = *reinterpret_cast<const float4*>(&S.Dm[i][j]);
+      a0 = fmaf(-l.x, xc[j], a0);
+      a1 = fmaf(-l.y, xc[j + 1], a1);
+      a2 = fmaf(-l.z, xc[j + 2], a2);
+      a3 = fmaf(-l.w, xc[j + 3], a3);
     }
-  }
-  bar_consumers();
-  for (int e = tid; e < kCB * kCB; e += kCons) {
-    const int R = e / kCB, k = e % kCB, I = R >> 3;
-    float a = 0.f;
-    if (k < 8 * I) {
 #pragma unroll
-      for (int m = 0; m < 8; ++m) a = fmaf(X[R][8 * I + m], L[8 * I + m][k], a);
-    }
-    Lp[R][k] = a;
+    for (int j = i & ~3; j < i; ++j) a0 = fmaf(-S.Dm[i][j], xc[j], a0);
+    xc[i] = ((a0 + a1) + (a2 + a3)) * S.rdiag[i];
   }
-  bar_consumers();
-  for (int d = 1; d < 8; ++d) {
-    for (int o = tid; o < (8 - d) * 64; o += kCons) {
-      const int J = o >> 6, i = (o >> 3) & 7, j = o & 7, I = J + d;
-      const int R = 8 * I + i, C = 8 * J + j;
-      float a0 = 0.f, a1 = 0.f;
-      for (int K = J; K < I; ++K) {
 #pragma unroll
-        for (int m = 0; m < 8; m += 2) {
-          a0 = fmaf(Lp[R][8 * K + m], X[8 * K + m][C], a0);
-          a1 = fmaf(Lp[R][8 * K + m + 1], X[8 * K + m + 1][C], a1);
-        }
-      }
-      X[R][C] = -(a0 + a1);
-    }
-    bar_consumers();
-  }
+  for (int i = 0; i < kCB; ++i) out[part][i][c ^ ((i & 7) << 2)] = xc[i];
 }
 
 __global__ void __launch_bounds__(kCThreads, 1)
@@ -585,79 +560,89 @@ k_trsv_cluster(const __grid_constant__ CUtensorMap amap, int n, float* x, size_t
     const float rhs_v = (tid < kCB && b0 + tid < n) ? x[(size_t)(b0 + tid) * incx] : 0.f;
     bool ok = tc::mbar_wait(&S.setup_bar, 0, limit_ns);
     // op(D) masked: stored element (b0 + rr, b0 + cc) sits at raw[0][cc][rr].
-    // An upper op(D) is stored index-reversed (P op(D) P, P the reversal),
-    // which is lower triangular; its inverse is reversed back below.
-    for (int e = tid; e < kCB * kCB; e += kCons) {
-      const int rr = e % kCB, cc = e / kCB;
-      float v = S.raw[0][cc][rr];
-      const int r = trans ? cc : rr, c = trans ? rr : cc;
-      const bool in_tri = lower_eff ? r >= c : r <= c;
-      if (r == c) v = (unit || b0 + r >= n) ? 1.f : v;
-      else if (!in_tri) v = 0.f;
-      if (lower_eff) S.Dm[r][c] = v;
-      else S.Dm[kCB - 1 - r][kCB - 1 - c] = v;
+    // An upper op(D) is stored index-reversed (L = P op(D) P, P the reversal),
+    // which is lower triangular, and so are the rows of the right-hand sides.
+    // Every load of a loop before its stores: a store the compiler cannot
+    // prove disjoint from the next load would cost a shared-memory round trip
+    // per element.
+    constexpr int kPerT = kCB * kCB / kCons;
+    {
+      float vals[kPerT];
+#pragma unroll
+      for (int k = 0; k < kPerT; ++k) {
+        const int e = tid + k * kCons;
+        vals[k] = S.raw[0][e / kCB][e % kCB];
+      }
+#pragma unroll
+      for (int k = 0; k < kPerT; ++k) {
+        const int e = tid + k * kCons;
+        const int rr = e % kCB, cc = e / kCB;
+        float v = vals[k];
+        const int r = trans ? cc : rr, c = trans ? rr : cc;
+        const bool in_tri = lower_eff ? r >= c : r <= c;
+        if (r == c) v = (unit || b0 + r >= n) ? 1.f : v;
+        else if (!in_tri) v = 0.f;
+        S.Dm[lower_eff ? r : kCB - 1 - r][lower_eff ? c : kCB - 1 - c] = v;
+      }
+    }
+    // op(tile) row-major for blocks b-1 (Top) and b-2 (W), rows in L's order;
+    // zero where absent
+    {
+      float t1[kPerT], t2[kPerT];
+#pragma unroll
+      for (int k = 0; k < kPerT; ++k) {
+        const int e = tid + k * kCons;
+        const int i = trans ? e / kCB : e % kCB, c = trans ? e % kCB : e / kCB;
+        t1[k] = s >= 1 ? (trans ? S.raw[1][i][c] : S.raw[1][c][i]) : 0.f;
+        t2[k] = s >= 2 ? (trans ? S.raw[2][i][c] : S.raw[2][c][i]) : 0.f;
+      }
+#pragma unroll
+      for (int k = 0; k < kPerT; ++k) {
+        const int e = tid + k * kCons;
+        const int i = trans ? e / kCB : e % kCB, c = trans ? e % kCB : e / kCB;
+        const int li = lower_eff ? i : kCB - 1 - i;
+        S.Top[li][c] = t1[k];
+        S.W[li][c] = t2[k];
+      }
     }
     if (tid < kCB) S.rhs[tid] = rhs_v;
     bar_consumers();
-    invert_lower64(S.Dm, S.W, S.Top, S.v, tid);
-    // Dm <- inv(op(D)) transposed: Dm[i][r] = inv(op(D))[r][i]
-    for (int e = tid; e < kCB * kCB; e += kCons) {
-      const int i = e / kCB, r = e % kCB;
-      S.Dm[i][r] = lower_eff ? S.W[r][i] : S.W[kCB - 1 - r][kCB - 1 - i];
+    if (tid < kCB) S.rdiag[tid] = 1.f / S.Dm[tid][tid];
+    bar_consumers();
+    // [inv(L) | inv(L) Top | inv(L) W] by column substitutions into raw[0..2]
+    // (the raw tiles are consumed); the products the block does not need
+    // (no block b-1 or b-2) are skipped.
+    {
+      const int ncols = kCB * (1 + (s >= 1) + (s >= 2));
+      if (tid < ncols) solve_column(S, tid, S.raw);
     }
     bar_consumers();
-    // op(tile) row-major for blocks b-1 (Top) and b-2 (W); zero where absent
-    for (int e = tid; e < kCB * kCB; e += kCons) {
-      const int i = trans ? e / kCB : e % kCB, c = trans ? e % kCB : e / kCB;
-      S.Top[i][c] = s >= 1 ? (trans ? S.raw[1][i][c] : S.raw[1][c][i]) : 0.f;
-      S.W[i][c] = s >= 2 ? (trans ? S.raw[2][i][c] : S.raw[2][c][i]) : 0.f;
-    }
-    bar_consumers();
+    // Registers of thread (r, q): inv(op(D))[r][16q + j], and rows r of
+    // M1 = inv(op(D)) op(tile b-1), M2 = inv(op(D)) op(tile b-2), columns
+    // 16q + j.  With op(D) upper, inv(op(D)) = P inv(L) P and M = P X.
     const int r = tid >> 2, q = tid & 3, c0 = q * 16;
     float inv[16], M1[16], M2[16];
+    const int xr = lower_eff ? r : kCB - 1 - r;
+    const int sw = (xr & 7) << 2;  // the swizzle moves whole aligned groups of 4
 #pragma unroll
-    for (int j = 0; j < 16; ++j) inv[j] = S.Dm[c0 + j][r];
-    if (s >= 1) {
-      // [M1 | M2] = inv(op(D)) [op(tile b-1) | op(tile b-2)] as 4 x 4 register
-      // outer products: rows 4 rg .. 4 rg + 3, columns 4 cg .. 4 cg + 3 of
-      // each; a quarter-warp reads 128 contiguous bytes of each tile row.
-      const int rg = 2 * warp + (lane >> 4), cg = lane & 15;
-      float a1[4][4], a2[4][4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) a1[u][v] = a2[u][v] = 0.f;
-#pragma unroll 2
-      for (int i = 0; i < kCB; ++i) {
-        const float4 dv = *reinterpret_cast<const float4*>(&S.Dm[i][4 * rg]);
-        const float4 p = *reinterpret_cast<const float4*>(&S.Top[i][4 * cg]);
-        const float4 w2 = *reinterpret_cast<const float4*>(&S.W[i][4 * cg]);
-        const float d4[4] = {dv.x, dv.y, dv.z, dv.w};
-        const float p4[4] = {p.x, p.y, p.z, p.w};
-        const float w4[4] = {w2.x, w2.y, w2.z, w2.w};
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-          for (int v = 0; v < 4; ++v) {
-            a1[u][v] = fmaf(d4[u], p4[v], a1[u][v]);
-            a2[u][v] = fmaf(d4[u], w4[v], a2[u][v]);
-          }
-      }
-      bar_consumers();
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        *reinterpret_cast<float4*>(&S.Top[4 * rg + u][4 * cg]) = make_float4(a1[u][0], a1[u][1], a1[u][2], a1[u][3]);
-        *reinterpret_cast<float4*>(&S.W[4 * rg + u][4 * cg]) = make_float4(a2[u][0], a2[u][1], a2[u][2], a2[u][3]);
-      }
-      bar_consumers();
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        M1[j] = S.Top[r][c0 + j];
-        M2[j] = S.W[r][c0 + j];
-      }
-    } else {
-#pragma unroll
-      for (int j = 0; j < 16; ++j) M1[j] = M2[j] = 0.f;
+    for (int g = 0; g < 4; ++g) {
+      // inv: columns c0 + 4g .. c0 + 4g + 3, or (upper) 63 - c0 - 4g down to 60 - c0 - 4g
+      const int ci = lower_eff ? c0 + 4 * g : kCB - 4 - c0 - 4 * g;
+      const float4 vi4 = *reinterpret_cast<const float4*>(&S.raw[0][xr][ci ^ sw]);
+      const float4 m14 = *reinterpret_cast<const float4*>(&S.raw[1][xr][(c0 + 4 * g) ^ sw]);
+      const float4 m24 = *reinterpret_cast<const float4*>(&S.raw[2][xr][(c0 + 4 * g) ^ sw]);
+      inv[4 * g + 0] = lower_eff ? vi4.x : vi4.w;
+      inv[4 * g + 1] = lower_eff ? vi4.y : vi4.z;
+      inv[4 * g + 2] = lower_eff ? vi4.z : vi4.y;
+      inv[4 * g + 3] = lower_eff ? vi4.w : vi4.x;
+      M1[4 * g + 0] = s >= 1 ? m14.x : 0.f;
+      M1[4 * g + 1] = s >= 1 ? m14.y : 0.f;
+      M1[4 * g + 2] = s >= 1 ? m14.z : 0.f;
+      M1[4 * g + 3] = s >= 1 ? m14.w : 0.f;
+      M2[4 * g + 0] = s >= 2 ? m24.x : 0.f;
+      M2[4 * g + 1] = s >= 2 ? m24.y : 0.f;
+      M2[4 * g + 2] = s >= 2 ? m24.z : 0.f;
+      M2[4 * g + 3] = s >= 2 ? m24.w : 0.f;
     }
 
     // panel: acc = sum over solve indices k <= s-3 of op(A)(b, k) x_k
