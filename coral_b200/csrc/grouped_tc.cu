@@ -10,11 +10,12 @@
 //
 // The instances' operands have arbitrary leading dimensions and alignments,
 // which tensor maps cannot describe without per-instance host work, so the
-// operands are staged by producer warps instead of TMA: plain loads coalesced
-// along whichever dimension the instance stores contiguously (for an operand
-// stored along K, one warp load covers 32
-// consecutive K values of a row), conversion to bf16 pieces in registers, and
-// shared stores into the K-major 64-byte-swizzled layout that a TMA
+// operands are staged by producer warps instead of TMA: each thread takes
+// items of 8 consecutive K values of one row -- one contiguous segment (16-byte
+// loads where it is aligned) for an operand stored along K, or 8 row-coalesced
+// loads for one stored along the rows -- converts them to bf16 pieces in
+// registers, and writes each piece with one 16-byte shared store into the
+// K-major 64-byte-swizzled layout that a TMA
 // CU_TENSOR_MAP_SWIZZLE_64B load would write (rows of 32 bf16, 8-row / 512-byte
 // atoms, 16-byte chunk c of row r at chunk c ^ ((r >> 1) & 3)), so the MMA
 // descriptors are the same as the TMA-fed kernels'.
@@ -188,37 +189,80 @@ __device__ __forceinline__ uint32_t sw64_offset(int r, int kk) {
                                                                            (kk & 7) * 2);
 }
 
+// Eight consecutive values p[0..8) as floats, with one or two 16-byte loads
+// when p is 16-byte aligned (8- and 4-byte pair loads for the other cases
+// measured slower for bf16 inputs).
+__device__ __forceinline__ void ld8(const float* p, float* v) {
+  if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+    const float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  } else {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = __ldg(p + j);
+  }
+}
+__device__ __forceinline__ void ld8(const __nv_bfloat16* p, float* v) {
+  if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+    const uint4 u = __ldg(reinterpret_cast<const uint4*>(p));
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float2 f = __bfloat1622float2(h[j]);
+      v[2 * j] = f.x;
+      v[2 * j + 1] = f.y;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = __bfloat162float(__ldg(p + j));
+  }
+}
+
+// Item e of an operand tile: 8 consecutive K values of one row.  Along K the
+// items run row-major (4 per row: lanes on the chunks of 8 consecutive rows,
+// each item one contiguous 16- or 32-byte segment); along the rows they run
+// chunk-major (lanes on consecutive rows, each of the 8 loads one coalesced
+// row segment).
+__device__ __forceinline__ void item_rc(bool kc, int e, int rows, int& r, int& c) {
+  if (kc) {
+    r = e >> 2;
+    c = e & 3;
+  } else {
+    r = e % rows;
+    c = e / rows;
+  }
+}
+
 // Loads one operand's share of a 32-deep slab for this producer thread into
 // v[0 .. kVals): rows [row0, row0 + rows) of an operand stored contiguous
-// along K (element (r, k) at X[k + r ld]) or along the rows (X[r + k ld]).
-//   along K: producer warp pw takes rows pw, pw + 8, ...; lane l holds K
-//     position l, so one warp load reads 32 consecutive elements of a row;
-//   along the rows: item e = (row e % rows, K chunk e / rows) of 8 K values,
-//     lanes on consecutive rows, so each of the 8 loads is one coalesced row
-//     segment.
-// Everything outside R x Kd (and rows past `rows`) reads as zero.
+// along K (element (r, k) at X[k + r ld]) or along the rows (X[r + k ld]),
+// one item of 8 K values per 8 entries of v.  Everything outside R x Kd (and
+// rows past `rows`) reads as zero.
 template <typename TIn, int kVals>
 __device__ __forceinline__ void load_share(const TIn* __restrict__ X, long long ld, bool kc, int R, int Kd,
                                            int row0, int rows, int k0, int ptid, float (&v)[kVals]) {
   constexpr int kPT = 32 * kProdWarps;
-  const int pw = ptid >> 5, lane = ptid & 31;
 #pragma unroll
   for (int i = 0; i < kVals; ++i) v[i] = 0.f;
-  if (kc) {
-    const int gk = k0 + lane;
 #pragma unroll
-    for (int i = 0; i < kVals; ++i) {
-      const int r = pw + kProdWarps * i;
-      if (r < rows && row0 + r < R && gk < Kd) v[i] = ld_val<TIn>(X + (size_t)(row0 + r) * ld + gk);
-    }
-  } else {
+  for (int it = 0; it < kVals / 8; ++it) {
+    const int e = ptid + it * kPT;
+    if (e >= rows * 4) continue;
+    int r, c;
+    item_rc(kc, e, rows, r, c);
+    const int gr = row0 + r, gk = k0 + 8 * c;
+    if (gr >= R) continue;
+    if (kc) {
+      const TIn* p = X + (size_t)gr * ld + gk;
+      if (gk + 8 <= Kd) {
+        ld8(p, &v[it * 8]);
+      } else {
 #pragma unroll
-    for (int it = 0; it < kVals / 8; ++it) {
-      const int e = ptid + it * kPT;
-      if (e >= rows * 4) continue;
-      const int r = e % rows, c = e / rows;
-      const int gr = row0 + r, gk = k0 + 8 * c;
-      if (gr >= R) continue;
+        for (int j = 0; j < 8; ++j)
+          if (gk + j < Kd) v[it * 8 + j] = ld_val<TIn>(p + j);
+      }
+    } else {
       const TIn* p = X + gr + (size_t)gk * ld;
 #pragma unroll
       for (int j = 0; j < 8; ++j)
@@ -227,43 +271,29 @@ __device__ __forceinline__ void load_share(const TIn* __restrict__ X, long long 
   }
 }
 
-// Converts and stores what load_share loaded: NPC bf16 pieces of each value
-// at dst + pc * piece_bytes (2-byte stores for the along-K layout, one 16-byte
-// store per item and piece for the along-rows layout).
+// Converts and stores what load_share loaded: NPC bf16 pieces of each value,
+// one 16-byte store per item and piece at dst + pc * piece_bytes.
 template <int NPC, int kVals>
 __device__ __forceinline__ void store_share(uint8_t* dst, uint32_t piece_bytes, bool kc, int rows, int ptid,
                                             const float (&v)[kVals]) {
   constexpr int kPT = 32 * kProdWarps;
-  const int pw = ptid >> 5, lane = ptid & 31;
-  if (kc) {
 #pragma unroll
-    for (int i = 0; i < kVals; ++i) {
-      const int r = pw + kProdWarps * i;
-      if (r >= rows) continue;
-      const uint32_t off = sw64_offset(r, lane);
-      const __nv_bfloat16 h0 = __float2bfloat16_rn(v[i]);
-      *reinterpret_cast<__nv_bfloat16*>(dst + off) = h0;
-      if constexpr (NPC == 2)
-        *reinterpret_cast<__nv_bfloat16*>(dst + piece_bytes + off) = __float2bfloat16_rn(v[i] - __bfloat162float(h0));
+  for (int it = 0; it < kVals / 8; ++it) {
+    const int e = ptid + it * kPT;
+    if (e >= rows * 4) continue;
+    int r, c;
+    item_rc(kc, e, rows, r, c);
+    __align__(16) __nv_bfloat16 q[NPC][8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const __nv_bfloat16 h0 = __float2bfloat16_rn(v[it * 8 + j]);
+      q[0][j] = h0;
+      if constexpr (NPC == 2) q[1][j] = __float2bfloat16_rn(v[it * 8 + j] - __bfloat162float(h0));
     }
-  } else {
+    const uint32_t off = sw64_offset(r, 8 * c);
 #pragma unroll
-    for (int it = 0; it < kVals / 8; ++it) {
-      const int e = ptid + it * kPT;
-      if (e >= rows * 4) continue;
-      const int r = e % rows, c = e / rows;
-      __align__(16) __nv_bfloat16 q[NPC][8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const __nv_bfloat16 h0 = __float2bfloat16_rn(v[it * 8 + j]);
-        q[0][j] = h0;
-        if constexpr (NPC == 2) q[1][j] = __float2bfloat16_rn(v[it * 8 + j] - __bfloat162float(h0));
-      }
-      const uint32_t off = sw64_offset(r, 8 * c);
-#pragma unroll
-      for (int pc = 0; pc < NPC; ++pc)
-        *reinterpret_cast<uint4*>(dst + pc * piece_bytes + off) = *reinterpret_cast<const uint4*>(q[pc]);
-    }
+    for (int pc = 0; pc < NPC; ++pc)
+      *reinterpret_cast<uint4*>(dst + pc * piece_bytes + off) = *reinterpret_cast<const uint4*>(q[pc]);
   }
 }
 
@@ -274,8 +304,8 @@ __device__ __forceinline__ void store_share(uint8_t* dst, uint32_t piece_bytes, 
 // one memory round trip.
 template <typename TIn, int NPC>
 __device__ __forceinline__ void stage_slab(const SlabSrc<TIn>& src, int k0, uint8_t* st, int ptid) {
-  constexpr int kAVals = kTM / kProdWarps;       // 16: along-K rows per warp, or 2 items of 8
-  constexpr int kBVals = kMaxBN / kProdWarps;    // 32: along-K rows per warp, or 4 items of 8
+  constexpr int kAVals = kTM / kProdWarps;       // 8: one item of 8 K values per producer thread
+  constexpr int kBVals = kMaxBN / kProdWarps;    // 16: two items
   float va[kAVals], vb[kBVals];
   load_share<TIn, kAVals>(src.a, src.lda, src.a_kc, src.m, src.k, src.m0, kTM, k0, ptid, va);
   load_share<TIn, kBVals>(src.b, src.ldb, src.b_kc, src.n, src.k, src.n0, src.bn, k0, ptid, vb);

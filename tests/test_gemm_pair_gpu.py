@@ -101,3 +101,15 @@ def test_sgemm_pair_4096_meets_1e6(cuda):
                                      C0.cpu().numpy(), m, ii, jj)
     got = C.cpu().numpy()[ii + jj * m].astype(np.float64)
     assert float((np.abs(got - want) / bound).max()) <= 1e-6
+
+
+@pytest.mark.parametrize("ops", [(0, 0), (2, 1)])
+def test_cgemm_pair_3m(cuda, pair_tiles, ops):
+    """3M mapping on pair tiles: the three real split GEMMs each run as
+    CTA-pair tiles; tolerance as in the single-CTA 3M tests."""
+    cb.set_gemm_mode(cb.GemmMode.SPLIT_BF16X3)
+    pair_tiles.set_complex_mapping(1)
+    try:
+        gemm_case(cb.cgemm, np.complex64, *ops, 300, 260, 700, 1.5 - 0.5j, 0.25 + 1j, 6 * 4e-5, sample=4096)
+    finally:
+        pair_tiles.set_complex_mapping(0)
