@@ -48,6 +48,8 @@
 
 #include <cuda_bf16.h>
 
+#include <type_traits>
+
 namespace coral {
 namespace {
 
@@ -297,6 +299,66 @@ __device__ __forceinline__ void store_share(uint8_t* dst, uint32_t piece_bytes, 
   }
 }
 
+// bf16 inputs need no conversion: their bits go to shared memory as loaded.
+// Loads one operand's share of a slab as packed bf16 pairs (w[it * 4 + h] =
+// K values 2h and 2h + 1 of item it), with the items of load_share; zero
+// bits (+0.0) outside R x Kd.
+template <int kItems>
+__device__ __forceinline__ void load_share_bf16(const __nv_bfloat16* __restrict__ X, long long ld, bool kc, int R,
+                                                int Kd, int row0, int rows, int k0, int ptid,
+                                                uint32_t (&w)[4 * kItems]) {
+  constexpr int kPT = 32 * kProdWarps;
+  const unsigned short* Xs = reinterpret_cast<const unsigned short*>(X);
+#pragma unroll
+  for (int i = 0; i < 4 * kItems; ++i) w[i] = 0u;
+#pragma unroll
+  for (int it = 0; it < kItems; ++it) {
+    const int e = ptid + it * kPT;
+    if (e >= rows * 4) continue;
+    int r, c;
+    item_rc(kc, e, rows, r, c);
+    const int gr = row0 + r, gk = k0 + 8 * c;
+    if (gr >= R) continue;
+    unsigned short h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (kc) {
+      const unsigned short* p = Xs + (size_t)gr * ld + gk;
+      if (gk + 8 <= Kd && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+        const uint4 u = __ldg(reinterpret_cast<const uint4*>(p));
+        w[it * 4 + 0] = u.x;
+        w[it * 4 + 1] = u.y;
+        w[it * 4 + 2] = u.z;
+        w[it * 4 + 3] = u.w;
+        continue;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (gk + j < Kd) h[j] = __ldg(p + j);
+    } else {
+      const unsigned short* p = Xs + gr + (size_t)gk * ld;
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (gk + j < Kd) h[j] = __ldg(p + (size_t)j * ld);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) w[it * 4 + j] = (uint32_t)h[2 * j] | ((uint32_t)h[2 * j + 1] << 16);
+  }
+}
+
+template <int kItems>
+__device__ __forceinline__ void store_share_bf16(uint8_t* dst, bool kc, int rows, int ptid,
+                                                 const uint32_t (&w)[4 * kItems]) {
+  constexpr int kPT = 32 * kProdWarps;
+#pragma unroll
+  for (int it = 0; it < kItems; ++it) {
+    const int e = ptid + it * kPT;
+    if (e >= rows * 4) continue;
+    int r, c;
+    item_rc(kc, e, rows, r, c);
+    *reinterpret_cast<uint4*>(dst + sw64_offset(r, 8 * c)) =
+        make_uint4(w[it * 4], w[it * 4 + 1], w[it * 4 + 2], w[it * 4 + 3]);
+  }
+}
+
 // Stages one 32-deep K slab of a tile: A rows [m0, m0 + 128) and B rows
 // [n0, n0 + bn) as NPC bf16 piece tiles, A pieces at st + i * kAPieceBytes
 // and B pieces after them, 64-byte swizzled.  Every load of the thread's share
@@ -306,11 +368,19 @@ template <typename TIn, int NPC>
 __device__ __forceinline__ void stage_slab(const SlabSrc<TIn>& src, int k0, uint8_t* st, int ptid) {
   constexpr int kAVals = kTM / kProdWarps;       // 8: one item of 8 K values per producer thread
   constexpr int kBVals = kMaxBN / kProdWarps;    // 16: two items
-  float va[kAVals], vb[kBVals];
-  load_share<TIn, kAVals>(src.a, src.lda, src.a_kc, src.m, src.k, src.m0, kTM, k0, ptid, va);
-  load_share<TIn, kBVals>(src.b, src.ldb, src.b_kc, src.n, src.k, src.n0, src.bn, k0, ptid, vb);
-  store_share<NPC, kAVals>(st, kAPieceBytes, src.a_kc, kTM, ptid, va);
-  store_share<NPC, kBVals>(st + NPC * kAPieceBytes, kBPieceBytes, src.b_kc, src.bn, ptid, vb);
+  if constexpr (std::is_same<TIn, __nv_bfloat16>::value) {
+    uint32_t wa[kAVals / 2], wb[kBVals / 2];
+    load_share_bf16<kAVals / 8>(src.a, src.lda, src.a_kc, src.m, src.k, src.m0, kTM, k0, ptid, wa);
+    load_share_bf16<kBVals / 8>(src.b, src.ldb, src.b_kc, src.n, src.k, src.n0, src.bn, k0, ptid, wb);
+    store_share_bf16<kAVals / 8>(st, src.a_kc, kTM, ptid, wa);
+    store_share_bf16<kBVals / 8>(st + kAPieceBytes, src.b_kc, src.bn, ptid, wb);
+  } else {
+    float va[kAVals], vb[kBVals];
+    load_share<TIn, kAVals>(src.a, src.lda, src.a_kc, src.m, src.k, src.m0, kTM, k0, ptid, va);
+    load_share<TIn, kBVals>(src.b, src.ldb, src.b_kc, src.n, src.k, src.n0, src.bn, k0, ptid, vb);
+    store_share<NPC, kAVals>(st, kAPieceBytes, src.a_kc, kTM, ptid, va);
+    store_share<NPC, kBVals>(st + NPC * kAPieceBytes, kBPieceBytes, src.b_kc, src.bn, ptid, vb);
+  }
 }
 
 template <typename TIn, int NPC>
