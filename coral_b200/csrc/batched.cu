@@ -213,7 +213,7 @@ k_gemm_grouped(const GemmProblem* __restrict__ probs, int count, const int* __re
 constexpr int kBT = 64;
 constexpr int kBTThreads = 256;
 
-__global__ void __launch_bounds__(kBTThreads)
+__global__ void __launch_bounds__(kBTThreads, 6)
 k_trsv_batched(const TrsvProblem* __restrict__ probs, int count) {
   __shared__ float D[kBT][kBT + 1];  // D[r][c] = op(A)(b0 + r, b0 + c)
   __shared__ float xb[kBT];
@@ -235,12 +235,23 @@ k_trsv_batched(const TrsvProblem* __restrict__ probs, int count) {
   for (int bi = 0; bi < nblk; ++bi) {
     const int blk = lower_eff ? bi : nblk - 1 - bi;
     const int b0 = blk * kBT, bn = min(kBT, n - b0);
-    // stage the diagonal block of op(A)
-    for (int e = threadIdx.x; e < kBT * kBT; e += kBTThreads) {
-      const int r = e % kBT, c = e / kBT;
-      float v = 0.f;
-      if (r < bn && c < bn) v = t ? A[(b0 + c) + (size_t)(b0 + r) * lda] : A[(b0 + r) + (size_t)(b0 + c) * lda];
-      D[r][c] = v;
+    // stage the diagonal block of op(A): loads in groups of 8 before their
+    // stores, so the block costs two memory round trips
+#pragma unroll
+    for (int q0 = 0; q0 < kBT * kBT / kBTThreads; q0 += 8) {
+      float dv[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int e = threadIdx.x + (q0 + q) * kBTThreads;
+        const int r = e % kBT, c = e / kBT;
+        dv[q] = (r < bn && c < bn) ? (t ? A[(b0 + c) + (size_t)(b0 + r) * lda] : A[(b0 + r) + (size_t)(b0 + c) * lda])
+                                   : 0.f;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int e = threadIdx.x + (q0 + q) * kBTThreads;
+        D[e % kBT][e / kBT] = dv[q];
+      }
     }
     if (threadIdx.x < kBT) xb[threadIdx.x] = threadIdx.x < bn ? x[(size_t)(b0 + threadIdx.x) * incx] : 0.f;
     __syncthreads();
@@ -274,11 +285,20 @@ k_trsv_batched(const TrsvProblem* __restrict__ probs, int count) {
     if (threadIdx.x < bn) x[(size_t)(b0 + threadIdx.x) * incx] = xb[threadIdx.x];
     // update the rows still to be solved: rhs_i -= sum_c op(A)(i, b0 + c) xb[c]
     const int r_lo = lower_eff ? b0 + bn : 0, r_hi = lower_eff ? n : b0;
+    // A row's loads go out 16 at a time before their sums (a single CTA
+    // solves the largest instances, so its memory parallelism sets the
+    // batch's tail)
     for (int i = r_lo + threadIdx.x; i < r_hi; i += kBTThreads) {
-      float s = 0.f;
-#pragma unroll 8
-      for (int c = 0; c < bn; ++c) s = fmaf(opA(i, b0 + c), xb[c], s);
-      x[(size_t)i * incx] -= s;
+      float s4[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 1
+      for (int c0 = 0; c0 < kBT; c0 += 16) {
+        float a[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) a[c] = c0 + c < bn ? opA(i, b0 + c0 + c) : 0.f;
+#pragma unroll
+        for (int c = 0; c < 16; ++c) s4[c & 3] = fmaf(a[c], xb[c0 + c], s4[c & 3]);
+      }
+      x[(size_t)i * incx] -= (s4[0] + s4[1]) + (s4[2] + s4[3]);
     }
     __syncthreads();
   }
