@@ -213,7 +213,7 @@ k_gemm_grouped(const GemmProblem* __restrict__ probs, int count, const int* __re
 constexpr int kBT = 64;
 constexpr int kBTThreads = 256;
 
-__global__ void __launch_bounds__(kBTThreads, 6)
+__global__ void __launch_bounds__(kBTThreads, 4)
 k_trsv_batched(const TrsvProblem* __restrict__ probs, int count) {
   __shared__ float D[kBT][kBT + 1];  // D[r][c] = op(A)(b0 + r, b0 + c)
   __shared__ float xb[kBT];
@@ -285,20 +285,29 @@ k_trsv_batched(const TrsvProblem* __restrict__ probs, int count) {
     if (threadIdx.x < bn) x[(size_t)(b0 + threadIdx.x) * incx] = xb[threadIdx.x];
     // update the rows still to be solved: rhs_i -= sum_c op(A)(i, b0 + c) xb[c]
     const int r_lo = lower_eff ? b0 + bn : 0, r_hi = lower_eff ? n : b0;
-    // A row's loads go out 16 at a time before their sums (a single CTA
-    // solves the largest instances, so its memory parallelism sets the
+    // Two rows at a time, their loads 16 per row before the sums (a single
+    // CTA solves the largest instances, so its memory parallelism sets the
     // batch's tail)
-    for (int i = r_lo + threadIdx.x; i < r_hi; i += kBTThreads) {
-      float s4[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int i = r_lo + threadIdx.x; i < r_hi; i += 2 * kBTThreads) {
+      const int i2 = i + kBTThreads;
+      const bool two = i2 < r_hi;
+      float s4[4] = {0.f, 0.f, 0.f, 0.f}, u4[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
       for (int c0 = 0; c0 < kBT; c0 += 16) {
-        float a[16];
+        float a[16], b[16];
 #pragma unroll
-        for (int c = 0; c < 16; ++c) a[c] = c0 + c < bn ? opA(i, b0 + c0 + c) : 0.f;
+        for (int c = 0; c < 16; ++c) {
+          a[c] = c0 + c < bn ? opA(i, b0 + c0 + c) : 0.f;
+          b[c] = two && c0 + c < bn ? opA(i2, b0 + c0 + c) : 0.f;
+        }
 #pragma unroll
-        for (int c = 0; c < 16; ++c) s4[c & 3] = fmaf(a[c], xb[c0 + c], s4[c & 3]);
+        for (int c = 0; c < 16; ++c) {
+          s4[c & 3] = fmaf(a[c], xb[c0 + c], s4[c & 3]);
+          u4[c & 3] = fmaf(b[c], xb[c0 + c], u4[c & 3]);
+        }
       }
       x[(size_t)i * incx] -= (s4[0] + s4[1]) + (s4[2] + s4[3]);
+      if (two) x[(size_t)i2 * incx] -= (u4[0] + u4[1]) + (u4[2] + u4[3]);
     }
     __syncthreads();
   }
