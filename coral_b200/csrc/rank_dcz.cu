@@ -83,7 +83,10 @@ k_rank_g(int m, int n, T alpha, const T* __restrict__ x, size_t incx, const T* _
 // Each element gets exactly k_rank_g's arithmetic. A vector that straddles
 // the edge of a column's triangle, or the last row, is read and written
 // element by element, in-range elements only.
-constexpr int kGCols = 8;
+// Columns per thread: 8, or 4 for CHER2, whose two complex coefficients per
+// column would otherwise hold the kernel to two CTAs per SM.
+template <typename T, int kKind>
+constexpr int gcols() { return (kKind == kHer2G && sizeof(T) == 8) ? 2 : 8; }
 
 template <typename T>
 struct alignas(16) Pack16 {
@@ -92,7 +95,7 @@ struct alignas(16) Pack16 {
 };
 
 template <typename T, int kKind>
-__global__ void __launch_bounds__(kRThreads, (kKind == kSyr2G || kKind == kHer2G) ? 2 : 3)
+__global__ void __launch_bounds__(kRThreads, gcols<T, kKind>() < 8 ? 6 : (kKind == kSyr2G || kKind == kHer2G) ? 2 : 3)
 k_rank_g_vec(int m, int n, T alpha, const T* __restrict__ x, const T* __restrict__ y, size_t incy,
              T* __restrict__ A, size_t lda, bool lower) {
   using F = Fld<T>;
@@ -101,6 +104,7 @@ k_rank_g_vec(int m, int n, T alpha, const T* __restrict__ x, const T* __restrict
   constexpr bool kTri = kKind >= kSyrG;
   constexpr bool kHerm = kKind == kHerG || kKind == kHer2G;
   constexpr bool kTwo = kKind == kSyr2G || kKind == kHer2G;
+  constexpr int kGCols = gcols<T, kKind>();
   const int rows = kTri ? n : m;
   // rows [lo, hi) of column j that the update touches
   auto range = [&](int j, int& lo, int& hi) {
@@ -202,14 +206,13 @@ coral_status_t launch_rank_g(Handle* h, size_t m, size_t n, T alpha, const T* x,
   const size_t rows = kKind >= kSyrG ? n : m;
   constexpr bool kTwo = kKind == kSyr2G || kKind == kHer2G;
   // complex128 keeps the element kernel: with one element per 16-byte
-  // vector it already streams at 81-98% of HBM. So does CHER2, which
-  // measured 68% of HBM on the element kernel against 48% on this one
-  // (n = 8192, upper).
-  constexpr bool kVecOk = sizeof(T) < 16 && !(kKind == kHer2G && sizeof(T) == 8);
+  // vector it already streams at 81-98% of HBM.
+  constexpr bool kVecOk = sizeof(T) < 16;
   if constexpr (kVecOk) {  // the vector kernel is only instantiated where it is used
     if (incx == 1 && (!kTwo || incy == 1) && aligned16(A) && (lda * sizeof(T)) % 16 == 0 && aligned16(x) &&
         (!kTwo || aligned16(y))) {
       constexpr int kV = Pack16<T>::kV;
+      constexpr int kGCols = gcols<T, kKind>();
       const size_t groups = (n + kGCols - 1) / kGCols;
       const dim3 vgrid = kKind < kSyrG
           ? dim3((unsigned)((rows + (size_t)kV * kRThreads - 1) / ((size_t)kV * kRThreads)),
