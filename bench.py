@@ -723,7 +723,9 @@ def profile_case(torch, cb, case):
     `grouped` -- the 4096-instance batch of the batched configuration, bf16
     then fp32 inputs, two tensor-core grouped calls each; `native` -- SGEMM
     4096^3 NN and DGEMM 2048^3 NN on the TMA-fed FMA kernel, two calls each;
-    `split` -- SGEMM 4096^3 NN split-BF16x3, two calls."""
+    `split` -- SGEMM 4096^3 NN split-BF16x3, two calls; `paths` -- one call
+    of each kernel the benchmarked workloads never reach (beta-only scales,
+    strided level-1 fallbacks, rotation constructors, plain-load STRSV)."""
     h = cb.handle()
     if case == "grouped":
         rng = np.random.default_rng(2024)
@@ -772,6 +774,37 @@ def profile_case(torch, cb, case):
             cb.sgemm(0, 0, n, n, n, 1.5, A, n, B, n, 0.5, C, n)
         torch.cuda.synchronize()
         h.set_gemm_mode(cb.GemmMode.NATIVE)
+    elif case == "paths":
+        # the kernels the bench's own workloads never reach: the beta-only
+        # scales (native GEMM and GEMV with alpha = 0, the allocation-free
+        # SGEMM with alpha = 0), the strided level-1 fallbacks, the rotation
+        # constructors and the plain-load STRSV (lda not a multiple of 4)
+        import ctypes as C
+        lib = h.lib
+        h.bind_current_stream()
+        n = 4096
+        Cm = torch.empty(n * n, device="cuda").uniform_(-1, 1)
+        cb.sgemm(0, 0, n, n, n, 0.0, Cm, n, Cm, n, 0.5, Cm, n)
+        st = lib.coral_sgemm_bf16x3_noalloc(C.c_void_p(torch.cuda.current_stream().cuda_stream), 0, 0, n, n, n,
+                                           0.0, C.c_void_p(Cm.data_ptr()), n, C.c_void_p(Cm.data_ptr()), n,
+                                           0.5, C.c_void_p(Cm.data_ptr()), n)
+        assert st == 0, st
+        Ad = torch.empty(1 << 24, dtype=torch.float64, device="cuda").uniform_(-1, 1)   # 2^24 x 1
+        xd = torch.ones(1, dtype=torch.float64, device="cuda")
+        yd = torch.empty(1 << 24, dtype=torch.float64, device="cuda").uniform_(-1, 1)
+        cb.dgemv(0, 1 << 24, 1, 0.0, Ad, 1 << 24, xd, 1, 0.5, yd, 1)
+        x = torch.empty(1 << 25, device="cuda").uniform_(-1, 1)
+        y = torch.empty(1 << 24, device="cuda").uniform_(-1, 1)
+        cb.saxpy(1 << 24, 0.5, x, 2, y, 1)
+        cb.scopy(1 << 24, x, 2, y, 1)
+        cb.srotg(3.0, 4.0)
+        cb.srotmg(1.0, 2.0, 3.0, 4.0)
+        lda = n + 1
+        A = torch.empty(lda * n, device="cuda").uniform_(-1, 1)
+        A.view(n, lda)[:, :n].diagonal().add_(float(n))
+        b = torch.empty(n, device="cuda").uniform_(-1, 1)
+        cb.strsv(1, 0, 1, n, A, lda, b, 1)
+        torch.cuda.synchronize()
     print(json.dumps({"profile_case": case, "ok": True}))
 
 
@@ -1017,7 +1050,7 @@ def main():
     ap.add_argument("--only-precision", action="store_true", help="run and print the precision-GEMM set only")
     ap.add_argument("--only-batched", action="store_true", help="run and print the batched set only")
     ap.add_argument("--routines", default="", help="with --only-level12: comma list of routines to time")
-    ap.add_argument("--profile-case", choices=["grouped", "native", "split"], default="",
+    ap.add_argument("--profile-case", choices=["grouped", "native", "split", "paths"], default="",
                     help="run one small case for an ncu capture and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
