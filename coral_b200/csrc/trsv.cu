@@ -143,7 +143,8 @@ k_trsv(int n, const float* __restrict__ A, size_t lda, float* x, size_t incx, bo
   if (tid < kNB) rhs[tid] = (b0 + tid < n) ? x[(size_t)(b0 + tid) * incx] : 0.f;
   __syncthreads();
 
-  // ---- 2. panel: acc = sum over solved blocks k of op(A)(blk, k) x_k ----
+  // ---- 2. panel: acc = sum over solved blocks k of op(A)(blk, k) x_k, in
+  // solve order, so the blocks solved first are applied first ----
   const int r = tid % kNB, q = tid / kNB;
   float acc = 0.f;
   const int npanel = lower_eff ? blk : nblk - 1 - blk;
@@ -152,7 +153,7 @@ k_trsv(int n, const float* __restrict__ A, size_t lda, float* x, size_t incx, bo
 #pragma unroll
     for (int g = 0; g < kG; ++g) {
       const int idx = g0 + g;
-      const int k = lower_eff ? idx : blk + 1 + idx;
+      const int k = lower_eff ? idx : nblk - 1 - idx;  // solve order: earliest first
       // stored block: rows (trans ? k : blk), cols (trans ? blk : k)
       const int R0 = (trans ? k : blk) * kNB, C0 = (trans ? blk : k) * kNB;
 #pragma unroll
@@ -167,7 +168,7 @@ k_trsv(int n, const float* __restrict__ A, size_t lda, float* x, size_t incx, bo
     for (int g = 0; g < kG; ++g) {
       const int idx = g0 + g;
       if (idx >= npanel) break;
-      const int k = lower_eff ? idx : blk + 1 + idx;
+      const int k = lower_eff ? idx : nblk - 1 - idx;  // solve order: earliest first
 #pragma unroll
       for (int p = 0; p < kPer; ++p) {
         const int e = tid + p * kTrsvThreads;

@@ -2,9 +2,10 @@
 // {N, T, C} (dtrsv.rs, ctrsv.rs, ztrsv.rs -> the *trlsv / *trusv files).
 // Complex data is interleaved (re, im) with lda / incx in complex units.
 //
-// One launch, one 64-row block of the solve per CTA.  Each CTA takes a
-// ticket, so block b is handled by the b-th CTA to start in solve order and
-// only waits for CTAs that started earlier -- no deadlock whatever the
+// One launch, one 64-row block of the solve per CTA, in clusters of 16 CTAs
+// (8 where 16 cannot be placed).  Rank 0 of each cluster takes a ticket, so
+// the cluster with ticket t solves blocks 16 t .. 16 t + 15 in solve order and
+// only waits for clusters that started earlier -- no deadlock whatever the
 // scheduling.  A CTA
 //   1. stages its diagonal block of op(A) in shared memory (unstored triangle
 //      masked, unit diagonal applied, conjugated for op C), forms the
@@ -17,7 +18,10 @@
 //   3. solves the row-scaled system by forward (backward) substitution in
 //      one warp, fully unrolled (the diagonal block is never inverted: FP64
 //      substitution as the reference does, dtrlsv.rs);
-//   4. writes x_b over b and publishes it in its slots.
+//   4. writes x_b over b, pushes it into the shared memory of the later CTAs
+//      of its cluster (the next block's first) and publishes it in its slots
+//      for later clusters: within a cluster a block's solution reaches the
+//      next one through distributed shared memory instead of an L2 round trip.
 // Slots: every 32-bit word of a block's solution is published as one 64-bit
 // slot (epoch << 32) | word, so a single load delivers both the readiness of
 // that word and its value (aligned 64-bit accesses are single-copy atomic):
@@ -26,6 +30,7 @@
 // after the handle's wait limit and set the status word.
 #include "common.cuh"
 #include "field.cuh"
+#include "tc_common.cuh"
 
 #include <type_traits>
 
@@ -53,6 +58,23 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+// Cluster shared-memory accesses: a 32-bit load from another CTA's shared
+// memory, a 64-bit store into it, and a 64-bit load of this CTA's shared
+// memory that observes those stores.
+__device__ __forceinline__ unsigned ld_cluster_u32(uint32_t addr) {
+  unsigned v;
+  asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_cluster_u64(uint32_t addr, unsigned long long v) {
+  asm volatile("st.relaxed.cluster.shared::cluster.u64 [%0], %1;" ::"r"(addr), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_local_tag(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.cluster.shared::cta.u64 %0, [%1];" : "=l"(v) : "r"(tc::smem_u32(p)) : "memory");
+  return v;
+}
+constexpr int kDczClMax = 16;  // CTAs per cluster: 16, or 8 where 16 cannot be placed
 
 // 32-bit words per element (slots per element).
 template <typename T> constexpr int kWords = (int)(sizeof(T) / 4);
@@ -134,28 +156,51 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
          bool unit, unsigned long long* slots, unsigned* ticket, unsigned* done, unsigned* epoch_word,
          unsigned* status, uint64_t limit_ns) {
   using F = Fld<T>;
+  constexpr int W = kWords<T>;
+  constexpr int kSlotWords = kTB * W;   // slots per block (<= kTThr)
   extern __shared__ __align__(16) unsigned char smem[];
   T(*D)[kTB + 1] = reinterpret_cast<T(*)[kTB + 1]>(smem);   // op(A) diagonal block
+  // solutions pushed by the earlier CTAs of the cluster: xin[rank][word]
+  unsigned long long(*xin)[kSlotWords] =
+      reinterpret_cast<unsigned long long(*)[kSlotWords]>(smem + sizeof(T) * kTB * (kTB + 1));
   __shared__ T xk[kTB];        // solution of the block being applied
   __shared__ T rv[kTB];        // right-hand side, then this block's solution
   __shared__ T rdiag[kTB];     // reciprocals of the diagonal
-  __shared__ int sblk, abort_flag;
-  __shared__ unsigned sepoch;
+  __shared__ int abort_flag;
+  __shared__ unsigned sticket, sepoch, my_ticket, my_epoch;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nblk = (n + kTB - 1) / kTB;
+  const unsigned rank = tc::cluster_ctarank();
+  unsigned ncl_u;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(ncl_u));
+  const int ncl = (int)ncl_u;
+  for (int i = tid; i < ncl * kSlotWords; i += kTThr) (&xin[0][0])[i] = 0ull;
   if (tid == 0) {
-    const unsigned t = atomicAdd(ticket, 1u);
-    unsigned e = *(volatile unsigned*)epoch_word + 1u;
-    sepoch = e ? e : 1u;   // slots start at 0: never a live epoch
     abort_flag = 0;
-    sblk = lower_eff ? (int)t : nblk - 1 - (int)t;
+    if (rank == 0) {
+      // one ticket per cluster: the cluster takes the next ncl blocks in solve
+      // order, so it only ever waits for clusters that started earlier
+      sticket = atomicAdd(ticket, 1u);
+      const unsigned e = *(volatile unsigned*)epoch_word + 1u;
+      sepoch = e ? e : 1u;   // slots start at 0: never a live epoch
+    }
+  }
+  tc::cluster_sync();
+  if (tid == 0) {
+    my_ticket = ld_cluster_u32(tc::mapa_shared(tc::smem_u32(&sticket), 0));
+    my_epoch = ld_cluster_u32(tc::mapa_shared(tc::smem_u32(&sepoch), 0));
   }
   __syncthreads();
-  const unsigned epoch = sepoch;
-  const int blk = sblk;
+  const unsigned epoch = my_epoch;
+  const int s_first = (int)my_ticket * ncl;   // solve index of this cluster's rank 0
+  const int s = s_first + (int)rank;          // this CTA's solve index
+  const bool active = s < nblk;
+  auto blk_of = [&](int sp) { return lower_eff ? sp : nblk - 1 - sp; };
+  const int blk = active ? blk_of(s) : 0;
   const int b0 = blk * kTB;
   auto opv = [](T v) { return kConj ? F::conj(v) : v; };
 
+  if (active) {
   // ---- 1. diagonal block, its reciprocals, the row scaling; right-hand side ----
   for (int e = tid; e < kTB * kTB; e += kTThr) {
     const int rr = e % kTB, cc = e / kTB;          // stored element (b0 + rr, b0 + cc)
@@ -176,17 +221,16 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
     if (r != c) D[r][c] = F::neg(F::mul(D[r][c], rdiag[r]));
   }
 
-  // ---- 2. panel: acc(r) = sum over earlier blocks k of op(A)(b, k) x_k ----
-  constexpr int W = kWords<T>;
-  constexpr int kSlotWords = kTB * W;   // slots per block (<= kTThr)
+  // ---- 2. panel: acc(r) = sum over earlier blocks k of op(A)(b, k) x_k,
+  // in solve order; a block of this cluster is read from the copy its CTA
+  // pushed into this CTA's shared memory, an earlier cluster's from its slots
   constexpr int kQ = kTB / 4;           // columns per thread of a panel tile
   static_assert(kSlotWords <= kTThr, "one slot per thread");
   uint32_t* xkw = reinterpret_cast<uint32_t*>(xk);
   const int r = tid >> 2, q = tid & 3;
   T acc = F::zero();
-  const int npanel = lower_eff ? blk : nblk - 1 - blk;
-  for (int idx = 0; idx < npanel; ++idx) {
-    const int k = lower_eff ? idx : blk + 1 + idx;
+  for (int idx = 0; idx < s; ++idx) {
+    const int k = blk_of(idx);
     const int k0 = k * kTB;
     T a[kQ];
 #pragma unroll
@@ -196,12 +240,13 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
       a[j] = in ? opv(trans ? A[gc + (size_t)gr * lda] : A[gr + (size_t)gc * lda]) : F::zero();
     }
     if (tid < kSlotWords) {
-      const unsigned long long* sp = slots + (size_t)k * kSlotWords + tid;
-      unsigned long long w = ld_relaxed_u64(sp);
+      const bool local = idx >= s_first;
+      const unsigned long long* sp = local ? &xin[idx - s_first][tid] : slots + (size_t)k * kSlotWords + tid;
+      unsigned long long w = local ? ld_local_tag(sp) : ld_relaxed_u64(sp);
       if ((unsigned)(w >> 32) != epoch) {
         const uint64_t t0 = gtime();
         for (unsigned spins = 1;; ++spins) {
-          w = ld_relaxed_u64(sp);
+          w = local ? ld_local_tag(sp) : ld_relaxed_u64(sp);
           if ((unsigned)(w >> 32) == epoch) break;
           const uint64_t el = gtime() - t0;
           if (el > limit_ns || ((spins & 15u) == 0 && el > 20000ull && *(volatile unsigned*)status != 0)) {
@@ -250,18 +295,29 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
   }
   __syncthreads();
 
-  // ---- 4. publish: x_b over b, and every word of it in the block's slots ----
+  // ---- 4. publish: x_b over b, every word of it into the shared memory of
+  // the later CTAs of the cluster (the next one first) and into the block's
+  // slots for later clusters ----
   if (!abort_flag) {
     if (tid < kTB && b0 + tid < n) x[(size_t)(b0 + tid) * incx] = rv[tid];
-    if (tid < kSlotWords)
-      st_relaxed_u64(slots + (size_t)blk * kSlotWords + tid,
-                     ((unsigned long long)epoch << 32) | reinterpret_cast<const uint32_t*>(rv)[tid]);
+    if (tid < kSlotWords) {
+      const unsigned long long val =
+          ((unsigned long long)epoch << 32) | reinterpret_cast<const uint32_t*>(rv)[tid];
+      const uint32_t mine = tc::smem_u32(&xin[rank][tid]);
+      for (int d = (int)rank + 1; d < ncl && s_first + d < nblk; ++d)
+        st_cluster_u64(tc::mapa_shared(mine, (uint32_t)d), val);
+      st_relaxed_u64(slots + (size_t)blk * kSlotWords + tid, val);
+    }
   }
+  }  // active
+  // No CTA leaves while a CTA of its cluster may still push into it.
+  __syncthreads();
+  tc::cluster_sync();
   // The last CTA to finish (aborted or not) resets the ticket counter and
   // publishes this call's epoch for the next call.
   if (tid == 0) {
     __threadfence();
-    if (atomicAdd(done, 1u) == (unsigned)nblk - 1) {
+    if (atomicAdd(done, 1u) == gridDim.x - 1) {
       *ticket = 0u;
       *done = 0u;
       __threadfence();
@@ -301,26 +357,55 @@ coral_status_t trsv_g(Handle* H, int uplo, int trans, int diag, size_t n, const 
   const bool t = trans != CORAL_NO_TRANSPOSE;
   const bool cj = trans == CORAL_CONJ_TRANSPOSE && !std::is_same<T, double>::value;
   const bool lower_eff = (uplo == CORAL_LOWER) != t;
-  const size_t smem = (size_t)kTB * (kTB + 1) * sizeof(T);
-  static uint64_t attr_devices[2] = {0, 0};
-  const uint64_t bit = H->device < 64 ? (1ull << H->device) : 0;
-  if (!(attr_devices[cj] & bit) || !bit) {
-    if (cj)
-      CORAL_CUDA(H, cudaFuncSetAttribute(k_trsv_g<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    else
-      CORAL_CUDA(H, cudaFuncSetAttribute(k_trsv_g<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_devices[cj] |= bit;
+  const size_t smem = (size_t)kTB * (kTB + 1) * sizeof(T) + (size_t)kDczClMax * kTB * kWords<T> * 8;
+  // per device and kernel form: the attributes are set, and the cluster size
+  // (16 where the hardware places it, else 8) is chosen, on the first call
+  static int cluster_size[2][64] = {{0}};
+  int& cl = cluster_size[cj][H->device < 64 ? H->device : 63];
+  auto kern = cj ? k_trsv_g<T, true> : k_trsv_g<T, false>;
+  if (cl == 0) {
+    CORAL_CUDA(H, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int c = 8;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+      cudaLaunchConfig_t q = {};
+      cudaLaunchAttribute qa[1];
+      qa[0].id = cudaLaunchAttributeClusterDimension;
+      qa[0].val.clusterDim.x = 16;
+      qa[0].val.clusterDim.y = qa[0].val.clusterDim.z = 1;
+      q.gridDim = dim3(16);
+      q.blockDim = dim3(kTThr);
+      q.dynamicSmemBytes = smem;
+      q.attrs = qa;
+      q.numAttrs = 1;
+      int activec = 0;
+      if (cudaOccupancyMaxActiveClusters(&activec, kern, &q) == cudaSuccess && activec >= 1) c = 16;
+    }
+    cudaGetLastError();  // a refused query leaves the size at 8, not an error
+    cl = c;
   }
   T* X = static_cast<T*>(x);
   const T* Am = static_cast<const T*>(matrix);
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)cl;
+  at[0].val.clusterDim.y = at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3((unsigned)(((nblk + cl - 1) / cl) * cl));
+  cfg.blockDim = dim3(kTThr);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = H->stream;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
   timed_begin(H);
-#define CORAL_TRSV_G(CJ)                                                                                \
-  k_trsv_g<T, CJ><<<(unsigned)nblk, kTThr, smem, H->stream>>>(                                          \
-      (int)n, Am, lda, X, incx, lower_eff, t, diag == CORAL_UNIT, H->trsv_slots, &H->words->trsv_ticket, \
-      &H->words->trsv_done, &H->words->trsv_epoch, &H->words->status, H->wait_limit * 32ull)
-  if (cj) CORAL_TRSV_G(true);
-  else CORAL_TRSV_G(false);
-#undef CORAL_TRSV_G
+  const cudaError_t le = cudaLaunchKernelEx(&cfg, kern, (int)n, Am, lda, X, incx, lower_eff, t, diag == CORAL_UNIT,
+                                            H->trsv_slots, &H->words->trsv_ticket, &H->words->trsv_done,
+                                            &H->words->trsv_epoch, &H->words->status, H->wait_limit * 32ull);
+  if (le != cudaSuccess) {
+    timed_end(H);
+    count_launch();
+    cudaGetLastError();
+    return cuda_status(H, le);
+  }
   coral_status_t s = launch_status(H);
   timed_end(H);
   return s;
