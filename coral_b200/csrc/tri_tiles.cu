@@ -318,6 +318,9 @@ k_tri_strips(int n, const T* __restrict__ A, size_t lda, const T* __restrict__ x
   const int row_hi = lower ? n : c0;
   const int s_lo = row_lo / kS;
   const int s_hi = row_hi > row_lo ? (row_hi + kS - 1) / kS : s_lo;
+  // A CTA past its column's last strip leaves at once: it writes no partial
+  // (the combine reads only the splits that hold strips).
+  if (s_lo + (int)blockIdx.y * kStripWarps >= s_hi) return;
   if (threadIdx.x < kC) {
     const int gc = c0 + threadIdx.x;
     T v = gc < n ? x[(size_t)gc * incx] : Cx<T>::zero();
@@ -799,7 +802,16 @@ k_strip_combine(int n, T beta, T* __restrict__ y, size_t incy, bool lower,
     // stored strip [q_lo, q_hi) of the block, its diagonal block included
     // (k_tri_strips_tma, nsplit = strips)
     int q_lo = 0, q_hi = nsplit;
-    if (folded) strip_range_fold(Jr, n, kS, lower, q_lo, q_hi);
+    if (folded) {
+      strip_range_fold(Jr, n, kS, lower, q_lo, q_hi);
+    } else {
+      // the splits of column block Jr that hold strips (k_tri_strips)
+      const int c0 = Jr * kC;
+      const int row_lo = lower ? c0 + kC : 0, row_hi = lower ? n : c0;
+      const int s_lo = row_lo / kS;
+      const int s_hi = row_hi > row_lo ? (row_hi + kS - 1) / kS : s_lo;
+      q_hi = min(nsplit, (s_hi - s_lo + kStripWarps - 1) / kStripWarps);
+    }
     const T* cp = colpart + (size_t)Jr * nsplit * kC + gr % kC;
     for (int qb = q_lo + g; qb < q_hi; qb += kCombineBatch * kCombineGroups) {
       T a[kCombineBatch];
