@@ -237,15 +237,15 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
     // q + 4 j when it is read transposed, where the 4 threads of a row then
     // read 4 consecutive elements of one stored column (measured: DTRSV T
     // 221 -> 134-140 us, CTRSV T 221 -> 146-153, ZTRSV T 274 -> 204-216 at
-    // n = 4096).  The conjugated forms keep the first order, under which they
-    // measured faster (CTRSV C 243 against 345 us, ZTRSV C 355 against 590).
-    const bool tcols = trans && !kConj;
+    // n = 4096).  The tile is held as stored; the conjugation of op C is
+    // applied where an element is used.
+    const bool tcols = trans;
     T a[kQ];
 #pragma unroll
     for (int j = 0; j < kQ; ++j) {
       const int gr = b0 + r, gc = k0 + (tcols ? q + 4 * j : q * kQ + j);   // op(A)(gr, gc)
       const bool in = gr < n && gc < n;
-      a[j] = in ? opv(trans ? A[gc + (size_t)gr * lda] : A[gr + (size_t)gc * lda]) : F::zero();
+      a[j] = in ? (trans ? A[gc + (size_t)gr * lda] : A[gr + (size_t)gc * lda]) : F::zero();
     }
     if (tid < kSlotWords) {
       const bool local = idx >= s_first;
@@ -269,7 +269,7 @@ k_trsv_g(int n, const T* __restrict__ A, size_t lda, T* x, size_t incx, bool low
     __syncthreads();
     if (abort_flag) break;
 #pragma unroll
-    for (int j = 0; j < kQ; ++j) F::mac(acc, a[j], xk[tcols ? q + 4 * j : q * kQ + j]);
+    for (int j = 0; j < kQ; ++j) F::mac(acc, opv(a[j]), xk[tcols ? q + 4 * j : q * kQ + j]);
     __syncthreads();
   }
   acc = F::add(acc, F::shfl_xor(acc, 1));
