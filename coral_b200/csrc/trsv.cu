@@ -365,6 +365,8 @@ __device__ __forceinline__ bool fetch_x(const unsigned long long* src, bool loca
     }
     const bool ok = (unsigned)(v0 >> 32) == epoch && (unsigned)(v1 >> 32) == epoch;
     if (__all_sync(0xffffffffu, ok)) break;
+    // the timer is read on every 4th poll only, so a healthy poll stays short
+    if ((spins & 3u) != 0) continue;
     const uint64_t now = tc::globaltimer();
     if (spins == 0) {
       t0 = now;
@@ -382,6 +384,14 @@ __device__ __forceinline__ bool fetch_x(const unsigned long long* src, bool loca
 #pragma unroll
   for (int j = 0; j < 16; ++j) xv[j] = __shfl_sync(0xffffffffu, (j & 1) ? f1 : f0, base + (j >> 1));
   return true;
+}
+
+// Sum of m[j] * x[j], j < 16, over four independent chains.
+__device__ __forceinline__ float dot16(const float (&m)[16], const float (&x)[16]) {
+  float a[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int j = 0; j < 16; ++j) a[j & 3] = fmaf(m[j], x[j], a[j & 3]);
+  return (a[0] + a[1]) + (a[2] + a[3]);
 }
 
 // Column `col` of X = inv(L) B for the 64 x 64 lower-triangular L in Dm
@@ -745,20 +755,14 @@ k_trsv_cluster(const __grid_constant__ CUtensorMap amap, int n, float* x, size_t
       const bool local = (int)rank >= 2;
       const unsigned long long* src = local ? &S.xin[rank - 2][0] : slots + (size_t)(s - 2) * kCB;
       bool got = ok && fetch_x(src, local, epoch, lane, xv, status, &S.abort_flag, limit_ns);
-      float d = 0.f;
-#pragma unroll
-      for (int j = 0; j < 16; ++j) d = fmaf(M2[j], xv[j], d);
-      y -= quad_sum(d);
+      y -= quad_sum(dot16(M2, xv));
       ok = __all_sync(0xffffffffu, got);
     }
     if (s >= 1) {
       const bool local = (int)rank >= 1;
       const unsigned long long* src = local ? &S.xin[rank - 1][0] : slots + (size_t)(s - 1) * kCB;
       bool got = ok && fetch_x(src, local, epoch, lane, xv, status, &S.abort_flag, limit_ns);
-      float d = 0.f;
-#pragma unroll
-      for (int j = 0; j < 16; ++j) d = fmaf(M1[j], xv[j], d);
-      y -= quad_sum(d);
+      y -= quad_sum(dot16(M1, xv));
       ok = __all_sync(0xffffffffu, got);
     }
     if (ok) {
