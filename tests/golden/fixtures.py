@@ -294,3 +294,204 @@ def rot_cs(case):
     real = np.float32 if case["kind"] in "sc" else np.float64
     t = real(case["theta"])
     return real(np.cos(t)), real(np.sin(t))
+
+
+# ---- symmetric / Hermitian matrix-vector (ssymv_tests.rs, chemv_tests.rs) ----
+def _sym_fill(n, lda, f, stored=None, garbage=np.nan, dt=np.float32):
+    """Column-major n x n buffer: f(lo, hi) on the stored triangle, mirrored
+    (or NaN garbage in the other triangle when `stored` is 'U' or 'L')."""
+    a = np.zeros(lda * n, dt)
+    for j in range(n):
+        i = np.arange(n)
+        lo = np.minimum(i, j).astype(np.float32)
+        hi = np.maximum(i, j).astype(np.float32)
+        col = f(lo, hi, i == j).astype(dt)
+        if stored == "U":
+            col = np.where(i <= j, col, dt(garbage))
+        elif stored == "L":
+            col = np.where(i >= j, col, dt(garbage))
+        a[j * lda:j * lda + n] = col
+    return a
+
+
+def symv_matrix(n, lda):
+    """ssymv_tests.rs:44-60 make_symmetric_col_major."""
+    return _sym_fill(n, lda, lambda lo, hi, d: f32(0.1) + f32(0.5) * lo + f32(0.25) * hi)
+
+
+SYMV_COEFFS = [(1.0, 0.0), (0.0, 0.7), (0.75, -0.25), (-0.6, 0.4), (1.1, 0.0), (0.85, 0.1)]  # ssymv_tests.rs:209-216
+# (n, lda, [(incx, incy)]): ssymv_tests.rs:227-245
+SYMV_SHAPES = [(6, 6, [(1, 1)]), (768, 768, [(1, 1)]), (300, 305, [(1, 1)]),
+               (640, 640, [(2, 3), (3, 2), (2, 1)])]
+
+
+def symv_garbage_cases():
+    """ssymv_tests.rs:287-378: one triangle stored, NaN in the other.
+    (uplo, n, lda, alpha, beta, a, x, y)."""
+    up = _sym_fill(200, 203, lambda lo, hi, d: f32(0.2) + f32(0.3) * lo + f32(0.15) * hi, "U")
+    lw = _sym_fill(180, 180, lambda lo, hi, d: f32(0.17) + f32(0.45) * lo + f32(0.08) * hi, "L")
+    return [
+        (0, 200, 203, 0.7, 0.25, up, strided(200, 1, lambda k: f32(0.03) * k - f32(0.5)),
+         strided(200, 1, lambda k: f32(-0.1) + f32(0.002) * k)),
+        (1, 180, 180, -0.9, 0.6, lw, strided(180, 1, lambda k: f32(0.2) - f32(0.001) * k),
+         strided(180, 1, lambda k: f32(0.15) + f32(0.004) * k)),
+    ]
+
+
+def cstrided(length: int, inc: int, fre, fim) -> np.ndarray:
+    """chemv_tests.rs:135-152 make_strided_cvec, as complex64."""
+    v = np.zeros((length - 1) * inc + 1, np.complex64)
+    k = np.arange(length).astype(np.float32)
+    v[np.arange(length) * inc] = fre(k).astype(np.float32) + 1j * fim(k).astype(np.float32)
+    return v
+
+
+def _herm(n, lda, fre, fim, stored=None):
+    """Column-major complex64 n x n buffer with re = fre(lo, hi) and
+    im = fim(lo, hi) (0 on the diagonal).  stored None: full Hermitian
+    matrix, (re, im) on and above the diagonal and (re, -im) below
+    (chemv_tests.rs:47-73); 'U' / 'L': only that triangle holds (re, im),
+    the other NaN (chemv_tests.rs:76-133)."""
+    a = np.zeros(lda * n, np.complex64)
+    for j in range(n):
+        i = np.arange(n)
+        lo = np.minimum(i, j).astype(np.float32)
+        hi = np.maximum(i, j).astype(np.float32)
+        re = np.asarray(fre(lo, hi), np.float32)
+        im = np.where(i == j, f32(0.0), np.asarray(fim(lo, hi), np.float32)).astype(np.float32)
+        if stored is None:
+            im = np.where(i <= j, im, -im)
+        val = np.empty(n, np.complex64)
+        val.real, val.imag = re, im
+        if stored == "U":
+            val[i > j] = np.complex64(complex(np.nan, np.nan))
+        elif stored == "L":
+            val[i < j] = np.complex64(complex(np.nan, np.nan))
+        a[j * lda:j * lda + n] = val
+    return a
+
+
+def hemv_matrix(n, lda):
+    """chemv_tests.rs:47-73 make_hermitian_col_major: upper (i <= j) holds
+    (re, im), lower holds (re, -im)."""
+    return _herm(n, lda, lambda lo, hi: f32(0.10) + f32(0.25) * lo + f32(0.15) * hi,
+                 lambda lo, hi: f32(0.04) + f32(0.02) * (hi - lo))
+
+
+# chemv_tests.rs:262-269 as (alpha, beta)
+HEMV_COEFFS = [(1.0 + 0j, 0j), (0j, 0.7 - 0.1j), (0.75 - 0.10j, -0.25 + 0.15j), (-0.6 + 0.2j, 0.4 - 0.1j),
+               (1.25 + 0j, -0.5 + 0j), (0.85 - 0.1j, 0.1 + 0.05j)]
+# (n, lda, [(incx, incy)]): chemv_tests.rs:281-299
+HEMV_SHAPES = [(6, 6, [(1, 1)]), (640, 640, [(1, 1)]), (300, 305, [(1, 1)]),
+               (384, 384, [(2, 3), (3, 2), (2, 1)])]
+
+
+def hemv_x(length, inc):
+    return cstrided(length, inc, lambda k: f32(0.2) + f32(0.1) * k, lambda k: f32(-0.3) + f32(0.05) * k)
+
+
+def hemv_y(length, inc):
+    return cstrided(length, inc, lambda k: f32(-0.3) + f32(0.05) * k, lambda k: f32(0.1) - f32(0.02) * k)
+
+
+def hemv_garbage_cases():
+    """chemv_tests.rs:360-478: one triangle stored, NaN in the other.
+    (uplo, n, lda, alpha, beta, a, x, y)."""
+    up = _herm(200, 203, lambda lo, hi: f32(0.20) + f32(0.30) * lo + f32(0.15) * hi,
+               lambda lo, hi: f32(0.05) + f32(0.01) * (hi - lo), "U")
+    lw = _herm(180, 180, lambda lo, hi: f32(0.17) + f32(0.45) * lo + f32(0.08) * hi,
+               lambda lo, hi: f32(-0.03) - f32(0.02) * (hi - lo), "L")
+    return [
+        (0, 200, 203, 0.7 + 0.1j, 0.25 - 0.05j, up,
+         cstrided(200, 1, lambda k: f32(0.03) * k - f32(0.5), lambda k: f32(0.02) - f32(0.01) * k),
+         cstrided(200, 1, lambda k: f32(-0.1) + f32(0.002) * k, lambda k: f32(0.05) - f32(0.003) * k)),
+        (1, 180, 180, -0.9 + 0.2j, 0.6 - 0.1j, lw,
+         cstrided(180, 1, lambda k: f32(0.2) - f32(0.001) * k, lambda k: f32(-0.03) + f32(0.004) * k),
+         cstrided(180, 1, lambda k: f32(0.15) + f32(0.004) * k, lambda k: f32(-0.02) + f32(0.003) * k)),
+    ]
+
+
+# ---- strmv_tests.rs:61-160, 200-240 ------------------------------------------
+def trmv_matrix(n, lda, uplo, diag):
+    """build_matrix: make_upper / make_lower, with a deliberately wrong
+    diagonal when diag is unit (CORAL diag 0) so that it must be ignored."""
+    a = np.zeros(lda * n, np.float32)
+    for j in range(n):
+        i = np.arange(n).astype(np.float32)
+        if uplo == 0:
+            col = f32(0.2) + i * f32(0.3) + f32(j) * f32(0.15)
+            rows = np.arange(n) <= j
+        else:
+            col = f32(-0.1) + i * f32(0.25) - f32(j) * f32(0.2)
+            rows = np.arange(n) >= j
+        a[j * lda:j * lda + n] = np.where(rows, col, f32(0.0))
+    if diag == 0:
+        for i in range(n):
+            a[i + i * lda] = (f32(7.5) + f32(i) * f32(0.1)) if uplo == 0 else (f32(-9.0) + f32(i) * f32(0.05))
+    return a
+
+
+def trmv_x(n, inc):
+    return strided(n, inc, lambda k: f32(0.1) + f32(0.2) * k)
+
+
+# (n, lda, incs): strmv_tests.rs:226-240 (trans N, T and C; C is T for real data)
+TRMV_SHAPES = [(7, 7, [1]), (1024, 1024, [1]), (640, 640, [2, 3])]
+
+
+# ---- sger_tests.rs, ssyr_tests.rs, ssyr2_tests.rs ------------------------------
+def ger_matrix(m, n, lda):
+    """sger_tests.rs:33-48 make_matrix (the same ramp as sgemv's)."""
+    return colmajor(m, n, lda, lambda i, j: f32(0.1) + i * f32(0.5) + j * f32(0.25))
+
+
+# (m, n, lda, incx, incy, alpha, x ramp, y ramp): sger_tests.rs:128-231
+GER_CASES = [
+    (7, 5, 7, 1, 1, 1.25, (0.2, 0.1), (-0.1, 0.07)),
+    (1024, 768, 1024, 1, 1, -0.37, (0.05, 0.002), (0.4, -0.003)),
+    (512, 1024, 512, 1, 1, 0.93, (-0.2, 0.0015), (0.1, 0.0020)),
+    (9, 4, 12, 2, 3, -0.85, (0.05, 0.03), (0.4, -0.02)),
+    (300, 200, 305, 1, 1, 0.0, (0.11, 0.01), (0.07, -0.01)),
+]
+
+
+def syr_matrix(n, lda):
+    """ssyr_tests.rs:55-70 / ssyr2_tests.rs:57-72 make_symmetric_col_major."""
+    return _sym_fill(n, lda, lambda lo, hi, d: f32(0.1) + f32(0.5) * lo + f32(0.25) * hi)
+
+
+# (uplo, n, lda, incx, alpha, x ramp): ssyr_tests.rs:178-244
+SYR_CASES = [
+    (0, 7, 7, 1, 1.25, (0.2, 0.1)),
+    (1, 7, 7, 1, -0.8, (-0.3, 0.05)),
+    (0, 1024, 1024, 1, -0.37, (0.05, 0.002)),
+    (1, 512, 512, 1, 0.93, (-0.2, 0.0015)),
+    (1, 9, 12, 2, -0.85, (0.05, 0.03)),
+    (0, 300, 305, 1, 0.0, (0.11, 0.01)),
+]
+
+# (uplo, n, lda, incx, incy, alpha, x ramp, y ramp): ssyr2_tests.rs:178-245, 350-361
+SYR2_CASES = [
+    (0, 7, 7, 1, 1, 1.25, (0.2, 0.1), (-0.3, 0.05)),
+    (1, 7, 7, 1, 1, -0.8, (-0.2, 0.07), (0.4, -0.055)),
+    (0, 1024, 1024, 1, 1, -0.37, (0.05, 0.002), (0.4, -0.003)),
+    (1, 512, 512, 1, 1, 0.93, (-0.2, 0.0015), (0.1, 0.0020)),
+    (1, 9, 12, 2, 3, -0.85, (0.05, 0.03), (0.4, -0.02)),
+    (0, 300, 305, 1, 1, 0.0, (0.11, 0.01), (0.07, -0.01)),
+]
+
+
+def ramp32(n, inc, g):
+    """make_strided_vec with |k| g0 + g1 * k in f32."""
+    return strided(n, inc, lambda k: f32(g[0]) + f32(g[1]) * k)
+
+
+def sample_positions(rows, cols, count=4096, seed=0):
+    """Fixed (row, col) positions at which large rank-update results are
+    stored: every entry when the matrix has at most `count`, else a seeded
+    sample."""
+    if rows * cols <= count:
+        r, c = np.meshgrid(np.arange(rows), np.arange(cols), indexing="ij")
+        return r.ravel(), c.ravel()
+    rng = np.random.default_rng(seed + rows * 7919 + cols)
+    return rng.integers(0, rows, count), rng.integers(0, cols, count)

@@ -114,6 +114,60 @@ def main() -> None:
             g[f"rotg_{kind}{ci}"] = np.array([c, s], np.float64)
     for ci, (kind, d1, d2, x1, y1) in enumerate(fx.ROTMG_CASES):
         g[f"rotmg_c{ci}"] = np.asarray(getattr(blas, kind + "rotmg")(d1, d2, x1, y1), np.float64)
+    # ---- SSYMV / CHEMV (uplo 0 upper, 1 lower), all of y
+    for si, (n, lda, strides) in enumerate(fx.SYMV_SHAPES):
+        A = logical(fx.symv_matrix(n, lda), n, n, lda)
+        for (incx, incy) in strides:
+            x, y0 = fx.gemv_x(n, incx), fx.gemv_y(n, incy)
+            for uplo in (0, 1):
+                for ci, (alpha, beta) in enumerate(fx.SYMV_COEFFS):
+                    r = blas.ssymv(alpha, A, x, beta=beta, y=y0.copy(), incx=incx, incy=incy, lower=uplo)
+                    g[f"ssymv_s{si}_{incx}{incy}_u{uplo}_c{ci}"] = np.asarray(r, np.float32)[::incy][:n]
+    for ci, (uplo, n, lda, alpha, beta, a, x, y0) in enumerate(fx.symv_garbage_cases()):
+        r = blas.ssymv(alpha, logical(a, n, n, lda), x, beta=beta, y=y0.copy(), lower=uplo)
+        g[f"ssymv_tri{ci}"] = np.asarray(r, np.float32)
+    for si, (n, lda, strides) in enumerate(fx.HEMV_SHAPES):
+        A = logical(fx.hemv_matrix(n, lda), n, n, lda)
+        for (incx, incy) in strides:
+            x, y0 = fx.hemv_x(n, incx), fx.hemv_y(n, incy)
+            for uplo in (0, 1):
+                for ci, (alpha, beta) in enumerate(fx.HEMV_COEFFS):
+                    r = blas.chemv(alpha, A, x, beta=beta, y=y0.copy(), incx=incx, incy=incy, lower=uplo)
+                    g[f"chemv_s{si}_{incx}{incy}_u{uplo}_c{ci}"] = np.asarray(r, np.complex64)[::incy][:n]
+    for ci, (uplo, n, lda, alpha, beta, a, x, y0) in enumerate(fx.hemv_garbage_cases()):
+        r = blas.chemv(alpha, logical(a, n, n, lda), x, beta=beta, y=y0.copy(), lower=uplo)
+        g[f"chemv_tri{ci}"] = np.asarray(r, np.complex64)
+    # ---- STRMV (trans 0 N, 1 T, 2 C; CORAL diag 0 = unit, 1 = non-unit)
+    for si, (n, lda, incs) in enumerate(fx.TRMV_SHAPES):
+        for uplo in (0, 1):
+            for diag in (0, 1):
+                A = logical(fx.trmv_matrix(n, lda, uplo, diag), n, n, lda)
+                for inc in incs:
+                    x = fx.trmv_x(n, inc)
+                    for trans in (0, 1, 2):
+                        r = blas.strmv(A, x.copy(), incx=inc, lower=uplo, trans=trans,
+                                       diag=1 if diag == 0 else 0)
+                        g[f"strmv_s{si}_u{uplo}_i{inc}_t{trans}_d{diag}"] = np.asarray(r, np.float32)[::inc][:n]
+    # ---- SGER / SSYR / SSYR2: the logical matrix at fixed positions
+    for ci, (m, n, lda, incx, incy, alpha, gx, gy) in enumerate(fx.GER_CASES):
+        A = logical(fx.ger_matrix(m, n, lda), m, n, lda)
+        x, y = fx.ramp32(m, incx, gx)[::incx], fx.ramp32(n, incy, gy)[::incy]
+        r = np.asarray(blas.sger(alpha, x, y, a=A.copy()), np.float32)
+        ri, cj = fx.sample_positions(m, n)
+        g[f"sger_c{ci}"] = r[ri, cj]
+    for ci, (uplo, n, lda, incx, alpha, gx) in enumerate(fx.SYR_CASES):
+        A = logical(fx.syr_matrix(n, lda), n, n, lda)
+        x = fx.ramp32(n, incx, gx)
+        r = np.asarray(blas.ssyr(alpha, x, lower=uplo, incx=incx, n=n, a=A.copy()), np.float32)
+        ri, cj = fx.sample_positions(n, n)
+        g[f"ssyr_c{ci}"] = r[ri, cj]
+    for ci, (uplo, n, lda, incx, incy, alpha, gx, gy) in enumerate(fx.SYR2_CASES):
+        A = logical(fx.syr_matrix(n, lda), n, n, lda)
+        x, y = fx.ramp32(n, incx, gx), fx.ramp32(n, incy, gy)
+        r = np.asarray(blas.ssyr2(alpha, x, y, lower=uplo, incx=incx, incy=incy, n=n, a=A.copy()),
+                       np.float32)
+        ri, cj = fx.sample_positions(n, n)
+        g[f"ssyr2_c{ci}"] = r[ri, cj]
     np.savez_compressed(OUT, **g)
     print(f"wrote {len(g)} arrays to {OUT} ({os.path.getsize(OUT)} bytes)")
 

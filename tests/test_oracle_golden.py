@@ -3,8 +3,9 @@
 Known answers: the sgemm and cgemm doctests (coral-aarch64/src/level3/
 sgemm.rs:36-81, cgemm.rs:36-96) and the planted-maximum isamax cases
 (tests/level1/iamax_tests.rs:79-170).  Fixtures: the closed-form cases of
-tests/level3/sgemm_tests.rs, tests/level2/sgemv_tests.rs and
-tests/level2/strsv_tests.rs, whose expected outputs were computed by
+tests/level3/sgemm_tests.rs, tests/level2/{sgemv,ssymv,chemv,strsv,strmv,
+sger,ssyr,ssyr2}_tests.rs and the level-1 tests, whose expected outputs were
+computed by
 CBLAS-class BLAS (tests/golden/make_golden.py) and are checked here with the
 reference's own tolerances.
 """
@@ -245,3 +246,139 @@ def test_l1_dcz_rounding_paths():
     xo, yo = oracle.rotm("d", 5, xd, 1, yd, 1, [-2, 1, 2, 3, 4])
     np.testing.assert_array_equal(xo, xd)
     np.testing.assert_array_equal(yo, yd)
+
+
+# ---- symmetric / Hermitian matrix-vector, triangular multiply, rank updates ----
+def test_ssymv_fixtures(golden):
+    """ssymv_tests.rs:155-249: every shape, stride pair, uplo and (alpha,
+    beta) at the reference's 1e-5 / 1e-5 (ssymv_tests.rs:152-153)."""
+    from conftest import allclose_ref
+    for si, (n, lda, strides) in enumerate(fx.SYMV_SHAPES):
+        a = fx.symv_matrix(n, lda)
+        for (incx, incy) in strides:
+            x, y0 = fx.gemv_x(n, incx), fx.gemv_y(n, incy)
+            for uplo in (0, 1):
+                for ci, (alpha, beta) in enumerate(fx.SYMV_COEFFS):
+                    got = oracle.ssymv(uplo, n, alpha, a, lda, x, incx, beta, y0, incy)
+                    allclose_ref(got, golden[f"ssymv_s{si}_{incx}{incy}_u{uplo}_c{ci}"], 1e-5, 1e-5)
+
+
+def test_ssymv_reads_only_the_stored_triangle(golden):
+    """ssymv_tests.rs:287-378: NaN in the unstored triangle never reaches y."""
+    from conftest import allclose_ref
+    for ci, (uplo, n, lda, alpha, beta, a, x, y0) in enumerate(fx.symv_garbage_cases()):
+        got = oracle.ssymv(uplo, n, alpha, a, lda, x, 1, beta, y0, 1)
+        assert np.isfinite(got).all()
+        allclose_ref(got, golden[f"ssymv_tri{ci}"], 1e-5, 1e-5)
+
+
+def test_ssymv_upper_equals_lower():
+    """ssymv_tests.rs:251-285: on a full symmetric matrix both triangles give
+    the same y."""
+    from conftest import allclose_ref
+    n = 513
+    a = fx.symv_matrix(n, n)
+    x = fx.strided(n, 1, lambda k: fx.f32(-0.07) + fx.f32(0.013) * k)
+    y0 = fx.strided(n, 1, lambda k: fx.f32(0.02) - fx.f32(0.004) * k)
+    up = oracle.ssymv(0, n, 1.123, a, n, x, 1, -0.321, y0, 1)
+    lo = oracle.ssymv(1, n, 1.123, a, n, x, 1, -0.321, y0, 1)
+    allclose_ref(up, lo, 1e-5, 1e-5)
+
+
+def _pair(v):
+    return np.array([complex(v).real, complex(v).imag], np.float32)
+
+
+def test_chemv_fixtures(golden):
+    """chemv_tests.rs:194-299 at the reference's 1e-5 / 1e-6
+    (chemv_tests.rs:190-191), real and imaginary parts separately."""
+    from conftest import allclose_ref
+    for si, (n, lda, strides) in enumerate(fx.HEMV_SHAPES):
+        a = fx.hemv_matrix(n, lda).view(np.float32)
+        for (incx, incy) in strides:
+            x, y0 = fx.hemv_x(n, incx).view(np.float32), fx.hemv_y(n, incy).view(np.float32)
+            for uplo in (0, 1):
+                for ci, (alpha, beta) in enumerate(fx.HEMV_COEFFS):
+                    got = oracle.chemv(uplo, n, _pair(alpha), a, lda, x, incx, _pair(beta), y0, incy)
+                    want = golden[f"chemv_s{si}_{incx}{incy}_u{uplo}_c{ci}"].view(np.float32)
+                    allclose_ref(got, want, 1e-5, 1e-6)
+
+
+def test_chemv_reads_only_the_stored_triangle(golden):
+    """chemv_tests.rs:360-478: one triangle stored, NaN in the other."""
+    from conftest import allclose_ref
+    for ci, (uplo, n, lda, alpha, beta, a, x, y0) in enumerate(fx.hemv_garbage_cases()):
+        got = oracle.chemv(uplo, n, _pair(alpha), a.view(np.float32), lda, x.view(np.float32), 1,
+                           _pair(beta), y0.view(np.float32), 1)
+        assert np.isfinite(got).all()
+        allclose_ref(got, golden[f"chemv_tri{ci}"].view(np.float32), 1e-5, 1e-6)
+
+
+def test_strmv_fixtures(golden):
+    """strmv_tests.rs:161-240: both triangles, N/T/C, unit (with a planted
+    diagonal that must be ignored) and non-unit, at 1e-5 / 1e-5
+    (strmv_tests.rs:154-155)."""
+    from conftest import allclose_ref
+    for si, (n, lda, incs) in enumerate(fx.TRMV_SHAPES):
+        for uplo in (0, 1):
+            for diag in (0, 1):
+                a = fx.trmv_matrix(n, lda, uplo, diag)
+                for inc in incs:
+                    x = fx.trmv_x(n, inc)
+                    for trans in (0, 1, 2):
+                        got = oracle.strmv(uplo, trans, diag, n, a, lda, x, inc)
+                        allclose_ref(got, golden[f"strmv_s{si}_u{uplo}_i{inc}_t{trans}_d{diag}"],
+                                     1e-5, 1e-5)
+
+
+def _logical_at(buf, ld, rows, cols):
+    return buf[rows + cols * ld]
+
+
+def test_sger_fixtures(golden):
+    """sger_tests.rs:128-197 and the alpha = 0 quick return (:352-356) at
+    1e-6 / 1e-6 (sger_tests.rs:82-83); rows past m in each column of a
+    padded lda stay as they were."""
+    from conftest import allclose_ref
+    for ci, (m, n, lda, incx, incy, alpha, gx, gy) in enumerate(fx.GER_CASES):
+        a0 = fx.ger_matrix(m, n, lda)
+        got = oracle.sger(m, n, alpha, fx.ramp32(m, incx, gx), incx, fx.ramp32(n, incy, gy), incy, a0, lda)
+        ri, cj = fx.sample_positions(m, n)
+        allclose_ref(_logical_at(got, lda, ri, cj), golden[f"sger_c{ci}"], 1e-6, 1e-6)
+        pad = np.ones(lda * n, bool)
+        for j in range(n):
+            pad[j * lda:j * lda + m] = False
+        np.testing.assert_array_equal(got[pad], a0[pad])
+        if alpha == 0.0:
+            np.testing.assert_array_equal(got, a0)
+
+
+def _only_triangle_touched(got, a0, n, lda, uplo):
+    """ssyr_tests.rs:106-127: the other triangle keeps its bits."""
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    other = (i > j) if uplo == 0 else (i < j)
+    idx = (i + j * lda)[other]
+    np.testing.assert_array_equal(got[idx].view(np.uint32), a0[idx].view(np.uint32))
+
+
+def test_ssyr_fixtures(golden):
+    """ssyr_tests.rs:132-244 at 1e-6 / 1e-5 (ssyr_tests.rs:129-130), with
+    the untouched-triangle check of the small and padded cases."""
+    from conftest import allclose_ref
+    for ci, (uplo, n, lda, incx, alpha, gx) in enumerate(fx.SYR_CASES):
+        a0 = fx.syr_matrix(n, lda)
+        got = oracle.ssyr(uplo, n, alpha, fx.ramp32(n, incx, gx), incx, a0, lda)
+        ri, cj = fx.sample_positions(n, n)
+        allclose_ref(_logical_at(got, lda, ri, cj), golden[f"ssyr_c{ci}"], 1e-6, 1e-5)
+        _only_triangle_touched(got, a0, n, lda, uplo)
+
+
+def test_ssyr2_fixtures(golden):
+    """ssyr2_tests.rs:134-245, 350-361 at 1e-6 / 1e-5 (ssyr2_tests.rs:131-132)."""
+    from conftest import allclose_ref
+    for ci, (uplo, n, lda, incx, incy, alpha, gx, gy) in enumerate(fx.SYR2_CASES):
+        a0 = fx.syr_matrix(n, lda)
+        got = oracle.ssyr2(uplo, n, alpha, fx.ramp32(n, incx, gx), incx, fx.ramp32(n, incy, gy), incy, a0, lda)
+        ri, cj = fx.sample_positions(n, n)
+        allclose_ref(_logical_at(got, lda, ri, cj), golden[f"ssyr2_c{ci}"], 1e-6, 1e-5)
+        _only_triangle_touched(got, a0, n, lda, uplo)
