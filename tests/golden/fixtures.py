@@ -296,118 +296,154 @@ def rot_cs(case):
     return real(np.cos(t)), real(np.sin(t))
 
 
-# ---- symmetric / Hermitian matrix-vector (ssymv_tests.rs, chemv_tests.rs) ----
-def _sym_fill(n, lda, f, stored=None, garbage=np.nan, dt=np.float32):
-    """Column-major n x n buffer: f(lo, hi) on the stored triangle, mirrored
-    (or NaN garbage in the other triangle when `stored` is 'U' or 'L')."""
-    a = np.zeros(lda * n, dt)
+# ---- symmetric / Hermitian matrix-vector -------------------------------------
+# ssymv_tests.rs / dsymv_tests.rs and chemv_tests.rs / zhemv_tests.rs use the
+# same closed forms in their element precision; `kind` picks it.
+def _real(kind):
+    return np.float32 if kind in "sc" else np.float64
+
+
+def _sym_fill(n, lda, f, stored=None, kind="s"):
+    """Column-major n x n buffer: f(R, lo, hi) on the stored triangle,
+    mirrored (or NaN in the other triangle when `stored` is 'U' or 'L')."""
+    R = _real(kind)
+    a = np.zeros(lda * n, R)
     for j in range(n):
         i = np.arange(n)
-        lo = np.minimum(i, j).astype(np.float32)
-        hi = np.maximum(i, j).astype(np.float32)
-        col = f(lo, hi, i == j).astype(dt)
+        lo = np.minimum(i, j).astype(R)
+        hi = np.maximum(i, j).astype(R)
+        col = np.asarray(f(R, lo, hi), R)
         if stored == "U":
-            col = np.where(i <= j, col, dt(garbage))
+            col = np.where(i <= j, col, R(np.nan))
         elif stored == "L":
-            col = np.where(i >= j, col, dt(garbage))
+            col = np.where(i >= j, col, R(np.nan))
         a[j * lda:j * lda + n] = col
     return a
 
 
-def symv_matrix(n, lda):
-    """ssymv_tests.rs:44-60 make_symmetric_col_major."""
-    return _sym_fill(n, lda, lambda lo, hi, d: f32(0.1) + f32(0.5) * lo + f32(0.25) * hi)
+def symv_matrix(n, lda, kind="s"):
+    """ssymv_tests.rs:44-60 / dsymv_tests.rs:46-62 make_symmetric_col_major."""
+    return _sym_fill(n, lda, lambda R, lo, hi: R(0.1) + R(0.5) * lo + R(0.25) * hi, kind=kind)
 
 
 SYMV_COEFFS = [(1.0, 0.0), (0.0, 0.7), (0.75, -0.25), (-0.6, 0.4), (1.1, 0.0), (0.85, 0.1)]  # ssymv_tests.rs:209-216
-# (n, lda, [(incx, incy)]): ssymv_tests.rs:227-245
+# (n, lda, [(incx, incy)]): ssymv_tests.rs:227-245, dsymv_tests.rs:230-248
 SYMV_SHAPES = [(6, 6, [(1, 1)]), (768, 768, [(1, 1)]), (300, 305, [(1, 1)]),
                (640, 640, [(2, 3), (3, 2), (2, 1)])]
 
 
-def symv_garbage_cases():
-    """ssymv_tests.rs:287-378: one triangle stored, NaN in the other.
-    (uplo, n, lda, alpha, beta, a, x, y)."""
-    up = _sym_fill(200, 203, lambda lo, hi, d: f32(0.2) + f32(0.3) * lo + f32(0.15) * hi, "U")
-    lw = _sym_fill(180, 180, lambda lo, hi, d: f32(0.17) + f32(0.45) * lo + f32(0.08) * hi, "L")
+def rvec(kind, length, inc, g):
+    """make_strided_vec with |k| g(R, k) in the element precision."""
+    R = _real(kind)
+    v = np.zeros((length - 1) * inc + 1 if length else 1, R)
+    k = np.arange(length).astype(R)
+    v[np.arange(length) * inc] = np.asarray(g(R, k), R)
+    return v
+
+
+def symv_x(kind, n, inc):
+    return rvec(kind, n, inc, lambda R, k: R(0.2) + R(0.1) * k)
+
+
+def symv_y(kind, n, inc):
+    return rvec(kind, n, inc, lambda R, k: R(-0.3) + R(0.05) * k)
+
+
+def symv_garbage_cases(kind="s"):
+    """ssymv_tests.rs:287-378 / dsymv_tests.rs:294-378: one triangle stored,
+    NaN in the other.  (uplo, n, lda, alpha, beta, a, x, y)."""
+    up = _sym_fill(200, 203, lambda R, lo, hi: R(0.2) + R(0.3) * lo + R(0.15) * hi, "U", kind)
+    lw = _sym_fill(180, 180, lambda R, lo, hi: R(0.17) + R(0.45) * lo + R(0.08) * hi, "L", kind)
     return [
-        (0, 200, 203, 0.7, 0.25, up, strided(200, 1, lambda k: f32(0.03) * k - f32(0.5)),
-         strided(200, 1, lambda k: f32(-0.1) + f32(0.002) * k)),
-        (1, 180, 180, -0.9, 0.6, lw, strided(180, 1, lambda k: f32(0.2) - f32(0.001) * k),
-         strided(180, 1, lambda k: f32(0.15) + f32(0.004) * k)),
+        (0, 200, 203, 0.7, 0.25, up, rvec(kind, 200, 1, lambda R, k: R(0.03) * k - R(0.5)),
+         rvec(kind, 200, 1, lambda R, k: R(-0.1) + R(0.002) * k)),
+        (1, 180, 180, -0.9, 0.6, lw, rvec(kind, 180, 1, lambda R, k: R(0.2) - R(0.001) * k),
+         rvec(kind, 180, 1, lambda R, k: R(0.15) + R(0.004) * k)),
     ]
+
+
+def cvec(kind, length, inc, gre, gim):
+    """make_strided_cvec: element k is (gre(R, k), gim(R, k))."""
+    R = _real(kind)
+    v = np.zeros((length - 1) * inc + 1 if length else 1, _DT[kind])
+    k = np.arange(length).astype(R)
+    val = np.empty(length, _DT[kind])
+    val.real, val.imag = np.asarray(gre(R, k), R), np.asarray(gim(R, k), R)
+    v[np.arange(length) * inc] = val
+    return v
 
 
 def cstrided(length: int, inc: int, fre, fim) -> np.ndarray:
     """chemv_tests.rs:135-152 make_strided_cvec, as complex64."""
-    v = np.zeros((length - 1) * inc + 1, np.complex64)
-    k = np.arange(length).astype(np.float32)
-    v[np.arange(length) * inc] = fre(k).astype(np.float32) + 1j * fim(k).astype(np.float32)
-    return v
+    return cvec("c", length, inc, lambda R, k: fre(k), lambda R, k: fim(k))
 
 
-def _herm(n, lda, fre, fim, stored=None):
-    """Column-major complex64 n x n buffer with re = fre(lo, hi) and
-    im = fim(lo, hi) (0 on the diagonal).  stored None: full Hermitian
+def _herm(n, lda, fre, fim, stored=None, kind="c"):
+    """Column-major complex n x n buffer with re = fre(R, lo, hi) and
+    im = fim(R, lo, hi) (0 on the diagonal).  stored None: full Hermitian
     matrix, (re, im) on and above the diagonal and (re, -im) below
     (chemv_tests.rs:47-73); 'U' / 'L': only that triangle holds (re, im),
     the other NaN (chemv_tests.rs:76-133)."""
-    a = np.zeros(lda * n, np.complex64)
+    R = _real(kind)
+    a = np.zeros(lda * n, _DT[kind])
     for j in range(n):
         i = np.arange(n)
-        lo = np.minimum(i, j).astype(np.float32)
-        hi = np.maximum(i, j).astype(np.float32)
-        re = np.asarray(fre(lo, hi), np.float32)
-        im = np.where(i == j, f32(0.0), np.asarray(fim(lo, hi), np.float32)).astype(np.float32)
+        lo = np.minimum(i, j).astype(R)
+        hi = np.maximum(i, j).astype(R)
+        re = np.asarray(fre(R, lo, hi), R)
+        im = np.where(i == j, R(0.0), np.asarray(fim(R, lo, hi), R)).astype(R)
         if stored is None:
             im = np.where(i <= j, im, -im)
-        val = np.empty(n, np.complex64)
+        val = np.empty(n, _DT[kind])
         val.real, val.imag = re, im
         if stored == "U":
-            val[i > j] = np.complex64(complex(np.nan, np.nan))
+            val[i > j] = complex(np.nan, np.nan)
         elif stored == "L":
-            val[i < j] = np.complex64(complex(np.nan, np.nan))
+            val[i < j] = complex(np.nan, np.nan)
         a[j * lda:j * lda + n] = val
     return a
 
 
-def hemv_matrix(n, lda):
-    """chemv_tests.rs:47-73 make_hermitian_col_major: upper (i <= j) holds
-    (re, im), lower holds (re, -im)."""
-    return _herm(n, lda, lambda lo, hi: f32(0.10) + f32(0.25) * lo + f32(0.15) * hi,
-                 lambda lo, hi: f32(0.04) + f32(0.02) * (hi - lo))
+def hemv_matrix(n, lda, kind="c"):
+    """chemv_tests.rs:47-73 / zhemv_tests.rs:48-74 make_hermitian_col_major:
+    upper (i <= j) holds (re, im), lower holds (re, -im)."""
+    return _herm(n, lda, lambda R, lo, hi: R(0.10) + R(0.25) * lo + R(0.15) * hi,
+                 lambda R, lo, hi: R(0.04) + R(0.02) * (hi - lo), kind=kind)
 
 
 # chemv_tests.rs:262-269 as (alpha, beta)
 HEMV_COEFFS = [(1.0 + 0j, 0j), (0j, 0.7 - 0.1j), (0.75 - 0.10j, -0.25 + 0.15j), (-0.6 + 0.2j, 0.4 - 0.1j),
                (1.25 + 0j, -0.5 + 0j), (0.85 - 0.1j, 0.1 + 0.05j)]
-# (n, lda, [(incx, incy)]): chemv_tests.rs:281-299
+# zhemv_tests.rs:260-268
+ZHEMV_COEFFS = [(1.0 + 0j, 0j), (0j, -0.75 + 0.2j), (0.75 - 0.10j, -0.25 + 0.15j), (-0.6 + 0.2j, 0.4 - 0.1j),
+                (1.25 + 0j, -0.5 + 0j), (0.85 - 0.1j, 0.1 + 0.05j), (1.1 - 0.2j, 0j)]
+# (n, lda, [(incx, incy)]): chemv_tests.rs:281-299, zhemv_tests.rs:280-298
 HEMV_SHAPES = [(6, 6, [(1, 1)]), (640, 640, [(1, 1)]), (300, 305, [(1, 1)]),
                (384, 384, [(2, 3), (3, 2), (2, 1)])]
 
 
-def hemv_x(length, inc):
-    return cstrided(length, inc, lambda k: f32(0.2) + f32(0.1) * k, lambda k: f32(-0.3) + f32(0.05) * k)
+def hemv_x(length, inc, kind="c"):
+    return cvec(kind, length, inc, lambda R, k: R(0.2) + R(0.1) * k, lambda R, k: R(-0.3) + R(0.05) * k)
 
 
-def hemv_y(length, inc):
-    return cstrided(length, inc, lambda k: f32(-0.3) + f32(0.05) * k, lambda k: f32(0.1) - f32(0.02) * k)
+def hemv_y(length, inc, kind="c"):
+    return cvec(kind, length, inc, lambda R, k: R(-0.3) + R(0.05) * k, lambda R, k: R(0.1) - R(0.02) * k)
 
 
-def hemv_garbage_cases():
-    """chemv_tests.rs:360-478: one triangle stored, NaN in the other.
-    (uplo, n, lda, alpha, beta, a, x, y)."""
-    up = _herm(200, 203, lambda lo, hi: f32(0.20) + f32(0.30) * lo + f32(0.15) * hi,
-               lambda lo, hi: f32(0.05) + f32(0.01) * (hi - lo), "U")
-    lw = _herm(180, 180, lambda lo, hi: f32(0.17) + f32(0.45) * lo + f32(0.08) * hi,
-               lambda lo, hi: f32(-0.03) - f32(0.02) * (hi - lo), "L")
+def hemv_garbage_cases(kind="c"):
+    """chemv_tests.rs:360-478 / zhemv_tests.rs:361-478: one triangle stored,
+    NaN in the other.  (uplo, n, lda, alpha, beta, a, x, y)."""
+    up = _herm(200, 203, lambda R, lo, hi: R(0.20) + R(0.30) * lo + R(0.15) * hi,
+               lambda R, lo, hi: R(0.05) + R(0.01) * (hi - lo), "U", kind)
+    lw = _herm(180, 180, lambda R, lo, hi: R(0.17) + R(0.45) * lo + R(0.08) * hi,
+               lambda R, lo, hi: R(-0.03) - R(0.02) * (hi - lo), "L", kind)
     return [
         (0, 200, 203, 0.7 + 0.1j, 0.25 - 0.05j, up,
-         cstrided(200, 1, lambda k: f32(0.03) * k - f32(0.5), lambda k: f32(0.02) - f32(0.01) * k),
-         cstrided(200, 1, lambda k: f32(-0.1) + f32(0.002) * k, lambda k: f32(0.05) - f32(0.003) * k)),
+         cvec(kind, 200, 1, lambda R, k: R(0.03) * k - R(0.5), lambda R, k: R(0.02) - R(0.01) * k),
+         cvec(kind, 200, 1, lambda R, k: R(-0.1) + R(0.002) * k, lambda R, k: R(0.05) - R(0.003) * k)),
         (1, 180, 180, -0.9 + 0.2j, 0.6 - 0.1j, lw,
-         cstrided(180, 1, lambda k: f32(0.2) - f32(0.001) * k, lambda k: f32(-0.03) + f32(0.004) * k),
-         cstrided(180, 1, lambda k: f32(0.15) + f32(0.004) * k, lambda k: f32(-0.02) + f32(0.003) * k)),
+         cvec(kind, 180, 1, lambda R, k: R(0.2) - R(0.001) * k, lambda R, k: R(-0.03) + R(0.004) * k),
+         cvec(kind, 180, 1, lambda R, k: R(0.15) + R(0.004) * k, lambda R, k: R(-0.02) + R(0.003) * k)),
     ]
 
 
@@ -455,9 +491,9 @@ GER_CASES = [
 ]
 
 
-def syr_matrix(n, lda):
+def syr_matrix(n, lda, kind="s"):
     """ssyr_tests.rs:55-70 / ssyr2_tests.rs:57-72 make_symmetric_col_major."""
-    return _sym_fill(n, lda, lambda lo, hi, d: f32(0.1) + f32(0.5) * lo + f32(0.25) * hi)
+    return _sym_fill(n, lda, lambda R, lo, hi: R(0.1) + R(0.5) * lo + R(0.25) * hi, kind=kind)
 
 
 # (uplo, n, lda, incx, alpha, x ramp): ssyr_tests.rs:178-244
@@ -495,3 +531,178 @@ def sample_positions(rows, cols, count=4096, seed=0):
         return r.ravel(), c.ravel()
     rng = np.random.default_rng(seed + rows * 7919 + cols)
     return rng.integers(0, rows, count), rng.integers(0, cols, count)
+
+
+# ---- d/c/z matrix-vector: dgemv/cgemv/zgemv_tests.rs -------------------------
+def cm_k(kind, rows, cols, ld, fre, fim=None):
+    """Column-major buffer in the element precision: element (i, j) is
+    fre(R, i, j) (+ 1j * fim(R, i, j) for complex kinds)."""
+    R = _real(kind)
+    a = np.zeros(ld * cols, _DT[kind])
+    i = np.arange(rows).astype(R)
+    for j in range(cols):
+        jj = R(j)
+        if kind in "sd":
+            a[j * ld:j * ld + rows] = fre(R, i, jj)
+        else:
+            col = np.empty(rows, _DT[kind])
+            col.real, col.imag = fre(R, i, jj), fim(R, i, jj)
+            a[j * ld:j * ld + rows] = col
+    return a
+
+
+def gemv_matrix_k(kind, m, n, lda):
+    """dgemv_tests.rs:50-62; cgemv_tests.rs:48-63 / zgemv_tests.rs:51-66 add
+    im = -0.2 + 0.3 i - 0.15 j."""
+    return cm_k(kind, m, n, lda, lambda R, i, j: R(0.1) + i * R(0.5) + j * R(0.25),
+                lambda R, i, j: R(-0.2) + i * R(0.3) - j * R(0.15))
+
+
+def gemv_x_k(kind, length, inc):
+    if kind in "sd":
+        return rvec(kind, length, inc, lambda R, k: R(0.2) + R(0.1) * k)
+    return cvec(kind, length, inc, lambda R, k: R(0.2) + R(0.1) * k, lambda R, k: R(-0.05) * k)
+
+
+def gemv_y_k(kind, length, inc):
+    if kind in "sd":
+        return rvec(kind, length, inc, lambda R, k: R(-0.3) + R(0.05) * k)
+    return cvec(kind, length, inc, lambda R, k: R(-0.3) + R(0.05) * k, lambda R, k: R(0.02) * k)
+
+
+# per kind: (ops, coefficients, shapes (m, n, lda, [(incx, incy)]), rtol, atol)
+GEMV_DCZ = {
+    "d": ((0, 1), [(1.0, 0.0), (0.0, -0.75), (0.75, -0.25), (-0.6, 0.4), (1.1, 0.0), (0.85, 0.1)],
+          [(5, 4, 5, [(1, 1)]), (1024, 512, 1024, [(1, 1), (2, 3), (3, 2), (2, 1)]), (256, 1024, 263, [(1, 1)]),
+           (640, 320, 640, [(1, 1)])], 1e-13, 1e-13),                      # dgemv_tests.rs:117-118, 193-246
+    "c": ((0, 1, 2), [(1.0 + 0j, 0j), (0j, 0.7 - 0.1j), (0.75 - 0.25j, 0.5 + 0j), (-0.5 + 0.2j, 0.3 - 0.15j),
+                      (1.1 - 0.6j, 0j), (0.3 + 0.7j, 0.1 - 0.2j)],
+          [(5, 4, 5, [(1, 1)]), (384, 256, 384, [(1, 1)]), (256, 512, 263, [(1, 1)]),
+           (300, 200, 305, [(2, 1), (1, 3), (2, 3)]), (64, 192, 64, [(1, 1)])], 5e-3, 1e-6),  # cgemv_tests.rs:125-126, 192-255
+    "z": ((0, 1, 2), [(1.0 + 0j, 0j), (0j, -0.75 + 0.2j), (0.75 - 0.10j, -0.25 + 0.05j), (-0.6 + 0.2j, 0.4 - 0.1j),
+                      (1.1 - 0.6j, 0j), (0.85 - 0.2j, 0.1 + 0j)],
+          [(5, 4, 5, [(1, 1)]), (384, 256, 384, [(1, 1)]), (256, 512, 263, [(1, 1)]),
+           (512, 256, 512, [(2, 3), (3, 2), (2, 1)]), (640, 320, 640, [(1, 1)])], 1e-11, 1e-12),  # zgemv_tests.rs:138-139, 218-273
+}
+
+
+# ---- d/c/z triangular multiply and solve -------------------------------------
+def tri_fill(kind, n, lda, uplo, fdiag, foff):
+    """Triangle `uplo` (0 upper, 1 lower) of a column-major buffer:
+    fdiag(R, i) on the diagonal, foff(R, d) off it, d = |i - j| as R.
+    Each callable returns a real value or a (re, im) pair."""
+    R = _real(kind)
+    a = np.zeros(lda * n, _DT[kind])
+    for j in range(n):
+        rows = np.arange(0, j + 1) if uplo == 0 else np.arange(j, n)
+        d = np.abs(rows - j).astype(R)
+        ii = rows.astype(R)
+        off, dia = foff(R, d), fdiag(R, ii)
+        if kind in "sd":
+            col = np.where(rows == j, dia, off)
+        else:
+            col = np.empty(rows.size, _DT[kind])
+            col.real = np.where(rows == j, dia[0], off[0])
+            col.imag = np.where(rows == j, dia[1], off[1])
+        a[j * lda + rows] = col
+    return a
+
+
+def set_diag(kind, a, n, lda, f):
+    R = _real(kind)
+    for i in range(n):
+        v = f(R, R(i))
+        a[i + i * lda] = v if kind in "sd" else complex(v[0], v[1])
+    return a
+
+
+def trmv_matrix_k(kind, n, lda, uplo, diag):
+    """dtrmv_tests.rs:63-176 (the strmv closed forms in f64);
+    ctrmv_tests.rs / ztrmv_tests.rs:63-155, 215-242 build_matrix."""
+    if kind == "d":
+        R = np.float64
+        f = (lambda i, j: R(0.2) + i * R(0.3) + j * R(0.15)) if uplo == 0 else \
+            (lambda i, j: R(-0.1) + i * R(0.25) - j * R(0.2))
+        a = cm_k("d", n, n, lda, lambda R_, i, j: f(i, j))
+        r, c = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+        keep = (r <= c) if uplo == 0 else (r >= c)
+        a[(r + c * lda)[~keep]] = 0.0
+        if diag == 0:
+            set_diag("d", a, n, lda, (lambda R_, i: R_(7.5) + i * R_(0.1)) if uplo == 0 else
+                     (lambda R_, i: R_(-9.0) + i * R_(0.05)))
+        return a
+    return _ctri(kind, n, lda, uplo, diag, trsv=False)
+
+
+def _ctri(kind, n, lda, uplo, diag, trsv):
+    """The complex triangles of ctrmv/ztrmv_tests.rs:63-155 and
+    ctrsv/ztrsv_tests.rs:91-183 (identical forms), with build_matrix's
+    planted diagonal for unit calls (its lower imaginary part is 2.1 - 0.03 i
+    in the multiply tests, 4.2 - 0.03 i in the solve tests)."""
+    if diag == 1:
+        if uplo == 0:
+            a = tri_fill(kind, n, lda, 0, lambda R, i: (R(1.0) + R(0.02) * i, R(0.01) - R(0.005) * i),
+                         lambda R, d: (R(0.01) / (R(1.0) + d), R(-0.008) / (R(1.0) + d)))
+        else:
+            a = tri_fill(kind, n, lda, 1, lambda R, i: (R(1.0) + R(0.02) * i, R(-0.012) + R(0.004) * i),
+                         lambda R, d: (R(0.01) / (R(1.0) + d), R(0.007) / (R(1.0) + d)))
+        return a
+    if uplo == 0:
+        a = tri_fill(kind, n, lda, 0, lambda R, i: (R(2.5) + R(0.05) * i, R(-1.7) + R(0.01) * i),
+                     lambda R, d: (R(5e-4) * (R(1.0) + d), R(-3e-4) * (R(1.0) + d)))
+        return set_diag(kind, a, n, lda, lambda R, i: (R(7.5) + i * R(0.1), R(-3.2) + i * R(0.07)))
+    a = tri_fill(kind, n, lda, 1, lambda R, i: (R(-2.0) + R(0.04) * i, R(1.2) - R(0.02) * i),
+                 lambda R, d: (R(6e-4) * (R(1.0) + d), R(4e-4) * (R(1.0) + d)))
+    return set_diag(kind, a, n, lda, lambda R, i: (R(-9.0) + i * R(0.05),
+                                                     (R(4.2) if trsv else R(2.1)) - i * R(0.03)))
+
+
+def trmv_x_k(kind, n, inc):
+    if kind == "d":
+        return rvec("d", n, inc, lambda R, k: R(0.1) + R(0.2) * k)
+    return cvec(kind, n, inc, lambda R, k: R(0.1) + R(0.2) * k, lambda R, k: R(-0.05) + R(0.03) * k)
+
+
+# per kind: (ops, shapes (n, lda, incs), rtol, atol)
+TRMV_DCZ = {
+    "d": ((0, 1, 2), [(7, 7, [1]), (1024, 1024, [1]), (640, 640, [2, 3])], 1e-13, 1e-13),   # dtrmv_tests.rs:154-155, 220-258
+    "c": ((0, 1, 2), [(7, 7, [1]), (768, 768, [1]), (256, 261, [1]), (384, 384, [2, 3, 4])], 1e-5, 1e-5),  # ctrmv_tests.rs:213-214, 295-337
+    "z": ((0, 1, 2), [(7, 7, [1]), (768, 768, [1]), (256, 261, [1]), (384, 384, [2, 3, 4])], 1e-13, 1e-13),  # ztrmv_tests.rs:213-214, 295-337
+}
+
+
+def trsv_matrix_k(kind, n, lda, uplo, diag):
+    """dtrsv_tests.rs:64-166, 216-241 build_matrix; c/z: ctrsv/ztrsv_tests.rs
+    91-183, 244-272."""
+    if kind != "d":
+        return _ctri(kind, n, lda, uplo, diag, trsv=True)
+    if diag == 1:
+        return tri_fill("d", n, lda, uplo, lambda R, i: R(1.0) + R(0.02) * i, lambda R, d: R(0.01) / (R(1.0) + d))
+    if uplo == 0:
+        a = tri_fill("d", n, lda, 0, lambda R, i: R(1.0) + R(0.05) * i, lambda R, d: R(5e-4) * (R(1.0) + d))
+        return set_diag("d", a, n, lda, lambda R, i: R(7.5) + i * R(0.1))
+    a = tri_fill("d", n, lda, 1, lambda R, i: R(1.0) - R(0.03) * i, lambda R, d: R(6e-4) * (R(1.0) + d))
+    return set_diag("d", a, n, lda, lambda R, i: R(-9.0) + i * R(0.05))
+
+
+def trsv_x_k(kind, n, inc):
+    if kind == "d":
+        return rvec("d", n, inc, lambda R, k: R(0.05) + R(0.01) * k)
+    return cvec(kind, n, inc, lambda R, k: R(0.1) + R(0.2) * k, lambda R, k: R(-0.05) + R(0.03) * k)
+
+
+TRSV_DCZ = {
+    "d": ((0, 1), [(7, 7, [1]), (1024, 1024, [1]), (640, 640, [2, 3, 4]), (127, 132, [1])], 1e-12, 1e-12),  # dtrsv_tests.rs:213-214, 285-332
+    "c": ((0, 1, 2), [(7, 7, [1]), (760, 768, [1]), (384, 384, [2, 3, 4]), (256, 263, [1])], 1e-2, 1e-3),  # ctrsv_tests.rs:241-242, 320-363
+    "z": ((0, 1, 2), [(7, 7, [1]), (768, 768, [1]), (384, 384, [2, 3, 4]), (256, 263, [1])], 1e-11, 1e-11),  # ztrsv_tests.rs:241-242, 320-363
+}
+
+
+def sample_index(length, count=96):
+    """Fixed positions of a result vector stored in the golden file: all of
+    it up to `count` entries, else the first and last 8 and an even spread
+    between them."""
+    if length <= count:
+        return np.arange(length)
+    mid = np.linspace(8, length - 9, count - 16).astype(np.int64)
+    return np.unique(np.concatenate([np.arange(8), mid, np.arange(length - 8, length)]))

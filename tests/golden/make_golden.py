@@ -25,6 +25,11 @@ def logical(buf, rows, cols, ld):
     return np.asfortranarray(buf.reshape(cols, ld).T[:rows, :])
 
 
+def S(v):
+    """The stored positions of a result vector (fixtures.sample_index)."""
+    return v[fx.sample_index(v.size)]
+
+
 def l1_reference(case) -> np.ndarray:
     """OpenBLAS result of one L1_CASES entry: the updated vector(s) or the
     scalar, as a flat array."""
@@ -114,18 +119,18 @@ def main() -> None:
             g[f"rotg_{kind}{ci}"] = np.array([c, s], np.float64)
     for ci, (kind, d1, d2, x1, y1) in enumerate(fx.ROTMG_CASES):
         g[f"rotmg_c{ci}"] = np.asarray(getattr(blas, kind + "rotmg")(d1, d2, x1, y1), np.float64)
-    # ---- SSYMV / CHEMV (uplo 0 upper, 1 lower), all of y
+    # ---- SSYMV / CHEMV (uplo 0 upper, 1 lower), y at fx.sample_index positions
     for si, (n, lda, strides) in enumerate(fx.SYMV_SHAPES):
         A = logical(fx.symv_matrix(n, lda), n, n, lda)
         for (incx, incy) in strides:
-            x, y0 = fx.gemv_x(n, incx), fx.gemv_y(n, incy)
+            x, y0 = fx.symv_x("s", n, incx), fx.symv_y("s", n, incy)
             for uplo in (0, 1):
                 for ci, (alpha, beta) in enumerate(fx.SYMV_COEFFS):
                     r = blas.ssymv(alpha, A, x, beta=beta, y=y0.copy(), incx=incx, incy=incy, lower=uplo)
-                    g[f"ssymv_s{si}_{incx}{incy}_u{uplo}_c{ci}"] = np.asarray(r, np.float32)[::incy][:n]
+                    g[f"ssymv_s{si}_{incx}{incy}_u{uplo}_c{ci}"] = S(np.asarray(r, np.float32)[::incy][:n])
     for ci, (uplo, n, lda, alpha, beta, a, x, y0) in enumerate(fx.symv_garbage_cases()):
         r = blas.ssymv(alpha, logical(a, n, n, lda), x, beta=beta, y=y0.copy(), lower=uplo)
-        g[f"ssymv_tri{ci}"] = np.asarray(r, np.float32)
+        g[f"ssymv_tri{ci}"] = S(np.asarray(r, np.float32))
     for si, (n, lda, strides) in enumerate(fx.HEMV_SHAPES):
         A = logical(fx.hemv_matrix(n, lda), n, n, lda)
         for (incx, incy) in strides:
@@ -133,10 +138,10 @@ def main() -> None:
             for uplo in (0, 1):
                 for ci, (alpha, beta) in enumerate(fx.HEMV_COEFFS):
                     r = blas.chemv(alpha, A, x, beta=beta, y=y0.copy(), incx=incx, incy=incy, lower=uplo)
-                    g[f"chemv_s{si}_{incx}{incy}_u{uplo}_c{ci}"] = np.asarray(r, np.complex64)[::incy][:n]
+                    g[f"chemv_s{si}_{incx}{incy}_u{uplo}_c{ci}"] = S(np.asarray(r, np.complex64)[::incy][:n])
     for ci, (uplo, n, lda, alpha, beta, a, x, y0) in enumerate(fx.hemv_garbage_cases()):
         r = blas.chemv(alpha, logical(a, n, n, lda), x, beta=beta, y=y0.copy(), lower=uplo)
-        g[f"chemv_tri{ci}"] = np.asarray(r, np.complex64)
+        g[f"chemv_tri{ci}"] = S(np.asarray(r, np.complex64))
     # ---- STRMV (trans 0 N, 1 T, 2 C; CORAL diag 0 = unit, 1 = non-unit)
     for si, (n, lda, incs) in enumerate(fx.TRMV_SHAPES):
         for uplo in (0, 1):
@@ -147,7 +152,7 @@ def main() -> None:
                     for trans in (0, 1, 2):
                         r = blas.strmv(A, x.copy(), incx=inc, lower=uplo, trans=trans,
                                        diag=1 if diag == 0 else 0)
-                        g[f"strmv_s{si}_u{uplo}_i{inc}_t{trans}_d{diag}"] = np.asarray(r, np.float32)[::inc][:n]
+                        g[f"strmv_s{si}_u{uplo}_i{inc}_t{trans}_d{diag}"] = S(np.asarray(r, np.float32)[::inc][:n])
     # ---- SGER / SSYR / SSYR2: the logical matrix at fixed positions
     for ci, (m, n, lda, incx, incy, alpha, gx, gy) in enumerate(fx.GER_CASES):
         A = logical(fx.ger_matrix(m, n, lda), m, n, lda)
@@ -168,6 +173,50 @@ def main() -> None:
                        np.float32)
         ri, cj = fx.sample_positions(n, n)
         g[f"ssyr2_c{ci}"] = r[ri, cj]
+    # ---- d/c/z GEMV (trans 0 N, 1 T, 2 C)
+    for kind, (ops, coeffs, shapes, _, _) in fx.GEMV_DCZ.items():
+        for si, (m, n, lda, strides) in enumerate(shapes):
+            A = logical(fx.gemv_matrix_k(kind, m, n, lda), m, n, lda)
+            for (incx, incy) in strides:
+                for trans in ops:
+                    xl, yl = (n, m) if trans == 0 else (m, n)
+                    x, y0 = fx.gemv_x_k(kind, xl, incx), fx.gemv_y_k(kind, yl, incy)
+                    for ci, (alpha, beta) in enumerate(coeffs):
+                        r = getattr(blas, kind + "gemv")(alpha, A, x, beta=beta, y=y0.copy(), incx=incx,
+                                                         incy=incy, trans=trans)
+                        g[f"{kind}gemv_s{si}_{incx}{incy}_t{trans}_c{ci}"] = S(np.asarray(r)[::incy][:yl])
+    # ---- DSYMV / ZHEMV
+    for kind, name, coeffs, shapes, mat, xg, yg, garbage in (
+            ("d", "dsymv", fx.SYMV_COEFFS, fx.SYMV_SHAPES, lambda n, l: fx.symv_matrix(n, l, "d"),
+             lambda n, i: fx.symv_x("d", n, i), lambda n, i: fx.symv_y("d", n, i), fx.symv_garbage_cases("d")),
+            ("z", "zhemv", fx.ZHEMV_COEFFS, fx.HEMV_SHAPES, lambda n, l: fx.hemv_matrix(n, l, "z"),
+             lambda n, i: fx.hemv_x(n, i, "z"), lambda n, i: fx.hemv_y(n, i, "z"), fx.hemv_garbage_cases("z"))):
+        for si, (n, lda, strides) in enumerate(shapes):
+            A = logical(mat(n, lda), n, n, lda)
+            for (incx, incy) in strides:
+                x, y0 = xg(n, incx), yg(n, incy)
+                for uplo in (0, 1):
+                    for ci, (alpha, beta) in enumerate(coeffs):
+                        r = getattr(blas, name)(alpha, A, x, beta=beta, y=y0.copy(), incx=incx, incy=incy,
+                                                lower=uplo)
+                        g[f"{name}_s{si}_{incx}{incy}_u{uplo}_c{ci}"] = S(np.asarray(r)[::incy][:n])
+        for ci, (uplo, n, lda, alpha, beta, a, x, y0) in enumerate(garbage):
+            r = getattr(blas, name)(alpha, logical(a, n, n, lda), x, beta=beta, y=y0.copy(), lower=uplo)
+            g[f"{name}_tri{ci}"] = S(np.asarray(r))
+    # ---- d/c/z TRMV and TRSV (CORAL diag 0 = unit, 1 = non-unit)
+    for fam, table, mat, xg in (("trmv", fx.TRMV_DCZ, fx.trmv_matrix_k, fx.trmv_x_k),
+                                ("trsv", fx.TRSV_DCZ, fx.trsv_matrix_k, fx.trsv_x_k)):
+        for kind, (ops, shapes, _, _) in table.items():
+            for si, (n, lda, incs) in enumerate(shapes):
+                for uplo in (0, 1):
+                    for diag in (0, 1):
+                        A = logical(mat(kind, n, lda, uplo, diag), n, n, lda)
+                        for inc in incs:
+                            x = xg(kind, n, inc)
+                            for trans in ops:
+                                r = getattr(blas, kind + fam)(A, x.copy(), incx=inc, lower=uplo, trans=trans,
+                                                              diag=1 if diag == 0 else 0)
+                                g[f"{kind}{fam}_s{si}_u{uplo}_i{inc}_t{trans}_d{diag}"] = S(np.asarray(r)[::inc][:n])
     np.savez_compressed(OUT, **g)
     print(f"wrote {len(g)} arrays to {OUT} ({os.path.getsize(OUT)} bytes)")
 

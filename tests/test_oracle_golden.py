@@ -3,9 +3,9 @@
 Known answers: the sgemm and cgemm doctests (coral-aarch64/src/level3/
 sgemm.rs:36-81, cgemm.rs:36-96) and the planted-maximum isamax cases
 (tests/level1/iamax_tests.rs:79-170).  Fixtures: the closed-form cases of
-tests/level3/sgemm_tests.rs, tests/level2/{sgemv,ssymv,chemv,strsv,strmv,
-sger,ssyr,ssyr2}_tests.rs and the level-1 tests, whose expected outputs were
-computed by
+tests/level3/sgemm_tests.rs, tests/level2/{s,d,c,z}gemv, {s,d}symv,
+{c,z}hemv, {s,d,c,z}trsv, {s,d,c,z}trmv, sger, ssyr and ssyr2_tests.rs and
+the level-1 tests, whose expected outputs were computed by
 CBLAS-class BLAS (tests/golden/make_golden.py) and are checked here with the
 reference's own tolerances.
 """
@@ -249,6 +249,12 @@ def test_l1_dcz_rounding_paths():
 
 
 # ---- symmetric / Hermitian matrix-vector, triangular multiply, rank updates ----
+def _S(v):
+    """The positions of a result vector that the golden file stores."""
+    v = np.asarray(v)
+    return v[fx.sample_index(v.size)]
+
+
 def test_ssymv_fixtures(golden):
     """ssymv_tests.rs:155-249: every shape, stride pair, uplo and (alpha,
     beta) at the reference's 1e-5 / 1e-5 (ssymv_tests.rs:152-153)."""
@@ -256,11 +262,11 @@ def test_ssymv_fixtures(golden):
     for si, (n, lda, strides) in enumerate(fx.SYMV_SHAPES):
         a = fx.symv_matrix(n, lda)
         for (incx, incy) in strides:
-            x, y0 = fx.gemv_x(n, incx), fx.gemv_y(n, incy)
+            x, y0 = fx.symv_x("s", n, incx), fx.symv_y("s", n, incy)
             for uplo in (0, 1):
                 for ci, (alpha, beta) in enumerate(fx.SYMV_COEFFS):
                     got = oracle.ssymv(uplo, n, alpha, a, lda, x, incx, beta, y0, incy)
-                    allclose_ref(got, golden[f"ssymv_s{si}_{incx}{incy}_u{uplo}_c{ci}"], 1e-5, 1e-5)
+                    allclose_ref(_S(got), golden[f"ssymv_s{si}_{incx}{incy}_u{uplo}_c{ci}"], 1e-5, 1e-5)
 
 
 def test_ssymv_reads_only_the_stored_triangle(golden):
@@ -269,7 +275,7 @@ def test_ssymv_reads_only_the_stored_triangle(golden):
     for ci, (uplo, n, lda, alpha, beta, a, x, y0) in enumerate(fx.symv_garbage_cases()):
         got = oracle.ssymv(uplo, n, alpha, a, lda, x, 1, beta, y0, 1)
         assert np.isfinite(got).all()
-        allclose_ref(got, golden[f"ssymv_tri{ci}"], 1e-5, 1e-5)
+        allclose_ref(_S(got), golden[f"ssymv_tri{ci}"], 1e-5, 1e-5)
 
 
 def test_ssymv_upper_equals_lower():
@@ -300,8 +306,8 @@ def test_chemv_fixtures(golden):
             for uplo in (0, 1):
                 for ci, (alpha, beta) in enumerate(fx.HEMV_COEFFS):
                     got = oracle.chemv(uplo, n, _pair(alpha), a, lda, x, incx, _pair(beta), y0, incy)
-                    want = golden[f"chemv_s{si}_{incx}{incy}_u{uplo}_c{ci}"].view(np.float32)
-                    allclose_ref(got, want, 1e-5, 1e-6)
+                    want = golden[f"chemv_s{si}_{incx}{incy}_u{uplo}_c{ci}"]
+                    allclose_ref(_S(got.view(np.complex128)).view(np.float64), want.view(np.float32), 1e-5, 1e-6)
 
 
 def test_chemv_reads_only_the_stored_triangle(golden):
@@ -311,7 +317,7 @@ def test_chemv_reads_only_the_stored_triangle(golden):
         got = oracle.chemv(uplo, n, _pair(alpha), a.view(np.float32), lda, x.view(np.float32), 1,
                            _pair(beta), y0.view(np.float32), 1)
         assert np.isfinite(got).all()
-        allclose_ref(got, golden[f"chemv_tri{ci}"].view(np.float32), 1e-5, 1e-6)
+        allclose_ref(_S(got.view(np.complex128)).view(np.float64), golden[f"chemv_tri{ci}"].view(np.float32), 1e-5, 1e-6)
 
 
 def test_strmv_fixtures(golden):
@@ -327,7 +333,7 @@ def test_strmv_fixtures(golden):
                     x = fx.trmv_x(n, inc)
                     for trans in (0, 1, 2):
                         got = oracle.strmv(uplo, trans, diag, n, a, lda, x, inc)
-                        allclose_ref(got, golden[f"strmv_s{si}_u{uplo}_i{inc}_t{trans}_d{diag}"],
+                        allclose_ref(_S(got), golden[f"strmv_s{si}_u{uplo}_i{inc}_t{trans}_d{diag}"],
                                      1e-5, 1e-5)
 
 
@@ -382,3 +388,100 @@ def test_ssyr2_fixtures(golden):
         ri, cj = fx.sample_positions(n, n)
         allclose_ref(_logical_at(got, lda, ri, cj), golden[f"ssyr2_c{ci}"], 1e-6, 1e-5)
         _only_triangle_touched(got, a0, n, lda, uplo)
+
+
+# ---- d/c/z matrix-vector, symmetric / Hermitian, triangular ----------------------
+def _cmp(got, want, rtol, atol):
+    """The reference's per-component criterion (real and imaginary parts
+    separately for complex results)."""
+    from conftest import allclose_ref
+    got, want = np.asarray(got), np.asarray(want)
+    if np.iscomplexobj(want):
+        got = np.asarray(got, np.complex128).view(np.float64)
+        want = np.asarray(want, np.complex128).view(np.float64)
+    allclose_ref(got, want, rtol, atol)
+
+
+@pytest.mark.parametrize("kind", ["d", "c", "z"])
+def test_gemv_dcz_fixtures(golden, kind):
+    """dgemv/cgemv/zgemv_tests.rs: every shape, stride pair, op and (alpha,
+    beta) at each file's tolerance."""
+    ops, coeffs, shapes, rtol, atol = fx.GEMV_DCZ[kind]
+    fn = getattr(oracle, kind + "gemv")
+    for si, (m, n, lda, strides) in enumerate(shapes):
+        a = fx.gemv_matrix_k(kind, m, n, lda)
+        for (incx, incy) in strides:
+            for trans in ops:
+                xl, yl = (n, m) if trans == 0 else (m, n)
+                x, y0 = fx.gemv_x_k(kind, xl, incx), fx.gemv_y_k(kind, yl, incy)
+                for ci, (alpha, beta) in enumerate(coeffs):
+                    got = fn(trans, m, n, alpha, a, lda, x, incx, beta, y0, incy)
+                    _cmp(_S(got), golden[f"{kind}gemv_s{si}_{incx}{incy}_t{trans}_c{ci}"], rtol, atol)
+
+
+def test_dsymv_fixtures(golden):
+    """dsymv_tests.rs:155-378 at 1e-13 / 1e-13 (dsymv_tests.rs:152-153),
+    including the NaN-garbage triangle cases."""
+    for si, (n, lda, strides) in enumerate(fx.SYMV_SHAPES):
+        a = fx.symv_matrix(n, lda, "d")
+        for (incx, incy) in strides:
+            x, y0 = fx.symv_x("d", n, incx), fx.symv_y("d", n, incy)
+            for uplo in (0, 1):
+                for ci, (alpha, beta) in enumerate(fx.SYMV_COEFFS):
+                    got = oracle.dsymv(uplo, n, alpha, a, lda, x, incx, beta, y0, incy)
+                    _cmp(_S(got), golden[f"dsymv_s{si}_{incx}{incy}_u{uplo}_c{ci}"], 1e-13, 1e-13)
+    for ci, (uplo, n, lda, alpha, beta, a, x, y0) in enumerate(fx.symv_garbage_cases("d")):
+        got = oracle.dsymv(uplo, n, alpha, a, lda, x, 1, beta, y0, 1)
+        assert np.isfinite(got).all()
+        _cmp(_S(got), golden[f"dsymv_tri{ci}"], 1e-13, 1e-13)
+
+
+def test_zhemv_fixtures(golden):
+    """zhemv_tests.rs:187-478 at 1e-12 / 1e-12 (zhemv_tests.rs:184-185),
+    including the NaN-garbage triangle cases."""
+    for si, (n, lda, strides) in enumerate(fx.HEMV_SHAPES):
+        a = fx.hemv_matrix(n, lda, "z")
+        for (incx, incy) in strides:
+            x, y0 = fx.hemv_x(n, incx, "z"), fx.hemv_y(n, incy, "z")
+            for uplo in (0, 1):
+                for ci, (alpha, beta) in enumerate(fx.ZHEMV_COEFFS):
+                    got = oracle.zhemv(uplo, n, alpha, a, lda, x, incx, beta, y0, incy)
+                    _cmp(_S(got), golden[f"zhemv_s{si}_{incx}{incy}_u{uplo}_c{ci}"], 1e-12, 1e-12)
+    for ci, (uplo, n, lda, alpha, beta, a, x, y0) in enumerate(fx.hemv_garbage_cases("z")):
+        got = oracle.zhemv(uplo, n, alpha, a, lda, x, 1, beta, y0, 1)
+        assert np.isfinite(got).all()
+        _cmp(_S(got), golden[f"zhemv_tri{ci}"], 1e-12, 1e-12)
+
+
+@pytest.mark.parametrize("kind", ["d", "c", "z"])
+def test_trmv_dcz_fixtures(golden, kind):
+    """dtrmv/ctrmv/ztrmv_tests.rs: both triangles, N/T/C, unit (planted
+    diagonal ignored) and non-unit, at each file's tolerance."""
+    ops, shapes, rtol, atol = fx.TRMV_DCZ[kind]
+    fn = getattr(oracle, kind + "trmv")
+    for si, (n, lda, incs) in enumerate(shapes):
+        for uplo in (0, 1):
+            for diag in (0, 1):
+                a = fx.trmv_matrix_k(kind, n, lda, uplo, diag)
+                for inc in incs:
+                    x = fx.trmv_x_k(kind, n, inc)
+                    for trans in ops:
+                        got = fn(uplo, trans, diag, n, a, lda, x, inc)
+                        _cmp(_S(got), golden[f"{kind}trmv_s{si}_u{uplo}_i{inc}_t{trans}_d{diag}"], rtol, atol)
+
+
+@pytest.mark.parametrize("kind", ["d", "c", "z"])
+def test_trsv_dcz_fixtures(golden, kind):
+    """dtrsv/ctrsv/ztrsv_tests.rs: both triangles, every op, unit (planted
+    diagonal ignored) and non-unit, padded lda and strides, at each file's
+    tolerance."""
+    ops, shapes, rtol, atol = fx.TRSV_DCZ[kind]
+    for si, (n, lda, incs) in enumerate(shapes):
+        for uplo in (0, 1):
+            for diag in (0, 1):
+                a = fx.trsv_matrix_k(kind, n, lda, uplo, diag)
+                for inc in incs:
+                    x = fx.trsv_x_k(kind, n, inc)
+                    for trans in ops:
+                        got = oracle.trsv_dcz(kind, uplo, trans, diag, n, a, lda, x, inc)
+                        _cmp(_S(got), golden[f"{kind}trsv_s{si}_u{uplo}_i{inc}_t{trans}_d{diag}"], rtol, atol)
