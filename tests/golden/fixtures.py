@@ -706,3 +706,56 @@ def sample_index(length, count=96):
         return np.arange(length)
     mid = np.linspace(8, length - 9, count - 16).astype(np.int64)
     return np.unique(np.concatenate([np.arange(8), mid, np.arange(length - 8, length)]))
+
+
+# ---- d/c/z rank updates: dger, dsyr, dsyr2, {c,z}ger{u,c}, {c,z}her, {c,z}her2 ----
+# dger/dsyr/dsyr2_tests.rs run the sger/ssyr/ssyr2 case tables in f64
+# (GER_CASES, SYR_CASES, SYR2_CASES); tolerances (rtol, atol):
+RANK_TOL = {"sger": (1e-6, 1e-6), "dger": (1e-13, 1e-13),        # sger/dger_tests.rs:82-83, 81-82
+            "ssyr": (1e-6, 1e-5), "dsyr": (1e-6, 1e-5),          # ssyr/dsyr_tests.rs:129-130, 128-129
+            "ssyr2": (1e-6, 1e-5), "dsyr2": (1e-6, 1e-5),        # ssyr2/dsyr2_tests.rs:131-132
+            "cger": (1e-6, 1e-6), "zger": (1e-12, 1e-12),        # cger/zger_tests.rs:118-119, 111-112
+            "cher": (1e-5, 1e-6), "zher": (1e-13, 1e-13),        # cher/zher_tests.rs:147-148, 149-150
+            "cher2": (1e-5, 1e-6), "zher2": (1e-13, 1e-13)}      # cher2/zher2_tests.rs:148-149, 156-157
+
+
+def rank_vec(kind, n, inc, g):
+    """Ramp g = (a, b) for real kinds, (re0, re1, im0, im1) for complex."""
+    if kind in "sd":
+        return rvec(kind, n, inc, lambda R, k: R(g[0]) + R(g[1]) * k)
+    return cvec(kind, n, inc, lambda R, k: R(g[0]) + R(g[1]) * k, lambda R, k: R(g[2]) + R(g[3]) * k)
+
+
+# (m, n, lda, incx, incy, alpha geru, alpha gerc, x ramp, y ramp):
+# cger_tests.rs / zger_tests.rs run_contiguous_sets, run_strided_padded,
+# run_alpha_zero(300, 200, 305)
+CGER_CASES = [
+    (7, 5, 7, 1, 1, 1.25 - 0.40j, 0.85 + 0.35j, (0.20, 0.10, -0.30, 0.05), (-0.10, 0.07, 0.20, -0.04)),
+    (1024, 768, 1024, 1, 1, -0.37 + 0.21j, -0.21 + 0.44j, (0.05, 0.002, -0.02, 0.001), (0.40, -0.003, 0.10, 0.002)),
+    (512, 1024, 512, 1, 1, 0.93 - 0.61j, 0.37 - 0.72j, (-0.20, 0.0015, 0.30, -0.0007), (0.10, 0.0020, 0.20, 0.0010)),
+    (9, 4, 12, 2, 3, -0.85 + 0j, 0.65 + 0.10j, (0.05, 0.03, 0.04, -0.01), (0.40, -0.02, -0.30, 0.05)),
+    (300, 200, 305, 1, 1, 0j, 0j, (0.11, 0.01, -0.02, 0.003), (0.07, -0.01, 0.05, 0.004)),
+]
+
+# (uplo, n, lda, incx, alpha, x ramp): cher_tests.rs / zher_tests.rs
+# run_small_and_large, run_lower_padded_strided, the alpha = 0 case
+HER_CASES = [
+    (0, 6, 6, 1, 0.9, (0.2, 0.1, -0.05, 0.02)),
+    (0, 512, 512, 1, -0.37, (0.03, 0.001, -0.02, 0.0007)),
+    (1, 7, 7, 1, -0.8, (-0.1, 0.03, 0.07, -0.01)),
+    (1, 256, 256, 1, 0.93, (-0.02, 0.0005, 0.01, -0.0003)),
+    (1, 9, 12, 2, -0.85, (0.05, 0.03, -0.02, 0.01)),
+    (0, 64, 69, 1, 0.0, (0.11, 0.01, -0.07, 0.004)),
+]
+
+# (uplo, n, lda, incx, incy, alpha, x ramp, y ramp): cher2_tests.rs /
+# zher2_tests.rs run_small_and_large, run_lower_padded_strided,
+# run_alpha_zero_does_nothing
+HER2_CASES = [
+    (0, 7, 7, 1, 1, 1.10 - 0.35j, (0.2, 0.10, -0.05, 0.02), (-0.3, 0.05, 0.07, -0.01)),
+    (0, 1024, 1024, 1, 1, -0.37 + 0.20j, (0.05, 0.002, -0.02, 0.0007), (0.40, -0.003, 0.01, -0.0005)),
+    (1, 7, 7, 1, 1, -0.80 + 0.50j, (-0.2, 0.07, 0.06, -0.01), (0.4, -0.055, -0.03, 0.02)),
+    (1, 512, 512, 1, 1, 0.93 - 0.10j, (-0.20, 0.0015, 0.03, -0.0004), (0.10, 0.0020, -0.01, 0.0003)),
+    (1, 9, 12, 2, 3, -0.85 + 0.25j, (0.05, 0.03, -0.02, 0.01), (0.40, -0.02, 0.03, -0.01)),
+    (0, 300, 305, 1, 1, 0j, (0.11, 0.01, -0.07, 0.004), (0.08, -0.01, 0.02, 0.003)),
+]

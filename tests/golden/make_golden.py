@@ -217,6 +217,46 @@ def main() -> None:
                                 r = getattr(blas, kind + fam)(A, x.copy(), incx=inc, lower=uplo, trans=trans,
                                                               diag=1 if diag == 0 else 0)
                                 g[f"{kind}{fam}_s{si}_u{uplo}_i{inc}_t{trans}_d{diag}"] = S(np.asarray(r)[::inc][:n])
+    # ---- d/c/z rank updates: the logical matrix at 512 fixed positions
+    for ci, (m, n, lda, incx, incy, alpha, gx, gy) in enumerate(fx.GER_CASES):
+        A = logical(fx.cm_k("d", m, n, lda, lambda R, i, j: R(0.1) + i * R(0.5) + j * R(0.25)), m, n, lda)
+        x, y = fx.rank_vec("d", m, incx, gx)[::incx], fx.rank_vec("d", n, incy, gy)[::incy]
+        r = np.asarray(blas.dger(alpha, x, y, a=A.copy()))
+        ri, cj = fx.sample_positions(m, n, 512)
+        g[f"dger_c{ci}"] = r[ri, cj]
+    for ci, (uplo, n, lda, incx, alpha, gx) in enumerate(fx.SYR_CASES):
+        A = logical(fx.syr_matrix(n, lda, "d"), n, n, lda)
+        r = np.asarray(blas.dsyr(alpha, fx.rank_vec("d", n, incx, gx), lower=uplo, incx=incx, n=n, a=A.copy()))
+        ri, cj = fx.sample_positions(n, n, 512)
+        g[f"dsyr_c{ci}"] = r[ri, cj]
+    for ci, (uplo, n, lda, incx, incy, alpha, gx, gy) in enumerate(fx.SYR2_CASES):
+        A = logical(fx.syr_matrix(n, lda, "d"), n, n, lda)
+        r = np.asarray(blas.dsyr2(alpha, fx.rank_vec("d", n, incx, gx), fx.rank_vec("d", n, incy, gy), lower=uplo,
+                                  incx=incx, incy=incy, n=n, a=A.copy()))
+        ri, cj = fx.sample_positions(n, n, 512)
+        g[f"dsyr2_c{ci}"] = r[ri, cj]
+    for kind in "cz":
+        for ci, (m, n, lda, incx, incy, au, ac, gx, gy) in enumerate(fx.CGER_CASES):
+            A = logical(fx.gemv_matrix_k(kind, m, n, lda), m, n, lda)
+            x, y = fx.rank_vec(kind, m, incx, gx)[::incx], fx.rank_vec(kind, n, incy, gy)[::incy]
+            ri, cj = fx.sample_positions(m, n, 512)
+            for conj, alpha in ((0, au), (1, ac)):
+                fn = getattr(blas, kind + ("gerc" if conj else "geru"))
+                r = np.asarray(fn(alpha, x, y, a=A.copy()))
+                g[f"{kind}ger_c{ci}_j{conj}"] = r[ri, cj]
+        for ci, (uplo, n, lda, incx, alpha, gx) in enumerate(fx.HER_CASES):
+            A = logical(fx.hemv_matrix(n, lda, kind), n, n, lda)
+            r = np.asarray(getattr(blas, kind + "her")(alpha, fx.rank_vec(kind, n, incx, gx), lower=uplo, incx=incx,
+                                                      n=n, a=A.copy()))
+            ri, cj = fx.sample_positions(n, n, 512)
+            g[f"{kind}her_c{ci}"] = r[ri, cj]
+        for ci, (uplo, n, lda, incx, incy, alpha, gx, gy) in enumerate(fx.HER2_CASES):
+            A = logical(fx.hemv_matrix(n, lda, kind), n, n, lda)
+            r = np.asarray(getattr(blas, kind + "her2")(alpha, fx.rank_vec(kind, n, incx, gx),
+                                                       fx.rank_vec(kind, n, incy, gy), lower=uplo, incx=incx,
+                                                       incy=incy, n=n, a=A.copy()))
+            ri, cj = fx.sample_positions(n, n, 512)
+            g[f"{kind}her2_c{ci}"] = r[ri, cj]
     np.savez_compressed(OUT, **g)
     print(f"wrote {len(g)} arrays to {OUT} ({os.path.getsize(OUT)} bytes)")
 

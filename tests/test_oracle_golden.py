@@ -4,8 +4,9 @@ Known answers: the sgemm and cgemm doctests (coral-aarch64/src/level3/
 sgemm.rs:36-81, cgemm.rs:36-96) and the planted-maximum isamax cases
 (tests/level1/iamax_tests.rs:79-170).  Fixtures: the closed-form cases of
 tests/level3/sgemm_tests.rs, tests/level2/{s,d,c,z}gemv, {s,d}symv,
-{c,z}hemv, {s,d,c,z}trsv, {s,d,c,z}trmv, sger, ssyr and ssyr2_tests.rs and
-the level-1 tests, whose expected outputs were computed by
+{c,z}hemv, {s,d,c,z}trsv, {s,d,c,z}trmv, {s,d}ger, {c,z}ger, {s,d}syr,
+{s,d}syr2, {c,z}her and {c,z}her2_tests.rs and the level-1 tests, whose
+expected outputs were computed by
 CBLAS-class BLAS (tests/golden/make_golden.py) and are checked here with the
 reference's own tolerances.
 """
@@ -359,12 +360,12 @@ def test_sger_fixtures(golden):
             np.testing.assert_array_equal(got, a0)
 
 
-def _only_triangle_touched(got, a0, n, lda, uplo):
+def _only_triangle_touched(got, a0, n, lda, uplo, bits=np.uint32):
     """ssyr_tests.rs:106-127: the other triangle keeps its bits."""
     i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
     other = (i > j) if uplo == 0 else (i < j)
     idx = (i + j * lda)[other]
-    np.testing.assert_array_equal(got[idx].view(np.uint32), a0[idx].view(np.uint32))
+    np.testing.assert_array_equal(got[idx].view(bits), a0[idx].view(bits))
 
 
 def test_ssyr_fixtures(golden):
@@ -485,3 +486,60 @@ def test_trsv_dcz_fixtures(golden, kind):
                     for trans in ops:
                         got = oracle.trsv_dcz(kind, uplo, trans, diag, n, a, lda, x, inc)
                         _cmp(_S(got), golden[f"{kind}trsv_s{si}_u{uplo}_i{inc}_t{trans}_d{diag}"], rtol, atol)
+
+
+def test_rank_dz_real_fixtures(golden):
+    """dger/dsyr/dsyr2_tests.rs: the sger/ssyr/ssyr2 case tables in f64 at
+    each file's tolerance; the syr forms leave the other triangle's bits."""
+    for ci, (m, n, lda, incx, incy, alpha, gx, gy) in enumerate(fx.GER_CASES):
+        a0 = fx.cm_k("d", m, n, lda, lambda R, i, j: R(0.1) + i * R(0.5) + j * R(0.25))
+        got = oracle.dger(m, n, alpha, fx.rank_vec("d", m, incx, gx), incx, fx.rank_vec("d", n, incy, gy), incy,
+                          a0, lda)
+        ri, cj = fx.sample_positions(m, n, 512)
+        _cmp(_logical_at(got, lda, ri, cj), golden[f"dger_c{ci}"], *fx.RANK_TOL["dger"])
+    for ci, (uplo, n, lda, incx, alpha, gx) in enumerate(fx.SYR_CASES):
+        a0 = fx.syr_matrix(n, lda, "d")
+        got = oracle.dsyr(uplo, n, alpha, fx.rank_vec("d", n, incx, gx), incx, a0, lda)
+        ri, cj = fx.sample_positions(n, n, 512)
+        _cmp(_logical_at(got, lda, ri, cj), golden[f"dsyr_c{ci}"], *fx.RANK_TOL["dsyr"])
+        _only_triangle_touched(got, a0, n, lda, uplo, np.uint64)
+    for ci, (uplo, n, lda, incx, incy, alpha, gx, gy) in enumerate(fx.SYR2_CASES):
+        a0 = fx.syr_matrix(n, lda, "d")
+        got = oracle.dsyr(uplo, n, alpha, fx.rank_vec("d", n, incx, gx), incx, a0, lda,
+                          y=fx.rank_vec("d", n, incy, gy), incy=incy)
+        ri, cj = fx.sample_positions(n, n, 512)
+        _cmp(_logical_at(got, lda, ri, cj), golden[f"dsyr2_c{ci}"], *fx.RANK_TOL["dsyr2"])
+        _only_triangle_touched(got, a0, n, lda, uplo, np.uint64)
+
+
+@pytest.mark.parametrize("kind", ["c", "z"])
+def test_rank_complex_fixtures(golden, kind):
+    """cger/zger (geru and gerc), cher/zher and cher2/zher2_tests.rs at each
+    file's tolerance; the Hermitian forms leave the other triangle's bits."""
+    for ci, (m, n, lda, incx, incy, au, ac, gx, gy) in enumerate(fx.CGER_CASES):
+        a0 = fx.gemv_matrix_k(kind, m, n, lda)
+        ri, cj = fx.sample_positions(m, n, 512)
+        for conj, alpha in ((0, au), (1, ac)):
+            got = oracle.gerc_u(kind, conj, m, n, alpha, fx.rank_vec(kind, m, incx, gx), incx,
+                                fx.rank_vec(kind, n, incy, gy), incy, a0, lda)
+            _cmp(_logical_at(got, lda, ri, cj), golden[f"{kind}ger_c{ci}_j{conj}"], *fx.RANK_TOL[kind + "ger"])
+    for ci, (uplo, n, lda, incx, alpha, gx) in enumerate(fx.HER_CASES):
+        a0 = fx.hemv_matrix(n, lda, kind)
+        got = oracle.her(kind, uplo, n, alpha, fx.rank_vec(kind, n, incx, gx), incx, a0, lda)
+        ri, cj = fx.sample_positions(n, n, 512)
+        _cmp(_logical_at(got, lda, ri, cj), golden[f"{kind}her_c{ci}"], *fx.RANK_TOL[kind + "her"])
+        _herm_other_triangle_kept(got, a0, n, lda, uplo)
+    for ci, (uplo, n, lda, incx, incy, alpha, gx, gy) in enumerate(fx.HER2_CASES):
+        a0 = fx.hemv_matrix(n, lda, kind)
+        got = oracle.her(kind, uplo, n, alpha, fx.rank_vec(kind, n, incx, gx), incx, a0, lda,
+                         y=fx.rank_vec(kind, n, incy, gy), incy=incy)
+        ri, cj = fx.sample_positions(n, n, 512)
+        _cmp(_logical_at(got, lda, ri, cj), golden[f"{kind}her2_c{ci}"], *fx.RANK_TOL[kind + "her2"])
+        _herm_other_triangle_kept(got, a0, n, lda, uplo)
+
+
+def _herm_other_triangle_kept(got, a0, n, lda, uplo):
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    other = (i > j) if uplo == 0 else (i < j)
+    idx = (i + j * lda)[other]
+    np.testing.assert_array_equal(np.asarray(got)[idx], np.asarray(a0, np.complex128)[idx])
