@@ -759,3 +759,37 @@ HER2_CASES = [
     (1, 9, 12, 2, 3, -0.85 + 0.25j, (0.05, 0.03, -0.02, 0.01), (0.40, -0.02, 0.03, -0.01)),
     (0, 300, 305, 1, 1, 0j, (0.11, 0.01, -0.07, 0.004), (0.08, -0.01, 0.02, 0.003)),
 ]
+
+
+# ---- d/c/z GEMM: dgemm_tests.rs, cgemm_tests.rs, zgemm_tests.rs ------------------
+def gemm_operands_k(kind, op_a, op_b, m, n, k, lda, ldb, ldc):
+    """dgemm_tests.rs:112-114 (the sgemm closed forms in f64);
+    cgemm_tests.rs:136-152 / zgemm_tests.rs:133-149 add the imaginary ramps."""
+    a_rows, a_cols = (m, k) if op_a == 0 else (k, m)
+    b_rows, b_cols = (k, n) if op_b == 0 else (n, k)
+    a = cm_k(kind, a_rows, a_cols, lda, lambda R, i, j: R(0.1) + i * R(0.25) + j * R(0.125),
+             lambda R, i, j: R(-0.05) + i * R(0.20) - j * R(0.075))
+    b = cm_k(kind, b_rows, b_cols, ldb, lambda R, i, j: R(-0.2) + i * R(0.05) - j * R(0.075),
+             lambda R, i, j: R(0.15) - i * R(0.03) + j * R(0.02))
+    c = cm_k(kind, m, n, ldc, lambda R, i, j: R(0.3) - i * R(0.01) + j * R(0.02),
+             lambda R, i, j: R(-0.1) + i * R(0.015) - j * R(0.025))
+    return a, b, c
+
+
+# dgemm_tests.rs:143-186: the four real op pairs for each (alpha, beta), and
+# (C, N) with the first pair and (N, C) with the second.
+DGEMM_CASES = [((oa, ob), ci) for ci in range(4) for (oa, ob) in [(0, 0), (0, 1), (1, 0), (1, 1)]] + \
+    [((2, 0), 0), ((0, 2), 1)]
+DGEMM_COEFFS = GEMM_ALPHA_BETA
+# cgemm_tests.rs:188-223 / zgemm_tests.rs:184-219: nine op pairs x four
+# (alpha, beta)
+CGEMM_OPS = [(0, 0), (0, 1), (1, 0), (1, 1), (0, 2), (1, 2), (2, 0), (2, 1), (2, 2)]
+CGEMM_COEFFS = [(1.0 + 0j, 0j), (0.5 + 0.25j, 1.0 + 0j), (0.75 - 0.25j, -0.5 + 0.3j), (0j, 0.7 - 0.2j)]
+GEMM_TOL = {"d": (1e-12, 1e-12), "c": (3e-3, 2e-3), "z": (3e-11, 2e-11)}  # dgemm:83-84, cgemm:109-110, zgemm:106-107
+
+
+def gemm_cases_k(kind):
+    """((op_a, op_b), (alpha, beta)) pairs of one kind's test file."""
+    if kind == "d":
+        return [(ops, DGEMM_COEFFS[ci]) for ops, ci in DGEMM_CASES]
+    return [(ops, ab) for ab in CGEMM_COEFFS for ops in CGEMM_OPS]

@@ -257,6 +257,19 @@ def main() -> None:
                                                        incy=incy, n=n, a=A.copy()))
             ri, cj = fx.sample_positions(n, n, 512)
             g[f"{kind}her2_c{ci}"] = r[ri, cj]
+    # ---- d/c/z GEMM over every fixture shape: C at fixed positions
+    for kind in "dcz":
+        for si, (m, n, k, lda_n, lda_t, ldb_n, ldb_t, ldc) in enumerate(fx.GEMM_SHAPES):
+            ri, cj = fx.sample_positions(m, n, 64)
+            for ci, ((op_a, op_b), (alpha, beta)) in enumerate(fx.gemm_cases_k(kind)):
+                lda = lda_n if op_a == 0 else lda_t
+                ldb = ldb_n if op_b == 0 else ldb_t
+                a, b, c = fx.gemm_operands_k(kind, op_a, op_b, m, n, k, lda, ldb, ldc)
+                A = logical(a, *((m, k) if op_a == 0 else (k, m)), lda)
+                B = logical(b, *((k, n) if op_b == 0 else (n, k)), ldb)
+                r = getattr(blas, kind + "gemm")(alpha, A, B, beta=beta, c=logical(c, m, n, ldc).copy(),
+                                                 trans_a=op_a, trans_b=op_b)
+                g[f"{kind}gemm_s{si}_c{ci}"] = np.asarray(r)[ri, cj]
     np.savez_compressed(OUT, **g)
     print(f"wrote {len(g)} arrays to {OUT} ({os.path.getsize(OUT)} bytes)")
 

@@ -543,3 +543,19 @@ def _herm_other_triangle_kept(got, a0, n, lda, uplo):
     other = (i > j) if uplo == 0 else (i < j)
     idx = (i + j * lda)[other]
     np.testing.assert_array_equal(np.asarray(got)[idx], np.asarray(a0, np.complex128)[idx])
+
+
+@pytest.mark.parametrize("kind", ["d", "c", "z"])
+def test_gemm_dcz_fixtures(golden, kind):
+    """dgemm/cgemm/zgemm_tests.rs over every fixture shape (including the
+    128^3 and the thin k = 15 panels), every op pair and (alpha, beta) of each
+    file, at each file's tolerance (real and imaginary parts separately)."""
+    rtol, atol = fx.GEMM_TOL[kind]
+    for si, (m, n, k, lda_n, lda_t, ldb_n, ldb_t, ldc) in enumerate(fx.GEMM_SHAPES):
+        ri, cj = fx.sample_positions(m, n, 64)
+        for ci, ((op_a, op_b), (alpha, beta)) in enumerate(fx.gemm_cases_k(kind)):
+            lda = lda_n if op_a == 0 else lda_t
+            ldb = ldb_n if op_b == 0 else ldb_t
+            a, b, c = fx.gemm_operands_k(kind, op_a, op_b, m, n, k, lda, ldb, ldc)
+            got, _ = oracle.gemm_sample(op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ri, cj)
+            _cmp(got, golden[f"{kind}gemm_s{si}_c{ci}"], rtol, atol)
