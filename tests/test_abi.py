@@ -1,7 +1,5 @@
 """The C-ABI library loads and exports every symbol include/coral_b200.h
 declares; the ctypes binding declares each of them.  No compute calls."""
-import ctypes
-import os
 import subprocess
 
 from coral_b200 import _lib

@@ -11,7 +11,6 @@ import socket
 import subprocess
 import sys
 
-import pytest
 import torch.multiprocessing as mp
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
