@@ -168,9 +168,6 @@ k_grouped_plan(const coral_sgemm_problem_t* __restrict__ probs, int count, Group
 
 template <typename TIn> __device__ __forceinline__ float ld_val(const TIn* p);
 template <> __device__ __forceinline__ float ld_val<float>(const float* p) { return __ldg(p); }
-template <> __device__ __forceinline__ float ld_val<__nv_bfloat16>(const __nv_bfloat16* p) {
-  return __bfloat162float(__ldg(p));
-}
 
 // Operand views of one tile's K slab for the producers.
 template <typename TIn>
@@ -191,9 +188,8 @@ __device__ __forceinline__ uint32_t sw64_offset(int r, int kk) {
                                                                            (kk & 7) * 2);
 }
 
-// Eight consecutive values p[0..8) as floats, with one or two 16-byte loads
-// when p is 16-byte aligned (8- and 4-byte pair loads for the other cases
-// measured slower for bf16 inputs).
+// Eight consecutive floats p[0..8), with two 16-byte loads when p is 16-byte
+// aligned (bf16 operands are staged raw by load_share_bf16 instead).
 __device__ __forceinline__ void ld8(const float* p, float* v) {
   if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
     const float4 a = __ldg(reinterpret_cast<const float4*>(p));
@@ -205,22 +201,6 @@ __device__ __forceinline__ void ld8(const float* p, float* v) {
     for (int j = 0; j < 8; ++j) v[j] = __ldg(p + j);
   }
 }
-__device__ __forceinline__ void ld8(const __nv_bfloat16* p, float* v) {
-  if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
-    const uint4 u = __ldg(reinterpret_cast<const uint4*>(p));
-    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const float2 f = __bfloat1622float2(h[j]);
-      v[2 * j] = f.x;
-      v[2 * j + 1] = f.y;
-    }
-  } else {
-#pragma unroll
-    for (int j = 0; j < 8; ++j) v[j] = __bfloat162float(__ldg(p + j));
-  }
-}
-
 // Item e of an operand tile: 8 consecutive K values of one row.  Along K the
 // items run row-major (4 per row: lanes on the chunks of 8 consecutive rows,
 // each item one contiguous 16- or 32-byte segment); along the rows they run
