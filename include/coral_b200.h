@@ -88,6 +88,10 @@ enum {
 typedef struct coral_handle_s* coral_handle_t;
 
 /* ---- handle ------------------------------------------------------------ */
+/* No reference counterpart: CORAL's routines are stateless free functions
+ * (coral-aarch64/src/lib.rs:70-82 exports modules of plain `pub fn`s).  The
+ * handle holds the stream, the device scratch, the status word that bounded
+ * waits set, and the per-handle configuration. */
 coral_status_t coral_create(coral_handle_t* handle);
 coral_status_t coral_destroy(coral_handle_t handle);
 /* `stream` is a cudaStream_t (NULL = legacy default stream). */
