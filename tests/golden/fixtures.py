@@ -793,3 +793,18 @@ def gemm_cases_k(kind):
     if kind == "d":
         return [(ops, DGEMM_COEFFS[ci]) for ops, ci in DGEMM_CASES]
     return [(ops, ab) for ab in CGEMM_COEFFS for ops in CGEMM_OPS]
+
+
+# ---- rank updates applied twice (each file's run_accumulate_twice) -------------
+# real: (m or n, alpha1, alpha2, x1, y1, x2, y2) with ramps (a, b); the ger
+# form is 64 x 48, the syr/syr2 forms 64 x 64 upper (sger/ssyr/ssyr2 and
+# dger/dsyr/dsyr2_tests.rs)
+ACC_REAL = dict(m=64, n=48, alpha=(1.2, -0.7), x1=(0.2, 0.01), y1=(-0.1, 0.02), x2=(-0.3, 0.03), y2=(0.4, -0.01))
+# cger/zger_tests.rs run_accumulate_twice: alphas per form (geru, gerc)
+ACC_CGER = dict(m=64, n=48, alpha={0: (1.20 - 0.30j, -0.70 + 0.15j), 1: (0.60 + 0.40j, -0.70 + 0.20j)},
+                x1=(0.20, 0.01, -0.10, 0.02), y1=(-0.10, 0.02, 0.40, -0.01),
+                x2=(-0.30, 0.03, 0.25, -0.02), y2=(0.40, -0.01, -0.20, 0.03))
+# cher/zher_tests.rs (n = 33, upper) and cher2/zher2_tests.rs (n = 64, upper)
+ACC_HER = dict(n=33, alpha=(1.2, -0.7), x1=(0.20, 0.01, -0.03, 0.005), x2=(-0.30, 0.03, 0.06, -0.004))
+ACC_HER2 = dict(n=64, alpha=(1.20 + 0.30j, -0.70 - 0.20j), x1=(0.20, 0.01, -0.03, 0.005),
+                y1=(-0.10, 0.02, 0.04, -0.003), x2=(-0.30, 0.03, 0.06, -0.004), y2=(0.40, -0.01, -0.02, 0.002))

@@ -270,6 +270,44 @@ def main() -> None:
                 r = getattr(blas, kind + "gemm")(alpha, A, B, beta=beta, c=logical(c, m, n, ldc).copy(),
                                                  trans_a=op_a, trans_b=op_b)
                 g[f"{kind}gemm_s{si}_c{ci}"] = np.asarray(r)[ri, cj]
+    # ---- rank updates applied twice (the reference's run_accumulate_twice)
+    ar = fx.ACC_REAL
+    for kind in "sd":
+        m, n = ar["m"], ar["n"]
+        R = np.float32 if kind == "s" else np.float64
+        A = logical(fx.cm_k(kind, m, n, m, lambda R_, i, j: R_(0.1) + i * R_(0.5) + j * R_(0.25)), m, n, m)
+        for t, (xg, yg) in enumerate(((ar["x1"], ar["y1"]), (ar["x2"], ar["y2"]))):
+            A = getattr(blas, kind + "ger")(ar["alpha"][t], fx.rank_vec(kind, m, 1, xg), fx.rank_vec(kind, n, 1, yg),
+                                            a=np.asarray(A, R).copy())
+        g[f"{kind}ger_acc"] = np.asarray(A, R).ravel(order="F")
+        S_ = logical(fx.syr_matrix(m, m, kind), m, m, m)
+        S2 = S_.copy()
+        for t, (xg, yg) in enumerate(((ar["x1"], ar["y1"]), (ar["x2"], ar["y2"]))):
+            S_ = getattr(blas, kind + "syr")(ar["alpha"][t], fx.rank_vec(kind, m, 1, xg), lower=0, a=np.asarray(S_, R).copy())
+            S2 = getattr(blas, kind + "syr2")(ar["alpha"][t], fx.rank_vec(kind, m, 1, xg), fx.rank_vec(kind, m, 1, yg),
+                                              lower=0, a=np.asarray(S2, R).copy())
+        g[f"{kind}syr_acc"] = np.asarray(S_, R).ravel(order="F")
+        g[f"{kind}syr2_acc"] = np.asarray(S2, R).ravel(order="F")
+    ac, ah, ah2 = fx.ACC_CGER, fx.ACC_HER, fx.ACC_HER2
+    for kind in "cz":
+        m, n = ac["m"], ac["n"]
+        for conj in (0, 1):
+            A = logical(fx.gemv_matrix_k(kind, m, n, m), m, n, m)
+            fn = getattr(blas, kind + ("gerc" if conj else "geru"))
+            for t, (xg, yg) in enumerate(((ac["x1"], ac["y1"]), (ac["x2"], ac["y2"]))):
+                A = fn(ac["alpha"][conj][t], fx.rank_vec(kind, m, 1, xg), fx.rank_vec(kind, n, 1, yg), a=A.copy())
+            g[f"{kind}ger_acc_j{conj}"] = np.asarray(A).ravel(order="F")
+        n = ah["n"]
+        H = logical(fx.hemv_matrix(n, n, kind), n, n, n)
+        for t, xg in enumerate((ah["x1"], ah["x2"])):
+            H = getattr(blas, kind + "her")(ah["alpha"][t], fx.rank_vec(kind, n, 1, xg), lower=0, a=H.copy())
+        g[f"{kind}her_acc"] = np.asarray(H).ravel(order="F")
+        n = ah2["n"]
+        H = logical(fx.hemv_matrix(n, n, kind), n, n, n)
+        for t, (xg, yg) in enumerate(((ah2["x1"], ah2["y1"]), (ah2["x2"], ah2["y2"]))):
+            H = getattr(blas, kind + "her2")(ah2["alpha"][t], fx.rank_vec(kind, n, 1, xg), fx.rank_vec(kind, n, 1, yg),
+                                             lower=0, a=H.copy())
+        g[f"{kind}her2_acc"] = np.asarray(H).ravel(order="F")
     np.savez_compressed(OUT, **g)
     print(f"wrote {len(g)} arrays to {OUT} ({os.path.getsize(OUT)} bytes)")
 

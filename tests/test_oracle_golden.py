@@ -559,3 +559,98 @@ def test_gemm_dcz_fixtures(golden, kind):
             a, b, c = fx.gemm_operands_k(kind, op_a, op_b, m, n, k, lda, ldb, ldc)
             got, _ = oracle.gemm_sample(op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ri, cj)
             _cmp(got, golden[f"{kind}gemm_s{si}_c{ci}"], rtol, atol)
+
+
+def test_rank_updates_applied_twice(golden):
+    """Each rank-update file's run_accumulate_twice: two updates in a row on
+    the same matrix, every entry against BLAS at the file's tolerance."""
+    ar = fx.ACC_REAL
+    m, n = ar["m"], ar["n"]
+    pairs = ((ar["x1"], ar["y1"]), (ar["x2"], ar["y2"]))
+    for kind in "sd":
+        a = fx.cm_k(kind, m, n, m, lambda R, i, j: R(0.1) + i * R(0.5) + j * R(0.25))
+        s1 = fx.syr_matrix(m, m, kind)
+        s2 = s1.copy()
+        for t, (xg, yg) in enumerate(pairs):
+            x, y = fx.rank_vec(kind, m, 1, xg), fx.rank_vec(kind, n, 1, yg)
+            xs, ys = x, fx.rank_vec(kind, m, 1, yg)
+            if kind == "s":
+                a = oracle.sger(m, n, ar["alpha"][t], x, 1, y, 1, a, m)
+                s1 = oracle.ssyr(0, m, ar["alpha"][t], xs, 1, s1, m)
+                s2 = oracle.ssyr2(0, m, ar["alpha"][t], xs, 1, ys, 1, s2, m)
+            else:
+                a = oracle.dger(m, n, ar["alpha"][t], x, 1, y, 1, a, m)
+                s1 = oracle.dsyr(0, m, ar["alpha"][t], xs, 1, s1, m)
+                s2 = oracle.dsyr(0, m, ar["alpha"][t], xs, 1, s2, m, y=ys, incy=1)
+        _cmp(a, golden[f"{kind}ger_acc"], *fx.RANK_TOL[kind + "ger"])
+        _cmp(s1, golden[f"{kind}syr_acc"], *fx.RANK_TOL[kind + "syr"])
+        _cmp(s2, golden[f"{kind}syr2_acc"], *fx.RANK_TOL[kind + "syr2"])
+    ac, ah, ah2 = fx.ACC_CGER, fx.ACC_HER, fx.ACC_HER2
+    for kind in "cz":
+        for conj in (0, 1):
+            a = fx.gemv_matrix_k(kind, m, n, m)
+            for t, (xg, yg) in enumerate(((ac["x1"], ac["y1"]), (ac["x2"], ac["y2"]))):
+                a = oracle.gerc_u(kind, conj, m, n, ac["alpha"][conj][t], fx.rank_vec(kind, m, 1, xg), 1,
+                                  fx.rank_vec(kind, n, 1, yg), 1, a, m)
+            _cmp(a, golden[f"{kind}ger_acc_j{conj}"], *fx.RANK_TOL[kind + "ger"])
+        nh = ah["n"]
+        h = fx.hemv_matrix(nh, nh, kind)
+        for t, xg in enumerate((ah["x1"], ah["x2"])):
+            h = oracle.her(kind, 0, nh, ah["alpha"][t], fx.rank_vec(kind, nh, 1, xg), 1, h, nh)
+        _cmp(h, golden[f"{kind}her_acc"], *fx.RANK_TOL[kind + "her"])
+        nh = ah2["n"]
+        h = fx.hemv_matrix(nh, nh, kind)
+        for t, (xg, yg) in enumerate(((ah2["x1"], ah2["y1"]), (ah2["x2"], ah2["y2"]))):
+            h = oracle.her(kind, 0, nh, ah2["alpha"][t], fx.rank_vec(kind, nh, 1, xg), 1, h, nh,
+                           y=fx.rank_vec(kind, nh, 1, yg), incy=1)
+        _cmp(h, golden[f"{kind}her2_acc"], *fx.RANK_TOL[kind + "her2"])
+
+
+def _mirror(au, al, n, lda, conj, rtol, atol):
+    """assert_upper_lower_equal(_c): upper (i, j), i <= j, against lower
+    (j, i) -- conjugated for the Hermitian forms."""
+    i, j = np.nonzero(np.triu(np.ones((n, n), bool)))
+    up = np.asarray(au)[i + j * lda]
+    lo = np.asarray(al)[j + i * lda]
+    _cmp(up, np.conj(lo) if conj else lo, rtol, atol)
+
+
+@pytest.mark.parametrize("real,cplx", [("s", "c"), ("d", "z")])
+def test_rank_updates_upper_equals_lower(real, cplx):
+    """ssyr/ssyr2/cher/cher2_tests.rs run_upper_equals_lower (and the d/z
+    files): on a full symmetric / Hermitian matrix the upper and the lower
+    update are mirror images."""
+    n = 33
+    x = fx.rank_vec(real, n, 1, (0.2, 0.005))
+    y = fx.rank_vec(real, n, 1, (0.1, 0.004))
+    a = fx.syr_matrix(n, n, real)
+    if real == "s":
+        up, lo = oracle.ssyr(0, n, 0.77, x, 1, a, n), oracle.ssyr(1, n, 0.77, x, 1, a, n)
+        up2, lo2 = oracle.ssyr2(0, n, 0.77, x, 1, y, 1, a, n), oracle.ssyr2(1, n, 0.77, x, 1, y, 1, a, n)
+    else:
+        up, lo = oracle.dsyr(0, n, 0.77, x, 1, a, n), oracle.dsyr(1, n, 0.77, x, 1, a, n)
+        up2 = oracle.dsyr(0, n, 0.77, x, 1, a, n, y=y, incy=1)
+        lo2 = oracle.dsyr(1, n, 0.77, x, 1, a, n, y=y, incy=1)
+    _mirror(up, lo, n, n, False, *fx.RANK_TOL[real + "syr"])
+    _mirror(up2, lo2, n, n, False, *fx.RANK_TOL[real + "syr2"])
+    nh = 25
+    xh = fx.rank_vec(cplx, nh, 1, (0.2, 0.005, -0.04, 0.002))
+    h = fx.hemv_matrix(nh, nh, cplx)
+    _mirror(oracle.her(cplx, 0, nh, 0.77, xh, 1, h, nh), oracle.her(cplx, 1, nh, 0.77, xh, 1, h, nh), nh, nh, True,
+            *fx.RANK_TOL[cplx + "her"])
+    x2 = fx.rank_vec(cplx, n, 1, (0.2, 0.005, -0.04, 0.002))
+    y2 = fx.rank_vec(cplx, n, 1, (0.1, 0.004, 0.03, -0.001))
+    h2 = fx.hemv_matrix(n, n, cplx)
+    _mirror(oracle.her(cplx, 0, n, 0.77 + 0.11j, x2, 1, h2, n, y=y2, incy=1),
+            oracle.her(cplx, 1, n, 0.77 + 0.11j, x2, 1, h2, n, y=y2, incy=1), n, n, True, *fx.RANK_TOL[cplx + "her2"])
+
+
+def test_rank_and_trmv_quick_returns():
+    """The quick-return cases of sger/ssyr/strmv_tests.rs (m = 0 or n = 0):
+    nothing is written."""
+    a = np.zeros(5, np.float32)
+    np.testing.assert_array_equal(oracle.sger(0, 5, 0.77, np.ones(1, np.float32), 1,
+                                              fx.rank_vec("s", 5, 1, (0.2, 0.1)), 1, a, 1), a)
+    np.testing.assert_array_equal(oracle.ssyr(0, 0, 0.55, np.zeros(1, np.float32), 1, np.zeros(1, np.float32), 1),
+                                  np.zeros(1, np.float32))
+    assert oracle.strmv(0, 0, 1, 0, np.zeros(1, np.float32), 1, np.zeros(1, np.float32), 1).size == 0
