@@ -619,16 +619,16 @@ def set_diag(kind, a, n, lda, f):
 def trmv_matrix_k(kind, n, lda, uplo, diag):
     """dtrmv_tests.rs:63-176 (the strmv closed forms in f64);
     ctrmv_tests.rs / ztrmv_tests.rs:63-155, 215-242 build_matrix."""
-    if kind == "d":
-        R = np.float64
+    if kind in "sd":
+        R = _real(kind)
         f = (lambda i, j: R(0.2) + i * R(0.3) + j * R(0.15)) if uplo == 0 else \
             (lambda i, j: R(-0.1) + i * R(0.25) - j * R(0.2))
-        a = cm_k("d", n, n, lda, lambda R_, i, j: f(i, j))
+        a = cm_k(kind, n, n, lda, lambda R_, i, j: f(i, j))
         r, c = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
         keep = (r <= c) if uplo == 0 else (r >= c)
         a[(r + c * lda)[~keep]] = 0.0
         if diag == 0:
-            set_diag("d", a, n, lda, (lambda R_, i: R_(7.5) + i * R_(0.1)) if uplo == 0 else
+            set_diag(kind, a, n, lda, (lambda R_, i: R_(7.5) + i * R_(0.1)) if uplo == 0 else
                      (lambda R_, i: R_(-9.0) + i * R_(0.05)))
         return a
     return _ctri(kind, n, lda, uplo, diag, trsv=False)
@@ -658,8 +658,8 @@ def _ctri(kind, n, lda, uplo, diag, trsv):
 
 
 def trmv_x_k(kind, n, inc):
-    if kind == "d":
-        return rvec("d", n, inc, lambda R, k: R(0.1) + R(0.2) * k)
+    if kind in "sd":
+        return rvec(kind, n, inc, lambda R, k: R(0.1) + R(0.2) * k)
     return cvec(kind, n, inc, lambda R, k: R(0.1) + R(0.2) * k, lambda R, k: R(-0.05) + R(0.03) * k)
 
 
@@ -672,22 +672,23 @@ TRMV_DCZ = {
 
 
 def trsv_matrix_k(kind, n, lda, uplo, diag):
-    """dtrsv_tests.rs:64-166, 216-241 build_matrix; c/z: ctrsv/ztrsv_tests.rs
-    91-183, 244-272."""
-    if kind != "d":
+    """strsv_tests.rs / dtrsv_tests.rs:64-166, 216-241 build_matrix (unit
+    calls get make_upper_unit / make_lower_unit with a planted diagonal);
+    c/z: ctrsv/ztrsv_tests.rs 91-183, 244-272."""
+    if kind in "cz":
         return _ctri(kind, n, lda, uplo, diag, trsv=True)
     if diag == 1:
-        return tri_fill("d", n, lda, uplo, lambda R, i: R(1.0) + R(0.02) * i, lambda R, d: R(0.01) / (R(1.0) + d))
+        return tri_fill(kind, n, lda, uplo, lambda R, i: R(1.0) + R(0.02) * i, lambda R, d: R(0.01) / (R(1.0) + d))
     if uplo == 0:
-        a = tri_fill("d", n, lda, 0, lambda R, i: R(1.0) + R(0.05) * i, lambda R, d: R(5e-4) * (R(1.0) + d))
-        return set_diag("d", a, n, lda, lambda R, i: R(7.5) + i * R(0.1))
-    a = tri_fill("d", n, lda, 1, lambda R, i: R(1.0) - R(0.03) * i, lambda R, d: R(6e-4) * (R(1.0) + d))
-    return set_diag("d", a, n, lda, lambda R, i: R(-9.0) + i * R(0.05))
+        a = tri_fill(kind, n, lda, 0, lambda R, i: R(1.0) + R(0.05) * i, lambda R, d: R(5e-4) * (R(1.0) + d))
+        return set_diag(kind, a, n, lda, lambda R, i: R(7.5) + i * R(0.1))
+    a = tri_fill(kind, n, lda, 1, lambda R, i: R(1.0) - R(0.03) * i, lambda R, d: R(6e-4) * (R(1.0) + d))
+    return set_diag(kind, a, n, lda, lambda R, i: R(-9.0) + i * R(0.05))
 
 
 def trsv_x_k(kind, n, inc):
-    if kind == "d":
-        return rvec("d", n, inc, lambda R, k: R(0.05) + R(0.01) * k)
+    if kind in "sd":
+        return rvec(kind, n, inc, lambda R, k: R(0.05) + R(0.01) * k)
     return cvec(kind, n, inc, lambda R, k: R(0.1) + R(0.2) * k, lambda R, k: R(-0.05) + R(0.03) * k)
 
 
@@ -808,3 +809,49 @@ ACC_CGER = dict(m=64, n=48, alpha={0: (1.20 - 0.30j, -0.70 + 0.15j), 1: (0.60 + 
 ACC_HER = dict(n=33, alpha=(1.2, -0.7), x1=(0.20, 0.01, -0.03, 0.005), x2=(-0.30, 0.03, 0.06, -0.004))
 ACC_HER2 = dict(n=64, alpha=(1.20 + 0.30j, -0.70 - 0.20j), x1=(0.20, 0.01, -0.03, 0.005),
                 y1=(-0.10, 0.02, 0.04, -0.003), x2=(-0.30, 0.03, 0.06, -0.004), y2=(0.40, -0.01, -0.02, 0.002))
+
+
+# ---- the triangular files' single-case tests -------------------------------------
+def padded_k(kind, n, lda, trsv):
+    """Both triangles populated: strsv/dtrsv make_padded (diagonal
+    1 + 0.02 i, 0.01 / (1 + d) off it), ctrsv/ztrsv make_padded_c32, and for
+    the multiply tests strmv/dtrmv make_padded_col_major (lower
+    0.1 + 0.2 i + 0.1 j, upper 0.1 + 0.1 i + 0.2 j)."""
+    R = _real(kind)
+    if not trsv:
+        return cm_k(kind, n, n, lda, lambda R_, i, j: np.where(i >= j, R_(0.1) + i * R_(0.2) + j * R_(0.1),
+                                                                R_(0.1) + i * R_(0.1) + j * R_(0.2)))
+    a = np.zeros(lda * n, _DT[kind])
+    for j in range(n):
+        i = np.arange(n)
+        d = np.abs(i - j).astype(R)
+        ii = i.astype(R)
+        re = np.where(i == j, R(1.0) + R(0.02) * ii, R(0.01) / (R(1.0) + d))
+        if kind in "sd":
+            a[j * lda:j * lda + n] = re
+            continue
+        im = np.where(i == j, R(0.01) - R(0.005) * ii,
+                      np.where(i < j, R(-0.008) / (R(1.0) + d), R(0.007) / (R(1.0) + d)))
+        col = np.empty(n, _DT[kind])
+        col.real, col.imag = re, im
+        a[j * lda:j * lda + n] = col
+    return a
+
+
+def tri_special_cases(kind, trsv):
+    """(name, uplo, trans, diag, n, lda, a, x) of lower_transpose_padded /
+    padded_lower_transpose, and for strsv/dtrsv unitdiag_upper_notranspose
+    and unitdiag_lower_transpose."""
+    if kind in "sd":
+        lda = 132
+        x = rvec(kind, 127, 1, lambda R, k: R(0.3) - R(0.006) * k)
+    else:
+        lda = 134
+        x = cvec(kind, 127, 1, lambda R, k: R(0.3) - R(0.006) * k, lambda R, k: R(-0.12) + R(0.003) * k)
+    out = [("ltp", 1, 1, 1, 127, lda, padded_k(kind, 127, lda, trsv), x)]
+    if trsv and kind in "sd":
+        out.append(("uun", 0, 0, 0, 40, 40, trsv_matrix_k(kind, 40, 40, 0, 0),
+                    rvec(kind, 40, 1, lambda R, k: R(0.2) + R(0.01) * k)))
+        out.append(("lut", 1, 1, 0, 48, 48, trsv_matrix_k(kind, 48, 48, 1, 0),
+                    rvec(kind, 48, 1, lambda R, k: R(-0.1) + R(0.02) * k)))
+    return out

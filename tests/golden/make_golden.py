@@ -308,6 +308,40 @@ def main() -> None:
             H = getattr(blas, kind + "her2")(ah2["alpha"][t], fx.rank_vec(kind, n, 1, xg), fx.rank_vec(kind, n, 1, yg),
                                              lower=0, a=H.copy())
         g[f"{kind}her2_acc"] = np.asarray(H).ravel(order="F")
+    # ---- STRSV on the reference's own unit-diagonal matrices, and the
+    # triangular files' single-case tests
+    for si, (n, lda, incs) in enumerate(fx.TRSV_SHAPES):
+        for uplo in (0, 1):
+            A = logical(fx.trsv_matrix_k("s", n, lda, uplo, 0), n, n, lda)
+            for inc in incs:
+                x = fx.trsv_x_k("s", n, inc)
+                for trans in (0, 1):
+                    r = blas.strsv(A, x.copy(), incx=inc, lower=uplo, trans=trans, diag=1)
+                    g[f"strsv_unit_s{si}_u{uplo}_i{inc}_t{trans}"] = S(np.asarray(r, np.float32)[::inc][:n])
+    for kind in "sdcz":
+        for name, uplo, trans, diag, n, lda, a, x in fx.tri_special_cases(kind, True):
+            r = getattr(blas, kind + "trsv")(logical(a, n, n, lda), x.copy(), lower=uplo, trans=trans,
+                                             diag=1 if diag == 0 else 0)
+            g[f"{kind}trsv_sp_{name}"] = S(np.asarray(r))
+    for kind in "sd":
+        for name, uplo, trans, diag, n, lda, a, x in fx.tri_special_cases(kind, False):
+            r = getattr(blas, kind + "trmv")(logical(a, n, n, lda), x.copy(), lower=uplo, trans=trans,
+                                             diag=1 if diag == 0 else 0)
+            g[f"{kind}trmv_sp_{name}"] = S(np.asarray(r))
+    # ---- SGEMM on the larger fixture shapes (128^3 and the k = 15 panels)
+    for si in range(3, len(fx.GEMM_SHAPES)):
+        m, n, k, lda_n, lda_t, ldb_n, ldb_t, ldc = fx.GEMM_SHAPES[si]
+        ri, cj = fx.sample_positions(m, n, 64)
+        for (op_a, op_b) in [(0, 0), (0, 1), (1, 0), (1, 1), (2, 0), (0, 2)]:
+            lda = lda_n if op_a == 0 else lda_t
+            ldb = ldb_n if op_b == 0 else ldb_t
+            a, b, c = fx.gemm_operands(op_a, op_b, m, n, k, lda, ldb, ldc)
+            A = logical(a, *((m, k) if op_a == 0 else (k, m)), lda)
+            B = logical(b, *((k, n) if op_b == 0 else (n, k)), ldb)
+            for ci, (alpha, beta) in enumerate(fx.GEMM_ALPHA_BETA):
+                r = blas.sgemm(alpha, A, B, beta=beta, c=logical(c, m, n, ldc).copy(), trans_a=int(op_a != 0),
+                               trans_b=int(op_b != 0))
+                g[f"sgemm_big_s{si}_{op_a}{op_b}_c{ci}"] = np.asarray(r, np.float32)[ri, cj]
     np.savez_compressed(OUT, **g)
     print(f"wrote {len(g)} arrays to {OUT} ({os.path.getsize(OUT)} bytes)")
 

@@ -654,3 +654,84 @@ def test_rank_and_trmv_quick_returns():
     np.testing.assert_array_equal(oracle.ssyr(0, 0, 0.55, np.zeros(1, np.float32), 1, np.zeros(1, np.float32), 1),
                                   np.zeros(1, np.float32))
     assert oracle.strmv(0, 0, 1, 0, np.zeros(1, np.float32), 1, np.zeros(1, np.float32), 1).size == 0
+
+
+def test_strsv_reference_unit_matrices(golden):
+    """strsv_tests.rs run_all with build_matrix's unit-diagonal matrices
+    (make_upper_unit / make_lower_unit with a planted diagonal that a unit
+    call must ignore), at 1e-4 (strsv_tests.rs:213-214)."""
+    for si, (n, lda, incs) in enumerate(fx.TRSV_SHAPES):
+        for uplo in (0, 1):
+            a = fx.trsv_matrix_k("s", n, lda, uplo, 0)
+            for inc in incs:
+                x = fx.trsv_x_k("s", n, inc)
+                for trans in (0, 1):
+                    got = oracle.strsv(uplo, trans, 0, n, a, lda, x, inc)
+                    _cmp(_S(got), golden[f"strsv_unit_s{si}_u{uplo}_i{inc}_t{trans}"], 1e-4, 1e-4)
+
+
+TRI_TOL = {"strsv": (1e-4, 1e-4), "dtrsv": (1e-12, 1e-12), "ctrsv": (1e-2, 1e-3), "ztrsv": (1e-11, 1e-11),
+           "strmv": (1e-5, 1e-5), "dtrmv": (1e-13, 1e-13)}
+
+
+@pytest.mark.parametrize("kind", ["s", "d", "c", "z"])
+def test_triangular_single_cases(golden, kind):
+    """lower_transpose_padded (both triangles populated, lda > n),
+    unitdiag_upper_notranspose and unitdiag_lower_transpose of
+    {s,d,c,z}trsv_tests.rs, padded_lower_transpose of {s,d}trmv_tests.rs,
+    and the n = 0 quick returns."""
+    for name, uplo, trans, diag, n, lda, a, x in fx.tri_special_cases(kind, True):
+        got = (oracle.strsv(uplo, trans, diag, n, a, lda, x, 1) if kind == "s"
+               else oracle.trsv_dcz(kind, uplo, trans, diag, n, a, lda, x, 1))
+        _cmp(_S(got), golden[f"{kind}trsv_sp_{name}"], *TRI_TOL[kind + "trsv"])
+    if kind in "sd":
+        for name, uplo, trans, diag, n, lda, a, x in fx.tri_special_cases(kind, False):
+            got = getattr(oracle, kind + "trmv")(uplo, trans, diag, n, a, lda, x, 1)
+            _cmp(_S(got), golden[f"{kind}trmv_sp_{name}"], *TRI_TOL[kind + "trmv"])
+    z = np.zeros(2, fx._DT[kind])
+    solve = (oracle.strsv(0, 0, 1, 0, z, 1, z, 1) if kind == "s" else oracle.trsv_dcz(kind, 0, 0, 1, 0, z, 1, z, 1))
+    assert solve.size == 0
+
+
+@pytest.mark.parametrize("si", range(3, len(fx.GEMM_SHAPES)))
+def test_sgemm_larger_fixtures(golden, si):
+    """sgemm_tests.rs medium_square_all_ops (128^3) and rectangular_all_ops
+    (k = 15 panels), C at 64 fixed positions, at the reference's 1e-3
+    (sgemm_tests.rs:85-86): at k = 128 the ramps cancel, and OpenBLAS's fp32
+    sums then sit about 1.5e-5 from the exact values the oracle gives."""
+    m, n, k, lda_n, lda_t, ldb_n, ldb_t, ldc = fx.GEMM_SHAPES[si]
+    ri, cj = fx.sample_positions(m, n, 64)
+    for (op_a, op_b) in [(0, 0), (0, 1), (1, 0), (1, 1), (2, 0), (0, 2)]:
+        lda = lda_n if op_a == 0 else lda_t
+        ldb = ldb_n if op_b == 0 else ldb_t
+        a, b, c = fx.gemm_operands(op_a, op_b, m, n, k, lda, ldb, ldc)
+        for ci, (alpha, beta) in enumerate(fx.GEMM_ALPHA_BETA):
+            got, _ = oracle.gemm_sample(op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ri, cj)
+            _cmp(got, golden[f"sgemm_big_s{si}_{op_a}{op_b}_c{ci}"], 1e-3, 1e-3)
+
+
+@pytest.mark.parametrize("kind", ["d", "c", "z"])
+def test_symv_hemv_upper_equals_lower(kind):
+    """dsymv_tests.rs (n = 513) and chemv/zhemv_tests.rs (n = 257)
+    upper_equals_lower: on a full symmetric / Hermitian matrix both
+    triangles give the same y."""
+    if kind == "d":
+        n = 513
+        a = fx.symv_matrix(n, n, "d")
+        x = fx.rvec("d", n, 1, lambda R, k: R(-0.07) + R(0.013) * k)
+        y = fx.rvec("d", n, 1, lambda R, k: R(0.02) - R(0.004) * k)
+        up = oracle.dsymv(0, n, 1.123, a, n, x, 1, -0.321, y, 1)
+        lo = oracle.dsymv(1, n, 1.123, a, n, x, 1, -0.321, y, 1)
+        _cmp(up, lo, 1e-13, 1e-13)
+        return
+    n = 257
+    a = fx.hemv_matrix(n, n, kind)
+    x = fx.cvec(kind, n, 1, lambda R, k: R(-0.07) + R(0.013) * k, lambda R, k: R(0.015) - R(0.002) * k)
+    y = fx.cvec(kind, n, 1, lambda R, k: R(0.02) - R(0.004) * k, lambda R, k: R(-0.01) + R(0.001) * k)
+    al, be = 1.123 - 0.321j, -0.321 + 0.777j
+    if kind == "c":
+        f = lambda u: oracle.chemv(u, n, _pair(al), a.view(np.float32), n, x.view(np.float32), 1,  # noqa: E731
+                                   _pair(be), y.view(np.float32), 1)
+        _cmp(f(0), f(1), 1e-5, 1e-6)
+    else:
+        _cmp(oracle.zhemv(0, n, al, a, n, x, 1, be, y, 1), oracle.zhemv(1, n, al, a, n, x, 1, be, y, 1), 1e-12, 1e-12)
