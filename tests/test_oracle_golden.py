@@ -735,3 +735,26 @@ def test_symv_hemv_upper_equals_lower(kind):
         _cmp(f(0), f(1), 1e-5, 1e-6)
     else:
         _cmp(oracle.zhemv(0, n, al, a, n, x, 1, be, y, 1), oracle.zhemv(1, n, al, a, n, x, 1, be, y, 1), 1e-12, 1e-12)
+
+
+@pytest.mark.parametrize("n,incx,incy", [(1024, 1, 1), (777, 3, 2), (0, 1, 1), (1, 5, 7)])
+def test_scopy_sswap_bitwise(n, incx, incy):
+    """copy_tests.rs / swap_tests.rs (real f32 cases): the strided copy and
+    swap move every bit, NaN payloads and -0.0 included; elements between
+    the strided positions are untouched."""
+    rng = np.random.default_rng(n + incx)
+    lx, ly = max((n - 1) * incx + 1, 1), max((n - 1) * incy + 1, 1)
+    bits = rng.integers(0, 2**32, lx + ly, dtype=np.uint64).astype(np.uint32)
+    bits[::7] = 0x7FC01234       # a NaN with a payload
+    bits[3::11] = 0x80000000     # -0.0
+    x, y = bits[:lx].view(np.float32).copy(), bits[lx:].view(np.float32).copy()
+    want_y = y.copy()
+    if n:
+        want_y[: (n - 1) * incy + 1: incy] = x[: (n - 1) * incx + 1: incx]
+    np.testing.assert_array_equal(oracle.scopy(n, x, incx, y, incy).view(np.uint32), want_y.view(np.uint32))
+    sx, sy = oracle.sswap(n, x, incx, y, incy)
+    want_x = x.copy()
+    if n:
+        want_x[: (n - 1) * incx + 1: incx] = y[: (n - 1) * incy + 1: incy]
+    np.testing.assert_array_equal(sx.view(np.uint32), want_x.view(np.uint32))
+    np.testing.assert_array_equal(sy.view(np.uint32), want_y.view(np.uint32))
