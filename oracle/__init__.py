@@ -170,7 +170,9 @@ def _vec(kind, a, copy=False):
 
 
 def axpy(kind, n, alpha, x, incx, y, incy):
-    """d/c/z axpy (bit-exact restatement) on a copy of y; returns it."""
+    """s/d/c/z axpy (bit-exact restatement) on a copy of y; returns it."""
+    if kind == "s":
+        return saxpy(n, float(np.float32(alpha)), x, incx, y, incy)
     al = np.array([complex(alpha).real, complex(alpha).imag], np.float64)
     x, px = _vec(kind, x)
     y, py = _vec(kind, y, copy=True)
@@ -179,7 +181,9 @@ def axpy(kind, n, alpha, x, incx, y, incy):
 
 
 def scal(kind, n, alpha, x, incx, real_alpha=False):
-    """d/c/z scal, or csscal / zdscal with real_alpha (bit-exact); returns a copy."""
+    """s/d/c/z scal, or csscal / zdscal with real_alpha (bit-exact); returns a copy."""
+    if kind == "s":
+        return sscal(n, float(np.float32(alpha)), x, incx)
     al = np.array([complex(alpha).real, complex(alpha).imag], np.float64)
     x, px = _vec(kind, x, copy=True)
     k = _KIND[kind][0]
@@ -241,6 +245,8 @@ def rotmg(kind, d1, d2, x1, y1):
 
 
 def iamax(kind, n, x, incx) -> int:
+    if kind == "s":
+        return isamax(n, x, incx)
     x, px = _vec(kind, x)
     return int(lib().or_iamax_exact(_KIND[kind][0], n, px, incx))
 

@@ -273,6 +273,30 @@ L1_CASES = [
          y=(-0.75, 0.05), src="rot_tests.rs:1181-1194"),
 ]
 
+# The f32 cases of the level-1 files' `real` tests, checked against the oracle
+# only (golden keys l1s_c<i>).
+L1_S_CASES = [
+    dict(fn="axpy", kind="s", n=1024, incx=1, incy=1, alpha=3.1415926, x=(0.05, 0.03), y=(0.10, 0.06),
+         src="axpy_tests.rs real, n = 1024"),
+    dict(fn="axpy", kind="s", n=777, incx=3, incy=2, alpha=-0.75, x=(0.2, -0.001), y=(-0.3, 0.002),
+         src="axpy_tests.rs real, n = 777 strided"),
+    dict(fn="axpy", kind="s", n=0, incx=1, incy=1, alpha=1.23, x=(0.0, 0.0), y=(0.0, 0.0),
+         src="axpy_tests.rs real, n = 0"),
+    dict(fn="scal", kind="s", n=1024, incx=1, alpha=3.1415926, x=(0.05, 0.03), src="scal_tests.rs real, n = 1024"),
+    dict(fn="scal", kind="s", n=777, incx=3, alpha=-0.75, x=(0.2, -0.001), src="scal_tests.rs real, n = 777"),
+    dict(fn="scal", kind="s", n=4096, incx=1, alpha=0.0, x=(-0.2, 0.001), src="scal_tests.rs real, alpha = 0"),
+    dict(fn="scal", kind="s", n=257, incx=1, alpha=1.0, x=(-0.3, 0.01), src="scal_tests.rs real, alpha = 1"),
+    dict(fn="dotu", kind="s", n=1024, incx=1, incy=1, x=(0.05, 0.03), y=(-0.3, 0.002),
+         src="dot_tests.rs real, n = 1024"),
+    dict(fn="dotu", kind="s", n=777, incx=3, incy=2, x=(0.2, -0.001), xalt=True, y=(-0.3, 0.002),
+         src="dot_tests.rs real, n = 777 alternating"),
+    dict(fn="dotu", kind="s", n=1, incx=5, incy=7, x=(3.14159, 0.0), y=(-2.71828, 0.0),
+         src="dot_tests.rs real, n = 1"),
+    dict(fn="nrm2", kind="s", n=1024, incx=1, x=(0.05, 0.03), src="nrm2_tests.rs real, n = 1024"),
+    dict(fn="nrm2", kind="s", n=777, incx=3, x=(0.2, -0.001), xalt=True, src="nrm2_tests.rs real, n = 777"),
+    dict(fn="nrm2", kind="s", n=1, incx=5, x=(-3.14159, 0.0), src="nrm2_tests.rs real, n = 1"),
+]
+
 # rot_tests.rs:455-715: (a, b) of the srotg (first four) and drotg (last four)
 # cases; both precisions run all eight here
 ROTG_CASES = [(3.5, -2.25), (0.0, 5.0), (-4.0, 0.0), (-1.25, -7.5), (12.0, -0.75), (0.0, 3.0), (-5.0, 0.0),

@@ -113,6 +113,8 @@ def main() -> None:
     # ---- double and complex level 1 (tests/level1/*.rs fixture ramps)
     for ci, case in enumerate(fx.L1_CASES):
         g[f"l1_c{ci}"] = l1_reference(case)
+    for ci, case in enumerate(fx.L1_S_CASES):
+        g[f"l1s_c{ci}"] = l1_reference(case)
     for ci, (a, b) in enumerate(fx.ROTG_CASES):
         for kind in "sd":
             c, s = getattr(blas, kind + "rotg")(a, b)

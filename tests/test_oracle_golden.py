@@ -176,10 +176,10 @@ def l1_tol(case):
     return 1e-12, 1e-12
 
 
-@pytest.mark.parametrize("ci", range(len(fx.L1_CASES)))
-def test_l1_dcz_fixtures(golden, ci):
-    case = fx.L1_CASES[ci]
-    got, want = oracle_l1(case), golden[f"l1_c{ci}"]
+@pytest.mark.parametrize("key,case", [(f"l1_c{i}", c) for i, c in enumerate(fx.L1_CASES)] +
+                         [(f"l1s_c{i}", c) for i, c in enumerate(fx.L1_S_CASES)])
+def test_l1_dcz_fixtures(golden, key, case):
+    got, want = oracle_l1(case), golden[key]
     if case["fn"] == "iamax":
         assert int(got[0]) == int(want[0]), case["src"]
         return
