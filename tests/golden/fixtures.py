@@ -879,3 +879,25 @@ def tri_special_cases(kind, trsv):
         out.append(("lut", 1, 1, 0, 48, 48, trsv_matrix_k(kind, 48, 48, 1, 0),
                     rvec(kind, 48, 1, lambda R, k: R(-0.1) + R(0.02) * k)))
     return out
+
+
+# Edge shapes of the level-1 files (n = 0, and n = 1 with increments past 1),
+# for every kind and routine, checked against the oracle only (golden keys
+# l1e_c<i>): a one-element vector of 3.14159 (x) and -2.71828 (y).
+L1_EDGE_CASES = []
+for _k in "sdcz":
+    _x = (3.14159, 0.0) if _k in "sd" else (3.14159, 0.0, -0.5, 0.0)
+    _y = (-2.71828, 0.0) if _k in "sd" else (-2.71828, 0.0, 0.25, 0.0)
+    for _n, _ix, _iy in ((0, 1, 1), (1, 5, 7)):
+        _src = f"level-1 edge, n = {_n}"
+        L1_EDGE_CASES += [
+            dict(fn="axpy", kind=_k, n=_n, incx=_ix, incy=_iy, alpha=1.23 if _k in "sd" else 1.23 - 0.5j, x=_x, y=_y,
+                 src=_src),
+            dict(fn="scal", kind=_k, n=_n, incx=_ix, alpha=1.23 if _k in "sd" else 1.23 - 0.5j, x=_x, src=_src),
+            dict(fn="dotu", kind=_k, n=_n, incx=_ix, incy=_iy, x=_x, y=_y, src=_src),
+            dict(fn="asum", kind=_k, n=_n, incx=_ix, x=_x, src=_src),
+            dict(fn="nrm2", kind=_k, n=_n, incx=_ix, x=_x, src=_src),
+            dict(fn="iamax", kind=_k, n=_n, incx=_ix, x=_x, src=_src),
+        ]
+        if _k in "cz":
+            L1_EDGE_CASES.append(dict(fn="dotc", kind=_k, n=_n, incx=_ix, incy=_iy, x=_x, y=_y, src=_src))

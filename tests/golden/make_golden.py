@@ -115,6 +115,11 @@ def main() -> None:
         g[f"l1_c{ci}"] = l1_reference(case)
     for ci, case in enumerate(fx.L1_S_CASES):
         g[f"l1s_c{ci}"] = l1_reference(case)
+    for ci, case in enumerate(fx.L1_EDGE_CASES):
+        # BLAS's i?amax reports -1 for n = 0; the reference returns 0
+        # (isamax.rs:43-151)
+        g[f"l1e_c{ci}"] = (np.array([0], np.int64) if case["fn"] == "iamax" and case["n"] == 0
+                           else l1_reference(case))
     for ci, (a, b) in enumerate(fx.ROTG_CASES):
         for kind in "sd":
             c, s = getattr(blas, kind + "rotg")(a, b)

@@ -177,7 +177,8 @@ def l1_tol(case):
 
 
 @pytest.mark.parametrize("key,case", [(f"l1_c{i}", c) for i, c in enumerate(fx.L1_CASES)] +
-                         [(f"l1s_c{i}", c) for i, c in enumerate(fx.L1_S_CASES)])
+                         [(f"l1s_c{i}", c) for i, c in enumerate(fx.L1_S_CASES)] +
+                         [(f"l1e_c{i}", c) for i, c in enumerate(fx.L1_EDGE_CASES)])
 def test_l1_dcz_fixtures(golden, key, case):
     got, want = oracle_l1(case), golden[key]
     if case["fn"] == "iamax":
