@@ -14,6 +14,7 @@
 #include "common.cuh"
 
 #include <algorithm>
+#include <climits>
 
 #include <cmath>
 #include <mutex>
@@ -624,10 +625,17 @@ coral_status_t coral_set_gemm_tile(coral_handle_t hh, int tile_m, int tile_n, in
   return CORAL_OK;
 }
 
+// Shapes whose sides do not fit an int have no configuration (the GEMM entry
+// points report those sizes as not supported).
+static bool shape_fits(size_t m, size_t n, size_t k) {
+  return m <= (size_t)INT_MAX && n <= (size_t)INT_MAX && k <= (size_t)INT_MAX;
+}
+
 coral_status_t coral_get_gemm_tile(coral_handle_t hh, int products, int op_a, int op_b, size_t m,
                                    size_t n, size_t k, int* tile_m, int* tile_n, int* split_k) {
   CORAL_HANDLE(hh);
   if (products != 3 && products != 6) return bad_arg(H, 1);
+  if (!shape_fits(m, n, k)) return CORAL_ERR_NOT_SUPPORTED;
   if (!tile_m) return bad_arg(H, 7);
   if (!tile_n) return bad_arg(H, 8);
   if (!split_k) return bad_arg(H, 9);
@@ -649,6 +657,7 @@ coral_status_t coral_get_gemm_config(coral_handle_t hh, int products, int op_a, 
                                      size_t n, size_t k, int* tile_n, int* split_k) {
   CORAL_HANDLE(hh);
   if (products != 3 && products != 6) return bad_arg(H, 1);
+  if (!shape_fits(m, n, k)) return CORAL_ERR_NOT_SUPPORTED;
   if (!tile_n) return bad_arg(H, 7);
   if (!split_k) return bad_arg(H, 8);
   SplitConfig c = choose_split_config(H, SplitShape{(int)m, (int)n, (int)k, products, op_a, op_b, 0, 1});
@@ -659,15 +668,17 @@ coral_status_t coral_get_gemm_config(coral_handle_t hh, int products, int op_a, 
 
 coral_status_t coral_selector_features(int products, int op_a, int op_b, size_t m, size_t n, size_t k,
                                        int tile_n, int split_k, float* out) {
-  if (!out) return CORAL_ERR_INVALID_ARG;
+  if (!out || tile_n <= 0 || split_k <= 0) return CORAL_ERR_INVALID_ARG;
+  if (!shape_fits(m, n, k)) return CORAL_ERR_NOT_SUPPORTED;
   selector_features(SplitShape{(int)m, (int)n, (int)k, products, op_a, op_b, 0, 1}, 128, tile_n, split_k, out);
   return CORAL_OK;
 }
 
 coral_status_t coral_selector_features_tile(int products, int op_a, int op_b, size_t m, size_t n, size_t k,
                                             int tile_m, int tile_n, int split_k, float* out) {
-  if (!out) return CORAL_ERR_INVALID_ARG;
+  if (!out || tile_n <= 0 || split_k <= 0) return CORAL_ERR_INVALID_ARG;
   if (tile_m != 128 && tile_m != 256) return CORAL_ERR_INVALID_ARG;
+  if (!shape_fits(m, n, k)) return CORAL_ERR_NOT_SUPPORTED;
   selector_features(SplitShape{(int)m, (int)n, (int)k, products, op_a, op_b, 0, 1}, tile_m, tile_n, split_k,
                     out);
   return CORAL_OK;

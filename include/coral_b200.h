@@ -484,7 +484,9 @@ coral_status_t coral_set_pair_raster(coral_handle_t h, int group);
 /* The configuration a split-BF16 SGEMM of this shape would use now. */
 coral_status_t coral_get_gemm_config(coral_handle_t h, int products, int op_a, int op_b, size_t m,
                                      size_t n, size_t k, int* tile_n, int* split_k);
-/* Features the selector network sees for (shape, configuration); 13 floats. */
+/* Features the selector network sees for (shape, configuration); 13 floats.
+ * Needs no device.  tile_n and split_k must be positive; sides past INT_MAX
+ * return CORAL_ERR_NOT_SUPPORTED (as the GEMM entry points do). */
 coral_status_t coral_selector_features(int products, int op_a, int op_b, size_t m, size_t n,
                                        size_t k, int tile_n, int split_k, float* out);
 /* Exhaustive autotuning of one split-BF16 SGEMM shape on the given device
@@ -508,7 +510,8 @@ coral_status_t coral_autotune_sgemm_tiles(coral_handle_t h, int products, int op
                                           size_t n, size_t k, const float* a, size_t lda, const float* b,
                                           size_t ldb, float* c, size_t ldc, int reps, float* ms_out,
                                           int capacity, int* count, int* best);
-/* Selector features of (shape, tile_m x tile_n, split_k); 13 floats. */
+/* Selector features of (shape, tile_m x tile_n, split_k); 13 floats.  Same
+ * checks, and tile_m must be 128 or 256. */
 coral_status_t coral_selector_features_tile(int products, int op_a, int op_b, size_t m, size_t n,
                                             size_t k, int tile_m, int tile_n, int split_k, float* out);
 

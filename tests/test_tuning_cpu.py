@@ -57,3 +57,24 @@ def test_candidates_and_validity():
 def test_regret_definition():
     t = np.array([[1.0, 2.0], [4.0, 2.0]])
     np.testing.assert_allclose(tuning.regret(t, np.array([0, 0])), [0.0, 1.0])
+
+
+def test_selector_features_reject_bad_arguments():
+    """The feature entry points need no device; they refuse sides past
+    INT_MAX (not supported, as the GEMM entry points) and non-positive tile
+    widths or split counts (invalid), instead of returning inf/NaN
+    features."""
+    import ctypes
+
+    from coral_b200 import _lib
+    lib = _lib.load()
+    out = (ctypes.c_float * 13)()
+    ok, invalid, unsupported = 0, 1, 5
+    assert lib.coral_selector_features_tile(3, 0, 0, 1024, 1024, 1024, 256, 256, 1, out) == ok
+    assert all(abs(v) < 10 for v in out)
+    assert lib.coral_selector_features_tile(3, 0, 0, 2**31, 1024, 1024, 128, 256, 1, out) == unsupported
+    assert lib.coral_selector_features_tile(3, 0, 0, 1024, 1024, 1024, 128, 0, 1, out) == invalid
+    assert lib.coral_selector_features_tile(3, 0, 0, 1024, 1024, 1024, 128, 256, 0, out) == invalid
+    assert lib.coral_selector_features_tile(3, 0, 0, 1024, 1024, 1024, 64, 256, 1, out) == invalid
+    assert lib.coral_selector_features(3, 0, 0, 1024, 1024, 2**40, 256, 1, out) == unsupported
+    assert lib.coral_selector_features(3, 0, 0, 1024, 1024, 1024, -1, 1, out) == invalid
